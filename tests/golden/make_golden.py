@@ -1,0 +1,76 @@
+"""Generate the golden fixtures in this directory from the reference itself.
+
+Runs the reference IBPM library (oracle/_ref/ref_driver_parity, built from the
+reference sources by oracle/Makefile with the project's FFTW shim) on small
+seeded cases and stores per-step forces and the final state as .npz.
+
+Usage (from the repository root, with the reference sources present):
+    make -C oracle all && python tests/golden/make_golden.py
+"""
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+from ibpm_b200 import configs  # noqa: E402
+from oracle import ibpm_oracle as O  # noqa: E402
+
+DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver_parity")
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+CASES = [
+    # name, nx, ny, ngrid, length, xoff, yoff, geom, Re, dt, nsteps, scheme, tol, noise(amp, seed)
+    ("cyl_l1_rk3", 48, 48, 1, 4.0, -2.0, -2.0, configs.cylinder_geom(36), 100.0, 0.02, 8, "rk3", 1e-7, None),
+    ("cyl_l3_noise_rk3", 64, 32, 3, 4.0, -1.5, -1.0, configs.cylinder_geom(32, r=0.4), 200.0, 0.01, 8, "rk3",
+     1e-7, (1e-3, 7)),
+    ("cyl_l2_euler", 32, 32, 2, 3.0, -1.5, -1.5, configs.cylinder_geom(24, r=0.4), 150.0, 0.02, 6, "euler",
+     1e-7, (1e-2, 3)),
+    ("cyl_l2_ab2", 32, 32, 2, 3.0, -1.5, -1.5, configs.cylinder_geom(24, r=0.4), 150.0, 0.02, 6, "ab2",
+     1e-7, (1e-2, 3)),
+    ("plate_l2_pitchplunge_cg", 64, 32, 2, 4.0, -2.0, -1.0,
+     configs.plate_geom(chord=1.0, npts=17, freq=0.5), 300.0, 0.01, 6, "rk3", 1e-10, None),
+    ("cyl_l1_rk3b", 40, 40, 1, 4.0, -2.0, -2.0, configs.cylinder_geom(30), 80.0, 0.02, 5, "rk3b", 1e-7, None),
+]
+
+
+def run(case):
+    name, nx, ny, ngrid, length, xoff, yoff, geom, Re, dt, nsteps, scheme, tol, noise = case
+    with tempfile.TemporaryDirectory() as td:
+        gpath = os.path.join(td, "body.geom")
+        with open(gpath, "w") as fh:
+            fh.write(geom)
+        args = [DRIVER, "-nx", str(nx), "-ny", str(ny), "-ngrid", str(ngrid), "-length", repr(length),
+                "-xoffset", repr(xoff), "-yoffset", repr(yoff), "-geom", gpath, "-Re", repr(Re),
+                "-dt", repr(dt), "-scheme", scheme, "-nsteps", str(nsteps), "-tol", repr(tol),
+                "-out", os.path.join(td, "run")]
+        w0 = None
+        if noise is not None:
+            wl = configs.Workload(name, nx, ny, ngrid, length, xoff, yoff, geom, Re, dt, nsteps,
+                                  noise_amp=noise[0], noise_seed=noise[1], noise_box=(0.0, 1e9, -0.8, 0.8))
+            w0 = wl.initial_vorticity()
+            g = O.Grid(nx, ny, ngrid, length, xoff, yoff)
+            from ibpm_b200 import geometry
+            npts = geometry.parse(geom).num_points
+            st = O.State(g, npts, omega=w0)
+            ic = os.path.join(td, "ic.bin")
+            O.save_restart(ic, st, g)
+            args += ["-ic", ic]
+        subprocess.run(args, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        forces = np.loadtxt(os.path.join(td, "run.forces")).reshape(-1, 6)
+        fin = O.load_restart(os.path.join(td, "run_final.bin"))
+    np.savez_compressed(
+        os.path.join(HERE, name + ".npz"),
+        nx=nx, ny=ny, ngrid=ngrid, length=length, xoffset=xoff, yoffset=yoff, geom=geom, Re=Re, dt=dt,
+        nsteps=nsteps, scheme=scheme, tol=tol,
+        omega0=(w0 if w0 is not None else np.zeros((ngrid, nx - 1, ny - 1))),
+        forces=forces, omega=fin["omega"], q=fin["q"], f=fin["f"], timestep=fin["timestep"], time=fin["time"])
+    print(name, "written", forces[-1, 2:4])
+
+
+if __name__ == "__main__":
+    for c in CASES:
+        run(c)

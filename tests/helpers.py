@@ -1,0 +1,48 @@
+"""Shared test helpers: golden fixtures, oracle construction, tolerances."""
+import glob
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+GOLDEN_DIR = os.path.join(ROOT, "tests", "golden")
+
+# FP64 parity bar against the reference (relative L2 / relative max for forces)
+FP64_TOL = 1e-10
+
+
+def golden_names():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+
+
+def load_golden(name):
+    z = np.load(os.path.join(GOLDEN_DIR, name + ".npz"), allow_pickle=False)
+    return {k: (z[k].item() if z[k].ndim == 0 else z[k]) for k in z.files}
+
+
+def oracle_from_golden(d):
+    from oracle import ibpm_oracle as O
+    from ibpm_b200 import geometry
+    g = O.Grid(int(d["nx"]), int(d["ny"]), int(d["ngrid"]), float(d["length"]), float(d["xoffset"]),
+               float(d["yoffset"]))
+    geo = geometry.parse(str(d["geom"]))
+    bodies = []
+    for b in geo.bodies:
+        motion = {0: "none", 1: "fixed", 2: "pitchplunge"}[b.motion]
+        params = b.params[:3] if motion == "fixed" else tuple(b.params)
+        bodies.append(O.Body(np.array(b.points, dtype=float), tuple(b.center), motion, params))
+    model = O.Model(g, bodies, float(d["Re"]))
+    solver = O.IBSolver(model, float(d["dt"]), str(d["scheme"]), float(d["tol"]))
+    x = O.State(g, model.npts, omega=np.array(d["omega0"], dtype=float))
+    return g, model, solver, x
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    nb = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
