@@ -1,0 +1,273 @@
+"""B200-native IBPM time step.
+
+Host side of the C ABI in ``include/ibpm_b200.h``; the names mirror the
+reference's classes (paths inside the reference project):
+
+* ``Grid``                 src/Grid.h
+* ``State``                src/State.h (omega, q, f, timestep, time; computeNetForce)
+* ``NavierStokesModel``    src/NavierStokesModel.h (Reynolds number, base flow, geometry)
+* ``NonlinearIBSolver``    src/IBSolver.h (init/load/save/advance)
+* ``PoissonSolver`` / ``HelmholtzSolver``  src/EllipticSolver.h
+
+The compute path is the CUDA library ``libibpm_b200.so``; nothing here
+computes on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import geometry as _geometry
+from ._native import (PRECISIONS, SCHEMES, IbgError, check, ibg_body, ibg_grid, ibg_params, lib)
+
+__all__ = ["Grid", "State", "NavierStokesModel", "NonlinearIBSolver", "IbgError", "geometry"]
+geometry = _geometry
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+@dataclass
+class Grid:
+    """Grid(nx, ny, ngrid, length, xoffset, yoffset) (src/Grid.h:36-44)."""
+    nx: int
+    ny: int
+    ngrid: int
+    length: float
+    xoffset: float
+    yoffset: float
+
+    @property
+    def dx(self) -> float:
+        return self.length / self.nx
+
+    @property
+    def n_scalar(self) -> int:
+        return self.ngrid * (self.nx - 1) * (self.ny - 1)
+
+    @property
+    def n_flux(self) -> int:
+        return self.ngrid * (2 * self.nx * self.ny + self.nx + self.ny)
+
+    def scalar(self) -> np.ndarray:
+        return np.zeros((self.ngrid, self.nx - 1, self.ny - 1))
+
+    def flux(self) -> np.ndarray:
+        return np.zeros((self.ngrid, 2 * self.nx * self.ny + self.nx + self.ny))
+
+
+@dataclass
+class State:
+    """State (src/State.h): vorticity, flux, boundary force, timestep, time."""
+    grid: Grid
+    npoints: int
+    omega: np.ndarray = None
+    q: np.ndarray = None
+    f: np.ndarray = None
+    timestep: int = 0
+    time: float = 0.0
+
+    def __post_init__(self):
+        if self.omega is None:
+            self.omega = self.grid.scalar()
+        if self.q is None:
+            self.q = self.grid.flux()
+        if self.f is None:
+            self.f = np.zeros(2 * self.npoints)
+
+    def computeNetForce(self):
+        """State::computeNetForce (src/State.cc:53-63)."""
+        n = self.npoints
+        dx2 = self.grid.dx * self.grid.dx
+        return float(self.f[:n].sum() * dx2), float(self.f[n:].sum() * dx2)
+
+
+@dataclass
+class NavierStokesModel:
+    """NavierStokesModel(grid, geometry, Re, q_potential) (src/NavierStokesModel.h:35-122);
+    the base flow is uniform with magnitude `u_mag` and angle `alpha` (radians)."""
+    grid: Grid
+    geom: _geometry.Geometry
+    Re: float
+    u_mag: float = 1.0
+    alpha: float = 0.0
+
+    def getAlpha(self) -> float:
+        return 1.0 / self.Re
+
+    def getNumPoints(self) -> int:
+        return self.geom.num_points
+
+
+class NonlinearIBSolver:
+    """NonlinearIBSolver(grid, model, dt, scheme, tol) (src/IBSolver.h:69-90) on the GPU.
+
+    ``advance(x)`` keeps the reference's contract (the host State is valid
+    after every call); ``advance_resident(n)`` steps the device-resident state
+    without host traffic.
+    """
+
+    def __init__(self, grid: Grid, model: NavierStokesModel, dt: float, scheme: str = "rk3", tol: float = 1e-7,
+                 precision: str = "fp64", stream: Optional[int] = None, cg_max_iter: int = 3000):
+        self.grid, self.model, self.dt = grid, model, dt
+        self.scheme = scheme
+        L = lib()
+        g = ibg_grid(grid.nx, grid.ny, grid.ngrid, grid.length, grid.xoffset, grid.yoffset)
+        self._keep = []
+        bodies = (ibg_body * len(model.geom.bodies))()
+        for k, b in enumerate(model.geom.bodies):
+            xy = np.ascontiguousarray(np.array(b.points, dtype=np.float64).reshape(-1))
+            self._keep.append(xy)
+            bodies[k].npoints = len(b.points)
+            bodies[k].xy = xy.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            bodies[k].xcenter, bodies[k].ycenter = b.center
+            bodies[k].motion = b.motion
+            for j in range(6):
+                bodies[k].params[j] = b.params[j] if j < len(b.params) else 0.0
+        p = ibg_params(model.Re, dt, SCHEMES[scheme], tol, cg_max_iter, model.u_mag, model.alpha,
+                       PRECISIONS[precision])
+        h = ctypes.c_void_p()
+        check(L.ibg_create(ctypes.byref(g), len(model.geom.bodies), bodies, ctypes.byref(p),
+                           ctypes.c_void_p(stream) if stream else None, ctypes.byref(h)), None)
+        self._h = h
+        self.npoints = model.geom.num_points
+        self._synced = None
+
+    # -- lifetime -----------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ibg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -- IBSolver interface -------------------------------------------------
+    def init(self):
+        check(lib().ibg_init(self._h), self._h)
+
+    def load(self, basename: str) -> bool:
+        return check(lib().ibg_load(self._h, basename.encode()), self._h) == 1
+
+    def save(self, basename: str) -> bool:
+        return check(lib().ibg_save(self._h, basename.encode()), self._h) == 1
+
+    def getTimestep(self) -> float:
+        return self.dt
+
+    def set_state(self, x: State, with_q: bool = True):
+        om = np.ascontiguousarray(x.omega, dtype=np.float64)
+        q = np.ascontiguousarray(x.q, dtype=np.float64) if with_q else None
+        f = np.ascontiguousarray(x.f, dtype=np.float64)
+        check(lib().ibg_set_state(self._h, _ptr(om), _ptr(q), _ptr(f), int(x.timestep), float(x.time)), self._h)
+        self._synced = x
+
+    def get_state(self, x: State):
+        om = np.empty(x.omega.shape)
+        q = np.empty(x.q.shape)
+        f = np.empty(x.f.shape)
+        ts = ctypes.c_int()
+        t = ctypes.c_double()
+        check(lib().ibg_get_state(self._h, _ptr(om), _ptr(q), _ptr(f), ctypes.byref(ts), ctypes.byref(t)), self._h)
+        x.omega, x.q, x.f, x.timestep, x.time = om, q, f, ts.value, t.value
+
+    def update_operators(self, time: float):
+        check(lib().ibg_update_operators(self._h, float(time)), self._h)
+
+    def refresh_state(self, x: State):
+        """model->refreshState(x): q from omega on the device."""
+        self.set_state(x, with_q=False)
+        self.get_state(x)
+
+    def advance(self, x: State):
+        """IBSolver::advance(State&) (src/IBSolver.cc:142-149)."""
+        if self._synced is not x:
+            self.set_state(x)
+        check(lib().ibg_advance(self._h, 1), self._h)
+        self.get_state(x)
+
+    def advance_resident(self, nsteps: int = 1):
+        check(lib().ibg_advance(self._h, int(nsteps)), self._h)
+
+    def force_history(self, n: int) -> np.ndarray:
+        out = np.zeros((n, 2))
+        k = check(lib().ibg_get_force_history(self._h, n, _ptr(out)), self._h)
+        return out[:k]
+
+    def net_force(self):
+        a, b = ctypes.c_double(), ctypes.c_double()
+        check(lib().ibg_get_net_force(self._h, ctypes.byref(a), ctypes.byref(b)), self._h)
+        return a.value, b.value
+
+    def cg_stats(self):
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib().ibg_cg_stats(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)), self._h)
+        return a.value, b.value, c.value
+
+    def stream(self) -> int:
+        return lib().ibg_stream(self._h) or 0
+
+    def last_launch_count(self) -> int:
+        return int(lib().ibg_last_launch_count(self._h))
+
+    # -- operators (host buffers) ------------------------------------------
+    def _op(self, name, *args, out_shape):
+        out = np.zeros(out_shape)
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) if isinstance(a, np.ndarray) else a for a in args]
+        cargs = [_ptr(a) if isinstance(a, np.ndarray) else a for a in arrs]
+        check(getattr(lib(), name)(self._h, *cargs, _ptr(out)), self._h)
+        return out
+
+    def poisson(self, f):
+        return self._op("ibg_poisson_solve", f, out_shape=self.grid.scalar().shape)
+
+    def helmholtz(self, alpha, f):
+        return self._op("ibg_helmholtz_solve", ctypes.c_double(alpha), f, out_shape=self.grid.scalar().shape)
+
+    def nonlinear(self, q, w):
+        return self._op("ibg_nonlinear", q, w, out_shape=self.grid.scalar().shape)
+
+    def laplacian(self, f):
+        return self._op("ibg_laplacian", f, out_shape=self.grid.scalar().shape)
+
+    def model_B(self, f):
+        return self._op("ibg_model_B", f, out_shape=self.grid.scalar().shape)
+
+    def model_C(self, w):
+        return self._op("ibg_model_C", w, out_shape=(2 * self.npoints,))
+
+    def reg_to_boundary(self, q0):
+        return self._op("ibg_reg_to_boundary", q0, out_shape=(2 * self.npoints,))
+
+    def projection_solve(self, k, a, b, f0):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        f = np.ascontiguousarray(f0, dtype=np.float64).copy()
+        w = np.zeros(self.grid.scalar().shape)
+        check(lib().ibg_projection_solve(self._h, int(k), _ptr(a), _ptr(b), _ptr(w), _ptr(f)), self._h)
+        return w, f
+
+
+def from_workload(wl, precision: str = "fp64", stream=None):
+    """Grid, model, solver and initial State for an ibpm_b200.configs.Workload."""
+    grid = Grid(wl.nx, wl.ny, wl.ngrid, wl.length, wl.xoffset, wl.yoffset)
+    geo = _geometry.parse(wl.geom)
+    model = NavierStokesModel(grid, geo, wl.Re)
+    solver = NonlinearIBSolver(grid, model, wl.dt, wl.scheme, wl.tol, precision=precision, stream=stream)
+    x = State(grid, geo.num_points)
+    w0 = wl.initial_vorticity()
+    if w0 is not None:
+        x.omega = w0
+    return grid, model, solver, x

@@ -1,0 +1,97 @@
+"""ctypes binding of libibpm_b200.so (the C ABI in include/ibpm_b200.h).
+
+The library is built in-tree (``python -m ibpm_b200.build``).  Loading fails
+loudly when it is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libibpm_b200.so")
+
+c_double_p = ctypes.POINTER(ctypes.c_double)
+
+
+class ibg_grid(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("ngrid", ctypes.c_int),
+                ("length", ctypes.c_double), ("xoffset", ctypes.c_double), ("yoffset", ctypes.c_double)]
+
+
+class ibg_body(ctypes.Structure):
+    _fields_ = [("npoints", ctypes.c_int), ("xy", c_double_p), ("xcenter", ctypes.c_double),
+                ("ycenter", ctypes.c_double), ("motion", ctypes.c_int), ("params", ctypes.c_double * 6)]
+
+
+class ibg_params(ctypes.Structure):
+    _fields_ = [("Re", ctypes.c_double), ("dt", ctypes.c_double), ("scheme", ctypes.c_int),
+                ("cg_tol", ctypes.c_double), ("cg_max_iter", ctypes.c_int), ("u_mag", ctypes.c_double),
+                ("alpha", ctypes.c_double), ("precision", ctypes.c_int)]
+
+
+SCHEMES = {"euler": 0, "ab2": 1, "rk3": 2, "rk3b": 3}
+PRECISIONS = {"fp64": 0, "fp32_refined": 1}
+
+# every entry point declared in include/ibpm_b200.h: name -> (restype, argtypes)
+_VP = ctypes.c_void_p
+_I = ctypes.c_int
+_D = ctypes.c_double
+SIGNATURES = {
+    "ibg_create": (_I, [ctypes.POINTER(ibg_grid), _I, ctypes.POINTER(ibg_body), ctypes.POINTER(ibg_params), _VP,
+                        ctypes.POINTER(_VP)]),
+    "ibg_destroy": (_I, [_VP]),
+    "ibg_last_error": (ctypes.c_char_p, [_VP]),
+    "ibg_init": (_I, [_VP]),
+    "ibg_save": (_I, [_VP, ctypes.c_char_p]),
+    "ibg_load": (_I, [_VP, ctypes.c_char_p]),
+    "ibg_set_state": (_I, [_VP, _VP, _VP, _VP, _I, _D]),
+    "ibg_get_state": (_I, [_VP, _VP, _VP, _VP, ctypes.POINTER(_I), ctypes.POINTER(_D)]),
+    "ibg_get_boundary_force": (_I, [_VP, _VP, ctypes.POINTER(_I), ctypes.POINTER(_D)]),
+    "ibg_update_operators": (_I, [_VP, _D]),
+    "ibg_refresh_state": (_I, [_VP]),
+    "ibg_advance": (_I, [_VP, _I]),
+    "ibg_get_net_force": (_I, [_VP, ctypes.POINTER(_D), ctypes.POINTER(_D)]),
+    "ibg_get_force_history": (_I, [_VP, _I, _VP]),
+    "ibg_sizes": (_I, [_VP, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
+                       ctypes.POINTER(_I)]),
+    "ibg_cg_stats": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "ibg_stream": (_VP, [_VP]),
+    "ibg_last_launch_count": (ctypes.c_longlong, [_VP]),
+    "ibg_poisson_solve": (_I, [_VP, _VP, _VP]),
+    "ibg_helmholtz_solve": (_I, [_VP, _D, _VP, _VP]),
+    "ibg_nonlinear": (_I, [_VP, _VP, _VP, _VP]),
+    "ibg_laplacian": (_I, [_VP, _VP, _VP]),
+    "ibg_model_B": (_I, [_VP, _VP, _VP]),
+    "ibg_model_C": (_I, [_VP, _VP, _VP]),
+    "ibg_reg_to_boundary": (_I, [_VP, _VP, _VP]),
+    "ibg_projection_solve": (_I, [_VP, _I, _VP, _VP, _VP, _VP]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load the library (raises OSError if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is missing: build it with `python -m ibpm_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+class IbgError(RuntimeError):
+    pass
+
+
+def check(status: int, ctx=None) -> int:
+    if status < 0:
+        msg = lib().ibg_last_error(ctx)
+        raise IbgError(f"ibg status {status}: {msg.decode() if msg else ''}")
+    return status

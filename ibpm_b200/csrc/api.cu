@@ -1,0 +1,850 @@
+// api.cu -- the C ABI (include/ibpm_b200.h): context, state, time step.
+//
+// One context = one IBPM simulation resident in HBM: the reference's
+// NavierStokesModel + NonlinearIBSolver + State (src/NavierStokesModel.*,
+// src/IBSolver.*, src/State.*).  A time step is a fixed sequence of kernel
+// launches on one stream; for fixed bodies the whole step is captured once
+// into a CUDA graph and replayed.  Moving bodies use CG, whose convergence
+// test is read back every few iterations.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/ibpm_b200.h"
+#include "ibg_force.cuh"
+#include "ibg_internal.cuh"
+#include "ibg_kernels.cuh"
+#include "ibg_ops.cuh"
+
+using namespace ibg;
+
+namespace {
+thread_local std::string g_create_error;
+
+struct Scheme {
+    int nsub;
+    double an[4], bn[4], cn[4];
+};
+
+// coefficients of src/Scheme.h:13-61
+Scheme make_scheme(int s) {
+    Scheme r{};
+    if (s == IBG_SCHEME_EULER) {
+        r.nsub = 1;
+        r.an[0] = 1.; r.bn[0] = 0.; r.cn[0] = 1.;
+    } else if (s == IBG_SCHEME_AB2) {
+        r.nsub = 1;
+        r.an[0] = 3. / 2.; r.bn[0] = -1. / 2.; r.cn[0] = 1.;
+    } else if (s == IBG_SCHEME_RK3) {
+        r.nsub = 3;
+        r.an[0] = 8. / 15.; r.an[1] = 5. / 12.; r.an[2] = 3. / 4.;
+        r.bn[0] = 0.; r.bn[1] = -17. / 60.; r.bn[2] = -5. / 12.;
+        r.cn[0] = 8. / 15.; r.cn[1] = 2. / 3.; r.cn[2] = 1.;
+    } else if (s == IBG_SCHEME_RK3B) {
+        r.nsub = 4;
+        r.an[0] = 8. / 17.; r.an[1] = 17. / 60.; r.an[2] = 5. / 12.; r.an[3] = 3. / 4.;
+        r.bn[0] = 0.; r.bn[1] = -15. / 68.; r.bn[2] = -17. / 60.; r.bn[3] = -5. / 12.;
+        r.cn[0] = 8. / 17.; r.cn[1] = 8. / 15.; r.cn[2] = 2. / 3.; r.cn[3] = 1.;
+    } else {
+        r.nsub = 0;
+    }
+    return r;
+}
+
+constexpr int kHistCap = 1 << 16;
+}  // namespace
+
+struct ibg_context {
+    // configuration
+    GridDev g{};
+    size_t S = 0, F = 0;
+    ibg_params prm{};
+    Scheme sch{};
+    double u0 = 0, v0 = 0;
+    int npts = 0, ncomp = 0;
+    bool moving = false;
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+    std::string err;
+    // plans
+    FftTables fft;
+    CosTables cosT;
+    EllipticPlan<double> poisson;
+    EllipticPlan<double> helm[4];
+    double beta[4] = {0, 0, 0, 0};
+    // bodies
+    std::vector<BodyDev> h_bodies;
+    std::vector<double> h_ref;
+    double *d_ref = nullptr, *d_pts = nullptr, *d_vel = nullptr;
+    int* d_body_of = nullptr;
+    BodyDev* d_bodies = nullptr;
+    RegSlots slots;
+    double* d_b = nullptr;
+    double* d_time = nullptr;
+    // state
+    double *w = nullptr, *q = nullptr, *f = nullptr;
+    int timestep = 0;
+    double time = 0;
+    bool old_saved = false;
+    // work
+    double* Nbuf[4] = {nullptr, nullptr, nullptr, nullptr};
+    int nring = 0;
+    double *a = nullptr, *ws = nullptr, *psi = nullptr, *cc = nullptr, *rc = nullptr, *tbuf = nullptr;
+    double *U = nullptr, *V = nullptr, *C = nullptr, *flux0 = nullptr, *Bf = nullptr;
+    double *rhsb = nullptr, *btmp = nullptr, *qtmp = nullptr;
+    // Cholesky factors per sub-step
+    double* Lr[4] = {nullptr, nullptr, nullptr, nullptr};
+    double* Lc[4] = {nullptr, nullptr, nullptr, nullptr};
+    double* Ld[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool chol_ready = false;
+    int* d_status = nullptr;
+    // CG
+    double *cg_r = nullptr, *cg_d = nullptr, *cg_q = nullptr, *cg_scal = nullptr;
+    int* cg_flags = nullptr;
+    int* h_flags = nullptr;  // pinned
+    int cg_last = 0, cg_max = 0, cg_capped = 0;
+    // force history
+    double* d_hist = nullptr;
+    int* d_hist_count = nullptr;
+    long long hist_steps = 0;
+    // graph
+    cudaGraphExec_t graph = nullptr;
+    long long graph_launches = 0;
+    long long launches = 0;
+    long long last_launches = 0;
+
+    ~ibg_context() { release(); }
+
+    int fail(int code, const std::string& m) {
+        err = m;
+        return code;
+    }
+    int cuda_check(const char* where) {
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return fail(IBG_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+        return IBG_OK;
+    }
+
+    template <typename P>
+    int alloc(P** p, size_t n, bool zero = true) {
+        if (n == 0) n = 1;
+        if (cudaMalloc((void**)p, sizeof(P) * n) != cudaSuccess) return fail(IBG_ERR_CUDA, "cudaMalloc failed");
+        if (zero) cudaMemset(*p, 0, sizeof(P) * n);
+        return IBG_OK;
+    }
+
+    void release() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        void* ptrs[] = {d_ref, d_pts, d_vel, d_body_of, d_bodies, slots.idx, slots.w, slots.n, d_b, d_time, w, q, f,
+                        a, ws, psi, cc, rc, tbuf, U, V, C, flux0, Bf, rhsb, btmp, d_status, cg_r, cg_d, cg_q,
+                        cg_scal, cg_flags, d_hist, d_hist_count, qtmp};
+        for (void* p : ptrs)
+            if (p) cudaFree(p);
+        for (int k = 0; k < 4; ++k) {
+            if (Nbuf[k]) cudaFree(Nbuf[k]);
+            if (Lr[k]) cudaFree(Lr[k]);
+            if (Lc[k]) cudaFree(Lc[k]);
+            if (Ld[k]) cudaFree(Ld[k]);
+            Nbuf[k] = Lr[k] = Lc[k] = Ld[k] = nullptr;
+        }
+        if (h_flags) cudaFreeHost(h_flags);
+        h_flags = nullptr;
+        fft.release();
+        cosT.release();
+        if (own_stream && st) cudaStreamDestroy(st);
+        st = nullptr;
+        d_ref = d_pts = d_vel = nullptr;
+        d_body_of = nullptr;
+        d_bodies = nullptr;
+        slots = RegSlots{};
+        d_b = d_time = w = q = f = a = ws = psi = cc = rc = tbuf = U = V = C = flux0 = Bf = rhsb = btmp = qtmp = nullptr;
+        d_status = nullptr;
+        cg_r = cg_d = cg_q = cg_scal = nullptr;
+        cg_flags = nullptr;
+        d_hist = nullptr;
+        d_hist_count = nullptr;
+    }
+
+    // -----------------------------------------------------------------------
+    SolveCall<double> call(const double* fin, double* uout, double scale, double* out2 = nullptr,
+                           const double* base = nullptr) {
+        SolveCall<double> c{};
+        c.f = fin;
+        c.u = uout;
+        c.rc = rc;
+        c.tbuf = tbuf;
+        c.bstride = S;
+        c.batch = 1;
+        c.in_scale = scale;
+        c.out2 = out2;
+        c.base = base;
+        return c;
+    }
+    long long solve_launches() const { return (g.L - 1) + 3LL * g.L; }
+
+    // M d = C A^-1 B d  (src/ProjectionSolver.cc:96-101)
+    void m_apply(int k, const double* din, double* dout) {
+        launch_smear_bf<double>(g, ncomp, slots, din, flux0, Bf, beta[k], st);
+        helm[k].solve(call(Bf, cc, 1.0), st);
+        poisson.solve(call(cc, psi, -1.0), st);
+        launch_reg_interp<double>(g, ncomp, slots, psi, S, 1, nullptr, dout, 0, st);
+        launches += 3 + 2 * solve_launches() + 1;
+    }
+
+    // CG with warm start x = f (src/ConjugateGradientSolver.cc:35-65); host reads the
+    // convergence flag every `chunk` iterations.
+    int cg_solve(int k, const double* b, double* x) {
+        m_apply(k, x, cg_q);
+        cg_begin(ncomp, b, cg_q, cg_r, cg_d, cg_scal, cg_flags, st);
+        launches += 1;
+        int chunk = cg_last > 4 ? cg_last - 2 : 4;
+        int done_iters = 0;
+        for (;;) {
+            for (int c = 0; c < chunk; ++c) {
+                m_apply(k, cg_d, cg_q);
+                cg_update(ncomp, x, cg_r, cg_d, cg_q, cg_scal, cg_flags, st);
+                launches += 1;
+            }
+            done_iters += chunk;
+            cudaMemcpyAsync(h_flags, cg_flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st);
+            if (cudaStreamSynchronize(st) != cudaSuccess) return cuda_check("cg");
+            if (h_flags[0] == 0) break;
+            if (done_iters > prm.cg_max_iter + chunk) break;
+            chunk = 4;
+        }
+        cg_last = h_flags[1];
+        if (cg_last > cg_max) cg_max = cg_last;
+        if (cg_last >= prm.cg_max_iter) ++cg_capped;
+        return IBG_OK;
+    }
+
+    // the projection of one sub-step (src/ProjectionSolver.cc:57-79) given a and b
+    int projection(int k, const double* a_in, const double* b_in) {
+        helm[k].solve(call(a_in, ws, 1.0), st);                          // omega* = A^-1 a
+        poisson.solve(call(ws, psi, -1.0), st);                          // psi* = L^-1(-omega*)
+        launch_reg_interp<double>(g, ncomp, slots, psi, S, 1, b_in, rhsb, 0, st);  // C omega* - b
+        launches += 2 * solve_launches() + 1;
+        if (!moving) {
+            chol_solve(ncomp, Lr[k], Lc[k], Ld[k], rhsb, f, st);        // f = M^-1 rhs
+            launches += 1;
+        } else {
+            int s = cg_solve(k, rhsb, f);
+            if (s) return s;
+        }
+        launch_smear_bf<double>(g, ncomp, slots, f, flux0, Bf, beta[k], st);  // B f
+        helm[k].solve(call(Bf, cc, 1.0, w, ws), st);                    // omega = omega* - A^-1 B f
+        launches += 3 + solve_launches();
+        return IBG_OK;
+    }
+
+    // q = Curl(L^-1(-omega)) + q0 (src/NavierStokesModel.cc:121-140)
+    void refresh() {
+        poisson.solve(call(w, psi, -1.0), st);
+        launch_refresh_flux<double>(g, psi, q, u0, v0, st);
+        launches += solve_launches() + 1;
+    }
+
+    void move_bodies(double toff) {
+        launch_kinematics(npts, d_ref, d_body_of, d_bodies, d_time, toff, d_pts, d_vel, st);
+        launch_reg_update(g, npts, d_pts, d_vel, slots, d_b, u0, v0, st);
+        launches += 2;
+    }
+
+    // IBSolver::advanceSubstep (src/IBSolver.cc:162-198)
+    int substep(int k) {
+        const double an = sch.an[k], bn = sch.bn[k], cn = sch.cn[k];
+        double* Nk;
+        double* Np;
+        if (sch.nsub == 1) {
+            Nk = Nbuf[0];
+            Np = Nbuf[1];
+        } else {
+            Nk = Nbuf[k];
+            Np = Nbuf[(k + sch.nsub - 1) % sch.nsub];
+        }
+        launch_nonlinear<double>(g, q, w, U, V, C, Nk, 1, S, F, st);
+        launches += 2 + g.L;
+        if (moving) move_bodies(cn * prm.dt);
+        const double* Nprev = nullptr;
+        if (bn != 0) Nprev = old_saved ? Np : Nk;
+        const double c1 = 0.5 * (1.0 / prm.Re) * (an + bn);
+        launch_rhs<double>(g, w, Nk, Nprev, a, c1, an, bn, prm.dt, st);
+        launches += 1;
+        int s = projection(k, a, d_b);
+        if (s) return s;
+        refresh();
+        if (sch.nsub == 1) {
+            cudaMemcpyAsync(Np, Nk, sizeof(double) * S, cudaMemcpyDeviceToDevice, st);
+            launches += 1;
+        }
+        old_saved = true;
+        return IBG_OK;
+    }
+
+    int enqueue_step() {
+        for (int k = 0; k < sch.nsub; ++k) {
+            int s = substep(k);
+            if (s) return s;
+        }
+        add_time(d_time, prm.dt, st);
+        net_force_record();
+        launches += 2;
+        return IBG_OK;
+    }
+
+    void net_force_record();
+};
+
+namespace ibg {
+__global__ void k_hist_force(int npts, const double* f, double dx2, double* hist, int* count) {
+    double sx = 0.0, sy = 0.0;
+    for (int k = threadIdx.x; k < npts; k += 32) {
+        sx += f[k];
+        sy += f[npts + k];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sx += __shfl_xor_sync(0xffffffffu, sx, o);
+        sy += __shfl_xor_sync(0xffffffffu, sy, o);
+    }
+    if (threadIdx.x == 0) {
+        const int i = *count;
+        hist[2 * (i % kHistCap)] = sx * dx2;
+        hist[2 * (i % kHistCap) + 1] = sy * dx2;
+        *count = i + 1;
+    }
+}
+}  // namespace ibg
+
+void ibg_context::net_force_record() {
+    ibg::k_hist_force<<<1, 32, 0, st>>>(npts, f, g.dx * g.dx, d_hist, d_hist_count);
+}
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* ibg_last_error(const ibg_context* ctx) {
+    if (!ctx) return g_create_error.c_str();
+    return ctx->err.c_str();
+}
+
+int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const ibg_params* params,
+               void* cuda_stream, ibg_context** out) {
+    if (!out || !grid || !params || (nbodies > 0 && !bodies) || nbodies < 1) {
+        g_create_error = "ibg_create: null argument or no bodies";
+        return IBG_ERR_ARG;
+    }
+    *out = nullptr;
+    const ibg_grid& G = *grid;
+    if (G.nx < 4 || G.ny < 4 || G.ngrid < 1 || G.ngrid > 16 || !(G.length > 0)) {
+        g_create_error = "ibg_create: invalid grid";
+        return IBG_ERR_ARG;
+    }
+    if (G.ngrid > 1 && (G.nx % 4 || G.ny % 4)) {
+        g_create_error = "ibg_create: nx and ny must be multiples of 4 when ngrid > 1";
+        return IBG_ERR_ARG;
+    }
+    Scheme sch = make_scheme(params->scheme);
+    if (sch.nsub == 0) {
+        g_create_error = "ibg_create: unknown scheme";
+        return IBG_ERR_ARG;
+    }
+    if (!(params->Re > 0) || !(params->dt > 0)) {
+        g_create_error = "ibg_create: Re and dt must be positive";
+        return IBG_ERR_ARG;
+    }
+    if (params->precision != IBG_PRECISION_FP64) {
+        g_create_error = "ibg_create: only IBG_PRECISION_FP64 is available in this build";
+        return IBG_ERR_UNSUPPORTED;
+    }
+    if (!fft_supported(2 * G.nx) || !fft_supported(2 * G.ny)) {
+        g_create_error = "ibg_create: 2*nx and 2*ny must factor into primes <= 13";
+        return IBG_ERR_UNSUPPORTED;
+    }
+    auto* c = new ibg_context();
+    c->prm = *params;
+    if (c->prm.cg_max_iter <= 0) c->prm.cg_max_iter = 3000;
+    if (!(c->prm.cg_tol > 0)) c->prm.cg_tol = 1e-7;
+    c->sch = sch;
+    GridDev& g = c->g;
+    g.nx = G.nx;
+    g.ny = G.ny;
+    g.L = G.ngrid;
+    g.nxe = (int)floor(G.nx / 4 * (1 - 0.0) + 0.5);  // src/Grid.h:60-62 with zero shift
+    g.nye = (int)floor(G.ny / 4 * (1 - 0.0) + 0.5);
+    g.NI = G.nx - 1;
+    g.NJ = G.ny - 1;
+    g.N1 = g.NI * g.NJ;
+    g.nXf = (G.nx + 1) * G.ny;
+    g.F1 = 2 * G.nx * G.ny + G.nx + G.ny;
+    g.dx = G.length / G.nx;
+    g.x0 = G.xoffset;
+    g.y0 = G.yoffset;
+    c->S = (size_t)g.L * g.N1;
+    c->F = (size_t)g.L * g.F1;
+    c->u0 = c->prm.u_mag * cos(c->prm.alpha);
+    c->v0 = c->prm.u_mag * sin(c->prm.alpha);
+    // bodies
+    const double twopi = 8. * atan(1.);
+    std::vector<int> body_of;
+    for (int b = 0; b < nbodies; ++b) {
+        const ibg_body& B = bodies[b];
+        if (B.npoints < 1 || !B.xy) {
+            delete c;
+            g_create_error = "ibg_create: body without points";
+            return IBG_ERR_ARG;
+        }
+        BodyDev d{};
+        d.xc = B.xcenter;
+        d.yc = B.ycenter;
+        d.motion = B.motion;
+        for (int k = 0; k < 6; ++k) d.p[k] = B.params[k];
+        if (B.motion == IBG_MOTION_PITCHPLUNGE) {
+            d.p[1] *= twopi;  // PitchPlunge stores 2 pi f (src/PitchPlunge.h:38-40)
+            d.p[4] *= twopi;
+            c->moving = true;
+        } else if (B.motion != IBG_MOTION_NONE && B.motion != IBG_MOTION_FIXED) {
+            delete c;
+            g_create_error = "ibg_create: unsupported motion type";
+            return IBG_ERR_UNSUPPORTED;
+        }
+        c->h_bodies.push_back(d);
+        for (int p = 0; p < B.npoints; ++p) {
+            c->h_ref.push_back(B.xy[2 * p]);
+            c->h_ref.push_back(B.xy[2 * p + 1]);
+            body_of.push_back(b);
+        }
+    }
+    c->npts = (int)body_of.size();
+    c->ncomp = 2 * c->npts;
+    if (c->ncomp > 16384) {
+        delete c;
+        g_create_error = "ibg_create: too many boundary points";
+        return IBG_ERR_UNSUPPORTED;
+    }
+    // stream
+    if (cuda_stream) {
+        c->st = (cudaStream_t)cuda_stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) {
+            delete c;
+            g_create_error = "ibg_create: no CUDA device or stream creation failed";
+            return IBG_ERR_CUDA;
+        }
+        c->own_stream = true;
+    }
+    int s = IBG_OK;
+    const size_t S = c->S, F = c->F, m = c->ncomp;
+    if ((s = c->fft.init(2 * g.ny, 2 * g.nx)) || (s = c->cosT.init(g.nx, g.ny))) {
+        g_create_error = "ibg_create: FFT table setup failed";
+        delete c;
+        return s;
+    }
+    s = c->poisson.init(&c->g, &c->fft, false, 0.0, c->cosT);
+    for (int k = 0; k < sch.nsub && !s; ++k) {
+        c->beta[k] = (sch.an[k] + sch.bn[k]) * c->prm.dt;           // src/IBSolver.cc:110-114
+        const double alpha = -c->beta[k] / 2. * (1. / c->prm.Re);    // src/ProjectionSolver.cc:33
+        s = c->helm[k].init(&c->g, &c->fft, true, alpha, c->cosT);
+    }
+    if (s) {
+        g_create_error = "ibg_create: solver plan setup failed";
+        delete c;
+        return s;
+    }
+    c->nring = sch.nsub == 1 ? 2 : sch.nsub;
+    s = s || c->alloc(&c->w, S) || c->alloc(&c->q, F) || c->alloc(&c->f, m) || c->alloc(&c->a, S) ||
+        c->alloc(&c->ws, S) || c->alloc(&c->psi, S) || c->alloc(&c->cc, S) || c->alloc(&c->rc, S) ||
+        c->alloc(&c->tbuf, (size_t)g.N1) || c->alloc(&c->U, S) || c->alloc(&c->V, S) || c->alloc(&c->C, F) ||
+        c->alloc(&c->flux0, (size_t)g.F1) || c->alloc(&c->Bf, S) || c->alloc(&c->rhsb, m) ||
+        c->alloc(&c->btmp, m) || c->alloc(&c->qtmp, F) || c->alloc(&c->d_ref, 2 * (size_t)c->npts) ||
+        c->alloc(&c->d_pts, 2 * (size_t)c->npts) || c->alloc(&c->d_vel, 2 * (size_t)c->npts) ||
+        c->alloc(&c->d_body_of, (size_t)c->npts) || c->alloc(&c->d_bodies, c->h_bodies.size()) ||
+        c->alloc(&c->slots.idx, 9 * m) || c->alloc(&c->slots.w, 9 * m) || c->alloc(&c->slots.n, m) ||
+        c->alloc(&c->d_b, m) || c->alloc(&c->d_time, 1) || c->alloc(&c->d_status, 1) || c->alloc(&c->cg_r, m) ||
+        c->alloc(&c->cg_d, m) || c->alloc(&c->cg_q, m) || c->alloc(&c->cg_scal, 4) || c->alloc(&c->cg_flags, 4) ||
+        c->alloc(&c->d_hist, 2 * (size_t)kHistCap) || c->alloc(&c->d_hist_count, 1);
+    for (int k = 0; k < c->nring && !s; ++k) s = c->alloc(&c->Nbuf[k], S);
+    if (!s && cudaMallocHost((void**)&c->h_flags, 4 * sizeof(int)) != cudaSuccess) s = IBG_ERR_CUDA;
+    if (s) {
+        g_create_error = "ibg_create: device allocation failed";
+        delete c;
+        return IBG_ERR_CUDA;
+    }
+    cudaMemcpy(c->d_ref, c->h_ref.data(), sizeof(double) * c->h_ref.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(c->d_body_of, body_of.data(), sizeof(int) * body_of.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(c->d_bodies, c->h_bodies.data(), sizeof(BodyDev) * c->h_bodies.size(), cudaMemcpyHostToDevice);
+    double sc[4] = {0, 0, c->prm.cg_tol * c->prm.cg_tol, 0};
+    cudaMemcpy(c->cg_scal, sc, sizeof(sc), cudaMemcpyHostToDevice);
+    int fl[4] = {0, 0, c->prm.cg_max_iter, 0};
+    cudaMemcpy(c->cg_flags, fl, sizeof(fl), cudaMemcpyHostToDevice);
+    if (chol_solve_prepare((int)m)) {
+        g_create_error = "ibg_create: too many boundary points for the Cholesky solve";
+        delete c;
+        return IBG_ERR_UNSUPPORTED;
+    }
+    // geom.moveBodies(t = 0); model->init() -> regularizer update
+    c->move_bodies(0.0);
+    if (cudaStreamSynchronize(c->st) != cudaSuccess || c->cuda_check("ibg_create")) {
+        g_create_error = "ibg_create: " + c->err;
+        delete c;
+        return IBG_ERR_CUDA;
+    }
+    *out = c;
+    return IBG_OK;
+}
+
+int ibg_destroy(ibg_context* ctx) {
+    if (!ctx) return IBG_ERR_ARG;
+    if (ctx->st) cudaStreamSynchronize(ctx->st);
+    delete ctx;
+    return IBG_OK;
+}
+
+// Cholesky build: columns M e_j for a chunk of j at once (batched solves).
+int ibg_init(ibg_context* c) {
+    if (!c) return IBG_ERR_ARG;
+    if (c->moving) return IBG_OK;
+    if (c->chol_ready) return IBG_OK;
+    const GridDev& g = c->g;
+    const int m = c->ncomp;
+    const size_t S = c->S;
+    // chunk so that the batched scratch stays below ~8 GB
+    const size_t per_col = sizeof(double) * (4 * S + (size_t)g.N1 + (size_t)g.F1);
+    size_t chunk = (size_t)8 << 30;
+    chunk /= per_col;
+    if (chunk < 1) chunk = 1;
+    if (chunk > (size_t)m) chunk = m;
+    if (chunk > 65535) chunk = 65535;
+    double *bf = nullptr, *u = nullptr, *p = nullptr, *rcb = nullptr, *tb = nullptr, *fl = nullptr, *Mcol = nullptr;
+    int s = c->alloc(&bf, chunk * S) || c->alloc(&u, chunk * S) || c->alloc(&p, chunk * S) ||
+            c->alloc(&rcb, chunk * S) || c->alloc(&tb, chunk * g.N1) || c->alloc(&fl, chunk * g.F1) ||
+            c->alloc(&Mcol, (size_t)m * m, false);
+    for (int k = 0; k < c->sch.nsub && !s; ++k)
+        s = c->alloc(&c->Lr[k], (size_t)m * m, false) || c->alloc(&c->Lc[k], (size_t)m * m, false) ||
+            c->alloc(&c->Ld[k], (size_t)m, false);
+    if (s) {
+        cudaFree(bf); cudaFree(u); cudaFree(p); cudaFree(rcb); cudaFree(tb); cudaFree(fl); cudaFree(Mcol);
+        return c->fail(IBG_ERR_CUDA, "ibg_init: not enough device memory for the Cholesky build");
+    }
+    for (int k = 0; k < c->sch.nsub && !s; ++k) {
+        for (int col0 = 0; col0 < m; col0 += (int)chunk) {
+            const int nb = (int)std::min(chunk, (size_t)(m - col0));
+            launch_smear_bf_unit<double>(g, m, col0, nb, c->slots, fl, g.F1, bf, S, c->beta[k], c->st);
+            SolveCall<double> h{};
+            h.f = bf; h.u = u; h.rc = rcb; h.tbuf = tb; h.bstride = S; h.batch = nb; h.in_scale = 1.0;
+            c->helm[k].solve(h, c->st);
+            SolveCall<double> pc{};
+            pc.f = u; pc.u = p; pc.rc = rcb; pc.tbuf = tb; pc.bstride = S; pc.batch = nb; pc.in_scale = -1.0;
+            c->poisson.solve(pc, c->st);
+            launch_reg_interp<double>(g, m, c->slots, p, S, nb, nullptr, Mcol + (size_t)col0 * m, (size_t)m, c->st);
+        }
+        s = chol_factor(m, Mcol, c->Lr[k], c->Lc[k], c->Ld[k], c->d_status, c->st);
+        int hs = 0;
+        cudaMemcpyAsync(&hs, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->st);
+        if (cudaStreamSynchronize(c->st) != cudaSuccess) s = c->cuda_check("ibg_init");
+        if (!s && hs) s = c->fail(IBG_ERR_NUMERIC, "ibg_init: matrix M is not positive definite");
+    }
+    cudaFree(bf); cudaFree(u); cudaFree(p); cudaFree(rcb); cudaFree(tb); cudaFree(fl); cudaFree(Mcol);
+    if (s) return s;
+    c->chol_ready = true;
+    return c->cuda_check("ibg_init");
+}
+
+int ibg_save(ibg_context* c, const char* basename) {
+    if (!c || !basename) return IBG_ERR_ARG;
+    if (c->moving) return 0;  // ProjectionSolver::save returns false for CG
+    if (!c->chol_ready) return c->fail(IBG_ERR_STATE, "ibg_save: call ibg_init first");
+    const int m = c->ncomp;
+    std::vector<double> Lr((size_t)m * m), d(m);
+    for (int k = 0; k < c->sch.nsub; ++k) {
+        cudaMemcpy(Lr.data(), c->Lr[k], sizeof(double) * m * m, cudaMemcpyDeviceToHost);
+        cudaMemcpy(d.data(), c->Ld[k], sizeof(double) * m, cudaMemcpyDeviceToHost);
+        char num[16];
+        snprintf(num, sizeof(num), "%02d", k + 1);
+        std::string fn = std::string(basename) + "_" + num + ".cholesky";
+        FILE* fp = fopen(fn.c_str(), "w");
+        if (!fp) return c->fail(IBG_ERR_IO, "ibg_save: cannot open " + fn);
+        fprintf(fp, "%d\n%.17g\n", m, (1.0 / c->prm.Re) * c->beta[k]);
+        for (int i = 0; i < m; ++i) fprintf(fp, "%.17g\n", d[i]);
+        fprintf(fp, "#\n");
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < i; ++j) fprintf(fp, "%.17g\n", Lr[(size_t)i * m + j]);
+        fclose(fp);
+    }
+    return 1;
+}
+
+int ibg_load(ibg_context* c, const char* basename) {
+    if (!c || !basename) return IBG_ERR_ARG;
+    if (c->moving) return 0;
+    const int m = c->ncomp;
+    std::vector<std::vector<double>> Ls(c->sch.nsub), Ds(c->sch.nsub);
+    for (int k = 0; k < c->sch.nsub; ++k) {
+        char num[16];
+        snprintf(num, sizeof(num), "%02d", k + 1);
+        std::string fn = std::string(basename) + "_" + num + ".cholesky";
+        std::ifstream in(fn.c_str());
+        if (!in.good()) return 0;
+        int n;
+        double ab;
+        in >> n;
+        if (!in || n != m) return 0;
+        in >> ab;
+        if (!in || ab != (1.0 / c->prm.Re) * c->beta[k]) return 0;
+        Ds[k].resize(m);
+        for (int i = 0; i < m; ++i) in >> Ds[k][i];
+        char mark = 0;
+        in >> mark;
+        if (mark != '#') return 0;
+        Ls[k].assign((size_t)m * m, 0.0);
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < i; ++j) in >> Ls[k][(size_t)i * m + j];
+        if (!in) return 0;
+    }
+    for (int k = 0; k < c->sch.nsub; ++k) {
+        if (!c->Lr[k] && (c->alloc(&c->Lr[k], (size_t)m * m) || c->alloc(&c->Lc[k], (size_t)m * m) ||
+                          c->alloc(&c->Ld[k], (size_t)m)))
+            return IBG_ERR_CUDA;
+        std::vector<double> Lc((size_t)m * m, 0.0);
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < i; ++j) Lc[(size_t)j * m + i] = Ls[k][(size_t)i * m + j];
+        cudaMemcpy(c->Lr[k], Ls[k].data(), sizeof(double) * m * m, cudaMemcpyHostToDevice);
+        cudaMemcpy(c->Lc[k], Lc.data(), sizeof(double) * m * m, cudaMemcpyHostToDevice);
+        cudaMemcpy(c->Ld[k], Ds[k].data(), sizeof(double) * m, cudaMemcpyHostToDevice);
+    }
+    c->chol_ready = true;
+    return c->cuda_check("ibg_load") ? IBG_ERR_CUDA : 1;
+}
+
+int ibg_set_state(ibg_context* c, const double* omega, const double* q, const double* f, int timestep, double time) {
+    if (!c) return IBG_ERR_ARG;
+    if (omega) cudaMemcpyAsync(c->w, omega, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
+    else cudaMemsetAsync(c->w, 0, sizeof(double) * c->S, c->st);
+    if (f) cudaMemcpyAsync(c->f, f, sizeof(double) * c->ncomp, cudaMemcpyHostToDevice, c->st);
+    else cudaMemsetAsync(c->f, 0, sizeof(double) * c->ncomp, c->st);
+    c->timestep = timestep;
+    c->time = time;
+    cudaMemcpyAsync(c->d_time, &c->time, sizeof(double), cudaMemcpyHostToDevice, c->st);
+    cudaMemsetAsync(c->d_hist_count, 0, sizeof(int), c->st);
+    c->hist_steps = 0;
+    if (q) {
+        cudaMemcpyAsync(c->q, q, sizeof(double) * c->F, cudaMemcpyHostToDevice, c->st);
+    } else {
+        if (c->moving) c->move_bodies(0.0);
+        c->refresh();
+    }
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->cuda_check("ibg_set_state");
+    return c->cuda_check("ibg_set_state");
+}
+
+int ibg_get_state(ibg_context* c, double* omega, double* q, double* f, int* timestep, double* time) {
+    if (!c) return IBG_ERR_ARG;
+    if (omega) cudaMemcpyAsync(omega, c->w, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
+    if (q) cudaMemcpyAsync(q, c->q, sizeof(double) * c->F, cudaMemcpyDeviceToHost, c->st);
+    if (f) cudaMemcpyAsync(f, c->f, sizeof(double) * c->ncomp, cudaMemcpyDeviceToHost, c->st);
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->cuda_check("ibg_get_state");
+    if (timestep) *timestep = c->timestep;
+    if (time) *time = c->time;
+    return c->cuda_check("ibg_get_state");
+}
+
+int ibg_get_boundary_force(ibg_context* c, double* f, int* timestep, double* time) {
+    return ibg_get_state(c, nullptr, nullptr, f, timestep, time);
+}
+
+int ibg_update_operators(ibg_context* c, double time) {
+    if (!c) return IBG_ERR_ARG;
+    c->time = time;
+    cudaMemcpyAsync(c->d_time, &c->time, sizeof(double), cudaMemcpyHostToDevice, c->st);
+    if (c->moving) c->move_bodies(0.0);
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->cuda_check("ibg_update_operators");
+    return c->cuda_check("ibg_update_operators");
+}
+
+int ibg_refresh_state(ibg_context* c) {
+    if (!c) return IBG_ERR_ARG;
+    c->refresh();
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->cuda_check("ibg_refresh_state");
+    return c->cuda_check("ibg_refresh_state");
+}
+
+int ibg_advance(ibg_context* c, int nsteps) {
+    if (!c || nsteps < 0) return IBG_ERR_ARG;
+    if (!c->moving && !c->chol_ready) return c->fail(IBG_ERR_STATE, "ibg_advance: call ibg_init (or ibg_load) first");
+    const long long l0 = c->launches;
+    for (int n = 0; n < nsteps; ++n) {
+        if (!c->moving && c->old_saved) {
+            if (!c->graph) {
+                // capture one whole step (all sub-steps) into a graph
+                cudaGraph_t gr;
+                const long long before = c->launches;
+                if (cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+                    return c->cuda_check("ibg_advance: capture");
+                int s = c->enqueue_step();
+                if (cudaStreamEndCapture(c->st, &gr) != cudaSuccess || s) {
+                    c->launches = before;
+                    return s ? s : c->cuda_check("ibg_advance: capture end");
+                }
+                c->graph_launches = c->launches - before;
+                c->launches = before;
+                if (cudaGraphInstantiate(&c->graph, gr, 0) != cudaSuccess) {
+                    cudaGraphDestroy(gr);
+                    return c->cuda_check("ibg_advance: instantiate");
+                }
+                cudaGraphDestroy(gr);
+            }
+            if (cudaGraphLaunch(c->graph, c->st) != cudaSuccess) return c->cuda_check("ibg_advance: graph launch");
+            c->launches += c->graph_launches;
+        } else {
+            int s = c->enqueue_step();
+            if (s) return s;
+        }
+        c->timestep += 1;
+        c->time += c->prm.dt;
+        c->hist_steps += 1;
+    }
+    c->last_launches = c->launches - l0;
+    return c->cuda_check("ibg_advance");
+}
+
+int ibg_get_net_force(ibg_context* c, double* xf, double* yf) {
+    if (!c) return IBG_ERR_ARG;
+    std::vector<double> f(c->ncomp);
+    int s = ibg_get_state(c, nullptr, nullptr, f.data(), nullptr, nullptr);
+    if (s) return s;
+    double sx = 0, sy = 0;
+    for (int i = 0; i < c->npts; ++i) {
+        sx += f[i];
+        sy += f[c->npts + i];
+    }
+    const double dx2 = c->g.dx * c->g.dx;
+    if (xf) *xf = sx * dx2;
+    if (yf) *yf = sy * dx2;
+    return IBG_OK;
+}
+
+int ibg_get_force_history(ibg_context* c, int n, double* xy) {
+    if (!c || n < 0 || (n > 0 && !xy)) return IBG_ERR_ARG;
+    long long have = c->hist_steps < kHistCap ? c->hist_steps : kHistCap;
+    if (n > have) n = (int)have;
+    std::vector<double> h(2 * (size_t)kHistCap);
+    cudaMemcpyAsync(h.data(), c->d_hist, sizeof(double) * 2 * kHistCap, cudaMemcpyDeviceToHost, c->st);
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->cuda_check("ibg_get_force_history");
+    for (int k = 0; k < n; ++k) {
+        long long step = c->hist_steps - n + k;
+        long long slot = step % kHistCap;
+        xy[2 * k] = h[2 * slot];
+        xy[2 * k + 1] = h[2 * slot + 1];
+    }
+    return n;
+}
+
+int ibg_sizes(const ibg_context* c, long long* ns, long long* nf, int* nb) {
+    if (!c) return IBG_ERR_ARG;
+    if (ns) *ns = (long long)c->S;
+    if (nf) *nf = (long long)c->F;
+    if (nb) *nb = c->ncomp;
+    return IBG_OK;
+}
+
+int ibg_cg_stats(const ibg_context* c, int* last, int* mx, int* capped) {
+    if (!c) return IBG_ERR_ARG;
+    if (last) *last = c->cg_last;
+    if (mx) *mx = c->cg_max;
+    if (capped) *capped = c->cg_capped;
+    return IBG_OK;
+}
+
+void* ibg_stream(const ibg_context* c) { return c ? (void*)c->st : nullptr; }
+long long ibg_last_launch_count(const ibg_context* c) { return c ? c->last_launches : 0; }
+
+// ---------------------------------------------------------------------------
+// operator entry points
+// ---------------------------------------------------------------------------
+static int finish(ibg_context* c, const char* where) {
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->cuda_check(where);
+    return c->cuda_check(where);
+}
+
+int ibg_poisson_solve(ibg_context* c, const double* f, double* u) {
+    if (!c || !f || !u) return IBG_ERR_ARG;
+    cudaMemcpyAsync(c->a, f, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
+    c->poisson.solve(c->call(c->a, c->psi, 1.0), c->st);
+    cudaMemcpyAsync(u, c->psi, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
+    return finish(c, "ibg_poisson_solve");
+}
+
+int ibg_helmholtz_solve(ibg_context* c, double alpha, const double* f, double* u) {
+    if (!c || !f || !u) return IBG_ERR_ARG;
+    EllipticPlan<double> h;
+    if (h.init(&c->g, &c->fft, true, alpha, c->cosT)) return c->fail(IBG_ERR_CUDA, "helmholtz plan");
+    cudaMemcpyAsync(c->a, f, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
+    h.solve(c->call(c->a, c->psi, 1.0), c->st);
+    cudaMemcpyAsync(u, c->psi, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
+    return finish(c, "ibg_helmholtz_solve");
+}
+
+int ibg_nonlinear(ibg_context* c, const double* q, const double* omega, double* out) {
+    if (!c || !q || !omega || !out) return IBG_ERR_ARG;
+    cudaMemcpyAsync(c->qtmp, q, sizeof(double) * c->F, cudaMemcpyHostToDevice, c->st);
+    cudaMemcpyAsync(c->a, omega, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
+    launch_nonlinear<double>(c->g, c->qtmp, c->a, c->U, c->V, c->C, c->cc, 1, c->S, c->F, c->st);
+    cudaMemcpyAsync(out, c->cc, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
+    return finish(c, "ibg_nonlinear");
+}
+
+int ibg_laplacian(ibg_context* c, const double* fin, double* out) {
+    if (!c || !fin || !out) return IBG_ERR_ARG;
+    cudaMemcpyAsync(c->a, fin, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
+    launch_laplacian<double>(c->g, c->a, c->psi, c->st);
+    cudaMemcpyAsync(out, c->psi, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
+    return finish(c, "ibg_laplacian");
+}
+
+int ibg_model_B(ibg_context* c, const double* fb, double* omega) {
+    if (!c || !fb || !omega) return IBG_ERR_ARG;
+    cudaMemcpyAsync(c->btmp, fb, sizeof(double) * c->ncomp, cudaMemcpyHostToDevice, c->st);
+    launch_smear_bf<double>(c->g, c->ncomp, c->slots, c->btmp, c->flux0, c->Bf, 1.0, c->st);
+    cudaMemcpyAsync(omega, c->Bf, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
+    return finish(c, "ibg_model_B");
+}
+
+int ibg_model_C(ibg_context* c, const double* omega, double* fb) {
+    if (!c || !omega || !fb) return IBG_ERR_ARG;
+    cudaMemcpyAsync(c->a, omega, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
+    c->poisson.solve(c->call(c->a, c->psi, -1.0), c->st);
+    launch_reg_interp<double>(c->g, c->ncomp, c->slots, c->psi, c->S, 1, nullptr, c->btmp, 0, c->st);
+    cudaMemcpyAsync(fb, c->btmp, sizeof(double) * c->ncomp, cudaMemcpyDeviceToHost, c->st);
+    return finish(c, "ibg_model_C");
+}
+
+int ibg_reg_to_boundary(ibg_context* c, const double* qin, double* fb) {
+    if (!c || !qin || !fb) return IBG_ERR_ARG;
+    cudaMemcpyAsync(c->qtmp, qin, sizeof(double) * c->g.F1, cudaMemcpyHostToDevice, c->st);
+    launch_reg_gather(c->g, c->ncomp, c->slots, c->qtmp, c->btmp, c->st);
+    cudaMemcpyAsync(fb, c->btmp, sizeof(double) * c->ncomp, cudaMemcpyDeviceToHost, c->st);
+    return finish(c, "ibg_reg_to_boundary");
+}
+
+int ibg_projection_solve(ibg_context* c, int k, const double* ain, const double* bin, double* omega, double* fio) {
+    if (!c || !ain || !bin || !omega || !fio || k < 0 || k >= c->sch.nsub) return IBG_ERR_ARG;
+    if (!c->moving && !c->chol_ready) return c->fail(IBG_ERR_STATE, "ibg_projection_solve: call ibg_init first");
+    cudaMemcpyAsync(c->a, ain, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
+    cudaMemcpyAsync(c->btmp, bin, sizeof(double) * c->ncomp, cudaMemcpyHostToDevice, c->st);
+    cudaMemcpyAsync(c->f, fio, sizeof(double) * c->ncomp, cudaMemcpyHostToDevice, c->st);
+    int s = c->projection(k, c->a, c->btmp);
+    if (s) return s;
+    cudaMemcpyAsync(omega, c->w, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
+    cudaMemcpyAsync(fio, c->f, sizeof(double) * c->ncomp, cudaMemcpyDeviceToHost, c->st);
+    return finish(c, "ibg_projection_solve");
+}
+
+}  // extern "C"

@@ -1,0 +1,50 @@
+// ibg_ops.cuh -- launchers for the stencil, regularizer and body kernels.
+#pragma once
+#include "ibg_internal.cuh"
+
+namespace ibg {
+
+// Rigid-body motion on the device: motion 0 = none, 1 = fixed (x, y, theta),
+// 2 = pitch/plunge with p = (A_theta, 2 pi f_theta, phi_theta, A_y, 2 pi f_y, phi_y).
+struct BodyDev {
+    double xc, yc;
+    int motion;
+    double p[6];
+};
+
+// Regularizer association slots: up to 9 level-0 fluxes per boundary component.
+struct RegSlots {
+    int* idx = nullptr;     // [2 npts][9] flux index (level 0)
+    double* w = nullptr;    // [2 npts][9] weight delta(dx) delta(dy)
+    int* n = nullptr;       // [2 npts] number of slots used
+};
+
+template <typename T>
+void launch_nonlinear(const GridDev& g, const T* q, const T* w, T* U, T* V, T* C, T* N, int batch, size_t sstride,
+                      size_t fstride, cudaStream_t st);
+template <typename T>
+void launch_curl_flux(const GridDev& g, const T* C, T* N, cudaStream_t st);
+template <typename T>
+void launch_rhs(const GridDev& g, const T* w, const T* N, const T* Nprev, T* a, double c1, double an, double bn,
+                double dt, cudaStream_t st);
+template <typename T>
+void launch_laplacian(const GridDev& g, const T* w, T* out, cudaStream_t st);
+void launch_reg_gather(const GridDev& g, int ncomp, const RegSlots& s, const double* q0, double* out,
+                       cudaStream_t st);
+template <typename T>
+void launch_refresh_flux(const GridDev& g, const T* psi, T* q, double u0, double v0, cudaStream_t st);
+void launch_kinematics(int npts, const double* ref_xy, const int* body_of, const BodyDev* bodies,
+                       const double* time_ptr, double toff, double* pts, double* vel, cudaStream_t st);
+void launch_reg_update(const GridDev& g, int npts, const double* pts, const double* vel, RegSlots& s, double* bcon,
+                       double u0, double v0, cudaStream_t st);
+template <typename T>
+void launch_reg_interp(const GridDev& g, int ncomp, const RegSlots& s, const T* psi, size_t sstride, int batch,
+                       const double* bcon, double* out, size_t ostride, cudaStream_t st);
+template <typename T>
+void launch_smear_bf(const GridDev& g, int ncomp, const RegSlots& s, const double* f, double* flux0, T* Bf,
+                     double beta, cudaStream_t st);
+template <typename T>
+void launch_smear_bf_unit(const GridDev& g, int ncomp, int col0, int batch, const RegSlots& s, double* flux0,
+                          size_t fstride, T* Bf, size_t sstride, double beta, cudaStream_t st);
+
+}  // namespace ibg

@@ -1,0 +1,527 @@
+// ops.cu -- stencil, nonlinear, regularizer and kinematics kernels.
+//
+// Reference functions replaced (paths inside the reference project):
+//   k_node_vel     FluxToXVelocity / FluxToYVelocity  src/VectorOperations.cc:488-667
+//                  and the products of CrossProduct     src/VectorOperations.cc:438-457
+//   k_cross_flux   XVelocityToFlux / YVelocityToFlux  src/VectorOperations.cc:669-916
+//   k_curl_flux    Curl(Flux)                          src/VectorOperations.cc:33-54
+//   k_rhs          IBSolver::advanceSubstep RHS        src/IBSolver.cc:168-183
+//                  with Laplacian = -Curl(Curl())      src/VectorOperations.cc:63-146
+//   k_refresh_flux computeFlux = Curl(psi) + q0         src/NavierStokesModel.cc:114-125
+//   k_kinematics   RigidBody::moveBody + PitchPlunge   src/RigidBody.cc:586-609, src/PitchPlunge.h:52-58
+//   k_reg_update   Regularizer::update                 src/Regularizer.cc:54-90
+//   k_reg_interp   Regularizer::toBoundary o Curl(psi) src/Regularizer.cc:111-128
+//   k_reg_smear/k_bf  Regularizer::toFlux, Curl, *beta  src/Regularizer.cc:92-109, src/ProjectionSolver.cc:87-90
+#include "ibg_internal.cuh"
+#include "ibg_ops.cuh"
+
+namespace ibg {
+
+template <typename T>
+__device__ __forceinline__ T qx_at(const T* q_lev, const GridDev& g, int i, int j) {
+    return q_lev[(size_t)i * g.ny + j];
+}
+template <typename T>
+__device__ __forceinline__ T qy_at(const T* q_lev, const GridDev& g, int i, int j) {
+    return q_lev[(size_t)g.nXf + (size_t)i * (g.ny + 1) + j];
+}
+
+// ---------------------------------------------------------------------------
+// node velocities times vorticity: U = -(u w), V = v w on every node where
+// the reference defines u, v (coarse overlap interior nodes are never read
+// downstream and are written as zero).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_node_vel(GridDev g, const T* __restrict__ q, const T* __restrict__ w, T* __restrict__ U,
+                           T* __restrict__ V, size_t sstride, size_t fstride) {
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t total = (size_t)g.L * g.N1;
+    if (tid >= total) return;
+    const size_t sb = (size_t)blockIdx.y * sstride, fb = (size_t)blockIdx.y * fstride;
+    const int lev = (int)(tid / g.N1);
+    const int r = (int)(tid % g.N1);
+    const int i = r / g.NJ + 1, j = r % g.NJ + 1;
+    const T* ql = q + fb + (size_t)lev * g.F1;
+    const int nx = g.nx, ny = g.ny, nx2 = g.nxe, ny2 = g.nye;
+    T u = (T)0, v = (T)0;
+    bool du = true, dv = true;
+    if (lev == 0) {
+        const T o2d = (T)(1.0 / (2 * g.dx));
+        u = (qx_at(ql, g, i, j) + qx_at(ql, g, i, j - 1)) * o2d;
+        v = (qy_at(ql, g, i - 1, j) + qy_at(ql, g, i, j)) * o2d;
+    } else {
+        const T bydx = (T)(1.0 / lev_dx(g, lev));
+        const T* qf = ql - g.F1;
+        const int il = nx2, ir = nx / 2 + nx2, jb = ny2, jt = ny / 2 + ny2;
+        // ---- u (x-velocity) regions B, C, D, E, F
+        if (i < il || i > ir || j < jb || j > jt || ((i == il || i == ir) && j > jb && j < jt)) {
+            u = (qx_at(ql, g, i, j) + qx_at(ql, g, i, j - 1)) * (T)0.5 * bydx;
+        } else if ((j == jb || j == jt) && i > il && i < ir) {
+            const int ii = (i - nx2) * 2;
+            if (j == jb)
+                u = (qx_at(ql, g, i, jb - 1) * (T)2 / (T)3 + qx_at(qf, g, ii, 0) * (T)1 / (T)3 +
+                     (qx_at(qf, g, ii - 1, 0) + qx_at(qf, g, ii + 1, 0)) * (T)1 / (T)6) * bydx;
+            else
+                u = (qx_at(ql, g, i, jt) * (T)2 / (T)3 + qx_at(qf, g, ii, ny - 1) * (T)1 / (T)3 +
+                     (qx_at(qf, g, ii - 1, ny - 1) + qx_at(qf, g, ii + 1, ny - 1)) * (T)1 / (T)6) * bydx;
+        } else if ((i == il || i == ir) && (j == jb || j == jt)) {
+            if (j == jb) {
+                const T fv = (i == il) ? qx_at(qf, g, 1, 0) : qx_at(qf, g, nx - 1, 0);
+                u = (qx_at(ql, g, i, j - 1) * (T)8 / (T)15 + qx_at(ql, g, i, j) * (T)6 / (T)15 + fv * (T)2 / (T)15) * bydx;
+            } else {
+                const T fv = (i == il) ? qx_at(qf, g, 1, ny - 1) : qx_at(qf, g, nx - 1, ny - 1);
+                u = (qx_at(ql, g, i, j) * (T)8 / (T)15 + qx_at(ql, g, i, j - 1) * (T)6 / (T)15 + fv * (T)2 / (T)15) * bydx;
+            }
+        } else {
+            du = false;
+        }
+        // ---- v (y-velocity): B (bottom/top borders), C (left/right), D, E, F
+        if (j < jb || j > jt || i < il || i > ir || ((j == jb || j == jt) && i > il && i < ir)) {
+            v = (qy_at(ql, g, i, j) + qy_at(ql, g, i - 1, j)) * (T)0.5 * bydx;
+        } else if ((i == il || i == ir) && j > jb && j < jt) {
+            const int jj = (j - ny2) * 2;
+            if (i == il)
+                v = (qy_at(ql, g, il - 1, j) * (T)2 / (T)3 + qy_at(qf, g, 0, jj) * (T)1 / (T)3 +
+                     (qy_at(qf, g, 0, jj - 1) + qy_at(qf, g, 0, jj + 1)) * (T)1 / (T)6) * bydx;
+            else
+                v = (qy_at(ql, g, ir, j) * (T)2 / (T)3 + qy_at(qf, g, nx - 1, jj) * (T)1 / (T)3 +
+                     (qy_at(qf, g, nx - 1, jj - 1) + qy_at(qf, g, nx - 1, jj + 1)) * (T)1 / (T)6) * bydx;
+        } else if ((i == il || i == ir) && (j == jb || j == jt)) {
+            if (i == il) {
+                const T fv = (j == jb) ? qy_at(qf, g, 0, 1) : qy_at(qf, g, 0, ny - 1);
+                v = (qy_at(ql, g, i - 1, j) * (T)8 / (T)15 + qy_at(ql, g, i, j) * (T)6 / (T)15 + fv * (T)2 / (T)15) * bydx;
+            } else {
+                const T fv = (j == jb) ? qy_at(qf, g, nx - 1, 1) : qy_at(qf, g, nx - 1, ny - 1);
+                v = (qy_at(ql, g, i, j) * (T)8 / (T)15 + qy_at(ql, g, i - 1, j) * (T)6 / (T)15 + fv * (T)2 / (T)15) * bydx;
+            }
+        } else {
+            dv = false;
+        }
+    }
+    const T wv = w[sb + tid];
+    U[sb + tid] = du ? (u * wv) * (T)-1 : (T)0;
+    V[sb + tid] = dv ? v * wv : (T)0;
+}
+
+// ---------------------------------------------------------------------------
+// cross-product fluxes of one level: x part from V (XVelocityToFlux), y part
+// from U (YVelocityToFlux).  Coarse-level interior fluxes over the finer
+// domain are sums of the finer level's fluxes, so levels run fine to coarse.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_cross_flux(GridDev g, int lev, const T* __restrict__ U, const T* __restrict__ V, T* __restrict__ C,
+                             size_t sstride, size_t fstride) {
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= g.F1) return;
+    const size_t sb = (size_t)blockIdx.y * sstride, fb = (size_t)blockIdx.y * fstride;
+    const int nx = g.nx, ny = g.ny, nx2 = g.nxe, ny2 = g.nye, L = g.L;
+    const T dx = (T)lev_dx(g, lev);
+    T* Cl = C + fb + (size_t)lev * g.F1;
+    const T* Cf = Cl - g.F1;  // finer level (lev >= 1)
+    T out;
+    if (tid < g.nXf) {
+        const int i = tid / ny, j = tid % ny;
+        const T* p = V + sb + (size_t)lev * g.N1;
+        const T* c = (lev < L - 1) ? V + sb + (size_t)(lev + 1) * g.N1 : nullptr;
+        if (i == 0 || i == nx) {
+            if (lev == L - 1) {
+                out = (T)0;
+            } else {
+                const int ic = (i == 0) ? nx2 : nx / 2 + nx2;
+                const int jj = j / 2 + ny2;
+                if ((j & 1) == 0)
+                    out = ((T)0.75 * node(c, g, ic, jj) + (T)0.25 * node(c, g, ic, jj + 1)) * dx;
+                else
+                    out = ((T)0.25 * node(c, g, ic, jj) + (T)0.75 * node(c, g, ic, jj + 1)) * dx;
+            }
+        } else if (j == 0 || j == ny - 1) {
+            const int jn = (j == 0) ? 1 : ny - 1;
+            if (lev == L - 1) {
+                out = node(p, g, i, jn) * (T)0.5 * dx;
+            } else {
+                const int jc = (j == 0) ? ny2 : ny / 2 + ny2;
+                const int ii = i / 2 + nx2;
+                if ((i & 1) == 0)
+                    out = (node(p, g, i, jn) + node(c, g, ii, jc)) * (T)0.5 * dx;
+                else
+                    out = ((T)0.5 * node(p, g, i, jn) + (T)0.25 * node(c, g, ii, jc) + (T)0.25 * node(c, g, ii + 1, jc)) * dx;
+            }
+        } else if (lev > 0 && j >= ny2 && j < ny / 2 + ny2 && i > nx2 && i < nx / 2 + nx2) {
+            const int ii = 2 * (i - nx2), jj = 2 * (j - ny2);
+            out = qx_at(Cf, g, ii, jj) + qx_at(Cf, g, ii, jj + 1);
+        } else {
+            out = (node(p, g, i, j) + node(p, g, i, j + 1)) * (T)0.5 * dx;
+        }
+    } else {
+        const int t = tid - g.nXf;
+        const int i = t / (ny + 1), j = t % (ny + 1);
+        const T* p = U + sb + (size_t)lev * g.N1;
+        const T* c = (lev < L - 1) ? U + sb + (size_t)(lev + 1) * g.N1 : nullptr;
+        if (j == 0 || j == ny) {
+            if (lev == L - 1) {
+                out = (T)0;
+            } else {
+                const int jc = (j == 0) ? ny2 : ny / 2 + ny2;
+                const int ii = i / 2 + nx2;
+                if ((i & 1) == 0)
+                    out = ((T)0.75 * node(c, g, ii, jc) + (T)0.25 * node(c, g, ii + 1, jc)) * dx;
+                else
+                    out = ((T)0.25 * node(c, g, ii, jc) + (T)0.75 * node(c, g, ii + 1, jc)) * dx;
+            }
+        } else if (i == 0 || i == nx - 1) {
+            const int in_ = (i == 0) ? 1 : nx - 1;
+            if (lev == L - 1) {
+                out = node(p, g, in_, j) * (T)0.5 * dx;
+            } else {
+                const int ic = (i == 0) ? nx2 : nx / 2 + nx2;
+                const int jj = j / 2 + ny2;
+                if ((j & 1) == 0)
+                    out = (node(p, g, in_, j) + node(c, g, ic, jj)) * (T)0.5 * dx;
+                else
+                    out = ((T)0.5 * node(p, g, in_, j) + (T)0.25 * node(c, g, ic, jj) + (T)0.25 * node(c, g, ic, jj + 1)) * dx;
+            }
+        } else if (lev > 0 && i >= nx2 && i < nx / 2 + nx2 && j > ny2 && j < ny / 2 + ny2) {
+            const int ii = 2 * (i - nx2), jj = 2 * (j - ny2);
+            out = qy_at(Cf, g, ii, jj) + qy_at(Cf, g, ii + 1, jj);
+        } else {
+            out = (node(p, g, i, j) + node(p, g, i + 1, j)) * (T)0.5 * dx;
+        }
+    }
+    Cl[tid] = out;
+}
+
+// Curl of a Flux on every level (no inter-level coupling)
+template <typename T>
+__global__ void k_curl_flux(GridDev g, const T* __restrict__ C, T* __restrict__ N, size_t sstride, size_t fstride) {
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (size_t)g.L * g.N1) return;
+    const size_t sb = (size_t)blockIdx.y * sstride, fb = (size_t)blockIdx.y * fstride;
+    const int lev = (int)(tid / g.N1);
+    const int r = (int)(tid % g.N1);
+    const int i = r / g.NJ + 1, j = r % g.NJ + 1;
+    const T* ql = C + fb + (size_t)lev * g.F1;
+    const double dxl = lev_dx(g, lev);
+    const T bydx2 = (T)(1. / (dxl * dxl));
+    N[sb + tid] = (qy_at(ql, g, i, j) - qy_at(ql, g, i - 1, j) + qx_at(ql, g, i, j - 1) - qx_at(ql, g, i, j)) * bydx2;
+}
+
+// a = omega + dt (c1 L omega + an N + bn Nprev)
+template <typename T>
+__global__ void k_rhs(GridDev g, const T* __restrict__ w, const T* __restrict__ N, const T* __restrict__ Nprev,
+                      T* __restrict__ a, T c1, T an, T bn, T dt, int lap_only) {
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (size_t)g.L * g.N1) return;
+    const int lev = (int)(tid / g.N1);
+    const int r = (int)(tid % g.N1);
+    const int i = r / g.NJ + 1, j = r % g.NJ + 1;
+    const T* f = w + (size_t)lev * g.N1;
+    const T* c = (lev < g.L - 1) ? w + (size_t)(lev + 1) * g.N1 : nullptr;
+    const T p = node(f, g, i, j);
+    const T pe = node_bc(f, c, g, i + 1, j), pw = node_bc(f, c, g, i - 1, j);
+    const T pn = node_bc(f, c, g, i, j + 1), ps = node_bc(f, c, g, i, j - 1);
+    const T qy_ij = p - pe, qy_im = pw - p, qx_jm = p - ps, qx_ij = pn - p;
+    const double dxl = lev_dx(g, lev);
+    const T bydx2 = (T)(1. / (dxl * dxl));
+    const T lap = ((qy_ij - qy_im + qx_jm - qx_ij) * bydx2) * (T)-1;
+    if (lap_only) {
+        a[tid] = lap;
+        return;
+    }
+    T v = lap * c1;
+    v = v + an * N[tid];
+    if (Nprev) v = v + bn * Nprev[tid];
+    v = v * dt;
+    a[tid] = v + p;
+}
+
+// Curl of a Scalar (with boundary values from the next coarser level) at a
+// flux index of level lev.
+template <typename T>
+__device__ __forceinline__ T curl_scalar_at(const GridDev& g, const T* f, const T* c, int idx) {
+    if (idx < g.nXf) {
+        const int i = idx / g.ny, j = idx % g.ny;
+        return node_bc(f, c, g, i, j + 1) - node_bc(f, c, g, i, j);
+    }
+    const int t = idx - g.nXf;
+    const int i = t / (g.ny + 1), j = t % (g.ny + 1);
+    return node_bc(f, c, g, i, j) - node_bc(f, c, g, i + 1, j);
+}
+
+// q = Curl(psi) + q0 on every level
+template <typename T>
+__global__ void k_refresh_flux(GridDev g, const T* __restrict__ psi, T* __restrict__ q, double u0, double v0) {
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (size_t)g.L * g.F1) return;
+    const int lev = (int)(tid / g.F1);
+    const int idx = (int)(tid % g.F1);
+    const T* f = psi + (size_t)lev * g.N1;
+    const T* c = (lev < g.L - 1) ? psi + (size_t)(lev + 1) * g.N1 : nullptr;
+    const double dxl = lev_dx(g, lev);
+    const T base = (T)((idx < g.nXf ? u0 : v0) * dxl);
+    q[tid] = curl_scalar_at(g, f, c, idx) + base;
+}
+
+// ---------------------------------------------------------------------------
+// bodies
+// ---------------------------------------------------------------------------
+__global__ void k_kinematics(int npts, const double* __restrict__ ref_xy, const int* __restrict__ body_of,
+                             const BodyDev* __restrict__ bodies, const double* __restrict__ time_ptr, double toff,
+                             double* __restrict__ pts, double* __restrict__ vel) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npts) return;
+    const BodyDev b = bodies[body_of[p]];
+    const double rx = ref_xy[2 * p], ry = ref_xy[2 * p + 1];
+    if (b.motion == 0) {
+        pts[2 * p] = rx;
+        pts[2 * p + 1] = ry;
+        vel[2 * p] = 0.0;
+        vel[2 * p + 1] = 0.0;
+        return;
+    }
+    const double t = *time_ptr + toff;
+    double x, y, th, xd, yd, thd;
+    if (b.motion == 1) {
+        x = b.p[0]; y = b.p[1]; th = b.p[2];
+        xd = yd = thd = 0.0;
+    } else {
+        // PitchPlunge: frequencies already multiplied by 2 pi
+        x = 0.0; xd = 0.0;
+        y = b.p[3] * sin(b.p[4] * t + b.p[5]);
+        yd = b.p[3] * b.p[4] * cos(b.p[4] * t + b.p[5]);
+        th = b.p[0] * sin(b.p[1] * t + b.p[2]);
+        thd = b.p[0] * b.p[1] * cos(b.p[1] * t + b.p[2]);
+    }
+    const double a = rx - b.xc, bb = ry - b.yc;
+    const double c = cos(th), s = sin(th);
+    pts[2 * p] = (x + a * c - bb * s) + b.xc;
+    pts[2 * p + 1] = (y + a * s + bb * c) + b.yc;
+    vel[2 * p] = -a * s * thd - bb * c * thd + xd;
+    vel[2 * p + 1] = a * c * thd - bb * s * thd + yd;
+}
+
+__device__ __forceinline__ double delta_fn(double r) {
+    if (r > 1.5) return 0.0;
+    if (r <= 0.5) return (1 + sqrt(1 - 3 * r * r)) / 3;
+    return (5 - 3 * r - sqrt(1 - 3 * (1 - r) * (1 - r))) / 6;
+}
+
+// Association slots per boundary component c = dir*npts + p: up to 9 level-0
+// fluxes within 1.5 cells in both directions, in increasing flux index, and
+// the constraint b_c = body velocity - E(q0)_c.
+__global__ void k_reg_update(GridDev g, int npts, const double* __restrict__ pts, const double* __restrict__ vel,
+                             int* __restrict__ sidx, double* __restrict__ sw, int* __restrict__ sn,
+                             double* __restrict__ bcon, double u0, double v0) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= 2 * npts) return;
+    const int dir = c / npts, p = c % npts;
+    const double h = g.dx;
+    const double px = pts[2 * p], py = pts[2 * p + 1];
+    const double offx = dir == 0 ? 0.0 : 0.5, offy = dir == 0 ? 0.5 : 0.0;
+    const int ni = dir == 0 ? g.nx + 1 : g.nx;
+    const int nj = dir == 0 ? g.ny : g.ny + 1;
+    const int base = dir == 0 ? 0 : g.nXf;
+    const int stride = dir == 0 ? g.ny : g.ny + 1;
+    const int ic = (int)floor((px - g.x0) / h - offx);
+    const int jc = (int)floor((py - g.y0) / h - offy);
+    int n = 0;
+    double e = 0.0;
+    const double q0 = (dir == 0 ? u0 : v0) * h;
+    for (int i = ic - 1; i <= ic + 2; ++i) {
+        if (i < 0 || i >= ni) continue;
+        // flux position as Flux::x (getXEdge / getXCenter): x0 + i dx or x0 + (i + .5) dx
+        const double fx = dir == 0 ? __dadd_rn(g.x0, __dmul_rn((double)i, h))
+                                   : __dadd_rn(g.x0, __dmul_rn((double)i + 0.5, h));
+        const double dxn = fabs(fx - px) / h;
+        if (!(dxn < 1.5)) continue;
+        for (int j = jc - 1; j <= jc + 2; ++j) {
+            if (j < 0 || j >= nj) continue;
+            const double fy = dir == 0 ? __dadd_rn(g.y0, __dmul_rn((double)j + 0.5, h))
+                                       : __dadd_rn(g.y0, __dmul_rn((double)j, h));
+            const double dyn = fabs(fy - py) / h;
+            if (!(dyn < 1.5)) continue;
+            if (n < 9) {
+                const double wgt = delta_fn(dxn) * delta_fn(dyn);
+                sidx[c * 9 + n] = base + i * stride + j;
+                sw[c * 9 + n] = wgt;
+                e = e + wgt * q0;
+                ++n;
+            }
+        }
+    }
+    sn[c] = n;
+    const double velc = vel[2 * p + dir];
+    bcon[c] = velc - e / h;
+}
+
+// rhs_c = E(Curl(psi))_c - b_c  (C operator of the projection, batched)
+template <typename T>
+__global__ void k_reg_interp(GridDev g, int ncomp, const int* __restrict__ sidx, const double* __restrict__ sw,
+                             const int* __restrict__ sn, const T* __restrict__ psi, size_t sstride,
+                             const double* __restrict__ bcon, double* __restrict__ out, size_t ostride) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncomp) return;
+    const T* f = psi + (size_t)blockIdx.y * sstride;
+    const T* cc = g.L > 1 ? f + g.N1 : nullptr;
+    double acc = 0.0;
+    const int n = sn[c];
+    for (int k = 0; k < n; ++k) acc = acc + sw[c * 9 + k] * (double)curl_scalar_at(g, f, cc, sidx[c * 9 + k]);
+    double v = acc / g.dx;
+    if (bcon) v = v - bcon[c];
+    out[(size_t)blockIdx.y * ostride + c] = v;
+}
+
+// smear: flux0[idx] += w f_c (atomic; flux0 is kept zero between uses)
+__global__ void k_reg_smear(int ncomp, const int* __restrict__ sidx, const double* __restrict__ sw,
+                            const int* __restrict__ sn, const double* __restrict__ f, double* __restrict__ flux0) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = t / 9, k = t % 9;
+    if (c >= ncomp || k >= sn[c]) return;
+    atomicAdd(&flux0[sidx[c * 9 + k]], sw[c * 9 + k] * f[c]);
+}
+
+// batched smear of unit vectors: item b carries e_{col0+b}
+__global__ void k_reg_smear_unit(int ncomp, int col0, const int* __restrict__ sidx, const double* __restrict__ sw,
+                                 const int* __restrict__ sn, double* __restrict__ flux0, size_t fstride) {
+    const int b = blockIdx.x;
+    const int c = col0 + b;
+    const int k = threadIdx.x;
+    if (c >= ncomp || k >= sn[c]) return;
+    flux0[(size_t)b * fstride + sidx[c * 9 + k]] = sw[c * 9 + k];
+}
+
+__global__ void k_reg_zero(int ncomp, int col0, int unit, const int* __restrict__ sidx, const int* __restrict__ sn,
+                           double* __restrict__ flux0, size_t fstride) {
+    if (unit) {
+        const int b = blockIdx.x, c = col0 + b, k = threadIdx.x;
+        if (c >= ncomp || k >= sn[c]) return;
+        flux0[(size_t)b * fstride + sidx[c * 9 + k]] = 0.0;
+        return;
+    }
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = t / 9, k = t % 9;
+    if (c >= ncomp || k >= sn[c]) return;
+    flux0[sidx[c * 9 + k]] = 0.0;
+}
+
+// Bf on level 0: beta * Curl(flux0 * dx); coarser levels of Bf stay zero
+template <typename T>
+__global__ void k_bf(GridDev g, const double* __restrict__ flux0, size_t fstride, T* __restrict__ Bf, size_t sstride,
+                     double beta) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= g.N1) return;
+    const double* q = flux0 + (size_t)blockIdx.y * fstride;
+    const int i = r / g.NJ + 1, j = r % g.NJ + 1;
+    const double h = g.dx;
+    const double bydx2 = 1. / (h * h);
+    const double qyij = qy_at(q, g, i, j) * h, qyim = qy_at(q, g, i - 1, j) * h;
+    const double qxjm = qx_at(q, g, i, j - 1) * h, qxij = qx_at(q, g, i, j) * h;
+    Bf[(size_t)blockIdx.y * sstride + r] = (T)(((qyij - qyim + qxjm - qxij) * bydx2) * beta);
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+static inline unsigned nblk(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+template <typename T>
+void launch_nonlinear(const GridDev& g, const T* q, const T* w, T* U, T* V, T* C, T* N, int batch, size_t sstride,
+                      size_t fstride, cudaStream_t st) {
+    const size_t S = (size_t)g.L * g.N1;
+    k_node_vel<T><<<dim3(nblk(S, 256), batch), 256, 0, st>>>(g, q, w, U, V, sstride, fstride);
+    for (int lev = 0; lev < g.L; ++lev)
+        k_cross_flux<T><<<dim3(nblk(g.F1, 256), batch), 256, 0, st>>>(g, lev, U, V, C, sstride, fstride);
+    k_curl_flux<T><<<dim3(nblk(S, 256), batch), 256, 0, st>>>(g, C, N, sstride, fstride);
+}
+
+template <typename T>
+void launch_curl_flux(const GridDev& g, const T* C, T* N, cudaStream_t st) {
+    const size_t S = (size_t)g.L * g.N1;
+    k_curl_flux<T><<<dim3(nblk(S, 256), 1), 256, 0, st>>>(g, C, N, S, (size_t)g.L * g.F1);
+}
+
+template <typename T>
+void launch_rhs(const GridDev& g, const T* w, const T* N, const T* Nprev, T* a, double c1, double an, double bn,
+                double dt, cudaStream_t st) {
+    const size_t S = (size_t)g.L * g.N1;
+    k_rhs<T><<<nblk(S, 256), 256, 0, st>>>(g, w, N, Nprev, a, (T)c1, (T)an, (T)bn, (T)dt, 0);
+}
+
+template <typename T>
+void launch_laplacian(const GridDev& g, const T* w, T* out, cudaStream_t st) {
+    const size_t S = (size_t)g.L * g.N1;
+    k_rhs<T><<<nblk(S, 256), 256, 0, st>>>(g, w, nullptr, nullptr, out, (T)0, (T)0, (T)0, (T)0, 1);
+}
+
+// E applied to given level-0 fluxes (Regularizer::toBoundary)
+__global__ void k_reg_gather(int ncomp, const int* __restrict__ sidx, const double* __restrict__ sw,
+                             const int* __restrict__ sn, const double* __restrict__ q0, double dx,
+                             double* __restrict__ out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncomp) return;
+    double acc = 0.0;
+    for (int k = 0; k < sn[c]; ++k) acc = acc + sw[c * 9 + k] * q0[sidx[c * 9 + k]];
+    out[c] = acc / dx;
+}
+
+void launch_reg_gather(const GridDev& g, int ncomp, const RegSlots& s, const double* q0, double* out,
+                       cudaStream_t st) {
+    k_reg_gather<<<nblk(ncomp, 128), 128, 0, st>>>(ncomp, s.idx, s.w, s.n, q0, g.dx, out);
+}
+
+template <typename T>
+void launch_refresh_flux(const GridDev& g, const T* psi, T* q, double u0, double v0, cudaStream_t st) {
+    const size_t F = (size_t)g.L * g.F1;
+    k_refresh_flux<T><<<nblk(F, 256), 256, 0, st>>>(g, psi, q, u0, v0);
+}
+
+void launch_kinematics(int npts, const double* ref_xy, const int* body_of, const BodyDev* bodies,
+                       const double* time_ptr, double toff, double* pts, double* vel, cudaStream_t st) {
+    k_kinematics<<<nblk(npts, 128), 128, 0, st>>>(npts, ref_xy, body_of, bodies, time_ptr, toff, pts, vel);
+}
+
+void launch_reg_update(const GridDev& g, int npts, const double* pts, const double* vel, RegSlots& s, double* bcon,
+                       double u0, double v0, cudaStream_t st) {
+    k_reg_update<<<nblk(2 * npts, 128), 128, 0, st>>>(g, npts, pts, vel, s.idx, s.w, s.n, bcon, u0, v0);
+}
+
+template <typename T>
+void launch_reg_interp(const GridDev& g, int ncomp, const RegSlots& s, const T* psi, size_t sstride, int batch,
+                       const double* bcon, double* out, size_t ostride, cudaStream_t st) {
+    k_reg_interp<T><<<dim3(nblk(ncomp, 128), batch), 128, 0, st>>>(g, ncomp, s.idx, s.w, s.n, psi, sstride, bcon, out,
+                                                                    ostride);
+}
+
+template <typename T>
+void launch_smear_bf(const GridDev& g, int ncomp, const RegSlots& s, const double* f, double* flux0, T* Bf,
+                     double beta, cudaStream_t st) {
+    k_reg_smear<<<nblk((size_t)ncomp * 9, 128), 128, 0, st>>>(ncomp, s.idx, s.w, s.n, f, flux0);
+    k_bf<T><<<dim3(nblk(g.N1, 256), 1), 256, 0, st>>>(g, flux0, 0, Bf, 0, beta);
+    k_reg_zero<<<nblk((size_t)ncomp * 9, 128), 128, 0, st>>>(ncomp, 0, 0, s.idx, s.n, flux0, 0);
+}
+
+template <typename T>
+void launch_smear_bf_unit(const GridDev& g, int ncomp, int col0, int batch, const RegSlots& s, double* flux0,
+                          size_t fstride, T* Bf, size_t sstride, double beta, cudaStream_t st) {
+    k_reg_smear_unit<<<batch, 32, 0, st>>>(ncomp, col0, s.idx, s.w, s.n, flux0, fstride);
+    k_bf<T><<<dim3(nblk(g.N1, 256), batch), 256, 0, st>>>(g, flux0, fstride, Bf, sstride, beta);
+    k_reg_zero<<<batch, 32, 0, st>>>(ncomp, col0, 1, s.idx, s.n, flux0, fstride);
+}
+
+#define IBG_INST(T)                                                                                            \
+    template void launch_nonlinear<T>(const GridDev&, const T*, const T*, T*, T*, T*, T*, int, size_t, size_t, \
+                                      cudaStream_t);                                                           \
+    template void launch_curl_flux<T>(const GridDev&, const T*, T*, cudaStream_t);                             \
+    template void launch_rhs<T>(const GridDev&, const T*, const T*, const T*, T*, double, double, double,      \
+                                double, cudaStream_t);                                                         \
+    template void launch_laplacian<T>(const GridDev&, const T*, T*, cudaStream_t);                             \
+    template void launch_refresh_flux<T>(const GridDev&, const T*, T*, double, double, cudaStream_t);          \
+    template void launch_reg_interp<T>(const GridDev&, int, const RegSlots&, const T*, size_t, int,            \
+                                       const double*, double*, size_t, cudaStream_t);                          \
+    template void launch_smear_bf<T>(const GridDev&, int, const RegSlots&, const double*, double*, T*, double, \
+                                     cudaStream_t);                                                            \
+    template void launch_smear_bf_unit<T>(const GridDev&, int, int, int, const RegSlots&, double*, size_t, T*, \
+                                          size_t, double, cudaStream_t);
+IBG_INST(double)
+IBG_INST(float)
+
+}  // namespace ibg

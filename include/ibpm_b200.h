@@ -1,0 +1,143 @@
+/*
+ * ibpm_b200.h -- C ABI of the B200 IBPM time step (libibpm_b200.so).
+ *
+ * Plain C: opaque handles, plain pointers and sizes, int status returns
+ * (0 = success, < 0 = error; ibg_last_error() says why).  No call aborts.
+ *
+ * Array layouts are the reference's own, so a host State can be moved in
+ * and out without reshuffling (paths are inside the reference project):
+ *   Scalar (omega, psi, rhs): [lev][i-1][j-1], lev < ngrid, 1 <= i < nx,
+ *       1 <= j < ny, j fastest                           (src/Scalar.h:76-90)
+ *   Flux (q): [lev][index], x-fluxes i*ny + j (i <= nx, j < ny) then
+ *       y-fluxes (nx+1)*ny + i*(ny+1) + j (i < nx, j <= ny) (src/Flux.h:176-185)
+ *   BoundaryVector (f, b): [fx_0 .. fx_{n-1}, fy_0 .. fy_{n-1}]
+ *                                                    (src/BoundaryVector.h:65-69)
+ *
+ * Each entry point names the reference interface it replaces.
+ */
+#ifndef IBPM_B200_H
+#define IBPM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define IBG_API __attribute__((visibility("default")))
+#else
+#define IBG_API
+#endif
+
+typedef struct ibg_context ibg_context;
+
+/* Grid(nx, ny, ngrid, length, xOffset, yOffset)  (src/Grid.h:36-44) */
+typedef struct {
+    int nx, ny, ngrid;
+    double length, xoffset, yoffset;
+} ibg_grid;
+
+/* motion kinds of a rigid body (src/Motion.h, src/FixedPosition.h, src/PitchPlunge.h) */
+enum { IBG_MOTION_NONE = 0, IBG_MOTION_FIXED = 1, IBG_MOTION_PITCHPLUNGE = 2 };
+
+/* RigidBody: reference points, centre and motion (src/RigidBody.h:35-190).
+ * FIXED: params = (x, y, theta).  PITCHPLUNGE: params = (pitch amplitude,
+ * pitch frequency, pitch phase, plunge amplitude, plunge frequency, plunge
+ * phase) exactly as the geometry file's `motion pitchplunge` line. */
+typedef struct {
+    int npoints;
+    const double* xy;       /* npoints interleaved (x, y) reference points */
+    double xcenter, ycenter;
+    int motion;
+    double params[6];
+} ibg_body;
+
+/* time-stepping schemes (src/Scheme.h:13-61) */
+enum { IBG_SCHEME_EULER = 0, IBG_SCHEME_AB2 = 1, IBG_SCHEME_RK3 = 2, IBG_SCHEME_RK3B = 3 };
+
+/* arithmetic forms of the bulk fields */
+enum { IBG_PRECISION_FP64 = 0, IBG_PRECISION_FP32_REFINED = 1 };
+
+typedef struct {
+    double Re;              /* Reynolds number                                  */
+    double dt;              /* time step                                        */
+    int scheme;             /* IBG_SCHEME_*                                     */
+    double cg_tol;          /* CG tolerance on |r| (moving bodies), 1e-7 default */
+    int cg_max_iter;        /* CG iteration cap (the reference has none that works) */
+    double u_mag;           /* base-flow magnitude (1 in the reference CLI)     */
+    double alpha;           /* base-flow angle in radians                       */
+    int precision;          /* IBG_PRECISION_*                                  */
+} ibg_params;
+
+/* --- lifetime ---------------------------------------------------------------
+ * ibg_create replaces the constructors NavierStokesModel(grid, geom, Re, q0)
+ * (src/NavierStokesModel.cc:19-33) and NonlinearIBSolver(grid, model, dt,
+ * scheme, tol) (src/IBSolver.h:79-86).  `cuda_stream` is a cudaStream_t
+ * (NULL: the library creates its own).  The geometry is moved to time 0 and
+ * the regularizer updated (model->init(), src/NavierStokesModel.cc:52-57). */
+IBG_API int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const ibg_params* params,
+               void* cuda_stream, ibg_context** out);
+IBG_API int ibg_destroy(ibg_context* ctx);
+/* message for the last failed call on ctx (ctx may be NULL for ibg_create) */
+IBG_API const char* ibg_last_error(const ibg_context* ctx);
+
+/* IBSolver::init (src/IBSolver.cc:62-66): builds the Cholesky factor of
+ * M = C A^-1 B for every sub-step (fixed bodies); no-op for moving bodies. */
+IBG_API int ibg_init(ibg_context* ctx);
+/* IBSolver::save / load (src/IBSolver.cc:77-108): <basename>_01.cholesky ...
+ * in the reference's ASCII format (src/CholeskySolver.cc:113-198).
+ * ibg_load returns 1 when every factor was read and matched (n and alpha*beta), 0 otherwise. */
+IBG_API int ibg_save(ibg_context* ctx, const char* basename);
+IBG_API int ibg_load(ibg_context* ctx, const char* basename);
+
+/* --- state -------------------------------------------------------------------
+ * State (src/State.h:25-60): omega, q, f, timestep, time.  `q` may be NULL in
+ * ibg_set_state; then it is recomputed from omega (model->refreshState). */
+IBG_API int ibg_set_state(ibg_context* ctx, const double* omega, const double* q, const double* f, int timestep, double time);
+IBG_API int ibg_get_state(ibg_context* ctx, double* omega, double* q, double* f, int* timestep, double* time);
+/* only f, timestep and time (what the reference CLI reads every step) */
+IBG_API int ibg_get_boundary_force(ibg_context* ctx, double* f, int* timestep, double* time);
+/* NavierStokesModel::updateOperators(time) + refreshState(x) (src/NavierStokesModel.cc:93-99, :127-129) */
+IBG_API int ibg_update_operators(ibg_context* ctx, double time);
+IBG_API int ibg_refresh_state(ibg_context* ctx);
+
+/* IBSolver::advance (src/IBSolver.cc:142-149), nsteps times. */
+IBG_API int ibg_advance(ibg_context* ctx, int nsteps);
+/* State::computeNetForce (src/State.cc:53-63) of the current f */
+IBG_API int ibg_get_net_force(ibg_context* ctx, double* xforce, double* yforce);
+/* net force after each of the last `n` steps (device-side record, oldest first);
+ * returns the number written (<= n, <= steps taken since ibg_set_state) */
+IBG_API int ibg_get_force_history(ibg_context* ctx, int n, double* xy);
+
+/* sizes: total Scalar values (ngrid*(nx-1)*(ny-1)), Flux values, BoundaryVector values */
+IBG_API int ibg_sizes(const ibg_context* ctx, long long* n_scalar, long long* n_flux, int* n_boundary);
+/* CG statistics of the last advance: iterations of the last sub-step solve,
+ * the largest count seen and how many solves hit the cap */
+IBG_API int ibg_cg_stats(const ibg_context* ctx, int* last_iterations, int* max_iterations, int* capped_solves);
+/* the CUDA stream the context launches on (a cudaStream_t) */
+IBG_API void* ibg_stream(const ibg_context* ctx);
+/* number of kernel launches issued by the last ibg_advance call */
+IBG_API long long ibg_last_launch_count(const ibg_context* ctx);
+
+/* --- operator entry points (host buffers, reference layouts) ----------------- */
+/* PoissonSolver::solve (src/EllipticSolver.cc:47-73, :83-94): L u = f on all levels */
+IBG_API int ibg_poisson_solve(ibg_context* ctx, const double* f, double* u);
+/* HelmholtzSolver::solve ((1 + alpha L) u = f), src/EllipticSolver.cc:96-108 */
+IBG_API int ibg_helmholtz_solve(ibg_context* ctx, double alpha, const double* f, double* u);
+/* NonlinearIBSolver::N = Curl(CrossProduct(q, omega)) (src/IBSolver.cc:205-209) */
+IBG_API int ibg_nonlinear(ibg_context* ctx, const double* q, const double* omega, double* out);
+/* Laplacian(Scalar) = -Curl(Curl(f)) (src/VectorOperations.cc:133-146) */
+IBG_API int ibg_laplacian(ibg_context* ctx, const double* f, double* out);
+/* NavierStokesModel::B: Curl(E^T f) (src/NavierStokesModel.cc:101-105) */
+IBG_API int ibg_model_B(ibg_context* ctx, const double* f, double* omega);
+/* NavierStokesModel::C: E(Curl(L^-1(-omega))) (src/NavierStokesModel.cc:107-112) */
+IBG_API int ibg_model_C(ibg_context* ctx, const double* omega, double* f);
+/* Regularizer::toBoundary (src/Regularizer.cc:111-128): level-0 fluxes -> boundary */
+IBG_API int ibg_reg_to_boundary(ibg_context* ctx, const double* q, double* f);
+/* ProjectionSolver::solve for sub-step k's beta (src/ProjectionSolver.cc:57-79):
+ * A omega + B f = a, C omega = b.  f is the warm start on input (CG). */
+IBG_API int ibg_projection_solve(ibg_context* ctx, int substep, const double* a, const double* b, double* omega, double* f);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,189 @@
+"""Parity of the CUDA time step (through the C ABI) with the oracle.
+
+The oracle is the numpy restatement in oracle/ibpm_oracle.py, itself pinned
+to the reference library; the golden fixtures in tests/golden/ come from the
+reference library directly.  FP64 bar: relative L2 <= 1e-10 (operators
+<= 1e-12).
+"""
+import numpy as np
+import pytest
+
+from helpers import FP64_TOL, golden_names, load_golden, oracle_from_golden, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+OP_TOL = 1e-12
+
+
+def _solver_for(gp, pts, Re=100.0, dt=0.01, scheme="rk3", motion=None, tol=1e-7):
+    import ibpm_b200 as ib
+    from ibpm_b200 import geometry
+    grid = ib.Grid(*gp)
+    body = geometry.RigidBody(points=[tuple(p) for p in pts])
+    if motion is not None:
+        body.motion, body.params, body.center = motion
+    geo = geometry.Geometry([body])
+    model = ib.NavierStokesModel(grid, geo, Re)
+    return grid, model, ib.NonlinearIBSolver(grid, model, dt, scheme, tol)
+
+
+GRIDS = [(16, 16, 1, 2.0, -1.0, -1.0), (32, 16, 3, 3.0, -1.5, -0.75), (64, 64, 2, 4.0, -2.0, -2.0),
+         (40, 24, 4, 2.0, -1.0, -0.6)]
+
+
+@pytest.mark.parametrize("gp", GRIDS)
+def test_elliptic_and_stencils(gp):
+    from oracle import ibpm_oracle as O
+    g = O.Grid(*gp)
+    pts = O.circle_points(0.0, 0.0, 0.2 * gp[3] / 2, 12)
+    grid, model, s = _solver_for(gp, pts)
+    rng = np.random.default_rng(sum(gp[:3]))
+    f = rng.standard_normal(g.scalar().shape)
+    q = rng.standard_normal(g.flux().shape)
+    assert rel_l2(s.poisson(f), O.EllipticSolver(g, "poisson").solve(f)) < OP_TOL
+    assert rel_l2(s.helmholtz(-0.0123, f), O.EllipticSolver(g, "helmholtz", -0.0123).solve(f)) < OP_TOL
+    assert rel_l2(s.nonlinear(q, f), O.nonlinear(g, q, f)) < OP_TOL
+    assert rel_l2(s.laplacian(f), O.laplacian(g, f)) < OP_TOL
+    reg = O.Regularizer(g)
+    reg.update(pts)
+    fb = rng.standard_normal(2 * len(pts))
+    assert rel_l2(s.model_B(fb), O.curl_flux(g, reg.to_flux(fb))) < OP_TOL
+    model_o = O.Model(g, [O.Body(pts)], 100.0)
+    assert rel_l2(s.model_C(f), model_o.C(f)) < OP_TOL
+    assert rel_l2(s.reg_to_boundary(q[0]), reg.to_boundary(q)) < OP_TOL
+    s.close()
+
+
+def test_multidomain_inverse_property_full_size():
+    """L(solve(f)) = coarsify(f) on every level at the 400x200, 5-level size
+    (the reference's EllipticSolverTest property, src test/EllipticSolverTest.cc:86-121)."""
+    from oracle import ibpm_oracle as O
+    gp = (400, 200, 5, 8.0, -2.0, -2.0)
+    g = O.Grid(*gp)
+    grid, model, s = _solver_for(gp, O.circle_points(0, 0, 0.5, 157))
+    rng = np.random.default_rng(0)
+    f = rng.standard_normal(g.scalar().shape)
+    u = s.poisson(f)
+    Lu = s.laplacian(u)
+    cf = O.coarsify(g, f)
+    # the multi-domain Laplacian uses boundary values from the coarser level, exactly as the solve
+    assert rel_l2(Lu, cf) < 1e-9
+    s.close()
+
+
+def test_projection_matches_oracle():
+    from oracle import ibpm_oracle as O
+    gp = (48, 32, 2, 3.0, -1.5, -1.0)
+    g = O.Grid(*gp)
+    pts = O.circle_points(0.1, 0.05, 0.35, 24)
+    grid, model, s = _solver_for(gp, pts, Re=150.0, dt=0.02)
+    s.init()
+    mo = O.Model(g, [O.Body(pts)], 150.0)
+    rng = np.random.default_rng(5)
+    a = rng.standard_normal(g.scalar().shape)
+    b = rng.standard_normal(48)
+    beta0 = (8. / 15.) * 0.02
+    ps = O.ProjectionSolver(mo, beta0)
+    ps.init()
+    w_o, f_o = ps.solve(a, b, np.zeros(48))
+    w_g, f_g = s.projection_solve(0, a, b, np.zeros(48))
+    assert rel_l2(w_g, w_o) < 1e-11
+    assert rel_l2(f_g, f_o) < 1e-10
+    s.close()
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_time_step_matches_reference_golden(name):
+    import ibpm_b200 as ib
+    d = load_golden(name)
+    grid = ib.Grid(int(d["nx"]), int(d["ny"]), int(d["ngrid"]), float(d["length"]), float(d["xoffset"]),
+                   float(d["yoffset"]))
+    geo = ib.geometry.parse(str(d["geom"]))
+    model = ib.NavierStokesModel(grid, geo, float(d["Re"]))
+    s = ib.NonlinearIBSolver(grid, model, float(d["dt"]), str(d["scheme"]), float(d["tol"]))
+    x = ib.State(grid, geo.num_points, omega=np.array(d["omega0"], dtype=float))
+    s.init()
+    s.set_state(x, with_q=False)
+    n = int(d["nsteps"])
+    s.advance_resident(n)
+    forces = s.force_history(n)
+    s.get_state(x)
+    assert rel_l2(forces, d["forces"][:, 2:4]) < FP64_TOL
+    assert rel_l2(x.omega, d["omega"]) < FP64_TOL
+    assert rel_l2(x.q, d["q"]) < FP64_TOL
+    assert rel_l2(x.f, d["f"]) < 1e-9
+    assert x.timestep == int(d["timestep"])
+    assert abs(x.time - float(d["time"])) < 1e-12
+    s.close()
+
+
+def test_drop_in_advance_keeps_host_state():
+    """advance(State&) leaves the host State valid after every call, like the reference."""
+    import ibpm_b200 as ib
+    d = load_golden("cyl_l1_rk3")
+    grid = ib.Grid(48, 48, 1, 4.0, -2.0, -2.0)
+    geo = ib.geometry.parse(str(d["geom"]))
+    model = ib.NavierStokesModel(grid, geo, float(d["Re"]))
+    s = ib.NonlinearIBSolver(grid, model, float(d["dt"]), "rk3")
+    s.init()
+    x = ib.State(grid, geo.num_points)
+    s.refresh_state(x)
+    F = []
+    for _ in range(int(d["nsteps"])):
+        s.advance(x)
+        F.append(x.computeNetForce())
+    assert rel_l2(np.array(F), d["forces"][:, 2:4]) < FP64_TOL
+    assert rel_l2(x.omega, d["omega"]) < FP64_TOL
+    s.close()
+
+
+def test_cholesky_save_load_roundtrip(tmp_path):
+    import ibpm_b200 as ib
+    d = load_golden("cyl_l1_rk3")
+    grid = ib.Grid(48, 48, 1, 4.0, -2.0, -2.0)
+    geo = ib.geometry.parse(str(d["geom"]))
+    model = ib.NavierStokesModel(grid, geo, float(d["Re"]))
+    s = ib.NonlinearIBSolver(grid, model, float(d["dt"]), "rk3")
+    s.init()
+    base = str(tmp_path / "run")
+    assert s.save(base)
+    s2 = ib.NonlinearIBSolver(grid, model, float(d["dt"]), "rk3")
+    assert s2.load(base)
+    x = ib.State(grid, geo.num_points)
+    s2.set_state(x, with_q=False)
+    s2.advance_resident(int(d["nsteps"]))
+    assert rel_l2(s2.force_history(int(d["nsteps"])), d["forces"][:, 2:4]) < FP64_TOL
+    # a factor for another dt is rejected (src/CholeskySolver.cc:131-136)
+    s3 = ib.NonlinearIBSolver(grid, model, float(d["dt"]) * 2, "rk3")
+    assert not s3.load(base)
+    for h in (s, s2, s3):
+        h.close()
+
+
+def test_c1_size_steps_match_oracle():
+    """The 200x200 fixed-cylinder workload: a few steps against the oracle."""
+    from ibpm_b200 import configs
+    import ibpm_b200 as ib
+    from oracle import ibpm_oracle as O
+    wl = configs.c1_fixed_cylinder()
+    grid, model, s, x = ib.from_workload(wl)
+    s.init()
+    s.set_state(x, with_q=False)
+    nsteps = 4
+    s.advance_resident(nsteps)
+    fg = s.force_history(nsteps)
+    s.get_state(x)
+    g = O.Grid(wl.nx, wl.ny, wl.ngrid, wl.length, wl.xoffset, wl.yoffset)
+    geo = ib.geometry.parse(wl.geom)
+    mo = O.Model(g, [O.Body(np.array(geo.bodies[0].points))], wl.Re)
+    so = O.IBSolver(mo, wl.dt, "rk3")
+    so.init()
+    xo = O.State(g, mo.npts)
+    xo.q = mo.flux(xo.omega)
+    fo = []
+    for _ in range(nsteps):
+        so.advance(xo)
+        fo.append(xo.net_force())
+    assert rel_l2(fg, np.array(fo)) < FP64_TOL
+    assert rel_l2(x.omega, xo.omega) < FP64_TOL
+    s.close()
