@@ -113,7 +113,8 @@ class NonlinearIBSolver:
     """
 
     def __init__(self, grid: Grid, model: NavierStokesModel, dt: float, scheme: str = "rk3", tol: float = 1e-7,
-                 precision: str = "fp64", stream: Optional[int] = None, cg_max_iter: int = 3000):
+                 precision: str = "fp64", stream: Optional[int] = None, cg_max_iter: int = 3000,
+                 device: int = -1):
         self.grid, self.model, self.dt = grid, model, dt
         self.scheme = scheme
         L = lib()
@@ -130,7 +131,7 @@ class NonlinearIBSolver:
             for j in range(6):
                 bodies[k].params[j] = b.params[j] if j < len(b.params) else 0.0
         p = ibg_params(model.Re, dt, SCHEMES[scheme], tol, cg_max_iter, model.u_mag, model.alpha,
-                       PRECISIONS[precision])
+                       PRECISIONS[precision], device)
         h = ctypes.c_void_p()
         check(L.ibg_create(ctypes.byref(g), len(model.geom.bodies), bodies, ctypes.byref(p),
                            ctypes.c_void_p(stream) if stream else None, ctypes.byref(h)), None)
@@ -260,12 +261,13 @@ class NonlinearIBSolver:
         return w, f
 
 
-def from_workload(wl, precision: str = "fp64", stream=None):
+def from_workload(wl, precision: str = "fp64", stream=None, device: int = -1):
     """Grid, model, solver and initial State for an ibpm_b200.configs.Workload."""
     grid = Grid(wl.nx, wl.ny, wl.ngrid, wl.length, wl.xoffset, wl.yoffset)
     geo = _geometry.parse(wl.geom)
     model = NavierStokesModel(grid, geo, wl.Re)
-    solver = NonlinearIBSolver(grid, model, wl.dt, wl.scheme, wl.tol, precision=precision, stream=stream)
+    solver = NonlinearIBSolver(grid, model, wl.dt, wl.scheme, wl.tol, precision=precision, stream=stream,
+                               device=device)
     x = State(grid, geo.num_points)
     w0 = wl.initial_vorticity()
     if w0 is not None:

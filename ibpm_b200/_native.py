@@ -27,7 +27,7 @@ class ibg_body(ctypes.Structure):
 class ibg_params(ctypes.Structure):
     _fields_ = [("Re", ctypes.c_double), ("dt", ctypes.c_double), ("scheme", ctypes.c_int),
                 ("cg_tol", ctypes.c_double), ("cg_max_iter", ctypes.c_int), ("u_mag", ctypes.c_double),
-                ("alpha", ctypes.c_double), ("precision", ctypes.c_int)]
+                ("alpha", ctypes.c_double), ("precision", ctypes.c_int), ("device", ctypes.c_int)]
 
 
 SCHEMES = {"euler": 0, "ab2": 1, "rk3": 2, "rk3b": 3}
@@ -58,6 +58,7 @@ SIGNATURES = {
     "ibg_cg_stats": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     "ibg_stream": (_VP, [_VP]),
     "ibg_last_launch_count": (ctypes.c_longlong, [_VP]),
+    "ibg_run_kernel": (ctypes.c_longlong, [_VP, _I, _I]),
     "ibg_poisson_solve": (_I, [_VP, _VP, _VP]),
     "ibg_helmholtz_solve": (_I, [_VP, _D, _VP, _VP]),
     "ibg_nonlinear": (_I, [_VP, _VP, _VP, _VP]),

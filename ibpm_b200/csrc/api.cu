@@ -101,6 +101,7 @@ struct ibg_context {
     double* Lr[4] = {nullptr, nullptr, nullptr, nullptr};
     double* Lc[4] = {nullptr, nullptr, nullptr, nullptr};
     double* Ld[4] = {nullptr, nullptr, nullptr, nullptr};
+    double* Mi[4] = {nullptr, nullptr, nullptr, nullptr};  // explicit M^-1 = L^-T L^-1 per sub-step
     bool chol_ready = false;
     int* d_status = nullptr;
     // CG
@@ -151,7 +152,8 @@ struct ibg_context {
             if (Lr[k]) cudaFree(Lr[k]);
             if (Lc[k]) cudaFree(Lc[k]);
             if (Ld[k]) cudaFree(Ld[k]);
-            Nbuf[k] = Lr[k] = Lc[k] = Ld[k] = nullptr;
+            if (Mi[k]) cudaFree(Mi[k]);
+            Nbuf[k] = Lr[k] = Lc[k] = Ld[k] = Mi[k] = nullptr;
         }
         if (h_flags) cudaFreeHost(h_flags);
         h_flags = nullptr;
@@ -231,7 +233,7 @@ struct ibg_context {
         launch_reg_interp<double>(g, ncomp, slots, psi, S, 1, b_in, rhsb, 0, st);  // C omega* - b
         launches += 2 * solve_launches() + 1;
         if (!moving) {
-            chol_solve(ncomp, Lr[k], Lc[k], Ld[k], rhsb, f, st);        // f = M^-1 rhs
+            minv_apply(ncomp, Mi[k], rhsb, f, st);                        // f = M^-1 rhs
             launches += 1;
         } else {
             int s = cg_solve(k, rhsb, f);
@@ -369,6 +371,10 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
         g_create_error = "ibg_create: 2*nx and 2*ny must factor into primes <= 13";
         return IBG_ERR_UNSUPPORTED;
     }
+    if (params->device >= 0 && cudaSetDevice(params->device) != cudaSuccess) {
+        g_create_error = "ibg_create: cannot select the requested CUDA device";
+        return IBG_ERR_CUDA;
+    }
     auto* c = new ibg_context();
     c->prm = *params;
     if (c->prm.cg_max_iter <= 0) c->prm.cg_max_iter = 3000;
@@ -467,7 +473,7 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
         c->alloc(&c->btmp, m) || c->alloc(&c->qtmp, F) || c->alloc(&c->d_ref, 2 * (size_t)c->npts) ||
         c->alloc(&c->d_pts, 2 * (size_t)c->npts) || c->alloc(&c->d_vel, 2 * (size_t)c->npts) ||
         c->alloc(&c->d_body_of, (size_t)c->npts) || c->alloc(&c->d_bodies, c->h_bodies.size()) ||
-        c->alloc(&c->slots.idx, 9 * m) || c->alloc(&c->slots.w, 9 * m) || c->alloc(&c->slots.n, m) ||
+        c->alloc(&c->slots.idx, kSlots * m) || c->alloc(&c->slots.w, kSlots * m) || c->alloc(&c->slots.n, m) ||
         c->alloc(&c->d_b, m) || c->alloc(&c->d_time, 1) || c->alloc(&c->d_status, 1) || c->alloc(&c->cg_r, m) ||
         c->alloc(&c->cg_d, m) || c->alloc(&c->cg_q, m) || c->alloc(&c->cg_scal, 4) || c->alloc(&c->cg_flags, 4) ||
         c->alloc(&c->d_hist, 2 * (size_t)kHistCap) || c->alloc(&c->d_hist_count, 1);
@@ -529,7 +535,7 @@ int ibg_init(ibg_context* c) {
             c->alloc(&Mcol, (size_t)m * m, false);
     for (int k = 0; k < c->sch.nsub && !s; ++k)
         s = c->alloc(&c->Lr[k], (size_t)m * m, false) || c->alloc(&c->Lc[k], (size_t)m * m, false) ||
-            c->alloc(&c->Ld[k], (size_t)m, false);
+            c->alloc(&c->Ld[k], (size_t)m, false) || c->alloc(&c->Mi[k], (size_t)m * m, false);
     if (s) {
         cudaFree(bf); cudaFree(u); cudaFree(p); cudaFree(rcb); cudaFree(tb); cudaFree(fl); cudaFree(Mcol);
         return c->fail(IBG_ERR_CUDA, "ibg_init: not enough device memory for the Cholesky build");
@@ -547,6 +553,7 @@ int ibg_init(ibg_context* c) {
             launch_reg_interp<double>(g, m, c->slots, p, S, nb, nullptr, Mcol + (size_t)col0 * m, (size_t)m, c->st);
         }
         s = chol_factor(m, Mcol, c->Lr[k], c->Lc[k], c->Ld[k], c->d_status, c->st);
+        if (!s) chol_inverse(m, c->Lr[k], c->Lc[k], c->Ld[k], c->Mi[k], c->st);
         int hs = 0;
         cudaMemcpyAsync(&hs, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->st);
         if (cudaStreamSynchronize(c->st) != cudaSuccess) s = c->cuda_check("ibg_init");
@@ -611,7 +618,7 @@ int ibg_load(ibg_context* c, const char* basename) {
     }
     for (int k = 0; k < c->sch.nsub; ++k) {
         if (!c->Lr[k] && (c->alloc(&c->Lr[k], (size_t)m * m) || c->alloc(&c->Lc[k], (size_t)m * m) ||
-                          c->alloc(&c->Ld[k], (size_t)m)))
+                          c->alloc(&c->Ld[k], (size_t)m) || c->alloc(&c->Mi[k], (size_t)m * m)))
             return IBG_ERR_CUDA;
         std::vector<double> Lc((size_t)m * m, 0.0);
         for (int i = 0; i < m; ++i)
@@ -619,7 +626,9 @@ int ibg_load(ibg_context* c, const char* basename) {
         cudaMemcpy(c->Lr[k], Ls[k].data(), sizeof(double) * m * m, cudaMemcpyHostToDevice);
         cudaMemcpy(c->Lc[k], Lc.data(), sizeof(double) * m * m, cudaMemcpyHostToDevice);
         cudaMemcpy(c->Ld[k], Ds[k].data(), sizeof(double) * m, cudaMemcpyHostToDevice);
+        chol_inverse(m, c->Lr[k], c->Lc[k], c->Ld[k], c->Mi[k], c->st);
     }
+    cudaStreamSynchronize(c->st);
     c->chol_ready = true;
     return c->cuda_check("ibg_load") ? IBG_ERR_CUDA : 1;
 }
@@ -845,6 +854,22 @@ int ibg_projection_solve(ibg_context* c, int k, const double* ain, const double*
     cudaMemcpyAsync(omega, c->w, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
     cudaMemcpyAsync(fio, c->f, sizeof(double) * c->ncomp, cudaMemcpyDeviceToHost, c->st);
     return finish(c, "ibg_projection_solve");
+}
+
+long long ibg_run_kernel(ibg_context* c, int which, int reps) {
+    if (!c || reps < 0) return IBG_ERR_ARG;
+    const GridDev& g = c->g;
+    long long bytes = 0;
+    for (int r = 0; r < reps; ++r) {
+        if (which == 0) c->poisson.run_pass(0, c->a, c->tbuf, c->st);
+        else if (which == 1) c->poisson.run_pass(1, c->tbuf, c->tbuf, c->st);
+        else if (which == 2) launch_nonlinear<double>(g, c->q, c->w, c->U, c->V, c->C, c->Nbuf[0], 1, c->S, c->F, c->st);
+        else return IBG_ERR_ARG;
+    }
+    if (which == 0 || which == 1) bytes = 16LL * g.N1;                 // one level read + written once
+    else bytes = 8LL * (long long)(c->F + c->S + 2 * c->S + c->F + c->F + c->S);  // q,w in; U,V; C; N
+    if (c->cuda_check("ibg_run_kernel")) return IBG_ERR_CUDA;
+    return bytes;
 }
 
 }  // extern "C"

@@ -464,6 +464,30 @@ int EllipticPlan<T>::solve(const SolveCall<T>& c, cudaStream_t st) const {
 }
 
 template <typename T>
+void EllipticPlan<T>::run_pass(int which, const T* in, T* tbuf, cudaStream_t st) const {
+    const GridDev& g = *grid;
+    const FftDesc& frow = sizeof(T) == 8 ? tables->row64 : tables->row32;
+    const FftDesc& fcol = sizeof(T) == 8 ? tables->col64 : tables->col32;
+    const int Pr = rows_pairs, Pc = cols_pairs;
+    if (which == 0) {
+        RowPassArgs<T> A{};
+        A.g = g; A.fft = frow; A.pairs_per_block = Pr; A.in = in; A.out = tbuf;
+        A.in_bstride = g.N1; A.out_bstride = g.N1; A.lift = 1; A.in_scale = (T)1; A.coarse = nullptr;
+        A.norm = (T)1;
+        const int npairs_r = (g.NI + 1) / 2;
+        k_dst_rows<T><<<dim3((unsigned)((npairs_r + Pr - 1) / Pr), 1), threads, fft_smem_bytes<T>(frow.m, Pr), st>>>(A);
+    } else {
+        ColPassArgs<T> B{};
+        B.g = g; B.fft = fcol; B.pairs_per_block = Pc; B.buf = tbuf; B.bstride = g.N1;
+        B.cosx = (const T*)(sizeof(T) == 8 ? (const void*)cos64x : (const void*)cos32x);
+        B.cosy = (const T*)(sizeof(T) == 8 ? (const void*)cos64y : (const void*)cos32y);
+        B.bydx2 = (T)(1.0 / (g.dx * g.dx)); B.helmholtz = helmholtz; B.alpha = (T)alpha;
+        const int ncolblk = (g.NJ + 2 * Pc - 1) / (2 * Pc);
+        k_dst_cols<T><<<dim3((unsigned)ncolblk, 1), threads, fft_smem_bytes<T>(fcol.m, Pc), st>>>(B);
+    }
+}
+
+template <typename T>
 int EllipticPlan<T>::init(const GridDev* g, const FftTables* t, bool helm, double a, const CosTables& ct) {
     grid = g;
     tables = t;

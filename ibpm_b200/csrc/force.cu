@@ -67,16 +67,14 @@ __global__ void __launch_bounds__(1024) k_chol_factor(int m, const double* __res
 }
 
 // ---------------------------------------------------------------------------
-// Forward then backward substitution with 32-row blocks.  One CTA of 1024
-// threads; x in shared memory.  Off-diagonal block products are spread over
-// 32 warps; each diagonal block is solved by warp 0 with shuffles.
+// Forward then backward substitution with 32-row blocks (CholeskySolver::Minv,
+// src/CholeskySolver.cc:200-224) on a vector held in shared memory: x holds b
+// on entry and the solution on exit.  Needs blockDim.x == 1024.  Off-diagonal
+// block products are spread over 32 warps; each diagonal block is solved by
+// warp 0 with shuffles.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_chol_solve(int m, const double* __restrict__ Lr, const double* __restrict__ Lc,
-                                                     const double* __restrict__ diag, const double* __restrict__ b,
-                                                     double* __restrict__ x_out) {
-    extern __shared__ double sh[];
-    double* x = sh;                 // m
-    double* red = sh + m;           // 32 x 33
+__device__ void chol_subst(int m, const double* __restrict__ Lr, const double* __restrict__ Lc,
+                           const double* __restrict__ diag, double* x, double* red) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int nb = (m + 31) / 32;
     // forward: L y = b
@@ -91,7 +89,7 @@ __global__ void __launch_bounds__(1024) k_chol_solve(int m, const double* __rest
         if (w == 0) {
             double s = 0.0;
             for (int ww = 0; ww < 32; ++ww) s += red[ww * 33 + lane];
-            double rhs = (r < m) ? b[r] - s : 0.0;
+            double rhs = (r < m) ? x[r] - s : 0.0;
             double mine = 0.0;
             for (int c = 0; c < 32 && r0 + c < m; ++c) {
                 const double xc = __shfl_sync(0xffffffffu, rhs, c) / diag[r0 + c];
@@ -126,7 +124,46 @@ __global__ void __launch_bounds__(1024) k_chol_solve(int m, const double* __rest
         }
         __syncthreads();
     }
+}
+
+__global__ void __launch_bounds__(1024) k_chol_solve(int m, const double* __restrict__ Lr, const double* __restrict__ Lc,
+                                                     const double* __restrict__ diag, const double* __restrict__ b,
+                                                     double* __restrict__ x_out) {
+    extern __shared__ double sh[];
+    double* x = sh;
+    double* red = sh + m;
+    for (int k = threadIdx.x; k < m; k += blockDim.x) x[k] = b[k];
+    __syncthreads();
+    chol_subst(m, Lr, Lc, diag, x, red);
     for (int k = threadIdx.x; k < m; k += blockDim.x) x_out[k] = x[k];
+}
+
+// M^-1 column j by substitution on e_j, one CTA per column; stored as row j
+// of Minv (Minv[i*m + j] = (M^-1 e_j)_i, so that row i of Minv is contiguous).
+__global__ void __launch_bounds__(1024) k_chol_inverse(int m, const double* __restrict__ Lr,
+                                                       const double* __restrict__ Lc, const double* __restrict__ diag,
+                                                       double* __restrict__ Minv) {
+    extern __shared__ double sh[];
+    double* x = sh;
+    double* red = sh + m;
+    const int j = blockIdx.x;
+    for (int k = threadIdx.x; k < m; k += blockDim.x) x[k] = (k == j) ? 1.0 : 0.0;
+    __syncthreads();
+    chol_subst(m, Lr, Lc, diag, x, red);
+    for (int k = threadIdx.x; k < m; k += blockDim.x) Minv[(size_t)k * m + j] = x[k];
+}
+
+// y = Minv b: one warp per row
+__global__ void k_minv_apply(int m, const double* __restrict__ Minv, const double* __restrict__ b,
+                             double* __restrict__ y) {
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= m) return;
+    const double* a = Minv + (size_t)row * m;
+    double acc = 0.0;
+    for (int k = lane; k < m; k += 32) acc += a[k] * b[k];
+    acc = warp_sum(acc);
+    if (lane == 0) y[row] = acc;
 }
 
 // ---------------------------------------------------------------------------
@@ -223,9 +260,19 @@ void chol_solve(int m, const double* Lr, const double* Lc, const double* diag, c
 int chol_solve_prepare(int m) {
     const size_t sm = sizeof(double) * (m + 32 * 33);
     if (sm > 200 * 1024) return IBG_ERR_UNSUPPORTED;
-    return cudaFuncSetAttribute(k_chol_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) == cudaSuccess
-               ? IBG_OK
-               : IBG_ERR_CUDA;
+    if (cudaFuncSetAttribute(k_chol_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess ||
+        cudaFuncSetAttribute(k_chol_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+        return IBG_ERR_CUDA;
+    return IBG_OK;
+}
+
+void chol_inverse(int m, const double* Lr, const double* Lc, const double* diag, double* Minv, cudaStream_t st) {
+    const size_t sm = sizeof(double) * (m + 32 * 33);
+    k_chol_inverse<<<m, 1024, sm, st>>>(m, Lr, Lc, diag, Minv);
+}
+
+void minv_apply(int m, const double* Minv, const double* b, double* y, cudaStream_t st) {
+    k_minv_apply<<<(m + 7) / 8, 256, 0, st>>>(m, Minv, b, y);
 }
 
 void cg_begin(int m, const double* b, const double* Mx, double* r, double* d, double* scal, int* flags,

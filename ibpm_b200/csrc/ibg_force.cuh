@@ -7,6 +7,8 @@ int chol_factor(int m, const double* Mcol, double* Lr, double* Lc, double* diag,
 int chol_solve_prepare(int m);
 void chol_solve(int m, const double* Lr, const double* Lc, const double* diag, const double* b, double* x,
                 cudaStream_t st);
+void chol_inverse(int m, const double* Lr, const double* Lc, const double* diag, double* Minv, cudaStream_t st);
+void minv_apply(int m, const double* Minv, const double* b, double* y, cudaStream_t st);
 void cg_begin(int m, const double* b, const double* Mx, double* r, double* d, double* scal, int* flags,
               cudaStream_t st);
 void cg_update(int m, double* x, double* r, double* d, const double* q, double* scal, int* flags, cudaStream_t st);

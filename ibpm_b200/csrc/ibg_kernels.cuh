@@ -84,6 +84,8 @@ struct EllipticPlan {
     const float* cos32y = nullptr;
     int init(const GridDev* g, const FftTables* t, bool helm, double a, const CosTables& ct);
     int solve(const SolveCall<T>& c, cudaStream_t st) const;
+    // one pass of the finest level alone (0: rows of pass A, 1: columns of pass B), for timing
+    void run_pass(int which, const T* in, T* tbuf, cudaStream_t st) const;
 };
 
 }  // namespace ibg

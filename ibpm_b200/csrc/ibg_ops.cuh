@@ -12,10 +12,11 @@ struct BodyDev {
     double p[6];
 };
 
-// Regularizer association slots: up to 9 level-0 fluxes per boundary component.
+// Regularizer association slots: up to kSlots level-0 fluxes per boundary component.
+constexpr int kSlots = 16;
 struct RegSlots {
-    int* idx = nullptr;     // [2 npts][9] flux index (level 0)
-    double* w = nullptr;    // [2 npts][9] weight delta(dx) delta(dy)
+    int* idx = nullptr;     // [2 npts][kSlots] flux index (level 0)
+    double* w = nullptr;    // [2 npts][kSlots] weight delta(dx) delta(dy)
     int* n = nullptr;       // [2 npts] number of slots used
 };
 

@@ -305,8 +305,10 @@ __device__ __forceinline__ double delta_fn(double r) {
     return (5 - 3 * r - sqrt(1 - 3 * (1 - r) * (1 - r))) / 6;
 }
 
-// Association slots per boundary component c = dir*npts + p: up to 9 level-0
-// fluxes within 1.5 cells in both directions, in increasing flux index, and
+// Association slots per boundary component c = dir*npts + p: the level-0
+// fluxes within 1.5 cells in both directions (3 x 3 in exact arithmetic, up to
+// 4 x 4 when rounding puts a flux at exactly 1.5 cells), in increasing flux
+// index, and
 // the constraint b_c = body velocity - E(q0)_c.
 __global__ void k_reg_update(GridDev g, int npts, const double* __restrict__ pts, const double* __restrict__ vel,
                              int* __restrict__ sidx, double* __restrict__ sw, int* __restrict__ sn,
@@ -339,10 +341,10 @@ __global__ void k_reg_update(GridDev g, int npts, const double* __restrict__ pts
                                        : __dadd_rn(g.y0, __dmul_rn((double)j, h));
             const double dyn = fabs(fy - py) / h;
             if (!(dyn < 1.5)) continue;
-            if (n < 9) {
+            if (n < kSlots) {
                 const double wgt = delta_fn(dxn) * delta_fn(dyn);
-                sidx[c * 9 + n] = base + i * stride + j;
-                sw[c * 9 + n] = wgt;
+                sidx[c * kSlots + n] = base + i * stride + j;
+                sw[c * kSlots + n] = wgt;
                 e = e + wgt * q0;
                 ++n;
             }
@@ -364,7 +366,7 @@ __global__ void k_reg_interp(GridDev g, int ncomp, const int* __restrict__ sidx,
     const T* cc = g.L > 1 ? f + g.N1 : nullptr;
     double acc = 0.0;
     const int n = sn[c];
-    for (int k = 0; k < n; ++k) acc = acc + sw[c * 9 + k] * (double)curl_scalar_at(g, f, cc, sidx[c * 9 + k]);
+    for (int k = 0; k < n; ++k) acc = acc + sw[c * kSlots + k] * (double)curl_scalar_at(g, f, cc, sidx[c * kSlots + k]);
     double v = acc / g.dx;
     if (bcon) v = v - bcon[c];
     out[(size_t)blockIdx.y * ostride + c] = v;
@@ -374,9 +376,9 @@ __global__ void k_reg_interp(GridDev g, int ncomp, const int* __restrict__ sidx,
 __global__ void k_reg_smear(int ncomp, const int* __restrict__ sidx, const double* __restrict__ sw,
                             const int* __restrict__ sn, const double* __restrict__ f, double* __restrict__ flux0) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int c = t / 9, k = t % 9;
+    const int c = t / kSlots, k = t % kSlots;
     if (c >= ncomp || k >= sn[c]) return;
-    atomicAdd(&flux0[sidx[c * 9 + k]], sw[c * 9 + k] * f[c]);
+    atomicAdd(&flux0[sidx[c * kSlots + k]], sw[c * kSlots + k] * f[c]);
 }
 
 // batched smear of unit vectors: item b carries e_{col0+b}
@@ -386,7 +388,7 @@ __global__ void k_reg_smear_unit(int ncomp, int col0, const int* __restrict__ si
     const int c = col0 + b;
     const int k = threadIdx.x;
     if (c >= ncomp || k >= sn[c]) return;
-    flux0[(size_t)b * fstride + sidx[c * 9 + k]] = sw[c * 9 + k];
+    flux0[(size_t)b * fstride + sidx[c * kSlots + k]] = sw[c * kSlots + k];
 }
 
 __global__ void k_reg_zero(int ncomp, int col0, int unit, const int* __restrict__ sidx, const int* __restrict__ sn,
@@ -394,13 +396,13 @@ __global__ void k_reg_zero(int ncomp, int col0, int unit, const int* __restrict_
     if (unit) {
         const int b = blockIdx.x, c = col0 + b, k = threadIdx.x;
         if (c >= ncomp || k >= sn[c]) return;
-        flux0[(size_t)b * fstride + sidx[c * 9 + k]] = 0.0;
+        flux0[(size_t)b * fstride + sidx[c * kSlots + k]] = 0.0;
         return;
     }
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int c = t / 9, k = t % 9;
+    const int c = t / kSlots, k = t % kSlots;
     if (c >= ncomp || k >= sn[c]) return;
-    flux0[sidx[c * 9 + k]] = 0.0;
+    flux0[sidx[c * kSlots + k]] = 0.0;
 }
 
 // Bf on level 0: beta * Curl(flux0 * dx); coarser levels of Bf stay zero
@@ -459,7 +461,7 @@ __global__ void k_reg_gather(int ncomp, const int* __restrict__ sidx, const doub
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncomp) return;
     double acc = 0.0;
-    for (int k = 0; k < sn[c]; ++k) acc = acc + sw[c * 9 + k] * q0[sidx[c * 9 + k]];
+    for (int k = 0; k < sn[c]; ++k) acc = acc + sw[c * kSlots + k] * q0[sidx[c * kSlots + k]];
     out[c] = acc / dx;
 }
 
@@ -494,9 +496,9 @@ void launch_reg_interp(const GridDev& g, int ncomp, const RegSlots& s, const T* 
 template <typename T>
 void launch_smear_bf(const GridDev& g, int ncomp, const RegSlots& s, const double* f, double* flux0, T* Bf,
                      double beta, cudaStream_t st) {
-    k_reg_smear<<<nblk((size_t)ncomp * 9, 128), 128, 0, st>>>(ncomp, s.idx, s.w, s.n, f, flux0);
+    k_reg_smear<<<nblk((size_t)ncomp * kSlots, 128), 128, 0, st>>>(ncomp, s.idx, s.w, s.n, f, flux0);
     k_bf<T><<<dim3(nblk(g.N1, 256), 1), 256, 0, st>>>(g, flux0, 0, Bf, 0, beta);
-    k_reg_zero<<<nblk((size_t)ncomp * 9, 128), 128, 0, st>>>(ncomp, 0, 0, s.idx, s.n, flux0, 0);
+    k_reg_zero<<<nblk((size_t)ncomp * kSlots, 128), 128, 0, st>>>(ncomp, 0, 0, s.idx, s.n, flux0, 0);
 }
 
 template <typename T>

@@ -66,6 +66,7 @@ typedef struct {
     double u_mag;           /* base-flow magnitude (1 in the reference CLI)     */
     double alpha;           /* base-flow angle in radians                       */
     int precision;          /* IBG_PRECISION_*                                  */
+    int device;             /* CUDA device ordinal, -1 = the calling thread's current device */
 } ibg_params;
 
 /* --- lifetime ---------------------------------------------------------------
@@ -117,6 +118,12 @@ IBG_API int ibg_cg_stats(const ibg_context* ctx, int* last_iterations, int* max_
 IBG_API void* ibg_stream(const ibg_context* ctx);
 /* number of kernel launches issued by the last ibg_advance call */
 IBG_API long long ibg_last_launch_count(const ibg_context* ctx);
+
+/* diagnostics: launch one kernel of the time step `reps` times on the context's
+ * stream (0: DST-I row pass of the finest level, 1: its column pass with the
+ * eigenvalue scaling, 2: the nonlinear term) and return the algorithmic bytes
+ * one launch moves (each operand read once, each result written once). */
+IBG_API long long ibg_run_kernel(ibg_context* ctx, int which, int reps);
 
 /* --- operator entry points (host buffers, reference layouts) ----------------- */
 /* PoissonSolver::solve (src/EllipticSolver.cc:47-73, :83-94): L u = f on all levels */

@@ -12,7 +12,7 @@
 // usage: ref_driver -nx N -ny N -ngrid L -length X -xoffset X -yoffset X
 //                   -geom FILE -Re R -dt DT -scheme rk3|euler|ab2|rk3b
 //                   -nsteps K [-tol T] [-alpha DEG] [-ic restart.bin]
-//                   [-out PREFIX] [-dump_every K] [-warmup W]
+//                   [-out PREFIX] [-dump_every K] [-warmup W] [-cholesky_cache BASENAME]
 #include "ibpm.h"
 #include <chrono>
 #include <cstdlib>
@@ -31,7 +31,7 @@ static double now_s() {
 int main(int argc, char* argv[]) {
     int nx = 200, ny = 200, ngrid = 1, nsteps = 10, dumpEvery = 0, warmup = 0;
     double length = 4, xoff = -2, yoff = -2, Re = 100, dt = 0.01, tol = 1e-7, alphaDeg = 0;
-    std::string geomFile, scheme = "rk3", ic, out;
+    std::string geomFile, scheme = "rk3", ic, out, cache;
     for (int a = 1; a + 1 < argc; a += 2) {
         std::string k = argv[a];
         const char* v = argv[a + 1];
@@ -52,6 +52,7 @@ int main(int argc, char* argv[]) {
         else if (k == "-out") out = v;
         else if (k == "-dump_every") dumpEvery = atoi(v);
         else if (k == "-warmup") warmup = atoi(v);
+        else if (k == "-cholesky_cache") cache = v;
         else { std::cerr << "unknown flag " << k << std::endl; return 2; }
     }
     Scheme::SchemeType st = Scheme::RK3;
@@ -76,7 +77,11 @@ int main(int argc, char* argv[]) {
     geom.moveBodies(x.time);
     model.init();
     double t0 = now_s();
-    solver.init();
+    // like src/ibpm.cc:291-297: reuse <cache>_0k.cholesky when it matches, else build and save
+    if (cache.empty() || !solver.load(cache)) {
+        solver.init();
+        if (!cache.empty()) solver.save(cache);
+    }
     double tInit = now_s() - t0;
     model.updateOperators(x.time);
     model.refreshState(x);
