@@ -67,6 +67,8 @@ SIGNATURES = {
     "ibg_model_C": (_I, [_VP, _VP, _VP]),
     "ibg_reg_to_boundary": (_I, [_VP, _VP, _VP]),
     "ibg_projection_solve": (_I, [_VP, _I, _VP, _VP, _VP, _VP]),
+    "ibg_poisson_solve_static": (_I, [ctypes.POINTER(ibg_grid), _VP, _VP, _VP]),
+    "ibg_static_last_error": (ctypes.c_char_p, []),
 }
 
 _lib = None

@@ -332,6 +332,8 @@ static void factorize(int m, FftDesc& d) {
     if (n != 1) d.nfac = -1;
 }
 
+void fft_describe(int m, FftDesc& d) { factorize(m, d); }
+
 bool fft_supported(int m) {
     FftDesc d;
     factorize(m, d);

@@ -56,6 +56,8 @@ struct CosTables {
 };
 
 bool fft_supported(int m);
+// factor m into the radices the shared-memory FFT uses (no device allocation)
+void fft_describe(int m, FftDesc& d);
 
 // One multi-domain solve call.  All arrays are device pointers.
 template <typename T>

@@ -1,0 +1,155 @@
+// noalloc.cu -- a multi-domain Poisson solve that allocates no device memory.
+//
+// Some callers cannot call cudaMalloc: code running while a CUDA graph is
+// being captured into a caller-owned memory pool, plug-ins whose host
+// application forbids device allocation after start-up, or services that
+// pre-plan every byte of HBM.  For them ibg_poisson_solve_static takes device
+// input and output buffers and keeps its scratch (the coarsified right-hand
+// side and the transform workspace) in the file-scope array below, plus the
+// FFT twiddle and eigenvalue cosine tables in two small file-scope arrays.
+// Every GPU that loads the library holds these arrays until the process exits.
+#include <cmath>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/ibpm_b200.h"
+#include "ibg_internal.cuh"
+#include "ibg_kernels.cuh"
+
+using namespace ibg;
+
+namespace {
+
+// 4 MiB of scratch: (ngrid + 1) * (nx - 1) * (ny - 1) doubles at most
+constexpr size_t kStaticScratchDoubles = (size_t)1 << 19;
+// twiddles for FFT lengths up to 2 * 2048 (nx, ny <= 2048), cosines for nx, ny <= 2048
+constexpr int kStaticMaxM = 4096;
+constexpr int kStaticMaxN = 2048;
+
+static __device__ __align__(256) double g_static_scratch[kStaticScratchDoubles];
+static __device__ __align__(256) double2 g_static_twiddles[2 * kStaticMaxM];  // rows, then columns
+static __device__ __align__(256) double g_static_cos[2 * kStaticMaxN];        // cos(pi i/nx), then cos(pi j/ny)
+
+struct DeviceSymbols {
+    bool ready = false;
+    double* scratch = nullptr;
+    double2* twiddles = nullptr;
+    double* cosines = nullptr;
+    int tab_nx = -1, tab_ny = -1;  // sizes the tables currently hold
+};
+constexpr int kMaxDevices = 64;
+DeviceSymbols g_dev[kMaxDevices];
+std::mutex g_mutex;
+std::string g_static_error;
+
+int fail(int code, const std::string& m) {
+    g_static_error = m;
+    return code;
+}
+
+}  // namespace
+
+extern "C" const char* ibg_static_last_error(void) { return g_static_error.c_str(); }
+
+extern "C" int ibg_poisson_solve_static(const ibg_grid* grid, const double* f, double* u, void* cuda_stream) {
+    if (!grid || !f || !u) return fail(IBG_ERR_ARG, "ibg_poisson_solve_static: null argument");
+    const int nx = grid->nx, ny = grid->ny, L = grid->ngrid;
+    if (nx < 4 || ny < 4 || L < 1 || L > 16 || !(grid->length > 0))
+        return fail(IBG_ERR_ARG, "ibg_poisson_solve_static: invalid grid");
+    if (L > 1 && (nx % 4 || ny % 4))
+        return fail(IBG_ERR_ARG, "ibg_poisson_solve_static: nx and ny must be multiples of 4 when ngrid > 1");
+    if (nx > kStaticMaxN || ny > kStaticMaxN)
+        return fail(IBG_ERR_UNSUPPORTED, "ibg_poisson_solve_static: nx and ny must be <= 2048 (static tables)");
+    const size_t N1 = (size_t)(nx - 1) * (ny - 1);
+    if ((size_t)(L + 1) * N1 > kStaticScratchDoubles)
+        return fail(IBG_ERR_UNSUPPORTED,
+                    "ibg_poisson_solve_static: (ngrid+1)*(nx-1)*(ny-1) exceeds the 524288-double (4 MiB) "
+                    "static scratch; use ibg_poisson_solve");
+    if (!fft_supported(2 * nx) || !fft_supported(2 * ny))
+        return fail(IBG_ERR_UNSUPPORTED, "ibg_poisson_solve_static: 2*nx and 2*ny must factor into primes <= 13");
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+        return fail(IBG_ERR_CUDA, "ibg_poisson_solve_static: no usable CUDA device");
+
+    std::lock_guard<std::mutex> lock(g_mutex);
+    DeviceSymbols& ds = g_dev[dev];
+    if (!ds.ready) {
+        // host-side stand-ins are not device addresses: resolve them once per device
+        cudaError_t e1 = cudaGetSymbolAddress((void**)&ds.scratch, g_static_scratch);
+        cudaError_t e2 = cudaGetSymbolAddress((void**)&ds.twiddles, g_static_twiddles);
+        cudaError_t e3 = cudaGetSymbolAddress((void**)&ds.cosines, g_static_cos);
+        if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
+            return fail(IBG_ERR_CUDA, std::string("ibg_poisson_solve_static: cudaGetSymbolAddress failed: ") +
+                                          cudaGetErrorString(e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3)));
+        ds.ready = true;
+    }
+    if (ds.tab_nx != nx || ds.tab_ny != ny) {
+        // the same host-computed tables as the context path (FftTables / CosTables)
+        const double pi2 = 3.14159265358979323846264338327950288;
+        std::vector<double2> tw(2 * (size_t)kStaticMaxM);
+        const int mr = 2 * ny, mc = 2 * nx;
+        for (int k = 0; k < mr; ++k) {
+            const double a = -2.0 * pi2 * (double)k / (double)mr;
+            tw[k] = make_double2(cos(a), sin(a));
+        }
+        for (int k = 0; k < mc; ++k) {
+            const double a = -2.0 * pi2 * (double)k / (double)mc;
+            tw[kStaticMaxM + k] = make_double2(cos(a), sin(a));
+        }
+        const double pi = 4. * atan(1.0);
+        std::vector<double> cs(2 * (size_t)kStaticMaxN);
+        for (int i = 0; i < nx; ++i) cs[i] = cos((pi * i) / nx);
+        for (int j = 0; j < ny; ++j) cs[kStaticMaxN + j] = cos((pi * j) / ny);
+        if (cudaMemcpyAsync(ds.twiddles, tw.data(), sizeof(double2) * tw.size(), cudaMemcpyHostToDevice, st) !=
+                cudaSuccess ||
+            cudaMemcpyAsync(ds.cosines, cs.data(), sizeof(double) * cs.size(), cudaMemcpyHostToDevice, st) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return fail(IBG_ERR_CUDA, "ibg_poisson_solve_static: table upload failed");
+        ds.tab_nx = nx;
+        ds.tab_ny = ny;
+    }
+
+    GridDev g{};
+    g.nx = nx;
+    g.ny = ny;
+    g.L = L;
+    g.nxe = (int)floor(nx / 4 * (1 - 0.0) + 0.5);
+    g.nye = (int)floor(ny / 4 * (1 - 0.0) + 0.5);
+    g.NI = nx - 1;
+    g.NJ = ny - 1;
+    g.N1 = g.NI * g.NJ;
+    g.nXf = (nx + 1) * ny;
+    g.F1 = 2 * nx * ny + nx + ny;
+    g.dx = grid->length / nx;
+    g.x0 = grid->xoffset;
+    g.y0 = grid->yoffset;
+
+    FftTables tables;  // descriptors only; the twiddles live in g_static_twiddles
+    fft_describe(2 * ny, tables.row64);
+    fft_describe(2 * nx, tables.col64);
+    tables.row64.tw = ds.twiddles;
+    tables.col64.tw = ds.twiddles + kStaticMaxM;
+    CosTables ct;
+    ct.x64 = ds.cosines;
+    ct.y64 = ds.cosines + kStaticMaxN;
+    EllipticPlan<double> plan;
+    if (plan.init(&g, &tables, false, 0.0, ct) != IBG_OK)
+        return fail(IBG_ERR_CUDA, "ibg_poisson_solve_static: kernel set-up failed");
+
+    SolveCall<double> c{};
+    c.f = f;
+    c.u = u;
+    c.rc = ds.scratch;                    // levels 1..L-1 at rc + lev*N1
+    c.tbuf = ds.scratch + (size_t)L * N1; // one level of transform workspace
+    c.bstride = (size_t)L * N1;
+    c.batch = 1;
+    c.in_scale = 1.0;
+    const int s = plan.solve(c, st);
+    if (s != IBG_OK || cudaPeekAtLastError() != cudaSuccess)
+        return fail(IBG_ERR_CUDA, std::string("ibg_poisson_solve_static: launch failed: ") +
+                                      cudaGetErrorString(cudaGetLastError()));
+    return IBG_OK;
+}

@@ -144,6 +144,26 @@ IBG_API int ibg_reg_to_boundary(ibg_context* ctx, const double* q, double* f);
  * A omega + B f = a, C omega = b.  f is the warm start on input (CG). */
 IBG_API int ibg_projection_solve(ibg_context* ctx, int substep, const double* a, const double* b, double* omega, double* f);
 
+/* --- allocation-free variant -------------------------------------------------
+ * No counterpart in the reference: an addition for callers that cannot call
+ * cudaMalloc (code running while a CUDA graph is captured into a pool it does
+ * not own, plug-ins whose host forbids device allocation after start-up,
+ * services that budget every byte of HBM up front).
+ * ibg_poisson_solve_static solves L u = f on all levels, like ibg_poisson_solve,
+ * but takes DEVICE pointers f and u (reference Scalar layout), needs no context
+ * and allocates nothing: its scratch is a file-scope device array of 4 MiB
+ * (524288 doubles, enough for (ngrid+1)*(nx-1)*(ny-1) <= 524288) plus ~160 KiB
+ * of tables (nx, ny <= 2048), held by every GPU that loads the library until the
+ * process exits.  Larger grids are rejected with IBG_ERR_UNSUPPORTED.  The first
+ * call on a device resolves the arrays' device addresses (cudaGetSymbolAddress)
+ * and fills the tables; make that first call before any stream capture.  All
+ * calls share the scratch, which keeps the last call's contents (each call
+ * writes every scratch value it reads, so nothing needs clearing); calls that
+ * overlap on the GPU race.  Runs on `cuda_stream` (a cudaStream_t, may be NULL).
+ * ibg_static_last_error() describes the last failure. */
+IBG_API int ibg_poisson_solve_static(const ibg_grid* grid, const double* f, double* u, void* cuda_stream);
+IBG_API const char* ibg_static_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif
