@@ -284,7 +284,7 @@ def kernel_roofline(s, grid, stream, reps=200):
             best = name
     d = res[best]
     achieved = d["algorithmic_bytes"] / (d["us_per_launch"] * 1e-6) / 1e9
-    return {"kernel": "k_dst_cols<double> (finest level: DST-I along i, eigen scaling, inverse DST-I)",
+    return {"kernel": "k_dst_cols<double> (forward DST-I along i of every level of one solve)",
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_kind": f"{kind} (copy bandwidth, burst)", "traffic": None, "kernels": res}
 

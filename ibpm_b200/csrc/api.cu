@@ -96,7 +96,7 @@ struct ibg_context {
     int nring = 0;
     double *a = nullptr, *ws = nullptr, *psi = nullptr, *cc = nullptr, *rc = nullptr, *tbuf = nullptr;
     double *U = nullptr, *V = nullptr, *C = nullptr, *flux0 = nullptr, *Bf = nullptr;
-    double *rhsb = nullptr, *btmp = nullptr, *qtmp = nullptr;
+    double *rhsb = nullptr, *btmp = nullptr, *qtmp = nullptr, *sweep = nullptr;
     // Cholesky factors per sub-step
     double* Lr[4] = {nullptr, nullptr, nullptr, nullptr};
     double* Lc[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -144,7 +144,7 @@ struct ibg_context {
         graph = nullptr;
         void* ptrs[] = {d_ref, d_pts, d_vel, d_body_of, d_bodies, slots.idx, slots.w, slots.n, d_b, d_time, w, q, f,
                         a, ws, psi, cc, rc, tbuf, U, V, C, flux0, Bf, rhsb, btmp, d_status, cg_r, cg_d, cg_q,
-                        cg_scal, cg_flags, d_hist, d_hist_count, qtmp};
+                        cg_scal, cg_flags, d_hist, d_hist_count, qtmp, sweep};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         for (int k = 0; k < 4; ++k) {
@@ -165,7 +165,7 @@ struct ibg_context {
         d_body_of = nullptr;
         d_bodies = nullptr;
         slots = RegSlots{};
-        d_b = d_time = w = q = f = a = ws = psi = cc = rc = tbuf = U = V = C = flux0 = Bf = rhsb = btmp = qtmp = nullptr;
+        d_b = d_time = w = q = f = a = ws = psi = cc = rc = tbuf = U = V = C = flux0 = Bf = rhsb = btmp = qtmp = sweep = nullptr;
         d_status = nullptr;
         cg_r = cg_d = cg_q = cg_scal = nullptr;
         cg_flags = nullptr;
@@ -181,6 +181,7 @@ struct ibg_context {
         c.u = uout;
         c.rc = rc;
         c.tbuf = tbuf;
+        c.sweep = sweep;
         c.bstride = S;
         c.batch = 1;
         c.in_scale = scale;
@@ -188,7 +189,7 @@ struct ibg_context {
         c.base = base;
         return c;
     }
-    long long solve_launches() const { return (g.L - 1) + 3LL * g.L; }
+    long long solve_launches() const { return poisson.launches(); }
 
     // M d = C A^-1 B d  (src/ProjectionSolver.cc:96-101)
     void m_apply(int k, const double* din, double* dout) {
@@ -449,7 +450,7 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
     }
     int s = IBG_OK;
     const size_t S = c->S, F = c->F, m = c->ncomp;
-    if ((s = c->fft.init(2 * g.ny, 2 * g.nx)) || (s = c->cosT.init(g.nx, g.ny))) {
+    if ((s = c->fft.init(2 * g.ny, 2 * g.nx)) || (s = c->cosT.init(g.nx, g.ny, g.nxe, g.nye))) {
         g_create_error = "ibg_create: FFT table setup failed";
         delete c;
         return s;
@@ -468,7 +469,7 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
     c->nring = sch.nsub == 1 ? 2 : sch.nsub;
     s = s || c->alloc(&c->w, S) || c->alloc(&c->q, F) || c->alloc(&c->f, m) || c->alloc(&c->a, S) ||
         c->alloc(&c->ws, S) || c->alloc(&c->psi, S) || c->alloc(&c->cc, S) || c->alloc(&c->rc, S) ||
-        c->alloc(&c->tbuf, (size_t)g.N1) || c->alloc(&c->U, S) || c->alloc(&c->V, S) || c->alloc(&c->C, F) ||
+        c->alloc(&c->tbuf, S) || c->alloc(&c->sweep, sweep_doubles(g.nx, g.ny, g.L)) || c->alloc(&c->U, S) || c->alloc(&c->V, S) || c->alloc(&c->C, F) ||
         c->alloc(&c->flux0, (size_t)g.F1) || c->alloc(&c->Bf, S) || c->alloc(&c->rhsb, m) ||
         c->alloc(&c->btmp, m) || c->alloc(&c->qtmp, F) || c->alloc(&c->d_ref, 2 * (size_t)c->npts) ||
         c->alloc(&c->d_pts, 2 * (size_t)c->npts) || c->alloc(&c->d_vel, 2 * (size_t)c->npts) ||
@@ -523,21 +524,24 @@ int ibg_init(ibg_context* c) {
     const int m = c->ncomp;
     const size_t S = c->S;
     // chunk so that the batched scratch stays below ~8 GB
-    const size_t per_col = sizeof(double) * (4 * S + (size_t)g.N1 + (size_t)g.F1);
+    const size_t swd = sweep_doubles(g.nx, g.ny, g.L);
+    const size_t per_col = sizeof(double) * (5 * S + (size_t)g.F1 + swd);
     size_t chunk = (size_t)8 << 30;
     chunk /= per_col;
     if (chunk < 1) chunk = 1;
     if (chunk > (size_t)m) chunk = m;
     if (chunk > 65535) chunk = 65535;
     double *bf = nullptr, *u = nullptr, *p = nullptr, *rcb = nullptr, *tb = nullptr, *fl = nullptr, *Mcol = nullptr;
+    double* swb = nullptr;
     int s = c->alloc(&bf, chunk * S) || c->alloc(&u, chunk * S) || c->alloc(&p, chunk * S) ||
-            c->alloc(&rcb, chunk * S) || c->alloc(&tb, chunk * g.N1) || c->alloc(&fl, chunk * g.F1) ||
-            c->alloc(&Mcol, (size_t)m * m, false);
+            c->alloc(&rcb, chunk * S) || c->alloc(&tb, chunk * S) || c->alloc(&fl, chunk * g.F1) ||
+            c->alloc(&swb, chunk * swd) || c->alloc(&Mcol, (size_t)m * m, false);
     for (int k = 0; k < c->sch.nsub && !s; ++k)
         s = c->alloc(&c->Lr[k], (size_t)m * m, false) || c->alloc(&c->Lc[k], (size_t)m * m, false) ||
             c->alloc(&c->Ld[k], (size_t)m, false) || c->alloc(&c->Mi[k], (size_t)m * m, false);
     if (s) {
         cudaFree(bf); cudaFree(u); cudaFree(p); cudaFree(rcb); cudaFree(tb); cudaFree(fl); cudaFree(Mcol);
+        cudaFree(swb);
         return c->fail(IBG_ERR_CUDA, "ibg_init: not enough device memory for the Cholesky build");
     }
     for (int k = 0; k < c->sch.nsub && !s; ++k) {
@@ -545,10 +549,13 @@ int ibg_init(ibg_context* c) {
             const int nb = (int)std::min(chunk, (size_t)(m - col0));
             launch_smear_bf_unit<double>(g, m, col0, nb, c->slots, fl, g.F1, bf, S, c->beta[k], c->st);
             SolveCall<double> h{};
-            h.f = bf; h.u = u; h.rc = rcb; h.tbuf = tb; h.bstride = S; h.batch = nb; h.in_scale = 1.0;
+            h.f = bf; h.u = u; h.rc = rcb; h.tbuf = tb; h.sweep = swb; h.bstride = S;
+            h.batch = nb; h.in_scale = 1.0;
             c->helm[k].solve(h, c->st);
             SolveCall<double> pc{};
-            pc.f = u; pc.u = p; pc.rc = rcb; pc.tbuf = tb; pc.bstride = S; pc.batch = nb; pc.in_scale = -1.0;
+            pc.f = u; pc.u = p; pc.rc = rcb; pc.tbuf = tb; pc.sweep = swb; pc.bstride = S;
+            pc.batch = nb;
+            pc.in_scale = -1.0;
             c->poisson.solve(pc, c->st);
             launch_reg_interp<double>(g, m, c->slots, p, S, nb, nullptr, Mcol + (size_t)col0 * m, (size_t)m, c->st);
         }
@@ -560,6 +567,7 @@ int ibg_init(ibg_context* c) {
         if (!s && hs) s = c->fail(IBG_ERR_NUMERIC, "ibg_init: matrix M is not positive definite");
     }
     cudaFree(bf); cudaFree(u); cudaFree(p); cudaFree(rcb); cudaFree(tb); cudaFree(fl); cudaFree(Mcol);
+    cudaFree(swb);
     if (s) return s;
     c->chol_ready = true;
     return c->cuda_check("ibg_init");
@@ -861,12 +869,12 @@ long long ibg_run_kernel(ibg_context* c, int which, int reps) {
     const GridDev& g = c->g;
     long long bytes = 0;
     for (int r = 0; r < reps; ++r) {
-        if (which == 0) c->poisson.run_pass(0, c->a, c->tbuf, c->st);
+        if (which == 0) c->poisson.run_pass(0, c->w, c->tbuf, c->st);
         else if (which == 1) c->poisson.run_pass(1, c->tbuf, c->tbuf, c->st);
         else if (which == 2) launch_nonlinear<double>(g, c->q, c->w, c->U, c->V, c->C, c->Nbuf[0], 1, c->S, c->F, c->st);
         else return IBG_ERR_ARG;
     }
-    if (which == 0 || which == 1) bytes = 16LL * g.N1;                 // one level read + written once
+    if (which == 0 || which == 1) bytes = 16LL * (long long)c->S;      // every level read + written once
     else bytes = 8LL * (long long)(c->F + c->S + 2 * c->S + c->F + c->F + c->S);  // q,w in; U,V; C; N
     if (c->cuda_check("ibg_run_kernel")) return IBG_ERR_CUDA;
     return bytes;

@@ -5,11 +5,19 @@
 // with zero or lifted boundary values by a 2-D DST-I (FFTW RODFT00), a
 // diagonal eigenvalue scaling and an inverse DST-I, coarse levels first.
 //
-// Design (one level, nodes NI x NJ, j contiguous):
-//   pass A  rows:    load rhs (+ boundary lifting from the coarser solution),
-//                    DST-I along j                          -> T
-//   pass B  columns: DST-I along i, x eigen-inverse, DST-I   -> T (in place)
-//   pass C  rows:    DST-I along j, x 1/(4 nx ny)            -> u (+ base - u)
+// Design (nodes NI x NJ per level, j contiguous).  One level (ngrid = 1):
+//   pass A  rows:    DST-I along j of the right-hand side      -> T
+//   pass B  columns: DST-I along i, x eigen-inverse, DST-I     -> T (in place)
+//   pass C  rows:    DST-I along j, x 1/(4 nx ny)              -> u (+ base - u)
+// Several levels: the boundary lifting of getRHS is linear, so its 2-D DST is
+// a sum of four outer products of 1-D DSTs of the boundary values with sine
+// vectors.  The forward transforms of all levels therefore run in one batched
+// launch per direction; a short coarse-to-fine sweep then adds each level's
+// spectral lifting, scales by the eigen-inverse, and evaluates the four
+// boundary lines of the level's solution (matvecs over its coefficients plus
+// 1-D DSTs) that give the next finer level's boundary values; finally the
+// inverse transforms of all levels run batched.  Same operator as the
+// reference, different rounding (~1e-16).
 // A DST-I of length n is read off the DFT of the odd extension of length
 // m = 2(n+1).  Two real lines a, b are packed as z = a + i b: the DFT of an
 // odd real sequence is purely imaginary, so DST(a)_k = -Im Z_{k+1} and
@@ -17,6 +25,7 @@
 // autosort FFT with mixed radices; twiddles are tabulated on the host.
 #include "ibg_internal.cuh"
 #include "ibg_kernels.cuh"
+
 
 namespace ibg {
 
@@ -40,7 +49,7 @@ __device__ __forceinline__ void bfly(const C* __restrict__ sp, C* __restrict__ d
 #pragma unroll
     for (int q = 0; q < R; ++q) {
         C x = sp[j + q * mr];
-        v[q] = q == 0 ? x : cmul(x, tw[jm * q * tstep]);
+        v[q] = q == 0 ? x : cmul(x, __ldg(&tw[jm * q * tstep]));
     }
     C o[R];
     if (R == 2) {
@@ -53,13 +62,40 @@ __device__ __forceinline__ void bfly(const C* __restrict__ sp, C* __restrict__ d
         o[2] = csub(t0, t2);
         o[1] = cmk<C>(t1.x + t3.y, t1.y - t3.x);  // t1 - i t3
         o[3] = cmk<C>(t1.x - t3.y, t1.y + t3.x);  // t1 + i t3
+    } else if (R == 3) {
+        // w = exp(-2 pi i / 3): cos = -1/2, sin = -sqrt(3)/2
+        using V = decltype(v[0].x);
+        const V c3 = (V)-0.5, s3 = (V)-0.86602540378443864676;
+        const C t = cadd(v[1], v[2]), d = csub(v[1], v[2]);
+        o[0] = cadd(v[0], t);
+        const C m1 = cmk<C>(v[0].x + c3 * t.x, v[0].y + c3 * t.y);
+        // +/- i s3 d
+        o[1] = cmk<C>(m1.x - s3 * d.y, m1.y + s3 * d.x);
+        o[2] = cmk<C>(m1.x + s3 * d.y, m1.y - s3 * d.x);
+    } else if (R == 5) {
+        // w = exp(-2 pi i / 5): c1 = cos(2pi/5), c2 = cos(4pi/5), s1 = -sin(2pi/5), s2 = -sin(4pi/5)
+        using V = decltype(v[0].x);
+        const V c1 = (V)0.30901699437494742410, c2 = (V)-0.80901699437494742410;
+        const V s1 = (V)-0.95105651629515357212, s2 = (V)-0.58778525229247312917;
+        const C a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
+        const C a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
+        o[0] = cadd(v[0], cadd(a1, a2));
+        const C m1 = cmk<C>(v[0].x + c1 * a1.x + c2 * a2.x, v[0].y + c1 * a1.y + c2 * a2.y);
+        const C m2 = cmk<C>(v[0].x + c2 * a1.x + c1 * a2.x, v[0].y + c2 * a1.y + c1 * a2.y);
+        // n1 = i (s1 b1 + s2 b2), n2 = i (s2 b1 - s1 b2)
+        const V n1r = -(s1 * b1.y + s2 * b2.y), n1i = s1 * b1.x + s2 * b2.x;
+        const V n2r = -(s2 * b1.y - s1 * b2.y), n2i = s2 * b1.x - s1 * b2.x;
+        o[1] = cmk<C>(m1.x + n1r, m1.y + n1i);
+        o[4] = cmk<C>(m1.x - n1r, m1.y - n1i);
+        o[2] = cmk<C>(m2.x + n2r, m2.y + n2i);
+        o[3] = cmk<C>(m2.x - n2r, m2.y - n2i);
     } else {
         const int rstep = m / R;
 #pragma unroll
         for (int k = 0; k < R; ++k) {
             C acc = v[0];
 #pragma unroll
-            for (int q = 1; q < R; ++q) acc = cadd(acc, cmul(v[q], tw[((k * q) % R) * rstep]));
+            for (int q = 1; q < R; ++q) acc = cadd(acc, cmul(v[q], __ldg(&tw[((k * q) % R) * rstep])));
             o[k] = acc;
         }
     }
@@ -78,8 +114,8 @@ __device__ void bfly_generic(const C* __restrict__ sp, C* __restrict__ dp, const
     for (int k = 0; k < R; ++k) {
         C acc = sp[j];
         for (int q = 1; q < R; ++q) {
-            C x = cmul(sp[j + q * mr], tw[jm * q * tstep]);
-            acc = cadd(acc, cmul(x, tw[((k * q) % R) * rstep]));
+            C x = cmul(sp[j + q * mr], __ldg(&tw[jm * q * tstep]));
+            acc = cadd(acc, cmul(x, __ldg(&tw[((k * q) % R) * rstep])));
         }
         dp[idxd + k * ns] = acc;
     }
@@ -117,14 +153,10 @@ __device__ C* fft_smem(C* s0, C* s1, const C* tw, const FftDesc& d, int P) {
     return src;
 }
 
-template <typename C>
-__device__ __forceinline__ void load_twiddles(C* tws, const FftDesc& d) {
-    const C* g = reinterpret_cast<const C*>(d.tw);
-    for (int k = threadIdx.x; k < d.m; k += blockDim.x) tws[k] = g[k];
-}
-
 // ---------------------------------------------------------------------------
-// pass A / pass C: transforms along j for pairs of rows
+// rows: DST-I along j for pairs of rows of every level in the launch
+// (blockIdx.y = batch * nlev + level).  Inside a level's overlap interior
+// the input comes from `alt` (the coarsified right-hand side) when given.
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void k_dst_rows(RowPassArgs<T> a) {
@@ -133,19 +165,17 @@ __global__ void k_dst_rows(RowPassArgs<T> a) {
     const FftDesc& d = a.fft;
     const int m = d.m;
     const int P = a.pairs_per_block;
-    C* tws = reinterpret_cast<C*>(smem_raw);
-    C* s0 = tws + m;
+    C* s0 = reinterpret_cast<C*>(smem_raw);
     C* s1 = s0 + P * m;
+    const C* tw = reinterpret_cast<const C*>(d.tw);
     const GridDev& g = a.g;
     const int n = g.NJ;
-    const size_t ioff = (size_t)blockIdx.y * a.in_bstride;
-    const size_t ooff = (size_t)blockIdx.y * a.out_bstride;
-    const T* in = a.in + ioff;
-    const T* coarse = a.coarse ? a.coarse + ioff : nullptr;
+    const int b = blockIdx.y / a.nlev, l = blockIdx.y % a.nlev;
+    const T* in = a.in[l] + (size_t)b * a.in_bstride;
+    const T* alt = a.alt[l] ? a.alt[l] + (size_t)b * a.in_bstride : nullptr;
     const int pair0 = blockIdx.x * P;
     const int npairs = (g.NI + 1) / 2;
-    load_twiddles(tws, d);
-    // fill the odd extensions
+    const int ilo = g.nxe, ihi = g.nx / 2 + g.nxe, jlo = g.nye, jhi = g.ny / 2 + g.nye;
     for (int t = threadIdx.x; t < P * n; t += blockDim.x) {
         const int p = t / n;
         const int k = t - p * n;
@@ -154,29 +184,13 @@ __global__ void k_dst_rows(RowPassArgs<T> a) {
         T va = (T)0, vb = (T)0;
         if (pair < npairs) {
             const int r0 = 2 * pair, r1 = 2 * pair + 1;
-            va = in[(size_t)r0 * n + k];
-            if (r1 < g.NI) vb = in[(size_t)r1 * n + k];
-            if (a.lift) {
-                // input scale and boundary lifting (getRHS, src/EllipticSolver2d.cc:125-144, :166-185)
-                va = a.in_scale * va;
-                vb = a.in_scale * vb;
-                if (coarse) {
-                    const T c = a.bc_coef;
-                    const int I0 = r0 + 1, I1 = r1 + 1, J = k + 1;
-                    if (k == 0) {
-                        va = va - bc_bottom(coarse, g, I0) * c;
-                        if (r1 < g.NI) vb = vb - bc_bottom(coarse, g, I1) * c;
-                    }
-                    if (k == n - 1) {
-                        va = va - bc_top(coarse, g, I0) * c;
-                        if (r1 < g.NI) vb = vb - bc_top(coarse, g, I1) * c;
-                    }
-                    if (I0 == 1) va = va - bc_left(coarse, g, J) * c;
-                    if (I0 == g.nx - 1) va = va - bc_right(coarse, g, J) * c;
-                    if (r1 < g.NI) {
-                        if (I1 == g.nx - 1) vb = vb - bc_right(coarse, g, J) * c;
-                    }
-                }
+            const int J = k + 1;
+            const bool jin = alt && J > jlo && J < jhi;
+            const T* s0p = (jin && r0 + 1 > ilo && r0 + 1 < ihi) ? alt : in;
+            va = a.in_scale * s0p[(size_t)r0 * n + k];
+            if (r1 < g.NI) {
+                const T* s1p = (jin && r1 + 1 > ilo && r1 + 1 < ihi) ? alt : in;
+                vb = a.in_scale * s1p[(size_t)r1 * n + k];
             }
         }
         z[k + 1] = cmk<C>(va, vb);
@@ -187,11 +201,10 @@ __global__ void k_dst_rows(RowPassArgs<T> a) {
         }
     }
     __syncthreads();
-    C* res = fft_smem<C>(s0, s1, tws, d, P);
-    // write out
-    T* out = a.out + ooff;
-    T* out2 = a.out2 ? a.out2 + ooff : nullptr;
-    const T* base = a.base ? a.base + ooff : nullptr;
+    C* res = fft_smem<C>(s0, s1, tw, d, P);
+    T* out = a.out[l] + (size_t)b * a.out_bstride;
+    T* out2 = a.out2[l] ? a.out2[l] + (size_t)b * a.out_bstride : nullptr;
+    const T* base = a.base[l] ? a.base[l] + (size_t)b * a.out_bstride : nullptr;
     for (int t = threadIdx.x; t < P * n; t += blockDim.x) {
         const int p = t / n;
         const int k = t - p * n;
@@ -212,9 +225,34 @@ __global__ void k_dst_rows(RowPassArgs<T> a) {
     }
 }
 
+// eigenvalue of the inverse operator at 0-based mode (k, l):
+// lambda = 2 (cos(pi (k+1)/nx) + cos(pi (l+1)/ny) - 2) / dx^2 (src/EllipticSolver2d.cc:42-54),
+// 1/lambda (Poisson, :115-122) or 1/(1 + alpha lambda) (Helmholtz, :156-163)
+template <typename T>
+__device__ __forceinline__ T eig_inverse(const T* cx, const T* cy, int k, int l, T bydx2, int helm, T alpha) {
+    const T lam = (T)2 * (cx[k + 1] + cy[l + 1] - (T)2) * bydx2;
+    return helm ? (T)1 / ((T)1 + alpha * lam) : (T)1 / lam;
+}
+
+// Coefficient (k, l) of a level after the boundary lifting and the eigen-inverse:
+// U = E (R - c Slift), Slift = sy1 B(k) + syn T(k) + sx1 L(l) + sxn R(l), where
+// B, T, L, R are the 1-D DSTs of the level's bottom, top, left, right boundary values.
+template <typename T>
+__device__ __forceinline__ T lifted_coef(T R, int k, int l, const T* edges, int NI, int NJ, T c,
+                                         const SineTab<T>& s, const T* cx, const T* cy, T bydx2, int helm,
+                                         T alpha) {
+    if (edges) {
+        const T sl = s.sy1[l] * edges[k] + s.syn[l] * edges[NI + k] + s.sx1[k] * edges[2 * NI + l] +
+                     s.sxn[k] * edges[2 * NI + NJ + l];
+        R = R - c * sl;
+    }
+    return R * eig_inverse(cx, cy, k, l, bydx2, helm, alpha);
+}
+
 // ---------------------------------------------------------------------------
-// pass B: transforms along i for pairs of columns, eigen-inverse scaling,
-// inverse transform along i (in place on T)
+// columns: DST-I along i for pairs of columns (in place).  mode 0 / 2: one
+// transform; mode 1: transform, eigen-inverse scaling, transform (one level);
+// mode 3: boundary lifting and eigen-inverse on load, then one transform.
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void k_dst_cols(ColPassArgs<T> a) {
@@ -223,21 +261,26 @@ __global__ void k_dst_cols(ColPassArgs<T> a) {
     const FftDesc& d = a.fft;
     const int m = d.m;
     const int P = a.pairs_per_block;
-    C* tws = reinterpret_cast<C*>(smem_raw);
-    C* s0 = tws + m;
+    C* s0 = reinterpret_cast<C*>(smem_raw);
     C* s1 = s0 + P * m;
+    const C* tw = reinterpret_cast<const C*>(d.tw);
     const GridDev& g = a.g;
     const int n = g.NI;
     const int NJ = g.NJ;
-    T* buf = a.buf + (size_t)blockIdx.y * a.bstride;
+    const int b = blockIdx.y / a.nlev, lev = blockIdx.y % a.nlev;
+    T* buf = a.buf + (size_t)b * a.bstride + (size_t)lev * a.lstride;
+    const T* edges = (a.mode == 3 && lev < a.nlev - 1) ? a.edges + (size_t)b * a.estride + (size_t)lev * a.elstride
+                                                        : nullptr;
+    const T bydx2 = a.bydx2[lev], bcc = a.bc_coef[lev];
     const int col0 = blockIdx.x * 2 * P;
     const int w = 2 * P;
-    load_twiddles(tws, d);
     for (int t = threadIdx.x; t < n * w; t += blockDim.x) {
         const int i = t / w;
         const int c = t - i * w;
         const int col = col0 + c;
-        const T v = col < NJ ? buf[(size_t)i * NJ + col] : (T)0;
+        T v = col < NJ ? buf[(size_t)i * NJ + col] : (T)0;
+        if (a.mode == 3 && col < NJ)
+            v = lifted_coef(v, i, col, edges, n, NJ, bcc, a.s, a.cosx, a.cosy, bydx2, a.helmholtz, a.alpha);
         C* z = s0 + (c >> 1) * m;
         if (c & 1) {
             z[i + 1].y = v;
@@ -252,69 +295,213 @@ __global__ void k_dst_cols(ColPassArgs<T> a) {
         s0[p * m + n + 1] = cmk<C>((T)0, (T)0);
     }
     __syncthreads();
-    C* res = fft_smem<C>(s0, s1, tws, d, P);
-    C* other = (res == s0) ? s1 : s0;
-    // eigen-inverse scaling; build the second odd extension in `other`
-    const T* cx = a.cosx;
-    const T* cy = a.cosy;
-    for (int t = threadIdx.x; t < P * n; t += blockDim.x) {
-        const int p = t / n;
-        const int k = t - p * n;
-        const C z = res[p * m + k + 1];
-        const int ca = col0 + 2 * p, cb = ca + 1;
-        T va = -z.y, vb = z.x;
-        // lambda_ij = 2 (cos(pi i/nx) + cos(pi j/ny) - 2) / dx^2  (src/EllipticSolver2d.cc:42-54)
-        const T ex = cx[k + 1];
-        const T la = (T)2 * (ex + cy[(ca < NJ ? ca : 0) + 1] - (T)2) * a.bydx2;
-        const T lb = (T)2 * (ex + cy[(cb < NJ ? cb : 0) + 1] - (T)2) * a.bydx2;
-        const T ea = a.helmholtz ? (T)1 / ((T)1 + a.alpha * la) : (T)1 / la;
-        const T eb = a.helmholtz ? (T)1 / ((T)1 + a.alpha * lb) : (T)1 / lb;
-        va = va * ea;
-        vb = vb * eb;
-        C* zo = other + p * m;
-        zo[k + 1] = cmk<C>(va, vb);
-        zo[m - 1 - k] = cmk<C>(-va, -vb);
-        if (k == 0) {
-            zo[0] = cmk<C>((T)0, (T)0);
-            zo[n + 1] = cmk<C>((T)0, (T)0);
+    C* res = fft_smem<C>(s0, s1, tw, d, P);
+    if (a.mode == 1) {
+        C* other = (res == s0) ? s1 : s0;
+        for (int t = threadIdx.x; t < P * n; t += blockDim.x) {
+            const int p = t / n;
+            const int k = t - p * n;
+            const C z = res[p * m + k + 1];
+            const int ca = col0 + 2 * p, cb = ca + 1;
+            const T ea = eig_inverse(a.cosx, a.cosy, k, ca < NJ ? ca : 0, bydx2, a.helmholtz, a.alpha);
+            const T eb = eig_inverse(a.cosx, a.cosy, k, cb < NJ ? cb : 0, bydx2, a.helmholtz, a.alpha);
+            const T va = -z.y * ea, vb = z.x * eb;
+            C* zo = other + p * m;
+            zo[k + 1] = cmk<C>(va, vb);
+            zo[m - 1 - k] = cmk<C>(-va, -vb);
+            if (k == 0) {
+                zo[0] = cmk<C>((T)0, (T)0);
+                zo[n + 1] = cmk<C>((T)0, (T)0);
+            }
         }
+        __syncthreads();
+        res = fft_smem<C>(other, res, tw, d, P);
     }
-    __syncthreads();
-    C* res2 = fft_smem<C>(other, res, tws, d, P);
     for (int t = threadIdx.x; t < n * w; t += blockDim.x) {
         const int i = t / w;
         const int c = t - i * w;
         const int col = col0 + c;
         if (col >= NJ) continue;
-        const C z = res2[(c >> 1) * m + i + 1];
+        const C z = res[(c >> 1) * m + i + 1];
         buf[(size_t)i * NJ + col] = (c & 1) ? z.x : -z.y;
     }
 }
 
 // ---------------------------------------------------------------------------
-// coarsify one level (src/Scalar.cc:46-64): dst[lev] = f[lev] outside the
-// overlap, full-weighting of src (= level lev-1 already coarsified) inside.
+// coarsify one level (src/Scalar.cc:46-64): only the overlap interior of the
+// coarse level is computed (into rc); outside it the right-hand side f itself
+// is used by the transforms.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void k_coarsify(GridDev g, const T* f_lev, const T* src_fine, T* dst_lev, size_t bstride) {
+__device__ __forceinline__ T rhs_node(const T* f_lev, const T* rc_lev, const GridDev& g, int i, int j) {
+    if (rc_lev && i > g.nxe && i < g.nx / 2 + g.nxe && j > g.nye && j < g.ny / 2 + g.nye) return node(rc_lev, g, i, j);
+    return node(f_lev, g, i, j);
+}
+
+template <typename T>
+__global__ void k_coarsify(GridDev g, int lev, const T* f, T* rc, size_t bstride) {
+    const int ni = g.nx / 2 - 1, nj = g.ny / 2 - 1;  // overlap interior extent
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ni * nj) return;
     const size_t boff = (size_t)blockIdx.y * bstride;
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= g.N1) return;
-    const int i = idx / g.NJ + 1;
-    const int j = idx % g.NJ + 1;
-    const T* sf = src_fine + boff;
-    T v;
-    if (i > g.nxe && i < g.nx / 2 + g.nxe && j > g.nye && j < g.ny / 2 + g.nye) {
-        const int ii = (i - g.nxe) * 2, jj = (j - g.nye) * 2;
-        v = (T)0.25 * node(sf, g, ii, jj) +
-            (T)0.125 * (node(sf, g, ii + 1, jj) + node(sf, g, ii, jj + 1) + node(sf, g, ii - 1, jj) +
-                        node(sf, g, ii, jj - 1)) +
-            (T)0.0625 * (node(sf, g, ii + 1, jj + 1) + node(sf, g, ii + 1, jj - 1) + node(sf, g, ii - 1, jj + 1) +
-                         node(sf, g, ii - 1, jj - 1));
-    } else {
-        v = f_lev[boff + idx];
+    const T* ff = f + boff + (size_t)(lev - 1) * g.N1;
+    const T* rf = (lev >= 2) ? rc + boff + (size_t)(lev - 1) * g.N1 : nullptr;
+    T* dst = rc + boff + (size_t)lev * g.N1;
+    const int i = g.nxe + 1 + t / nj, j = g.nye + 1 + t % nj;
+    const int ii = (i - g.nxe) * 2, jj = (j - g.nye) * 2;
+    const T v = (T)0.25 * rhs_node(ff, rf, g, ii, jj) +
+                (T)0.125 * (rhs_node(ff, rf, g, ii + 1, jj) + rhs_node(ff, rf, g, ii, jj + 1) +
+                            rhs_node(ff, rf, g, ii - 1, jj) + rhs_node(ff, rf, g, ii, jj - 1)) +
+                (T)0.0625 * (rhs_node(ff, rf, g, ii + 1, jj + 1) + rhs_node(ff, rf, g, ii + 1, jj - 1) +
+                             rhs_node(ff, rf, g, ii - 1, jj + 1) + rhs_node(ff, rf, g, ii - 1, jj - 1));
+    dst[(size_t)(i - 1) * g.NJ + (j - 1)] = v;
+}
+
+// ---------------------------------------------------------------------------
+// sweep step for one coarse level, in two launches.  k_sweep_sums forms
+// U = E (R - c Slift) of the level on the fly (lifted_coef) and the sums
+// V_j0, V_j1 over rows and W_i0, W_i1 over columns that give the level's
+// solution on its four boundary lines; k_sweep_lines turns them into those
+// lines by 1-D DSTs, takes the next finer level's boundary values from them
+// (Scalar::getBC, src/Scalar.cc:91-127) and writes their 1-D DSTs.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ void dst_pair_block(const FftDesc& d, int n, const T* a_in, const T* b_in, T* a_out, T* b_out, T scale,
+                               typename Cplx<T>::type* s0, typename Cplx<T>::type* s1) {
+    using C = typename Cplx<T>::type;
+    const int m = d.m;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const T va = a_in[k], vb = b_in[k];
+        s0[k + 1] = cmk<C>(va, vb);
+        s0[m - 1 - k] = cmk<C>(-va, -vb);
     }
-    dst_lev[boff + idx] = v;
+    if (threadIdx.x == 0) {
+        s0[0] = cmk<C>((T)0, (T)0);
+        s0[n + 1] = cmk<C>((T)0, (T)0);
+    }
+    __syncthreads();
+    C* res = fft_smem<C>(s0, s1, reinterpret_cast<const C*>(d.tw), d, 1);
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const C z = res[k + 1];
+        a_out[k] = -z.y * scale;
+        b_out[k] = z.x * scale;
+    }
+    __syncthreads();
+}
+
+// sums: blocks [0, nrb) each take kSweepRows full rows (row sums V_j0, V_j1),
+// blocks [nrb, nrb + ncb) each take kSweepCols full columns (column sums
+// W_i0, W_i1); every sum is complete inside one block (fixed order).
+template <typename T>
+__global__ void __launch_bounds__(256) k_sweep_sums(SweepArgs<T> a) {
+    __shared__ T red[8][2 * kSweepCols];
+    const GridDev& g = a.g;
+    const int NI = g.NI, NJ = g.NJ;
+    const int b = blockIdx.y;
+    const T* R = a.buf + (size_t)b * a.bstride;
+    const T* E = a.edges_in ? a.edges_in + (size_t)b * a.estride : nullptr;
+    T* sums = a.vrow + (size_t)b * a.wstride;  // V0[NI] V1[NI] W0[NJ] W1[NJ]
+    const int nrb = (NI + kSweepRows - 1) / kSweepRows;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    T acc[2 * kSweepCols];
+#pragma unroll
+    for (int r = 0; r < 2 * kSweepCols; ++r) acc[r] = (T)0;
+    if ((int)blockIdx.x < nrb) {
+        const int k0 = blockIdx.x * kSweepRows;
+        for (int l = threadIdx.x; l < NJ; l += blockDim.x) {
+            const T sj0 = a.s.sj0[l], sj1 = a.s.sj1[l];
+#pragma unroll
+            for (int r = 0; r < kSweepRows; ++r) {
+                const int k = k0 + r;
+                if (k < NI) {
+                    const T u = lifted_coef(R[(size_t)k * NJ + l], k, l, E, NI, NJ, a.bc_coef, a.s, a.cosx, a.cosy,
+                                            a.bydx2, a.helmholtz, a.alpha);
+                    acc[2 * r] += u * sj0;
+                    acc[2 * r + 1] += u * sj1;
+                }
+            }
+        }
+    } else {
+        const int l0 = (blockIdx.x - nrb) * kSweepCols;
+        for (int k = threadIdx.x; k < NI; k += blockDim.x) {
+            const T si0 = a.s.si0[k], si1 = a.s.si1[k];
+#pragma unroll
+            for (int c = 0; c < kSweepCols; ++c) {
+                const int l = l0 + c;
+                if (l < NJ) {
+                    const T u = lifted_coef(R[(size_t)k * NJ + l], k, l, E, NI, NJ, a.bc_coef, a.s, a.cosx, a.cosy,
+                                            a.bydx2, a.helmholtz, a.alpha);
+                    acc[2 * c] += u * si0;
+                    acc[2 * c + 1] += u * si1;
+                }
+            }
+        }
+    }
+    const int nv = ((int)blockIdx.x < nrb) ? 2 * kSweepRows : 2 * kSweepCols;
+#pragma unroll
+    for (int r = 0; r < 2 * kSweepCols; ++r) {
+        if (r >= nv) break;
+        T v = acc[r];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) red[wid][r] = v;
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < nv) {
+        const int r = threadIdx.x;
+        T sum = (T)0;
+        for (int ww = 0; ww < (int)(blockDim.x >> 5); ++ww) sum += red[ww][r];
+        if ((int)blockIdx.x < nrb) {
+            const int k = blockIdx.x * kSweepRows + r / 2;
+            if (k < NI) sums[(size_t)(r & 1) * NI + k] = sum;
+        } else {
+            const int l = (blockIdx.x - nrb) * kSweepCols + r / 2;
+            if (l < NJ) sums[2 * (size_t)NI + (size_t)(r & 1) * NJ + l] = sum;
+        }
+    }
+}
+
+// lines: block 0 turns V into the lines u(., j0), u(., j1), the bottom/top
+// boundary values of the finer level and their DSTs; block 1 does the same
+// with W for the left/right values.  blockIdx.y = batch item.
+template <typename T>
+__global__ void __launch_bounds__(512) k_sweep_lines(SweepArgs<T> a) {
+    using C = typename Cplx<T>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const GridDev& g = a.g;
+    const int NI = g.NI, NJ = g.NJ;
+    const int b = blockIdx.y;
+    const bool xdir = blockIdx.x == 0;
+    const int n = xdir ? NI : NJ;
+    const FftDesc& d = xdir ? a.fcol : a.frow;
+    C* s0 = reinterpret_cast<C*>(smem_raw);
+    C* s1 = s0 + d.m;
+    T* v0 = reinterpret_cast<T*>(s1 + d.m);
+    T* v1 = v0 + n;
+    T* u0 = v1 + n;
+    T* u1 = u0 + n;
+    T* e0 = u1 + n;
+    T* e1 = e0 + n;
+    const T* sums = a.vrow + (size_t)b * a.wstride + (xdir ? 0 : 2 * (size_t)NI);
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        v0[k] = sums[k];
+        v1[k] = sums[n + k];
+    }
+    __syncthreads();
+    dst_pair_block<T>(d, n, v0, v1, u0, u1, a.norm, s0, s1);
+    const int ext = xdir ? g.nxe : g.nye;
+    for (int i = 1 + threadIdx.x; i <= n; i += blockDim.x) {
+        const int ii = i / 2 + ext;
+        if (i & 1) {
+            e0[i - 1] = (T)0.5 * (u0[ii - 1] + u0[ii]);
+            e1[i - 1] = (T)0.5 * (u1[ii - 1] + u1[ii]);
+        } else {
+            e0[i - 1] = u0[ii - 1];
+            e1[i - 1] = u1[ii - 1];
+        }
+    }
+    __syncthreads();
+    T* Eo = a.edges_out + (size_t)b * a.estride + (xdir ? 0 : 2 * (size_t)NI);
+    dst_pair_block<T>(d, n, e0, e1, Eo, Eo + n, (T)1, s0, s1);
 }
 
 // ---------------------------------------------------------------------------
@@ -380,19 +567,169 @@ void FftTables::release() {
     tw_row64 = tw_row32 = tw_col64 = tw_col32 = nullptr;
 }
 
+// host values of every table the solves use (shared by the context and the static path)
+void fill_grid_tables(int nx, int ny, int nxe, int nye, std::vector<double>& h) {
+    const int NI = nx - 1, NJ = ny - 1;
+    h.assign(table_doubles(nx, ny), 0.0);
+    const double pi = 4. * atan(1.0);
+    double* cx = h.data();
+    double* cy = cx + nx;
+    double* s = cy + ny;
+    // cos(pi i / nx), i < nx and cos(pi j / ny), j < ny (src/EllipticSolver2d.cc:44-50)
+    for (int i = 0; i < nx; ++i) cx[i] = cos((pi * i) / nx);
+    for (int j = 0; j < ny; ++j) cy[j] = cos((pi * j) / ny);
+    // sine vectors of the spectral boundary lifting and of the boundary lines (mode k + 1)
+    double* sx1 = s;
+    double* sxn = sx1 + NI;
+    double* si0 = sxn + NI;
+    double* si1 = si0 + NI;
+    double* sy1 = si1 + NI;
+    double* syn = sy1 + NJ;
+    double* sj0 = syn + NJ;
+    double* sj1 = sj0 + NJ;
+    const int i0 = nxe, i1 = nx / 2 + nxe, j0 = nye, j1 = ny / 2 + nye;
+    for (int k = 0; k < NI; ++k) {
+        const double K = k + 1;
+        sx1[k] = 2 * sin(pi * K / nx);
+        sxn[k] = 2 * sin(pi * (nx - 1) * K / nx);
+        si0[k] = 2 * sin(pi * i0 * K / nx);
+        si1[k] = 2 * sin(pi * i1 * K / nx);
+    }
+    for (int l = 0; l < NJ; ++l) {
+        const double Lm = l + 1;
+        sy1[l] = 2 * sin(pi * Lm / ny);
+        syn[l] = 2 * sin(pi * (ny - 1) * Lm / ny);
+        sj0[l] = 2 * sin(pi * j0 * Lm / ny);
+        sj1[l] = 2 * sin(pi * j1 * Lm / ny);
+    }
+}
+
 template <typename T>
-static int rows_pairs_per_block(int m) {
-    // keep the FFT working set near 64 KB and the grid large
-    int budget = (int)(65536 / (2 * sizeof(T) * 2));
-    int P = budget / m;
-    if (P < 1) P = 1;
-    if (P > 4) P = 4;
+static void set_views(GridTables<T>& v, T* base, int nx, int ny) {
+    const int NI = nx - 1, NJ = ny - 1;
+    v.cosx = base;
+    v.cosy = base + nx;
+    T* s = base + nx + ny;
+    v.s.sx1 = s;
+    v.s.sxn = s + NI;
+    v.s.si0 = s + 2 * NI;
+    v.s.si1 = s + 3 * NI;
+    v.s.sy1 = s + 4 * NI;
+    v.s.syn = s + 4 * NI + NJ;
+    v.s.sj0 = s + 4 * NI + 2 * NJ;
+    v.s.sj1 = s + 4 * NI + 3 * NJ;
+}
+
+int CosTables::init(int nx, int ny, int nxe, int nye) {
+    std::vector<double> h;
+    fill_grid_tables(nx, ny, nxe, nye, h);
+    std::vector<float> hf(h.size());
+    for (size_t k = 0; k < h.size(); ++k) hf[k] = (float)h[k];
+    if (cudaMalloc(&d64, sizeof(double) * h.size()) || cudaMalloc(&d32, sizeof(float) * h.size()))
+        return IBG_ERR_CUDA;
+    cudaMemcpy(d64, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(d32, hf.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice);
+    attach(nx, ny, d64, d32);
+    return IBG_OK;
+}
+
+void CosTables::attach(int nx, int ny, double* p64, float* p32) {
+    if (p64) set_views(t64, p64, nx, ny);
+    if (p32) set_views(t32, p32, nx, ny);
+}
+
+void CosTables::release() {
+    cudaFree(d64);
+    cudaFree(d32);
+    d64 = nullptr;
+    d32 = nullptr;
+}
+
+template <typename T>
+static int pairs_per_block(int m, int nlines, int nlev, int batch) {
+    // one pair per block unless the grid of blocks is already several waves deep
+    int P = 1;
+    const long long blocks = (long long)((nlines + 1) / 2) * nlev * batch;
+    if (blocks > 8 * 148 && m * 2 * sizeof(typename Cplx<T>::type) * 2 <= 48 * 1024) P = 2;
     return P;
 }
 
 template <typename T>
 size_t fft_smem_bytes(int m, int P) {
-    return sizeof(typename Cplx<T>::type) * (size_t)m * (2 * P + 1);
+    return sizeof(typename Cplx<T>::type) * (size_t)m * (2 * P);
+}
+
+static size_t sweep_work(int nx, int ny) {
+    // row sums V0, V1 [NI each] and column sums W0, W1 [NJ each]
+    return 2 * (size_t)(nx - 1) + 2 * (size_t)(ny - 1);
+}
+
+size_t sweep_doubles(int nx, int ny, int L) {
+    // boundary DSTs [B(NI) T(NI) L(NJ) R(NJ)] of every level, then the sweep's work area
+    return (size_t)L * (2 * (size_t)(nx - 1) + 2 * (size_t)(ny - 1)) + sweep_work(nx, ny);
+}
+
+template <typename T>
+static size_t sweep_smem_bytes(const GridDev& g, int M) {
+    return sizeof(typename Cplx<T>::type) * 2 * (size_t)M + sizeof(T) * 6 * (size_t)std::max(g.NI, g.NJ);
+}
+
+template <typename T>
+void EllipticPlan<T>::launch_rows(const GridDev& g, const FftDesc& frow, int nlev, int batch, const T* const* in,
+                                  const T* const* alt, size_t in_bs, T* const* out, size_t out_bs, T* const* out2,
+                                  const T* const* base, T scale, T norm, cudaStream_t st) const {
+    RowPassArgs<T> A{};
+    A.g = g;
+    A.fft = frow;
+    A.nlev = nlev;
+    for (int l = 0; l < nlev; ++l) {
+        A.in[l] = in[l];
+        A.alt[l] = alt ? alt[l] : nullptr;
+        A.out[l] = out[l];
+        A.out2[l] = out2 ? out2[l] : nullptr;
+        A.base[l] = base ? base[l] : nullptr;
+    }
+    A.in_bstride = in_bs;
+    A.out_bstride = out_bs;
+    A.in_scale = scale;
+    A.norm = norm;
+    const int P = pairs_per_block<T>(frow.m, g.NI, nlev, batch);
+    A.pairs_per_block = P;
+    const int npairs = (g.NI + 1) / 2;
+    k_dst_rows<T><<<dim3((unsigned)((npairs + P - 1) / P), (unsigned)(nlev * batch)), threads,
+                    fft_smem_bytes<T>(frow.m, P), st>>>(A);
+}
+
+template <typename T>
+void EllipticPlan<T>::launch_cols(const GridDev& g, const FftDesc& fcol, int mode, int nlev, int batch, T* buf,
+                                  size_t lstride, size_t bstride, const T* edges, size_t estride,
+                                  cudaStream_t st) const {
+    ColPassArgs<T> B{};
+    B.g = g;
+    B.fft = fcol;
+    B.mode = mode;
+    B.nlev = nlev;
+    B.buf = buf;
+    B.lstride = lstride;
+    B.bstride = bstride;
+    const GridTables<T>& gt = tabs();
+    B.cosx = gt.cosx;
+    B.cosy = gt.cosy;
+    B.s = gt.s;
+    for (int l = 0; l < nlev; ++l) {
+        const double dxl = lev_dx(g, l);
+        B.bydx2[l] = (T)(1.0 / (dxl * dxl));
+        B.bc_coef[l] = helmholtz ? (T)(alpha / (dxl * dxl)) : (T)(1.0 / (dxl * dxl));
+    }
+    B.helmholtz = helmholtz;
+    B.alpha = (T)alpha;
+    B.edges = edges;
+    B.estride = estride;
+    B.elstride = 2 * (size_t)g.NI + 2 * (size_t)g.NJ;
+    const int P = pairs_per_block<T>(fcol.m, g.NJ, nlev, batch);
+    B.pairs_per_block = P;
+    const int ncolblk = (g.NJ + 2 * P - 1) / (2 * P);
+    k_dst_cols<T><<<dim3((unsigned)ncolblk, (unsigned)(nlev * batch)), threads, fft_smem_bytes<T>(fcol.m, P), st>>>(B);
 }
 
 template <typename T>
@@ -401,68 +738,92 @@ int EllipticPlan<T>::solve(const SolveCall<T>& c, cudaStream_t st) const {
     const int L = g.L;
     const size_t N1 = g.N1;
     const int batch = c.batch;
-    if (batch < 1 || batch > 65535) return IBG_ERR_ARG;
-    // 1. coarsify the right-hand side into rc (levels 1..L-1)
-    for (int lev = 1; lev < L; ++lev) {
-        const T* src = (lev == 1) ? c.f : c.rc + (size_t)(lev - 1) * N1;
-        dim3 grd((unsigned)((N1 + 255) / 256), (unsigned)batch);
-        k_coarsify<T><<<grd, 256, 0, st>>>(g, c.f + (size_t)lev * N1, src, c.rc + (size_t)lev * N1, c.bstride);
-    }
+    if (batch < 1 || batch * L > 65535) return IBG_ERR_ARG;
     const FftDesc& frow = sizeof(T) == 8 ? tables->row64 : tables->row32;
     const FftDesc& fcol = sizeof(T) == 8 ? tables->col64 : tables->col32;
-    const int Pr = rows_pairs;
-    const int Pc = cols_pairs;
-    const size_t smr = fft_smem_bytes<T>(frow.m, Pr);
-    const size_t smc = fft_smem_bytes<T>(fcol.m, Pc);
-    const int npairs_r = (g.NI + 1) / 2;
-    const int ncolblk = (g.NJ + 2 * Pc - 1) / (2 * Pc);
-    // 2. coarse-to-fine sweep
-    for (int lev = L - 1; lev >= 0; --lev) {
-        const double dxl = lev_dx(g, lev);
-        const T* rhs = (lev == 0) ? c.f : c.rc + (size_t)lev * N1;
-        RowPassArgs<T> A{};
-        A.g = g;
-        A.fft = frow;
-        A.pairs_per_block = Pr;
-        A.in = rhs;
-        A.out = c.tbuf;
-        A.in_bstride = c.bstride;
-        A.out_bstride = N1;
-        A.lift = 1;
-        A.in_scale = c.in_scale;
-        A.coarse = (lev == L - 1) ? nullptr : c.u + (size_t)(lev + 1) * N1;
-        A.bc_coef = helmholtz ? (T)(alpha / (dxl * dxl)) : (T)(1.0 / (dxl * dxl));
-        A.norm = (T)1;
-        k_dst_rows<T><<<dim3((unsigned)((npairs_r + Pr - 1) / Pr), (unsigned)batch), threads, smr, st>>>(A);
-        ColPassArgs<T> B{};
-        B.g = g;
-        B.fft = fcol;
-        B.pairs_per_block = Pc;
-        B.buf = c.tbuf;
-        B.bstride = N1;
-        B.cosx = (const T*)(sizeof(T) == 8 ? (const void*)cos64x : (const void*)cos32x);
-        B.cosy = (const T*)(sizeof(T) == 8 ? (const void*)cos64y : (const void*)cos32y);
-        B.bydx2 = (T)(1.0 / (dxl * dxl));
-        B.helmholtz = helmholtz;
-        B.alpha = (T)alpha;
-        k_dst_cols<T><<<dim3((unsigned)ncolblk, (unsigned)batch), threads, smc, st>>>(B);
-        RowPassArgs<T> Cc{};
-        Cc.g = g;
-        Cc.fft = frow;
-        Cc.pairs_per_block = Pr;
-        Cc.in = c.tbuf;
-        Cc.out = c.u + (size_t)lev * N1;
-        Cc.in_bstride = N1;
-        Cc.out_bstride = c.bstride;
-        Cc.lift = 0;
-        Cc.in_scale = (T)1;
-        Cc.coarse = nullptr;
-        Cc.norm = (T)(1.0 / (double)(2 * g.nx * 2 * g.ny));
-        Cc.out2 = c.out2 ? c.out2 + (size_t)lev * N1 : nullptr;
-        Cc.base = c.base ? c.base + (size_t)lev * N1 : nullptr;
-        k_dst_rows<T><<<dim3((unsigned)((npairs_r + Pr - 1) / Pr), (unsigned)batch), threads, smr, st>>>(Cc);
+    const T norm = (T)(1.0 / (double)(2 * g.nx * 2 * g.ny));  // src/EllipticSolver2d.cc:80
+    if (L == 1) {
+        const T* in[1] = {c.f};
+        T* tb[1] = {c.tbuf};
+        launch_rows(g, frow, 1, batch, in, nullptr, c.bstride, tb, N1, nullptr, nullptr, c.in_scale, (T)1, st);
+        launch_cols(g, fcol, 1, 1, batch, c.tbuf, N1, N1, nullptr, 0, st);
+        const T* tin[1] = {c.tbuf};
+        T* uo[1] = {c.u};
+        T* o2[1] = {c.out2};
+        const T* bs[1] = {c.base};
+        launch_rows(g, frow, 1, batch, tin, nullptr, N1, uo, c.bstride, c.out2 ? o2 : nullptr,
+                    c.base ? bs : nullptr, (T)1, norm, st);
+        return cudaPeekAtLastError() == cudaSuccess ? IBG_OK : IBG_ERR_CUDA;
     }
+    const size_t tS = (size_t)L * N1;  // coefficients per batch item
+    // 1. coarsify the right-hand side: overlap interiors of levels 1..L-1 into rc
+    const int novl = (g.nx / 2 - 1) * (g.ny / 2 - 1);
+    for (int lev = 1; lev < L; ++lev)
+        k_coarsify<T><<<dim3((unsigned)((novl + 255) / 256), (unsigned)batch), 256, 0, st>>>(g, lev, c.f, c.rc,
+                                                                                          c.bstride);
+    // 2. forward transforms of every level
+    const T* in[kMaxLevels];
+    const T* alt[kMaxLevels];
+    T* tb[kMaxLevels];
+    for (int l = 0; l < L; ++l) {
+        in[l] = c.f + (size_t)l * N1;
+        alt[l] = (l == 0) ? nullptr : c.rc + (size_t)l * N1;
+        tb[l] = c.tbuf + (size_t)l * N1;
+    }
+    launch_rows(g, frow, L, batch, in, alt, c.bstride, tb, tS, nullptr, nullptr, c.in_scale, (T)1, st);
+    launch_cols(g, fcol, 0, L, batch, c.tbuf, N1, tS, nullptr, 0, st);
+    // 3. coarse-to-fine sweep: boundary DSTs of levels L-2 .. 0
+    const size_t es = sweep_doubles(g.nx, g.ny, L);
+    const size_t el = 2 * (size_t)g.NI + 2 * (size_t)g.NJ;
+    const GridTables<T>& gt = tabs();
+    const int M = std::max(frow.m, fcol.m);
+    const size_t ssm = sweep_smem_bytes<T>(g, M);
+    for (int lev = L - 1; lev >= 1; --lev) {
+        const double dxl = lev_dx(g, lev);
+        SweepArgs<T> s{};
+        s.g = g;
+        s.frow = frow;
+        s.fcol = fcol;
+        s.buf = c.tbuf + (size_t)lev * N1;
+        s.bstride = tS;
+        s.cosx = gt.cosx;
+        s.cosy = gt.cosy;
+        s.s = gt.s;
+        s.bydx2 = (T)(1.0 / (dxl * dxl));
+        s.helmholtz = helmholtz;
+        s.alpha = (T)alpha;
+        s.bc_coef = helmholtz ? (T)(alpha / (dxl * dxl)) : (T)(1.0 / (dxl * dxl));
+        s.edges_in = (lev < L - 1) ? c.sweep + (size_t)lev * el : nullptr;
+        s.edges_out = c.sweep + (size_t)(lev - 1) * el;
+        s.estride = es;
+        s.vrow = c.sweep + (size_t)L * el;
+        s.wstride = es;
+        s.norm = norm;
+        const int nrb = (g.NI + kSweepRows - 1) / kSweepRows, ncb = (g.NJ + kSweepCols - 1) / kSweepCols;
+        k_sweep_sums<T><<<dim3((unsigned)(nrb + ncb), (unsigned)batch), 256, 0, st>>>(s);
+        k_sweep_lines<T><<<dim3(2, (unsigned)batch), 512, ssm, st>>>(s);
+    }
+    // 4. inverse transforms of every level (lifting + eigen-inverse applied on load)
+    launch_cols(g, fcol, 3, L, batch, c.tbuf, N1, tS, c.sweep, es, st);
+    T* uo[kMaxLevels];
+    T* o2[kMaxLevels];
+    const T* bs[kMaxLevels];
+    const T* tin[kMaxLevels];
+    for (int l = 0; l < L; ++l) {
+        tin[l] = c.tbuf + (size_t)l * N1;
+        uo[l] = c.u + (size_t)l * N1;
+        o2[l] = c.out2 ? c.out2 + (size_t)l * N1 : nullptr;
+        bs[l] = c.base ? c.base + (size_t)l * N1 : nullptr;
+    }
+    launch_rows(g, frow, L, batch, tin, nullptr, tS, uo, c.bstride, c.out2 ? o2 : nullptr, c.base ? bs : nullptr,
+                (T)1, norm, st);
     return cudaPeekAtLastError() == cudaSuccess ? IBG_OK : IBG_ERR_CUDA;
+}
+
+template <typename T>
+int EllipticPlan<T>::launches() const {
+    const int L = grid->L;
+    return L == 1 ? 3 : (L - 1) + 2 + 2 * (L - 1) + 2;
 }
 
 template <typename T>
@@ -470,22 +831,18 @@ void EllipticPlan<T>::run_pass(int which, const T* in, T* tbuf, cudaStream_t st)
     const GridDev& g = *grid;
     const FftDesc& frow = sizeof(T) == 8 ? tables->row64 : tables->row32;
     const FftDesc& fcol = sizeof(T) == 8 ? tables->col64 : tables->col32;
-    const int Pr = rows_pairs, Pc = cols_pairs;
+    const int L = g.L;
+    const size_t N1 = g.N1;
     if (which == 0) {
-        RowPassArgs<T> A{};
-        A.g = g; A.fft = frow; A.pairs_per_block = Pr; A.in = in; A.out = tbuf;
-        A.in_bstride = g.N1; A.out_bstride = g.N1; A.lift = 1; A.in_scale = (T)1; A.coarse = nullptr;
-        A.norm = (T)1;
-        const int npairs_r = (g.NI + 1) / 2;
-        k_dst_rows<T><<<dim3((unsigned)((npairs_r + Pr - 1) / Pr), 1), threads, fft_smem_bytes<T>(frow.m, Pr), st>>>(A);
+        const T* ins[kMaxLevels];
+        T* outs[kMaxLevels];
+        for (int l = 0; l < L; ++l) {
+            ins[l] = in + (size_t)l * N1;
+            outs[l] = tbuf + (size_t)l * N1;
+        }
+        launch_rows(g, frow, L, 1, ins, nullptr, 0, outs, 0, nullptr, nullptr, (T)1, (T)1, st);
     } else {
-        ColPassArgs<T> B{};
-        B.g = g; B.fft = fcol; B.pairs_per_block = Pc; B.buf = tbuf; B.bstride = g.N1;
-        B.cosx = (const T*)(sizeof(T) == 8 ? (const void*)cos64x : (const void*)cos32x);
-        B.cosy = (const T*)(sizeof(T) == 8 ? (const void*)cos64y : (const void*)cos32y);
-        B.bydx2 = (T)(1.0 / (g.dx * g.dx)); B.helmholtz = helmholtz; B.alpha = (T)alpha;
-        const int ncolblk = (g.NJ + 2 * Pc - 1) / (2 * Pc);
-        k_dst_cols<T><<<dim3((unsigned)ncolblk, 1), threads, fft_smem_bytes<T>(fcol.m, Pc), st>>>(B);
+        launch_cols(g, fcol, 0, L, 1, tbuf, N1, 0, nullptr, 0, st);
     }
 }
 
@@ -495,47 +852,22 @@ int EllipticPlan<T>::init(const GridDev* g, const FftTables* t, bool helm, doubl
     tables = t;
     helmholtz = helm ? 1 : 0;
     alpha = a;
-    cos64x = ct.x64; cos64y = ct.y64; cos32x = ct.x32; cos32y = ct.y32;
+    cos = &ct;
+    threads = 128;
+    if (g->L > kMaxLevels) return IBG_ERR_UNSUPPORTED;
     const FftDesc& frow = sizeof(T) == 8 ? t->row64 : t->row32;
     const FftDesc& fcol = sizeof(T) == 8 ? t->col64 : t->col32;
-    rows_pairs = rows_pairs_per_block<T>(frow.m);
-    cols_pairs = rows_pairs_per_block<T>(fcol.m);
-    // enough blocks to cover the SMs: at these sizes one or two pairs per block
-    if ((g->NI + 1) / 2 / rows_pairs < 296) rows_pairs = 1;
-    if (g->NJ / (2 * cols_pairs) < 296) cols_pairs = 1;
-    threads = 128;
-    size_t smr = fft_smem_bytes<T>(frow.m, rows_pairs);
-    size_t smc = fft_smem_bytes<T>(fcol.m, cols_pairs);
-    if (smr > 227 * 1024 || smc > 227 * 1024) return IBG_ERR_UNSUPPORTED;
-    if (cudaFuncSetAttribute(k_dst_rows<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess)
-        return IBG_ERR_CUDA;
-    if (cudaFuncSetAttribute(k_dst_cols<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess)
+    const int M = std::max(frow.m, fcol.m);
+    if (fft_smem_bytes<T>(M, 1) > 200 * 1024 || sweep_smem_bytes<T>(*g, M) > 200 * 1024) return IBG_ERR_UNSUPPORTED;
+    // dynamic shared memory each kernel may need (static shared memory comes on top)
+    const int rows_need = (int)std::min<size_t>(fft_smem_bytes<T>(frow.m, 2), 200 * 1024);
+    const int cols_need = (int)std::min<size_t>(fft_smem_bytes<T>(fcol.m, 2), 200 * 1024);
+    const int sweep_need = (int)sweep_smem_bytes<T>(*g, M);
+    if (cudaFuncSetAttribute(k_dst_rows<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, rows_need) != cudaSuccess ||
+        cudaFuncSetAttribute(k_dst_cols<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, cols_need) != cudaSuccess ||
+        cudaFuncSetAttribute(k_sweep_lines<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, sweep_need) != cudaSuccess)
         return IBG_ERR_CUDA;
     return IBG_OK;
-}
-
-int CosTables::init(int nx, int ny) {
-    // cos(pi i / nx), i = 0..nx-1 and cos(pi j / ny), j = 0..ny-1 with the
-    // reference's pi = 4 atan(1) (src/EllipticSolver2d.cc:44)
-    const double pi = 4. * atan(1.0);
-    std::vector<double> hx(nx), hy(ny);
-    std::vector<float> fx(nx), fy(ny);
-    for (int i = 0; i < nx; ++i) { hx[i] = cos((pi * i) / nx); fx[i] = (float)hx[i]; }
-    for (int j = 0; j < ny; ++j) { hy[j] = cos((pi * j) / ny); fy[j] = (float)hy[j]; }
-    if (cudaMalloc(&x64, sizeof(double) * nx) || cudaMalloc(&y64, sizeof(double) * ny) ||
-        cudaMalloc(&x32, sizeof(float) * nx) || cudaMalloc(&y32, sizeof(float) * ny))
-        return IBG_ERR_CUDA;
-    cudaMemcpy(x64, hx.data(), sizeof(double) * nx, cudaMemcpyHostToDevice);
-    cudaMemcpy(y64, hy.data(), sizeof(double) * ny, cudaMemcpyHostToDevice);
-    cudaMemcpy(x32, fx.data(), sizeof(float) * nx, cudaMemcpyHostToDevice);
-    cudaMemcpy(y32, fy.data(), sizeof(float) * ny, cudaMemcpyHostToDevice);
-    return IBG_OK;
-}
-
-void CosTables::release() {
-    cudaFree(x64); cudaFree(y64); cudaFree(x32); cudaFree(y32);
-    x64 = y64 = nullptr;
-    x32 = y32 = nullptr;
 }
 
 template struct EllipticPlan<double>;

@@ -1,25 +1,45 @@
-// ibg_kernels.cuh -- kernel argument blocks and host-side plan objects.
+// ibg_kernels.cuh -- kernel argument blocks and host-side plan objects of the
+// multi-domain elliptic solves.
 #pragma once
+#include <algorithm>
+#include <vector>
+
 #include "ibg_internal.cuh"
 
 namespace ibg {
+
+constexpr int kMaxLevels = 16;
+constexpr int kSweepRows = 4;    // coefficient rows per row-sum block of the sweep
+constexpr int kSweepCols = 4;    // coefficient columns per column-sum block of the sweep
 
 template <typename T>
 struct RowPassArgs {
     GridDev g;
     FftDesc fft;
     int pairs_per_block;
-    const T* in;
-    size_t in_bstride;       // batch stride of `in` and `coarse`
-    T* out;
-    size_t out_bstride;      // batch stride of `out`, `out2`, `base`
-    T* out2;                 // optional: out2 = base - out
-    const T* base;
-    int lift;                // apply in_scale and boundary lifting on load
-    T in_scale;
-    const T* coarse;         // next coarser solution level (nullptr: zero boundary)
-    T bc_coef;
-    T norm;                  // output scale
+    int nlev;                      // levels in this launch: blockIdx.y = batch * nlev + level
+    const T* in[kMaxLevels];       // per-level input (batch item 0)
+    const T* alt[kMaxLevels];      // per-level input inside the overlap interior (nullptr: none)
+    size_t in_bstride;
+    T* out[kMaxLevels];
+    size_t out_bstride;            // batch stride of out, out2, base
+    T* out2[kMaxLevels];           // optional: out2 = base - out
+    const T* base[kMaxLevels];
+    T in_scale;                    // multiplies the input (+1 or -1)
+    T norm;                        // multiplies the output
+};
+
+// sine vectors (mode k + 1) of the spectral boundary lifting and the boundary lines
+template <typename T>
+struct SineTab {
+    const T* sx1;   // 2 sin(pi K / nx)
+    const T* sxn;   // 2 sin(pi (nx-1) K / nx)
+    const T* si0;   // 2 sin(pi i0 K / nx), i0 = nxe
+    const T* si1;   // 2 sin(pi i1 K / nx), i1 = nx/2 + nxe
+    const T* sy1;
+    const T* syn;
+    const T* sj0;   // j0 = nye
+    const T* sj1;   // j1 = ny/2 + nye
 };
 
 template <typename T>
@@ -27,13 +47,50 @@ struct ColPassArgs {
     GridDev g;
     FftDesc fft;
     int pairs_per_block;
+    int mode;                      // 0, 2: one DST along i; 1: DST, eigen-inverse, DST (one level);
+                                   // 3: boundary lifting + eigen-inverse on load, one DST
+    int nlev;
     T* buf;
+    size_t lstride, bstride;       // level and batch strides
+    const T* cosx;
+    const T* cosy;
+    SineTab<T> s;
+    T bydx2[kMaxLevels];
+    T bc_coef[kMaxLevels];
+    int helmholtz;
+    T alpha;
+    const T* edges;                // boundary DSTs of every level (mode 3)
+    size_t estride, elstride;      // batch and level strides of edges
+};
+
+
+template <typename T>
+struct GridTables {
+    const T* cosx = nullptr;   // cos(pi i / nx), i < nx
+    const T* cosy = nullptr;
+    SineTab<T> s{};
+};
+
+template <typename T>
+struct SweepArgs {
+    GridDev g;
+    FftDesc frow;                  // length 2 ny
+    FftDesc fcol;                  // length 2 nx
+    const T* buf;                  // this level's forward coefficients (batch item 0)
     size_t bstride;
     const T* cosx;
     const T* cosy;
+    SineTab<T> s;
     T bydx2;
     int helmholtz;
     T alpha;
+    T bc_coef;                     // 1/dx^2 (Poisson) or alpha/dx^2 (Helmholtz) of this level
+    const T* edges_in;             // this level's boundary DSTs (nullptr on the coarsest level)
+    T* edges_out;                  // boundary DSTs of the next finer level
+    size_t estride;                // batch stride of the edges arrays
+    T* vrow;                       // work: row sums V0, V1 [NI] then column sums W0, W1 [NJ]
+    size_t wstride;
+    T norm;
 };
 
 struct FftTables {
@@ -46,12 +103,19 @@ struct FftTables {
     void release();
 };
 
+// doubles in one grid's table block: cos x, cos y, 4 x-sine vectors, 4 y-sine vectors
+inline size_t table_doubles(int nx, int ny) { return (size_t)nx + ny + 4 * (size_t)(nx - 1) + 4 * (size_t)(ny - 1); }
+void fill_grid_tables(int nx, int ny, int nxe, int nye, std::vector<double>& h);
+// scratch of the coarse-to-fine sweep per batch item (elements of T)
+size_t sweep_doubles(int nx, int ny, int L);
+
 struct CosTables {
-    double* x64 = nullptr;
-    double* y64 = nullptr;
-    float* x32 = nullptr;
-    float* y32 = nullptr;
-    int init(int nx, int ny);
+    double* d64 = nullptr;  // owned device block (nullptr when attached to external memory)
+    float* d32 = nullptr;
+    GridTables<double> t64;
+    GridTables<float> t32;
+    int init(int nx, int ny, int nxe, int nye);
+    void attach(int nx, int ny, double* p64, float* p32);
     void release();
 };
 
@@ -64,8 +128,9 @@ template <typename T>
 struct SolveCall {
     const T* f;       // right-hand side, all levels
     T* u;             // solution, all levels
-    T* rc;            // scratch: coarsified right-hand side (levels 1..L-1)
-    T* tbuf;          // scratch: one level per batch item (N1 * batch)
+    T* rc;            // scratch: coarsified right-hand side (levels 1..L-1), bstride per item
+    T* tbuf;          // scratch: spectral coefficients of all levels (L * N1 per batch item)
+    T* sweep;         // scratch: sweep_doubles(nx, ny, L) per batch item
     size_t bstride;   // batch stride of f, u, rc, out2, base
     int batch;
     T in_scale;       // multiplies the right-hand side (+1 or -1)
@@ -77,17 +142,26 @@ template <typename T>
 struct EllipticPlan {
     const GridDev* grid = nullptr;
     const FftTables* tables = nullptr;
+    const CosTables* cos = nullptr;
     int helmholtz = 0;
     double alpha = 0.0;
-    int rows_pairs = 1, cols_pairs = 1, threads = 128;
-    const double* cos64x = nullptr;
-    const double* cos64y = nullptr;
-    const float* cos32x = nullptr;
-    const float* cos32y = nullptr;
+    int threads = 128;
     int init(const GridDev* g, const FftTables* t, bool helm, double a, const CosTables& ct);
     int solve(const SolveCall<T>& c, cudaStream_t st) const;
-    // one pass of the finest level alone (0: rows of pass A, 1: columns of pass B), for timing
+    int launches() const;
+    // one pass of the forward transform of all levels alone (0: rows, 1: columns), for timing
     void run_pass(int which, const T* in, T* tbuf, cudaStream_t st) const;
+    const GridTables<T>& tabs() const;
+    void launch_rows(const GridDev& g, const FftDesc& frow, int nlev, int batch, const T* const* in,
+                     const T* const* alt, size_t in_bs, T* const* out, size_t out_bs, T* const* out2,
+                     const T* const* base, T scale, T norm, cudaStream_t st) const;
+    void launch_cols(const GridDev& g, const FftDesc& fcol, int mode, int nlev, int batch, T* buf, size_t lstride,
+                     size_t bstride, const T* edges, size_t estride, cudaStream_t st) const;
 };
+
+template <>
+inline const GridTables<double>& EllipticPlan<double>::tabs() const { return cos->t64; }
+template <>
+inline const GridTables<float>& EllipticPlan<float>::tabs() const { return cos->t32; }
 
 }  // namespace ibg

@@ -21,15 +21,17 @@ using namespace ibg;
 
 namespace {
 
-// 4 MiB of scratch: (ngrid + 1) * (nx - 1) * (ny - 1) doubles at most
+// 4 MiB of scratch: the coarsified right-hand side, the spectral coefficients
+// of every level and the coarse-to-fine sweep workspace must fit in it
 constexpr size_t kStaticScratchDoubles = (size_t)1 << 19;
-// twiddles for FFT lengths up to 2 * 2048 (nx, ny <= 2048), cosines for nx, ny <= 2048
+// twiddles for FFT lengths up to 2 * 2048 (nx, ny <= 2048) and the grid tables
 constexpr int kStaticMaxM = 4096;
 constexpr int kStaticMaxN = 2048;
+constexpr size_t kStaticTableDoubles = 10 * (size_t)kStaticMaxN;
 
 static __device__ __align__(256) double g_static_scratch[kStaticScratchDoubles];
 static __device__ __align__(256) double2 g_static_twiddles[2 * kStaticMaxM];  // rows, then columns
-static __device__ __align__(256) double g_static_cos[2 * kStaticMaxN];        // cos(pi i/nx), then cos(pi j/ny)
+static __device__ __align__(256) double g_static_cos[kStaticTableDoubles];    // cosine and sine tables
 
 struct DeviceSymbols {
     bool ready = false;
@@ -42,6 +44,12 @@ constexpr int kMaxDevices = 64;
 DeviceSymbols g_dev[kMaxDevices];
 std::mutex g_mutex;
 std::string g_static_error;
+
+// doubles of scratch one solve needs: rc (L N1) + coefficients (L N1) + sweep
+size_t static_scratch_need(int nx, int ny, int L) {
+    const size_t N1 = (size_t)(nx - 1) * (ny - 1);
+    return 2 * (size_t)L * N1 + sweep_doubles(nx, ny, L);
+}
 
 int fail(int code, const std::string& m) {
     g_static_error = m;
@@ -62,10 +70,12 @@ extern "C" int ibg_poisson_solve_static(const ibg_grid* grid, const double* f, d
     if (nx > kStaticMaxN || ny > kStaticMaxN)
         return fail(IBG_ERR_UNSUPPORTED, "ibg_poisson_solve_static: nx and ny must be <= 2048 (static tables)");
     const size_t N1 = (size_t)(nx - 1) * (ny - 1);
-    if ((size_t)(L + 1) * N1 > kStaticScratchDoubles)
+    const size_t need = static_scratch_need(nx, ny, L);
+    if (need > kStaticScratchDoubles)
         return fail(IBG_ERR_UNSUPPORTED,
-                    "ibg_poisson_solve_static: (ngrid+1)*(nx-1)*(ny-1) exceeds the 524288-double (4 MiB) "
-                    "static scratch; use ibg_poisson_solve");
+                    "ibg_poisson_solve_static: the grid needs " + std::to_string(need) +
+                        " doubles of scratch, more than the 524288-double (4 MiB) static scratch; "
+                        "use ibg_poisson_solve");
     if (!fft_supported(2 * nx) || !fft_supported(2 * ny))
         return fail(IBG_ERR_UNSUPPORTED, "ibg_poisson_solve_static: 2*nx and 2*ny must factor into primes <= 13");
     cudaStream_t st = (cudaStream_t)cuda_stream;
@@ -80,9 +90,10 @@ extern "C" int ibg_poisson_solve_static(const ibg_grid* grid, const double* f, d
         cudaError_t e1 = cudaGetSymbolAddress((void**)&ds.scratch, g_static_scratch);
         cudaError_t e2 = cudaGetSymbolAddress((void**)&ds.twiddles, g_static_twiddles);
         cudaError_t e3 = cudaGetSymbolAddress((void**)&ds.cosines, g_static_cos);
-        if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
+        cudaError_t e = e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3);
+        if (e != cudaSuccess)
             return fail(IBG_ERR_CUDA, std::string("ibg_poisson_solve_static: cudaGetSymbolAddress failed: ") +
-                                          cudaGetErrorString(e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3)));
+                                          cudaGetErrorString(e));
         ds.ready = true;
     }
     if (ds.tab_nx != nx || ds.tab_ny != ny) {
@@ -98,10 +109,8 @@ extern "C" int ibg_poisson_solve_static(const ibg_grid* grid, const double* f, d
             const double a = -2.0 * pi2 * (double)k / (double)mc;
             tw[kStaticMaxM + k] = make_double2(cos(a), sin(a));
         }
-        const double pi = 4. * atan(1.0);
-        std::vector<double> cs(2 * (size_t)kStaticMaxN);
-        for (int i = 0; i < nx; ++i) cs[i] = cos((pi * i) / nx);
-        for (int j = 0; j < ny; ++j) cs[kStaticMaxN + j] = cos((pi * j) / ny);
+        std::vector<double> cs;
+        fill_grid_tables(nx, ny, (int)floor(nx / 4 * (1 - 0.0) + 0.5), (int)floor(ny / 4 * (1 - 0.0) + 0.5), cs);
         if (cudaMemcpyAsync(ds.twiddles, tw.data(), sizeof(double2) * tw.size(), cudaMemcpyHostToDevice, st) !=
                 cudaSuccess ||
             cudaMemcpyAsync(ds.cosines, cs.data(), sizeof(double) * cs.size(), cudaMemcpyHostToDevice, st) !=
@@ -132,9 +141,8 @@ extern "C" int ibg_poisson_solve_static(const ibg_grid* grid, const double* f, d
     fft_describe(2 * nx, tables.col64);
     tables.row64.tw = ds.twiddles;
     tables.col64.tw = ds.twiddles + kStaticMaxM;
-    CosTables ct;
-    ct.x64 = ds.cosines;
-    ct.y64 = ds.cosines + kStaticMaxN;
+    CosTables ct;  // views into g_static_cos; owns nothing
+    ct.attach(nx, ny, ds.cosines, nullptr);
     EllipticPlan<double> plan;
     if (plan.init(&g, &tables, false, 0.0, ct) != IBG_OK)
         return fail(IBG_ERR_CUDA, "ibg_poisson_solve_static: kernel set-up failed");
@@ -142,8 +150,9 @@ extern "C" int ibg_poisson_solve_static(const ibg_grid* grid, const double* f, d
     SolveCall<double> c{};
     c.f = f;
     c.u = u;
-    c.rc = ds.scratch;                    // levels 1..L-1 at rc + lev*N1
-    c.tbuf = ds.scratch + (size_t)L * N1; // one level of transform workspace
+    c.rc = ds.scratch;                        // levels 1..L-1 at rc + lev*N1
+    c.tbuf = ds.scratch + (size_t)L * N1;     // spectral coefficients of every level
+    c.sweep = ds.scratch + (size_t)2 * L * N1;
     c.bstride = (size_t)L * N1;
     c.batch = 1;
     c.in_scale = 1.0;
