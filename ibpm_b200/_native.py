@@ -31,7 +31,7 @@ class ibg_params(ctypes.Structure):
 
 
 SCHEMES = {"euler": 0, "ab2": 1, "rk3": 2, "rk3b": 3}
-PRECISIONS = {"fp64": 0, "fp32_refined": 1}
+PRECISIONS = {"fp64": 0, "fp32_refined": 1, "fp32": 2}
 
 # every entry point declared in include/ibpm_b200.h: name -> (restype, argtypes)
 _VP = ctypes.c_void_p

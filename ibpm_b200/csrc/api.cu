@@ -59,6 +59,33 @@ Scheme make_scheme(int s) {
 constexpr int kHistCap = 1 << 16;
 }  // namespace
 
+// bulk fields and solver plans in one arithmetic type
+template <typename T>
+struct Bulk {
+    T *w = nullptr, *q = nullptr, *a = nullptr, *ws = nullptr, *psi = nullptr, *cc = nullptr, *rc = nullptr;
+    T *tbuf = nullptr, *sweep = nullptr, *U = nullptr, *V = nullptr, *C = nullptr, *Bf = nullptr, *qtmp = nullptr;
+    T* Nbuf[4] = {nullptr, nullptr, nullptr, nullptr};
+    EllipticPlan<T> poisson;
+    EllipticPlan<T> helm[4];
+    bool ready = false;
+    void release() {
+        T* ptrs[] = {w, q, a, ws, psi, cc, rc, tbuf, sweep, U, V, C, Bf, qtmp, Nbuf[0], Nbuf[1], Nbuf[2], Nbuf[3]};
+        for (T* p : ptrs)
+            if (p) cudaFree(p);
+        w = q = a = ws = psi = cc = rc = tbuf = sweep = U = V = C = Bf = qtmp = nullptr;
+        for (auto& n : Nbuf) n = nullptr;
+        ready = false;
+    }
+};
+
+namespace ibg {
+template <typename A, typename B>
+__global__ void k_convert(size_t n, const A* __restrict__ in, B* __restrict__ out) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (B)in[i];
+}
+}  // namespace ibg
+
 struct ibg_context {
     // configuration
     GridDev g{};
@@ -68,14 +95,15 @@ struct ibg_context {
     double u0 = 0, v0 = 0;
     int npts = 0, ncomp = 0;
     bool moving = false;
+    bool fp32 = false;  // bulk fields of the time step in FP32
     cudaStream_t st = nullptr;
     bool own_stream = false;
     std::string err;
-    // plans
+    // plans and bulk fields (FP64 always: state I/O, operator entry points, Cholesky build)
     FftTables fft;
     CosTables cosT;
-    EllipticPlan<double> poisson;
-    EllipticPlan<double> helm[4];
+    Bulk<double> b64;
+    Bulk<float> b32;
     double beta[4] = {0, 0, 0, 0};
     // bodies
     std::vector<BodyDev> h_bodies;
@@ -86,17 +114,15 @@ struct ibg_context {
     RegSlots slots;
     double* d_b = nullptr;
     double* d_time = nullptr;
-    // state
-    double *w = nullptr, *q = nullptr, *f = nullptr;
+    // state (f is FP64 in every form)
+    double* f = nullptr;
     int timestep = 0;
     double time = 0;
     bool old_saved = false;
+    bool state_in_32 = false;  // the FP32 copy of omega/q is the current one
     // work
-    double* Nbuf[4] = {nullptr, nullptr, nullptr, nullptr};
     int nring = 0;
-    double *a = nullptr, *ws = nullptr, *psi = nullptr, *cc = nullptr, *rc = nullptr, *tbuf = nullptr;
-    double *U = nullptr, *V = nullptr, *C = nullptr, *flux0 = nullptr, *Bf = nullptr;
-    double *rhsb = nullptr, *btmp = nullptr, *qtmp = nullptr, *sweep = nullptr;
+    double *flux0 = nullptr, *rhsb = nullptr, *btmp = nullptr;
     // Cholesky factors per sub-step
     double* Lr[4] = {nullptr, nullptr, nullptr, nullptr};
     double* Lc[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -139,21 +165,39 @@ struct ibg_context {
         return IBG_OK;
     }
 
+    template <typename T>
+    int alloc_bulk(Bulk<T>& B) {
+        int s = alloc(&B.w, S) || alloc(&B.q, F) || alloc(&B.a, S) || alloc(&B.ws, S) || alloc(&B.psi, S) ||
+                alloc(&B.cc, S) || alloc(&B.rc, S) || alloc(&B.tbuf, S) ||
+                alloc(&B.sweep, sweep_doubles(g.nx, g.ny, g.L)) || alloc(&B.U, S) || alloc(&B.V, S) ||
+                alloc(&B.C, F) || alloc(&B.Bf, S) || alloc(&B.qtmp, F);
+        for (int k = 0; k < nring && !s; ++k) s = alloc(&B.Nbuf[k], S);
+        if (s) return IBG_ERR_CUDA;
+        s = B.poisson.init(&g, &fft, false, 0.0, cosT);
+        for (int k = 0; k < sch.nsub && !s; ++k) {
+            const double alpha = -beta[k] / 2. * (1. / prm.Re);  // src/ProjectionSolver.cc:33
+            s = B.helm[k].init(&g, &fft, true, alpha, cosT);
+        }
+        if (s) return s;
+        B.ready = true;
+        return IBG_OK;
+    }
+
     void release() {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
-        void* ptrs[] = {d_ref, d_pts, d_vel, d_body_of, d_bodies, slots.idx, slots.w, slots.n, d_b, d_time, w, q, f,
-                        a, ws, psi, cc, rc, tbuf, U, V, C, flux0, Bf, rhsb, btmp, d_status, cg_r, cg_d, cg_q,
-                        cg_scal, cg_flags, d_hist, d_hist_count, qtmp, sweep};
+        b64.release();
+        b32.release();
+        void* ptrs[] = {d_ref, d_pts, d_vel, d_body_of, d_bodies, slots.idx, slots.w, slots.n, d_b, d_time, f,
+                        flux0, rhsb, btmp, d_status, cg_r, cg_d, cg_q, cg_scal, cg_flags, d_hist, d_hist_count};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         for (int k = 0; k < 4; ++k) {
-            if (Nbuf[k]) cudaFree(Nbuf[k]);
             if (Lr[k]) cudaFree(Lr[k]);
             if (Lc[k]) cudaFree(Lc[k]);
             if (Ld[k]) cudaFree(Ld[k]);
             if (Mi[k]) cudaFree(Mi[k]);
-            Nbuf[k] = Lr[k] = Lc[k] = Ld[k] = Mi[k] = nullptr;
+            Lr[k] = Lc[k] = Ld[k] = Mi[k] = nullptr;
         }
         if (h_flags) cudaFreeHost(h_flags);
         h_flags = nullptr;
@@ -165,7 +209,7 @@ struct ibg_context {
         d_body_of = nullptr;
         d_bodies = nullptr;
         slots = RegSlots{};
-        d_b = d_time = w = q = f = a = ws = psi = cc = rc = tbuf = U = V = C = flux0 = Bf = rhsb = btmp = qtmp = sweep = nullptr;
+        d_b = d_time = f = flux0 = rhsb = btmp = nullptr;
         d_status = nullptr;
         cg_r = cg_d = cg_q = cg_scal = nullptr;
         cg_flags = nullptr;
@@ -173,15 +217,18 @@ struct ibg_context {
         d_hist_count = nullptr;
     }
 
+    Bulk<double>& bulk(double*) { return b64; }
+    Bulk<float>& bulk(float*) { return b32; }
+
     // -----------------------------------------------------------------------
-    SolveCall<double> call(const double* fin, double* uout, double scale, double* out2 = nullptr,
-                           const double* base = nullptr) {
-        SolveCall<double> c{};
+    template <typename T>
+    SolveCall<T> call(Bulk<T>& B, const T* fin, T* uout, T scale, T* out2 = nullptr, const T* base = nullptr) {
+        SolveCall<T> c{};
         c.f = fin;
         c.u = uout;
-        c.rc = rc;
-        c.tbuf = tbuf;
-        c.sweep = sweep;
+        c.rc = B.rc;
+        c.tbuf = B.tbuf;
+        c.sweep = B.sweep;
         c.bstride = S;
         c.batch = 1;
         c.in_scale = scale;
@@ -189,28 +236,30 @@ struct ibg_context {
         c.base = base;
         return c;
     }
-    long long solve_launches() const { return poisson.launches(); }
+    long long solve_launches() const { return b64.poisson.launches(); }
 
     // M d = C A^-1 B d  (src/ProjectionSolver.cc:96-101)
-    void m_apply(int k, const double* din, double* dout) {
-        launch_smear_bf<double>(g, ncomp, slots, din, flux0, Bf, beta[k], st);
-        helm[k].solve(call(Bf, cc, 1.0), st);
-        poisson.solve(call(cc, psi, -1.0), st);
-        launch_reg_interp<double>(g, ncomp, slots, psi, S, 1, nullptr, dout, 0, st);
+    template <typename T>
+    void m_apply(Bulk<T>& B, int k, const double* din, double* dout) {
+        launch_smear_bf<T>(g, ncomp, slots, din, flux0, B.Bf, beta[k], st);
+        B.helm[k].solve(call<T>(B, B.Bf, B.cc, (T)1), st);
+        B.poisson.solve(call<T>(B, B.cc, B.psi, (T)-1), st);
+        launch_reg_interp<T>(g, ncomp, slots, B.psi, S, 1, nullptr, dout, 0, st);
         launches += 3 + 2 * solve_launches() + 1;
     }
 
     // CG with warm start x = f (src/ConjugateGradientSolver.cc:35-65); host reads the
     // convergence flag every `chunk` iterations.
-    int cg_solve(int k, const double* b, double* x) {
-        m_apply(k, x, cg_q);
+    template <typename T>
+    int cg_solve(Bulk<T>& B, int k, const double* b, double* x) {
+        m_apply<T>(B, k, x, cg_q);
         cg_begin(ncomp, b, cg_q, cg_r, cg_d, cg_scal, cg_flags, st);
         launches += 1;
         int chunk = cg_last > 4 ? cg_last - 2 : 4;
         int done_iters = 0;
         for (;;) {
             for (int c = 0; c < chunk; ++c) {
-                m_apply(k, cg_d, cg_q);
+                m_apply<T>(B, k, cg_d, cg_q);
                 cg_update(ncomp, x, cg_r, cg_d, cg_q, cg_scal, cg_flags, st);
                 launches += 1;
             }
@@ -228,28 +277,30 @@ struct ibg_context {
     }
 
     // the projection of one sub-step (src/ProjectionSolver.cc:57-79) given a and b
-    int projection(int k, const double* a_in, const double* b_in) {
-        helm[k].solve(call(a_in, ws, 1.0), st);                          // omega* = A^-1 a
-        poisson.solve(call(ws, psi, -1.0), st);                          // psi* = L^-1(-omega*)
-        launch_reg_interp<double>(g, ncomp, slots, psi, S, 1, b_in, rhsb, 0, st);  // C omega* - b
+    template <typename T>
+    int projection(Bulk<T>& B, int k, const T* a_in, const double* b_in) {
+        B.helm[k].solve(call<T>(B, a_in, B.ws, (T)1), st);                        // omega* = A^-1 a
+        B.poisson.solve(call<T>(B, B.ws, B.psi, (T)-1), st);                      // psi* = L^-1(-omega*)
+        launch_reg_interp<T>(g, ncomp, slots, B.psi, S, 1, b_in, rhsb, 0, st);   // C omega* - b
         launches += 2 * solve_launches() + 1;
         if (!moving) {
-            minv_apply(ncomp, Mi[k], rhsb, f, st);                        // f = M^-1 rhs
+            minv_apply(ncomp, Mi[k], rhsb, f, st);                                  // f = M^-1 rhs
             launches += 1;
         } else {
-            int s = cg_solve(k, rhsb, f);
+            int s = cg_solve<T>(B, k, rhsb, f);
             if (s) return s;
         }
-        launch_smear_bf<double>(g, ncomp, slots, f, flux0, Bf, beta[k], st);  // B f
-        helm[k].solve(call(Bf, cc, 1.0, w, ws), st);                    // omega = omega* - A^-1 B f
+        launch_smear_bf<T>(g, ncomp, slots, f, flux0, B.Bf, beta[k], st);         // B f
+        B.helm[k].solve(call<T>(B, B.Bf, B.cc, (T)1, B.w, B.ws), st);            // omega = omega* - A^-1 B f
         launches += 3 + solve_launches();
         return IBG_OK;
     }
 
     // q = Curl(L^-1(-omega)) + q0 (src/NavierStokesModel.cc:121-140)
-    void refresh() {
-        poisson.solve(call(w, psi, -1.0), st);
-        launch_refresh_flux<double>(g, psi, q, u0, v0, st);
+    template <typename T>
+    void refresh(Bulk<T>& B) {
+        B.poisson.solve(call<T>(B, B.w, B.psi, (T)-1), st);
+        launch_refresh_flux<T>(g, B.psi, B.q, u0, v0, st);
         launches += solve_launches() + 1;
     }
 
@@ -260,30 +311,31 @@ struct ibg_context {
     }
 
     // IBSolver::advanceSubstep (src/IBSolver.cc:162-198)
-    int substep(int k) {
+    template <typename T>
+    int substep(Bulk<T>& B, int k) {
         const double an = sch.an[k], bn = sch.bn[k], cn = sch.cn[k];
-        double* Nk;
-        double* Np;
+        T* Nk;
+        T* Np;
         if (sch.nsub == 1) {
-            Nk = Nbuf[0];
-            Np = Nbuf[1];
+            Nk = B.Nbuf[0];
+            Np = B.Nbuf[1];
         } else {
-            Nk = Nbuf[k];
-            Np = Nbuf[(k + sch.nsub - 1) % sch.nsub];
+            Nk = B.Nbuf[k];
+            Np = B.Nbuf[(k + sch.nsub - 1) % sch.nsub];
         }
-        launch_nonlinear<double>(g, q, w, U, V, C, Nk, 1, S, F, st);
+        launch_nonlinear<T>(g, B.q, B.w, B.U, B.V, B.C, Nk, 1, S, F, st);
         launches += 2 + g.L;
         if (moving) move_bodies(cn * prm.dt);
-        const double* Nprev = nullptr;
+        const T* Nprev = nullptr;
         if (bn != 0) Nprev = old_saved ? Np : Nk;
         const double c1 = 0.5 * (1.0 / prm.Re) * (an + bn);
-        launch_rhs<double>(g, w, Nk, Nprev, a, c1, an, bn, prm.dt, st);
+        launch_rhs<T>(g, B.w, Nk, Nprev, B.a, c1, an, bn, prm.dt, st);
         launches += 1;
-        int s = projection(k, a, d_b);
+        int s = projection<T>(B, k, B.a, d_b);
         if (s) return s;
-        refresh();
+        refresh<T>(B);
         if (sch.nsub == 1) {
-            cudaMemcpyAsync(Np, Nk, sizeof(double) * S, cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(Np, Nk, sizeof(T) * S, cudaMemcpyDeviceToDevice, st);
             launches += 1;
         }
         old_saved = true;
@@ -292,13 +344,26 @@ struct ibg_context {
 
     int enqueue_step() {
         for (int k = 0; k < sch.nsub; ++k) {
-            int s = substep(k);
+            int s = fp32 ? substep<float>(b32, k) : substep<double>(b64, k);
             if (s) return s;
         }
         add_time(d_time, prm.dt, st);
         net_force_record();
         launches += 2;
         return IBG_OK;
+    }
+
+    // make the FP32 copy current (after the FP64 state was written) or the FP64 copy current
+    void to32() {
+        if (!fp32) return;
+        k_convert<double, float><<<(unsigned)((S + 255) / 256), 256, 0, st>>>(S, b64.w, b32.w);
+        k_convert<double, float><<<(unsigned)((F + 255) / 256), 256, 0, st>>>(F, b64.q, b32.q);
+        state_in_32 = true;
+    }
+    void to64() {
+        if (!fp32 || !state_in_32) return;
+        k_convert<float, double><<<(unsigned)((S + 255) / 256), 256, 0, st>>>(S, b32.w, b64.w);
+        k_convert<float, double><<<(unsigned)((F + 255) / 256), 256, 0, st>>>(F, b32.q, b64.q);
     }
 
     void net_force_record();
@@ -364,8 +429,8 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
         g_create_error = "ibg_create: Re and dt must be positive";
         return IBG_ERR_ARG;
     }
-    if (params->precision != IBG_PRECISION_FP64) {
-        g_create_error = "ibg_create: only IBG_PRECISION_FP64 is available in this build";
+    if (params->precision != IBG_PRECISION_FP64 && params->precision != IBG_PRECISION_FP32) {
+        g_create_error = "ibg_create: precision must be IBG_PRECISION_FP64 or IBG_PRECISION_FP32";
         return IBG_ERR_UNSUPPORTED;
     }
     if (!fft_supported(2 * G.nx) || !fft_supported(2 * G.ny)) {
@@ -455,30 +520,24 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
         delete c;
         return s;
     }
-    s = c->poisson.init(&c->g, &c->fft, false, 0.0, c->cosT);
-    for (int k = 0; k < sch.nsub && !s; ++k) {
-        c->beta[k] = (sch.an[k] + sch.bn[k]) * c->prm.dt;           // src/IBSolver.cc:110-114
-        const double alpha = -c->beta[k] / 2. * (1. / c->prm.Re);    // src/ProjectionSolver.cc:33
-        s = c->helm[k].init(&c->g, &c->fft, true, alpha, c->cosT);
-    }
+    for (int k = 0; k < sch.nsub; ++k) c->beta[k] = (sch.an[k] + sch.bn[k]) * c->prm.dt;  // src/IBSolver.cc:110-114
+    c->nring = sch.nsub == 1 ? 2 : sch.nsub;
+    c->fp32 = (c->prm.precision == IBG_PRECISION_FP32);
+    s = c->alloc_bulk(c->b64);
+    if (!s && c->fp32) s = c->alloc_bulk(c->b32);
     if (s) {
-        g_create_error = "ibg_create: solver plan setup failed";
+        g_create_error = "ibg_create: solver set-up or device allocation failed";
         delete c;
         return s;
     }
-    c->nring = sch.nsub == 1 ? 2 : sch.nsub;
-    s = s || c->alloc(&c->w, S) || c->alloc(&c->q, F) || c->alloc(&c->f, m) || c->alloc(&c->a, S) ||
-        c->alloc(&c->ws, S) || c->alloc(&c->psi, S) || c->alloc(&c->cc, S) || c->alloc(&c->rc, S) ||
-        c->alloc(&c->tbuf, S) || c->alloc(&c->sweep, sweep_doubles(g.nx, g.ny, g.L)) || c->alloc(&c->U, S) || c->alloc(&c->V, S) || c->alloc(&c->C, F) ||
-        c->alloc(&c->flux0, (size_t)g.F1) || c->alloc(&c->Bf, S) || c->alloc(&c->rhsb, m) ||
-        c->alloc(&c->btmp, m) || c->alloc(&c->qtmp, F) || c->alloc(&c->d_ref, 2 * (size_t)c->npts) ||
+    s = s || c->alloc(&c->f, m) || c->alloc(&c->flux0, (size_t)g.F1) || c->alloc(&c->rhsb, m) ||
+        c->alloc(&c->btmp, m) || c->alloc(&c->d_ref, 2 * (size_t)c->npts) ||
         c->alloc(&c->d_pts, 2 * (size_t)c->npts) || c->alloc(&c->d_vel, 2 * (size_t)c->npts) ||
         c->alloc(&c->d_body_of, (size_t)c->npts) || c->alloc(&c->d_bodies, c->h_bodies.size()) ||
         c->alloc(&c->slots.idx, kSlots * m) || c->alloc(&c->slots.w, kSlots * m) || c->alloc(&c->slots.n, m) ||
         c->alloc(&c->d_b, m) || c->alloc(&c->d_time, 1) || c->alloc(&c->d_status, 1) || c->alloc(&c->cg_r, m) ||
         c->alloc(&c->cg_d, m) || c->alloc(&c->cg_q, m) || c->alloc(&c->cg_scal, 4) || c->alloc(&c->cg_flags, 4) ||
         c->alloc(&c->d_hist, 2 * (size_t)kHistCap) || c->alloc(&c->d_hist_count, 1);
-    for (int k = 0; k < c->nring && !s; ++k) s = c->alloc(&c->Nbuf[k], S);
     if (!s && cudaMallocHost((void**)&c->h_flags, 4 * sizeof(int)) != cudaSuccess) s = IBG_ERR_CUDA;
     if (s) {
         g_create_error = "ibg_create: device allocation failed";
@@ -551,12 +610,12 @@ int ibg_init(ibg_context* c) {
             SolveCall<double> h{};
             h.f = bf; h.u = u; h.rc = rcb; h.tbuf = tb; h.sweep = swb; h.bstride = S;
             h.batch = nb; h.in_scale = 1.0;
-            c->helm[k].solve(h, c->st);
+            c->b64.helm[k].solve(h, c->st);
             SolveCall<double> pc{};
             pc.f = u; pc.u = p; pc.rc = rcb; pc.tbuf = tb; pc.sweep = swb; pc.bstride = S;
             pc.batch = nb;
             pc.in_scale = -1.0;
-            c->poisson.solve(pc, c->st);
+            c->b64.poisson.solve(pc, c->st);
             launch_reg_interp<double>(g, m, c->slots, p, S, nb, nullptr, Mcol + (size_t)col0 * m, (size_t)m, c->st);
         }
         s = chol_factor(m, Mcol, c->Lr[k], c->Lc[k], c->Ld[k], c->d_status, c->st);
@@ -643,8 +702,9 @@ int ibg_load(ibg_context* c, const char* basename) {
 
 int ibg_set_state(ibg_context* c, const double* omega, const double* q, const double* f, int timestep, double time) {
     if (!c) return IBG_ERR_ARG;
-    if (omega) cudaMemcpyAsync(c->w, omega, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
-    else cudaMemsetAsync(c->w, 0, sizeof(double) * c->S, c->st);
+    Bulk<double>& B = c->b64;
+    if (omega) cudaMemcpyAsync(B.w, omega, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
+    else cudaMemsetAsync(B.w, 0, sizeof(double) * c->S, c->st);
     if (f) cudaMemcpyAsync(c->f, f, sizeof(double) * c->ncomp, cudaMemcpyHostToDevice, c->st);
     else cudaMemsetAsync(c->f, 0, sizeof(double) * c->ncomp, c->st);
     c->timestep = timestep;
@@ -653,19 +713,22 @@ int ibg_set_state(ibg_context* c, const double* omega, const double* q, const do
     cudaMemsetAsync(c->d_hist_count, 0, sizeof(int), c->st);
     c->hist_steps = 0;
     if (q) {
-        cudaMemcpyAsync(c->q, q, sizeof(double) * c->F, cudaMemcpyHostToDevice, c->st);
+        cudaMemcpyAsync(B.q, q, sizeof(double) * c->F, cudaMemcpyHostToDevice, c->st);
     } else {
         if (c->moving) c->move_bodies(0.0);
-        c->refresh();
+        c->refresh<double>(B);
     }
+    c->state_in_32 = false;
+    c->to32();
     if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->cuda_check("ibg_set_state");
     return c->cuda_check("ibg_set_state");
 }
 
 int ibg_get_state(ibg_context* c, double* omega, double* q, double* f, int* timestep, double* time) {
     if (!c) return IBG_ERR_ARG;
-    if (omega) cudaMemcpyAsync(omega, c->w, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
-    if (q) cudaMemcpyAsync(q, c->q, sizeof(double) * c->F, cudaMemcpyDeviceToHost, c->st);
+    if (omega || q) c->to64();
+    if (omega) cudaMemcpyAsync(omega, c->b64.w, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
+    if (q) cudaMemcpyAsync(q, c->b64.q, sizeof(double) * c->F, cudaMemcpyDeviceToHost, c->st);
     if (f) cudaMemcpyAsync(f, c->f, sizeof(double) * c->ncomp, cudaMemcpyDeviceToHost, c->st);
     if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->cuda_check("ibg_get_state");
     if (timestep) *timestep = c->timestep;
@@ -688,7 +751,12 @@ int ibg_update_operators(ibg_context* c, double time) {
 
 int ibg_refresh_state(ibg_context* c) {
     if (!c) return IBG_ERR_ARG;
-    c->refresh();
+    if (c->fp32) {
+        if (!c->state_in_32) c->to32();
+        c->refresh<float>(c->b32);
+    } else {
+        c->refresh<double>(c->b64);
+    }
     if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->cuda_check("ibg_refresh_state");
     return c->cuda_check("ibg_refresh_state");
 }
@@ -697,6 +765,7 @@ int ibg_advance(ibg_context* c, int nsteps) {
     if (!c || nsteps < 0) return IBG_ERR_ARG;
     if (!c->moving && !c->chol_ready) return c->fail(IBG_ERR_STATE, "ibg_advance: call ibg_init (or ibg_load) first");
     const long long l0 = c->launches;
+    if (c->fp32 && !c->state_in_32) c->to32();
     for (int n = 0; n < nsteps; ++n) {
         if (!c->moving && c->old_saved) {
             if (!c->graph) {
@@ -793,9 +862,10 @@ static int finish(ibg_context* c, const char* where) {
 
 int ibg_poisson_solve(ibg_context* c, const double* f, double* u) {
     if (!c || !f || !u) return IBG_ERR_ARG;
-    cudaMemcpyAsync(c->a, f, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
-    c->poisson.solve(c->call(c->a, c->psi, 1.0), c->st);
-    cudaMemcpyAsync(u, c->psi, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
+    Bulk<double>& B = c->b64;
+    cudaMemcpyAsync(B.a, f, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
+    B.poisson.solve(c->call<double>(B, B.a, B.psi, 1.0), c->st);
+    cudaMemcpyAsync(u, B.psi, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
     return finish(c, "ibg_poisson_solve");
 }
 
@@ -803,50 +873,54 @@ int ibg_helmholtz_solve(ibg_context* c, double alpha, const double* f, double* u
     if (!c || !f || !u) return IBG_ERR_ARG;
     EllipticPlan<double> h;
     if (h.init(&c->g, &c->fft, true, alpha, c->cosT)) return c->fail(IBG_ERR_CUDA, "helmholtz plan");
-    cudaMemcpyAsync(c->a, f, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
-    h.solve(c->call(c->a, c->psi, 1.0), c->st);
-    cudaMemcpyAsync(u, c->psi, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
+    Bulk<double>& B = c->b64;
+    cudaMemcpyAsync(B.a, f, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
+    h.solve(c->call<double>(B, B.a, B.psi, 1.0), c->st);
+    cudaMemcpyAsync(u, B.psi, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
     return finish(c, "ibg_helmholtz_solve");
 }
 
 int ibg_nonlinear(ibg_context* c, const double* q, const double* omega, double* out) {
     if (!c || !q || !omega || !out) return IBG_ERR_ARG;
-    cudaMemcpyAsync(c->qtmp, q, sizeof(double) * c->F, cudaMemcpyHostToDevice, c->st);
-    cudaMemcpyAsync(c->a, omega, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
-    launch_nonlinear<double>(c->g, c->qtmp, c->a, c->U, c->V, c->C, c->cc, 1, c->S, c->F, c->st);
-    cudaMemcpyAsync(out, c->cc, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
+    Bulk<double>& B = c->b64;
+    cudaMemcpyAsync(B.qtmp, q, sizeof(double) * c->F, cudaMemcpyHostToDevice, c->st);
+    cudaMemcpyAsync(B.a, omega, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
+    launch_nonlinear<double>(c->g, B.qtmp, B.a, B.U, B.V, B.C, B.cc, 1, c->S, c->F, c->st);
+    cudaMemcpyAsync(out, B.cc, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
     return finish(c, "ibg_nonlinear");
 }
 
 int ibg_laplacian(ibg_context* c, const double* fin, double* out) {
     if (!c || !fin || !out) return IBG_ERR_ARG;
-    cudaMemcpyAsync(c->a, fin, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
-    launch_laplacian<double>(c->g, c->a, c->psi, c->st);
-    cudaMemcpyAsync(out, c->psi, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
+    Bulk<double>& B = c->b64;
+    cudaMemcpyAsync(B.a, fin, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
+    launch_laplacian<double>(c->g, B.a, B.psi, c->st);
+    cudaMemcpyAsync(out, B.psi, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
     return finish(c, "ibg_laplacian");
 }
 
 int ibg_model_B(ibg_context* c, const double* fb, double* omega) {
     if (!c || !fb || !omega) return IBG_ERR_ARG;
     cudaMemcpyAsync(c->btmp, fb, sizeof(double) * c->ncomp, cudaMemcpyHostToDevice, c->st);
-    launch_smear_bf<double>(c->g, c->ncomp, c->slots, c->btmp, c->flux0, c->Bf, 1.0, c->st);
-    cudaMemcpyAsync(omega, c->Bf, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
+    launch_smear_bf<double>(c->g, c->ncomp, c->slots, c->btmp, c->flux0, c->b64.Bf, 1.0, c->st);
+    cudaMemcpyAsync(omega, c->b64.Bf, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
     return finish(c, "ibg_model_B");
 }
 
 int ibg_model_C(ibg_context* c, const double* omega, double* fb) {
     if (!c || !omega || !fb) return IBG_ERR_ARG;
-    cudaMemcpyAsync(c->a, omega, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
-    c->poisson.solve(c->call(c->a, c->psi, -1.0), c->st);
-    launch_reg_interp<double>(c->g, c->ncomp, c->slots, c->psi, c->S, 1, nullptr, c->btmp, 0, c->st);
+    Bulk<double>& B = c->b64;
+    cudaMemcpyAsync(B.a, omega, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
+    B.poisson.solve(c->call<double>(B, B.a, B.psi, -1.0), c->st);
+    launch_reg_interp<double>(c->g, c->ncomp, c->slots, B.psi, c->S, 1, nullptr, c->btmp, 0, c->st);
     cudaMemcpyAsync(fb, c->btmp, sizeof(double) * c->ncomp, cudaMemcpyDeviceToHost, c->st);
     return finish(c, "ibg_model_C");
 }
 
 int ibg_reg_to_boundary(ibg_context* c, const double* qin, double* fb) {
     if (!c || !qin || !fb) return IBG_ERR_ARG;
-    cudaMemcpyAsync(c->qtmp, qin, sizeof(double) * c->g.F1, cudaMemcpyHostToDevice, c->st);
-    launch_reg_gather(c->g, c->ncomp, c->slots, c->qtmp, c->btmp, c->st);
+    cudaMemcpyAsync(c->b64.qtmp, qin, sizeof(double) * c->g.F1, cudaMemcpyHostToDevice, c->st);
+    launch_reg_gather(c->g, c->ncomp, c->slots, c->b64.qtmp, c->btmp, c->st);
     cudaMemcpyAsync(fb, c->btmp, sizeof(double) * c->ncomp, cudaMemcpyDeviceToHost, c->st);
     return finish(c, "ibg_reg_to_boundary");
 }
@@ -854,12 +928,14 @@ int ibg_reg_to_boundary(ibg_context* c, const double* qin, double* fb) {
 int ibg_projection_solve(ibg_context* c, int k, const double* ain, const double* bin, double* omega, double* fio) {
     if (!c || !ain || !bin || !omega || !fio || k < 0 || k >= c->sch.nsub) return IBG_ERR_ARG;
     if (!c->moving && !c->chol_ready) return c->fail(IBG_ERR_STATE, "ibg_projection_solve: call ibg_init first");
-    cudaMemcpyAsync(c->a, ain, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
+    Bulk<double>& B = c->b64;
+    cudaMemcpyAsync(B.a, ain, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
     cudaMemcpyAsync(c->btmp, bin, sizeof(double) * c->ncomp, cudaMemcpyHostToDevice, c->st);
     cudaMemcpyAsync(c->f, fio, sizeof(double) * c->ncomp, cudaMemcpyHostToDevice, c->st);
-    int s = c->projection(k, c->a, c->btmp);
+    int s = c->projection<double>(B, k, B.a, c->btmp);
     if (s) return s;
-    cudaMemcpyAsync(omega, c->w, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
+    c->state_in_32 = false;
+    cudaMemcpyAsync(omega, B.w, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
     cudaMemcpyAsync(fio, c->f, sizeof(double) * c->ncomp, cudaMemcpyDeviceToHost, c->st);
     return finish(c, "ibg_projection_solve");
 }
@@ -869,9 +945,10 @@ long long ibg_run_kernel(ibg_context* c, int which, int reps) {
     const GridDev& g = c->g;
     long long bytes = 0;
     for (int r = 0; r < reps; ++r) {
-        if (which == 0) c->poisson.run_pass(0, c->w, c->tbuf, c->st);
-        else if (which == 1) c->poisson.run_pass(1, c->tbuf, c->tbuf, c->st);
-        else if (which == 2) launch_nonlinear<double>(g, c->q, c->w, c->U, c->V, c->C, c->Nbuf[0], 1, c->S, c->F, c->st);
+        Bulk<double>& B = c->b64;
+        if (which == 0) B.poisson.run_pass(0, B.w, B.tbuf, c->st);
+        else if (which == 1) B.poisson.run_pass(1, B.tbuf, B.tbuf, c->st);
+        else if (which == 2) launch_nonlinear<double>(g, B.q, B.w, B.U, B.V, B.C, B.Nbuf[0], 1, c->S, c->F, c->st);
         else return IBG_ERR_ARG;
     }
     if (which == 0 || which == 1) bytes = 16LL * (long long)c->S;      // every level read + written once

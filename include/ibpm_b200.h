@@ -54,8 +54,10 @@ typedef struct {
 /* time-stepping schemes (src/Scheme.h:13-61) */
 enum { IBG_SCHEME_EULER = 0, IBG_SCHEME_AB2 = 1, IBG_SCHEME_RK3 = 2, IBG_SCHEME_RK3B = 3 };
 
-/* arithmetic forms of the bulk fields */
-enum { IBG_PRECISION_FP64 = 0, IBG_PRECISION_FP32_REFINED = 1 };
+/* arithmetic forms of the bulk fields: FP64 throughout, or FP32 vorticity,
+ * flux, nonlinear term and transforms with the force solve (M^-1, CG dot
+ * products and norms) and the forces kept in FP64 */
+enum { IBG_PRECISION_FP64 = 0, IBG_PRECISION_FP32_REFINED = 1, IBG_PRECISION_FP32 = 2 };
 
 typedef struct {
     double Re;              /* Reynolds number                                  */
