@@ -273,3 +273,40 @@ def from_workload(wl, precision: str = "fp64", stream=None, device: int = -1):
     if w0 is not None:
         x.omega = w0
     return grid, model, solver, x
+
+
+class Ensemble:
+    """Independent simulations advanced together: one CUDA graph whose branches
+    are the members' time steps (fixed bodies; each member keeps its own grid,
+    Reynolds number, time step and bodies)."""
+
+    def __init__(self, members):
+        self.members = list(members)
+        arr = (ctypes.c_void_p * len(self.members))(*[m.handle.value for m in self.members])
+        h = ctypes.c_void_p()
+        st = lib().ibg_ensemble_create(len(self.members), arr, ctypes.byref(h))
+        if st < 0:
+            raise IbgError(f"ibg_ensemble_create: {lib().ibg_ensemble_last_error(None).decode()}")
+        self._h = h
+
+    def advance(self, nsteps: int = 1):
+        st = lib().ibg_ensemble_advance(self._h, int(nsteps))
+        if st < 0:
+            raise IbgError(f"ibg_ensemble_advance: {lib().ibg_ensemble_last_error(self._h).decode()}")
+
+    def stream(self) -> int:
+        return lib().ibg_ensemble_stream(self._h) or 0
+
+    def launches_per_step(self) -> int:
+        return int(lib().ibg_ensemble_launches_per_step(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ibg_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -68,6 +68,12 @@ SIGNATURES = {
     "ibg_reg_to_boundary": (_I, [_VP, _VP, _VP]),
     "ibg_projection_solve": (_I, [_VP, _I, _VP, _VP, _VP, _VP]),
     "ibg_poisson_solve_static": (_I, [ctypes.POINTER(ibg_grid), _VP, _VP, _VP]),
+    "ibg_ensemble_create": (_I, [_I, ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),
+    "ibg_ensemble_advance": (_I, [_VP, _I]),
+    "ibg_ensemble_destroy": (_I, [_VP]),
+    "ibg_ensemble_stream": (_VP, [_VP]),
+    "ibg_ensemble_launches_per_step": (ctypes.c_longlong, [_VP]),
+    "ibg_ensemble_last_error": (ctypes.c_char_p, [_VP]),
     "ibg_static_last_error": (ctypes.c_char_p, []),
 }
 

@@ -119,14 +119,16 @@ def ensemble_members(count=64, seed=11):
         th = float(rng.uniform(0, math.pi))
         Re = float(rng.uniform(50, 300))
         dx = 4.0 / n
-        # ellipse with semi-axes a = 0.5, b, point spacing ~ dx
-        per = math.pi * (3 * (0.5 + b) - math.sqrt((3 * 0.5 + b) * (0.5 + 3 * b)))
-        npts = max(8, int(round(per / dx)))
-        t = 2 * math.pi * np.arange(npts) / npts
+        # ellipse with semi-axes a = 0.5, b; points equally spaced in arc length, spacing ~ dx
+        t = np.linspace(0.0, 2 * math.pi, 20001)
         ex, ey = 0.5 * np.cos(t), b * np.sin(t)
+        arc = np.concatenate([[0.0], np.cumsum(np.hypot(np.diff(ex), np.diff(ey)))])
+        npts = max(8, int(round(arc[-1] / dx)))
+        ts = np.interp(np.arange(npts) * arc[-1] / npts, arc, t)
+        ex, ey = 0.5 * np.cos(ts), b * np.sin(ts)
         px = ex * math.cos(th) - ey * math.sin(th)
         py = ex * math.sin(th) + ey * math.cos(th)
-        geom = "body Ellipse\n" + "".join(f"  point {x!r} {y!r}\n" for x, y in zip(px, py)) + "end\n"
+        geom = "body Ellipse\n" + "".join(f"  point {float(x)!r} {float(y)!r}\n" for x, y in zip(px, py)) + "end\n"
         out.append(Workload(f"ellipse_{k}", n, n, ngrid, 4.0, -2.0, -2.0, geom, Re=Re, dt=0.5 * dx,
                             nsteps=1000))
     return out

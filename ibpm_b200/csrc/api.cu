@@ -140,6 +140,7 @@ struct ibg_context {
     int* d_hist_count = nullptr;
     long long hist_steps = 0;
     // graph
+    cudaGraph_t graph_def = nullptr;   // the captured step (kept for ensembles)
     cudaGraphExec_t graph = nullptr;
     long long graph_launches = 0;
     long long launches = 0;
@@ -186,6 +187,8 @@ struct ibg_context {
     void release() {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
+        if (graph_def) cudaGraphDestroy(graph_def);
+        graph_def = nullptr;
         b64.release();
         b32.release();
         void* ptrs[] = {d_ref, d_pts, d_vel, d_body_of, d_bodies, slots.idx, slots.w, slots.n, d_b, d_time, f,
@@ -367,6 +370,28 @@ struct ibg_context {
     }
 
     void net_force_record();
+
+    // capture one whole step (all sub-steps) into a graph, once
+    int ensure_graph() {
+        if (graph) return IBG_OK;
+        cudaGraph_t gr;
+        const long long before = launches;
+        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            return cuda_check("capture");
+        int s = enqueue_step();
+        if (cudaStreamEndCapture(st, &gr) != cudaSuccess || s) {
+            launches = before;
+            return s ? s : cuda_check("capture end");
+        }
+        graph_launches = launches - before;
+        launches = before;
+        if (cudaGraphInstantiate(&graph, gr, 0) != cudaSuccess) {
+            cudaGraphDestroy(gr);
+            return cuda_check("instantiate");
+        }
+        graph_def = gr;
+        return IBG_OK;
+    }
 };
 
 namespace ibg {
@@ -768,25 +793,8 @@ int ibg_advance(ibg_context* c, int nsteps) {
     if (c->fp32 && !c->state_in_32) c->to32();
     for (int n = 0; n < nsteps; ++n) {
         if (!c->moving && c->old_saved) {
-            if (!c->graph) {
-                // capture one whole step (all sub-steps) into a graph
-                cudaGraph_t gr;
-                const long long before = c->launches;
-                if (cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-                    return c->cuda_check("ibg_advance: capture");
-                int s = c->enqueue_step();
-                if (cudaStreamEndCapture(c->st, &gr) != cudaSuccess || s) {
-                    c->launches = before;
-                    return s ? s : c->cuda_check("ibg_advance: capture end");
-                }
-                c->graph_launches = c->launches - before;
-                c->launches = before;
-                if (cudaGraphInstantiate(&c->graph, gr, 0) != cudaSuccess) {
-                    cudaGraphDestroy(gr);
-                    return c->cuda_check("ibg_advance: instantiate");
-                }
-                cudaGraphDestroy(gr);
-            }
+            int gs = c->ensure_graph();
+            if (gs) return gs;
             if (cudaGraphLaunch(c->graph, c->st) != cudaSuccess) return c->cuda_check("ibg_advance: graph launch");
             c->launches += c->graph_launches;
         } else {
@@ -939,6 +947,149 @@ int ibg_projection_solve(ibg_context* c, int k, const double* ain, const double*
     cudaMemcpyAsync(fio, c->f, sizeof(double) * c->ncomp, cudaMemcpyDeviceToHost, c->st);
     return finish(c, "ibg_projection_solve");
 }
+
+// ---------------------------------------------------------------------------
+// ensembles: one graph whose independent branches are the members' steps
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+struct ibg_ensemble {
+    std::vector<ibg_context*> members;
+    std::vector<cudaEvent_t> ev;  // one per member: orders member streams and the ensemble stream
+    cudaEvent_t done = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t st = nullptr;
+    long long launches_per_step = 0;
+    std::string err;
+    ~ibg_ensemble() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (cudaEvent_t x : ev) cudaEventDestroy(x);
+        if (done) cudaEventDestroy(done);
+        if (st) cudaStreamDestroy(st);
+    }
+};
+
+namespace {
+thread_local std::string g_ens_error;
+}
+
+extern "C" {
+
+int ibg_ensemble_create(int n, ibg_context* const* members, ibg_ensemble** out) {
+    if (n < 1 || !members || !out) {
+        g_ens_error = "ibg_ensemble_create: no members";
+        return IBG_ERR_ARG;
+    }
+    *out = nullptr;
+    for (int i = 0; i < n; ++i) {
+        ibg_context* c = members[i];
+        if (!c) {
+            g_ens_error = "ibg_ensemble_create: null member";
+            return IBG_ERR_ARG;
+        }
+        if (c->moving) {
+            g_ens_error = "ibg_ensemble_create: members must have fixed bodies (their step is one graph)";
+            return IBG_ERR_UNSUPPORTED;
+        }
+        if (!c->chol_ready) {
+            g_ens_error = "ibg_ensemble_create: call ibg_init (or ibg_load) on every member first";
+            return IBG_ERR_STATE;
+        }
+    }
+    auto* e = new ibg_ensemble();
+    e->members.assign(members, members + n);
+    e->ev.assign(n, nullptr);
+    bool ok = cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaGraphCreate(&e->graph, 0) == cudaSuccess &&
+              cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming) == cudaSuccess;
+    for (int i = 0; i < n && ok; ++i) ok = cudaEventCreateWithFlags(&e->ev[i], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+        g_ens_error = "ibg_ensemble_create: stream or graph creation failed";
+        delete e;
+        return IBG_ERR_CUDA;
+    }
+    *out = e;
+    return IBG_OK;
+}
+
+static int ensemble_build(ibg_ensemble* e) {
+    for (ibg_context* c : e->members) {
+        int s = c->ensure_graph();
+        if (s) {
+            e->err = std::string("member capture: ") + c->err;
+            return s;
+        }
+        cudaStreamSynchronize(c->st);
+        cudaGraphNode_t node;
+        if (cudaGraphAddChildGraphNode(&node, e->graph, nullptr, 0, c->graph_def) != cudaSuccess) {
+            e->err = "ibg_ensemble: adding a member graph failed";
+            return IBG_ERR_CUDA;
+        }
+        e->launches_per_step += c->graph_launches;
+    }
+    if (cudaGraphInstantiate(&e->exec, e->graph, 0) != cudaSuccess) {
+        e->err = "ibg_ensemble: graph instantiation failed";
+        return IBG_ERR_CUDA;
+    }
+    return IBG_OK;
+}
+
+int ibg_ensemble_advance(ibg_ensemble* e, int nsteps) {
+    if (!e || nsteps < 0) return IBG_ERR_ARG;
+    if (!e->exec) {
+        // a member's first step runs on its own (start-up of the N_prev history);
+        // if any member has not stepped yet, every member takes that first step alone
+        bool fresh = false;
+        for (ibg_context* c : e->members) fresh = fresh || !c->old_saved;
+        if (fresh && nsteps > 0) {
+            for (ibg_context* c : e->members) {
+                int s = ibg_advance(c, 1);
+                if (s) {
+                    e->err = std::string("member first step: ") + c->err;
+                    return s;
+                }
+            }
+            --nsteps;
+        }
+        if (fresh && nsteps == 0) return IBG_OK;
+        int s = ensemble_build(e);
+        if (s) return s;
+    }
+    // the ensemble step follows whatever the members' own streams have queued ...
+    for (size_t i = 0; i < e->members.size(); ++i) {
+        cudaEventRecord(e->ev[i], e->members[i]->st);
+        cudaStreamWaitEvent(e->st, e->ev[i], 0);
+    }
+    for (int n = 0; n < nsteps; ++n) {
+        if (cudaGraphLaunch(e->exec, e->st) != cudaSuccess) {
+            e->err = std::string("ibg_ensemble_advance: ") + cudaGetErrorString(cudaGetLastError());
+            return IBG_ERR_CUDA;
+        }
+        for (ibg_context* c : e->members) {
+            c->timestep += 1;
+            c->time += c->prm.dt;
+            c->hist_steps += 1;
+            c->last_launches = c->graph_launches;
+        }
+    }
+    // ... and whatever the members do next follows the ensemble step
+    cudaEventRecord(e->done, e->st);
+    for (ibg_context* c : e->members) cudaStreamWaitEvent(c->st, e->done, 0);
+    return IBG_OK;
+}
+
+int ibg_ensemble_destroy(ibg_ensemble* e) {
+    if (!e) return IBG_ERR_ARG;
+    cudaStreamSynchronize(e->st);
+    delete e;
+    return IBG_OK;
+}
+
+void* ibg_ensemble_stream(const ibg_ensemble* e) { return e ? (void*)e->st : nullptr; }
+long long ibg_ensemble_launches_per_step(const ibg_ensemble* e) { return e ? e->launches_per_step : 0; }
+const char* ibg_ensemble_last_error(const ibg_ensemble* e) { return e ? e->err.c_str() : g_ens_error.c_str(); }
 
 long long ibg_run_kernel(ibg_context* c, int which, int reps) {
     if (!c || reps < 0) return IBG_ERR_ARG;

@@ -127,6 +127,24 @@ IBG_API long long ibg_last_launch_count(const ibg_context* ctx);
  * one launch moves (each operand read once, each result written once). */
 IBG_API long long ibg_run_kernel(ibg_context* ctx, int which, int reps);
 
+/* --- ensembles ------------------------------------------------------------------
+ * No single reference interface: an ensemble of independent simulations, each an
+ * ibg_context with fixed bodies and its own grid, Reynolds number, time step and
+ * bodies (the reference would run one `ibpm` process per member).  The members'
+ * captured step graphs become independent branches of one CUDA graph, so one
+ * graph launch advances every member by one step and their kernels overlap on
+ * the GPU.  Members keep their own state (ibg_get_state, ibg_get_force_history).
+ * The first ibg_ensemble_advance captures the members' graphs; if any member has
+ * not stepped yet, the first of its steps runs member by member (the start-up of
+ * the previous-nonlinear-term history) and the rest as ensemble graphs. */
+typedef struct ibg_ensemble ibg_ensemble;
+IBG_API int ibg_ensemble_create(int n, ibg_context* const* members, ibg_ensemble** out);
+IBG_API int ibg_ensemble_advance(ibg_ensemble* ens, int nsteps);
+IBG_API int ibg_ensemble_destroy(ibg_ensemble* ens);
+IBG_API void* ibg_ensemble_stream(const ibg_ensemble* ens);
+IBG_API long long ibg_ensemble_launches_per_step(const ibg_ensemble* ens);
+IBG_API const char* ibg_ensemble_last_error(const ibg_ensemble* ens);
+
 /* --- operator entry points (host buffers, reference layouts) ----------------- */
 /* PoissonSolver::solve (src/EllipticSolver.cc:47-73, :83-94): L u = f on all levels */
 IBG_API int ibg_poisson_solve(ibg_context* ctx, const double* f, double* u);

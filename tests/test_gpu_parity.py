@@ -213,3 +213,41 @@ def test_fp32_form_within_force_and_vorticity_bars(name):
     assert rel_l2(forces, d["forces"][:, 2:4]) < 3e-4
     assert rel_l2(x.omega, d["omega"]) < 1e-5
     s.close()
+
+
+def test_ensemble_matches_members_stepped_alone():
+    """Members advanced by one ensemble graph give the same forces and
+    vorticity as the same members advanced one by one."""
+    import ibpm_b200 as ib
+    from ibpm_b200 import configs
+    specs = [(32, 32, 2, 3.0, -1.5, -1.5, 24, 0.4, 150.0, 0.02), (48, 48, 1, 4.0, -2.0, -2.0, 36, 0.5, 100.0, 0.02),
+             (64, 32, 3, 4.0, -1.5, -1.0, 32, 0.4, 200.0, 0.01)]
+
+    def make():
+        out = []
+        for (nx, ny, L, length, xo, yo, npts, r, Re, dt) in specs:
+            grid = ib.Grid(nx, ny, L, length, xo, yo)
+            geo = ib.geometry.parse(configs.cylinder_geom(npts, r=r))
+            s = ib.NonlinearIBSolver(grid, ib.NavierStokesModel(grid, geo, Re), dt, "rk3")
+            s.init()
+            s.set_state(ib.State(grid, geo.num_points), with_q=False)
+            out.append((s, grid, geo))
+        return out
+
+    nsteps = 5
+    alone = make()
+    for s, _, _ in alone:
+        s.advance_resident(nsteps)
+    together = make()
+    ens = ib.Ensemble([s for s, _, _ in together])
+    ens.advance(nsteps)
+    for (sa, grid, geo), (sb, _, _) in zip(alone, together):
+        fa, fb = sa.force_history(nsteps), sb.force_history(nsteps)
+        assert rel_l2(fb, fa) < 1e-12
+        xa, xb = ib.State(grid, geo.num_points), ib.State(grid, geo.num_points)
+        sa.get_state(xa)
+        sb.get_state(xb)
+        assert rel_l2(xb.omega, xa.omega) < 1e-12
+    ens.close()
+    for s, _, _ in alone + together:
+        s.close()
