@@ -22,7 +22,7 @@ from typing import Optional
 import numpy as np
 
 from . import geometry as _geometry
-from ._native import (PRECISIONS, SCHEMES, IbgError, check, ibg_body, ibg_grid, ibg_params, lib)
+from ._native import (PRECISIONS, PRECONDS, SCHEMES, IbgError, check, ibg_body, ibg_grid, ibg_params, lib)
 
 __all__ = ["Grid", "State", "NavierStokesModel", "NonlinearIBSolver", "IbgError", "geometry"]
 geometry = _geometry
@@ -114,7 +114,7 @@ class NonlinearIBSolver:
 
     def __init__(self, grid: Grid, model: NavierStokesModel, dt: float, scheme: str = "rk3", tol: float = 1e-7,
                  precision: str = "fp64", stream: Optional[int] = None, cg_max_iter: int = 3000,
-                 device: int = -1):
+                 device: int = -1, precond: str = "none", pc_refresh: int = 10):
         self.grid, self.model, self.dt = grid, model, dt
         self.scheme = scheme
         L = lib()
@@ -131,7 +131,7 @@ class NonlinearIBSolver:
             for j in range(6):
                 bodies[k].params[j] = b.params[j] if j < len(b.params) else 0.0
         p = ibg_params(model.Re, dt, SCHEMES[scheme], tol, cg_max_iter, model.u_mag, model.alpha,
-                       PRECISIONS[precision], device)
+                       PRECISIONS[precision], device, PRECONDS[precond], pc_refresh)
         h = ctypes.c_void_p()
         check(L.ibg_create(ctypes.byref(g), len(model.geom.bodies), bodies, ctypes.byref(p),
                            ctypes.c_void_p(stream) if stream else None, ctypes.byref(h)), None)
@@ -212,6 +212,11 @@ class NonlinearIBSolver:
         check(lib().ibg_get_net_force(self._h, ctypes.byref(a), ctypes.byref(b)), self._h)
         return a.value, b.value
 
+    def cg_totals(self):
+        it, n = ctypes.c_longlong(), ctypes.c_longlong()
+        check(lib().ibg_cg_totals(self._h, ctypes.byref(it), ctypes.byref(n)), self._h)
+        return it.value, n.value
+
     def cg_stats(self):
         a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         check(lib().ibg_cg_stats(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)), self._h)
@@ -261,13 +266,14 @@ class NonlinearIBSolver:
         return w, f
 
 
-def from_workload(wl, precision: str = "fp64", stream=None, device: int = -1):
+def from_workload(wl, precision: str = "fp64", stream=None, device: int = -1, precond: str = "none",
+                  pc_refresh: int = 10):
     """Grid, model, solver and initial State for an ibpm_b200.configs.Workload."""
     grid = Grid(wl.nx, wl.ny, wl.ngrid, wl.length, wl.xoffset, wl.yoffset)
     geo = _geometry.parse(wl.geom)
     model = NavierStokesModel(grid, geo, wl.Re)
     solver = NonlinearIBSolver(grid, model, wl.dt, wl.scheme, wl.tol, precision=precision, stream=stream,
-                               device=device)
+                               device=device, precond=precond, pc_refresh=pc_refresh)
     x = State(grid, geo.num_points)
     w0 = wl.initial_vorticity()
     if w0 is not None:

@@ -27,11 +27,13 @@ class ibg_body(ctypes.Structure):
 class ibg_params(ctypes.Structure):
     _fields_ = [("Re", ctypes.c_double), ("dt", ctypes.c_double), ("scheme", ctypes.c_int),
                 ("cg_tol", ctypes.c_double), ("cg_max_iter", ctypes.c_int), ("u_mag", ctypes.c_double),
-                ("alpha", ctypes.c_double), ("precision", ctypes.c_int), ("device", ctypes.c_int)]
+                ("alpha", ctypes.c_double), ("precision", ctypes.c_int), ("device", ctypes.c_int),
+                ("cg_precond", ctypes.c_int), ("pc_refresh", ctypes.c_int)]
 
 
 SCHEMES = {"euler": 0, "ab2": 1, "rk3": 2, "rk3b": 3}
 PRECISIONS = {"fp64": 0, "fp32_refined": 1, "fp32": 2}
+PRECONDS = {"none": 0, "cholesky": 1, "learned": 2}
 
 # every entry point declared in include/ibpm_b200.h: name -> (restype, argtypes)
 _VP = ctypes.c_void_p
@@ -56,6 +58,7 @@ SIGNATURES = {
     "ibg_sizes": (_I, [_VP, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
                        ctypes.POINTER(_I)]),
     "ibg_cg_stats": (_I, [_VP, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    "ibg_cg_totals": (_I, [_VP, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
     "ibg_stream": (_VP, [_VP]),
     "ibg_last_launch_count": (ctypes.c_longlong, [_VP]),
     "ibg_run_kernel": (ctypes.c_longlong, [_VP, _I, _I]),

@@ -132,9 +132,12 @@ struct ibg_context {
     int* d_status = nullptr;
     // CG
     double *cg_r = nullptr, *cg_d = nullptr, *cg_q = nullptr, *cg_scal = nullptr;
+    double *cg_z = nullptr, *cg_zold = nullptr;
     int* cg_flags = nullptr;
     int* h_flags = nullptr;  // pinned
     int cg_last = 0, cg_max = 0, cg_capped = 0;
+    long long cg_total = 0, cg_solves = 0;
+    int steps_since_pc = 0;
     // force history
     double* d_hist = nullptr;
     int* d_hist_count = nullptr;
@@ -191,8 +194,9 @@ struct ibg_context {
         graph_def = nullptr;
         b64.release();
         b32.release();
+        release_build_scratch();
         void* ptrs[] = {d_ref, d_pts, d_vel, d_body_of, d_bodies, slots.idx, slots.w, slots.n, d_b, d_time, f,
-                        flux0, rhsb, btmp, d_status, cg_r, cg_d, cg_q, cg_scal, cg_flags, d_hist, d_hist_count};
+                        flux0, rhsb, btmp, d_status, cg_r, cg_d, cg_q, cg_scal, cg_flags, d_hist, d_hist_count, cg_z, cg_zold};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         for (int k = 0; k < 4; ++k) {
@@ -214,7 +218,7 @@ struct ibg_context {
         slots = RegSlots{};
         d_b = d_time = f = flux0 = rhsb = btmp = nullptr;
         d_status = nullptr;
-        cg_r = cg_d = cg_q = cg_scal = nullptr;
+        cg_r = cg_d = cg_q = cg_scal = cg_z = cg_zold = nullptr;
         cg_flags = nullptr;
         d_hist = nullptr;
         d_hist_count = nullptr;
@@ -255,6 +259,7 @@ struct ibg_context {
     // convergence flag every `chunk` iterations.
     template <typename T>
     int cg_solve(Bulk<T>& B, int k, const double* b, double* x) {
+        if (prm.cg_precond != IBG_PRECOND_NONE) return pcg_solve<T>(B, k, b, x);
         m_apply<T>(B, k, x, cg_q);
         cg_begin(ncomp, b, cg_q, cg_r, cg_d, cg_scal, cg_flags, st);
         launches += 1;
@@ -276,6 +281,53 @@ struct ibg_context {
         cg_last = h_flags[1];
         if (cg_last > cg_max) cg_max = cg_last;
         if (cg_last >= prm.cg_max_iter) ++cg_capped;
+        cg_total += cg_last;
+        ++cg_solves;
+        return IBG_OK;
+    }
+
+    // z = P r
+    void precondition(int k, const double* r, double* z) {
+        if (prm.cg_precond == IBG_PRECOND_CHOLESKY) {
+            minv_apply(ncomp, Mi[k], r, z, st);
+        } else {
+            apply_learned_precond(r, z);
+        }
+        launches += 1;
+    }
+    void apply_learned_precond(const double* r, double* z);
+
+    // flexible preconditioned CG (Polak-Ribiere beta, so a preconditioner that
+    // changes between iterations is allowed); same absolute test r.r <= tol^2
+    template <typename T>
+    int pcg_solve(Bulk<T>& B, int k, const double* b, double* x) {
+        m_apply<T>(B, k, x, cg_q);
+        pcg_begin(ncomp, b, cg_q, cg_r, cg_scal, cg_flags, st);
+        precondition(k, cg_r, cg_z);
+        pcg_begin2(ncomp, cg_r, cg_z, cg_d, cg_scal, cg_flags, st);
+        launches += 2;
+        int chunk = cg_last > 1 ? cg_last : 1;
+        int done_iters = 0;
+        for (;;) {
+            for (int c = 0; c < chunk; ++c) {
+                m_apply<T>(B, k, cg_d, cg_q);
+                pcg_step1(ncomp, x, cg_r, cg_d, cg_q, cg_z, cg_zold, cg_scal, cg_flags, st);
+                precondition(k, cg_r, cg_z);
+                pcg_step2(ncomp, cg_r, cg_z, cg_zold, cg_d, cg_scal, cg_flags, st);
+                launches += 2;
+            }
+            done_iters += chunk;
+            cudaMemcpyAsync(h_flags, cg_flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st);
+            if (cudaStreamSynchronize(st) != cudaSuccess) return cuda_check("pcg");
+            if (h_flags[0] == 0) break;
+            if (done_iters > prm.cg_max_iter + chunk) break;
+            chunk = 2;
+        }
+        cg_last = h_flags[1];
+        if (cg_last > cg_max) cg_max = cg_last;
+        if (cg_last >= prm.cg_max_iter) ++cg_capped;
+        cg_total += cg_last;
+        ++cg_solves;
         return IBG_OK;
     }
 
@@ -371,6 +423,70 @@ struct ibg_context {
 
     void net_force_record();
 
+    // ---- explicit force operator M = C A^-1 B at the current body configuration
+    // (src/CholeskySolver.cc:49-111): columns M e_j for a chunk of j at once
+    // (batched solves), Cholesky factor, explicit inverse; one per sub-step.
+    double *bs_bf = nullptr, *bs_u = nullptr, *bs_p = nullptr, *bs_rc = nullptr, *bs_tb = nullptr;
+    double *bs_fl = nullptr, *bs_sw = nullptr, *bs_M = nullptr;
+    size_t bs_chunk = 0;
+    void release_build_scratch() {
+        double* p[] = {bs_bf, bs_u, bs_p, bs_rc, bs_tb, bs_fl, bs_sw, bs_M};
+        for (double* x : p)
+            if (x) cudaFree(x);
+        bs_bf = bs_u = bs_p = bs_rc = bs_tb = bs_fl = bs_sw = bs_M = nullptr;
+        bs_chunk = 0;
+    }
+    int build_operator() {
+        const int m = ncomp;
+        const size_t swd = sweep_doubles(g.nx, g.ny, g.L);
+        if (!bs_M) {
+            // chunk so that the batched scratch stays below ~8 GB
+            const size_t per_col = sizeof(double) * (5 * S + (size_t)g.F1 + swd);
+            size_t chunk = ((size_t)8 << 30) / per_col;
+            if (chunk < 1) chunk = 1;
+            if (chunk > (size_t)m) chunk = m;
+            if (chunk > 65535) chunk = 65535;
+            int s = alloc(&bs_bf, chunk * S) || alloc(&bs_u, chunk * S) || alloc(&bs_p, chunk * S) ||
+                    alloc(&bs_rc, chunk * S) || alloc(&bs_tb, chunk * S) || alloc(&bs_fl, chunk * g.F1) ||
+                    alloc(&bs_sw, chunk * swd) || alloc(&bs_M, (size_t)m * m, false);
+            if (s) {
+                release_build_scratch();
+                return fail(IBG_ERR_CUDA, "not enough device memory for the force-operator build");
+            }
+            bs_chunk = chunk;
+        }
+        for (int k = 0; k < sch.nsub; ++k)
+            if (!Lr[k] && (alloc(&Lr[k], (size_t)m * m, false) || alloc(&Lc[k], (size_t)m * m, false) ||
+                           alloc(&Ld[k], (size_t)m, false) || alloc(&Mi[k], (size_t)m * m, false)))
+                return fail(IBG_ERR_CUDA, "not enough device memory for the Cholesky factors");
+        const size_t chunk = bs_chunk;
+        int s = IBG_OK;
+        for (int k = 0; k < sch.nsub && !s; ++k) {
+            for (int col0 = 0; col0 < m; col0 += (int)chunk) {
+                const int nb = (int)std::min(chunk, (size_t)(m - col0));
+                launch_smear_bf_unit<double>(g, m, col0, nb, slots, bs_fl, g.F1, bs_bf, S, beta[k], st);
+                SolveCall<double> h{};
+                h.f = bs_bf; h.u = bs_u; h.rc = bs_rc; h.tbuf = bs_tb; h.sweep = bs_sw; h.bstride = S;
+                h.batch = nb; h.in_scale = 1.0;
+                b64.helm[k].solve(h, st);
+                SolveCall<double> pc{};
+                pc.f = bs_u; pc.u = bs_p; pc.rc = bs_rc; pc.tbuf = bs_tb; pc.sweep = bs_sw; pc.bstride = S;
+                pc.batch = nb; pc.in_scale = -1.0;
+                b64.poisson.solve(pc, st);
+                launch_reg_interp<double>(g, m, slots, bs_p, S, nb, nullptr, bs_M + (size_t)col0 * m, (size_t)m, st);
+            }
+            s = chol_factor(m, bs_M, Lr[k], Lc[k], Ld[k], d_status, st);
+            if (!s) chol_inverse(m, Lr[k], Lc[k], Ld[k], Mi[k], st);
+            int hs = 0;
+            cudaMemcpyAsync(&hs, d_status, sizeof(int), cudaMemcpyDeviceToHost, st);
+            if (cudaStreamSynchronize(st) != cudaSuccess) s = cuda_check("force operator build");
+            if (!s && hs) s = fail(IBG_ERR_NUMERIC, "matrix M is not positive definite");
+        }
+        if (s) return s;
+        chol_ready = true;
+        return cuda_check("force operator build");
+    }
+
     // capture one whole step (all sub-steps) into a graph, once
     int ensure_graph() {
         if (graph) return IBG_OK;
@@ -415,6 +531,11 @@ __global__ void k_hist_force(int npts, const double* f, double dx2, double* hist
 }
 }  // namespace ibg
 
+void ibg_context::apply_learned_precond(const double* r, double* z) {
+    // until a network is loaded the learned preconditioner is the identity (plain CG directions)
+    cudaMemcpyAsync(z, r, sizeof(double) * ncomp, cudaMemcpyDeviceToDevice, st);
+}
+
 void ibg_context::net_force_record() {
     ibg::k_hist_force<<<1, 32, 0, st>>>(npts, f, g.dx * g.dx, d_hist, d_hist_count);
 }
@@ -441,8 +562,10 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
         g_create_error = "ibg_create: invalid grid";
         return IBG_ERR_ARG;
     }
-    if (G.ngrid > 1 && (G.nx % 4 || G.ny % 4)) {
-        g_create_error = "ibg_create: nx and ny must be multiples of 4 when ngrid > 1";
+    // the reference asserts multiples of 4 only in debug builds (src/Grid.cc:72); its
+    // release build nests with integer division, which the kernels reproduce for even sizes
+    if (G.ngrid > 1 && (G.nx % 2 || G.ny % 2)) {
+        g_create_error = "ibg_create: nx and ny must be even when ngrid > 1";
         return IBG_ERR_ARG;
     }
     Scheme sch = make_scheme(params->scheme);
@@ -469,6 +592,12 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
     auto* c = new ibg_context();
     c->prm = *params;
     if (c->prm.cg_max_iter <= 0) c->prm.cg_max_iter = 3000;
+    if (c->prm.pc_refresh <= 0) c->prm.pc_refresh = 10;
+    if (c->prm.cg_precond < IBG_PRECOND_NONE || c->prm.cg_precond > IBG_PRECOND_LEARNED) {
+        delete c;
+        g_create_error = "ibg_create: unknown preconditioner";
+        return IBG_ERR_ARG;
+    }
     if (!(c->prm.cg_tol > 0)) c->prm.cg_tol = 1e-7;
     c->sch = sch;
     GridDev& g = c->g;
@@ -561,7 +690,7 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
         c->alloc(&c->d_body_of, (size_t)c->npts) || c->alloc(&c->d_bodies, c->h_bodies.size()) ||
         c->alloc(&c->slots.idx, kSlots * m) || c->alloc(&c->slots.w, kSlots * m) || c->alloc(&c->slots.n, m) ||
         c->alloc(&c->d_b, m) || c->alloc(&c->d_time, 1) || c->alloc(&c->d_status, 1) || c->alloc(&c->cg_r, m) ||
-        c->alloc(&c->cg_d, m) || c->alloc(&c->cg_q, m) || c->alloc(&c->cg_scal, 4) || c->alloc(&c->cg_flags, 4) ||
+        c->alloc(&c->cg_d, m) || c->alloc(&c->cg_q, m) || c->alloc(&c->cg_z, m) || c->alloc(&c->cg_zold, m) || c->alloc(&c->cg_scal, 4) || c->alloc(&c->cg_flags, 4) ||
         c->alloc(&c->d_hist, 2 * (size_t)kHistCap) || c->alloc(&c->d_hist_count, 1);
     if (!s && cudaMallocHost((void**)&c->h_flags, 4 * sizeof(int)) != cudaSuccess) s = IBG_ERR_CUDA;
     if (s) {
@@ -602,59 +731,15 @@ int ibg_destroy(ibg_context* ctx) {
 // Cholesky build: columns M e_j for a chunk of j at once (batched solves).
 int ibg_init(ibg_context* c) {
     if (!c) return IBG_ERR_ARG;
-    if (c->moving) return IBG_OK;
+    if (c->moving) {
+        if (c->prm.cg_precond == IBG_PRECOND_CHOLESKY) return c->build_operator();
+        return IBG_OK;
+    }
     if (c->chol_ready) return IBG_OK;
-    const GridDev& g = c->g;
-    const int m = c->ncomp;
-    const size_t S = c->S;
-    // chunk so that the batched scratch stays below ~8 GB
-    const size_t swd = sweep_doubles(g.nx, g.ny, g.L);
-    const size_t per_col = sizeof(double) * (5 * S + (size_t)g.F1 + swd);
-    size_t chunk = (size_t)8 << 30;
-    chunk /= per_col;
-    if (chunk < 1) chunk = 1;
-    if (chunk > (size_t)m) chunk = m;
-    if (chunk > 65535) chunk = 65535;
-    double *bf = nullptr, *u = nullptr, *p = nullptr, *rcb = nullptr, *tb = nullptr, *fl = nullptr, *Mcol = nullptr;
-    double* swb = nullptr;
-    int s = c->alloc(&bf, chunk * S) || c->alloc(&u, chunk * S) || c->alloc(&p, chunk * S) ||
-            c->alloc(&rcb, chunk * S) || c->alloc(&tb, chunk * S) || c->alloc(&fl, chunk * g.F1) ||
-            c->alloc(&swb, chunk * swd) || c->alloc(&Mcol, (size_t)m * m, false);
-    for (int k = 0; k < c->sch.nsub && !s; ++k)
-        s = c->alloc(&c->Lr[k], (size_t)m * m, false) || c->alloc(&c->Lc[k], (size_t)m * m, false) ||
-            c->alloc(&c->Ld[k], (size_t)m, false) || c->alloc(&c->Mi[k], (size_t)m * m, false);
-    if (s) {
-        cudaFree(bf); cudaFree(u); cudaFree(p); cudaFree(rcb); cudaFree(tb); cudaFree(fl); cudaFree(Mcol);
-        cudaFree(swb);
-        return c->fail(IBG_ERR_CUDA, "ibg_init: not enough device memory for the Cholesky build");
-    }
-    for (int k = 0; k < c->sch.nsub && !s; ++k) {
-        for (int col0 = 0; col0 < m; col0 += (int)chunk) {
-            const int nb = (int)std::min(chunk, (size_t)(m - col0));
-            launch_smear_bf_unit<double>(g, m, col0, nb, c->slots, fl, g.F1, bf, S, c->beta[k], c->st);
-            SolveCall<double> h{};
-            h.f = bf; h.u = u; h.rc = rcb; h.tbuf = tb; h.sweep = swb; h.bstride = S;
-            h.batch = nb; h.in_scale = 1.0;
-            c->b64.helm[k].solve(h, c->st);
-            SolveCall<double> pc{};
-            pc.f = u; pc.u = p; pc.rc = rcb; pc.tbuf = tb; pc.sweep = swb; pc.bstride = S;
-            pc.batch = nb;
-            pc.in_scale = -1.0;
-            c->b64.poisson.solve(pc, c->st);
-            launch_reg_interp<double>(g, m, c->slots, p, S, nb, nullptr, Mcol + (size_t)col0 * m, (size_t)m, c->st);
-        }
-        s = chol_factor(m, Mcol, c->Lr[k], c->Lc[k], c->Ld[k], c->d_status, c->st);
-        if (!s) chol_inverse(m, c->Lr[k], c->Lc[k], c->Ld[k], c->Mi[k], c->st);
-        int hs = 0;
-        cudaMemcpyAsync(&hs, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->st);
-        if (cudaStreamSynchronize(c->st) != cudaSuccess) s = c->cuda_check("ibg_init");
-        if (!s && hs) s = c->fail(IBG_ERR_NUMERIC, "ibg_init: matrix M is not positive definite");
-    }
-    cudaFree(bf); cudaFree(u); cudaFree(p); cudaFree(rcb); cudaFree(tb); cudaFree(fl); cudaFree(Mcol);
-    cudaFree(swb);
+    int s = c->build_operator();
     if (s) return s;
-    c->chol_ready = true;
-    return c->cuda_check("ibg_init");
+    c->release_build_scratch();
+    return IBG_OK;
 }
 
 int ibg_save(ibg_context* c, const char* basename) {
@@ -792,6 +877,14 @@ int ibg_advance(ibg_context* c, int nsteps) {
     const long long l0 = c->launches;
     if (c->fp32 && !c->state_in_32) c->to32();
     for (int n = 0; n < nsteps; ++n) {
+        if (c->moving && c->prm.cg_precond == IBG_PRECOND_CHOLESKY &&
+            (!c->chol_ready || c->steps_since_pc >= c->prm.pc_refresh)) {
+            // rebuild the preconditioner at the current body configuration
+            int s = c->build_operator();
+            if (s) return s;
+            c->steps_since_pc = 0;
+        }
+        ++c->steps_since_pc;
         if (!c->moving && c->old_saved) {
             int gs = c->ensure_graph();
             if (gs) return gs;
@@ -846,6 +939,13 @@ int ibg_sizes(const ibg_context* c, long long* ns, long long* nf, int* nb) {
     if (ns) *ns = (long long)c->S;
     if (nf) *nf = (long long)c->F;
     if (nb) *nb = c->ncomp;
+    return IBG_OK;
+}
+
+int ibg_cg_totals(const ibg_context* c, long long* iterations, long long* solves) {
+    if (!c) return IBG_ERR_ARG;
+    if (iterations) *iterations = c->cg_total;
+    if (solves) *solves = c->cg_solves;
     return IBG_OK;
 }
 

@@ -220,6 +220,89 @@ __global__ void __launch_bounds__(1024) k_cg_update(int m, double* __restrict__ 
     }
 }
 
+// ---------------------------------------------------------------------------
+// flexible preconditioned CG (one CTA per update).  scal: [0] r.z, [2] tol^2,
+// [3] r.r; flags: [0] active, [1] iterations, [2] max iterations
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_pcg_begin(int m, const double* __restrict__ b, const double* __restrict__ Mx,
+                                                    double* __restrict__ r, double* __restrict__ scal,
+                                                    int* __restrict__ flags) {
+    __shared__ double red[32];
+    double part = 0.0;
+    for (int k = threadIdx.x; k < m; k += blockDim.x) {
+        const double rv = b[k] - Mx[k];
+        r[k] = rv;
+        part += rv * rv;
+    }
+    const double rr = block_sum(part, red);
+    if (threadIdx.x == 0) {
+        scal[3] = rr;
+        flags[1] = 0;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_pcg_begin2(int m, const double* __restrict__ r, const double* __restrict__ z,
+                                                     double* __restrict__ d, double* __restrict__ scal,
+                                                     int* __restrict__ flags) {
+    __shared__ double red[32];
+    double part = 0.0;
+    for (int k = threadIdx.x; k < m; k += blockDim.x) {
+        d[k] = z[k];
+        part += r[k] * z[k];
+    }
+    const double rz = block_sum(part, red);
+    if (threadIdx.x == 0) {
+        scal[0] = rz;
+        flags[0] = (scal[3] > scal[2] && flags[2] > 0 && rz > 0.0) ? 1 : 0;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_pcg_step1(int m, double* __restrict__ x, double* __restrict__ r,
+                                                    const double* __restrict__ d, const double* __restrict__ q,
+                                                    const double* __restrict__ z, double* __restrict__ zold,
+                                                    double* __restrict__ scal, int* __restrict__ flags) {
+    __shared__ double red[32];
+    if (flags[0] == 0) return;
+    double part = 0.0;
+    for (int k = threadIdx.x; k < m; k += blockDim.x) part += d[k] * q[k];
+    const double dq = block_sum(part, red);
+    const double alpha = scal[0] / dq;
+    part = 0.0;
+    for (int k = threadIdx.x; k < m; k += blockDim.x) {
+        x[k] = x[k] + alpha * d[k];
+        const double rv = r[k] - alpha * q[k];
+        r[k] = rv;
+        zold[k] = z[k];
+        part += rv * rv;
+    }
+    const double rr = block_sum(part, red);
+    if (threadIdx.x == 0) scal[3] = rr;
+}
+
+__global__ void __launch_bounds__(1024) k_pcg_step2(int m, const double* __restrict__ r, const double* __restrict__ z,
+                                                    const double* __restrict__ zold, double* __restrict__ d,
+                                                    double* __restrict__ scal, int* __restrict__ flags) {
+    __shared__ double red[32];
+    if (flags[0] == 0) return;
+    double p1 = 0.0, p2 = 0.0;
+    for (int k = threadIdx.x; k < m; k += blockDim.x) {
+        p1 += r[k] * z[k];
+        p2 += r[k] * zold[k];
+    }
+    const double rz = block_sum(p1, red);
+    const double rzo = block_sum(p2, red);
+    const double beta = (rz - rzo) / scal[0];  // Polak-Ribiere
+    for (int k = threadIdx.x; k < m; k += blockDim.x) d[k] = z[k] + beta * d[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        scal[0] = rz;
+        const int it = flags[1] + 1;
+        flags[1] = it;
+        const double rr = scal[3];
+        flags[0] = (rr > scal[2] && it < flags[2] && rz > 0.0 && rr == rr) ? 1 : 0;
+    }
+}
+
 // net force sum(f) dx^2 in each direction, appended to a history buffer
 __global__ void k_net_force(int npts, const double* __restrict__ f, double dx2, double* __restrict__ out) {
     double sx = 0.0, sy = 0.0;
@@ -282,6 +365,21 @@ void cg_begin(int m, const double* b, const double* Mx, double* r, double* d, do
 
 void cg_update(int m, double* x, double* r, double* d, const double* q, double* scal, int* flags, cudaStream_t st) {
     k_cg_update<<<1, 1024, 0, st>>>(m, x, r, d, q, scal, flags);
+}
+
+void pcg_begin(int m, const double* b, const double* Mx, double* r, double* scal, int* flags, cudaStream_t st) {
+    k_pcg_begin<<<1, 1024, 0, st>>>(m, b, Mx, r, scal, flags);
+}
+void pcg_begin2(int m, const double* r, const double* z, double* d, double* scal, int* flags, cudaStream_t st) {
+    k_pcg_begin2<<<1, 1024, 0, st>>>(m, r, z, d, scal, flags);
+}
+void pcg_step1(int m, double* x, double* r, const double* d, const double* q, const double* z, double* zold,
+               double* scal, int* flags, cudaStream_t st) {
+    k_pcg_step1<<<1, 1024, 0, st>>>(m, x, r, d, q, z, zold, scal, flags);
+}
+void pcg_step2(int m, const double* r, const double* z, const double* zold, double* d, double* scal, int* flags,
+               cudaStream_t st) {
+    k_pcg_step2<<<1, 1024, 0, st>>>(m, r, z, zold, d, scal, flags);
 }
 
 void net_force(int npts, const double* f, double dx2, double* out, cudaStream_t st) {

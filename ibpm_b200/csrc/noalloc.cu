@@ -65,8 +65,8 @@ extern "C" int ibg_poisson_solve_static(const ibg_grid* grid, const double* f, d
     const int nx = grid->nx, ny = grid->ny, L = grid->ngrid;
     if (nx < 4 || ny < 4 || L < 1 || L > 16 || !(grid->length > 0))
         return fail(IBG_ERR_ARG, "ibg_poisson_solve_static: invalid grid");
-    if (L > 1 && (nx % 4 || ny % 4))
-        return fail(IBG_ERR_ARG, "ibg_poisson_solve_static: nx and ny must be multiples of 4 when ngrid > 1");
+    if (L > 1 && (nx % 2 || ny % 2))
+        return fail(IBG_ERR_ARG, "ibg_poisson_solve_static: nx and ny must be even when ngrid > 1");
     if (nx > kStaticMaxN || ny > kStaticMaxN)
         return fail(IBG_ERR_UNSUPPORTED, "ibg_poisson_solve_static: nx and ny must be <= 2048 (static tables)");
     const size_t N1 = (size_t)(nx - 1) * (ny - 1);

@@ -69,7 +69,15 @@ typedef struct {
     double alpha;           /* base-flow angle in radians                       */
     int precision;          /* IBG_PRECISION_*                                  */
     int device;             /* CUDA device ordinal, -1 = the calling thread's current device */
+    int cg_precond;         /* moving bodies: IBG_PRECOND_* (NONE = the reference's plain CG) */
+    int pc_refresh;         /* steps between rebuilds of the Cholesky preconditioner (default 10) */
 } ibg_params;
+
+/* preconditioners of the moving-body force solve (all keep the reference's
+ * absolute test r.r <= tol^2; NONE is the reference's CG exactly):
+ * CHOLESKY: the exact M^-1 of the body configuration at the last rebuild,
+ * LEARNED: the boundary-point network (flexible CG, plain-CG fallback) */
+enum { IBG_PRECOND_NONE = 0, IBG_PRECOND_CHOLESKY = 1, IBG_PRECOND_LEARNED = 2 };
 
 /* --- lifetime ---------------------------------------------------------------
  * ibg_create replaces the constructors NavierStokesModel(grid, geom, Re, q0)
@@ -116,6 +124,8 @@ IBG_API int ibg_sizes(const ibg_context* ctx, long long* n_scalar, long long* n_
 /* CG statistics of the last advance: iterations of the last sub-step solve,
  * the largest count seen and how many solves hit the cap */
 IBG_API int ibg_cg_stats(const ibg_context* ctx, int* last_iterations, int* max_iterations, int* capped_solves);
+/* total CG iterations and CG solves since ibg_create */
+IBG_API int ibg_cg_totals(const ibg_context* ctx, long long* iterations, long long* solves);
 /* the CUDA stream the context launches on (a cudaStream_t) */
 IBG_API void* ibg_stream(const ibg_context* ctx);
 /* number of kernel launches issued by the last ibg_advance call */

@@ -47,8 +47,10 @@ class Grid:
     yshift: float = 0.0
 
     def __post_init__(self):
-        if self.ngrid > 1 and (self.nx % 4 or self.ny % 4):
-            raise ValueError("nx and ny must be multiples of 4 when ngrid > 1 (src/Grid.cc:72)")
+        # src/Grid.cc:72 asserts multiples of 4 in debug builds only; the release build
+        # (-DNDEBUG) nests with integer division, restated here for even sizes
+        if self.ngrid > 1 and (self.nx % 2 or self.ny % 2):
+            raise ValueError("nx and ny must be even when ngrid > 1")
 
     @property
     def dx(self) -> float:

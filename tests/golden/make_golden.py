@@ -34,6 +34,11 @@ CASES = [
     ("plate_l2_pitchplunge_cg", 64, 32, 2, 4.0, -2.0, -1.0,
      configs.plate_geom(chord=1.0, npts=17, freq=0.5), 300.0, 0.01, 6, "rk3", 1e-10, None),
     ("cyl_l1_rk3b", 40, 40, 1, 4.0, -2.0, -2.0, configs.cylinder_geom(30), 80.0, 0.02, 5, "rk3b", 1e-7, None),
+    # ny = 2 (mod 4) with several domains, as in the 500x250 plate workload (release-build nesting)
+    ("cyl_l3_ny2mod4", 48, 26, 3, 4.8, -2.0, -1.3, configs.cylinder_geom(18, r=0.3), 120.0, 0.02, 5, "rk3",
+     1e-7, (1e-3, 5)),
+    ("plate_l3_ny2mod4_cg", 60, 30, 3, 6.0, -3.0, -1.5,
+     configs.plate_geom(chord=1.0, npts=11, freq=0.5), 300.0, 0.01, 4, "rk3", 1e-10, None),
 ]
 
 
@@ -72,5 +77,7 @@ def run(case):
 
 
 if __name__ == "__main__":
+    only = set(sys.argv[1:])
     for c in CASES:
-        run(c)
+        if not only or c[0] in only:
+            run(c)
