@@ -114,7 +114,7 @@ class NonlinearIBSolver:
 
     def __init__(self, grid: Grid, model: NavierStokesModel, dt: float, scheme: str = "rk3", tol: float = 1e-7,
                  precision: str = "fp64", stream: Optional[int] = None, cg_max_iter: int = 3000,
-                 device: int = -1, precond: str = "none", pc_refresh: int = 10):
+                 device: int = -1, precond: str = "none", pc_refresh: int = 10, cg_graph: bool = True):
         self.grid, self.model, self.dt = grid, model, dt
         self.scheme = scheme
         L = lib()
@@ -131,7 +131,7 @@ class NonlinearIBSolver:
             for j in range(6):
                 bodies[k].params[j] = b.params[j] if j < len(b.params) else 0.0
         p = ibg_params(model.Re, dt, SCHEMES[scheme], tol, cg_max_iter, model.u_mag, model.alpha,
-                       PRECISIONS[precision], device, PRECONDS[precond], pc_refresh)
+                       PRECISIONS[precision], device, PRECONDS[precond], pc_refresh, int(cg_graph))
         h = ctypes.c_void_p()
         check(L.ibg_create(ctypes.byref(g), len(model.geom.bodies), bodies, ctypes.byref(p),
                            ctypes.c_void_p(stream) if stream else None, ctypes.byref(h)), None)
@@ -267,13 +267,13 @@ class NonlinearIBSolver:
 
 
 def from_workload(wl, precision: str = "fp64", stream=None, device: int = -1, precond: str = "none",
-                  pc_refresh: int = 10):
+                  pc_refresh: int = 10, cg_graph: bool = True):
     """Grid, model, solver and initial State for an ibpm_b200.configs.Workload."""
     grid = Grid(wl.nx, wl.ny, wl.ngrid, wl.length, wl.xoffset, wl.yoffset)
     geo = _geometry.parse(wl.geom)
     model = NavierStokesModel(grid, geo, wl.Re)
     solver = NonlinearIBSolver(grid, model, wl.dt, wl.scheme, wl.tol, precision=precision, stream=stream,
-                               device=device, precond=precond, pc_refresh=pc_refresh)
+                               device=device, precond=precond, pc_refresh=pc_refresh, cg_graph=cg_graph)
     x = State(grid, geo.num_points)
     w0 = wl.initial_vorticity()
     if w0 is not None:

@@ -28,7 +28,7 @@ class ibg_params(ctypes.Structure):
     _fields_ = [("Re", ctypes.c_double), ("dt", ctypes.c_double), ("scheme", ctypes.c_int),
                 ("cg_tol", ctypes.c_double), ("cg_max_iter", ctypes.c_int), ("u_mag", ctypes.c_double),
                 ("alpha", ctypes.c_double), ("precision", ctypes.c_int), ("device", ctypes.c_int),
-                ("cg_precond", ctypes.c_int), ("pc_refresh", ctypes.c_int)]
+                ("cg_precond", ctypes.c_int), ("pc_refresh", ctypes.c_int), ("cg_graph", ctypes.c_int)]
 
 
 SCHEMES = {"euler": 0, "ab2": 1, "rk3": 2, "rk3b": 3}

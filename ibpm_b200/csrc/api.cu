@@ -79,6 +79,28 @@ struct Bulk {
 };
 
 namespace ibg {
+// End of one device-side CG iteration: keep looping while the solve is active.
+// flags: [0] active, [1] iterations of this solve, [2] cap, [3] total iterations,
+// [4] solves, [5] largest count, [6] solves that hit the cap, [7] loop counter.
+// The loop also stops after cap + 2 passes whatever the solver flags say.
+__global__ void k_cg_loop_cond(cudaGraphConditionalHandle h, int* flags) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int loops = flags[7] + 1;
+    flags[7] = loops;
+    const bool more = flags[0] != 0 && loops <= flags[2] + 2;
+    if (!more) {
+        const int it = flags[1];
+        flags[3] += it;
+        flags[4] += 1;
+        if (it > flags[5]) flags[5] = it;
+        if (it >= flags[2]) flags[6] += 1;
+    }
+    cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+__global__ void k_cg_loop_reset(int* flags) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) flags[7] = 0;
+}
+
 template <typename A, typename B>
 __global__ void k_convert(size_t n, const A* __restrict__ in, B* __restrict__ out) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -212,6 +234,8 @@ struct ibg_context {
         cosT.release();
         if (own_stream && st) cudaStreamDestroy(st);
         st = nullptr;
+        if (side) cudaStreamDestroy(side);
+        side = nullptr;
         d_ref = d_pts = d_vel = nullptr;
         d_body_of = nullptr;
         d_bodies = nullptr;
@@ -257,8 +281,70 @@ struct ibg_context {
 
     // CG with warm start x = f (src/ConjugateGradientSolver.cc:35-65); host reads the
     // convergence flag every `chunk` iterations.
+    // The CG loop inside a stream capture: prologue, then a WHILE conditional node
+    // whose body (one iteration + the loop-condition kernel) is captured on a side
+    // stream.  Iteration counts accumulate on the device (flags[3..6]).
+    cudaStream_t side = nullptr;
+    bool capturing = false;
+    template <typename T>
+    int cg_solve_graph(Bulk<T>& B, int k, const double* b, double* x) {
+        const bool pc = prm.cg_precond != IBG_PRECOND_NONE;
+        m_apply<T>(B, k, x, cg_q);
+        if (pc) {
+            pcg_begin(ncomp, b, cg_q, cg_r, cg_scal, cg_flags, st);
+            precondition(k, cg_r, cg_z);
+            pcg_begin2(ncomp, cg_r, cg_z, cg_d, cg_scal, cg_flags, st);
+        } else {
+            cg_begin(ncomp, b, cg_q, cg_r, cg_d, cg_scal, cg_flags, st);
+        }
+        k_cg_loop_reset<<<1, 1, 0, st>>>(cg_flags);
+        launches += pc ? 3 : 2;
+        cudaStreamCaptureStatus cs;
+        unsigned long long id = 0;
+        cudaGraph_t cgraph = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        if (cudaStreamGetCaptureInfo(st, &cs, &id, &cgraph, &deps, &ndeps) != cudaSuccess ||
+            cs != cudaStreamCaptureStatusActive)
+            return fail(IBG_ERR_CUDA, "cg graph: stream is not capturing");
+        cudaGraphConditionalHandle h;
+        if (cudaGraphConditionalHandleCreate(&h, cgraph, 1, cudaGraphCondAssignDefault) != cudaSuccess)
+            return cuda_check("cg graph: conditional handle");
+        cudaGraphNodeParams p{};
+        p.type = cudaGraphNodeTypeConditional;
+        p.conditional.handle = h;
+        p.conditional.type = cudaGraphCondTypeWhile;
+        p.conditional.size = 1;
+        cudaGraphNode_t node;
+        if (cudaGraphAddNode(&node, cgraph, deps, ndeps, &p) != cudaSuccess) return cuda_check("cg graph: while node");
+        cudaGraph_t body = p.conditional.phGraph_out[0];
+        if (cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies) != cudaSuccess)
+            return cuda_check("cg graph: dependencies");
+        if (!side && cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking) != cudaSuccess)
+            return cuda_check("cg graph: side stream");
+        if (cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
+            cudaSuccess)
+            return cuda_check("cg graph: body capture");
+        cudaStream_t main = st;
+        st = side;
+        m_apply<T>(B, k, cg_d, cg_q);
+        if (pc) {
+            pcg_step1(ncomp, x, cg_r, cg_d, cg_q, cg_z, cg_zold, cg_scal, cg_flags, st);
+            precondition(k, cg_r, cg_z);
+            pcg_step2(ncomp, cg_r, cg_z, cg_zold, cg_d, cg_scal, cg_flags, st);
+        } else {
+            cg_update(ncomp, x, cg_r, cg_d, cg_q, cg_scal, cg_flags, st);
+        }
+        k_cg_loop_cond<<<1, 1, 0, st>>>(h, cg_flags);
+        st = main;
+        cudaGraph_t out = nullptr;
+        if (cudaStreamEndCapture(side, &out) != cudaSuccess) return cuda_check("cg graph: body end");
+        return IBG_OK;
+    }
+
     template <typename T>
     int cg_solve(Bulk<T>& B, int k, const double* b, double* x) {
+        if (capturing) return cg_solve_graph<T>(B, k, b, x);
         if (prm.cg_precond != IBG_PRECOND_NONE) return pcg_solve<T>(B, k, b, x);
         m_apply<T>(B, k, x, cg_q);
         cg_begin(ncomp, b, cg_q, cg_r, cg_d, cg_scal, cg_flags, st);
@@ -494,7 +580,9 @@ struct ibg_context {
         const long long before = launches;
         if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
             return cuda_check("capture");
+        capturing = true;
         int s = enqueue_step();
+        capturing = false;
         if (cudaStreamEndCapture(st, &gr) != cudaSuccess || s) {
             launches = before;
             return s ? s : cuda_check("capture end");
@@ -690,7 +778,7 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
         c->alloc(&c->d_body_of, (size_t)c->npts) || c->alloc(&c->d_bodies, c->h_bodies.size()) ||
         c->alloc(&c->slots.idx, kSlots * m) || c->alloc(&c->slots.w, kSlots * m) || c->alloc(&c->slots.n, m) ||
         c->alloc(&c->d_b, m) || c->alloc(&c->d_time, 1) || c->alloc(&c->d_status, 1) || c->alloc(&c->cg_r, m) ||
-        c->alloc(&c->cg_d, m) || c->alloc(&c->cg_q, m) || c->alloc(&c->cg_z, m) || c->alloc(&c->cg_zold, m) || c->alloc(&c->cg_scal, 4) || c->alloc(&c->cg_flags, 4) ||
+        c->alloc(&c->cg_d, m) || c->alloc(&c->cg_q, m) || c->alloc(&c->cg_z, m) || c->alloc(&c->cg_zold, m) || c->alloc(&c->cg_scal, 4) || c->alloc(&c->cg_flags, 8) ||
         c->alloc(&c->d_hist, 2 * (size_t)kHistCap) || c->alloc(&c->d_hist_count, 1);
     if (!s && cudaMallocHost((void**)&c->h_flags, 4 * sizeof(int)) != cudaSuccess) s = IBG_ERR_CUDA;
     if (s) {
@@ -703,7 +791,7 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
     cudaMemcpy(c->d_bodies, c->h_bodies.data(), sizeof(BodyDev) * c->h_bodies.size(), cudaMemcpyHostToDevice);
     double sc[4] = {0, 0, c->prm.cg_tol * c->prm.cg_tol, 0};
     cudaMemcpy(c->cg_scal, sc, sizeof(sc), cudaMemcpyHostToDevice);
-    int fl[4] = {0, 0, c->prm.cg_max_iter, 0};
+    int fl[8] = {0, 0, c->prm.cg_max_iter, 0, 0, 0, 0, 0};
     cudaMemcpy(c->cg_flags, fl, sizeof(fl), cudaMemcpyHostToDevice);
     if (chol_solve_prepare((int)m)) {
         g_create_error = "ibg_create: too many boundary points for the Cholesky solve";
@@ -885,7 +973,7 @@ int ibg_advance(ibg_context* c, int nsteps) {
             c->steps_since_pc = 0;
         }
         ++c->steps_since_pc;
-        if (!c->moving && c->old_saved) {
+        if (c->old_saved && (!c->moving || c->prm.cg_graph)) {
             int gs = c->ensure_graph();
             if (gs) return gs;
             if (cudaGraphLaunch(c->graph, c->st) != cudaSuccess) return c->cuda_check("ibg_advance: graph launch");
@@ -942,15 +1030,32 @@ int ibg_sizes(const ibg_context* c, long long* ns, long long* nf, int* nb) {
     return IBG_OK;
 }
 
+static void cg_device_stats(const ibg_context* c, int out[8]) {
+    for (int i = 0; i < 8; ++i) out[i] = 0;
+    if (!c->cg_flags) return;
+    cudaMemcpyAsync(out, c->cg_flags, 8 * sizeof(int), cudaMemcpyDeviceToHost, c->st);
+    cudaStreamSynchronize(c->st);
+}
+
 int ibg_cg_totals(const ibg_context* c, long long* iterations, long long* solves) {
     if (!c) return IBG_ERR_ARG;
-    if (iterations) *iterations = c->cg_total;
-    if (solves) *solves = c->cg_solves;
+    int d[8];
+    cg_device_stats(c, d);
+    if (iterations) *iterations = c->cg_total + d[3];
+    if (solves) *solves = c->cg_solves + d[4];
     return IBG_OK;
 }
 
 int ibg_cg_stats(const ibg_context* c, int* last, int* mx, int* capped) {
     if (!c) return IBG_ERR_ARG;
+    int d[8];
+    cg_device_stats(c, d);
+    if (d[4] > 0) {
+        if (last) *last = d[1];
+        if (mx) *mx = std::max(c->cg_max, d[5]);
+        if (capped) *capped = c->cg_capped + d[6];
+        return IBG_OK;
+    }
     if (last) *last = c->cg_last;
     if (mx) *mx = c->cg_max;
     if (capped) *capped = c->cg_capped;

@@ -71,6 +71,8 @@ typedef struct {
     int device;             /* CUDA device ordinal, -1 = the calling thread's current device */
     int cg_precond;         /* moving bodies: IBG_PRECOND_* (NONE = the reference's plain CG) */
     int pc_refresh;         /* steps between rebuilds of the Cholesky preconditioner (default 10) */
+    int cg_graph;           /* moving bodies: 1 = the whole step, CG loop included, is one CUDA graph
+                               (the loop is a device-side WHILE node), 0 = host-driven CG loop */
 } ibg_params;
 
 /* preconditioners of the moving-body force solve (all keep the reference's

@@ -279,3 +279,21 @@ def test_cholesky_preconditioned_cg_matches_reference(name):
         assert rel_l2(x.omega, d["omega"]) < 1e-9
         s.close()
     assert its["cholesky"] * 3 < its["none"], its
+
+
+def test_host_driven_cg_loop_matches_reference():
+    """The host-driven CG loop (no device-side WHILE node) on the moving plate."""
+    import ibpm_b200 as ib
+    d = load_golden("plate_l2_pitchplunge_cg")
+    grid = ib.Grid(int(d["nx"]), int(d["ny"]), int(d["ngrid"]), float(d["length"]), float(d["xoffset"]),
+                   float(d["yoffset"]))
+    geo = ib.geometry.parse(str(d["geom"]))
+    s = ib.NonlinearIBSolver(grid, ib.NavierStokesModel(grid, geo, float(d["Re"])), float(d["dt"]), "rk3",
+                             float(d["tol"]), cg_graph=False)
+    x = ib.State(grid, geo.num_points)
+    s.init()
+    s.set_state(x, with_q=False)
+    n = int(d["nsteps"])
+    s.advance_resident(n)
+    assert rel_l2(s.force_history(n), d["forces"][:, 2:4]) < FP64_TOL
+    s.close()
