@@ -114,7 +114,8 @@ class NonlinearIBSolver:
 
     def __init__(self, grid: Grid, model: NavierStokesModel, dt: float, scheme: str = "rk3", tol: float = 1e-7,
                  precision: str = "fp64", stream: Optional[int] = None, cg_max_iter: int = 3000,
-                 device: int = -1, precond: str = "none", pc_refresh: int = 10, cg_graph: bool = True):
+                 device: int = -1, precond: str = "none", pc_refresh: int = 10, cg_graph: bool = True,
+                 pc_fallback_iter: int = 0):
         self.grid, self.model, self.dt = grid, model, dt
         self.scheme = scheme
         L = lib()
@@ -131,7 +132,8 @@ class NonlinearIBSolver:
             for j in range(6):
                 bodies[k].params[j] = b.params[j] if j < len(b.params) else 0.0
         p = ibg_params(model.Re, dt, SCHEMES[scheme], tol, cg_max_iter, model.u_mag, model.alpha,
-                       PRECISIONS[precision], device, PRECONDS[precond], pc_refresh, int(cg_graph))
+                       PRECISIONS[precision], device, PRECONDS[precond], pc_refresh, int(cg_graph),
+                       pc_fallback_iter)
         h = ctypes.c_void_p()
         check(L.ibg_create(ctypes.byref(g), len(model.geom.bodies), bodies, ctypes.byref(p),
                            ctypes.c_void_p(stream) if stream else None, ctypes.byref(h)), None)
@@ -228,6 +230,61 @@ class NonlinearIBSolver:
     def last_launch_count(self) -> int:
         return int(lib().ibg_last_launch_count(self._h))
 
+    # -- learned preconditioner (no reference counterpart) -----------------
+    def lpc_generate(self, nconfig: int, t0: float, t1: float, nres: int, seed: int = 0):
+        """Training pairs from this solver: geometry [n, npts, 4], residuals r and
+        targets beta M^-1 r [n, 2 npts] (float32), n = nconfig * nres."""
+        n, P = nconfig * nres, self.npoints
+        geom = np.zeros((n, P, 4), np.float32)
+        r = np.zeros((n, 2 * P), np.float32)
+        zb = np.zeros((n, 2 * P), np.float32)
+        check(lib().ibg_lpc_generate(self._h, int(nconfig), float(t0), float(t1), int(nres), int(seed),
+                                     _ptr(geom), _ptr(r), _ptr(zb)), self._h)
+        return geom, r, zb
+
+    def lpc_train(self, geom, r, zb, epochs: int = 20, batch: int = 32, lr: float = 1e-3, seed: int = 0):
+        """Fit the network on the device (Adam, FP32) and enable it; returns the
+        mean loss of every epoch."""
+        geom, r, zb = (np.ascontiguousarray(a, dtype=np.float32) for a in (geom, r, zb))
+        hist = np.zeros(epochs, np.float32)
+        check(lib().ibg_lpc_train(self._h, int(r.shape[0]), _ptr(geom), _ptr(r), _ptr(zb), int(epochs), int(batch),
+                                  ctypes.c_float(lr), int(seed), _ptr(hist)), self._h)
+        return hist
+
+    def lpc_loss_grad(self, geom, r, zb, params=None):
+        """Mean loss and its gradient over the given samples (params: None keeps the current ones)."""
+        geom, r, zb = (np.ascontiguousarray(a, dtype=np.float32) for a in (geom, r, zb))
+        pp = None if params is None else np.ascontiguousarray(params, dtype=np.float32)
+        grad = np.zeros(int(lib().ibg_lpc_num_params()), np.float32)
+        loss = ctypes.c_float()
+        check(lib().ibg_lpc_loss_grad(self._h, int(r.shape[0]), _ptr(geom), _ptr(r), _ptr(zb), _ptr(pp),
+                                      ctypes.byref(loss), _ptr(grad)), self._h)
+        return loss.value, grad
+
+    def lpc_apply(self, k: int, r):
+        """The preconditioner action z = P_k r at the current body configuration
+        (BF16 inference) and the geometry features it used [npts, 4]."""
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.zeros_like(r)
+        geom = np.zeros((self.npoints, 4), np.float32)
+        check(lib().ibg_lpc_apply(self._h, int(k), _ptr(r), _ptr(z), _ptr(geom)), self._h)
+        return z, geom
+
+    def beta(self, k: int) -> float:
+        """Sub-step factor beta_k of M_k = beta_k C A_k^-1 B."""
+        b = ctypes.c_double()
+        check(lib().ibg_substep_beta(self._h, int(k), ctypes.byref(b)), self._h)
+        return b.value
+
+    def lpc_params(self) -> np.ndarray:
+        p = np.zeros(int(lib().ibg_lpc_num_params()), np.float32)
+        check(lib().ibg_lpc_get_params(self._h, _ptr(p), p.size), self._h)
+        return p
+
+    def lpc_set_params(self, params):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        check(lib().ibg_lpc_set_params(self._h, _ptr(p), p.size), self._h)
+
     # -- operators (host buffers) ------------------------------------------
     def _op(self, name, *args, out_shape):
         out = np.zeros(out_shape)
@@ -267,13 +324,14 @@ class NonlinearIBSolver:
 
 
 def from_workload(wl, precision: str = "fp64", stream=None, device: int = -1, precond: str = "none",
-                  pc_refresh: int = 10, cg_graph: bool = True):
+                  pc_refresh: int = 10, cg_graph: bool = True, pc_fallback_iter: int = 0):
     """Grid, model, solver and initial State for an ibpm_b200.configs.Workload."""
     grid = Grid(wl.nx, wl.ny, wl.ngrid, wl.length, wl.xoffset, wl.yoffset)
     geo = _geometry.parse(wl.geom)
     model = NavierStokesModel(grid, geo, wl.Re)
     solver = NonlinearIBSolver(grid, model, wl.dt, wl.scheme, wl.tol, precision=precision, stream=stream,
-                               device=device, precond=precond, pc_refresh=pc_refresh, cg_graph=cg_graph)
+                               device=device, precond=precond, pc_refresh=pc_refresh, cg_graph=cg_graph,
+                               pc_fallback_iter=pc_fallback_iter)
     x = State(grid, geo.num_points)
     w0 = wl.initial_vorticity()
     if w0 is not None:

@@ -28,7 +28,8 @@ class ibg_params(ctypes.Structure):
     _fields_ = [("Re", ctypes.c_double), ("dt", ctypes.c_double), ("scheme", ctypes.c_int),
                 ("cg_tol", ctypes.c_double), ("cg_max_iter", ctypes.c_int), ("u_mag", ctypes.c_double),
                 ("alpha", ctypes.c_double), ("precision", ctypes.c_int), ("device", ctypes.c_int),
-                ("cg_precond", ctypes.c_int), ("pc_refresh", ctypes.c_int), ("cg_graph", ctypes.c_int)]
+                ("cg_precond", ctypes.c_int), ("pc_refresh", ctypes.c_int), ("cg_graph", ctypes.c_int),
+                ("pc_fallback_iter", ctypes.c_int)]
 
 
 SCHEMES = {"euler": 0, "ab2": 1, "rk3": 2, "rk3b": 3}
@@ -62,6 +63,14 @@ SIGNATURES = {
     "ibg_stream": (_VP, [_VP]),
     "ibg_last_launch_count": (ctypes.c_longlong, [_VP]),
     "ibg_run_kernel": (ctypes.c_longlong, [_VP, _I, _I]),
+    "ibg_lpc_num_params": (ctypes.c_size_t, []),
+    "ibg_lpc_generate": (_I, [_VP, _I, _D, _D, _I, ctypes.c_uint, _VP, _VP, _VP]),
+    "ibg_lpc_train": (_I, [_VP, _I, _VP, _VP, _VP, _I, _I, ctypes.c_float, ctypes.c_uint, _VP]),
+    "ibg_lpc_loss_grad": (_I, [_VP, _I, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "ibg_lpc_get_params": (_I, [_VP, _VP, ctypes.c_size_t]),
+    "ibg_lpc_set_params": (_I, [_VP, _VP, ctypes.c_size_t]),
+    "ibg_lpc_apply": (_I, [_VP, _I, _VP, _VP, _VP]),
+    "ibg_substep_beta": (_I, [_VP, _I, _VP]),
     "ibg_poisson_solve": (_I, [_VP, _VP, _VP]),
     "ibg_helmholtz_solve": (_I, [_VP, _D, _VP, _VP]),
     "ibg_nonlinear": (_I, [_VP, _VP, _VP, _VP]),

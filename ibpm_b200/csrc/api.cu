@@ -6,8 +6,10 @@
 // launches on one stream; for fixed bodies the whole step is captured once
 // into a CUDA graph and replayed.  Moving bodies use CG, whose convergence
 // test is read back every few iterations.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <random>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
@@ -19,6 +21,7 @@
 #include "ibg_force.cuh"
 #include "ibg_internal.cuh"
 #include "ibg_kernels.cuh"
+#include "ibg_lpc.cuh"
 #include "ibg_ops.cuh"
 
 using namespace ibg;
@@ -160,6 +163,12 @@ struct ibg_context {
     int cg_last = 0, cg_max = 0, cg_capped = 0;
     long long cg_total = 0, cg_solves = 0;
     int steps_since_pc = 0;
+    // learned preconditioner
+    Lpc lpc;
+    bool lpc_ready = false;
+    LpcBodies lb;
+    std::vector<int> h_nbr, h_cnt;
+    TrainScratch tws;
     // force history
     double* d_hist = nullptr;
     int* d_hist_count = nullptr;
@@ -209,14 +218,23 @@ struct ibg_context {
         return IBG_OK;
     }
 
-    void release() {
+    void drop_graph() {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
         if (graph_def) cudaGraphDestroy(graph_def);
         graph_def = nullptr;
+    }
+    void release() {
+        drop_graph();
         b64.release();
         b32.release();
         release_build_scratch();
+        lpc.release();
+        tws.release();
+        if (lb.start) cudaFree(lb.start);
+        if (lb.len) cudaFree(lb.len);
+        if (lb.closed) cudaFree(lb.closed);
+        lb = LpcBodies{};
         void* ptrs[] = {d_ref, d_pts, d_vel, d_body_of, d_bodies, slots.idx, slots.w, slots.n, d_b, d_time, f,
                         flux0, rhsb, btmp, d_status, cg_r, cg_d, cg_q, cg_scal, cg_flags, d_hist, d_hist_count, cg_z, cg_zold};
         for (void* p : ptrs)
@@ -376,12 +394,12 @@ struct ibg_context {
     void precondition(int k, const double* r, double* z) {
         if (prm.cg_precond == IBG_PRECOND_CHOLESKY) {
             minv_apply(ncomp, Mi[k], r, z, st);
+            launches += 1;
         } else {
-            apply_learned_precond(r, z);
+            apply_learned_precond(k, r, z);
         }
-        launches += 1;
     }
-    void apply_learned_precond(const double* r, double* z);
+    void apply_learned_precond(int k, const double* r, double* z);
 
     // flexible preconditioned CG (Polak-Ribiere beta, so a preconditioner that
     // changes between iterations is allowed); same absolute test r.r <= tol^2
@@ -619,9 +637,25 @@ __global__ void k_hist_force(int npts, const double* f, double dx2, double* hist
 }
 }  // namespace ibg
 
-void ibg_context::apply_learned_precond(const double* r, double* z) {
-    // until a network is loaded the learned preconditioner is the identity (plain CG directions)
-    cudaMemcpyAsync(z, r, sizeof(double) * ncomp, cudaMemcpyDeviceToDevice, st);
+namespace ibg {
+// after a fallback to plain CG (flags[8]), the preconditioner is the identity
+__global__ void k_fallback_identity(int m, const int* __restrict__ flags, const double* __restrict__ r,
+                                    double* __restrict__ z) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m && flags[8]) z[i] = r[i];
+}
+}  // namespace ibg
+
+void ibg_context::apply_learned_precond(int k, const double* r, double* z) {
+    if (lpc_ready) {
+        lpc.apply(d_pts, lb, r, z, beta[k], st);
+        k_fallback_identity<<<(ncomp + 255) / 256, 256, 0, st>>>(ncomp, cg_flags, r, z);
+        launches += 5;
+    } else {
+        // no network yet: identity (plain CG directions)
+        cudaMemcpyAsync(z, r, sizeof(double) * ncomp, cudaMemcpyDeviceToDevice, st);
+        launches += 1;
+    }
 }
 
 void ibg_context::net_force_record() {
@@ -681,6 +715,8 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
     c->prm = *params;
     if (c->prm.cg_max_iter <= 0) c->prm.cg_max_iter = 3000;
     if (c->prm.pc_refresh <= 0) c->prm.pc_refresh = 10;
+    if (c->prm.pc_fallback_iter <= 0) c->prm.pc_fallback_iter = c->prm.cg_max_iter;
+    if (c->prm.cg_precond == IBG_PRECOND_LEARNED && c->prm.pc_refresh <= 0) c->prm.pc_refresh = 10;
     if (c->prm.cg_precond < IBG_PRECOND_NONE || c->prm.cg_precond > IBG_PRECOND_LEARNED) {
         delete c;
         g_create_error = "ibg_create: unknown preconditioner";
@@ -739,6 +775,40 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
     }
     c->npts = (int)body_of.size();
     c->ncomp = 2 * c->npts;
+    // boundary neighbours (i +- 1..4 along each body, wrapping on closed curves) for the learned preconditioner
+    std::vector<int> bstart, blen, bclosed;
+    {
+        int p0 = 0;
+        for (int b = 0; b < nbodies; ++b) {
+            const int n = bodies[b].npoints;
+            bstart.push_back(p0);
+            blen.push_back(n);
+            // closed if the end points are about one spacing apart
+            std::vector<double> d;
+            for (int q = 0; q + 1 < n; ++q)
+                d.push_back(std::hypot(bodies[b].xy[2 * q + 2] - bodies[b].xy[2 * q], bodies[b].xy[2 * q + 3] - bodies[b].xy[2 * q + 1]));
+            std::sort(d.begin(), d.end());
+            const double med = d.empty() ? 0.0 : d[d.size() / 2];
+            const double gap = n > 1 ? std::hypot(bodies[b].xy[2 * (n - 1)] - bodies[b].xy[0], bodies[b].xy[2 * (n - 1) + 1] - bodies[b].xy[1]) : 0.0;
+            const int closed = (n > 2 && gap < 1.5 * med) ? 1 : 0;
+            bclosed.push_back(closed);
+            for (int q = 0; q < n; ++q) {
+                int cntq = 0;
+                for (int off = 1; off <= 4; ++off)
+                    for (int sgn = -1; sgn <= 1; sgn += 2) {
+                        int j = q + sgn * off;
+                        if (closed) j = ((j % n) + n) % n;
+                        else if (j < 0 || j >= n) continue;
+                        if (j == q) continue;
+                        c->h_nbr.push_back(p0 + j);
+                        ++cntq;
+                    }
+                for (int f = cntq; f < 8; ++f) c->h_nbr.push_back(-1);
+                c->h_cnt.push_back(cntq);
+            }
+            p0 += n;
+        }
+    }
     if (c->ncomp > 16384) {
         delete c;
         g_create_error = "ibg_create: too many boundary points";
@@ -778,7 +848,7 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
         c->alloc(&c->d_body_of, (size_t)c->npts) || c->alloc(&c->d_bodies, c->h_bodies.size()) ||
         c->alloc(&c->slots.idx, kSlots * m) || c->alloc(&c->slots.w, kSlots * m) || c->alloc(&c->slots.n, m) ||
         c->alloc(&c->d_b, m) || c->alloc(&c->d_time, 1) || c->alloc(&c->d_status, 1) || c->alloc(&c->cg_r, m) ||
-        c->alloc(&c->cg_d, m) || c->alloc(&c->cg_q, m) || c->alloc(&c->cg_z, m) || c->alloc(&c->cg_zold, m) || c->alloc(&c->cg_scal, 4) || c->alloc(&c->cg_flags, 8) ||
+        c->alloc(&c->cg_d, m) || c->alloc(&c->cg_q, m) || c->alloc(&c->cg_z, m) || c->alloc(&c->cg_zold, m) || c->alloc(&c->cg_scal, 4) || c->alloc(&c->cg_flags, 10) ||
         c->alloc(&c->d_hist, 2 * (size_t)kHistCap) || c->alloc(&c->d_hist_count, 1);
     if (!s && cudaMallocHost((void**)&c->h_flags, 4 * sizeof(int)) != cudaSuccess) s = IBG_ERR_CUDA;
     if (s) {
@@ -787,11 +857,21 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
         return IBG_ERR_CUDA;
     }
     cudaMemcpy(c->d_ref, c->h_ref.data(), sizeof(double) * c->h_ref.size(), cudaMemcpyHostToDevice);
+    c->lb.n = nbodies;
+    c->lb.body_of = c->d_body_of;
+    if (c->alloc(&c->lb.start, nbodies) || c->alloc(&c->lb.len, nbodies) || c->alloc(&c->lb.closed, nbodies)) {
+        g_create_error = "ibg_create: device allocation failed";
+        delete c;
+        return IBG_ERR_CUDA;
+    }
+    cudaMemcpy(c->lb.start, bstart.data(), sizeof(int) * nbodies, cudaMemcpyHostToDevice);
+    cudaMemcpy(c->lb.len, blen.data(), sizeof(int) * nbodies, cudaMemcpyHostToDevice);
+    cudaMemcpy(c->lb.closed, bclosed.data(), sizeof(int) * nbodies, cudaMemcpyHostToDevice);
     cudaMemcpy(c->d_body_of, body_of.data(), sizeof(int) * body_of.size(), cudaMemcpyHostToDevice);
     cudaMemcpy(c->d_bodies, c->h_bodies.data(), sizeof(BodyDev) * c->h_bodies.size(), cudaMemcpyHostToDevice);
     double sc[4] = {0, 0, c->prm.cg_tol * c->prm.cg_tol, 0};
     cudaMemcpy(c->cg_scal, sc, sizeof(sc), cudaMemcpyHostToDevice);
-    int fl[8] = {0, 0, c->prm.cg_max_iter, 0, 0, 0, 0, 0};
+    int fl[10] = {0, 0, c->prm.cg_max_iter, 0, 0, 0, 0, 0, 0, c->prm.pc_fallback_iter};
     cudaMemcpy(c->cg_flags, fl, sizeof(fl), cudaMemcpyHostToDevice);
     if (chol_solve_prepare((int)m)) {
         g_create_error = "ibg_create: too many boundary points for the Cholesky solve";
@@ -1295,6 +1375,241 @@ int ibg_ensemble_destroy(ibg_ensemble* e) {
 void* ibg_ensemble_stream(const ibg_ensemble* e) { return e ? (void*)e->st : nullptr; }
 long long ibg_ensemble_launches_per_step(const ibg_ensemble* e) { return e ? e->launches_per_step : 0; }
 const char* ibg_ensemble_last_error(const ibg_ensemble* e) { return e ? e->err.c_str() : g_ens_error.c_str(); }
+
+// ---------------------------------------------------------------------------
+// learned preconditioner: data from the solver, training, parameters
+// ---------------------------------------------------------------------------
+namespace ibg {
+__global__ void k_lpc_targets(int P, const float* __restrict__ r, const float* __restrict__ zb, float* __restrict__ t) {
+    __shared__ float red[32];
+    const int b = blockIdx.x;
+    float acc = 0.f;
+    for (int k = threadIdx.x; k < 2 * P; k += blockDim.x) {
+        const float v = r[(size_t)b * 2 * P + k];
+        acc += v * v;
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    float tot = 0.f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
+    const float s = sqrtf(tot / (2 * P)) + 1e-30f;
+    for (int k = threadIdx.x; k < 2 * P; k += blockDim.x) t[(size_t)b * 2 * P + k] = zb[(size_t)b * 2 * P + k] / s;
+}
+__global__ void k_gather_rows(int nrows, int width, const int* __restrict__ idx, const float* __restrict__ src,
+                              float* __restrict__ dst) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)nrows * width) return;
+    const int r = (int)(t / width), c = (int)(t % width);
+    dst[t] = src[(size_t)idx[r] * width + c];
+}
+}  // namespace ibg
+
+static int lpc_ensure(ibg_context* c) {
+    if (c->lpc.params) return IBG_OK;
+    if (c->lpc.init(c->npts, c->h_nbr, c->h_cnt)) return c->fail(IBG_ERR_CUDA, "learned preconditioner set-up failed");
+    return IBG_OK;
+}
+
+size_t ibg_lpc_num_params(void) { return lpc_num_params(); }
+
+int ibg_lpc_generate(ibg_context* c, int nconfig, double t0, double t1, int nres, unsigned int seed, float* geom,
+                     float* r_out, float* zb_out) {
+    if (!c || nconfig < 1 || nres < 1 || !geom || !r_out || !zb_out) return IBG_ERR_ARG;
+    if (lpc_ensure(c)) return IBG_ERR_CUDA;
+    const int P = c->npts, m = c->ncomp;
+    std::mt19937 rng(seed);
+    std::normal_distribution<double> nd(0.0, 1.0);
+    std::vector<double> r((size_t)nres * m), z((size_t)nres * m);
+    std::vector<float> gh((size_t)P * 4);
+    double* dr = nullptr;
+    double* dz = nullptr;
+    if (c->alloc(&dr, (size_t)nres * m) || c->alloc(&dz, (size_t)nres * m)) return IBG_ERR_CUDA;
+    const double keep_time = c->time;
+    int status = IBG_OK;
+    for (int cf = 0; cf < nconfig && !status; ++cf) {
+        const double t = nconfig == 1 ? t0 : t0 + (t1 - t0) * cf / (nconfig - 1);
+        cudaMemcpyAsync(c->d_time, &t, sizeof(double), cudaMemcpyHostToDevice, c->st);
+        c->move_bodies(0.0);
+        status = c->build_operator();
+        if (status) break;
+        c->lpc.apply(c->d_pts, c->lb, c->btmp, c->rhsb, 1.0, c->st);  // computes the geometry features
+        cudaMemcpyAsync(gh.data(), c->lpc.geom, sizeof(float) * 4 * P, cudaMemcpyDeviceToHost, c->st);
+        // residuals: white N(0,1) and boundary-smooth random modes, alternately
+        for (int j = 0; j < nres; ++j) {
+            double* rj = r.data() + (size_t)j * m;
+            if (j % 2 == 0) {
+                for (int q = 0; q < m; ++q) rj[q] = nd(rng);
+            } else {
+                double a[2][4], bcoef[2][4];
+                for (int cc = 0; cc < 2; ++cc)
+                    for (int q = 0; q < 4; ++q) {
+                        a[cc][q] = nd(rng);
+                        bcoef[cc][q] = nd(rng);
+                    }
+                for (int i = 0; i < P; ++i) {
+                    const double sarc = (double)i / P;
+                    for (int cc = 0; cc < 2; ++cc) {
+                        double v = 0.1 * nd(rng);
+                        for (int q = 0; q < 4; ++q)
+                            v += a[cc][q] * sin(M_PI * (q + 1) * sarc) + bcoef[cc][q] * cos(M_PI * (q + 1) * sarc);
+                        rj[cc * P + i] = v;
+                    }
+                }
+            }
+        }
+        cudaMemcpyAsync(dr, r.data(), sizeof(double) * r.size(), cudaMemcpyHostToDevice, c->st);
+        for (int j = 0; j < nres; ++j) {
+            const int k = j % c->sch.nsub;
+            minv_apply(m, c->Mi[k], dr + (size_t)j * m, dz + (size_t)j * m, c->st);
+        }
+        cudaMemcpyAsync(z.data(), dz, sizeof(double) * z.size(), cudaMemcpyDeviceToHost, c->st);
+        if (cudaStreamSynchronize(c->st) != cudaSuccess) status = c->cuda_check("ibg_lpc_generate");
+        for (int j = 0; j < nres; ++j) {
+            const int k = j % c->sch.nsub;
+            const size_t sidx = (size_t)cf * nres + j;
+            std::memcpy(geom + sidx * 4 * P, gh.data(), sizeof(float) * 4 * P);
+            for (int q = 0; q < m; ++q) {
+                r_out[sidx * m + q] = (float)r[(size_t)j * m + q];
+                zb_out[sidx * m + q] = (float)(c->beta[k] * z[(size_t)j * m + q]);
+            }
+        }
+    }
+    cudaFree(dr);
+    cudaFree(dz);
+    // back to the current configuration
+    cudaMemcpyAsync(c->d_time, &keep_time, sizeof(double), cudaMemcpyHostToDevice, c->st);
+    c->move_bodies(0.0);
+    if (c->prm.cg_precond == IBG_PRECOND_CHOLESKY) {
+        int s2 = c->build_operator();
+        if (!status) status = s2;
+    }
+    if (cudaStreamSynchronize(c->st) != cudaSuccess && !status) status = c->cuda_check("ibg_lpc_generate");
+    return status;
+}
+
+int ibg_lpc_loss_grad(ibg_context* c, int nsamp, const float* geom, const float* r, const float* zb,
+                      const float* params, float* loss, float* grad) {
+    if (!c || nsamp < 1 || !geom || !r || !zb) return IBG_ERR_ARG;
+    if (lpc_ensure(c)) return IBG_ERR_CUDA;
+    const int P = c->npts, m = c->ncomp;
+    const size_t np = lpc_num_params();
+    float *dg = nullptr, *dr = nullptr, *dzb = nullptr, *dt = nullptr, *dl = nullptr, *dgrad = nullptr;
+    if (c->alloc(&dg, (size_t)nsamp * 4 * P) || c->alloc(&dr, (size_t)nsamp * m) || c->alloc(&dzb, (size_t)nsamp * m) ||
+        c->alloc(&dt, (size_t)nsamp * m) || c->alloc(&dl, nsamp) || c->alloc(&dgrad, np))
+        return IBG_ERR_CUDA;
+    if (params) cudaMemcpy(c->lpc.params, params, sizeof(float) * np, cudaMemcpyHostToDevice);
+    cudaMemcpy(dg, geom, sizeof(float) * (size_t)nsamp * 4 * P, cudaMemcpyHostToDevice);
+    cudaMemcpy(dr, r, sizeof(float) * (size_t)nsamp * m, cudaMemcpyHostToDevice);
+    cudaMemcpy(dzb, zb, sizeof(float) * (size_t)nsamp * m, cudaMemcpyHostToDevice);
+    k_lpc_targets<<<nsamp, 256, 0, c->st>>>(P, dr, dzb, dt);
+    int s = c->lpc.loss_grad(nsamp, dg, dr, dt, dl, grad ? dgrad : nullptr, c->tws, c->st);
+    std::vector<float> lh(nsamp);
+    cudaMemcpyAsync(lh.data(), dl, sizeof(float) * nsamp, cudaMemcpyDeviceToHost, c->st);
+    if (grad) cudaMemcpyAsync(grad, dgrad, sizeof(float) * np, cudaMemcpyDeviceToHost, c->st);
+    cudaStreamSynchronize(c->st);
+    if (loss) {
+        double a = 0;
+        for (float v : lh) a += v;
+        *loss = (float)(a / nsamp);
+    }
+    cudaFree(dg); cudaFree(dr); cudaFree(dzb); cudaFree(dt); cudaFree(dl); cudaFree(dgrad);
+    if (s) return s;
+    return c->cuda_check("ibg_lpc_loss_grad");
+}
+
+int ibg_lpc_train(ibg_context* c, int nsamp, const float* geom, const float* r, const float* zb, int epochs,
+                  int batch, float lr, unsigned int seed, float* loss_hist) {
+    if (!c || nsamp < 1 || epochs < 1 || batch < 1 || !geom || !r || !zb) return IBG_ERR_ARG;
+    if (lpc_ensure(c)) return IBG_ERR_CUDA;
+    const int P = c->npts, m = c->ncomp;
+    const size_t np = lpc_num_params();
+    if (batch > nsamp) batch = nsamp;
+    float *dg = nullptr, *dr = nullptr, *dt = nullptr, *dzb = nullptr, *bg = nullptr, *br = nullptr, *bt = nullptr;
+    float *dl = nullptr, *grad = nullptr, *m1 = nullptr, *m2 = nullptr;
+    int* didx = nullptr;
+    if (c->alloc(&dg, (size_t)nsamp * 4 * P) || c->alloc(&dr, (size_t)nsamp * m) || c->alloc(&dzb, (size_t)nsamp * m) ||
+        c->alloc(&dt, (size_t)nsamp * m) || c->alloc(&bg, (size_t)batch * 4 * P) || c->alloc(&br, (size_t)batch * m) ||
+        c->alloc(&bt, (size_t)batch * m) || c->alloc(&dl, batch) || c->alloc(&grad, np) || c->alloc(&m1, np) ||
+        c->alloc(&m2, np) || c->alloc(&didx, batch))
+        return IBG_ERR_CUDA;
+    cudaMemcpy(dg, geom, sizeof(float) * (size_t)nsamp * 4 * P, cudaMemcpyHostToDevice);
+    cudaMemcpy(dr, r, sizeof(float) * (size_t)nsamp * m, cudaMemcpyHostToDevice);
+    cudaMemcpy(dzb, zb, sizeof(float) * (size_t)nsamp * m, cudaMemcpyHostToDevice);
+    k_lpc_targets<<<nsamp, 256, 0, c->st>>>(P, dr, dzb, dt);
+    std::mt19937 rng(seed);
+    std::vector<int> perm(nsamp);
+    for (int i = 0; i < nsamp; ++i) perm[i] = i;
+    std::vector<float> lh(batch);
+    int step = 0, s = IBG_OK;
+    for (int ep = 0; ep < epochs && !s; ++ep) {
+        std::shuffle(perm.begin(), perm.end(), rng);
+        double acc = 0;
+        int counted = 0;
+        for (int b0 = 0; b0 + batch <= nsamp && !s; b0 += batch) {
+            cudaMemcpyAsync(didx, perm.data() + b0, sizeof(int) * batch, cudaMemcpyHostToDevice, c->st);
+            const unsigned gb = (unsigned)(((long)batch * 4 * P + 255) / 256), gm = (unsigned)(((long)batch * m + 255) / 256);
+            k_gather_rows<<<gb, 256, 0, c->st>>>(batch, 4 * P, didx, dg, bg);
+            k_gather_rows<<<gm, 256, 0, c->st>>>(batch, m, didx, dr, br);
+            k_gather_rows<<<gm, 256, 0, c->st>>>(batch, m, didx, dt, bt);
+            s = c->lpc.loss_grad(batch, bg, br, bt, dl, grad, c->tws, c->st);
+            adam_step((long)np, c->lpc.params, grad, m1, m2, lr, ++step, c->st);
+            cudaMemcpyAsync(lh.data(), dl, sizeof(float) * batch, cudaMemcpyDeviceToHost, c->st);
+            if (cudaStreamSynchronize(c->st) != cudaSuccess) s = c->cuda_check("ibg_lpc_train");
+            for (float v : lh) acc += v;
+            counted += batch;
+        }
+        if (loss_hist) loss_hist[ep] = (float)(acc / std::max(1, counted));
+    }
+    c->lpc.refresh_bf16(c->st);
+    cudaStreamSynchronize(c->st);
+    cudaFree(dg); cudaFree(dr); cudaFree(dzb); cudaFree(dt); cudaFree(bg); cudaFree(br); cudaFree(bt);
+    cudaFree(dl); cudaFree(grad); cudaFree(m1); cudaFree(m2); cudaFree(didx);
+    if (s) return s;
+    c->lpc_ready = true;
+    c->drop_graph();  // a step captured before held the identity preconditioner
+    return c->cuda_check("ibg_lpc_train");
+}
+
+int ibg_lpc_get_params(ibg_context* c, float* p, size_t n) {
+    if (!c || !p || n != lpc_num_params()) return IBG_ERR_ARG;
+    if (lpc_ensure(c)) return IBG_ERR_CUDA;
+    cudaMemcpy(p, c->lpc.params, sizeof(float) * n, cudaMemcpyDeviceToHost);
+    return c->cuda_check("ibg_lpc_get_params");
+}
+
+int ibg_lpc_set_params(ibg_context* c, const float* p, size_t n) {
+    if (!c || !p || n != lpc_num_params()) return IBG_ERR_ARG;
+    if (lpc_ensure(c)) return IBG_ERR_CUDA;
+    cudaMemcpy(c->lpc.params, p, sizeof(float) * n, cudaMemcpyHostToDevice);
+    c->lpc.refresh_bf16(c->st);
+    cudaStreamSynchronize(c->st);
+    c->lpc_ready = true;
+    c->drop_graph();
+    return c->cuda_check("ibg_lpc_set_params");
+}
+
+int ibg_lpc_apply(ibg_context* c, int k, const double* r, double* z, float* geom) {
+    if (!c || !r || !z || k < 0 || k >= c->sch.nsub) return IBG_ERR_ARG;
+    if (lpc_ensure(c)) return IBG_ERR_CUDA;
+    const int m = c->ncomp;
+    double *dr = nullptr, *dz = nullptr;
+    if (c->alloc(&dr, m) || c->alloc(&dz, m)) return IBG_ERR_CUDA;
+    cudaMemcpyAsync(dr, r, sizeof(double) * m, cudaMemcpyHostToDevice, c->st);
+    c->lpc.apply(c->d_pts, c->lb, dr, dz, c->beta[k], c->st);
+    cudaMemcpyAsync(z, dz, sizeof(double) * m, cudaMemcpyDeviceToHost, c->st);
+    if (geom) cudaMemcpyAsync(geom, c->lpc.geom, sizeof(float) * 4 * c->npts, cudaMemcpyDeviceToHost, c->st);
+    cudaStreamSynchronize(c->st);
+    cudaFree(dr);
+    cudaFree(dz);
+    return c->cuda_check("ibg_lpc_apply");
+}
+
+int ibg_substep_beta(ibg_context* c, int k, double* beta) {
+    if (!c || !beta || k < 0 || k >= c->sch.nsub) return IBG_ERR_ARG;
+    *beta = c->beta[k];
+    return IBG_OK;
+}
 
 long long ibg_run_kernel(ibg_context* c, int which, int reps) {
     if (!c || reps < 0) return IBG_ERR_ARG;

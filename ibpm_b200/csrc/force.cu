@@ -238,22 +238,29 @@ __global__ void __launch_bounds__(1024) k_pcg_begin(int m, const double* __restr
     if (threadIdx.x == 0) {
         scal[3] = rr;
         flags[1] = 0;
+        flags[8] = 0;  // preconditioner in use (no fallback yet)
     }
 }
 
-__global__ void __launch_bounds__(1024) k_pcg_begin2(int m, const double* __restrict__ r, const double* __restrict__ z,
+__global__ void __launch_bounds__(1024) k_pcg_begin2(int m, const double* __restrict__ r, double* __restrict__ z,
                                                      double* __restrict__ d, double* __restrict__ scal,
                                                      int* __restrict__ flags) {
     __shared__ double red[32];
     double part = 0.0;
-    for (int k = threadIdx.x; k < m; k += blockDim.x) {
-        d[k] = z[k];
-        part += r[k] * z[k];
-    }
+    for (int k = threadIdx.x; k < m; k += blockDim.x) part += r[k] * z[k];
     const double rz = block_sum(part, red);
+    // a preconditioner that is not positive on the first residual: plain CG from the start
+    const bool fallback = !(rz > 0.0);
+    for (int k = threadIdx.x; k < m; k += blockDim.x) {
+        const double v = fallback ? r[k] : z[k];
+        z[k] = v;
+        d[k] = v;
+    }
     if (threadIdx.x == 0) {
-        scal[0] = rz;
-        flags[0] = (scal[3] > scal[2] && flags[2] > 0 && rz > 0.0) ? 1 : 0;
+        const double rr = scal[3];
+        scal[0] = fallback ? rr : rz;
+        flags[8] = fallback ? 1 : 0;
+        flags[0] = (rr > scal[2] && flags[2] > 0 && rr == rr) ? 1 : 0;
     }
 }
 
@@ -279,26 +286,48 @@ __global__ void __launch_bounds__(1024) k_pcg_step1(int m, double* __restrict__ 
     if (threadIdx.x == 0) scal[3] = rr;
 }
 
-__global__ void __launch_bounds__(1024) k_pcg_step2(int m, const double* __restrict__ r, const double* __restrict__ z,
+__global__ void __launch_bounds__(1024) k_pcg_step2(int m, const double* __restrict__ r, double* __restrict__ z,
                                                     const double* __restrict__ zold, double* __restrict__ d,
                                                     double* __restrict__ scal, int* __restrict__ flags) {
     __shared__ double red[32];
+    __shared__ int restart;
     if (flags[0] == 0) return;
-    double p1 = 0.0, p2 = 0.0;
+    double p1 = 0.0, p2 = 0.0, p3 = 0.0;
     for (int k = threadIdx.x; k < m; k += blockDim.x) {
         p1 += r[k] * z[k];
         p2 += r[k] * zold[k];
+        p3 += r[k] * r[k];
     }
     const double rz = block_sum(p1, red);
     const double rzo = block_sum(p2, red);
+    const double rr = block_sum(p3, red);
+    const int it = flags[1] + 1;
+    if (threadIdx.x == 0) {
+        // fall back to plain CG (restart with d = r) when the preconditioner is not
+        // positive on r or has not converged within its iteration budget
+        restart = (flags[8] == 0 && (!(rz > 0.0) || it >= flags[9])) ? 1 : 0;
+    }
+    __syncthreads();
+    if (restart) {
+        for (int k = threadIdx.x; k < m; k += blockDim.x) {
+            z[k] = r[k];
+            d[k] = r[k];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            flags[8] = 1;
+            scal[0] = rr;
+            flags[1] = it;
+            flags[0] = (rr > scal[2] && it < flags[2] && rr == rr) ? 1 : 0;
+        }
+        return;
+    }
     const double beta = (rz - rzo) / scal[0];  // Polak-Ribiere
     for (int k = threadIdx.x; k < m; k += blockDim.x) d[k] = z[k] + beta * d[k];
     __syncthreads();
     if (threadIdx.x == 0) {
         scal[0] = rz;
-        const int it = flags[1] + 1;
         flags[1] = it;
-        const double rr = scal[3];
         flags[0] = (rr > scal[2] && it < flags[2] && rz > 0.0 && rr == rr) ? 1 : 0;
     }
 }
@@ -370,14 +399,14 @@ void cg_update(int m, double* x, double* r, double* d, const double* q, double* 
 void pcg_begin(int m, const double* b, const double* Mx, double* r, double* scal, int* flags, cudaStream_t st) {
     k_pcg_begin<<<1, 1024, 0, st>>>(m, b, Mx, r, scal, flags);
 }
-void pcg_begin2(int m, const double* r, const double* z, double* d, double* scal, int* flags, cudaStream_t st) {
+void pcg_begin2(int m, const double* r, double* z, double* d, double* scal, int* flags, cudaStream_t st) {
     k_pcg_begin2<<<1, 1024, 0, st>>>(m, r, z, d, scal, flags);
 }
 void pcg_step1(int m, double* x, double* r, const double* d, const double* q, const double* z, double* zold,
                double* scal, int* flags, cudaStream_t st) {
     k_pcg_step1<<<1, 1024, 0, st>>>(m, x, r, d, q, z, zold, scal, flags);
 }
-void pcg_step2(int m, const double* r, const double* z, const double* zold, double* d, double* scal, int* flags,
+void pcg_step2(int m, const double* r, double* z, const double* zold, double* d, double* scal, int* flags,
                cudaStream_t st) {
     k_pcg_step2<<<1, 1024, 0, st>>>(m, r, z, zold, d, scal, flags);
 }

@@ -13,10 +13,10 @@ void cg_begin(int m, const double* b, const double* Mx, double* r, double* d, do
               cudaStream_t st);
 void cg_update(int m, double* x, double* r, double* d, const double* q, double* scal, int* flags, cudaStream_t st);
 void pcg_begin(int m, const double* b, const double* Mx, double* r, double* scal, int* flags, cudaStream_t st);
-void pcg_begin2(int m, const double* r, const double* z, double* d, double* scal, int* flags, cudaStream_t st);
+void pcg_begin2(int m, const double* r, double* z, double* d, double* scal, int* flags, cudaStream_t st);
 void pcg_step1(int m, double* x, double* r, const double* d, const double* q, const double* z, double* zold,
                double* scal, int* flags, cudaStream_t st);
-void pcg_step2(int m, const double* r, const double* z, const double* zold, double* d, double* scal, int* flags,
+void pcg_step2(int m, const double* r, double* z, const double* zold, double* d, double* scal, int* flags,
                cudaStream_t st);
 void net_force(int npts, const double* f, double dx2, double* out, cudaStream_t st);
 void add_time(double* t, double dt, cudaStream_t st);

@@ -73,6 +73,8 @@ typedef struct {
     int pc_refresh;         /* steps between rebuilds of the Cholesky preconditioner (default 10) */
     int cg_graph;           /* moving bodies: 1 = the whole step, CG loop included, is one CUDA graph
                                (the loop is a device-side WHILE node), 0 = host-driven CG loop */
+    int pc_fallback_iter;   /* LEARNED: iterations after which the solve restarts as plain CG
+                               (also when r.z <= 0); <= 0 means cg_max_iter */
 } ibg_params;
 
 /* preconditioners of the moving-body force solve (all keep the reference's
@@ -157,6 +159,34 @@ IBG_API void* ibg_ensemble_stream(const ibg_ensemble* ens);
 IBG_API long long ibg_ensemble_launches_per_step(const ibg_ensemble* ens);
 IBG_API const char* ibg_ensemble_last_error(const ibg_ensemble* ens);
 
+/* --- learned preconditioner (no reference counterpart) -----------------------
+ * A network over the boundary points approximating z = M^-1 r (lpc.cu): per
+ * point the position about the body centroid, the unit normal and the
+ * residual over its rms, averaged with 8 boundary neighbours, a 3-layer MLP of
+ * width 256, output scaled by rms(r)/beta.  ibg_lpc_generate produces training
+ * pairs from the solver itself: body configurations at nconfig times in
+ * [t0, t1], nres residuals each (white and boundary-smooth), targets
+ * zb = beta_k M_k^-1 r from the exact Cholesky operator.  Arrays are float,
+ * sample-major: geom [nsamp][npts][4], r and zb [nsamp][2 npts] with
+ * nsamp = nconfig * nres.  ibg_lpc_train fits the network (Adam, FP32) and
+ * enables it for IBG_PRECOND_LEARNED (BF16 inference).  ibg_lpc_loss_grad gives
+ * the mean loss and its gradient (for checking against a CPU restatement). */
+IBG_API size_t ibg_lpc_num_params(void);
+IBG_API int ibg_lpc_generate(ibg_context* ctx, int nconfig, double t0, double t1, int nres, unsigned int seed,
+                             float* geom, float* r, float* zb);
+IBG_API int ibg_lpc_train(ibg_context* ctx, int nsamp, const float* geom, const float* r, const float* zb, int epochs,
+                          int batch, float lr, unsigned int seed, float* loss_history);
+IBG_API int ibg_lpc_loss_grad(ibg_context* ctx, int nsamp, const float* geom, const float* r, const float* zb,
+                              const float* params, float* loss, float* grad);
+IBG_API int ibg_lpc_get_params(ibg_context* ctx, float* params, size_t n);
+IBG_API int ibg_lpc_set_params(ibg_context* ctx, const float* params, size_t n);
+/* z = P_k r with the current network at the current body configuration (host
+ * buffers of 2 npts doubles); geom (optional, npts x 4 floats) receives the
+ * geometry features it used */
+IBG_API int ibg_lpc_apply(ibg_context* ctx, int substep, const double* r, double* z, float* geom);
+/* beta_k of sub-step k (M_k = beta_k C A_k^-1 B, src/ProjectionSolver.cc:43-55) */
+IBG_API int ibg_substep_beta(ibg_context* ctx, int substep, double* beta);
+
 /* --- operator entry points (host buffers, reference layouts) ----------------- */
 /* PoissonSolver::solve (src/EllipticSolver.cc:47-73, :83-94): L u = f on all levels */
 IBG_API int ibg_poisson_solve(ibg_context* ctx, const double* f, double* u);
@@ -184,7 +214,8 @@ IBG_API int ibg_projection_solve(ibg_context* ctx, int substep, const double* a,
  * ibg_poisson_solve_static solves L u = f on all levels, like ibg_poisson_solve,
  * but takes DEVICE pointers f and u (reference Scalar layout), needs no context
  * and allocates nothing: its scratch is a file-scope device array of 4 MiB
- * (524288 doubles, enough for (ngrid+1)*(nx-1)*(ny-1) <= 524288) plus ~160 KiB
+ * (524288 doubles; a solve needs 2*ngrid*(nx-1)*(ny-1) + 2*(ngrid+1)*(nx+ny-2)
+ * of them) plus ~160 KiB
  * of tables (nx, ny <= 2048), held by every GPU that loads the library until the
  * process exits.  Larger grids are rejected with IBG_ERR_UNSUPPORTED.  The first
  * call on a device resolves the arrays' device addresses (cudaGetSymbolAddress)

@@ -34,7 +34,7 @@ def test_create_without_gpu_fails_cleanly():
     g = _native.ibg_grid(16, 16, 1, 1.0, -0.5, -0.5)
     xy = (ctypes.c_double * 2)(0.0, 0.0)
     b = _native.ibg_body(1, ctypes.cast(xy, ctypes.POINTER(ctypes.c_double)), 0.0, 0.0, 0)
-    p = _native.ibg_params(100.0, 0.01, 2, 1e-7, 100, 1.0, 0.0, 0, -1, 0, 10, 1)
+    p = _native.ibg_params(100.0, 0.01, 2, 1e-7, 100, 1.0, 0.0, 0, -1, 0, 10, 1, 0)
     h = ctypes.c_void_p()
     st = L.ibg_create(ctypes.byref(g), 1, ctypes.byref(b), ctypes.byref(p), None, ctypes.byref(h))
     assert st < 0
