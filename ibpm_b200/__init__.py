@@ -231,33 +231,34 @@ class NonlinearIBSolver:
         return int(lib().ibg_last_launch_count(self._h))
 
     # -- learned preconditioner (no reference counterpart) -----------------
-    def lpc_generate(self, nconfig: int, t0: float, t1: float, nres: int, seed: int = 0):
-        """Training pairs from this solver: geometry [n, npts, 4], residuals r and
-        targets beta M^-1 r [n, 2 npts] (float32), n = nconfig * nres."""
-        n, P = nconfig * nres, self.npoints
-        geom = np.zeros((n, P, 4), np.float32)
-        r = np.zeros((n, 2 * P), np.float32)
-        zb = np.zeros((n, 2 * P), np.float32)
-        check(lib().ibg_lpc_generate(self._h, int(nconfig), float(t0), float(t1), int(nres), int(seed),
-                                     _ptr(geom), _ptr(r), _ptr(zb)), self._h)
-        return geom, r, zb
+    def lpc_generate(self, nconfig: int, t0: float, t1: float):
+        """Training data from this solver's exact force operator: geometry
+        features [nconfig, npts, 4] and M / beta [nconfig, m, m] (float32) at
+        nconfig body configurations evenly spread over [t0, t1]."""
+        P = self.npoints
+        m = 2 * P
+        geom = np.zeros((nconfig, P, 4), np.float32)
+        mb = np.zeros((nconfig, m, m), np.float32)
+        check(lib().ibg_lpc_generate(self._h, int(nconfig), float(t0), float(t1), _ptr(geom), _ptr(mb)), self._h)
+        return geom, mb
 
-    def lpc_train(self, geom, r, zb, epochs: int = 20, batch: int = 32, lr: float = 1e-3, seed: int = 0):
+    def lpc_train(self, geom, mb, epochs: int = 200, batch: int = 4, lr: float = 1e-3, seed: int = 0):
         """Fit the network on the device (Adam, FP32) and enable it; returns the
         mean loss of every epoch."""
-        geom, r, zb = (np.ascontiguousarray(a, dtype=np.float32) for a in (geom, r, zb))
+        geom, mb = (np.ascontiguousarray(a, dtype=np.float32) for a in (geom, mb))
         hist = np.zeros(epochs, np.float32)
-        check(lib().ibg_lpc_train(self._h, int(r.shape[0]), _ptr(geom), _ptr(r), _ptr(zb), int(epochs), int(batch),
+        check(lib().ibg_lpc_train(self._h, int(mb.shape[0]), _ptr(geom), _ptr(mb), int(epochs), int(batch),
                                   ctypes.c_float(lr), int(seed), _ptr(hist)), self._h)
         return hist
 
-    def lpc_loss_grad(self, geom, r, zb, params=None):
-        """Mean loss and its gradient over the given samples (params: None keeps the current ones)."""
-        geom, r, zb = (np.ascontiguousarray(a, dtype=np.float32) for a in (geom, r, zb))
+    def lpc_loss_grad(self, geom, mb, params=None):
+        """Mean loss and its gradient over the given configurations (params:
+        None keeps the current ones)."""
+        geom, mb = (np.ascontiguousarray(a, dtype=np.float32) for a in (geom, mb))
         pp = None if params is None else np.ascontiguousarray(params, dtype=np.float32)
         grad = np.zeros(int(lib().ibg_lpc_num_params()), np.float32)
         loss = ctypes.c_float()
-        check(lib().ibg_lpc_loss_grad(self._h, int(r.shape[0]), _ptr(geom), _ptr(r), _ptr(zb), _ptr(pp),
+        check(lib().ibg_lpc_loss_grad(self._h, int(mb.shape[0]), _ptr(geom), _ptr(mb), _ptr(pp),
                                       ctypes.byref(loss), _ptr(grad)), self._h)
         return loss.value, grad
 

@@ -502,6 +502,12 @@ struct ibg_context {
     }
 
     int enqueue_step() {
+        if (moving && prm.cg_precond == IBG_PRECOND_LEARNED && lpc_ready) {
+            // the network's approximate inverse of M at the current body configuration
+            lpc.geometry(d_pts, lb, st);
+            lpc.operators(sch.nsub, beta, Mi, st);
+            launches += 4;
+        }
         for (int k = 0; k < sch.nsub; ++k) {
             int s = fp32 ? substep<float>(b32, k) : substep<double>(b64, k);
             if (s) return s;
@@ -540,7 +546,8 @@ struct ibg_context {
         bs_bf = bs_u = bs_p = bs_rc = bs_tb = bs_fl = bs_sw = bs_M = nullptr;
         bs_chunk = 0;
     }
-    int build_operator() {
+    // columns M_k e_j of sub-step k into bs_M (column j at bs_M + j m)
+    int build_m(int k) {
         const int m = ncomp;
         const size_t swd = sweep_doubles(g.nx, g.ny, g.L);
         if (!bs_M) {
@@ -559,26 +566,32 @@ struct ibg_context {
             }
             bs_chunk = chunk;
         }
+        const size_t chunk = bs_chunk;
+        for (int col0 = 0; col0 < m; col0 += (int)chunk) {
+            const int nb = (int)std::min(chunk, (size_t)(m - col0));
+            launch_smear_bf_unit<double>(g, m, col0, nb, slots, bs_fl, g.F1, bs_bf, S, beta[k], st);
+            SolveCall<double> h{};
+            h.f = bs_bf; h.u = bs_u; h.rc = bs_rc; h.tbuf = bs_tb; h.sweep = bs_sw; h.bstride = S;
+            h.batch = nb; h.in_scale = 1.0;
+            b64.helm[k].solve(h, st);
+            SolveCall<double> pc{};
+            pc.f = bs_u; pc.u = bs_p; pc.rc = bs_rc; pc.tbuf = bs_tb; pc.sweep = bs_sw; pc.bstride = S;
+            pc.batch = nb; pc.in_scale = -1.0;
+            b64.poisson.solve(pc, st);
+            launch_reg_interp<double>(g, m, slots, bs_p, S, nb, nullptr, bs_M + (size_t)col0 * m, (size_t)m, st);
+        }
+        return IBG_OK;
+    }
+    int build_operator() {
+        const int m = ncomp;
         for (int k = 0; k < sch.nsub; ++k)
             if (!Lr[k] && (alloc(&Lr[k], (size_t)m * m, false) || alloc(&Lc[k], (size_t)m * m, false) ||
                            alloc(&Ld[k], (size_t)m, false) || alloc(&Mi[k], (size_t)m * m, false)))
                 return fail(IBG_ERR_CUDA, "not enough device memory for the Cholesky factors");
-        const size_t chunk = bs_chunk;
         int s = IBG_OK;
         for (int k = 0; k < sch.nsub && !s; ++k) {
-            for (int col0 = 0; col0 < m; col0 += (int)chunk) {
-                const int nb = (int)std::min(chunk, (size_t)(m - col0));
-                launch_smear_bf_unit<double>(g, m, col0, nb, slots, bs_fl, g.F1, bs_bf, S, beta[k], st);
-                SolveCall<double> h{};
-                h.f = bs_bf; h.u = bs_u; h.rc = bs_rc; h.tbuf = bs_tb; h.sweep = bs_sw; h.bstride = S;
-                h.batch = nb; h.in_scale = 1.0;
-                b64.helm[k].solve(h, st);
-                SolveCall<double> pc{};
-                pc.f = bs_u; pc.u = bs_p; pc.rc = bs_rc; pc.tbuf = bs_tb; pc.sweep = bs_sw; pc.bstride = S;
-                pc.batch = nb; pc.in_scale = -1.0;
-                b64.poisson.solve(pc, st);
-                launch_reg_interp<double>(g, m, slots, bs_p, S, nb, nullptr, bs_M + (size_t)col0 * m, (size_t)m, st);
-            }
+            s = build_m(k);
+            if (s) break;
             s = chol_factor(m, bs_M, Lr[k], Lc[k], Ld[k], d_status, st);
             if (!s) chol_inverse(m, Lr[k], Lc[k], Ld[k], Mi[k], st);
             int hs = 0;
@@ -648,9 +661,9 @@ __global__ void k_fallback_identity(int m, const int* __restrict__ flags, const 
 
 void ibg_context::apply_learned_precond(int k, const double* r, double* z) {
     if (lpc_ready) {
-        lpc.apply(d_pts, lb, r, z, beta[k], st);
+        minv_apply(ncomp, Mi[k], r, z, st);
         k_fallback_identity<<<(ncomp + 255) / 256, 256, 0, st>>>(ncomp, cg_flags, r, z);
-        launches += 5;
+        launches += 2;
     } else {
         // no network yet: identity (plain CG directions)
         cudaMemcpyAsync(z, r, sizeof(double) * ncomp, cudaMemcpyDeviceToDevice, st);
@@ -1380,27 +1393,11 @@ const char* ibg_ensemble_last_error(const ibg_ensemble* e) { return e ? e->err.c
 // learned preconditioner: data from the solver, training, parameters
 // ---------------------------------------------------------------------------
 namespace ibg {
-__global__ void k_lpc_targets(int P, const float* __restrict__ r, const float* __restrict__ zb, float* __restrict__ t) {
-    __shared__ float red[32];
-    const int b = blockIdx.x;
-    float acc = 0.f;
-    for (int k = threadIdx.x; k < 2 * P; k += blockDim.x) {
-        const float v = r[(size_t)b * 2 * P + k];
-        acc += v * v;
-    }
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    float tot = 0.f;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
-    const float s = sqrtf(tot / (2 * P)) + 1e-30f;
-    for (int k = threadIdx.x; k < 2 * P; k += blockDim.x) t[(size_t)b * 2 * P + k] = zb[(size_t)b * 2 * P + k] / s;
-}
-__global__ void k_gather_rows(int nrows, int width, const int* __restrict__ idx, const float* __restrict__ src,
+__global__ void k_gather_rows(int nrows, long width, const int* __restrict__ idx, const float* __restrict__ src,
                               float* __restrict__ dst) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)nrows * width) return;
-    const int r = (int)(t / width), c = (int)(t % width);
+    const long r = t / width, c = t % width;
     dst[t] = src[(size_t)idx[r] * width + c];
 }
 }  // namespace ibg
@@ -1408,166 +1405,151 @@ __global__ void k_gather_rows(int nrows, int width, const int* __restrict__ idx,
 static int lpc_ensure(ibg_context* c) {
     if (c->lpc.params) return IBG_OK;
     if (c->lpc.init(c->npts, c->h_nbr, c->h_cnt)) return c->fail(IBG_ERR_CUDA, "learned preconditioner set-up failed");
+    if (c->prm.cg_precond == IBG_PRECOND_LEARNED)
+        for (int k = 0; k < c->sch.nsub; ++k)
+            if (!c->Mi[k] && c->alloc(&c->Mi[k], (size_t)c->ncomp * c->ncomp)) return IBG_ERR_CUDA;
     return IBG_OK;
 }
 
 size_t ibg_lpc_num_params(void) { return lpc_num_params(); }
 
-int ibg_lpc_generate(ibg_context* c, int nconfig, double t0, double t1, int nres, unsigned int seed, float* geom,
-                     float* r_out, float* zb_out) {
-    if (!c || nconfig < 1 || nres < 1 || !geom || !r_out || !zb_out) return IBG_ERR_ARG;
+int ibg_lpc_generate(ibg_context* c, int nconfig, double t0, double t1, float* geom, float* mb) {
+    if (!c || nconfig < 1 || !geom || !mb) return IBG_ERR_ARG;
     if (lpc_ensure(c)) return IBG_ERR_CUDA;
-    const int P = c->npts, m = c->ncomp;
-    std::mt19937 rng(seed);
-    std::normal_distribution<double> nd(0.0, 1.0);
-    std::vector<double> r((size_t)nres * m), z((size_t)nres * m);
-    std::vector<float> gh((size_t)P * 4);
-    double* dr = nullptr;
-    double* dz = nullptr;
-    if (c->alloc(&dr, (size_t)nres * m) || c->alloc(&dz, (size_t)nres * m)) return IBG_ERR_CUDA;
+    const int P = c->npts, m = c->ncomp, k = c->sch.nsub - 1;
+    std::vector<double> Mh((size_t)m * m);
     const double keep_time = c->time;
     int status = IBG_OK;
     for (int cf = 0; cf < nconfig && !status; ++cf) {
         const double t = nconfig == 1 ? t0 : t0 + (t1 - t0) * cf / (nconfig - 1);
         cudaMemcpyAsync(c->d_time, &t, sizeof(double), cudaMemcpyHostToDevice, c->st);
         c->move_bodies(0.0);
-        status = c->build_operator();
+        status = c->build_m(k);
         if (status) break;
-        c->lpc.apply(c->d_pts, c->lb, c->btmp, c->rhsb, 1.0, c->st);  // computes the geometry features
-        cudaMemcpyAsync(gh.data(), c->lpc.geom, sizeof(float) * 4 * P, cudaMemcpyDeviceToHost, c->st);
-        // residuals: white N(0,1) and boundary-smooth random modes, alternately
-        for (int j = 0; j < nres; ++j) {
-            double* rj = r.data() + (size_t)j * m;
-            if (j % 2 == 0) {
-                for (int q = 0; q < m; ++q) rj[q] = nd(rng);
-            } else {
-                double a[2][4], bcoef[2][4];
-                for (int cc = 0; cc < 2; ++cc)
-                    for (int q = 0; q < 4; ++q) {
-                        a[cc][q] = nd(rng);
-                        bcoef[cc][q] = nd(rng);
-                    }
-                for (int i = 0; i < P; ++i) {
-                    const double sarc = (double)i / P;
-                    for (int cc = 0; cc < 2; ++cc) {
-                        double v = 0.1 * nd(rng);
-                        for (int q = 0; q < 4; ++q)
-                            v += a[cc][q] * sin(M_PI * (q + 1) * sarc) + bcoef[cc][q] * cos(M_PI * (q + 1) * sarc);
-                        rj[cc * P + i] = v;
-                    }
-                }
-            }
+        c->lpc.geometry(c->d_pts, c->lb, c->st);
+        cudaMemcpyAsync(geom + (size_t)cf * 4 * P, c->lpc.geom, sizeof(float) * 4 * P, cudaMemcpyDeviceToHost, c->st);
+        cudaMemcpyAsync(Mh.data(), c->bs_M, sizeof(double) * Mh.size(), cudaMemcpyDeviceToHost, c->st);
+        if (cudaStreamSynchronize(c->st) != cudaSuccess) {
+            status = c->cuda_check("ibg_lpc_generate");
+            break;
         }
-        cudaMemcpyAsync(dr, r.data(), sizeof(double) * r.size(), cudaMemcpyHostToDevice, c->st);
-        for (int j = 0; j < nres; ++j) {
-            const int k = j % c->sch.nsub;
-            minv_apply(m, c->Mi[k], dr + (size_t)j * m, dz + (size_t)j * m, c->st);
-        }
-        cudaMemcpyAsync(z.data(), dz, sizeof(double) * z.size(), cudaMemcpyDeviceToHost, c->st);
-        if (cudaStreamSynchronize(c->st) != cudaSuccess) status = c->cuda_check("ibg_lpc_generate");
-        for (int j = 0; j < nres; ++j) {
-            const int k = j % c->sch.nsub;
-            const size_t sidx = (size_t)cf * nres + j;
-            std::memcpy(geom + sidx * 4 * P, gh.data(), sizeof(float) * 4 * P);
-            for (int q = 0; q < m; ++q) {
-                r_out[sidx * m + q] = (float)r[(size_t)j * m + q];
-                zb_out[sidx * m + q] = (float)(c->beta[k] * z[(size_t)j * m + q]);
-            }
-        }
+        // bs_M holds column j of M at j m: M[i][j] = Mh[j m + i]
+        float* out = mb + (size_t)cf * m * m;
+        for (int i = 0; i < m; ++i)
+            for (int j = 0; j < m; ++j) out[(size_t)i * m + j] = (float)(Mh[(size_t)j * m + i] / c->beta[k]);
     }
-    cudaFree(dr);
-    cudaFree(dz);
     // back to the current configuration
     cudaMemcpyAsync(c->d_time, &keep_time, sizeof(double), cudaMemcpyHostToDevice, c->st);
     c->move_bodies(0.0);
-    if (c->prm.cg_precond == IBG_PRECOND_CHOLESKY) {
-        int s2 = c->build_operator();
-        if (!status) status = s2;
-    }
     if (cudaStreamSynchronize(c->st) != cudaSuccess && !status) status = c->cuda_check("ibg_lpc_generate");
     return status;
 }
 
-int ibg_lpc_loss_grad(ibg_context* c, int nsamp, const float* geom, const float* r, const float* zb,
-                      const float* params, float* loss, float* grad) {
-    if (!c || nsamp < 1 || !geom || !r || !zb) return IBG_ERR_ARG;
-    if (lpc_ensure(c)) return IBG_ERR_CUDA;
-    const int P = c->npts, m = c->ncomp;
-    const size_t np = lpc_num_params();
-    float *dg = nullptr, *dr = nullptr, *dzb = nullptr, *dt = nullptr, *dl = nullptr, *dgrad = nullptr;
-    if (c->alloc(&dg, (size_t)nsamp * 4 * P) || c->alloc(&dr, (size_t)nsamp * m) || c->alloc(&dzb, (size_t)nsamp * m) ||
-        c->alloc(&dt, (size_t)nsamp * m) || c->alloc(&dl, nsamp) || c->alloc(&dgrad, np))
-        return IBG_ERR_CUDA;
-    if (params) cudaMemcpy(c->lpc.params, params, sizeof(float) * np, cudaMemcpyHostToDevice);
-    cudaMemcpy(dg, geom, sizeof(float) * (size_t)nsamp * 4 * P, cudaMemcpyHostToDevice);
-    cudaMemcpy(dr, r, sizeof(float) * (size_t)nsamp * m, cudaMemcpyHostToDevice);
-    cudaMemcpy(dzb, zb, sizeof(float) * (size_t)nsamp * m, cudaMemcpyHostToDevice);
-    k_lpc_targets<<<nsamp, 256, 0, c->st>>>(P, dr, dzb, dt);
-    int s = c->lpc.loss_grad(nsamp, dg, dr, dt, dl, grad ? dgrad : nullptr, c->tws, c->st);
-    std::vector<float> lh(nsamp);
-    cudaMemcpyAsync(lh.data(), dl, sizeof(float) * nsamp, cudaMemcpyDeviceToHost, c->st);
-    if (grad) cudaMemcpyAsync(grad, dgrad, sizeof(float) * np, cudaMemcpyDeviceToHost, c->st);
-    cudaStreamSynchronize(c->st);
-    if (loss) {
-        double a = 0;
-        for (float v : lh) a += v;
-        *loss = (float)(a / nsamp);
+// device copies of a training set
+struct LpcData {
+    float* g = nullptr;
+    float* mb = nullptr;
+    void release() {
+        if (g) cudaFree(g);
+        if (mb) cudaFree(mb);
+        g = mb = nullptr;
     }
-    cudaFree(dg); cudaFree(dr); cudaFree(dzb); cudaFree(dt); cudaFree(dl); cudaFree(dgrad);
-    if (s) return s;
+};
+
+static int lpc_upload(ibg_context* c, int n, const float* geom, const float* mb, LpcData& d) {
+    const size_t P = c->npts, m = c->ncomp;
+    if (c->alloc(&d.g, n * 4 * P, false) || c->alloc(&d.mb, n * m * m, false)) return IBG_ERR_CUDA;
+    cudaMemcpy(d.g, geom, sizeof(float) * n * 4 * P, cudaMemcpyHostToDevice);
+    cudaMemcpy(d.mb, mb, sizeof(float) * n * m * m, cudaMemcpyHostToDevice);
+    return IBG_OK;
+}
+
+int ibg_lpc_loss_grad(ibg_context* c, int nconfig, const float* geom, const float* mb, const float* params,
+                      float* loss, float* grad) {
+    if (!c || nconfig < 1 || !geom || !mb) return IBG_ERR_ARG;
+    if (lpc_ensure(c)) return IBG_ERR_CUDA;
+    const size_t np = lpc_num_params();
+    LpcData d;
+    float* dgrad = nullptr;
+    if (lpc_upload(c, nconfig, geom, mb, d) || (grad && c->alloc(&dgrad, np))) {
+        d.release();
+        return IBG_ERR_CUDA;
+    }
+    if (params) {
+        cudaMemcpy(c->lpc.params, params, sizeof(float) * np, cudaMemcpyHostToDevice);
+        c->lpc.refresh_bf16(c->st);
+    }
+    float l = 0.f;
+    int s = c->lpc.loss_grad(nconfig, d.g, d.mb, &l, dgrad, c->tws, c->st);
+    if (!s && grad) cudaMemcpy(grad, dgrad, sizeof(float) * np, cudaMemcpyDeviceToHost);
+    if (loss) *loss = l;
+    d.release();
+    if (dgrad) cudaFree(dgrad);
+    if (s) return c->fail(s, "ibg_lpc_loss_grad: training work arrays");
     return c->cuda_check("ibg_lpc_loss_grad");
 }
 
-int ibg_lpc_train(ibg_context* c, int nsamp, const float* geom, const float* r, const float* zb, int epochs,
-                  int batch, float lr, unsigned int seed, float* loss_hist) {
-    if (!c || nsamp < 1 || epochs < 1 || batch < 1 || !geom || !r || !zb) return IBG_ERR_ARG;
+int ibg_lpc_train(ibg_context* c, int nconfig, const float* geom, const float* mb, int epochs, int batch, float lr,
+                  unsigned int seed, float* loss_hist) {
+    if (!c || nconfig < 1 || epochs < 1 || batch < 1 || !geom || !mb || !(lr > 0.f)) return IBG_ERR_ARG;
     if (lpc_ensure(c)) return IBG_ERR_CUDA;
     const int P = c->npts, m = c->ncomp;
     const size_t np = lpc_num_params();
-    if (batch > nsamp) batch = nsamp;
-    float *dg = nullptr, *dr = nullptr, *dt = nullptr, *dzb = nullptr, *bg = nullptr, *br = nullptr, *bt = nullptr;
-    float *dl = nullptr, *grad = nullptr, *m1 = nullptr, *m2 = nullptr;
+    if (batch > nconfig) batch = nconfig;
+    // operator scale c0: mean diagonal of M / beta over the data (stored after the weights)
+    double dsum = 0.0;
+    for (int cf = 0; cf < nconfig; ++cf)
+        for (int i = 0; i < m; ++i) dsum += mb[(size_t)cf * m * m + (size_t)i * m + i];
+    const float c0 = (float)(dsum / ((double)nconfig * m));
+    if (!(c0 > 0.f)) return c->fail(IBG_ERR_ARG, "ibg_lpc_train: the operators' diagonal is not positive");
+    cudaMemcpy(c->lpc.params + (np - 1), &c0, sizeof(float), cudaMemcpyHostToDevice);
+    LpcData d;
+    float *bg = nullptr, *bm = nullptr, *grad = nullptr, *m1 = nullptr, *m2 = nullptr;
     int* didx = nullptr;
-    if (c->alloc(&dg, (size_t)nsamp * 4 * P) || c->alloc(&dr, (size_t)nsamp * m) || c->alloc(&dzb, (size_t)nsamp * m) ||
-        c->alloc(&dt, (size_t)nsamp * m) || c->alloc(&bg, (size_t)batch * 4 * P) || c->alloc(&br, (size_t)batch * m) ||
-        c->alloc(&bt, (size_t)batch * m) || c->alloc(&dl, batch) || c->alloc(&grad, np) || c->alloc(&m1, np) ||
-        c->alloc(&m2, np) || c->alloc(&didx, batch))
+    auto cleanup = [&]() {
+        d.release();
+        float* f[] = {bg, bm, grad, m1, m2};
+        for (float* x : f)
+            if (x) cudaFree(x);
+        if (didx) cudaFree(didx);
+    };
+    if (lpc_upload(c, nconfig, geom, mb, d) || c->alloc(&bg, (size_t)batch * 4 * P) ||
+        c->alloc(&bm, (size_t)batch * m * m) || c->alloc(&grad, np) || c->alloc(&m1, np) || c->alloc(&m2, np) ||
+        c->alloc(&didx, batch)) {
+        cleanup();
         return IBG_ERR_CUDA;
-    cudaMemcpy(dg, geom, sizeof(float) * (size_t)nsamp * 4 * P, cudaMemcpyHostToDevice);
-    cudaMemcpy(dr, r, sizeof(float) * (size_t)nsamp * m, cudaMemcpyHostToDevice);
-    cudaMemcpy(dzb, zb, sizeof(float) * (size_t)nsamp * m, cudaMemcpyHostToDevice);
-    k_lpc_targets<<<nsamp, 256, 0, c->st>>>(P, dr, dzb, dt);
+    }
     std::mt19937 rng(seed);
-    std::vector<int> perm(nsamp);
-    for (int i = 0; i < nsamp; ++i) perm[i] = i;
-    std::vector<float> lh(batch);
+    std::vector<int> perm(nconfig);
+    for (int i = 0; i < nconfig; ++i) perm[i] = i;
     int step = 0, s = IBG_OK;
+    const int total = epochs * (nconfig / batch);
     for (int ep = 0; ep < epochs && !s; ++ep) {
         std::shuffle(perm.begin(), perm.end(), rng);
         double acc = 0;
-        int counted = 0;
-        for (int b0 = 0; b0 + batch <= nsamp && !s; b0 += batch) {
+        int nb = 0;
+        for (int b0 = 0; b0 + batch <= nconfig && !s; b0 += batch) {
             cudaMemcpyAsync(didx, perm.data() + b0, sizeof(int) * batch, cudaMemcpyHostToDevice, c->st);
-            const unsigned gb = (unsigned)(((long)batch * 4 * P + 255) / 256), gm = (unsigned)(((long)batch * m + 255) / 256);
-            k_gather_rows<<<gb, 256, 0, c->st>>>(batch, 4 * P, didx, dg, bg);
-            k_gather_rows<<<gm, 256, 0, c->st>>>(batch, m, didx, dr, br);
-            k_gather_rows<<<gm, 256, 0, c->st>>>(batch, m, didx, dt, bt);
-            s = c->lpc.loss_grad(batch, bg, br, bt, dl, grad, c->tws, c->st);
-            adam_step((long)np, c->lpc.params, grad, m1, m2, lr, ++step, c->st);
-            cudaMemcpyAsync(lh.data(), dl, sizeof(float) * batch, cudaMemcpyDeviceToHost, c->st);
-            if (cudaStreamSynchronize(c->st) != cudaSuccess) s = c->cuda_check("ibg_lpc_train");
-            for (float v : lh) acc += v;
-            counted += batch;
+            const long wg = 4L * P, wm = (long)m * m;
+            k_gather_rows<<<(unsigned)((batch * wg + 255) / 256), 256, 0, c->st>>>(batch, wg, didx, d.g, bg);
+            k_gather_rows<<<(unsigned)((batch * wm + 255) / 256), 256, 0, c->st>>>(batch, wm, didx, d.mb, bm);
+            float l = 0.f;
+            s = c->lpc.loss_grad(batch, bg, bm, &l, grad, c->tws, c->st);
+            if (s) break;
+            // cosine learning-rate decay to lr / 20; c0 stays fixed
+            const float lr_t = lr * (0.05f + 0.95f * 0.5f * (1.f + std::cos(3.14159265f * step / std::max(1, total))));
+            adam_step((long)np - 1, c->lpc.params, grad, m1, m2, lr_t, ++step, c->st);
+            acc += l;
+            ++nb;
         }
-        if (loss_hist) loss_hist[ep] = (float)(acc / std::max(1, counted));
+        if (loss_hist) loss_hist[ep] = (float)(acc / std::max(1, nb));
     }
     c->lpc.refresh_bf16(c->st);
-    cudaStreamSynchronize(c->st);
-    cudaFree(dg); cudaFree(dr); cudaFree(dzb); cudaFree(dt); cudaFree(bg); cudaFree(br); cudaFree(bt);
-    cudaFree(dl); cudaFree(grad); cudaFree(m1); cudaFree(m2); cudaFree(didx);
-    if (s) return s;
+    if (cudaStreamSynchronize(c->st) != cudaSuccess && !s) s = c->cuda_check("ibg_lpc_train");
+    cleanup();
+    if (s) return c->fail(s, "ibg_lpc_train failed");
     c->lpc_ready = true;
-    c->drop_graph();  // a step captured before held the identity preconditioner
+    c->drop_graph();  // a step captured before ran with the identity preconditioner
     return c->cuda_check("ibg_lpc_train");
 }
 
@@ -1594,14 +1576,23 @@ int ibg_lpc_apply(ibg_context* c, int k, const double* r, double* z, float* geom
     if (lpc_ensure(c)) return IBG_ERR_CUDA;
     const int m = c->ncomp;
     double *dr = nullptr, *dz = nullptr;
-    if (c->alloc(&dr, m) || c->alloc(&dz, m)) return IBG_ERR_CUDA;
-    cudaMemcpyAsync(dr, r, sizeof(double) * m, cudaMemcpyHostToDevice, c->st);
-    c->lpc.apply(c->d_pts, c->lb, dr, dz, c->beta[k], c->st);
-    cudaMemcpyAsync(z, dz, sizeof(double) * m, cudaMemcpyDeviceToHost, c->st);
-    if (geom) cudaMemcpyAsync(geom, c->lpc.geom, sizeof(float) * 4 * c->npts, cudaMemcpyDeviceToHost, c->st);
-    cudaStreamSynchronize(c->st);
-    cudaFree(dr);
-    cudaFree(dz);
+    double* K[4] = {nullptr, nullptr, nullptr, nullptr};
+    int s = c->alloc(&dr, m) || c->alloc(&dz, m);
+    for (int q = 0; q < c->sch.nsub && !s; ++q) s = c->alloc(&K[q], (size_t)m * m);
+    if (!s) {
+        cudaMemcpyAsync(dr, r, sizeof(double) * m, cudaMemcpyHostToDevice, c->st);
+        c->lpc.geometry(c->d_pts, c->lb, c->st);
+        c->lpc.operators(c->sch.nsub, c->beta, K, c->st);
+        minv_apply(m, K[k], dr, dz, c->st);
+        cudaMemcpyAsync(z, dz, sizeof(double) * m, cudaMemcpyDeviceToHost, c->st);
+        if (geom) cudaMemcpyAsync(geom, c->lpc.geom, sizeof(float) * 4 * c->npts, cudaMemcpyDeviceToHost, c->st);
+        cudaStreamSynchronize(c->st);
+    }
+    if (dr) cudaFree(dr);
+    if (dz) cudaFree(dz);
+    for (double* x : K)
+        if (x) cudaFree(x);
+    if (s) return IBG_ERR_CUDA;
     return c->cuda_check("ibg_lpc_apply");
 }
 

@@ -17,30 +17,35 @@ struct LpcBodies {
     int* closed = nullptr;         // per body: 1 if the points form a closed curve
 };
 
+// FP32 training work arrays, grown on demand (rows = configurations x P^2 point pairs)
 struct TrainScratch {
-    int rows = 0;
-    float *A = nullptr, *s = nullptr, *h1 = nullptr, *C = nullptr, *h2 = nullptr, *out = nullptr, *dout = nullptr;
-    float *dh2 = nullptr, *dC = nullptr, *dh1 = nullptr;
+    long rows = 0;
+    int cfgs = 0;
+    float *gbar = nullptr, *X = nullptr, *H1 = nullptr, *H2 = nullptr, *KO = nullptr, *K = nullptr, *E = nullptr;
+    float *dK = nullptr, *dKO = nullptr, *dH2 = nullptr, *dH1 = nullptr, *lossc = nullptr;
     void release();
 };
 
 struct Lpc {
     int P = 0;
-    float* params = nullptr;   // FP32 master weights
-    void* wbf = nullptr;       // BF16 copy for inference
+    float* params = nullptr;   // FP32 master weights (+ the operator scale c0 as the last entry)
+    void* wbf = nullptr;       // BF16 inference weights: W1 (256 x 19), W2 transposed (256 x 256), W3 (4 x 256)
     int *nbr = nullptr, *cnt = nullptr;
-    void *h1 = nullptr, *h2 = nullptr;  // BF16 inference activations
     float* geom = nullptr;     // current geometry features (P x 4)
-    float* scale = nullptr;
+    float* gbar = nullptr;     // their neighbour means (P x 4)
+    float* kraw = nullptr;     // network output per point pair (P^2 x 4)
     int init(int npts, const std::vector<int>& nbr_h, const std::vector<int>& cnt_h);
     void release();
     void refresh_bf16(cudaStream_t st);
-    // z = (s/beta) net(r) for the current boundary (device pointers)
-    void apply(const double* pts, const LpcBodies& bodies, const double* r, double* z, double beta,
-               cudaStream_t st) const;
-    // loss per sample over B samples (device arrays); gradient (kNParams floats) when grad != nullptr
-    int loss_grad(int B, const float* g, const float* r, const float* t, float* loss_per_sample, float* grad,
-                  TrainScratch& ws, cudaStream_t st) const;
+    // geometry features of the current body configuration
+    void geometry(const double* pts, const LpcBodies& bodies, cudaStream_t st) const;
+    // K_k = sym(net) / (c0 beta_k) for every sub-step k < nsub into Kout[k] (m x m, FP64), at the
+    // geometry last computed by geometry()
+    void operators(int nsub, const double* beta, double* const* Kout, cudaStream_t st) const;
+    // mean loss |K Mn - I|_F^2 / m over B configurations (device arrays: g [B][P][4], Mb [B][m][m]
+    // = M / beta); gradient (lpc_num_params floats, the c0 entry 0) when grad != nullptr
+    int loss_grad(int B, const float* g, const float* Mb, float* loss, float* grad, TrainScratch& ws,
+                  cudaStream_t st) const;
 };
 
 void adam_step(long n, float* p, const float* g, float* m1, float* m2, float lr, int t, cudaStream_t st);

@@ -1,23 +1,30 @@
 // lpc.cu -- learned preconditioner for the moving-body force solve.
 //
-// A network over the boundary points maps a CG residual r to z ~ M^-1 r,
-// used as the preconditioner of the flexible CG (the reference has no
-// counterpart; it runs plain CG, src/ConjugateGradientSolver.cc:35-65).
+// The reference solves M f = r, M = C A^-1 B, by plain CG whenever the bodies
+// move (src/ConjugateGradientSolver.cc:35-65), because M changes every step.
+// Here a network maps the current body geometry to an approximate inverse K of
+// M, used as the preconditioner of the flexible CG (z = K r: linear in the
+// residual, so the usual PCG theory applies).
 //
-//   input per point i:  a_i = (x, y, nx, ny, rx/s, ry/s), s = rms(r),
-//                       x, y about the body centroid over its extent,
-//                       (nx, ny) the unit normal from the neighbours
-//   layer 1:            h1_i = relu(W1 [a_i | mean_{j in N(i)} a_j] + b1)      12 -> 256
-//   layer 2:            h2_i = relu(W2 [h1_i | mean_{j in N(i)} h1_j] + b2)   512 -> 256
-//   layer 3:            o_i  = W3 h2_i + b3                                    256 -> 2
-//   output:             z_i  = (s / beta) o_i
-// N(i) are up to 8 neighbours along the body (i +- 1..4, wrapping on closed
-// bodies).  The factor s makes P(c r) = c P(r) for c > 0; 1/beta carries the
-// sub-step scale of M = beta C A^-1 B.
+// Per boundary point i: g_i = (x, y, nx, ny) (position about its body's
+// centroid over the body's extent, unit normal), gbar_i = mean of g_j over its
+// up to 8 boundary neighbours (i +- 1..4 along the body).  For every ordered
+// pair (i, j):
+//   x_ij = [g_i, gbar_i, g_j, gbar_j, x_i - x_j, y_i - y_j, |p_i - p_j|]     19
+//   h1   = relu(W1 x_ij + b1)                                          19 -> 256
+//   h2   = relu(W2 h1 + b2)                                           256 -> 256
+//   k_ij = W3 h2 + b3                                                 256 -> 4
+// k_ij is the 2 x 2 block coupling force component c at j to component a at i:
+// Kraw[a P + i][c P + j] = k_ij[2a + c]; K = (Kraw + Kraw^T) / 2, and the
+// preconditioner of sub-step k is K / (c0 beta_k), c0 the mean diagonal of
+// M / beta over the training configurations (stored after the weights).
 //
-// Training (FP32): loss = mean over samples of |o - t|^2 / |t|^2 with targets
-// t = beta z / s, gradients by hand-written backward kernels, Adam.
-// Inference (BF16 weights and hidden activations, FP32 accumulation).
+// Training data are what the solver generates with its exact operator: the
+// columns of M = beta C A^-1 B at sampled body configurations, i.e. the pairs
+// (residual M e_j, exact force e_j).  Loss (FP32): mean over configurations of
+// |K Mn - I|_F^2 / m with Mn = M / (beta c0), minimised by Adam with the
+// hand-written backward pass below.  Inference runs with BF16 weights and
+// activations (FP32 accumulation) and writes K in FP64.
 #include <cuda_bf16.h>
 
 #include <cmath>
@@ -33,32 +40,42 @@
 namespace ibg {
 
 // parameter layout (floats)
-constexpr int kIn = 6, kIn2 = 12, kH = 256, kH2 = 512, kOut = 2;
-constexpr size_t oW1 = 0, oB1 = oW1 + (size_t)kH * kIn2, oW2 = oB1 + kH, oB2 = oW2 + (size_t)kH * kH2,
-                 oW3 = oB2 + kH, oB3 = oW3 + (size_t)kOut * kH, kNParams = oB3 + kOut;
+constexpr int kF = 19, kH = 256, kO = 4;
+constexpr size_t oW1 = 0, oB1 = oW1 + (size_t)kH * kF, oW2 = oB1 + kH, oB2 = oW2 + (size_t)kH * kH,
+                 oW3 = oB2 + kH, oB3 = oW3 + (size_t)kO * kH, oC0 = oB3 + kO, kNParams = oC0 + 1;
 
 size_t lpc_num_params() { return kNParams; }
 
 // ---------------------------------------------------------------------------
-// generic FP32 GEMM: C[M x N] = alpha op(A) op(B) + beta C, element (i, k) of
-// op(A) at A[i * as0 + k * as1], (k, j) of op(B) at B[k * bs0 + j * bs1].
-// 64 x 64 tiles, 256 threads, 4 x 4 outputs per thread.
+// generic batched FP32 GEMM: C[z][M x N] = alpha op(A) op(B) + beta C, element
+// (i, k) of op(A) at A[z sA + i as0 + k as1], (k, j) of op(B) at
+// B[z sB + k bs0 + j bs1].  64 x 64 tiles, 256 threads, 4 x 4 outputs per thread.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_sgemm(int M, int N, int K, float alpha, const float* __restrict__ A,
-                                               long as0, long as1, const float* __restrict__ B, long bs0, long bs1,
-                                               float beta, float* __restrict__ C, long ldc) {
+                                               long as0, long as1, long sA, const float* __restrict__ B, long bs0,
+                                               long bs1, long sB, float beta, float* __restrict__ C, long ldc,
+                                               long sC) {
     __shared__ float As[16][64 + 1];
     __shared__ float Bs[16][64 + 1];
+    A += blockIdx.z * sA;
+    B += blockIdx.z * sB;
+    C += blockIdx.z * sC;
     const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    const int i0 = blockIdx.y * 64, j0 = blockIdx.x * 64;
+    const long i0 = (long)blockIdx.y * 64, j0 = (long)blockIdx.x * 64;
     float acc[4][4] = {};
     for (int k0 = 0; k0 < K; k0 += 16) {
         for (int t = threadIdx.x; t < 16 * 64; t += 256) {
-            const int kk = t / 64, ii = t % 64;
-            const int gi = i0 + ii, gk = k0 + kk;
+            // consecutive threads walk the operand's contiguous index
+            int kk, ii;
+            if (as1 == 1) { kk = t % 16; ii = t / 16; } else { kk = t / 64; ii = t % 64; }
+            const long gi = i0 + ii;
+            const int gk = k0 + kk;
             As[kk][ii] = (gi < M && gk < K) ? A[gi * as0 + gk * as1] : 0.f;
-            const int gj = j0 + ii;
-            Bs[kk][ii] = (gk < K && gj < N) ? B[gk * bs0 + gj * bs1] : 0.f;
+            int kb, jj;
+            if (bs0 == 1) { kb = t % 16; jj = t / 16; } else { kb = t / 64; jj = t % 64; }
+            const long gj = j0 + jj;
+            const int gkb = k0 + kb;
+            Bs[kb][jj] = (gkb < K && gj < N) ? B[gkb * bs0 + gj * bs1] : 0.f;
         }
         __syncthreads();
 #pragma unroll
@@ -77,11 +94,11 @@ __global__ void __launch_bounds__(256) k_sgemm(int M, int N, int K, float alpha,
     }
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-        const int gi = i0 + ty * 4 + r;
+        const long gi = i0 + ty * 4 + r;
         if (gi >= M) continue;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-            const int gj = j0 + tx * 4 + c;
+            const long gj = j0 + tx * 4 + c;
             if (gj >= N) continue;
             float v = alpha * acc[r][c];
             if (beta != 0.f) v += beta * C[gi * ldc + gj];
@@ -90,61 +107,55 @@ __global__ void __launch_bounds__(256) k_sgemm(int M, int N, int K, float alpha,
     }
 }
 
-static void sgemm(int M, int N, int K, float alpha, const float* A, long as0, long as1, const float* B, long bs0,
-                  long bs1, float beta, float* C, long ldc, cudaStream_t st) {
-    dim3 grid((N + 63) / 64, (M + 63) / 64);
-    k_sgemm<<<grid, 256, 0, st>>>(M, N, K, alpha, A, as0, as1, B, bs0, bs1, beta, C, ldc);
+static void sgemm(long M, int N, int K, float alpha, const float* A, long as0, long as1, const float* B, long bs0,
+                  long bs1, float beta, float* C, long ldc, cudaStream_t st, int batch = 1, long sA = 0, long sB = 0,
+                  long sC = 0) {
+    dim3 grid((N + 63) / 64, (unsigned)((M + 63) / 64), batch);
+    k_sgemm<<<grid, 256, 0, st>>>((int)M, N, K, alpha, A, as0, as1, sA, B, bs0, bs1, sB, beta, C, ldc, sC);
 }
 
 // ---------------------------------------------------------------------------
-// training kernels (rows = samples x points, row = b * P + i)
+// features
 // ---------------------------------------------------------------------------
-// per-sample residual scale s = rms(r) (one block per sample)
-__global__ void k_lpc_scale(int P, const float* __restrict__ r, float* __restrict__ s) {
-    __shared__ float red[32];
-    const int b = blockIdx.x;
-    float acc = 0.f;
-    for (int k = threadIdx.x; k < 2 * P; k += blockDim.x) {
-        const float v = r[(size_t)b * 2 * P + k];
-        acc += v * v;
-    }
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float t = 0.f;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-        s[b] = sqrtf(t / (2 * P)) + 1e-30f;
-    }
-}
-
-// A = [a_i | mean_nbr a_j] (rows x 12); geometry per sample g[b][i][4], residual r[b][2P] as [x.. | y..]
-__global__ void k_lpc_inputs(int P, int rows, const float* __restrict__ g, const float* __restrict__ r,
-                             const float* __restrict__ s, const int* __restrict__ nbr, const int* __restrict__ cnt,
-                             float* __restrict__ A) {
-    const int row = blockIdx.x * blockDim.x + threadIdx.x;
-    if (row >= rows) return;
-    const int b = row / P, i = row % P;
-    auto feat = [&](int j, float* f) {
-        const float* gg = g + ((size_t)b * P + j) * 4;
-        f[0] = gg[0]; f[1] = gg[1]; f[2] = gg[2]; f[3] = gg[3];
-        f[4] = r[(size_t)b * 2 * P + j] / s[b];
-        f[5] = r[(size_t)b * 2 * P + P + j] / s[b];
-    };
-    float own[kIn], mean[kIn] = {0, 0, 0, 0, 0, 0};
-    feat(i, own);
-    const int n = cnt[i];
+// gbar[b][i] = mean of g[b][j] over the neighbours of i
+__global__ void k_lpc_nbrmean(int B, int P, const float* __restrict__ g, const int* __restrict__ nbr,
+                              const int* __restrict__ cnt, float* __restrict__ gbar) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= B * P) return;
+    const int b = t / P, i = t % P, n = cnt[i];
+    float s[4] = {0.f, 0.f, 0.f, 0.f};
     for (int q = 0; q < n; ++q) {
-        float f[kIn];
-        feat(nbr[i * 8 + q], f);
-        for (int c = 0; c < kIn; ++c) mean[c] += f[c];
+        const float* gj = g + ((size_t)b * P + nbr[i * 8 + q]) * 4;
+        for (int c = 0; c < 4; ++c) s[c] += gj[c];
     }
     const float inv = n > 0 ? 1.f / n : 0.f;
-    float* a = A + (size_t)row * kIn2;
-    for (int c = 0; c < kIn; ++c) {
-        a[c] = own[c];
-        a[kIn + c] = mean[c] * inv;
+    for (int c = 0; c < 4; ++c) gbar[(size_t)t * 4 + c] = s[c] * inv;
+}
+
+__device__ __forceinline__ void pair_features(const float* gi, const float* bi, const float* gj, const float* bj,
+                                              float* x) {
+    for (int c = 0; c < 4; ++c) {
+        x[c] = gi[c];
+        x[4 + c] = bi[c];
+        x[8 + c] = gj[c];
+        x[12 + c] = bj[c];
     }
+    const float dx = gi[0] - gj[0], dy = gi[1] - gj[1];
+    x[16] = dx;
+    x[17] = dy;
+    x[18] = sqrtf(dx * dx + dy * dy);
+}
+
+// X[(b P + i) P + j][19]
+__global__ void k_lpc_pair_inputs(int B, int P, const float* __restrict__ g, const float* __restrict__ gbar,
+                                  float* __restrict__ X) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)B * P * P) return;
+    const int j = (int)(t % P);
+    const long bi = t / P;
+    const int i = (int)(bi % P), b = (int)(bi / P);
+    const size_t pi = (size_t)b * P + i, pj = (size_t)b * P + j;
+    pair_features(g + pi * 4, gbar + pi * 4, g + pj * 4, gbar + pj * 4, X + t * kF);
 }
 
 // y = relu(x + bias) in place on a rows x n matrix
@@ -155,94 +166,80 @@ __global__ void k_bias_relu(long total, int n, const float* __restrict__ bias, f
     x[t] = v > 0.f ? v : 0.f;
 }
 
-// C = [h1_i | mean_nbr h1_j] (rows x 512)
-__global__ void k_lpc_concat(int P, int rows, const float* __restrict__ h1, const int* __restrict__ nbr,
-                             const int* __restrict__ cnt, float* __restrict__ C) {
+// K[b] = sym(Kraw) with Kraw[a P + i][c P + j] = KO[(b P + i) P + j][2a + c] + b3[2a + c]
+__global__ void k_lpc_assemble_train(int B, int P, const float* __restrict__ KO, const float* __restrict__ b3,
+                                     float* __restrict__ K) {
+    const int m = 2 * P;
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)rows * kH) return;
-    const int row = (int)(t / kH), o = (int)(t % kH);
-    const int b = row / P, i = row % P;
-    const int n = cnt[i];
-    float m = 0.f;
-    for (int q = 0; q < n; ++q) m += h1[((size_t)b * P + nbr[i * 8 + q]) * kH + o];
-    C[(size_t)row * kH2 + o] = h1[(size_t)row * kH + o];
-    C[(size_t)row * kH2 + kH + o] = n > 0 ? m / n : 0.f;
+    if (t >= (long)B * m * m) return;
+    const int col = (int)(t % m);
+    const long br = t / m;
+    const int row = (int)(br % m), b = (int)(br / m);
+    auto raw = [&](int r, int c) {
+        const int a = r / P, i = r % P, cc = c / P, j = c % P;
+        return KO[(((size_t)b * P + i) * P + j) * kO + 2 * a + cc] + b3[2 * a + cc];
+    };
+    K[t] = 0.5f * (raw(row, col) + raw(col, row));
 }
 
-// output layer, per-sample loss and dL/do (one block per sample)
-__global__ void k_lpc_out_loss(int P, int B, const float* __restrict__ h2, const float* __restrict__ W3,
-                               const float* __restrict__ b3, const float* __restrict__ t, float* __restrict__ out,
-                               float* __restrict__ dout, float* __restrict__ loss_per_sample) {
+// E[b] -= I; loss per configuration sum(E^2) / m; E <- 2 E / (B m) (the loss gradient)
+__global__ void k_lpc_residual_loss(int m, int B, float* __restrict__ E, float* __restrict__ lossc) {
     __shared__ float red[32];
     const int b = blockIdx.x;
-    // |t_b|^2
-    float tt = 0.f;
-    for (int k = threadIdx.x; k < 2 * P; k += blockDim.x) {
-        const float v = t[(size_t)b * 2 * P + k];
-        tt += v * v;
+    float* e = E + (size_t)b * m * m;
+    float acc = 0.f;
+    for (long t = threadIdx.x; t < (long)m * m; t += blockDim.x) {
+        float v = e[t];
+        if (t / m == t % m) v -= 1.f;
+        acc += v * v;
+        e[t] = 2.f * v / ((float)B * m);
     }
-    for (int o = 16; o > 0; o >>= 1) tt += __shfl_xor_sync(0xffffffffu, tt, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = tt;
-    __syncthreads();
-    float tsum = 0.f;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tsum += red[w];
-    __syncthreads();
-    const float denom = tsum + 1e-12f;
-    float el = 0.f;
-    for (int q = threadIdx.x; q < 2 * P; q += blockDim.x) {
-        const int c = q / P, i = q % P;  // component, point
-        const float* h = h2 + ((size_t)b * P + i) * kH;
-        float o = b3[c];
-        for (int k = 0; k < kH; ++k) o += W3[c * kH + k] * h[k];
-        const float e = o - t[(size_t)b * 2 * P + c * P + i];
-        out[((size_t)b * P + i) * 2 + c] = o;
-        dout[((size_t)b * P + i) * 2 + c] = 2.f * e / (denom * B);
-        el += e * e;
-    }
-    for (int o = 16; o > 0; o >>= 1) el += __shfl_xor_sync(0xffffffffu, el, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = el;
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
     __syncthreads();
     if (threadIdx.x == 0) {
         float s = 0.f;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
-        loss_per_sample[b] = s / denom;
+        lossc[b] = s / m;
     }
 }
 
-// dh = (dY W) masked by (h > 0): dh[row][o] = (sum_c dY[row][c] W[c][o]) (h[row][o] > 0), for the 2-output layer
-__global__ void k_lpc_back3(long rows, const float* __restrict__ dout, const float* __restrict__ W3,
-                            const float* __restrict__ h2, float* __restrict__ dh2) {
+// dKO[(b P + i) P + j][2a + c] = (dK[b][aP+i][cP+j] + dK[b][cP+j][aP+i]) / 2
+__global__ void k_lpc_dko(int B, int P, const float* __restrict__ dK, float* __restrict__ dKO) {
+    const int m = 2 * P;
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= rows * kH) return;
-    const long row = t / kH;
-    const int o = (int)(t % kH);
-    const float g = dout[row * 2] * W3[o] + dout[row * 2 + 1] * W3[kH + o];
-    dh2[t] = h2[t] > 0.f ? g : 0.f;
+    if (t >= (long)B * P * P * kO) return;
+    const int q = (int)(t % kO);
+    const long pair = t / kO;
+    const int j = (int)(pair % P);
+    const long bi = pair / P;
+    const int i = (int)(bi % P), b = (int)(bi / P);
+    const int a = q / 2, c = q % 2;
+    const float* d = dK + (size_t)b * m * m;
+    const int r = a * P + i, cc = c * P + j;
+    dKO[t] = 0.5f * (d[(size_t)r * m + cc] + d[(size_t)cc * m + r]);
 }
 
-// dh1_i = (dC_i[:256] + sum_{j in N(i)} dC_j[256:] / |N(j)|) masked by h1 > 0
-__global__ void k_lpc_back_concat(int P, int rows, const float* __restrict__ dC, const int* __restrict__ nbr,
-                                  const int* __restrict__ cnt, const float* __restrict__ h1, float* __restrict__ dh1) {
+// dh *= (h > 0)
+__global__ void k_relu_mask(long total, const float* __restrict__ h, float* __restrict__ dh) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)rows * kH) return;
-    const int row = (int)(t / kH), o = (int)(t % kH);
-    const int b = row / P, i = row % P;
-    float g = dC[(size_t)row * kH2 + o];
-    const int n = cnt[i];
-    for (int q = 0; q < n; ++q) {
-        const int j = nbr[i * 8 + q];
-        g += dC[((size_t)b * P + j) * kH2 + kH + o] / cnt[j];
-    }
-    dh1[t] = h1[t] > 0.f ? g : 0.f;
+    if (t < total && !(h[t] > 0.f)) dh[t] = 0.f;
 }
 
-// column sums of a rows x n matrix into out[n] (+= scale * sum), deterministic order
-__global__ void k_colsum(int rows, int n, const float* __restrict__ x, float* __restrict__ out) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n) return;
+// column sums of a rows x n matrix: one block per column, fixed summation order
+__global__ void k_colsum(long rows, int n, const float* __restrict__ x, float* __restrict__ out) {
+    __shared__ float red[32];
+    const int c = blockIdx.x;
     float s = 0.f;
-    for (int r = 0; r < rows; ++r) s += x[(size_t)r * n + c];
-    out[c] = s;
+    for (long r = threadIdx.x; r < rows; r += blockDim.x) s += x[r * n + c];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        out[c] = t;
+    }
 }
 
 __global__ void k_adam(long n, float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m1,
@@ -258,11 +255,11 @@ __global__ void k_adam(long n, float* __restrict__ p, const float* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-// inference kernels (one sample = the current boundary, BF16 weights)
+// inference (one configuration, BF16 weights and activations)
 // ---------------------------------------------------------------------------
 // geometry features of the current body configuration: positions about each
 // body's centroid over its extent, unit normals from the boundary neighbours
-__global__ void k_lpc_geometry(int P, int nbodies, const double* __restrict__ pts, const int* __restrict__ body_of,
+__global__ void k_lpc_geometry(int P, const double* __restrict__ pts, const int* __restrict__ body_of,
                                const int* __restrict__ body_start, const int* __restrict__ body_len,
                                const int* __restrict__ closed, float* __restrict__ g) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -295,112 +292,105 @@ __global__ void k_lpc_geometry(int P, int nbodies, const double* __restrict__ pt
     g[i * 4 + 1] = (float)((pts[2 * i + 1] - cy) / ext);
     g[i * 4 + 2] = (float)(ty / tl);
     g[i * 4 + 3] = (float)(-tx / tl);
-    (void)nbodies;
 }
 
-// z = (s / beta) net(r): one CTA of 256 threads per 8 points for layers 1-2,
-// with the scale computed in the first phase of every CTA
-__global__ void __launch_bounds__(256) k_lpc_infer_l1(int P, const double* __restrict__ r,
-                                                      const float* __restrict__ g, const int* __restrict__ nbr,
-                                                      const int* __restrict__ cnt,
-                                                      const __nv_bfloat16* __restrict__ W1,
-                                                      const float* __restrict__ b1, __nv_bfloat16* __restrict__ h1,
-                                                      float* __restrict__ s_out) {
-    __shared__ float red[8];
-    __shared__ float s_sh;
-    __shared__ float A[8][kIn2];
-    // residual scale
-    float acc = 0.f;
-    for (int k = threadIdx.x; k < 2 * P; k += blockDim.x) acc += (float)(r[k] * r[k]);
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float t = 0.f;
-        for (int w = 0; w < 8; ++w) t += red[w];
-        s_sh = sqrtf(t / (2 * P)) + 1e-30f;
-        if (blockIdx.x == 0) *s_out = s_sh;
-    }
-    __syncthreads();
-    const float s = s_sh;
-    const int i0 = blockIdx.x * 8;
-    if (threadIdx.x < 8 && i0 + threadIdx.x < P) {
-        const int i = i0 + threadIdx.x;
-        auto feat = [&](int j, float* f) {
-            f[0] = g[j * 4]; f[1] = g[j * 4 + 1]; f[2] = g[j * 4 + 2]; f[3] = g[j * 4 + 3];
-            f[4] = (float)r[j] / s;
-            f[5] = (float)r[P + j] / s;
-        };
-        float own[kIn], mean[kIn] = {0, 0, 0, 0, 0, 0};
-        feat(i, own);
-        const int n = cnt[i];
-        for (int q = 0; q < n; ++q) {
-            float f[kIn];
-            feat(nbr[i * 8 + q], f);
-            for (int c = 0; c < kIn; ++c) mean[c] += f[c];
-        }
-        for (int c = 0; c < kIn; ++c) {
-            A[threadIdx.x][c] = own[c];
-            A[threadIdx.x][kIn + c] = n > 0 ? mean[c] / n : 0.f;
-        }
-    }
-    __syncthreads();
-    const int o = threadIdx.x;  // 256 outputs
-    for (int pi = 0; pi < 8 && i0 + pi < P; ++pi) {
-        float v = b1[o];
-        for (int c = 0; c < kIn2; ++c) v += __bfloat162float(W1[o * kIn2 + c]) * A[pi][c];
-        h1[(size_t)(i0 + pi) * kH + o] = __float2bfloat16(v > 0.f ? v : 0.f);
-    }
-}
+constexpr int kPairsPerCta = 32;
 
-__global__ void __launch_bounds__(256) k_lpc_infer_l2(int P, const int* __restrict__ nbr, const int* __restrict__ cnt,
-                                                      const __nv_bfloat16* __restrict__ h1,
-                                                      const __nv_bfloat16* __restrict__ W2,
-                                                      const float* __restrict__ b2, __nv_bfloat16* __restrict__ h2) {
-    __shared__ float Cs[4][kH2];
-    const int i0 = blockIdx.x * 4;
-    for (int t = threadIdx.x; t < 4 * kH; t += blockDim.x) {
-        const int pi = t / kH, o = t % kH, i = i0 + pi;
-        float own = 0.f, m = 0.f;
-        if (i < P) {
-            own = __bfloat162float(h1[(size_t)i * kH + o]);
-            const int n = cnt[i];
-            for (int q = 0; q < n; ++q) m += __bfloat162float(h1[(size_t)nbr[i * 8 + q] * kH + o]);
-            if (n > 0) m /= n;
-        }
-        Cs[pi][o] = own;
-        Cs[pi][kH + o] = m;
-    }
-    __syncthreads();
+// one CTA of 256 threads (thread = hidden unit) per 32 point pairs
+__global__ void __launch_bounds__(256) k_lpc_pair_infer(int P, const float* __restrict__ g,
+                                                        const float* __restrict__ gbar,
+                                                        const __nv_bfloat16* __restrict__ W1,
+                                                        const float* __restrict__ b1,
+                                                        const __nv_bfloat16* __restrict__ W2t,
+                                                        const float* __restrict__ b2,
+                                                        const __nv_bfloat16* __restrict__ W3,
+                                                        const float* __restrict__ b3, float* __restrict__ kraw) {
+    __shared__ float X[kPairsPerCta][kF + 1];
+    __shared__ float H[kPairsPerCta][kH + 1];
+    const long npairs = (long)P * P;
+    const long p0 = (long)blockIdx.x * kPairsPerCta;
     const int o = threadIdx.x;
-    float acc[4];
-    for (int pi = 0; pi < 4; ++pi) acc[pi] = b2[o];
-    const __nv_bfloat16* w = W2 + (size_t)o * kH2;
-    for (int c = 0; c < kH2; ++c) {
-        const float wv = __bfloat162float(w[c]);
-#pragma unroll
-        for (int pi = 0; pi < 4; ++pi) acc[pi] += wv * Cs[pi][c];
+    if (o < kPairsPerCta) {
+        const long pr = p0 + o;
+        if (pr < npairs) {
+            const int i = (int)(pr / P), j = (int)(pr % P);
+            pair_features(g + (size_t)i * 4, gbar + (size_t)i * 4, g + (size_t)j * 4, gbar + (size_t)j * 4, X[o]);
+        } else {
+            for (int c = 0; c < kF; ++c) X[o][c] = 0.f;
+        }
     }
-    for (int pi = 0; pi < 4 && i0 + pi < P; ++pi)
-        h2[(size_t)(i0 + pi) * kH + o] = __float2bfloat16(acc[pi] > 0.f ? acc[pi] : 0.f);
+    __syncthreads();
+    // layer 1
+    {
+        float w[kF];
+        for (int c = 0; c < kF; ++c) w[c] = __bfloat162float(W1[o * kF + c]);
+        const float bb = b1[o];
+        for (int p = 0; p < kPairsPerCta; ++p) {
+            float v = bb;
+#pragma unroll
+            for (int c = 0; c < kF; ++c) v += w[c] * X[p][c];
+            H[p][o] = __bfloat162float(__float2bfloat16(v > 0.f ? v : 0.f));
+        }
+    }
+    __syncthreads();
+    // layer 2 (W2 stored transposed: W2t[k][o], coalesced over o)
+    float acc[kPairsPerCta];
+    {
+        const float bb = b2[o];
+#pragma unroll
+        for (int p = 0; p < kPairsPerCta; ++p) acc[p] = bb;
+        for (int k = 0; k < kH; ++k) {
+            const float w = __bfloat162float(W2t[(size_t)k * kH + o]);
+#pragma unroll
+            for (int p = 0; p < kPairsPerCta; ++p) acc[p] += w * H[p][k];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < kPairsPerCta; ++p) H[p][o] = __bfloat162float(__float2bfloat16(acc[p] > 0.f ? acc[p] : 0.f));
+    __syncthreads();
+    // layer 3: 32 pairs x 4 outputs, one warp per 16 of them
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int q = warp; q < kPairsPerCta * kO; q += 8) {
+        const int p = q / kO, c = q % kO;
+        float v = 0.f;
+        for (int k = lane; k < kH; k += 32) v += __bfloat162float(W3[c * kH + k]) * H[p][k];
+        for (int s = 16; s > 0; s >>= 1) v += __shfl_xor_sync(0xffffffffu, v, s);
+        if (lane == 0 && p0 + p < npairs) kraw[(size_t)(p0 + p) * kO + c] = v + b3[c];
+    }
 }
 
-__global__ void k_lpc_infer_l3(int P, const __nv_bfloat16* __restrict__ h2, const __nv_bfloat16* __restrict__ W3,
-                               const float* __restrict__ b3, const float* __restrict__ s, double inv_beta,
-                               double* __restrict__ z) {
-    const int q = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (q >= 2 * P) return;
-    const int c = q / P, i = q % P;
-    float acc = 0.f;
-    for (int k = lane; k < kH; k += 32) acc += __bfloat162float(W3[c * kH + k]) * __bfloat162float(h2[(size_t)i * kH + k]);
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) z[c * P + i] = (double)(acc + b3[c]) * (double)(*s) * inv_beta;
+// Kout[k][r][c] = (kraw(r, c) + kraw(c, r)) / (2 c0 beta_k) for every sub-step k
+struct KOut {
+    double* p[4];
+    double s[4];
+};
+__global__ void k_lpc_assemble(int P, int nsub, const float* __restrict__ kraw, const float* __restrict__ c0p,
+                               KOut out) {
+    const int m = 2 * P;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)m * m) return;
+    const int row = (int)(t / m), col = (int)(t % m);
+    auto raw = [&](int r, int c) {
+        const int a = r / P, i = r % P, cc = c / P, j = c % P;
+        return (double)kraw[((size_t)i * P + j) * kO + 2 * a + cc];
+    };
+    const double v = 0.5 * (raw(row, col) + raw(col, row)) / (double)(*c0p);
+    for (int k = 0; k < nsub; ++k) out.p[k][t] = v * out.s[k];
 }
 
-__global__ void k_to_bf16(long n, const float* __restrict__ x, __nv_bfloat16* __restrict__ y) {
-    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) y[i] = __float2bfloat16(x[i]);
+// BF16 copies: W1 as is, W2 transposed, W3 as is
+__global__ void k_lpc_to_bf16(const float* __restrict__ p, __nv_bfloat16* __restrict__ w) {
+    const long n1 = (long)kH * kF, n2 = (long)kH * kH, n3 = (long)kO * kH;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n1) {
+        w[t] = __float2bfloat16(p[oW1 + t]);
+    } else if (t < n1 + n2) {
+        const long u = t - n1, k = u / kH, o = u % kH;  // W2t[k][o] = W2[o][k]
+        w[t] = __float2bfloat16(p[oW2 + o * kH + k]);
+    } else if (t < n1 + n2 + n3) {
+        w[t] = __float2bfloat16(p[oW3 + (t - n1 - n2)]);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -408,112 +398,144 @@ __global__ void k_to_bf16(long n, const float* __restrict__ x, __nv_bfloat16* __
 // ---------------------------------------------------------------------------
 int Lpc::init(int npts, const std::vector<int>& nbr_h, const std::vector<int>& cnt_h) {
     P = npts;
+    const long w = (long)kH * kF + (long)kH * kH + (long)kO * kH;
     if (cudaMalloc(&params, sizeof(float) * kNParams) || cudaMalloc(&nbr, sizeof(int) * 8 * P) ||
-        cudaMalloc(&cnt, sizeof(int) * P) || cudaMalloc(&wbf, sizeof(__nv_bfloat16) * kNParams) ||
-        cudaMalloc(&h1, sizeof(__nv_bfloat16) * (size_t)P * kH) ||
-        cudaMalloc(&h2, sizeof(__nv_bfloat16) * (size_t)P * kH) || cudaMalloc(&geom, sizeof(float) * 4 * P) ||
-        cudaMalloc(&scale, sizeof(float)))
+        cudaMalloc(&cnt, sizeof(int) * P) || cudaMalloc(&wbf, sizeof(__nv_bfloat16) * w) ||
+        cudaMalloc(&geom, sizeof(float) * 4 * P) || cudaMalloc(&gbar, sizeof(float) * 4 * P) ||
+        cudaMalloc(&kraw, sizeof(float) * (size_t)P * P * kO))
         return IBG_ERR_CUDA;
     cudaMemcpy(nbr, nbr_h.data(), sizeof(int) * 8 * P, cudaMemcpyHostToDevice);
     cudaMemcpy(cnt, cnt_h.data(), sizeof(int) * P, cudaMemcpyHostToDevice);
-    // He initialisation, fixed seed
+    // He initialisation with a fixed seed; the output layer starts small
     std::vector<float> h(kNParams, 0.f);
     std::mt19937 rng(1234);
-    auto fill = [&](size_t off, int rows, int cols) {
-        std::normal_distribution<float> nd(0.f, std::sqrt(2.f / cols));
+    auto fill = [&](size_t off, int rows, int cols, float gain) {
+        std::normal_distribution<float> nd(0.f, gain * std::sqrt(2.f / cols));
         for (int k = 0; k < rows * cols; ++k) h[off + k] = nd(rng);
     };
-    fill(oW1, kH, kIn2);
-    fill(oW2, kH, kH2);
-    fill(oW3, kOut, kH);
-    for (int k = 0; k < kOut * kH; ++k) h[oW3 + k] *= 0.1f;
+    fill(oW1, kH, kF, 1.f);
+    fill(oW2, kH, kH, 1.f);
+    fill(oW3, kO, kH, 0.1f);
+    h[oC0] = 1.f;
     cudaMemcpy(params, h.data(), sizeof(float) * kNParams, cudaMemcpyHostToDevice);
     refresh_bf16(nullptr);
-    return IBG_OK;
+    return cudaDeviceSynchronize() == cudaSuccess ? IBG_OK : IBG_ERR_CUDA;
 }
 
 void Lpc::release() {
-    void* p[] = {params, nbr, cnt, wbf, h1, h2, geom, scale};
+    void* p[] = {params, nbr, cnt, wbf, geom, gbar, kraw};
     for (void* x : p)
         if (x) cudaFree(x);
     params = nullptr;
     nbr = cnt = nullptr;
     wbf = nullptr;
-    h1 = h2 = nullptr;
-    geom = scale = nullptr;
+    geom = gbar = kraw = nullptr;
 }
 
 void Lpc::refresh_bf16(cudaStream_t st) {
-    k_to_bf16<<<(unsigned)((kNParams + 255) / 256), 256, 0, st>>>((long)kNParams, params, (__nv_bfloat16*)wbf);
+    const long w = (long)kH * kF + (long)kH * kH + (long)kO * kH;
+    k_lpc_to_bf16<<<(unsigned)((w + 255) / 256), 256, 0, st>>>(params, (__nv_bfloat16*)wbf);
 }
 
-void Lpc::apply(const double* pts, const LpcBodies& bodies, const double* r, double* z, double beta,
-                cudaStream_t st) const {
+void Lpc::geometry(const double* pts, const LpcBodies& bodies, cudaStream_t st) const {
+    k_lpc_geometry<<<(P + 127) / 128, 128, 0, st>>>(P, pts, bodies.body_of, bodies.start, bodies.len, bodies.closed,
+                                                    geom);
+    k_lpc_nbrmean<<<(P + 127) / 128, 128, 0, st>>>(1, P, geom, nbr, cnt, gbar);
+}
+
+void Lpc::operators(int nsub, const double* beta, double* const* Kout, cudaStream_t st) const {
     const __nv_bfloat16* w = (const __nv_bfloat16*)wbf;
-    k_lpc_geometry<<<(P + 127) / 128, 128, 0, st>>>(P, bodies.n, pts, bodies.body_of, bodies.start, bodies.len,
-                                                    bodies.closed, geom);
-    k_lpc_infer_l1<<<(P + 7) / 8, 256, 0, st>>>(P, r, geom, nbr, cnt, w + oW1, params + oB1, (__nv_bfloat16*)h1,
-                                                 scale);
-    k_lpc_infer_l2<<<(P + 3) / 4, 256, 0, st>>>(P, nbr, cnt, (const __nv_bfloat16*)h1, w + oW2, params + oB2,
-                                                 (__nv_bfloat16*)h2);
-    k_lpc_infer_l3<<<(2 * P + 7) / 8, 256, 0, st>>>(P, (const __nv_bfloat16*)h2, w + oW3, params + oB3, scale,
-                                                     1.0 / beta, z);
+    const __nv_bfloat16* W1 = w;
+    const __nv_bfloat16* W2t = W1 + (size_t)kH * kF;
+    const __nv_bfloat16* W3 = W2t + (size_t)kH * kH;
+    const long npairs = (long)P * P;
+    k_lpc_pair_infer<<<(unsigned)((npairs + kPairsPerCta - 1) / kPairsPerCta), 256, 0, st>>>(
+        P, geom, gbar, W1, params + oB1, W2t, params + oB2, W3, params + oB3, kraw);
+    KOut o{};
+    for (int k = 0; k < nsub && k < 4; ++k) {
+        o.p[k] = Kout[k];
+        o.s[k] = 1.0 / beta[k];
+    }
+    const long m2 = 4 * npairs;
+    k_lpc_assemble<<<(unsigned)((m2 + 255) / 256), 256, 0, st>>>(P, nsub < 4 ? nsub : 4, kraw, params + oC0, o);
 }
 
-// one forward (and backward when grad != nullptr) pass over B samples held on the device
-int Lpc::loss_grad(int B, const float* g, const float* r, const float* t, float* loss_per_sample, float* grad,
-                   TrainScratch& ws, cudaStream_t st) const {
-    const int rows = B * P;
-    if (ws.rows < rows) {
+int Lpc::loss_grad(int B, const float* g, const float* Mb, float* loss, float* grad, TrainScratch& ws,
+                   cudaStream_t st) const {
+    const int m = 2 * P;
+    const long rows = (long)B * P * P;
+    if (ws.rows < rows || ws.cfgs < B) {
         ws.release();
-        if (cudaMalloc(&ws.A, sizeof(float) * (size_t)rows * kIn2) || cudaMalloc(&ws.s, sizeof(float) * B) ||
-            cudaMalloc(&ws.h1, sizeof(float) * (size_t)rows * kH) ||
-            cudaMalloc(&ws.C, sizeof(float) * (size_t)rows * kH2) ||
-            cudaMalloc(&ws.h2, sizeof(float) * (size_t)rows * kH) ||
-            cudaMalloc(&ws.out, sizeof(float) * (size_t)rows * 2) ||
-            cudaMalloc(&ws.dout, sizeof(float) * (size_t)rows * 2) ||
-            cudaMalloc(&ws.dh2, sizeof(float) * (size_t)rows * kH) ||
-            cudaMalloc(&ws.dC, sizeof(float) * (size_t)rows * kH2) ||
-            cudaMalloc(&ws.dh1, sizeof(float) * (size_t)rows * kH))
+        const size_t mm = (size_t)B * m * m;
+        if (cudaMalloc(&ws.gbar, sizeof(float) * (size_t)B * P * 4) || cudaMalloc(&ws.X, sizeof(float) * rows * kF) ||
+            cudaMalloc(&ws.H1, sizeof(float) * rows * kH) || cudaMalloc(&ws.H2, sizeof(float) * rows * kH) ||
+            cudaMalloc(&ws.KO, sizeof(float) * rows * kO) || cudaMalloc(&ws.K, sizeof(float) * mm) ||
+            cudaMalloc(&ws.E, sizeof(float) * mm) || cudaMalloc(&ws.dK, sizeof(float) * mm) ||
+            cudaMalloc(&ws.dKO, sizeof(float) * rows * kO) || cudaMalloc(&ws.dH2, sizeof(float) * rows * kH) ||
+            cudaMalloc(&ws.dH1, sizeof(float) * rows * kH) || cudaMalloc(&ws.lossc, sizeof(float) * B)) {
+            ws.release();
             return IBG_ERR_CUDA;
+        }
         ws.rows = rows;
+        ws.cfgs = B;
     }
+    float c0 = 1.f;
+    cudaMemcpyAsync(&c0, params + oC0, sizeof(float), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return IBG_ERR_CUDA;
     const float* W1 = params + oW1;
     const float* W2 = params + oW2;
     const float* W3 = params + oW3;
+    const long mm = (long)m * m;
+    auto blocks = [](long n) { return (unsigned)((n + 255) / 256); };
     // forward
-    k_lpc_scale<<<B, 256, 0, st>>>(P, r, ws.s);
-    k_lpc_inputs<<<(rows + 127) / 128, 128, 0, st>>>(P, rows, g, r, ws.s, nbr, cnt, ws.A);
-    sgemm(rows, kH, kIn2, 1.f, ws.A, kIn2, 1, W1, 1, kIn2, 0.f, ws.h1, kH, st);
-    k_bias_relu<<<(unsigned)(((long)rows * kH + 255) / 256), 256, 0, st>>>((long)rows * kH, kH, params + oB1, ws.h1);
-    k_lpc_concat<<<(unsigned)(((long)rows * kH + 255) / 256), 256, 0, st>>>(P, rows, ws.h1, nbr, cnt, ws.C);
-    sgemm(rows, kH, kH2, 1.f, ws.C, kH2, 1, W2, 1, kH2, 0.f, ws.h2, kH, st);
-    k_bias_relu<<<(unsigned)(((long)rows * kH + 255) / 256), 256, 0, st>>>((long)rows * kH, kH, params + oB2, ws.h2);
-    k_lpc_out_loss<<<B, 256, 0, st>>>(P, B, ws.h2, W3, params + oB3, t, ws.out, ws.dout, loss_per_sample);
-    if (!grad) return IBG_OK;
-    // backward
-    // dW3 = dout^T h2 (2 x 256), db3 = column sums of dout
-    sgemm(kOut, kH, rows, 1.f, ws.dout, 1, 2, ws.h2, kH, 1, 0.f, grad + oW3, kH, st);
-    k_colsum<<<1, 32, 0, st>>>(rows, kOut, ws.dout, grad + oB3);
-    k_lpc_back3<<<(unsigned)(((long)rows * kH + 255) / 256), 256, 0, st>>>((long)rows, ws.dout, W3, ws.h2, ws.dh2);
-    // dW2 = dh2^T C (256 x 512), db2, dC = dh2 W2 (rows x 512)
-    sgemm(kH, kH2, rows, 1.f, ws.dh2, 1, kH, ws.C, kH2, 1, 0.f, grad + oW2, kH2, st);
-    k_colsum<<<(kH + 127) / 128, 128, 0, st>>>(rows, kH, ws.dh2, grad + oB2);
-    sgemm(rows, kH2, kH, 1.f, ws.dh2, kH, 1, W2, kH2, 1, 0.f, ws.dC, kH2, st);
-    k_lpc_back_concat<<<(unsigned)(((long)rows * kH + 255) / 256), 256, 0, st>>>(P, rows, ws.dC, nbr, cnt, ws.h1,
-                                                                                ws.dh1);
-    // dW1 = dh1^T A (256 x 12), db1
-    sgemm(kH, kIn2, rows, 1.f, ws.dh1, 1, kH, ws.A, kIn2, 1, 0.f, grad + oW1, kIn2, st);
-    k_colsum<<<(kH + 127) / 128, 128, 0, st>>>(rows, kH, ws.dh1, grad + oB1);
-    return cudaPeekAtLastError() == cudaSuccess ? IBG_OK : IBG_ERR_CUDA;
+    k_lpc_nbrmean<<<(B * P + 127) / 128, 128, 0, st>>>(B, P, g, nbr, cnt, ws.gbar);
+    k_lpc_pair_inputs<<<blocks(rows), 256, 0, st>>>(B, P, g, ws.gbar, ws.X);
+    sgemm(rows, kH, kF, 1.f, ws.X, kF, 1, W1, 1, kF, 0.f, ws.H1, kH, st);
+    k_bias_relu<<<blocks(rows * kH), 256, 0, st>>>(rows * kH, kH, params + oB1, ws.H1);
+    sgemm(rows, kH, kH, 1.f, ws.H1, kH, 1, W2, 1, kH, 0.f, ws.H2, kH, st);
+    k_bias_relu<<<blocks(rows * kH), 256, 0, st>>>(rows * kH, kH, params + oB2, ws.H2);
+    sgemm(rows, kO, kH, 1.f, ws.H2, kH, 1, W3, 1, kH, 0.f, ws.KO, kO, st);
+    k_lpc_assemble_train<<<blocks((long)B * mm), 256, 0, st>>>(B, P, ws.KO, params + oB3, ws.K);
+    // E = K Mn - I with Mn = Mb / c0; loss; E <- dL/dE
+    sgemm(m, m, m, 1.f / c0, ws.K, m, 1, Mb, m, 1, 0.f, ws.E, m, st, B, mm, mm, mm);
+    k_lpc_residual_loss<<<B, 256, 0, st>>>(m, B, ws.E, ws.lossc);
+    std::vector<float> lc(B);
+    cudaMemcpyAsync(lc.data(), ws.lossc, sizeof(float) * B, cudaMemcpyDeviceToHost, st);
+    if (grad) {
+        // dK = dE Mn^T, then through the symmetrisation to the per-pair outputs
+        sgemm(m, m, m, 1.f / c0, ws.E, m, 1, Mb, 1, m, 0.f, ws.dK, m, st, B, mm, mm, mm);
+        k_lpc_dko<<<blocks(rows * kO), 256, 0, st>>>(B, P, ws.dK, ws.dKO);
+        // layer 3: dW3 = dKO^T H2, db3, dH2 = dKO W3 (masked)
+        sgemm(kO, kH, (int)rows, 1.f, ws.dKO, 1, kO, ws.H2, kH, 1, 0.f, grad + oW3, kH, st);
+        k_colsum<<<kO, 256, 0, st>>>(rows, kO, ws.dKO, grad + oB3);
+        sgemm(rows, kH, kO, 1.f, ws.dKO, kO, 1, W3, kH, 1, 0.f, ws.dH2, kH, st);
+        k_relu_mask<<<blocks(rows * kH), 256, 0, st>>>(rows * kH, ws.H2, ws.dH2);
+        // layer 2: dW2 = dH2^T H1, db2, dH1 = dH2 W2 (masked)
+        sgemm(kH, kH, (int)rows, 1.f, ws.dH2, 1, kH, ws.H1, kH, 1, 0.f, grad + oW2, kH, st);
+        k_colsum<<<kH, 256, 0, st>>>(rows, kH, ws.dH2, grad + oB2);
+        sgemm(rows, kH, kH, 1.f, ws.dH2, kH, 1, W2, kH, 1, 0.f, ws.dH1, kH, st);
+        k_relu_mask<<<blocks(rows * kH), 256, 0, st>>>(rows * kH, ws.H1, ws.dH1);
+        // layer 1: dW1 = dH1^T X, db1
+        sgemm(kH, kF, (int)rows, 1.f, ws.dH1, 1, kH, ws.X, kF, 1, 0.f, grad + oW1, kF, st);
+        k_colsum<<<kH, 256, 0, st>>>(rows, kH, ws.dH1, grad + oB1);
+        cudaMemsetAsync(grad + oC0, 0, sizeof(float), st);
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess) return IBG_ERR_CUDA;
+    if (loss) {
+        double a = 0;
+        for (float v : lc) a += v;
+        *loss = (float)(a / B);
+    }
+    return IBG_OK;
 }
 
 void TrainScratch::release() {
-    float* p[] = {A, s, h1, C, h2, out, dout, dh2, dC, dh1};
+    float* p[] = {gbar, X, H1, H2, KO, K, E, dK, dKO, dH2, dH1, lossc};
     for (float* x : p)
         if (x) cudaFree(x);
-    A = s = h1 = C = h2 = out = dout = dh2 = dC = dh1 = nullptr;
+    gbar = X = H1 = H2 = KO = K = E = dK = dKO = dH2 = dH1 = lossc = nullptr;
     rows = 0;
+    cfgs = 0;
 }
 
 void adam_step(long n, float* p, const float* g, float* m1, float* m2, float lr, int t, cudaStream_t st) {

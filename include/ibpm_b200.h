@@ -160,27 +160,33 @@ IBG_API long long ibg_ensemble_launches_per_step(const ibg_ensemble* ens);
 IBG_API const char* ibg_ensemble_last_error(const ibg_ensemble* ens);
 
 /* --- learned preconditioner (no reference counterpart) -----------------------
- * A network over the boundary points approximating z = M^-1 r (lpc.cu): per
- * point the position about the body centroid, the unit normal and the
- * residual over its rms, averaged with 8 boundary neighbours, a 3-layer MLP of
- * width 256, output scaled by rms(r)/beta.  ibg_lpc_generate produces training
- * pairs from the solver itself: body configurations at nconfig times in
- * [t0, t1], nres residuals each (white and boundary-smooth), targets
- * zb = beta_k M_k^-1 r from the exact Cholesky operator.  Arrays are float,
- * sample-major: geom [nsamp][npts][4], r and zb [nsamp][2 npts] with
- * nsamp = nconfig * nres.  ibg_lpc_train fits the network (Adam, FP32) and
- * enables it for IBG_PRECOND_LEARNED (BF16 inference).  ibg_lpc_loss_grad gives
- * the mean loss and its gradient (for checking against a CPU restatement). */
+ * For moving bodies the reference runs plain CG on M f = r every sub-step
+ * (src/ConjugateGradientSolver.cc:35-65).  With IBG_PRECOND_LEARNED a network
+ * (lpc.cu) maps the body geometry to an approximate inverse K of M: an MLP
+ * (19 -> 256 -> 256 -> 4, ReLU) over every pair of boundary points whose
+ * inputs are the two points' positions and normals, their means over 8
+ * boundary neighbours and the pair's offset; its outputs are the 2 x 2 blocks
+ * of K.  K is evaluated (BF16) at the start of every step and applied as the
+ * PCG preconditioner z = K r; until a network is trained or loaded, and
+ * whenever a solve falls back, the iteration is plain CG.
+ * ibg_lpc_generate samples nconfig body configurations at times evenly spread
+ * over [t0, t1] and returns their geometry features (geom, nconfig x npts x 4
+ * floats) and operators M / beta (mb, nconfig x m x m floats, m = 2 npts,
+ * row-major) from the solver's own exact force-operator build; column j of M
+ * is the residual of the unit force e_j.  ibg_lpc_train fits the network to
+ * them (Adam, FP32, loss |K M/(beta c0) - I|_F^2 / m averaged over the
+ * configurations; c0 = mean diagonal of M / beta, stored as the last
+ * parameter) and enables it; loss_history receives one mean loss per epoch.
+ * ibg_lpc_loss_grad returns the loss and its gradient for checking. */
 IBG_API size_t ibg_lpc_num_params(void);
-IBG_API int ibg_lpc_generate(ibg_context* ctx, int nconfig, double t0, double t1, int nres, unsigned int seed,
-                             float* geom, float* r, float* zb);
-IBG_API int ibg_lpc_train(ibg_context* ctx, int nsamp, const float* geom, const float* r, const float* zb, int epochs,
-                          int batch, float lr, unsigned int seed, float* loss_history);
-IBG_API int ibg_lpc_loss_grad(ibg_context* ctx, int nsamp, const float* geom, const float* r, const float* zb,
+IBG_API int ibg_lpc_generate(ibg_context* ctx, int nconfig, double t0, double t1, float* geom, float* mb);
+IBG_API int ibg_lpc_train(ibg_context* ctx, int nconfig, const float* geom, const float* mb, int epochs, int batch,
+                          float lr, unsigned int seed, float* loss_history);
+IBG_API int ibg_lpc_loss_grad(ibg_context* ctx, int nconfig, const float* geom, const float* mb,
                               const float* params, float* loss, float* grad);
 IBG_API int ibg_lpc_get_params(ibg_context* ctx, float* params, size_t n);
 IBG_API int ibg_lpc_set_params(ibg_context* ctx, const float* params, size_t n);
-/* z = P_k r with the current network at the current body configuration (host
+/* z = K_k r with the current network at the current body configuration (host
  * buffers of 2 npts doubles); geom (optional, npts x 4 floats) receives the
  * geometry features it used */
 IBG_API int ibg_lpc_apply(ibg_context* ctx, int substep, const double* r, double* z, float* geom);

@@ -6,32 +6,33 @@ no counterpart: it solves the moving-body force system with plain CG
 (src/ConjugateGradientSolver.cc:35-65); the network only preconditions that
 same solve, so what the oracle pins is the network arithmetic itself.
 
-Network (per boundary point i, N(i) = up to 8 neighbours i +- 1..4 along the
-body, wrapping on closed curves):
-  a_i  = (x, y, nx, ny, rx/s, ry/s),  s = rms(r)
-  h1_i = relu(W1 [a_i | mean_N a_j] + b1)          12 -> 256
-  h2_i = relu(W2 [h1_i | mean_N h1_j] + b2)        512 -> 256
-  o_i  = W3 h2_i + b3                               256 -> 2
-Loss: mean over samples of |o - t|^2 / (|t|^2 + 1e-12), t = zb / s.
+Network, per ordered pair (i, j) of boundary points:
+  x_ij = [g_i, gbar_i, g_j, gbar_j, x_i - x_j, y_i - y_j, |p_i - p_j|]   19
+  h1 = relu(W1 x + b1), h2 = relu(W2 h1 + b2), k_ij = W3 h2 + b3         -> 4
+g = (x, y, nx, ny) per point, gbar its mean over up to 8 boundary neighbours
+(i +- 1..4, wrapping on closed curves).  Kraw[a P + i][c P + j] = k_ij[2a + c],
+K = (Kraw + Kraw^T) / 2.  Loss: mean over configurations of
+|K Mn - I|_F^2 / m with Mn = Mb / c0 (Mb = M / beta, c0 the last parameter).
 """
 from __future__ import annotations
 
 import numpy as np
 
-K_IN, K_IN2, K_H, K_H2, K_OUT = 6, 12, 256, 512, 2
+K_F, K_H, K_O = 19, 256, 4
 O_W1 = 0
-O_B1 = O_W1 + K_H * K_IN2
+O_B1 = O_W1 + K_H * K_F
 O_W2 = O_B1 + K_H
-O_B2 = O_W2 + K_H * K_H2
+O_B2 = O_W2 + K_H * K_H
 O_W3 = O_B2 + K_H
-O_B3 = O_W3 + K_OUT * K_H
-N_PARAMS = O_B3 + K_OUT
+O_B3 = O_W3 + K_O * K_H
+O_C0 = O_B3 + K_O
+N_PARAMS = O_C0 + 1
 
 
 def unpack(p):
     p = np.asarray(p, dtype=np.float64)
-    return (p[O_W1:O_B1].reshape(K_H, K_IN2), p[O_B1:O_W2], p[O_W2:O_B2].reshape(K_H, K_H2), p[O_B2:O_W3],
-            p[O_W3:O_B3].reshape(K_OUT, K_H), p[O_B3:N_PARAMS])
+    return (p[O_W1:O_B1].reshape(K_H, K_F), p[O_B1:O_W2], p[O_W2:O_B2].reshape(K_H, K_H), p[O_B2:O_W3],
+            p[O_W3:O_B3].reshape(K_O, K_H), p[O_B3:O_C0], float(p[O_C0]))
 
 
 def neighbours(bodies_xy):
@@ -64,65 +65,68 @@ def neighbours(bodies_xy):
     return np.array(nbr, dtype=np.int64), np.array(cnt, dtype=np.int64)
 
 
-def _nbr_mean(x, nbr, cnt):
-    """x [B, P, C] -> mean over each point's neighbours."""
-    out = np.zeros_like(x)
+def nbr_mean(g, nbr, cnt):
+    """g [B, P, C] -> mean over each point's neighbours."""
+    out = np.zeros_like(g)
     for q in range(8):
         has = cnt > q
         idx = np.where(has, nbr[:, q], 0)
-        out += x[:, idx, :] * has[None, :, None]
+        out += g[:, idx, :] * has[None, :, None]
     return out / np.maximum(cnt, 1)[None, :, None] * (cnt > 0)[None, :, None]
 
 
-def forward(params, geom, r, nbr, cnt):
-    """Outputs o [B, P, 2] and the intermediates of one batch."""
-    W1, b1, W2, b2, W3, b3 = unpack(params)
-    geom = np.asarray(geom, dtype=np.float64)
-    r = np.asarray(r, dtype=np.float64)
-    B, P = r.shape[0], r.shape[1] // 2
-    s = np.sqrt(np.mean(r * r, axis=1)) + 1e-30
-    feats = np.concatenate([geom, (r[:, :P] / s[:, None])[..., None], (r[:, P:] / s[:, None])[..., None]], axis=2)
-    A = np.concatenate([feats, _nbr_mean(feats, nbr, cnt)], axis=2)        # [B, P, 12]
-    h1 = np.maximum(A @ W1.T + b1, 0.0)
-    C = np.concatenate([h1, _nbr_mean(h1, nbr, cnt)], axis=2)               # [B, P, 512]
-    h2 = np.maximum(C @ W2.T + b2, 0.0)
-    o = h2 @ W3.T + b3
-    return o, dict(s=s, A=A, h1=h1, C=C, h2=h2)
+def pair_inputs(geom, nbr, cnt):
+    g = np.asarray(geom, dtype=np.float64)
+    B, P = g.shape[0], g.shape[1]
+    gb = nbr_mean(g, nbr, cnt)
+    gi = np.broadcast_to(g[:, :, None, :], (B, P, P, 4))
+    gj = np.broadcast_to(g[:, None, :, :], (B, P, P, 4))
+    bi = np.broadcast_to(gb[:, :, None, :], (B, P, P, 4))
+    bj = np.broadcast_to(gb[:, None, :, :], (B, P, P, 4))
+    d = gi[..., :2] - gj[..., :2]
+    return np.concatenate([gi, bi, gj, bj, d, np.sqrt((d * d).sum(-1, keepdims=True))], axis=-1)  # [B,P,P,19]
 
 
-def loss_grad(params, geom, r, zb, nbr, cnt):
-    """Mean loss and its gradient with respect to the packed parameters."""
-    W1, b1, W2, b2, W3, b3 = unpack(params)
-    o, c = forward(params, geom, r, nbr, cnt)
-    B, P = o.shape[0], o.shape[1]
-    zb = np.asarray(zb, dtype=np.float64)
-    t = np.stack([zb[:, :P], zb[:, P:]], axis=2) / c["s"][:, None, None]   # [B, P, 2]
-    e = o - t
-    denom = np.sum(t * t, axis=(1, 2)) + 1e-12
-    loss = np.mean(np.sum(e * e, axis=(1, 2)) / denom)
-    do = 2.0 * e / (denom[:, None, None] * B)
+def forward(params, geom, nbr, cnt):
+    """K [B, m, m] (before the 1 / (c0 beta) scale) and the intermediates."""
+    W1, b1, W2, b2, W3, b3, c0 = unpack(params)
+    X = pair_inputs(geom, nbr, cnt)
+    B, P = X.shape[0], X.shape[1]
+    h1 = np.maximum(X @ W1.T + b1, 0.0)
+    h2 = np.maximum(h1 @ W2.T + b2, 0.0)
+    k = h2 @ W3.T + b3                                              # [B,P,P,4]
+    Kraw = k.reshape(B, P, P, 2, 2).transpose(0, 3, 1, 4, 2).reshape(B, 2 * P, 2 * P)
+    K = 0.5 * (Kraw + Kraw.transpose(0, 2, 1))
+    return K, dict(X=X, h1=h1, h2=h2, c0=c0)
+
+
+def loss_grad(params, geom, mb, nbr, cnt):
+    """Mean loss and its gradient with respect to the packed parameters (the c0 entry gets 0)."""
+    W1, b1, W2, b2, W3, b3, c0 = unpack(params)
+    K, c = forward(params, geom, nbr, cnt)
+    B, m = K.shape[0], K.shape[1]
+    P = m // 2
+    Mn = np.asarray(mb, dtype=np.float64) / c0
+    E = K @ Mn - np.eye(m)
+    loss = float(np.mean(np.sum(E * E, axis=(1, 2)) / m))
+    dE = 2.0 * E / (B * m)
+    dK = dE @ Mn.transpose(0, 2, 1)
+    dKraw = 0.5 * (dK + dK.transpose(0, 2, 1))
+    dk = dKraw.reshape(B, 2, P, 2, P).transpose(0, 2, 4, 1, 3).reshape(B, P, P, 4)
+    X, h1, h2 = c["X"], c["h1"], c["h2"]
     g = np.zeros(N_PARAMS)
-    h2, C, h1, A = c["h2"], c["C"], c["h1"], c["A"]
-    g[O_W3:O_B3] = np.einsum("bpc,bpk->ck", do, h2).ravel()
-    g[O_B3:N_PARAMS] = do.sum(axis=(0, 1))
-    dh2 = (do @ W3) * (h2 > 0)
-    g[O_W2:O_B2] = np.einsum("bpo,bpk->ok", dh2, C).ravel()
-    g[O_B2:O_W3] = dh2.sum(axis=(0, 1))
-    dC = dh2 @ W2
-    # the neighbour mean's adjoint: point j receives dC_i[256:] / cnt_i from every i with j in N(i)
-    dmean = dC[:, :, K_H:] / np.maximum(cnt, 1)[None, :, None]
-    dh1 = dC[:, :, :K_H].copy()
-    for q in range(8):
-        has = cnt > q
-        for i in np.nonzero(has)[0]:
-            dh1[:, nbr[i, q], :] += dmean[:, i, :]
-    dh1 *= h1 > 0
-    g[O_W1:O_B1] = np.einsum("bpo,bpk->ok", dh1, A).ravel()
-    g[O_B1:O_W2] = dh1.sum(axis=(0, 1))
+    g[O_W3:O_B3] = np.einsum("bijq,bijk->qk", dk, h2).ravel()
+    g[O_B3:O_C0] = dk.sum(axis=(0, 1, 2))
+    dh2 = (dk @ W3) * (h2 > 0)
+    g[O_W2:O_B2] = np.einsum("bijo,bijk->ok", dh2, h1).ravel()
+    g[O_B2:O_W3] = dh2.sum(axis=(0, 1, 2))
+    dh1 = (dh2 @ W2) * (h1 > 0)
+    g[O_W1:O_B1] = np.einsum("bijo,bijk->ok", dh1, X).ravel()
+    g[O_B1:O_W2] = dh1.sum(axis=(0, 1, 2))
     return loss, g
 
 
-def apply(params, geom, r, nbr, cnt, beta):
-    """z = (s / beta) o for one residual r [2P] (the preconditioner action)."""
-    o, c = forward(params, geom[None], np.asarray(r, dtype=np.float64)[None], nbr, cnt)
-    return np.concatenate([o[0, :, 0], o[0, :, 1]]) * c["s"][0] / beta
+def operator(params, geom, nbr, cnt, beta):
+    """The preconditioner matrix K / (c0 beta) for one configuration geom [P, 4]."""
+    K, c = forward(params, np.asarray(geom)[None], nbr, cnt)
+    return K[0] / (c["c0"] * beta)
