@@ -1,23 +1,42 @@
-"""Benchmark of the IBPM time step on B200: timesteps/s on the multi-domain
-shedding-cylinder workload (400x200 cells, 5 nested domains, 157-point
-cylinder, Re 200, dt 0.005, RK3, seeded 1e-3 vorticity noise in the wake).
+"""Benchmark of the IBPM time step on B200 (timesteps/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c2|c3|c4] [--form ...]
+
+Workloads (seeded synthetic inputs; no dataset is involved):
+
+* c2 (default) multi-domain shedding cylinder: 400x200 cells, 5 nested
+  domains, 157-point cylinder, Re 200, dt 0.005, RK3, seeded 1e-3 vorticity
+  noise in the wake; forms fp64 (plain, default) and fp32 (FP32 bulk, FP64
+  force solve).
+* c3 pitching and plunging plate: 500x250 cells, 3 domains, 51 points,
+  Re 300, dt 0.004, CG tolerance 1e-10; forms cg (the reference's plain CG),
+  cholesky (flexible PCG with the exact inverse rebuilt every 10 steps,
+  default) and learned (flexible PCG with the learned preconditioner,
+  trained first; training time reported, not timed).
+* c4 ensemble of 64 independent ellipse runs (n in {128..512}, 1-3 domains,
+  seeded b, orientation, Re; dt = 0.5 dx): forms ensemble (all members' steps
+  as branches of one CUDA graph, default) and serial (each member's captured
+  step launched after the other on one stream).
 
 One process per GPU (torchrun for N > 1).  One simulation does not shard
 (its multi-domain solve is global per level and levels are serially
 dependent), so N GPUs run N independent replicas (weak scaling) and `value`
-is the total timesteps/s of the job.  Rank 0 prints one JSON line.
+is the total timesteps/s of the job (member-timesteps/s for c4).  Rank 0
+prints one JSON line.
 
 * value        K steps with the state resident in HBM, CUDA events around each
-               step on the solver's stream, L2 flushed (256 MB write) between
+               step on the stream it runs on, L2 flushed (256 MB write) between
                steps outside the timed events; max over ranks.
+* plain        (c2 fp32, c3, c4) the plain FP64 GPU path of the same workload
+               timed the same way, with the relative L2 difference of the
+               forces of the two runs over the same steps.
 * e2e          the same metric through the public API with host buffers: every
                step uploads omega, q, f from pinned host memory, advances one
                step and reads the boundary force f back.
-* roofline     the dominant kernel (the column pass of the DST-I solve) timed
-               alone with CUDA events on the solver's stream against the
-               measured HBM copy bandwidth.
+* roofline     the DST-I column pass (the dominant kernel) timed alone with
+               CUDA events on the solver's stream against the measured HBM
+               copy bandwidth.
 * cpu_baseline the reference's own CPU code (oracle/_ref/ref_driver: the
                reference sources built with -Ofast and the FFTW shim), one core,
                a bounded sample of steps of the same workload.
@@ -34,8 +53,14 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "timesteps/s (400x200 x5-domain shedding cylinder, RK3)"
 UNIT = "timesteps/s"
+METRICS = {
+    "c2": "timesteps/s (400x200 x5-domain shedding cylinder, RK3)",
+    "c3": "timesteps/s (500x250 x3-domain pitching/plunging plate, RK3, CG tol 1e-10)",
+    "c4": "member-timesteps/s (ensemble of 64 ellipse runs, n 128-512, 1-3 domains, RK3)",
+}
+FORMS = {"c2": ("fp64", "fp32"), "c3": ("cholesky", "learned", "cg"), "c4": ("ensemble", "serial")}
+PLAIN = {"c2": "fp64", "c3": "cg", "c4": "serial"}
 
 
 def _dist():
@@ -45,12 +70,16 @@ def _dist():
     return ws, rank, local
 
 
-def _config(wl, precision):
-    return {"workload": wl.name, "nx": wl.nx, "ny": wl.ny, "ngrid": wl.ngrid, "length": wl.length,
-            "Re": wl.Re, "dt": wl.dt, "scheme": wl.scheme, "boundary_points": 157,
-            "force_solve": "cholesky (fixed body)", "form": precision,
-            "l2": "flushed between timed steps (256 MB write outside the events)",
-            "initial_condition": f"seeded N(0, {wl.noise_amp:g}^2) level-0 wake vorticity (seed {wl.noise_seed})"}
+def _config(workload, form, wl=None, extra=None):
+    c = {"workload": workload, "form": form, "l2": "flushed between timed steps (256 MB write outside the events)"}
+    if wl is not None:
+        c.update({"name": wl.name, "nx": wl.nx, "ny": wl.ny, "ngrid": wl.ngrid, "length": wl.length, "Re": wl.Re,
+                  "dt": wl.dt, "scheme": wl.scheme, "cg_tol": wl.tol})
+        if wl.noise_amp:
+            c["initial_condition"] = f"seeded N(0, {wl.noise_amp:g}^2) level-0 wake vorticity (seed {wl.noise_seed})"
+    if extra:
+        c.update(extra)
+    return c
 
 
 class ClockSampler:
@@ -112,63 +141,268 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def cpu_baseline(wl, steps=10):
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own code on the host cores (bounded samples)
+# ---------------------------------------------------------------------------
+def _c4_sample():
+    from ibpm_b200 import configs
+    small = [w for w in configs.ensemble_members() if w.nx <= 256][:2]
+    return small
+
+
+def cpu_baseline(workload, steps=None):
     from oracle import ref_runner
+    from ibpm_b200 import configs
     if not ref_runner.available():
         return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
                 "sample": "unavailable: oracle/_ref/ref_driver not built"}
-    r = ref_runner.run(wl, "c2", steps=steps, warmup=1)
-    return {"value": r["steps_per_s"], "unit": UNIT, "cores": 1, "kind": "reference",
-            "sample": f"{r['timed_steps']} RK3 steps of the same workload after 1 warm-up step, Cholesky factors "
-                      f"from the reference's own cache (init {r['init_s']:.1f} s excluded), "
-                      f"reference sources -Ofast + project DST-I FFTW shim, 1 core of {ref_runner.host_cpu()}"}
+    cpu = ref_runner.host_cpu()
+    if workload == "c2":
+        n = steps or 10
+        r = ref_runner.run(configs.c2_shedding_cylinder(), "c2", steps=n, warmup=1)
+        return {"value": r["steps_per_s"], "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": f"{r['timed_steps']} RK3 steps of the same workload after 1 warm-up step, Cholesky set-up "
+                          f"(init {r['init_s']:.1f} s) excluded, reference sources -Ofast + project DST-I FFTW "
+                          f"shim, 1 core of {cpu}"}
+    if workload == "c3":
+        n = steps or 2
+        r = ref_runner.run(configs.c3_pitching_plate(), "c3", steps=n, warmup=1)
+        return {"value": r["steps_per_s"], "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": f"{r['timed_steps']} RK3 steps (plain CG force solve, tol 1e-10) after 1 warm-up step, "
+                          f"reference sources -Ofast + project DST-I FFTW shim, 1 core of {cpu}"}
+    n = steps or 3
+    tot_s, tot_n, names = 0.0, 0, []
+    for k, wl in enumerate(_c4_sample()):
+        r = ref_runner.run(wl, f"c4_{wl.name}", steps=n, warmup=1)
+        tot_s += r["timed_steps"] / r["steps_per_s"]
+        tot_n += r["timed_steps"]
+        names.append(f"{wl.name} ({wl.nx}^2, ngrid {wl.ngrid})")
+    return {"value": tot_n / tot_s, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"{n} RK3 steps each of members {', '.join(names)} (the first two with n <= 256; larger "
+                      f"members' CPU Cholesky set-up is too long to sample), Cholesky set-up excluded, 1 core of {cpu}"}
 
 
 def run_reference(args):
     ws, rank, local = _dist()
     if rank != 0:
         return 0
-    from ibpm_b200 import configs
     from oracle import ref_runner
-    wl = configs.c2_shedding_cylinder()
-    base = {"metric": METRIC, "unit": UNIT, "n_gpus": args.gpus, "steps": None, "warmup": None,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": _config(wl, "reference FP64 CPU"), "impl": "reference"}
+    wlname = args.workload
     if not ref_runner.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_driver is not built on this host"}))
         return 0
-    steps = max(1, min(args.steps, 20))
-    warm = max(1, min(args.warmup, 2))
-    r = ref_runner.run(wl, "c2", steps=steps, warmup=warm)
-    v = r["steps_per_s"]
-    base.update({"steps": r["timed_steps"], "warmup": warm, "value": v, "ms_per_step": 1000.0 / v,
-                 "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
-                                  "sample": f"{r['timed_steps']} steps after {warm} warm-up (requested --steps "
-                                            f"{args.steps}; capped at 20 to bound CPU time), Cholesky set-up "
-                                            f"{r['init_s']:.1f} s excluded, single-threaded reference on "
-                                            f"1 core of {ref_runner.host_cpu()}"},
-                 "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
-    print(json.dumps(base))
+    cap = {"c2": 20, "c3": 3, "c4": 3}[wlname]
+    steps = max(1, min(args.steps, cap))
+    cb = cpu_baseline(wlname, steps=steps)
+    v = cb["value"]
+    out = {"metric": METRICS[wlname], "unit": UNIT, "n_gpus": args.gpus, "steps": steps, "warmup": 1,
+           "value": v, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": "synthetic", "config": _config(wlname, "reference FP64 CPU"), "impl": "reference",
+           "cpu_baseline": dict(cb, sample=cb["sample"] + f" (requested --steps {args.steps}; capped at {cap} to "
+                                                          f"bound CPU time)"),
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
     return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def time_steps(K, stream, step, flush):
+    """K steps, each bracketed by CUDA events on `stream`, L2 flushed before each; returns ms."""
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    launches = 0
+    with torch.cuda.stream(stream):
+        for k in range(K):
+            flush.zero_()
+            ev[k][0].record(stream)
+            launches += step()
+            ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in ev), launches
+
+
+def rel_l2(a, b):
+    import numpy as np
+    a, b = np.asarray(a, dtype=float), np.asarray(b, dtype=float)
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
+class Single:
+    """One simulation (c2, c3) in a given form."""
+
+    def __init__(self, workload, form, stream, device):
+        import ibpm_b200 as ib
+        from ibpm_b200 import configs
+        self.wl = configs.c2_shedding_cylinder() if workload == "c2" else configs.c3_pitching_plate()
+        kw = {}
+        if workload == "c2":
+            kw["precision"] = form
+        else:
+            kw["precond"] = {"cg": "none", "cholesky": "cholesky", "learned": "learned"}[form]
+            kw["pc_refresh"] = 10
+        self.grid, self.model, self.s, self.x = ib.from_workload(self.wl, stream=stream.cuda_stream, device=device,
+                                                                 **kw)
+        self.extra = {}
+        if form == "learned":
+            t0 = time.perf_counter()
+            geom, mb = self.s.lpc_generate(32, 0.0, 8.0)
+            t1 = time.perf_counter()
+            hist = self.s.lpc_train(geom, mb, epochs=500, batch=4, lr=1e-3, seed=1)
+            t2 = time.perf_counter()
+            self.extra = {"training": {"configurations": 32, "times": [0.0, 8.0], "epochs": 500, "batch": 4,
+                                       "generate_s": t1 - t0, "train_s": t2 - t1, "loss_first": float(hist[0]),
+                                       "loss_last": float(hist[-1])}}
+        self.s.init()
+        self.s.set_state(self.x, with_q=False)
+        self.stream = stream
+
+    def step(self):
+        self.s.advance_resident(1)
+        return self.s.last_launch_count()
+
+    def forces(self, K):
+        return self.s.force_history(K)
+
+    def iterations(self):
+        it, n = self.s.cg_totals()
+        return it, n
+
+    def e2e(self, Ke, sync):
+        import torch
+        import ibpm_b200 as ib
+        x = self.x
+        s = self.s
+        s.get_state(x)
+        om = torch.empty(x.omega.shape, dtype=torch.float64, pin_memory=True).numpy()
+        qh = torch.empty(x.q.shape, dtype=torch.float64, pin_memory=True).numpy()
+        fh = torch.empty(x.f.shape, dtype=torch.float64, pin_memory=True).numpy()
+        om[...] = x.omega
+        qh[...] = x.q
+        fh[...] = x.f
+        xs = ib.State(self.grid, x.f.size // 2, omega=om, q=qh, f=fh, timestep=x.timestep, time=x.time)
+        sync()
+        t0 = time.perf_counter()
+        for _ in range(Ke):
+            s.set_state(xs)                                   # H2D omega, q, f
+            s.advance_resident(1)
+            ib._native.check(ib._native.lib().ibg_get_boundary_force(s.handle, ib._ptr(fh), None, None), s.handle)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, int(8 * (x.omega.size + x.q.size + x.f.size)), int(8 * x.f.size)
+
+    def roof_solver(self):
+        return self.s, self.stream
+
+    def close(self):
+        self.s.close()
+
+
+class Ens:
+    """The 64-member ensemble (c4): one graph (ensemble) or member after member (serial)."""
+
+    def __init__(self, form, stream, device, count=64):
+        import ibpm_b200 as ib
+        from ibpm_b200 import configs
+        import torch
+        self.members = []
+        for wl in configs.ensemble_members(count=count):
+            grid, model, s, x = ib.from_workload(wl, stream=stream.cuda_stream, device=device)
+            s.init()
+            s.set_state(x, with_q=False)
+            self.members.append((wl, grid, s, x))
+        self.form = form
+        self.ens = None
+        self.stream = stream
+        self.member_stream = stream
+        if form == "ensemble":
+            self.ens = ib.Ensemble([m[2] for m in self.members])
+            self.stream = torch.cuda.ExternalStream(self.ens.stream(), device=torch.device("cuda", device))
+        self.extra = {"members": len(self.members),
+                      "grid_points_all_levels": int(sum(w.nx * w.ny * w.ngrid for w, *_ in self.members)),
+                      "boundary_points": [int(m[3].f.size // 2) for m in self.members][:8] + ["..."]}
+
+    def step(self):
+        if self.ens is not None:
+            self.ens.advance(1)
+            return self.ens.launches_per_step()
+        n = 0
+        for _, _, s, _ in self.members:
+            s.advance_resident(1)
+            n += s.last_launch_count()
+        return n
+
+    def forces(self, K):
+        import numpy as np
+        return np.concatenate([m[2].force_history(K) for m in self.members])
+
+    def e2e(self, Ke, sync):
+        import torch
+        import ibpm_b200 as ib
+        import numpy as np
+        hs = []
+        for wl, grid, s, x in self.members:
+            s.get_state(x)
+            om = torch.empty(x.omega.shape, dtype=torch.float64, pin_memory=True).numpy()
+            qh = torch.empty(x.q.shape, dtype=torch.float64, pin_memory=True).numpy()
+            fh = torch.empty(x.f.shape, dtype=torch.float64, pin_memory=True).numpy()
+            om[...] = x.omega
+            qh[...] = x.q
+            fh[...] = x.f
+            hs.append((s, ib.State(grid, x.f.size // 2, omega=om, q=qh, f=fh, timestep=x.timestep, time=x.time), fh))
+        sync()
+        t0 = time.perf_counter()
+        for _ in range(Ke):
+            for s, xs, _ in hs:
+                s.set_state(xs)
+            self.step()
+            for s, _, fh in hs:
+                ib._native.check(ib._native.lib().ibg_get_boundary_force(s.handle, ib._ptr(fh), None, None),
+                                 s.handle)
+        torch.cuda.synchronize()
+        bi = sum(int(8 * (x.omega.size + x.q.size + x.f.size)) for *_, x in self.members)
+        bo = sum(int(8 * x.f.size) for *_, x in self.members)
+        return time.perf_counter() - t0, bi, bo
+
+    def roof_solver(self):
+        # the largest member (it runs on the members' stream)
+        return max(self.members, key=lambda m: m[0].nx * m[0].ny * m[0].ngrid)[2], self.member_stream
+
+    def close(self):
+        if self.ens is not None:
+            self.ens.close()
+        for m in self.members:
+            m[2].close()
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--warmup", type=int, default=None)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_refined"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4"])
+    ap.add_argument("--form", default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-path comparison run")
+    ap.add_argument("--profile", action="store_true",
+                    help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off) "
+                         "and skip the e2e, roofline, plain and CPU legs")
     args = ap.parse_args()
+    wlname = args.workload
+    if args.steps is None:
+        args.steps = {"c2": 200, "c3": 50, "c4": 20}[wlname]
+    if args.warmup is None:
+        args.warmup = {"c2": 10, "c3": 3, "c4": 3}[wlname]
     if args.impl == "reference":
         return run_reference(args)
+    form = args.form or FORMS[wlname][0]
+    if form not in FORMS[wlname]:
+        raise SystemExit(f"--form for {wlname} must be one of {FORMS[wlname]}")
 
-    import numpy as np
     import torch
     import torch.distributed as dist
-    import ibpm_b200 as ib
-    from ibpm_b200 import configs
 
     ws, rank, local = _dist()
     if ws > 1:
@@ -176,84 +410,101 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    wl = configs.c2_shedding_cylinder()
-    stream = torch.cuda.Stream(device=dev)
-    grid, model, s, x = ib.from_workload(wl, precision=args.precision, stream=stream.cuda_stream, device=local)
-    s.init()
-    s.set_state(x, with_q=False)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
     W = max(3, args.warmup)
     K = max(1, args.steps)
-    s.advance_resident(W)
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
-    torch.cuda.synchronize()
-    if ws > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
+
+    def build(f):
+        stream = torch.cuda.Stream(device=dev)
+        return Ens(f, stream, local) if wlname == "c4" else Single(wlname, f, stream, local)
+
+    def maxrank(v):
+        if ws > 1:
+            t = torch.tensor([v], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return v
+
+    def sync():
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    run = build(form)
+    for _ in range(W):
+        run.step()
+    it0 = run.iterations() if hasattr(run, "iterations") else None
+    sync()
     clocks = ClockSampler(local)
     clocks.start()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
-    launches = 0
-    with torch.cuda.stream(stream):
-        for k in range(K):
-            flush.zero_()
-            ev[k][0].record(stream)
-            s.advance_resident(1)
-            ev[k][1].record(stream)
-            launches += s.last_launch_count()
-    torch.cuda.synchronize()
+    if args.profile:
+        torch.cuda.cudart().cudaProfilerStart()
+    ms, launches = time_steps(K, run.stream, run.step, flush)
+    if args.profile:
+        torch.cuda.cudart().cudaProfilerStop()
     clk = clocks.stop()
-    ms = sum(a.elapsed_time(b) for a, b in ev)
-    if ws > 1:
-        dist.barrier()
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = ws * K / (ms / 1000.0)
-    forces = s.force_history(K)
+    ms = maxrank(ms)
+    per_step_units = len(run.members) if wlname == "c4" else 1
+    value = ws * K * per_step_units / (ms / 1000.0)
+    forces = run.forces(W + K)
+    cg = None
+    if it0 is not None:
+        it1 = run.iterations()
+        solves = it1[1] - it0[1]
+        cg = {"iterations_per_solve": (it1[0] - it0[0]) / max(1, solves), "solves": solves}
 
-    # ---- e2e through the public API with pinned host buffers
-    Ke = min(K, 50)
-    om = torch.empty(x.omega.shape, dtype=torch.float64, pin_memory=True).numpy()
-    qh = torch.empty(x.q.shape, dtype=torch.float64, pin_memory=True).numpy()
-    fh = torch.empty(x.f.shape, dtype=torch.float64, pin_memory=True).numpy()
-    s.get_state(x)
-    om[...] = x.omega
-    qh[...] = x.q
-    fh[...] = x.f
-    xs = ib.State(grid, x.f.size // 2, omega=om, q=qh, f=fh, timestep=x.timestep, time=x.time)
-    torch.cuda.synchronize()
-    if ws > 1:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(Ke):
-        s.set_state(xs)                                   # H2D omega, q, f
-        s.advance_resident(1)
-        ib._native.check(ib._native.lib().ibg_get_boundary_force(s.handle, ib._ptr(fh), None, None), s.handle)
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if ws > 1:
-        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = {"value": ws * Ke / e2e_s, "unit": UNIT,
-           "h2d_bytes_per_step": int(8 * (x.omega.size + x.q.size + x.f.size)),
-           "d2h_bytes_per_step": int(8 * x.f.size)}
+    if args.profile:
+        run.close()
+        if rank == 0:
+            print(json.dumps({"metric": METRICS[wlname], "value": value, "unit": UNIT, "profile_run": True,
+                              "ms_per_step": ms / K, "steps": K, "gpu_launches": int(launches)}))
+        if ws > 1:
+            dist.destroy_process_group()
+        return 0
+    Ke = min(K, 20 if wlname != "c2" else 50)
+    e2e_s, bi, bo = run.e2e(Ke, sync)
+    e2e_s = maxrank(e2e_s)
+    e2e = {"value": ws * Ke * per_step_units / e2e_s, "unit": UNIT, "h2d_bytes_per_step": bi,
+           "d2h_bytes_per_step": bo}
+    roof = kernel_roofline(*run.roof_solver(), dtype="float" if form == "fp32" else "double")
+    extra = dict(run.extra)
+    run.close()
 
-    # ---- roofline of the dominant kernel (DST-I column pass, finest level) timed alone
-    roof = kernel_roofline(s, grid, stream)
-    s.close()
-    out = None
+    plain = None
+    if form != PLAIN[wlname] and not args.no_plain:
+        p = build(PLAIN[wlname])
+        for _ in range(W):
+            p.step()
+        pit0 = p.iterations() if hasattr(p, "iterations") else None
+        sync()
+        pms, _ = time_steps(K, p.stream, p.step, flush)
+        pms = maxrank(pms)
+        pforces = p.forces(W + K)
+        plain = {"form": PLAIN[wlname], "value": ws * K * per_step_units / (pms / 1000.0), "ms_per_step": pms / K,
+                 "force_rel_l2_vs_plain": rel_l2(forces, pforces)}
+        if pit0 is not None:
+            pit1 = p.iterations()
+            plain["iterations_per_solve"] = (pit1[0] - pit0[0]) / max(1, pit1[1] - pit0[1])
+        plain["speedup"] = value / plain["value"]
+        p.close()
+
     if rank == 0:
-        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
+        wl = getattr(run, "wl", None)
+        dtype = {"fp32": "f32+f64"}.get(form, "f64")
+        out = {"metric": METRICS[wlname], "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
                "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-               "dtype": "f64" if args.precision == "fp64" else "f32+f64",
-               "data": "synthetic (seeded noise initial condition, generated geometry)",
-               "config": _config(wl, args.precision), "e2e": e2e, "gpu_launches": int(launches),
+               "dtype": dtype, "data": "synthetic (seeded initial conditions and generated geometry)",
+               "config": _config(wlname, form, wl, extra), "e2e": e2e, "gpu_launches": int(launches),
                "roofline": roof, "clocks": clk,
                "final_force": [float(forces[-1][0]), float(forces[-1][1])] if len(forces) else None}
+        if cg:
+            out["cg"] = cg
+        if plain:
+            out["plain"] = plain
         if ws == 1 and not args.no_cpu_baseline:
             try:
-                out["cpu_baseline"] = cpu_baseline(wl)
+                out["cpu_baseline"] = cpu_baseline(wlname)
             except Exception as e:  # the baseline is reported, never required
                 out["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
                                        "sample": f"failed: {e}"}
@@ -263,14 +514,13 @@ def main():
     return 0
 
 
-def kernel_roofline(s, grid, stream, reps=200):
+def kernel_roofline(s, stream, reps=200, dtype="double"):
     import torch
     import ibpm_b200 as ib
     L = ib._native.lib()
     res = {}
     peak, kind = peaks()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    best = None
     for which, name in ((0, "dst_rows"), (1, "dst_cols"), (2, "nonlinear_node_vel")):
         L.ibg_run_kernel(s.handle, which, 5)
         torch.cuda.synchronize()
@@ -279,12 +529,11 @@ def kernel_roofline(s, grid, stream, reps=200):
         e1.record(stream)
         torch.cuda.synchronize()
         us = 1000.0 * e0.elapsed_time(e1) / reps
-        res[name] = {"us_per_launch": us, "algorithmic_bytes": nbytes}
-        if best is None or name == "dst_cols":
-            best = name
-    d = res[best]
+        res[name] = {"us_per_launch": us, "algorithmic_bytes": nbytes,
+                     "GBps": nbytes / (us * 1e-6) / 1e9 if us > 0 else None}
+    d = res["dst_cols"]
     achieved = d["algorithmic_bytes"] / (d["us_per_launch"] * 1e-6) / 1e9
-    return {"kernel": "k_dst_cols<double> (forward DST-I along i of every level of one solve)",
+    return {"kernel": f"k_dst_cols<{dtype}> (forward DST-I along i of every level of one solve)",
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_kind": f"{kind} (copy bandwidth, burst)", "traffic": None, "kernels": res}
 
