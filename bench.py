@@ -31,9 +31,10 @@ prints one JSON line.
 * plain        (c2 fp32, c3, c4) the plain FP64 GPU path of the same workload
                timed the same way, with the relative L2 difference of the
                forces of the two runs over the same steps.
-* e2e          the same metric through the public API with host buffers: every
-               step uploads omega, q, f from pinned host memory, advances one
-               step and reads the boundary force f back.
+* e2e          the same metric through the public API with the state on the
+               host, as the reference's IBSolver::advance(State&) contract has
+               it: every step uploads omega, q, f from pinned host memory,
+               advances one step and reads omega, q, f back.
 * roofline     the DST-I column pass (the dominant kernel) timed alone with
                CUDA events on the solver's stream against the measured HBM
                copy bandwidth.
@@ -230,6 +231,41 @@ def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
 
 
+def _pinned_state(x):
+    """Pinned host copies of a State's arrays plus its step counter and time."""
+    import torch
+    h = {}
+    for k in ("omega", "q", "f"):
+        a = getattr(x, k)
+        h[k] = torch.empty(a.shape, dtype=torch.float64, pin_memory=True).numpy()
+        h[k][...] = a
+    h["ts"], h["t"] = int(x.timestep), float(x.time)
+    return h
+
+
+def _upload(s, h):
+    import ibpm_b200 as ib
+    L = ib._native.lib()
+    ib._native.check(L.ibg_set_state(s.handle, ib._ptr(h["omega"]), ib._ptr(h["q"]), ib._ptr(h["f"]), h["ts"],
+                                     h["t"]), s.handle)
+
+
+def _download(s, h):
+    import ctypes
+    import ibpm_b200 as ib
+    L = ib._native.lib()
+    ts, t = ctypes.c_int(), ctypes.c_double()
+    ib._native.check(L.ibg_get_state(s.handle, ib._ptr(h["omega"]), ib._ptr(h["q"]), ib._ptr(h["f"]),
+                                     ctypes.byref(ts), ctypes.byref(t)), s.handle)
+    h["ts"], h["t"] = ts.value, t.value
+
+
+def _round_trip(s, h, advance):
+    _upload(s, h)
+    advance(1)
+    _download(s, h)
+
+
 class Single:
     """One simulation (c2, c3) in a given form."""
 
@@ -271,26 +307,19 @@ class Single:
         return it, n
 
     def e2e(self, Ke, sync):
+        """The reference's contract (src/IBSolver.cc:142-149): the State lives on
+        the host; every step uploads omega, q, f, advances and reads them back."""
         import torch
-        import ibpm_b200 as ib
         x = self.x
-        s = self.s
-        s.get_state(x)
-        om = torch.empty(x.omega.shape, dtype=torch.float64, pin_memory=True).numpy()
-        qh = torch.empty(x.q.shape, dtype=torch.float64, pin_memory=True).numpy()
-        fh = torch.empty(x.f.shape, dtype=torch.float64, pin_memory=True).numpy()
-        om[...] = x.omega
-        qh[...] = x.q
-        fh[...] = x.f
-        xs = ib.State(self.grid, x.f.size // 2, omega=om, q=qh, f=fh, timestep=x.timestep, time=x.time)
+        self.s.get_state(x)
+        host = _pinned_state(x)
         sync()
         t0 = time.perf_counter()
         for _ in range(Ke):
-            s.set_state(xs)                                   # H2D omega, q, f
-            s.advance_resident(1)
-            ib._native.check(ib._native.lib().ibg_get_boundary_force(s.handle, ib._ptr(fh), None, None), s.handle)
+            _round_trip(self.s, host, self.s.advance_resident)
         torch.cuda.synchronize()
-        return time.perf_counter() - t0, int(8 * (x.omega.size + x.q.size + x.f.size)), int(8 * x.f.size)
+        nb = int(8 * (x.omega.size + x.q.size + x.f.size))
+        return time.perf_counter() - t0, nb, nb
 
     def roof_solver(self):
         return self.s, self.stream
@@ -339,31 +368,21 @@ class Ens:
 
     def e2e(self, Ke, sync):
         import torch
-        import ibpm_b200 as ib
-        import numpy as np
-        hs = []
+        hosts = []
         for wl, grid, s, x in self.members:
             s.get_state(x)
-            om = torch.empty(x.omega.shape, dtype=torch.float64, pin_memory=True).numpy()
-            qh = torch.empty(x.q.shape, dtype=torch.float64, pin_memory=True).numpy()
-            fh = torch.empty(x.f.shape, dtype=torch.float64, pin_memory=True).numpy()
-            om[...] = x.omega
-            qh[...] = x.q
-            fh[...] = x.f
-            hs.append((s, ib.State(grid, x.f.size // 2, omega=om, q=qh, f=fh, timestep=x.timestep, time=x.time), fh))
+            hosts.append((s, _pinned_state(x)))
         sync()
         t0 = time.perf_counter()
         for _ in range(Ke):
-            for s, xs, _ in hs:
-                s.set_state(xs)
+            for s, h in hosts:
+                _upload(s, h)
             self.step()
-            for s, _, fh in hs:
-                ib._native.check(ib._native.lib().ibg_get_boundary_force(s.handle, ib._ptr(fh), None, None),
-                                 s.handle)
+            for s, h in hosts:
+                _download(s, h)
         torch.cuda.synchronize()
-        bi = sum(int(8 * (x.omega.size + x.q.size + x.f.size)) for *_, x in self.members)
-        bo = sum(int(8 * x.f.size) for *_, x in self.members)
-        return time.perf_counter() - t0, bi, bo
+        nb = sum(int(8 * (x.omega.size + x.q.size + x.f.size)) for *_, x in self.members)
+        return time.perf_counter() - t0, nb, nb
 
     def roof_solver(self):
         # the largest member (it runs on the members' stream)

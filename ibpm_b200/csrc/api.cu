@@ -840,7 +840,8 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
     }
     int s = IBG_OK;
     const size_t S = c->S, F = c->F, m = c->ncomp;
-    if ((s = c->fft.init(2 * g.ny, 2 * g.nx)) || (s = c->cosT.init(g.nx, g.ny, g.nxe, g.nye))) {
+    if ((s = c->fft.init(2 * g.ny, 2 * g.nx)) || (s = c->cosT.init(g.nx, g.ny, g.nxe, g.nye)) ||
+        (g.L > 1 && (s = c->cosT.build_edge_maps(g.nx, g.ny, g.nxe, g.nye, c->fft)))) {
         g_create_error = "ibg_create: FFT table setup failed";
         delete c;
         return s;

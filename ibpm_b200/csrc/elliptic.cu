@@ -23,11 +23,28 @@
 // odd real sequence is purely imaginary, so DST(a)_k = -Im Z_{k+1} and
 // DST(b)_k = Re Z_{k+1}.  The complex FFT is a shared-memory Stockham
 // autosort FFT with mixed radices; twiddles are tabulated on the host.
+#include <map>
+#include <mutex>
+
 #include "ibg_internal.cuh"
 #include "ibg_kernels.cuh"
 
 
 namespace ibg {
+
+int raise_smem_limit(const void* func, int bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, int> set;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return IBG_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(mu);
+    int& cur = set[{dev, func}];
+    if (bytes <= cur) return IBG_OK;
+    if (cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
+        return IBG_ERR_CUDA;
+    cur = bytes;
+    return IBG_OK;
+}
 
 template <typename T> struct Cplx;
 template <> struct Cplx<double> { using type = double2; };
@@ -504,6 +521,91 @@ __global__ void __launch_bounds__(512) k_sweep_lines(SweepArgs<T> a) {
     dst_pair_block<T>(d, n, e0, e1, Eo, Eo + n, (T)1, s0, s1);
 }
 
+// The lines step is linear in the sums: E0 = norm A V0, E1 = norm A V1 with
+// A = D P D (D the DST-I of the line, P the getBC interpolation to the finer
+// level), the same matrix for every level because every level has the same
+// NI x NJ nodes.  k_edge_map builds A column by column with the FFT steps of
+// k_sweep_lines applied to unit vectors; k_sweep_edges applies it with one
+// warp per output row, spread over the whole GPU instead of two blocks.
+__global__ void __launch_bounds__(512) k_edge_map(FftDesc d, int n, int ext, double* __restrict__ A) {
+    using C = typename Cplx<double>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* s0 = reinterpret_cast<C*>(smem_raw);
+    C* s1 = s0 + d.m;
+    double* v0 = reinterpret_cast<double*>(s1 + d.m);
+    double* v1 = v0 + n;
+    double* u0 = v1 + n;
+    double* u1 = u0 + n;
+    double* e0 = u1 + n;
+    double* e1 = e0 + n;
+    const int k0 = 2 * blockIdx.x, k1 = k0 + 1;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        v0[k] = k == k0 ? 1.0 : 0.0;
+        v1[k] = k == k1 ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    dst_pair_block<double>(d, n, v0, v1, u0, u1, 1.0, s0, s1);
+    for (int i = 1 + threadIdx.x; i <= n; i += blockDim.x) {
+        const int ii = i / 2 + ext;
+        if (i & 1) {
+            e0[i - 1] = 0.5 * (u0[ii - 1] + u0[ii]);
+            e1[i - 1] = 0.5 * (u1[ii - 1] + u1[ii]);
+        } else {
+            e0[i - 1] = u0[ii - 1];
+            e1[i - 1] = u1[ii - 1];
+        }
+    }
+    __syncthreads();
+    dst_pair_block<double>(d, n, e0, e1, u0, u1, 1.0, s0, s1);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        A[(size_t)i * n + k0] = u0[i];
+        if (k1 < n) A[(size_t)i * n + k1] = u1[i];
+    }
+}
+
+__global__ void k_map_to_f32(long n, const double* __restrict__ a, float* __restrict__ b) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) b[t] = (float)a[t];
+}
+
+constexpr int kEdgeRows = 8;  // output rows (warps) per block of k_sweep_edges
+
+// blockIdx.y = 0: bottom/top lines (A_x, V sums), 1: left/right (A_y, W sums);
+// blockIdx.z = batch item
+template <typename T>
+__global__ void __launch_bounds__(32 * kEdgeRows) k_sweep_edges(SweepArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* v = reinterpret_cast<T*>(smem_raw);
+    const GridDev& g = a.g;
+    const int NI = g.NI, NJ = g.NJ;
+    const bool xdir = blockIdx.y == 0;
+    const int n = xdir ? NI : NJ;
+    const int row = blockIdx.x * kEdgeRows + (threadIdx.x >> 5);
+    if ((int)blockIdx.x * kEdgeRows >= n) return;
+    const int b = blockIdx.z;
+    const T* sums = a.vrow + (size_t)b * a.wstride + (xdir ? 0 : 2 * (size_t)NI);
+    for (int k = threadIdx.x; k < 2 * n; k += blockDim.x) v[k] = sums[k];
+    __syncthreads();
+    if (row >= n) return;
+    const T* Ar = (xdir ? a.ax : a.ay) + (size_t)row * n;
+    const int lane = threadIdx.x & 31;
+    T s0 = (T)0, s1 = (T)0;
+    for (int k = lane; k < n; k += 32) {
+        const T w = Ar[k];
+        s0 += w * v[k];
+        s1 += w * v[n + k];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    }
+    if (lane == 0) {
+        T* Eo = a.edges_out + (size_t)b * a.estride + (xdir ? 0 : 2 * (size_t)NI);
+        Eo[row] = s0 * a.norm;
+        Eo[n + row] = s1 * a.norm;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -643,6 +745,37 @@ void CosTables::release() {
     cudaFree(d32);
     d64 = nullptr;
     d32 = nullptr;
+    if (map64) cudaFree(map64);
+    if (map32) cudaFree(map32);
+    map64 = nullptr;
+    map32 = nullptr;
+    t64.ax = t64.ay = nullptr;
+    t32.ax = t32.ay = nullptr;
+}
+
+int CosTables::build_edge_maps(int nx, int ny, int nxe, int nye, const FftTables& ft) {
+    const int NI = nx - 1, NJ = ny - 1;
+    const size_t nmap = (size_t)NI * NI + (size_t)NJ * NJ;
+    if (cudaMalloc(&map64, sizeof(double) * nmap) != cudaSuccess ||
+        cudaMalloc(&map32, sizeof(float) * nmap) != cudaSuccess)
+        return IBG_ERR_CUDA;
+    double* ax = map64;
+    double* ay = map64 + (size_t)NI * NI;
+    auto smem = [](const FftDesc& d, int n) {
+        return sizeof(typename Cplx<double>::type) * 2 * (size_t)d.m + sizeof(double) * 6 * (size_t)n;
+    };
+    const size_t sx = smem(ft.col64, NI), sy = smem(ft.row64, NJ);
+    if (std::max(sx, sy) > 200 * 1024 || raise_smem_limit((const void*)k_edge_map, (int)std::max(sx, sy)))
+        return IBG_ERR_UNSUPPORTED;
+    k_edge_map<<<(NI + 1) / 2, 512, sx>>>(ft.col64, NI, nxe, ax);
+    k_edge_map<<<(NJ + 1) / 2, 512, sy>>>(ft.row64, NJ, nye, ay);
+    k_map_to_f32<<<(unsigned)((nmap + 255) / 256), 256>>>((long)nmap, map64, map32);
+    if (cudaDeviceSynchronize() != cudaSuccess) return IBG_ERR_CUDA;
+    t64.ax = ax;
+    t64.ay = ay;
+    t32.ax = map32;
+    t32.ay = map32 + (size_t)NI * NI;
+    return IBG_OK;
 }
 
 template <typename T>
@@ -799,9 +932,17 @@ int EllipticPlan<T>::solve(const SolveCall<T>& c, cudaStream_t st) const {
         s.vrow = c.sweep + (size_t)L * el;
         s.wstride = es;
         s.norm = norm;
+        s.ax = gt.ax;
+        s.ay = gt.ay;
         const int nrb = (g.NI + kSweepRows - 1) / kSweepRows, ncb = (g.NJ + kSweepCols - 1) / kSweepCols;
         k_sweep_sums<T><<<dim3((unsigned)(nrb + ncb), (unsigned)batch), 256, 0, st>>>(s);
-        k_sweep_lines<T><<<dim3(2, (unsigned)batch), 512, ssm, st>>>(s);
+        if (gt.ax && gt.ay) {
+            const int nmax = std::max(g.NI, g.NJ);
+            k_sweep_edges<T><<<dim3((unsigned)((nmax + kEdgeRows - 1) / kEdgeRows), 2, (unsigned)batch),
+                               32 * kEdgeRows, sizeof(T) * 2 * (size_t)nmax, st>>>(s);
+        } else {
+            k_sweep_lines<T><<<dim3(2, (unsigned)batch), 512, ssm, st>>>(s);
+        }
     }
     // 4. inverse transforms of every level (lifting + eigen-inverse applied on load)
     launch_cols(g, fcol, 3, L, batch, c.tbuf, N1, tS, c.sweep, es, st);
@@ -863,9 +1004,9 @@ int EllipticPlan<T>::init(const GridDev* g, const FftTables* t, bool helm, doubl
     const int rows_need = (int)std::min<size_t>(fft_smem_bytes<T>(frow.m, 2), 200 * 1024);
     const int cols_need = (int)std::min<size_t>(fft_smem_bytes<T>(fcol.m, 2), 200 * 1024);
     const int sweep_need = (int)sweep_smem_bytes<T>(*g, M);
-    if (cudaFuncSetAttribute(k_dst_rows<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, rows_need) != cudaSuccess ||
-        cudaFuncSetAttribute(k_dst_cols<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, cols_need) != cudaSuccess ||
-        cudaFuncSetAttribute(k_sweep_lines<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, sweep_need) != cudaSuccess)
+    if (raise_smem_limit((const void*)k_dst_rows<T>, rows_need) ||
+        raise_smem_limit((const void*)k_dst_cols<T>, cols_need) ||
+        raise_smem_limit((const void*)k_sweep_lines<T>, sweep_need))
         return IBG_ERR_CUDA;
     return IBG_OK;
 }

@@ -355,7 +355,7 @@ __global__ void k_add_time(double* t, double dt) {
 int chol_factor(int m, const double* Mcol, double* Lr, double* Lc, double* diag, int* d_status, cudaStream_t st) {
     const size_t sm = sizeof(double) * (m + 32);
     if (sm > 200 * 1024) return IBG_ERR_UNSUPPORTED;
-    cudaFuncSetAttribute(k_chol_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (raise_smem_limit((const void*)k_chol_factor, (int)sm)) return IBG_ERR_CUDA;
     cudaMemsetAsync(d_status, 0, sizeof(int), st);
     cudaMemsetAsync(Lr, 0, sizeof(double) * m * m, st);
     cudaMemsetAsync(Lc, 0, sizeof(double) * m * m, st);
@@ -372,8 +372,7 @@ void chol_solve(int m, const double* Lr, const double* Lc, const double* diag, c
 int chol_solve_prepare(int m) {
     const size_t sm = sizeof(double) * (m + 32 * 33);
     if (sm > 200 * 1024) return IBG_ERR_UNSUPPORTED;
-    if (cudaFuncSetAttribute(k_chol_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess ||
-        cudaFuncSetAttribute(k_chol_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+    if (raise_smem_limit((const void*)k_chol_solve, (int)sm) || raise_smem_limit((const void*)k_chol_inverse, (int)sm))
         return IBG_ERR_CUDA;
     return IBG_OK;
 }

@@ -15,6 +15,12 @@
 
 namespace ibg {
 
+// Raise a kernel's dynamic shared-memory limit to at least `bytes` on the
+// current device.  The limit is a property of the function, shared by every
+// context in the process, so it only ever grows (a context with a smaller grid
+// must not lower the limit another context's launches rely on).
+int raise_smem_limit(const void* func, int bytes);
+
 // ---------------------------------------------------------------------------
 // grid description passed by value to kernels
 // ---------------------------------------------------------------------------

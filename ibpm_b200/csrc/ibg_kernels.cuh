@@ -69,6 +69,9 @@ struct GridTables {
     const T* cosx = nullptr;   // cos(pi i / nx), i < nx
     const T* cosy = nullptr;
     SineTab<T> s{};
+    // edge maps of the coarse-to-fine sweep (row-major NI x NI and NJ x NJ; nullptr: FFT path)
+    const T* ax = nullptr;
+    const T* ay = nullptr;
 };
 
 template <typename T>
@@ -91,6 +94,8 @@ struct SweepArgs {
     T* vrow;                       // work: row sums V0, V1 [NI] then column sums W0, W1 [NJ]
     size_t wstride;
     T norm;
+    const T* ax;                   // edge maps (k_sweep_edges)
+    const T* ay;
 };
 
 struct FftTables {
@@ -112,9 +117,14 @@ size_t sweep_doubles(int nx, int ny, int L);
 struct CosTables {
     double* d64 = nullptr;  // owned device block (nullptr when attached to external memory)
     float* d32 = nullptr;
+    double* map64 = nullptr;  // owned edge maps: A_x (NI x NI) then A_y (NJ x NJ)
+    float* map32 = nullptr;
     GridTables<double> t64;
     GridTables<float> t32;
     int init(int nx, int ny, int nxe, int nye);
+    // the sweep's linear map from boundary-line sums to the finer level's boundary
+    // DSTs, one matrix per direction, built with the FFT tables (optional)
+    int build_edge_maps(int nx, int ny, int nxe, int nye, const FftTables& ft);
     void attach(int nx, int ny, double* p64, float* p32);
     void release();
 };

@@ -297,3 +297,30 @@ def test_host_driven_cg_loop_matches_reference():
     s.advance_resident(n)
     assert rel_l2(s.force_history(n), d["forces"][:, 2:4]) < FP64_TOL
     s.close()
+
+
+def test_contexts_of_different_sizes_coexist():
+    """Kernel shared-memory limits are per process: a context created after
+    another with a smaller grid must not break the larger one's launches."""
+    import ibpm_b200 as ib
+    from ibpm_b200 import configs
+
+    def make(n, L):
+        grid = ib.Grid(n, n, L, 4.0, -2.0, -2.0)
+        geo = ib.geometry.parse(configs.cylinder_geom(48, r=0.4))
+        s = ib.NonlinearIBSolver(grid, ib.NavierStokesModel(grid, geo, 100.0), 0.005, "rk3")
+        s.init()
+        s.set_state(ib.State(grid, geo.num_points), with_q=False)
+        return s
+
+    alone = make(384, 2)
+    alone.advance_resident(3)
+    fa = alone.force_history(3)
+    alone.close()
+    big = make(384, 2)
+    small = make(64, 1)
+    big.advance_resident(3)
+    small.advance_resident(3)
+    assert rel_l2(big.force_history(3), fa) < 1e-13
+    big.close()
+    small.close()
