@@ -487,6 +487,11 @@ def main():
     e2e = {"value": ws * Ke * per_step_units / e2e_s, "unit": UNIT, "h2d_bytes_per_step": bi,
            "d2h_bytes_per_step": bo}
     roof = kernel_roofline(*run.roof_solver(), dtype="float" if form == "fp32" else "double")
+    if wlname == "c2" and form == "fp64":
+        # dram__bytes_read.sum + dram__bytes_write.sum of one k_dst_cols<double> launch on this workload
+        # (ncu --set full, cold launch; profiles/dst_cols_c2_fp64.md)
+        roof["traffic"] = 3.22e6
+        roof["traffic_note"] = "ncu dram read + write of one cold launch; writes stay in L2"
     extra = dict(run.extra)
     run.close()
 
