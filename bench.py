@@ -16,8 +16,9 @@ Workloads (seeded synthetic inputs; no dataset is involved):
   trained first; training time reported, not timed).
 * c4 ensemble of 64 independent ellipse runs (n in {128..512}, 1-3 domains,
   seeded b, orientation, Re; dt = 0.5 dx): forms ensemble (all members' steps
-  as branches of one CUDA graph, default) and serial (each member's captured
-  step launched after the other on one stream).
+  as branches of one CUDA graph, default), ensemble_fp32 (the same with FP32
+  bulk members) and serial (each member's captured FP64 step launched after
+  the other on one stream).
 
 One process per GPU (torchrun for N > 1).  One simulation does not shard
 (its multi-domain solve is global per level and levels are serially
@@ -60,7 +61,7 @@ METRICS = {
     "c3": "timesteps/s (500x250 x3-domain pitching/plunging plate, RK3, CG tol 1e-10)",
     "c4": "member-timesteps/s (ensemble of 64 ellipse runs, n 128-512, 1-3 domains, RK3)",
 }
-FORMS = {"c2": ("fp64", "fp32"), "c3": ("cholesky", "learned", "cg"), "c4": ("ensemble", "serial")}
+FORMS = {"c2": ("fp64", "fp32"), "c3": ("cholesky", "learned", "cg"), "c4": ("ensemble", "ensemble_fp32", "serial")}
 PLAIN = {"c2": "fp64", "c3": "cg", "c4": "serial"}
 
 
@@ -336,8 +337,9 @@ class Ens:
         from ibpm_b200 import configs
         import torch
         self.members = []
+        prec = "fp32" if form == "ensemble_fp32" else "fp64"
         for wl in configs.ensemble_members(count=count):
-            grid, model, s, x = ib.from_workload(wl, stream=stream.cuda_stream, device=device)
+            grid, model, s, x = ib.from_workload(wl, stream=stream.cuda_stream, device=device, precision=prec)
             s.init()
             s.set_state(x, with_q=False)
             self.members.append((wl, grid, s, x))
@@ -345,7 +347,7 @@ class Ens:
         self.ens = None
         self.stream = stream
         self.member_stream = stream
-        if form == "ensemble":
+        if form.startswith("ensemble"):
             self.ens = ib.Ensemble([m[2] for m in self.members])
             self.stream = torch.cuda.ExternalStream(self.ens.stream(), device=torch.device("cuda", device))
         self.extra = {"members": len(self.members),
@@ -493,6 +495,8 @@ def main():
         roof["traffic"] = 3.22e6
         roof["traffic_note"] = "ncu dram read + write of one cold launch; writes stay in L2"
     extra = dict(run.extra)
+    import ibpm_b200 as ib
+    extra["autotuned_dst_shapes"] = ib.autotune_log()
     run.close()
 
     plain = None
@@ -515,7 +519,7 @@ def main():
 
     if rank == 0:
         wl = getattr(run, "wl", None)
-        dtype = {"fp32": "f32+f64"}.get(form, "f64")
+        dtype = {"fp32": "f32+f64", "ensemble_fp32": "f32+f64"}.get(form, "f64")
         out = {"metric": METRICS[wlname], "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
                "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                "dtype": dtype, "data": "synthetic (seeded initial conditions and generated geometry)",

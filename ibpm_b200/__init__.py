@@ -324,6 +324,16 @@ class NonlinearIBSolver:
         return w, f
 
 
+def autotune_log():
+    """Launch shapes the autotuner chose in this process: one dict per
+    (precision, pass, FFT length, lines, levels)."""
+    n = lib().ibg_autotune_log(None, 0)
+    buf = np.zeros(8 * max(n, 1), np.int32)
+    n = lib().ibg_autotune_log(buf.ctypes.data_as(ctypes.c_void_p), n)
+    keys = ("bytes", "pass", "fft_length", "lines", "levels", "pairs_per_cta", "threads", "twiddles_in_smem")
+    return [dict(zip(keys, (int(v) for v in buf[8 * k:8 * k + 8]))) for k in range(n)]
+
+
 def from_workload(wl, precision: str = "fp64", stream=None, device: int = -1, precond: str = "none",
                   pc_refresh: int = 10, cg_graph: bool = True, pc_fallback_iter: int = 0):
     """Grid, model, solver and initial State for an ibpm_b200.configs.Workload."""

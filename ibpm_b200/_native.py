@@ -63,6 +63,7 @@ SIGNATURES = {
     "ibg_stream": (_VP, [_VP]),
     "ibg_last_launch_count": (ctypes.c_longlong, [_VP]),
     "ibg_run_kernel": (ctypes.c_longlong, [_VP, _I, _I]),
+    "ibg_autotune_log": (_I, [_VP, _I]),
     "ibg_lpc_num_params": (ctypes.c_size_t, []),
     "ibg_lpc_generate": (_I, [_VP, _I, _D, _D, _VP, _VP]),
     "ibg_lpc_train": (_I, [_VP, _I, _VP, _VP, _I, _I, ctypes.c_float, ctypes.c_uint, _VP]),

@@ -208,6 +208,9 @@ struct ibg_context {
                 alloc(&B.C, F) || alloc(&B.Bf, S) || alloc(&B.qtmp, F);
         for (int k = 0; k < nring && !s; ++k) s = alloc(&B.Nbuf[k], S);
         if (s) return IBG_ERR_CUDA;
+        // time the DST passes' launch shapes for this grid once per process (before the plans read them)
+        s = tune_passes<T>(&g, &fft, cosT, call<T>(B, B.a, B.ws, (T)1), st);
+        if (s) return s;
         s = B.poisson.init(&g, &fft, false, 0.0, cosT);
         for (int k = 0; k < sch.nsub && !s; ++k) {
             const double alpha = -beta[k] / 2. * (1. / prm.Re);  // src/ProjectionSolver.cc:33
@@ -218,6 +221,21 @@ struct ibg_context {
         return IBG_OK;
     }
 
+    // rule-based DST shapes and per-step line FFTs in every plan (ensemble members: their
+    // kernels run side by side, where fewer, smaller blocks give more throughput)
+    void use_rule_shapes() {
+        auto reset = [](auto& plan) {
+            plan.rows_P = plan.rows_T = plan.cols_P = plan.cols_T = plan.rows_tws = plan.cols_tws = 0;
+            plan.edge_maps = false;
+        };
+        reset(b64.poisson);
+        reset(b32.poisson);
+        for (int k = 0; k < 4; ++k) {
+            reset(b64.helm[k]);
+            reset(b32.helm[k]);
+        }
+        drop_graph();
+    }
     void drop_graph() {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
@@ -1299,6 +1317,7 @@ int ibg_ensemble_create(int n, ibg_context* const* members, ibg_ensemble** out) 
     }
     auto* e = new ibg_ensemble();
     e->members.assign(members, members + n);
+    for (ibg_context* c : e->members) c->use_rule_shapes();
     e->ev.assign(n, nullptr);
     bool ok = cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) == cudaSuccess &&
               cudaGraphCreate(&e->graph, 0) == cudaSuccess &&
@@ -1601,6 +1620,17 @@ int ibg_substep_beta(ibg_context* c, int k, double* beta) {
     if (!c || !beta || k < 0 || k >= c->sch.nsub) return IBG_ERR_ARG;
     *beta = c->beta[k];
     return IBG_OK;
+}
+
+int ibg_autotune_log(int* out, int max_rows) {
+    const std::vector<TuneResult> r = tune_log();
+    if (out)
+        for (int k = 0; k < (int)r.size() && k < max_rows; ++k) {
+            const TuneResult& t = r[k];
+            const int row[8] = {t.wbytes, t.pass, t.m, t.nlines, t.nlev, t.P, t.threads, t.tw_smem};
+            for (int q = 0; q < 8; ++q) out[8 * k + q] = row[q];
+        }
+    return (int)r.size();
 }
 
 long long ibg_run_kernel(ibg_context* c, int which, int reps) {

@@ -23,6 +23,7 @@
 // odd real sequence is purely imaginary, so DST(a)_k = -Im Z_{k+1} and
 // DST(b)_k = Re Z_{k+1}.  The complex FFT is a shared-memory Stockham
 // autosort FFT with mixed radices; twiddles are tabulated on the host.
+#include <array>
 #include <map>
 #include <mutex>
 
@@ -66,7 +67,7 @@ __device__ __forceinline__ void bfly(const C* __restrict__ sp, C* __restrict__ d
 #pragma unroll
     for (int q = 0; q < R; ++q) {
         C x = sp[j + q * mr];
-        v[q] = q == 0 ? x : cmul(x, __ldg(&tw[jm * q * tstep]));
+        v[q] = q == 0 ? x : cmul(x, tw[jm * q * tstep]);
     }
     C o[R];
     if (R == 2) {
@@ -112,7 +113,7 @@ __device__ __forceinline__ void bfly(const C* __restrict__ sp, C* __restrict__ d
         for (int k = 0; k < R; ++k) {
             C acc = v[0];
 #pragma unroll
-            for (int q = 1; q < R; ++q) acc = cadd(acc, cmul(v[q], __ldg(&tw[((k * q) % R) * rstep])));
+            for (int q = 1; q < R; ++q) acc = cadd(acc, cmul(v[q], tw[((k * q) % R) * rstep]));
             o[k] = acc;
         }
     }
@@ -131,8 +132,8 @@ __device__ void bfly_generic(const C* __restrict__ sp, C* __restrict__ dp, const
     for (int k = 0; k < R; ++k) {
         C acc = sp[j];
         for (int q = 1; q < R; ++q) {
-            C x = cmul(sp[j + q * mr], __ldg(&tw[jm * q * tstep]));
-            acc = cadd(acc, cmul(x, __ldg(&tw[((k * q) % R) * rstep])));
+            C x = cmul(sp[j + q * mr], tw[jm * q * tstep]);
+            acc = cadd(acc, cmul(x, tw[((k * q) % R) * rstep]));
         }
         dp[idxd + k * ns] = acc;
     }
@@ -184,7 +185,13 @@ __global__ void k_dst_rows(RowPassArgs<T> a) {
     const int P = a.pairs_per_block;
     C* s0 = reinterpret_cast<C*>(smem_raw);
     C* s1 = s0 + P * m;
+    // twiddles from a shared-memory copy (a.tw_smem) or straight from the global table
     const C* tw = reinterpret_cast<const C*>(d.tw);
+    if (a.tw_smem) {
+        C* tws = s1 + P * m;
+        for (int k = threadIdx.x; k < m; k += blockDim.x) tws[k] = tw[k];
+        tw = tws;
+    }
     const GridDev& g = a.g;
     const int n = g.NJ;
     const int b = blockIdx.y / a.nlev, l = blockIdx.y % a.nlev;
@@ -280,7 +287,13 @@ __global__ void k_dst_cols(ColPassArgs<T> a) {
     const int P = a.pairs_per_block;
     C* s0 = reinterpret_cast<C*>(smem_raw);
     C* s1 = s0 + P * m;
+    // twiddles from a shared-memory copy (a.tw_smem) or straight from the global table
     const C* tw = reinterpret_cast<const C*>(d.tw);
+    if (a.tw_smem) {
+        C* tws = s1 + P * m;
+        for (int k = threadIdx.x; k < m; k += blockDim.x) tws[k] = tw[k];
+        tw = tws;
+    }
     const GridDev& g = a.g;
     const int n = g.NI;
     const int NJ = g.NJ;
@@ -745,36 +758,50 @@ void CosTables::release() {
     cudaFree(d32);
     d64 = nullptr;
     d32 = nullptr;
-    if (map64) cudaFree(map64);
-    if (map32) cudaFree(map32);
-    map64 = nullptr;
-    map32 = nullptr;
+    maps.reset();
     t64.ax = t64.ay = nullptr;
     t32.ax = t32.ay = nullptr;
 }
 
+EdgeMaps::~EdgeMaps() {
+    if (m64) cudaFree(m64);
+    if (m32) cudaFree(m32);
+}
+
+namespace {
+std::mutex g_maps_mu;
+std::map<std::array<int, 3>, std::weak_ptr<EdgeMaps>> g_maps;  // (device, nx, ny) -> maps in use
+}  // namespace
+
 int CosTables::build_edge_maps(int nx, int ny, int nxe, int nye, const FftTables& ft) {
     const int NI = nx - 1, NJ = ny - 1;
     const size_t nmap = (size_t)NI * NI + (size_t)NJ * NJ;
-    if (cudaMalloc(&map64, sizeof(double) * nmap) != cudaSuccess ||
-        cudaMalloc(&map32, sizeof(float) * nmap) != cudaSuccess)
-        return IBG_ERR_CUDA;
-    double* ax = map64;
-    double* ay = map64 + (size_t)NI * NI;
-    auto smem = [](const FftDesc& d, int n) {
-        return sizeof(typename Cplx<double>::type) * 2 * (size_t)d.m + sizeof(double) * 6 * (size_t)n;
-    };
-    const size_t sx = smem(ft.col64, NI), sy = smem(ft.row64, NJ);
-    if (std::max(sx, sy) > 200 * 1024 || raise_smem_limit((const void*)k_edge_map, (int)std::max(sx, sy)))
-        return IBG_ERR_UNSUPPORTED;
-    k_edge_map<<<(NI + 1) / 2, 512, sx>>>(ft.col64, NI, nxe, ax);
-    k_edge_map<<<(NJ + 1) / 2, 512, sy>>>(ft.row64, NJ, nye, ay);
-    k_map_to_f32<<<(unsigned)((nmap + 255) / 256), 256>>>((long)nmap, map64, map32);
-    if (cudaDeviceSynchronize() != cudaSuccess) return IBG_ERR_CUDA;
-    t64.ax = ax;
-    t64.ay = ay;
-    t32.ax = map32;
-    t32.ay = map32 + (size_t)NI * NI;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return IBG_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(g_maps_mu);
+    std::shared_ptr<EdgeMaps> e = g_maps[{dev, nx, ny}].lock();
+    if (!e) {
+        e = std::make_shared<EdgeMaps>();
+        if (cudaMalloc(&e->m64, sizeof(double) * nmap) != cudaSuccess ||
+            cudaMalloc(&e->m32, sizeof(float) * nmap) != cudaSuccess)
+            return IBG_ERR_CUDA;
+        auto smem = [](const FftDesc& d, int n) {
+            return sizeof(typename Cplx<double>::type) * 2 * (size_t)d.m + sizeof(double) * 6 * (size_t)n;
+        };
+        const size_t sx = smem(ft.col64, NI), sy = smem(ft.row64, NJ);
+        if (std::max(sx, sy) > 200 * 1024 || raise_smem_limit((const void*)k_edge_map, (int)std::max(sx, sy)))
+            return IBG_ERR_UNSUPPORTED;
+        k_edge_map<<<(NI + 1) / 2, 512, sx>>>(ft.col64, NI, nxe, e->m64);
+        k_edge_map<<<(NJ + 1) / 2, 512, sy>>>(ft.row64, NJ, nye, e->m64 + (size_t)NI * NI);
+        k_map_to_f32<<<(unsigned)((nmap + 255) / 256), 256>>>((long)nmap, e->m64, e->m32);
+        if (cudaDeviceSynchronize() != cudaSuccess) return IBG_ERR_CUDA;
+        g_maps[{dev, nx, ny}] = e;
+    }
+    maps = e;
+    t64.ax = e->m64;
+    t64.ay = e->m64 + (size_t)NI * NI;
+    t32.ax = e->m32;
+    t32.ay = e->m32 + (size_t)NI * NI;
     return IBG_OK;
 }
 
@@ -788,8 +815,9 @@ static int pairs_per_block(int m, int nlines, int nlev, int batch) {
 }
 
 template <typename T>
-size_t fft_smem_bytes(int m, int P) {
-    return sizeof(typename Cplx<T>::type) * (size_t)m * (2 * P);
+size_t fft_smem_bytes(int m, int P, int tw_smem = 0) {
+    // P ping-pong pairs of length-m buffers, plus a copy of the twiddles when they live in shared memory
+    return sizeof(typename Cplx<T>::type) * (size_t)m * (2 * P + (tw_smem ? 1 : 0));
 }
 
 static size_t sweep_work(int nx, int ny) {
@@ -826,11 +854,17 @@ void EllipticPlan<T>::launch_rows(const GridDev& g, const FftDesc& frow, int nle
     A.out_bstride = out_bs;
     A.in_scale = scale;
     A.norm = norm;
-    const int P = pairs_per_block<T>(frow.m, g.NI, nlev, batch);
+    int P = pairs_per_block<T>(frow.m, g.NI, nlev, batch), nt = threads, tws = 0;
+    if (batch == 1 && rows_P > 0) {
+        P = rows_P;
+        nt = rows_T;
+        tws = rows_tws;
+    }
     A.pairs_per_block = P;
+    A.tw_smem = tws;
     const int npairs = (g.NI + 1) / 2;
-    k_dst_rows<T><<<dim3((unsigned)((npairs + P - 1) / P), (unsigned)(nlev * batch)), threads,
-                    fft_smem_bytes<T>(frow.m, P), st>>>(A);
+    k_dst_rows<T><<<dim3((unsigned)((npairs + P - 1) / P), (unsigned)(nlev * batch)), nt,
+                    fft_smem_bytes<T>(frow.m, P, tws), st>>>(A);
 }
 
 template <typename T>
@@ -859,10 +893,17 @@ void EllipticPlan<T>::launch_cols(const GridDev& g, const FftDesc& fcol, int mod
     B.edges = edges;
     B.estride = estride;
     B.elstride = 2 * (size_t)g.NI + 2 * (size_t)g.NJ;
-    const int P = pairs_per_block<T>(fcol.m, g.NJ, nlev, batch);
+    int P = pairs_per_block<T>(fcol.m, g.NJ, nlev, batch), nt = threads, tws = 0;
+    if (batch == 1 && cols_P > 0) {
+        P = cols_P;
+        nt = cols_T;
+        tws = cols_tws;
+    }
     B.pairs_per_block = P;
+    B.tw_smem = tws;
     const int ncolblk = (g.NJ + 2 * P - 1) / (2 * P);
-    k_dst_cols<T><<<dim3((unsigned)ncolblk, (unsigned)(nlev * batch)), threads, fft_smem_bytes<T>(fcol.m, P), st>>>(B);
+    k_dst_cols<T><<<dim3((unsigned)ncolblk, (unsigned)(nlev * batch)), nt, fft_smem_bytes<T>(fcol.m, P, tws),
+                    st>>>(B);
 }
 
 template <typename T>
@@ -936,7 +977,7 @@ int EllipticPlan<T>::solve(const SolveCall<T>& c, cudaStream_t st) const {
         s.ay = gt.ay;
         const int nrb = (g.NI + kSweepRows - 1) / kSweepRows, ncb = (g.NJ + kSweepCols - 1) / kSweepCols;
         k_sweep_sums<T><<<dim3((unsigned)(nrb + ncb), (unsigned)batch), 256, 0, st>>>(s);
-        if (gt.ax && gt.ay) {
+        if (gt.ax && gt.ay && edge_maps) {
             const int nmax = std::max(g.NI, g.NJ);
             k_sweep_edges<T><<<dim3((unsigned)((nmax + kEdgeRows - 1) / kEdgeRows), 2, (unsigned)batch),
                                32 * kEdgeRows, sizeof(T) * 2 * (size_t)nmax, st>>>(s);
@@ -987,6 +1028,119 @@ void EllipticPlan<T>::run_pass(int which, const T* in, T* tbuf, cudaStream_t st)
     }
 }
 
+// ---------------------------------------------------------------------------
+// autotuner of the DST passes' launch shape: line pairs per CTA (P), threads
+// per CTA and whether the twiddles are first copied to shared memory, chosen by
+// timing whole multi-domain solves on the device for each (precision, pass,
+// FFT length, line count, level count) the first time a context with that
+// shape is made; the choice is kept for the process.  Every shape computes the
+// same butterflies in the same order, so the results do not depend on the
+// choice.  Ensemble members use the rule-based shapes instead (their kernels run
+// side by side, where the single-solve optimum does not hold).
+// ---------------------------------------------------------------------------
+namespace {
+std::mutex g_tune_mu;
+std::map<std::array<int, 5>, std::array<int, 3>> g_tuned;
+}  // namespace
+
+void tuned_config(int wbytes, int pass, int m, int nlines, int nlev, int& P, int& nt, int& tws) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tuned.find({wbytes, pass, m, nlines, nlev});
+    if (it == g_tuned.end()) {
+        P = nt = tws = 0;
+    } else {
+        P = it->second[0];
+        nt = it->second[1];
+        tws = it->second[2];
+    }
+}
+
+std::vector<TuneResult> tune_log() {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    std::vector<TuneResult> out;
+    for (auto& kv : g_tuned)
+        out.push_back({kv.first[0], kv.first[1], kv.first[2], kv.first[3], kv.first[4], kv.second[0],
+                       kv.second[1], kv.second[2]});
+    return out;
+}
+
+template <typename T>
+int tune_passes(const GridDev* g, const FftTables* t, const CosTables& ct, const SolveCall<T>& call, cudaStream_t st) {
+    const FftDesc& frow = sizeof(T) == 8 ? t->row64 : t->row32;
+    const FftDesc& fcol = sizeof(T) == 8 ? t->col64 : t->col32;
+    int have_r, have_c, tmp, tmp2;
+    tuned_config(sizeof(T), 0, frow.m, g->NI, g->L, have_r, tmp, tmp2);
+    tuned_config(sizeof(T), 1, fcol.m, g->NJ, g->L, have_c, tmp, tmp2);
+    if (have_r > 0 && have_c > 0) return IBG_OK;
+    EllipticPlan<T> p;
+    int s = p.init(g, t, false, 0.0, ct);
+    if (s) return s;
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return IBG_ERR_CUDA;
+    // objective: the time of the whole multi-domain solve, back to back as in a time step;
+    // the best of 3 trials of 8 solves after 2 warm-up solves
+    auto time_solve = [&](float& ms) -> int {
+        for (int w = 0; w < 2; ++w) p.solve(call, st);
+        ms = 1e30f;
+        for (int trial = 0; trial < 3; ++trial) {
+            cudaEventRecord(e0, st);
+            for (int r = 0; r < 8; ++r) p.solve(call, st);
+            cudaEventRecord(e1, st);
+            if (cudaEventSynchronize(e1) != cudaSuccess) return IBG_ERR_CUDA;
+            float tt = 0.f;
+            cudaEventElapsedTime(&tt, e0, e1);
+            ms = std::min(ms, tt);
+        }
+        return IBG_OK;
+    };
+    // coordinate descent: the row pass with the column pass at its rule, then the column pass
+    const int Ps[3] = {1, 2, 4}, Ts[3] = {128, 256, 512};
+    for (int pass = 0; pass < 2 && !s; ++pass) {
+        const int m = pass == 0 ? frow.m : fcol.m;
+        const int nlines = pass == 0 ? g->NI : g->NJ;
+        const int ruleP = pairs_per_block<T>(m, nlines, g->L, 1);
+        int bP = ruleP, bT = p.threads, bW = 0;
+        auto set = [&](int P, int nt, int tws) {
+            if (pass == 0) { p.rows_P = P; p.rows_T = nt; p.rows_tws = tws; }
+            else { p.cols_P = P; p.cols_T = nt; p.cols_tws = tws; }
+        };
+        // the rule's own shape first, so the choice is never slower than the rule on this measure
+        set(bP, bT, bW);
+        float best = 1e30f;
+        if ((s = time_solve(best))) break;
+        for (int tws = 0; tws < 2 && !s; ++tws)
+            for (int P : Ps)
+                for (int nt : Ts) {
+                    if (P == ruleP && nt == p.threads && tws == 0) continue;
+                    const size_t smem = fft_smem_bytes<T>(m, P, tws);
+                    if (smem > 200 * 1024) continue;
+                    const void* fn = pass == 0 ? (const void*)k_dst_rows<T> : (const void*)k_dst_cols<T>;
+                    if (raise_smem_limit(fn, (int)smem)) continue;
+                    set(P, nt, tws);
+                    float ms = 0.f;
+                    if ((s = time_solve(ms))) break;
+                    if (ms < best * 0.99f) {  // a change must win by more than the timing noise
+                        best = ms;
+                        bP = P;
+                        bT = nt;
+                        bW = tws;
+                    }
+                }
+        set(bP, bT, bW);
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tuned[{(int)sizeof(T), pass, m, nlines, g->L}] = {bP, bT, bW};
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (s) return s;
+    return cudaPeekAtLastError() == cudaSuccess ? IBG_OK : IBG_ERR_CUDA;
+}
+
+template int tune_passes<double>(const GridDev*, const FftTables*, const CosTables&, const SolveCall<double>&,
+                                 cudaStream_t);
+template int tune_passes<float>(const GridDev*, const FftTables*, const CosTables&, const SolveCall<float>&,
+                                cudaStream_t);
+
 template <typename T>
 int EllipticPlan<T>::init(const GridDev* g, const FftTables* t, bool helm, double a, const CosTables& ct) {
     grid = g;
@@ -1001,8 +1155,10 @@ int EllipticPlan<T>::init(const GridDev* g, const FftTables* t, bool helm, doubl
     const int M = std::max(frow.m, fcol.m);
     if (fft_smem_bytes<T>(M, 1) > 200 * 1024 || sweep_smem_bytes<T>(*g, M) > 200 * 1024) return IBG_ERR_UNSUPPORTED;
     // dynamic shared memory each kernel may need (static shared memory comes on top)
-    const int rows_need = (int)std::min<size_t>(fft_smem_bytes<T>(frow.m, 2), 200 * 1024);
-    const int cols_need = (int)std::min<size_t>(fft_smem_bytes<T>(fcol.m, 2), 200 * 1024);
+    tuned_config(sizeof(T), 0, frow.m, g->NI, g->L, rows_P, rows_T, rows_tws);
+    tuned_config(sizeof(T), 1, fcol.m, g->NJ, g->L, cols_P, cols_T, cols_tws);
+    const int rows_need = (int)std::min<size_t>(fft_smem_bytes<T>(frow.m, std::max(2, rows_P), 1), 200 * 1024);
+    const int cols_need = (int)std::min<size_t>(fft_smem_bytes<T>(fcol.m, std::max(2, cols_P), 1), 200 * 1024);
     const int sweep_need = (int)sweep_smem_bytes<T>(*g, M);
     if (raise_smem_limit((const void*)k_dst_rows<T>, rows_need) ||
         raise_smem_limit((const void*)k_dst_cols<T>, cols_need) ||

@@ -2,6 +2,7 @@
 // multi-domain elliptic solves.
 #pragma once
 #include <algorithm>
+#include <memory>
 #include <vector>
 
 #include "ibg_internal.cuh"
@@ -17,6 +18,7 @@ struct RowPassArgs {
     GridDev g;
     FftDesc fft;
     int pairs_per_block;
+    int tw_smem;                   // 1: twiddles copied to shared memory first
     int nlev;                      // levels in this launch: blockIdx.y = batch * nlev + level
     const T* in[kMaxLevels];       // per-level input (batch item 0)
     const T* alt[kMaxLevels];      // per-level input inside the overlap interior (nullptr: none)
@@ -47,6 +49,7 @@ struct ColPassArgs {
     GridDev g;
     FftDesc fft;
     int pairs_per_block;
+    int tw_smem;                   // 1: twiddles copied to shared memory first
     int mode;                      // 0, 2: one DST along i; 1: DST, eigen-inverse, DST (one level);
                                    // 3: boundary lifting + eigen-inverse on load, one DST
     int nlev;
@@ -114,11 +117,18 @@ void fill_grid_tables(int nx, int ny, int nxe, int nye, std::vector<double>& h);
 // scratch of the coarse-to-fine sweep per batch item (elements of T)
 size_t sweep_doubles(int nx, int ny, int L);
 
+// the sweep's edge maps A_x (NI x NI) then A_y (NJ x NJ) in FP64 and FP32, one
+// device copy per (device, nx, ny) in the process
+struct EdgeMaps {
+    double* m64 = nullptr;
+    float* m32 = nullptr;
+    ~EdgeMaps();
+};
+
 struct CosTables {
     double* d64 = nullptr;  // owned device block (nullptr when attached to external memory)
     float* d32 = nullptr;
-    double* map64 = nullptr;  // owned edge maps: A_x (NI x NI) then A_y (NJ x NJ)
-    float* map32 = nullptr;
+    std::shared_ptr<struct EdgeMaps> maps;  // edge maps, shared by every context with the same grid size
     GridTables<double> t64;
     GridTables<float> t32;
     int init(int nx, int ny, int nxe, int nye);
@@ -156,6 +166,9 @@ struct EllipticPlan {
     int helmholtz = 0;
     double alpha = 0.0;
     int threads = 128;
+    // tuned launch shape of the row and column passes for batch 1 (0: rule-based)
+    int rows_P = 0, rows_T = 0, cols_P = 0, cols_T = 0, rows_tws = 0, cols_tws = 0;
+    bool edge_maps = true;  // the sweep applies the precomputed edge maps (else the per-step line FFTs)
     int init(const GridDev* g, const FftTables* t, bool helm, double a, const CosTables& ct);
     int solve(const SolveCall<T>& c, cudaStream_t st) const;
     int launches() const;
@@ -168,6 +181,16 @@ struct EllipticPlan {
     void launch_cols(const GridDev& g, const FftDesc& fcol, int mode, int nlev, int batch, T* buf, size_t lstride,
                      size_t bstride, const T* edges, size_t estride, cudaStream_t st) const;
 };
+
+// autotuner of the row/column passes (elliptic.cu): time the launch shapes once per
+// (precision, pass, FFT length, line count, level count) in the process
+template <typename T>
+int tune_passes(const GridDev* g, const FftTables* t, const CosTables& ct, const SolveCall<T>& call, cudaStream_t st);
+void tuned_config(int wbytes, int pass, int m, int nlines, int nlev, int& P, int& nt, int& tws);
+struct TuneResult {
+    int wbytes, pass, m, nlines, nlev, P, threads, tw_smem;
+};
+std::vector<TuneResult> tune_log();
 
 template <>
 inline const GridTables<double>& EllipticPlan<double>::tabs() const { return cos->t64; }

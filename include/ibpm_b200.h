@@ -159,6 +159,15 @@ IBG_API void* ibg_ensemble_stream(const ibg_ensemble* ens);
 IBG_API long long ibg_ensemble_launches_per_step(const ibg_ensemble* ens);
 IBG_API const char* ibg_ensemble_last_error(const ibg_ensemble* ens);
 
+/* --- launch-shape autotuner (no reference counterpart) -----------------------
+ * The DST row and column passes time their launch shapes (line pairs per CTA,
+ * threads per CTA, twiddles in shared memory or not) on whole solves the first
+ * time a grid shape is created in the process; ensemble members use the rules.
+ * ibg_autotune_log writes up to max_rows rows of 8 ints {bytes per word,
+ * pass (0 rows, 1 columns), FFT length, lines, levels, pairs per CTA, threads,
+ * twiddles in shared memory} and returns the number of tuned shapes. */
+IBG_API int ibg_autotune_log(int* out, int max_rows);
+
 /* --- learned preconditioner (no reference counterpart) -----------------------
  * For moving bodies the reference runs plain CG on M f = r every sub-step
  * (src/ConjugateGradientSolver.cc:35-65).  With IBG_PRECOND_LEARNED a network

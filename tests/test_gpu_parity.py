@@ -324,3 +324,19 @@ def test_contexts_of_different_sizes_coexist():
     assert rel_l2(big.force_history(3), fa) < 1e-13
     big.close()
     small.close()
+
+
+def test_autotuner_records_valid_shapes():
+    """Creating a context times the DST passes' launch shapes once per grid shape."""
+    import ibpm_b200 as ib
+    from ibpm_b200 import configs
+    grid = ib.Grid(96, 64, 2, 4.0, -2.0, -2.0)
+    geo = ib.geometry.parse(configs.cylinder_geom(40, r=0.4))
+    s = ib.NonlinearIBSolver(grid, ib.NavierStokesModel(grid, geo, 100.0), 0.01, "rk3")
+    log = ib.autotune_log()
+    mine = [r for r in log if r["levels"] == 2 and r["lines"] in (95, 63) and r["bytes"] == 8]
+    assert {r["pass"] for r in mine} == {0, 1}
+    for r in mine:
+        assert r["pairs_per_cta"] in (1, 2, 4) and r["threads"] in (128, 256, 512)
+        assert r["twiddles_in_smem"] in (0, 1)
+    s.close()
