@@ -439,12 +439,10 @@ def main():
         stream = torch.cuda.Stream(device=dev)
         return Ens(f, stream, local) if wlname == "c4" else Single(wlname, f, stream, local)
 
+    from ibpm_b200.replicas import job_throughput, max_over_ranks
+
     def maxrank(v):
-        if ws > 1:
-            t = torch.tensor([v], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            return float(t.item())
-        return v
+        return max_over_ranks(v, device=dev)
 
     def sync():
         torch.cuda.synchronize()
@@ -467,7 +465,7 @@ def main():
     clk = clocks.stop()
     ms = maxrank(ms)
     per_step_units = len(run.members) if wlname == "c4" else 1
-    value = ws * K * per_step_units / (ms / 1000.0)
+    value = job_throughput(ws, K, per_step_units, ms)
     forces = run.forces(W + K)
     cg = None
     if it0 is not None:
@@ -486,7 +484,7 @@ def main():
     Ke = min(K, 20 if wlname != "c2" else 50)
     e2e_s, bi, bo = run.e2e(Ke, sync)
     e2e_s = maxrank(e2e_s)
-    e2e = {"value": ws * Ke * per_step_units / e2e_s, "unit": UNIT, "h2d_bytes_per_step": bi,
+    e2e = {"value": job_throughput(ws, Ke, per_step_units, 1000.0 * e2e_s), "unit": UNIT, "h2d_bytes_per_step": bi,
            "d2h_bytes_per_step": bo}
     roof = kernel_roofline(*run.roof_solver(), dtype="float" if form == "fp32" else "double")
     if wlname == "c2" and form == "fp64":
@@ -509,7 +507,7 @@ def main():
         pms, _ = time_steps(K, p.stream, p.step, flush)
         pms = maxrank(pms)
         pforces = p.forces(W + K)
-        plain = {"form": PLAIN[wlname], "value": ws * K * per_step_units / (pms / 1000.0), "ms_per_step": pms / K,
+        plain = {"form": PLAIN[wlname], "value": job_throughput(ws, K, per_step_units, pms), "ms_per_step": pms / K,
                  "force_rel_l2_vs_plain": rel_l2(forces, pforces)}
         if pit0 is not None:
             pit1 = p.iterations()
