@@ -186,6 +186,20 @@ class NonlinearIBSolver:
         check(lib().ibg_get_state(self._h, _ptr(om), _ptr(q), _ptr(f), ctypes.byref(ts), ctypes.byref(t)), self._h)
         x.omega, x.q, x.f, x.timestep, x.time = om, q, f, ts.value, t.value
 
+    # -- restart files (State::save / State::load, src/State.cc:65-223) -------
+    def save_restart(self, filename: str) -> bool:
+        return check(lib().ibg_save_restart(self._h, filename.encode()), self._h) == 1
+
+    def load_restart(self, filename: str) -> bool:
+        return check(lib().ibg_load_restart(self._h, filename.encode()), self._h) == 1
+
+    def snapshot(self):
+        """Copy the current state for a later restart file without stalling the GPU."""
+        check(lib().ibg_snapshot(self._h), self._h)
+
+    def snapshot_save(self, filename: str) -> bool:
+        return check(lib().ibg_snapshot_save(self._h, filename.encode()), self._h) == 1
+
     def update_operators(self, time: float):
         check(lib().ibg_update_operators(self._h, float(time)), self._h)
 

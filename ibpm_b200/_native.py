@@ -64,6 +64,10 @@ SIGNATURES = {
     "ibg_last_launch_count": (ctypes.c_longlong, [_VP]),
     "ibg_run_kernel": (ctypes.c_longlong, [_VP, _I, _I]),
     "ibg_autotune_log": (_I, [_VP, _I]),
+    "ibg_save_restart": (_I, [_VP, ctypes.c_char_p]),
+    "ibg_load_restart": (_I, [_VP, ctypes.c_char_p]),
+    "ibg_snapshot": (_I, [_VP]),
+    "ibg_snapshot_save": (_I, [_VP, ctypes.c_char_p]),
     "ibg_lpc_num_params": (ctypes.c_size_t, []),
     "ibg_lpc_generate": (_I, [_VP, _I, _D, _D, _VP, _VP]),
     "ibg_lpc_train": (_I, [_VP, _I, _VP, _VP, _I, _I, ctypes.c_float, ctypes.c_uint, _VP]),

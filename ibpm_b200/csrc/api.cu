@@ -236,6 +236,27 @@ struct ibg_context {
         }
         drop_graph();
     }
+    // asynchronous state snapshots (restart output at logger cadence)
+    double* snap_dev = nullptr;    // device copy of omega | q | f taken in stream order
+    double* snap_host = nullptr;   // pinned host copy
+    cudaStream_t snap_st = nullptr;
+    cudaEvent_t snap_copied = nullptr, snap_done = nullptr;
+    int snap_timestep = -1;
+    double snap_time = 0.0;
+    bool snap_valid = false;
+    void release_snapshot() {
+        if (snap_done) cudaEventSynchronize(snap_done);
+        if (snap_dev) cudaFree(snap_dev);
+        if (snap_host) cudaFreeHost(snap_host);
+        if (snap_st) cudaStreamDestroy(snap_st);
+        if (snap_copied) cudaEventDestroy(snap_copied);
+        if (snap_done) cudaEventDestroy(snap_done);
+        snap_dev = snap_host = nullptr;
+        snap_st = nullptr;
+        snap_copied = snap_done = nullptr;
+        snap_valid = false;
+    }
+
     void drop_graph() {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
@@ -243,6 +264,7 @@ struct ibg_context {
         graph_def = nullptr;
     }
     void release() {
+        release_snapshot();
         drop_graph();
         b64.release();
         b32.release();
@@ -1008,6 +1030,109 @@ int ibg_load(ibg_context* c, const char* basename) {
     cudaStreamSynchronize(c->st);
     c->chol_ready = true;
     return c->cuda_check("ibg_load") ? IBG_ERR_CUDA : 1;
+}
+
+// ---------------------------------------------------------------------------
+// restart files: State::save / State::load (src/State.cc:65-223).  Layout:
+// int nx, ny, ngrid; double dx, x0, y0; int numPoints; q (ngrid x fluxes, the
+// Flux index order); omega (ngrid x (nx-1) x (ny-1), j fastest); f as
+// (fx, fy) pairs per point; int timestep; double time.  Native byte order.
+// ---------------------------------------------------------------------------
+static int write_restart(ibg_context* c, const char* filename, const double* w, const double* q, const double* f,
+                         int timestep, double time) {
+    FILE* fp = fopen(filename, "wb");
+    if (!fp) return 0;
+    const int hdr_i[3] = {c->g.nx, c->g.ny, c->g.L};
+    const double hdr_d[3] = {c->g.dx, c->g.x0, c->g.y0};
+    const int np = c->npts;
+    bool ok = fwrite(hdr_i, sizeof(int), 3, fp) == 3 && fwrite(hdr_d, sizeof(double), 3, fp) == 3 &&
+              fwrite(&np, sizeof(int), 1, fp) == 1 && fwrite(q, sizeof(double), c->F, fp) == c->F &&
+              fwrite(w, sizeof(double), c->S, fp) == c->S;
+    for (int i = 0; i < np && ok; ++i) {
+        const double xy[2] = {f[i], f[np + i]};
+        ok = fwrite(xy, sizeof(double), 2, fp) == 2;
+    }
+    ok = ok && fwrite(&timestep, sizeof(int), 1, fp) == 1 && fwrite(&time, sizeof(double), 1, fp) == 1;
+    ok = (fclose(fp) == 0) && ok;
+    return ok ? 1 : c->fail(IBG_ERR_IO, std::string("restart file ") + filename + ": write failed");
+}
+
+int ibg_save_restart(ibg_context* c, const char* filename) {
+    if (!c || !filename) return IBG_ERR_ARG;
+    std::vector<double> w(c->S), q(c->F), f(c->ncomp);
+    int ts = 0;
+    double t = 0.0;
+    int s = ibg_get_state(c, w.data(), q.data(), f.data(), &ts, &t);
+    if (s) return s;
+    return write_restart(c, filename, w.data(), q.data(), f.data(), ts, t);
+}
+
+int ibg_load_restart(ibg_context* c, const char* filename) {
+    if (!c || !filename) return IBG_ERR_ARG;
+    FILE* fp = fopen(filename, "rb");
+    if (!fp) return 0;
+    int hdr_i[3] = {0, 0, 0}, np = 0, ts = 0;
+    double hdr_d[3] = {0, 0, 0}, t = 0.0;
+    bool ok = fread(hdr_i, sizeof(int), 3, fp) == 3 && fread(hdr_d, sizeof(double), 3, fp) == 3 &&
+              fread(&np, sizeof(int), 1, fp) == 1;
+    // the reference resizes its State on a mismatch; a context's grid is fixed, so refuse instead
+    if (ok && (hdr_i[0] != c->g.nx || hdr_i[1] != c->g.ny || hdr_i[2] != c->g.L || hdr_d[0] != c->g.dx ||
+               hdr_d[1] != c->g.x0 || hdr_d[2] != c->g.y0 || np != c->npts)) {
+        fclose(fp);
+        return c->fail(IBG_ERR_ARG, std::string("restart file ") + filename +
+                                        ": grid or number of boundary points differs from the context's");
+    }
+    std::vector<double> w(c->S), q(c->F), f(c->ncomp), xy(2 * (size_t)np);
+    ok = ok && fread(q.data(), sizeof(double), c->F, fp) == c->F && fread(w.data(), sizeof(double), c->S, fp) == c->S &&
+         fread(xy.data(), sizeof(double), xy.size(), fp) == xy.size() && fread(&ts, sizeof(int), 1, fp) == 1 &&
+         fread(&t, sizeof(double), 1, fp) == 1;
+    fclose(fp);
+    if (!ok) return c->fail(IBG_ERR_IO, std::string("restart file ") + filename + ": truncated");
+    for (int i = 0; i < np; ++i) {
+        f[i] = xy[2 * (size_t)i];
+        f[np + i] = xy[2 * (size_t)i + 1];
+    }
+    int s = ibg_set_state(c, w.data(), q.data(), f.data(), ts, t);
+    return s ? s : 1;
+}
+
+int ibg_snapshot(ibg_context* c) {
+    if (!c) return IBG_ERR_ARG;
+    const size_t n = c->S + c->F + c->ncomp;
+    if (!c->snap_dev) {
+        if (cudaMalloc(&c->snap_dev, sizeof(double) * n) != cudaSuccess ||
+            cudaHostAlloc(&c->snap_host, sizeof(double) * n, cudaHostAllocDefault) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&c->snap_st, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&c->snap_copied, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&c->snap_done, cudaEventDisableTiming) != cudaSuccess) {
+            c->release_snapshot();
+            return c->fail(IBG_ERR_CUDA, "ibg_snapshot: staging set-up failed");
+        }
+    } else {
+        // the previous snapshot's host copy must finish before its device copy is overwritten
+        cudaStreamWaitEvent(c->st, c->snap_done, 0);
+    }
+    c->to64();
+    // device copy in stream order (the next steps may run while it travels to the host)
+    cudaMemcpyAsync(c->snap_dev, c->b64.w, sizeof(double) * c->S, cudaMemcpyDeviceToDevice, c->st);
+    cudaMemcpyAsync(c->snap_dev + c->S, c->b64.q, sizeof(double) * c->F, cudaMemcpyDeviceToDevice, c->st);
+    cudaMemcpyAsync(c->snap_dev + c->S + c->F, c->f, sizeof(double) * c->ncomp, cudaMemcpyDeviceToDevice, c->st);
+    cudaEventRecord(c->snap_copied, c->st);
+    cudaStreamWaitEvent(c->snap_st, c->snap_copied, 0);
+    cudaMemcpyAsync(c->snap_host, c->snap_dev, sizeof(double) * n, cudaMemcpyDeviceToHost, c->snap_st);
+    cudaEventRecord(c->snap_done, c->snap_st);
+    c->snap_timestep = c->timestep;
+    c->snap_time = c->time;
+    c->snap_valid = true;
+    return c->cuda_check("ibg_snapshot");
+}
+
+int ibg_snapshot_save(ibg_context* c, const char* filename) {
+    if (!c || !filename) return IBG_ERR_ARG;
+    if (!c->snap_valid) return c->fail(IBG_ERR_STATE, "ibg_snapshot_save: no snapshot taken");
+    if (cudaEventSynchronize(c->snap_done) != cudaSuccess) return c->cuda_check("ibg_snapshot_save");
+    const double* h = c->snap_host;
+    return write_restart(c, filename, h, h + c->S, h + c->S + c->F, c->snap_timestep, c->snap_time);
 }
 
 int ibg_set_state(ibg_context* c, const double* omega, const double* q, const double* f, int timestep, double time) {

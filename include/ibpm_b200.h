@@ -115,6 +115,24 @@ IBG_API int ibg_get_boundary_force(ibg_context* ctx, double* f, int* timestep, d
 IBG_API int ibg_update_operators(ibg_context* ctx, double time);
 IBG_API int ibg_refresh_state(ibg_context* ctx);
 
+/* --- restart files ------------------------------------------------------------
+ * State::save / State::load (src/State.cc:65-223) in the reference's binary
+ * restart format (grid header, q, omega, f as (fx, fy) pairs, timestep, time).
+ * ibg_save_restart writes the current state: 1 on success, 0 if the file
+ * cannot be opened.  ibg_load_restart reads a file into the context: 1 on
+ * success, 0 if the file cannot be opened, < 0 if its grid or point count
+ * differs from the context's (the reference resizes its State instead) or it
+ * is truncated.
+ * ibg_snapshot copies the current state on the device in stream order and
+ * sends it to pinned host memory on a side stream, so that the following
+ * ibg_advance calls run while it travels; ibg_snapshot_save waits for that
+ * copy and writes it as a restart file (the restart output of the reference's
+ * logger, src/OutputRestart.cc, without stalling the GPU). */
+IBG_API int ibg_save_restart(ibg_context* ctx, const char* filename);
+IBG_API int ibg_load_restart(ibg_context* ctx, const char* filename);
+IBG_API int ibg_snapshot(ibg_context* ctx);
+IBG_API int ibg_snapshot_save(ibg_context* ctx, const char* filename);
+
 /* IBSolver::advance (src/IBSolver.cc:142-149), nsteps times. */
 IBG_API int ibg_advance(ibg_context* ctx, int nsteps);
 /* State::computeNetForce (src/State.cc:53-63) of the current f */
