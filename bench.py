@@ -489,7 +489,7 @@ def main():
     roof = kernel_roofline(*run.roof_solver(), dtype="float" if form == "fp32" else "double")
     if wlname == "c2" and form == "fp64":
         # dram__bytes_read.sum + dram__bytes_write.sum of one k_dst_cols<double> launch on this workload
-        # (ncu --set full, cold launch; profiles/dst_cols_c2_fp64.md)
+        # (ncu --set full, cold launch; profiles/step_kernels_c2_fp64.md)
         roof["traffic"] = 3.22e6
         roof["traffic_note"] = "ncu dram read + write of one cold launch; writes stay in L2"
     extra = dict(run.extra)
