@@ -386,6 +386,12 @@ class Ensemble:
     def stream(self) -> int:
         return lib().ibg_ensemble_stream(self._h) or 0
 
+    def set_shapes(self, pairs_per_cta: int = 0, threads: int = 128, edge_maps: bool = False):
+        """One DST launch shape for all members (0 pairs: the rule); recaptured at the next advance."""
+        st = lib().ibg_ensemble_set_shapes(self._h, int(pairs_per_cta), int(threads), int(edge_maps))
+        if st < 0:
+            raise IbgError(f"ibg_ensemble_set_shapes: {lib().ibg_ensemble_last_error(self._h).decode()}")
+
     def launches_per_step(self) -> int:
         return int(lib().ibg_ensemble_launches_per_step(self._h))
 

@@ -257,6 +257,23 @@ struct ibg_context {
         snap_valid = false;
     }
 
+    // one launch shape for every DST pass of every plan (pairs 0: the rule); the next step recaptures
+    void set_shapes(int pairs, int threads, bool edge_maps) {
+        auto set = [&](auto& plan) {
+            plan.rows_P = plan.cols_P = pairs;
+            plan.rows_T = plan.cols_T = pairs > 0 ? threads : 0;
+            plan.rows_tws = plan.cols_tws = 0;
+            plan.edge_maps = edge_maps;
+        };
+        set(b64.poisson);
+        set(b32.poisson);
+        for (int k = 0; k < 4; ++k) {
+            set(b64.helm[k]);
+            set(b32.helm[k]);
+        }
+        drop_graph();
+    }
+
     void drop_graph() {
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
@@ -1520,6 +1537,28 @@ int ibg_ensemble_advance(ibg_ensemble* e, int nsteps) {
     // ... and whatever the members do next follows the ensemble step
     cudaEventRecord(e->done, e->st);
     for (ibg_context* c : e->members) cudaStreamWaitEvent(c->st, e->done, 0);
+    return IBG_OK;
+}
+
+int ibg_ensemble_set_shapes(ibg_ensemble* e, int pairs_per_cta, int threads, int edge_maps) {
+    if (!e || pairs_per_cta < 0 || pairs_per_cta > 2 ||
+        (pairs_per_cta > 0 && (threads < 32 || threads > 512 || threads % 32)))
+        return IBG_ERR_ARG;
+    cudaStreamSynchronize(e->st);
+    for (ibg_context* c : e->members) {
+        cudaStreamSynchronize(c->st);
+        c->set_shapes(pairs_per_cta, threads, edge_maps != 0);
+    }
+    // the parent graph is rebuilt from the members' new captures at the next advance
+    if (e->exec) cudaGraphExecDestroy(e->exec);
+    e->exec = nullptr;
+    if (e->graph) cudaGraphDestroy(e->graph);
+    e->graph = nullptr;
+    e->launches_per_step = 0;
+    if (cudaGraphCreate(&e->graph, 0) != cudaSuccess) {
+        e->err = "ibg_ensemble_set_shapes: graph creation failed";
+        return IBG_ERR_CUDA;
+    }
     return IBG_OK;
 }
 

@@ -173,6 +173,11 @@ typedef struct ibg_ensemble ibg_ensemble;
 IBG_API int ibg_ensemble_create(int n, ibg_context* const* members, ibg_ensemble** out);
 IBG_API int ibg_ensemble_advance(ibg_ensemble* ens, int nsteps);
 IBG_API int ibg_ensemble_destroy(ibg_ensemble* ens);
+/* one launch shape for every member's DST passes: pairs_per_cta 0 (the rule-based default), 1 or 2
+ * line pairs per CTA with `threads` threads; edge_maps 1 applies the precomputed sweep edge maps,
+ * 0 the per-step line FFTs (the default for members).  The members' steps are recaptured at the next
+ * ibg_ensemble_advance; results do not depend on the shape. */
+IBG_API int ibg_ensemble_set_shapes(ibg_ensemble* ens, int pairs_per_cta, int threads, int edge_maps);
 IBG_API void* ibg_ensemble_stream(const ibg_ensemble* ens);
 IBG_API long long ibg_ensemble_launches_per_step(const ibg_ensemble* ens);
 IBG_API const char* ibg_ensemble_last_error(const ibg_ensemble* ens);
