@@ -285,11 +285,12 @@ class Single:
         self.extra = {}
         if form == "learned":
             t0 = time.perf_counter()
-            geom, mb = self.s.lpc_generate(32, 0.0, 8.0)
+            geom, mb = self.s.lpc_generate(64, 0.0, 8.0)
             t1 = time.perf_counter()
-            hist = self.s.lpc_train(geom, mb, epochs=500, batch=4, lr=1e-3, seed=1)
+            hist = self.s.lpc_train(geom, mb, epochs=1500, batch=4, lr=2e-3, seed=1)
             t2 = time.perf_counter()
-            self.extra = {"training": {"configurations": 32, "times": [0.0, 8.0], "epochs": 500, "batch": 4,
+            self.extra = {"training": {"configurations": 64, "times": [0.0, 8.0], "epochs": 1500, "batch": 4,
+                                       "lr": 2e-3,
                                        "generate_s": t1 - t0, "train_s": t2 - t1, "loss_first": float(hist[0]),
                                        "loss_last": float(hist[-1])}}
         self.s.init()

@@ -340,3 +340,36 @@ def test_autotuner_records_valid_shapes():
         assert r["pairs_per_cta"] in (1, 2, 4) and r["threads"] in (128, 256, 512)
         assert r["twiddles_in_smem"] in (0, 1)
     s.close()
+
+
+def test_ensemble_shapes_do_not_change_results():
+    """Setting one launch shape for every member recaptures the members' steps; the
+    results stay those of the members run alone."""
+    import ibpm_b200 as ib
+    from ibpm_b200 import configs
+
+    def make():
+        grid = ib.Grid(64, 64, 2, 4.0, -2.0, -2.0)
+        geo = ib.geometry.parse(configs.cylinder_geom(48, r=0.4))
+        s = ib.NonlinearIBSolver(grid, ib.NavierStokesModel(grid, geo, 150.0), 0.01, "rk3")
+        s.init()
+        s.set_state(ib.State(grid, geo.num_points), with_q=False)
+        return s
+
+    alone = make()
+    alone.advance_resident(6)
+    fa = alone.force_history(6)
+    a, b = make(), make()
+    ens = ib.Ensemble([a, b])
+    ens.advance(2)
+    ens.set_shapes(2, 64, edge_maps=True)
+    ens.advance(2)
+    ens.set_shapes(0)
+    ens.advance(2)
+    for s in (a, b):
+        assert rel_l2(s.force_history(6), fa) < 1e-12
+    with pytest.raises(ib.IbgError):
+        ens.set_shapes(3, 128)
+    ens.close()
+    for s in (alone, a, b):
+        s.close()
