@@ -186,6 +186,31 @@ class NonlinearIBSolver:
         check(lib().ibg_get_state(self._h, _ptr(om), _ptr(q), _ptr(f), ctypes.byref(ts), ctypes.byref(t)), self._h)
         x.omega, x.q, x.f, x.timestep, x.time = om, q, f, ts.value, t.value
 
+    # -- the other N(x) forms (src/IBSolver.cc:211-283) ----------------------
+    def set_linearized(self, omega0, q0=None):
+        """LinearizedIBSolver (one base state) or LinearizedPeriodicIBSolver (a list of
+        them, phase = timestep % period).  None restores the nonlinear solver."""
+        if omega0 is None:
+            check(lib().ibg_set_linearized(self._h, 0, None, None), self._h)
+            return
+        w = np.ascontiguousarray(np.stack([np.asarray(a, dtype=np.float64) for a in
+                                           (omega0 if isinstance(omega0, (list, tuple)) else [omega0])]))
+        q = np.ascontiguousarray(np.stack([np.asarray(a, dtype=np.float64) for a in
+                                           (q0 if isinstance(q0, (list, tuple)) else [q0])]))
+        if w.shape[0] != q.shape[0]:
+            raise ValueError("as many base vorticity fields as base flux fields")
+        check(lib().ibg_set_linearized(self._h, int(w.shape[0]), _ptr(w), _ptr(q)), self._h)
+
+    def set_sfd(self, chi: float, Delta: float, omega_hat=None):
+        """SFDSolver: selective frequency damping with gain chi and filter width Delta."""
+        wh = None if omega_hat is None else np.ascontiguousarray(omega_hat, dtype=np.float64)
+        check(lib().ibg_set_sfd(self._h, float(chi), float(Delta), _ptr(wh)), self._h)
+
+    def sfd_filtered(self) -> np.ndarray:
+        out = np.zeros(self.grid.scalar().shape)
+        check(lib().ibg_get_sfd_state(self._h, _ptr(out)), self._h)
+        return out
+
     # -- restart files (State::save / State::load, src/State.cc:65-223) -------
     def save_restart(self, filename: str) -> bool:
         return check(lib().ibg_save_restart(self._h, filename.encode()), self._h) == 1

@@ -7,6 +7,7 @@
 // into a CUDA graph and replayed.  Moving bodies use CG, whose convergence
 // test is read back every few iterations.
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstdio>
 #include <random>
@@ -172,6 +173,24 @@ struct ibg_context {
     // force history
     double* d_hist = nullptr;
     int* d_hist_count = nullptr;
+    // the other N(x) forms (src/IBSolver.cc:211-283): 0 nonlinear, 1 linearized (period >= 1), 2 SFD
+    int nmode = 0;
+    int period = 0;
+    double* d_base_w = nullptr;  // period x S base vorticity
+    double* d_base_q = nullptr;  // period x F base fluxes
+    int* d_ts0 = nullptr;        // State timestep at the last upload (steps since then: d_hist_count)
+    double* d_what = nullptr;    // SFD filtered vorticity
+    double* d_rprev = nullptr;   // SFD previous filter right-hand side
+    double sfd_chi = 0.0, sfd_Delta = 1.0;
+    bool sfd_rhs_saved = false;
+    void release_variant() {
+        double* p[] = {d_base_w, d_base_q, d_what, d_rprev};
+        for (double* x : p)
+            if (x) cudaFree(x);
+        d_base_w = d_base_q = d_what = d_rprev = nullptr;
+        nmode = 0;
+        period = 0;
+    }
     long long hist_steps = 0;
     // graph
     cudaGraph_t graph_def = nullptr;   // the captured step (kept for ensembles)
@@ -282,6 +301,9 @@ struct ibg_context {
     }
     void release() {
         release_snapshot();
+        release_variant();
+        if (d_ts0) cudaFree(d_ts0);
+        d_ts0 = nullptr;
         drop_graph();
         b64.release();
         b32.release();
@@ -539,7 +561,20 @@ struct ibg_context {
             Nk = B.Nbuf[k];
             Np = B.Nbuf[(k + sch.nsub - 1) % sch.nsub];
         }
-        launch_nonlinear<T>(g, B.q, B.w, B.U, B.V, B.C, Nk, 1, S, F, st);
+        if constexpr (std::is_same<T, double>::value) {
+            if (nmode == 1)
+                launch_nonlinear_lin(g, B.q, B.w, d_base_q, d_base_w, period, d_ts0, d_hist_count, B.U, B.V, B.C,
+                                     Nk, st);
+            else
+                launch_nonlinear<T>(g, B.q, B.w, B.U, B.V, B.C, Nk, 1, S, F, st);
+            if (nmode == 2) {
+                launch_sfd(S, B.w, d_what, d_rprev, Nk, sfd_chi, sfd_Delta, an, bn, prm.dt, !sfd_rhs_saved, st);
+                sfd_rhs_saved = true;
+                launches += 1;
+            }
+        } else {
+            launch_nonlinear<T>(g, B.q, B.w, B.U, B.V, B.C, Nk, 1, S, F, st);
+        }
         launches += 2 + g.L;
         if (moving) move_bodies(cn * prm.dt);
         const T* Nprev = nullptr;
@@ -920,7 +955,7 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
         c->alloc(&c->slots.idx, kSlots * m) || c->alloc(&c->slots.w, kSlots * m) || c->alloc(&c->slots.n, m) ||
         c->alloc(&c->d_b, m) || c->alloc(&c->d_time, 1) || c->alloc(&c->d_status, 1) || c->alloc(&c->cg_r, m) ||
         c->alloc(&c->cg_d, m) || c->alloc(&c->cg_q, m) || c->alloc(&c->cg_z, m) || c->alloc(&c->cg_zold, m) || c->alloc(&c->cg_scal, 4) || c->alloc(&c->cg_flags, 10) ||
-        c->alloc(&c->d_hist, 2 * (size_t)kHistCap) || c->alloc(&c->d_hist_count, 1);
+        c->alloc(&c->d_hist, 2 * (size_t)kHistCap) || c->alloc(&c->d_hist_count, 1) || c->alloc(&c->d_ts0, 1);
     if (!s && cudaMallocHost((void**)&c->h_flags, 4 * sizeof(int)) != cudaSuccess) s = IBG_ERR_CUDA;
     if (s) {
         g_create_error = "ibg_create: device allocation failed";
@@ -1152,6 +1187,48 @@ int ibg_snapshot_save(ibg_context* c, const char* filename) {
     return write_restart(c, filename, h, h + c->S, h + c->S + c->F, c->snap_timestep, c->snap_time);
 }
 
+// ---------------------------------------------------------------------------
+// the other N(x) forms
+// ---------------------------------------------------------------------------
+int ibg_set_linearized(ibg_context* c, int period, const double* omega0, const double* q0) {
+    if (!c || period < 0 || (period > 0 && (!omega0 || !q0))) return IBG_ERR_ARG;
+    if (c->fp32) return c->fail(IBG_ERR_UNSUPPORTED, "ibg_set_linearized: the linearized forms run in FP64 only");
+    cudaStreamSynchronize(c->st);
+    c->release_variant();
+    c->drop_graph();
+    if (period == 0) return IBG_OK;  // back to NonlinearIBSolver
+    if (c->alloc(&c->d_base_w, (size_t)period * c->S, false) || c->alloc(&c->d_base_q, (size_t)period * c->F, false))
+        return IBG_ERR_CUDA;
+    cudaMemcpy(c->d_base_w, omega0, sizeof(double) * period * c->S, cudaMemcpyHostToDevice);
+    cudaMemcpy(c->d_base_q, q0, sizeof(double) * period * c->F, cudaMemcpyHostToDevice);
+    c->nmode = 1;
+    c->period = period;
+    return c->cuda_check("ibg_set_linearized");
+}
+
+int ibg_set_sfd(ibg_context* c, double chi, double Delta, const double* omega_hat) {
+    if (!c || !(Delta != 0.0)) return IBG_ERR_ARG;
+    if (c->fp32) return c->fail(IBG_ERR_UNSUPPORTED, "ibg_set_sfd: selective frequency damping runs in FP64 only");
+    cudaStreamSynchronize(c->st);
+    c->release_variant();
+    c->drop_graph();
+    if (c->alloc(&c->d_what, c->S) || c->alloc(&c->d_rprev, c->S)) return IBG_ERR_CUDA;
+    if (omega_hat) cudaMemcpy(c->d_what, omega_hat, sizeof(double) * c->S, cudaMemcpyHostToDevice);
+    c->nmode = 2;
+    c->sfd_chi = chi;
+    c->sfd_Delta = Delta;
+    c->sfd_rhs_saved = false;
+    return c->cuda_check("ibg_set_sfd");
+}
+
+int ibg_get_sfd_state(ibg_context* c, double* omega_hat) {
+    if (!c || !omega_hat) return IBG_ERR_ARG;
+    if (c->nmode != 2) return c->fail(IBG_ERR_STATE, "ibg_get_sfd_state: selective frequency damping is not on");
+    cudaMemcpyAsync(omega_hat, c->d_what, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->cuda_check("ibg_get_sfd_state");
+    return IBG_OK;
+}
+
 int ibg_set_state(ibg_context* c, const double* omega, const double* q, const double* f, int timestep, double time) {
     if (!c) return IBG_ERR_ARG;
     Bulk<double>& B = c->b64;
@@ -1163,6 +1240,7 @@ int ibg_set_state(ibg_context* c, const double* omega, const double* q, const do
     c->time = time;
     cudaMemcpyAsync(c->d_time, &c->time, sizeof(double), cudaMemcpyHostToDevice, c->st);
     cudaMemsetAsync(c->d_hist_count, 0, sizeof(int), c->st);
+    cudaMemcpyAsync(c->d_ts0, &c->timestep, sizeof(int), cudaMemcpyHostToDevice, c->st);
     c->hist_steps = 0;
     if (q) {
         cudaMemcpyAsync(B.q, q, sizeof(double) * c->F, cudaMemcpyHostToDevice, c->st);

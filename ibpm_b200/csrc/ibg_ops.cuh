@@ -48,4 +48,11 @@ template <typename T>
 void launch_smear_bf_unit(const GridDev& g, int ncomp, int col0, int batch, const RegSlots& s, double* flux0,
                           size_t fstride, T* Bf, size_t sstride, double beta, cudaStream_t st);
 
+// the other N(x) forms (FP64 only)
+void launch_nonlinear_lin(const GridDev& g, const double* q, const double* w, const double* qb, const double* wb,
+                          int period, const int* ts0, const int* count, double* U, double* V, double* C, double* N,
+                          cudaStream_t st);
+void launch_sfd(size_t n, const double* w, double* what, double* rprev, double* N, double chi, double Delta,
+                double an, double bn, double dt, bool first, cudaStream_t st);
+
 }  // namespace ibg

@@ -31,20 +31,16 @@ __device__ __forceinline__ T qy_at(const T* q_lev, const GridDev& g, int i, int 
 // the reference defines u, v (coarse overlap interior nodes are never read
 // downstream and are written as zero).
 // ---------------------------------------------------------------------------
+// velocities (u, v) at node (i, j) of level `lev` from the fluxes of that level (ql) and of the
+// next finer one (FluxToXVelocity / FluxToYVelocity, src/VectorOperations.cc:224-368); du / dv
+// false where the reference leaves the value undefined (coarse overlap interior)
 template <typename T>
-__global__ void k_node_vel(GridDev g, const T* __restrict__ q, const T* __restrict__ w, T* __restrict__ U,
-                           T* __restrict__ V, size_t sstride, size_t fstride) {
-    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const size_t total = (size_t)g.L * g.N1;
-    if (tid >= total) return;
-    const size_t sb = (size_t)blockIdx.y * sstride, fb = (size_t)blockIdx.y * fstride;
-    const int lev = (int)(tid / g.N1);
-    const int r = (int)(tid % g.N1);
-    const int i = r / g.NJ + 1, j = r % g.NJ + 1;
-    const T* ql = q + fb + (size_t)lev * g.F1;
+__device__ __forceinline__ void node_uv(const GridDev& g, const T* ql, int lev, int i, int j, T& u, T& v, bool& du,
+                                        bool& dv) {
     const int nx = g.nx, ny = g.ny, nx2 = g.nxe, ny2 = g.nye;
-    T u = (T)0, v = (T)0;
-    bool du = true, dv = true;
+    u = (T)0;
+    v = (T)0;
+    du = dv = true;
     if (lev == 0) {
         const T o2d = (T)(1.0 / (2 * g.dx));
         u = (qx_at(ql, g, i, j) + qx_at(ql, g, i, j - 1)) * o2d;
@@ -98,9 +94,68 @@ __global__ void k_node_vel(GridDev g, const T* __restrict__ q, const T* __restri
             dv = false;
         }
     }
+}
+
+template <typename T>
+__global__ void k_node_vel(GridDev g, const T* __restrict__ q, const T* __restrict__ w, T* __restrict__ U,
+                           T* __restrict__ V, size_t sstride, size_t fstride) {
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t total = (size_t)g.L * g.N1;
+    if (tid >= total) return;
+    const size_t sb = (size_t)blockIdx.y * sstride, fb = (size_t)blockIdx.y * fstride;
+    const int lev = (int)(tid / g.N1);
+    const int r = (int)(tid % g.N1);
+    const int i = r / g.NJ + 1, j = r % g.NJ + 1;
+    T u, v;
+    bool du, dv;
+    node_uv(g, q + fb + (size_t)lev * g.F1, lev, i, j, u, v, du, dv);
     const T wv = w[sb + tid];
     U[sb + tid] = du ? (u * wv) * (T)-1 : (T)0;
     V[sb + tid] = dv ? v * wv : (T)0;
+}
+
+// LinearizedIBSolver / LinearizedPeriodicIBSolver node products (src/IBSolver.cc:211-216, 224-232):
+// CrossProduct(q0, omega) + CrossProduct(q, omega0) before the flux stencils (which are linear),
+// with the base state of phase (timestep % period); the step counter lives on the device
+// (ts0 = timestep at the last state upload, count = steps since then).
+__global__ void k_node_vel_lin(GridDev g, const double* __restrict__ q, const double* __restrict__ w,
+                               const double* __restrict__ qb, const double* __restrict__ wb, int period,
+                               const int* __restrict__ ts0, const int* __restrict__ count, double* __restrict__ U,
+                               double* __restrict__ V) {
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t total = (size_t)g.L * g.N1;
+    if (tid >= total) return;
+    const int phase = ((*ts0 + *count) % period + period) % period;
+    const double* q0 = qb + (size_t)phase * g.L * g.F1;
+    const double* w0 = wb + (size_t)phase * total;
+    const int lev = (int)(tid / g.N1);
+    const int r = (int)(tid % g.N1);
+    const int i = r / g.NJ + 1, j = r % g.NJ + 1;
+    double u, v, ub, vb;
+    bool du, dv;
+    node_uv(g, q + (size_t)lev * g.F1, lev, i, j, u, v, du, dv);
+    node_uv(g, q0 + (size_t)lev * g.F1, lev, i, j, ub, vb, du, dv);
+    const double wv = w[tid], w0v = w0[tid];
+    U[tid] = du ? (ub * wv) * -1.0 + (u * w0v) * -1.0 : 0.0;
+    V[tid] = dv ? vb * wv + v * w0v : 0.0;
+}
+
+// SFDSolver (src/IBSolver.cc:238-283): N -= chi (omega - omega_hat), then the filtered state
+// advances from the vorticity at the start of the sub-step:
+// rhs = (omega - omega_hat) / Delta, omega_hat += dt (an rhs + bn rhs_prev), rhs_prev = rhs
+__global__ void k_sfd(size_t n, const double* __restrict__ w, double* __restrict__ what, double* __restrict__ rprev,
+                      double* __restrict__ N, double chi, double Delta, double an, double bn, double dt,
+                      int first) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const double d = w[t] - what[t];
+    N[t] = N[t] - chi * d;
+    const double rhs = d / Delta;
+    double a = an * rhs;
+    if (bn != 0.0) a += bn * (first ? rhs : rprev[t]);
+    a *= dt;
+    what[t] = what[t] + a;
+    rprev[t] = rhs;
 }
 
 // ---------------------------------------------------------------------------
@@ -433,6 +488,21 @@ void launch_nonlinear(const GridDev& g, const T* q, const T* w, T* U, T* V, T* C
     for (int lev = 0; lev < g.L; ++lev)
         k_cross_flux<T><<<dim3(nblk(g.F1, 256), batch), 256, 0, st>>>(g, lev, U, V, C, sstride, fstride);
     k_curl_flux<T><<<dim3(nblk(S, 256), batch), 256, 0, st>>>(g, C, N, sstride, fstride);
+}
+
+void launch_nonlinear_lin(const GridDev& g, const double* q, const double* w, const double* qb, const double* wb,
+                          int period, const int* ts0, const int* count, double* U, double* V, double* C, double* N,
+                          cudaStream_t st) {
+    const size_t S = (size_t)g.L * g.N1, F = (size_t)g.L * g.F1;
+    k_node_vel_lin<<<nblk(S, 256), 256, 0, st>>>(g, q, w, qb, wb, period, ts0, count, U, V);
+    for (int lev = 0; lev < g.L; ++lev)
+        k_cross_flux<double><<<dim3(nblk(g.F1, 256), 1), 256, 0, st>>>(g, lev, U, V, C, S, F);
+    k_curl_flux<double><<<dim3(nblk(S, 256), 1), 256, 0, st>>>(g, C, N, S, F);
+}
+
+void launch_sfd(size_t n, const double* w, double* what, double* rprev, double* N, double chi, double Delta,
+                double an, double bn, double dt, bool first, cudaStream_t st) {
+    k_sfd<<<nblk(n, 256), 256, 0, st>>>(n, w, what, rprev, N, chi, Delta, an, bn, dt, first ? 1 : 0);
 }
 
 template <typename T>

@@ -133,6 +133,22 @@ IBG_API int ibg_load_restart(ibg_context* ctx, const char* filename);
 IBG_API int ibg_snapshot(ibg_context* ctx);
 IBG_API int ibg_snapshot_save(ibg_context* ctx, const char* filename);
 
+/* --- the other N(x) forms (src/IBSolver.cc:211-283), FP64 ------------------------
+ * ibg_set_linearized: LinearizedIBSolver (period 1) or LinearizedPeriodicIBSolver
+ * (period P): N(x) = Curl(q0 x omega + q x omega0) with the base state of phase
+ * timestep % period; omega0 and q0 hold `period` states one after the other in
+ * the Scalar and Flux layouts.  As the reference CLI builds the linear models,
+ * create the context with u_mag = 0 (no uniform base flow).  period 0 restores
+ * NonlinearIBSolver.
+ * ibg_set_sfd: SFDSolver, N(x) = Curl(q x omega) - chi (omega - omega_hat) with
+ * the filtered vorticity omega_hat advanced every sub-step by
+ * (omega - omega_hat) / Delta; omega_hat starts from the given field (NULL: zero,
+ * what the reference CLI's loadFilteredState leaves without a _xhat file).
+ * ibg_get_sfd_state reads omega_hat (SFDSolver::saveFilteredState). */
+IBG_API int ibg_set_linearized(ibg_context* ctx, int period, const double* omega0, const double* q0);
+IBG_API int ibg_set_sfd(ibg_context* ctx, double chi, double Delta, const double* omega_hat);
+IBG_API int ibg_get_sfd_state(ibg_context* ctx, double* omega_hat);
+
 /* IBSolver::advance (src/IBSolver.cc:142-149), nsteps times. */
 IBG_API int ibg_advance(ibg_context* ctx, int nsteps);
 /* State::computeNetForce (src/State.cc:53-63) of the current f */

@@ -489,6 +489,14 @@ def nonlinear(g: Grid, q: np.ndarray, w: np.ndarray) -> np.ndarray:
     return curl_flux(g, cross_product(g, q, w))
 
 
+def linearized(g: Grid, q: np.ndarray, w: np.ndarray, q0: np.ndarray, w0: np.ndarray) -> np.ndarray:
+    """LinearizedIBSolver::N = Curl(q0 x omega + q x omega0) (src/IBSolver.cc:211-216); the periodic
+    form uses the base state of phase timestep % period (src/IBSolver.cc:224-232)."""
+    v = cross_product(g, q0, w)
+    v = v + cross_product(g, q, w0)
+    return curl_flux(g, v)
+
+
 # ----------------------------------------------------------------------------
 # Elliptic solvers (src/EllipticSolver2d.cc:26-185, src/EllipticSolver.cc:47-108)
 # ----------------------------------------------------------------------------
@@ -895,10 +903,19 @@ class State:
 
 
 class IBSolver:
-    """NonlinearIBSolver::advance / advanceSubstep (src/IBSolver.cc:142-198)."""
+    """NonlinearIBSolver::advance / advanceSubstep (src/IBSolver.cc:142-198), and the other N(x)
+    forms: `base` = list of (omega0, q0) for LinearizedIBSolver (one state) or
+    LinearizedPeriodicIBSolver (one per phase); `sfd` = (chi, Delta, omega_hat) for SFDSolver
+    (src/IBSolver.cc:238-283; omega_hat is the filtered vorticity it starts from)."""
 
-    def __init__(self, model: Model, dt: float, scheme: str = "rk3", tol: float = 1e-7, max_iter: int = 3000):
+    def __init__(self, model: Model, dt: float, scheme: str = "rk3", tol: float = 1e-7, max_iter: int = 3000,
+                 base=None, sfd=None):
         self.model, self.dt, self.coef = model, dt, SCHEMES[scheme]
+        self.base = base
+        self.sfd = None
+        if sfd is not None:
+            chi, Delta, what = sfd
+            self.sfd = dict(chi=chi, Delta=Delta, what=np.array(what, dtype=float), rhs_prev=None)
         method = "cholesky" if model.stationary else "cg"
         self.solvers = [ProjectionSolver(model, (an + bn) * dt, method, tol, max_iter)
                         for (an, bn, cn) in self.coef]
@@ -913,7 +930,21 @@ class IBSolver:
     def advance(self, x: State) -> None:
         g, m = self.model.g, self.model
         for k, (an, bn, cn) in enumerate(self.coef):
-            n = nonlinear(g, x.q, x.omega)
+            if self.base is not None:
+                w0, q0 = self.base[x.timestep % len(self.base)]
+                n = linearized(g, x.q, x.omega, q0, w0)
+            else:
+                n = nonlinear(g, x.q, x.omega)
+            if self.sfd is not None:
+                sf = self.sfd
+                n = n - sf["chi"] * (x.omega - sf["what"])
+                # the filtered state advances from the vorticity at the start of the sub-step
+                rhs = (x.omega - sf["what"]) / sf["Delta"]
+                a_f = an * rhs
+                if bn != 0:
+                    a_f = a_f + bn * (sf["rhs_prev"] if sf["rhs_prev"] is not None else rhs)
+                sf["what"] = sf["what"] + a_f * self.dt
+                sf["rhs_prev"] = rhs
             if not m.stationary:
                 m.update_operators(x.time + cn * self.dt)
             a = laplacian(g, x.omega) * (0.5 * m.alpha * (an + bn))

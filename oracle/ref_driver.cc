@@ -13,12 +13,19 @@
 //                   -geom FILE -Re R -dt DT -scheme rk3|euler|ab2|rk3b
 //                   -nsteps K [-tol T] [-alpha DEG] [-ic restart.bin]
 //                   [-out PREFIX] [-dump_every K] [-warmup W] [-cholesky_cache BASENAME]
+//                   [-model nonlinear|linear|linearperiodic|sfd] [-baseflow FILE]
+//                   [-pbase PREFIX -period P] [-chi X -Delta X]
+// -model selects the solver class as the CLI does (src/ibpm.cc:184-229): the
+// linear models get a NavierStokesModel without base flow and the base state(s)
+// from restart files (FILE, or PREFIX_<k>.bin for k < P); sfd reads its filtered
+// state like the CLI (loadFilteredState of the initial condition's name).
 #include "ibpm.h"
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
 #include <cmath>
 #include <string>
+#include <vector>
 #include <iostream>
 
 using namespace ibpm;
@@ -31,7 +38,9 @@ static double now_s() {
 int main(int argc, char* argv[]) {
     int nx = 200, ny = 200, ngrid = 1, nsteps = 10, dumpEvery = 0, warmup = 0;
     double length = 4, xoff = -2, yoff = -2, Re = 100, dt = 0.01, tol = 1e-7, alphaDeg = 0;
-    std::string geomFile, scheme = "rk3", ic, out, cache;
+    std::string geomFile, scheme = "rk3", ic, out, cache, modelName = "nonlinear", baseFile, pbase;
+    int period = 1;
+    double chi = 0.02, Delta = 15.;
     for (int a = 1; a + 1 < argc; a += 2) {
         std::string k = argv[a];
         const char* v = argv[a + 1];
@@ -53,6 +62,12 @@ int main(int argc, char* argv[]) {
         else if (k == "-dump_every") dumpEvery = atoi(v);
         else if (k == "-warmup") warmup = atoi(v);
         else if (k == "-cholesky_cache") cache = v;
+        else if (k == "-model") modelName = v;
+        else if (k == "-baseflow") baseFile = v;
+        else if (k == "-pbase") pbase = v;
+        else if (k == "-period") period = atoi(v);
+        else if (k == "-chi") chi = atof(v);
+        else if (k == "-Delta") Delta = atof(v);
         else { std::cerr << "unknown flag " << k << std::endl; return 2; }
     }
     Scheme::SchemeType st = Scheme::RK3;
@@ -66,14 +81,40 @@ int main(int argc, char* argv[]) {
     double pi = 4. * atan(1.);
     double alpha = alphaDeg * pi / 180.;
     BaseFlow q_potential(grid, 1.0, alpha);
-    NavierStokesModel model(grid, geom, Re, q_potential);
-    NonlinearIBSolver solver(grid, model, dt, st, tol);
+    const bool linear = modelName == "linear" || modelName == "linearperiodic";
+    NavierStokesModel* mp = linear ? new NavierStokesModel(grid, geom, Re) : new NavierStokesModel(grid, geom, Re, q_potential);
+    NavierStokesModel& model = *mp;
+    IBSolver* sp = NULL;
+    SFDSolver* sfd = NULL;
+    if (modelName == "nonlinear") {
+        sp = new NonlinearIBSolver(grid, model, dt, st, tol);
+    } else if (modelName == "linear") {
+        State x00(grid, geom.getNumPoints());
+        if (!x00.load(baseFile)) { std::cerr << "baseflow load failed\n"; return 5; }
+        sp = new LinearizedIBSolver(grid, model, dt, st, tol, x00);
+    } else if (modelName == "linearperiodic") {
+        std::vector<State> x0;
+        for (int k = 0; k < period; ++k) {
+            State xk(grid, geom.getNumPoints());
+            if (!xk.load(pbase + "_" + std::to_string(k) + ".bin")) { std::cerr << "periodic base load failed\n"; return 5; }
+            x0.push_back(xk);
+        }
+        sp = new LinearizedPeriodicIBSolver(grid, model, dt, st, tol, x0, period);
+    } else if (modelName == "sfd") {
+        sfd = new SFDSolver(grid, model, dt, st, Delta, chi);
+        sp = sfd;
+    } else {
+        std::cerr << "unknown model " << modelName << std::endl;
+        return 2;
+    }
+    IBSolver& solver = *sp;
 
     State x(grid, geom.getNumPoints());
     x.omega = 0.; x.f = 0.; x.q = 0.;
     if (!ic.empty()) {
         if (!x.load(ic)) { std::cerr << "ic load failed\n"; return 4; }
     }
+    if (sfd) sfd->loadFilteredState(ic);
     geom.moveBodies(x.time);
     model.init();
     double t0 = now_s();

@@ -76,8 +76,77 @@ def run(case):
     print(name, "written", forces[-1, 2:4])
 
 
+# The other N(x) variants of the reference (src/IBSolver.cc:211-311) on one small two-domain case.
+# The base states of the linear models are states of a short nonlinear run written by the reference.
+VARIANT_GRID = dict(nx=32, ny=32, ngrid=2, length=3.0, xoff=-1.5, yoff=-1.5)
+VARIANT_GEOM = configs.cylinder_geom(24, r=0.4)
+VARIANTS = [
+    # name, model, Re, dt, nsteps, scheme, extra
+    ("var_linear_l2_rk3", "linear", 150.0, 0.02, 6, "rk3", {}),
+    ("var_linearperiodic_l2_rk3", "linearperiodic", 150.0, 0.02, 6, "rk3", {"period": 2}),
+    ("var_sfd_l2_rk3", "sfd", 150.0, 0.02, 6, "rk3", {"chi": 0.5, "Delta": 2.0}),
+    ("var_sfd_l2_ab2", "sfd", 150.0, 0.02, 6, "ab2", {"chi": 0.5, "Delta": 2.0}),
+]
+
+
+def run_variant(case):
+    name, model, Re, dt, nsteps, scheme, extra = case
+    G = VARIANT_GRID
+    nx, ny, ngrid = G["nx"], G["ny"], G["ngrid"]
+    from ibpm_b200 import geometry
+    npts = geometry.parse(VARIANT_GEOM).num_points
+    g = O.Grid(nx, ny, ngrid, G["length"], G["xoff"], G["yoff"])
+    with tempfile.TemporaryDirectory() as td:
+        gpath = os.path.join(td, "body.geom")
+        with open(gpath, "w") as fh:
+            fh.write(VARIANT_GEOM)
+        common = [DRIVER, "-nx", str(nx), "-ny", str(ny), "-ngrid", str(ngrid), "-length", repr(G["length"]),
+                  "-xoffset", repr(G["xoff"]), "-yoffset", repr(G["yoff"]), "-geom", gpath, "-Re", repr(Re),
+                  "-dt", repr(dt), "-scheme", scheme]
+        wl = configs.Workload(name, nx, ny, ngrid, G["length"], G["xoff"], G["yoff"], VARIANT_GEOM, Re, dt, nsteps,
+                              noise_amp=1e-2, noise_seed=11, noise_box=(0.0, 1e9, -0.8, 0.8))
+        w0 = wl.initial_vorticity()
+        ic = os.path.join(td, "ic.bin")
+        O.save_restart(ic, O.State(g, npts, omega=w0), g)
+        # base states: a nonlinear run from the same noise, steps 3 and 4
+        subprocess.run(common + ["-nsteps", "4", "-ic", ic, "-out", os.path.join(td, "base"), "-dump_every", "1"],
+                       check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        bases = [O.load_restart(os.path.join(td, "base_%05d.bin" % k)) for k in (3, 4)]
+        args = common + ["-nsteps", str(nsteps), "-model", model, "-out", os.path.join(td, "run")]
+        rec = {"model": model}
+        if model in ("linear", "linearperiodic"):
+            # the perturbation starts as the noise alone (no base flow in a linear model)
+            period = extra.get("period", 1)
+            for k in range(period):
+                O.save_restart(os.path.join(td, "pb_%d.bin" % k),
+                               O.State(g, npts, omega=bases[k]["omega"], q=bases[k]["q"]), g)
+            if model == "linear":
+                args += ["-baseflow", os.path.join(td, "pb_0.bin")]
+            else:
+                args += ["-pbase", os.path.join(td, "pb"), "-period", str(period)]
+            rec["period"] = period
+            rec["base_omega"] = np.stack([bases[k]["omega"] for k in range(period)])
+            rec["base_q"] = np.stack([bases[k]["q"] for k in range(period)])
+        else:
+            args += ["-chi", repr(extra["chi"]), "-Delta", repr(extra["Delta"])]
+            rec["chi"], rec["Delta"] = extra["chi"], extra["Delta"]
+        args += ["-ic", ic]
+        subprocess.run(args, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        forces = np.loadtxt(os.path.join(td, "run.forces")).reshape(-1, 6)
+        fin = O.load_restart(os.path.join(td, "run_final.bin"))
+    np.savez_compressed(
+        os.path.join(HERE, name + ".npz"),
+        nx=nx, ny=ny, ngrid=ngrid, length=G["length"], xoffset=G["xoff"], yoffset=G["yoff"], geom=VARIANT_GEOM,
+        Re=Re, dt=dt, nsteps=nsteps, scheme=scheme, tol=1e-7, omega0=w0,
+        forces=forces, omega=fin["omega"], q=fin["q"], f=fin["f"], timestep=fin["timestep"], time=fin["time"], **rec)
+    print(name, "written", forces[-1, 2:4])
+
+
 if __name__ == "__main__":
     only = set(sys.argv[1:])
     for c in CASES:
         if not only or c[0] in only:
             run(c)
+    for c in VARIANTS:
+        if not only or c[0] in only:
+            run_variant(c)

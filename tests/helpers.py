@@ -16,7 +16,14 @@ FP64_TOL = 1e-10
 
 
 def golden_names():
-    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+    """Fixtures of the nonlinear solver (NonlinearIBSolver)."""
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz"))
+                  if not os.path.basename(p).startswith("var_"))
+
+
+def variant_names():
+    """Fixtures of the other N(x) forms: linearized, linearized-periodic, SFD."""
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "var_*.npz")))
 
 
 def load_golden(name):
@@ -46,3 +53,25 @@ def rel_l2(a, b):
     b = np.asarray(b, dtype=np.float64)
     nb = np.linalg.norm(b)
     return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
+
+
+def oracle_from_variant(d):
+    """Oracle solver and initial state for a fixture of tests/golden/var_*.npz."""
+    from oracle import ibpm_oracle as O
+    from ibpm_b200 import geometry
+    g = O.Grid(int(d["nx"]), int(d["ny"]), int(d["ngrid"]), float(d["length"]), float(d["xoffset"]),
+               float(d["yoffset"]))
+    geo = geometry.parse(str(d["geom"]))
+    bodies = [O.Body(np.array(b.points, dtype=float)) for b in geo.bodies]
+    model_name = str(d["model"])
+    linear = model_name in ("linear", "linearperiodic")
+    # the linear models run without the uniform base flow, as the reference CLI builds them
+    model = O.Model(g, bodies, float(d["Re"]), u_mag=0.0 if linear else 1.0)
+    base = sfd = None
+    if linear:
+        base = [(np.array(d["base_omega"][k]), np.array(d["base_q"][k])) for k in range(int(d["period"]))]
+    else:
+        sfd = (float(d["chi"]), float(d["Delta"]), g.scalar())
+    solver = O.IBSolver(model, float(d["dt"]), str(d["scheme"]), float(d["tol"]), base=base, sfd=sfd)
+    x = O.State(g, model.npts, omega=np.array(d["omega0"], dtype=float))
+    return g, model, solver, x

@@ -126,3 +126,22 @@ def test_restart_roundtrip(tmp_path):
     assert d["nx"] == 16 and d["ny"] == 8 and d["ngrid"] == 2 and d["npts"] == 5
     assert np.array_equal(d["omega"], x.omega) and np.array_equal(d["q"], x.q) and np.array_equal(d["f"], x.f)
     assert d["timestep"] == 7 and d["time"] == 0.125
+
+
+@pytest.mark.parametrize("name", __import__("helpers").variant_names())
+def test_oracle_reproduces_variant_golden(name):
+    """Linearized, linearized-periodic and SFD solvers (src/IBSolver.cc:211-283) against
+    fixtures the reference itself produced."""
+    from helpers import oracle_from_variant
+    d = load_golden(name)
+    g, model, solver, x = oracle_from_variant(d)
+    model.update_operators(x.time)
+    x.q = model.flux(x.omega)
+    solver.init()
+    forces = []
+    for _ in range(int(d["nsteps"])):
+        solver.advance(x)
+        forces.append(x.net_force())
+    assert rel_l2(np.array(forces), d["forces"][:, 2:4]) < FP64_TOL
+    assert rel_l2(x.omega, d["omega"]) < FP64_TOL
+    assert rel_l2(x.q, d["q"]) < FP64_TOL
