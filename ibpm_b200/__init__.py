@@ -201,6 +201,12 @@ class NonlinearIBSolver:
             raise ValueError("as many base vorticity fields as base flux fields")
         check(lib().ibg_set_linearized(self._h, int(w.shape[0]), _ptr(w), _ptr(q)), self._h)
 
+    def set_adjoint(self, omega0, q0):
+        """AdjointIBSolver about the base state (omega0, q0)."""
+        w = np.ascontiguousarray(omega0, dtype=np.float64)
+        q = np.ascontiguousarray(q0, dtype=np.float64)
+        check(lib().ibg_set_adjoint(self._h, _ptr(w), _ptr(q)), self._h)
+
     def set_sfd(self, chi: float, Delta: float, omega_hat=None):
         """SFDSolver: selective frequency damping with gain chi and filter width Delta."""
         wh = None if omega_hat is None else np.ascontiguousarray(omega_hat, dtype=np.float64)

@@ -562,11 +562,21 @@ struct ibg_context {
             Np = B.Nbuf[(k + sch.nsub - 1) % sch.nsub];
         }
         if constexpr (std::is_same<T, double>::value) {
-            if (nmode == 1)
+            if (nmode == 1) {
                 launch_nonlinear_lin(g, B.q, B.w, d_base_q, d_base_w, period, d_ts0, d_hist_count, B.U, B.V, B.C,
                                      Nk, st);
-            else
+            } else if (nmode == 3) {
+                // AdjointIBSolver: Laplacian(CrossProduct(q0, q)) - Curl(CrossProduct(q, omega0)); the
+                // right-hand-side and omega* buffers are free until later in the sub-step
+                launch_flux_cross(g, d_base_q, B.q, B.a, st);
+                coarsify_field(g, B.a, st);
+                launch_laplacian<T>(g, B.a, B.ws, st);
+                launch_nonlinear<T>(g, B.q, d_base_w, B.U, B.V, B.C, Nk, 1, S, F, st);
+                launch_sub(S, B.ws, Nk, Nk, st);
+                launches += 3 + g.L;
+            } else {
                 launch_nonlinear<T>(g, B.q, B.w, B.U, B.V, B.C, Nk, 1, S, F, st);
+            }
             if (nmode == 2) {
                 launch_sfd(S, B.w, d_what, d_rprev, Nk, sfd_chi, sfd_Delta, an, bn, prm.dt, !sfd_rhs_saved, st);
                 sfd_rhs_saved = true;
@@ -1204,6 +1214,14 @@ int ibg_set_linearized(ibg_context* c, int period, const double* omega0, const d
     c->nmode = 1;
     c->period = period;
     return c->cuda_check("ibg_set_linearized");
+}
+
+int ibg_set_adjoint(ibg_context* c, const double* omega0, const double* q0) {
+    if (!c || !omega0 || !q0) return IBG_ERR_ARG;
+    int s = ibg_set_linearized(c, 1, omega0, q0);
+    if (s) return s;
+    c->nmode = 3;
+    return IBG_OK;
 }
 
 int ibg_set_sfd(ibg_context* c, double chi, double Delta, const double* omega_hat) {

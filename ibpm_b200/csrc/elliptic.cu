@@ -1002,6 +1002,13 @@ int EllipticPlan<T>::solve(const SolveCall<T>& c, cudaStream_t st) const {
     return cudaPeekAtLastError() == cudaSuccess ? IBG_OK : IBG_ERR_CUDA;
 }
 
+// Scalar::coarsify (src/Scalar.cc:46-64) of a field in place, finest level first
+void coarsify_field(const GridDev& g, double* f, cudaStream_t st) {
+    const int novl = (g.nx / 2 - 1) * (g.ny / 2 - 1);
+    for (int lev = 1; lev < g.L; ++lev)
+        k_coarsify<double><<<dim3((unsigned)((novl + 255) / 256), 1), 256, 0, st>>>(g, lev, f, f, 0);
+}
+
 template <typename T>
 int EllipticPlan<T>::launches() const {
     const int L = grid->L;

@@ -140,6 +140,8 @@ struct CosTables {
 };
 
 bool fft_supported(int m);
+// Scalar::coarsify of a field in place (every level, finest first)
+void coarsify_field(const GridDev& g, double* f, cudaStream_t st);
 // factor m into the radices the shared-memory FFT uses (no device allocation)
 void fft_describe(int m, FftDesc& d);
 

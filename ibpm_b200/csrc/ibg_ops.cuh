@@ -52,6 +52,8 @@ void launch_smear_bf_unit(const GridDev& g, int ncomp, int col0, int batch, cons
 void launch_nonlinear_lin(const GridDev& g, const double* q, const double* w, const double* qb, const double* wb,
                           int period, const int* ts0, const int* count, double* U, double* V, double* C, double* N,
                           cudaStream_t st);
+void launch_flux_cross(const GridDev& g, const double* q1, const double* q2, double* out, cudaStream_t st);
+void launch_sub(size_t n, const double* a, const double* b, double* out, cudaStream_t st);
 void launch_sfd(size_t n, const double* w, double* what, double* rprev, double* N, double chi, double Delta,
                 double an, double bn, double dt, bool first, cudaStream_t st);
 

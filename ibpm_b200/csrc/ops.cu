@@ -140,6 +140,27 @@ __global__ void k_node_vel_lin(GridDev g, const double* __restrict__ q, const do
     V[tid] = dv ? vb * wv + v * w0v : 0.0;
 }
 
+// CrossProduct(Flux q1, Flux q2) = u1 v2 - u2 v1 at the nodes (src/VectorOperations.cc:465-486);
+// the coarse overlap interior, undefined here as in the reference, is then filled by coarsify
+__global__ void k_flux_cross(GridDev g, const double* __restrict__ q1, const double* __restrict__ q2,
+                             double* __restrict__ out) {
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (size_t)g.L * g.N1) return;
+    const int lev = (int)(tid / g.N1);
+    const int r = (int)(tid % g.N1);
+    const int i = r / g.NJ + 1, j = r % g.NJ + 1;
+    double u1, v1, u2, v2;
+    bool du, dv;
+    node_uv(g, q1 + (size_t)lev * g.F1, lev, i, j, u1, v1, du, dv);
+    node_uv(g, q2 + (size_t)lev * g.F1, lev, i, j, u2, v2, du, dv);
+    out[tid] = (du && dv) ? u1 * v2 - u2 * v1 : 0.0;
+}
+
+__global__ void k_sub(size_t n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) out[t] = a[t] - b[t];
+}
+
 // SFDSolver (src/IBSolver.cc:238-283): N -= chi (omega - omega_hat), then the filtered state
 // advances from the vorticity at the start of the sub-step:
 // rhs = (omega - omega_hat) / Delta, omega_hat += dt (an rhs + bn rhs_prev), rhs_prev = rhs
@@ -498,6 +519,15 @@ void launch_nonlinear_lin(const GridDev& g, const double* q, const double* w, co
     for (int lev = 0; lev < g.L; ++lev)
         k_cross_flux<double><<<dim3(nblk(g.F1, 256), 1), 256, 0, st>>>(g, lev, U, V, C, S, F);
     k_curl_flux<double><<<dim3(nblk(S, 256), 1), 256, 0, st>>>(g, C, N, S, F);
+}
+
+void launch_flux_cross(const GridDev& g, const double* q1, const double* q2, double* out, cudaStream_t st) {
+    const size_t S = (size_t)g.L * g.N1;
+    k_flux_cross<<<nblk(S, 256), 256, 0, st>>>(g, q1, q2, out);
+}
+
+void launch_sub(size_t n, const double* a, const double* b, double* out, cudaStream_t st) {
+    k_sub<<<nblk(n, 256), 256, 0, st>>>(n, a, b, out);
 }
 
 void launch_sfd(size_t n, const double* w, double* what, double* rprev, double* N, double chi, double Delta,

@@ -147,6 +147,10 @@ IBG_API int ibg_snapshot_save(ibg_context* ctx, const char* filename);
  * ibg_get_sfd_state reads omega_hat (SFDSolver::saveFilteredState). */
 IBG_API int ibg_set_linearized(ibg_context* ctx, int period, const double* omega0, const double* q0);
 IBG_API int ibg_set_sfd(ibg_context* ctx, double chi, double Delta, const double* omega_hat);
+/* AdjointIBSolver (src/IBSolver.cc:218-222): N(x) = Laplacian(CrossProduct(q0, q))
+ * - Curl(CrossProduct(q, omega0)) about one base state (u_mag = 0, as for the
+ * linear models); ibg_set_linearized(ctx, 0, NULL, NULL) restores the nonlinear N(x). */
+IBG_API int ibg_set_adjoint(ibg_context* ctx, const double* omega0, const double* q0);
 IBG_API int ibg_get_sfd_state(ibg_context* ctx, double* omega_hat);
 
 /* IBSolver::advance (src/IBSolver.cc:142-149), nsteps times. */

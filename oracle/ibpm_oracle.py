@@ -489,6 +489,20 @@ def nonlinear(g: Grid, q: np.ndarray, w: np.ndarray) -> np.ndarray:
     return curl_flux(g, cross_product(g, q, w))
 
 
+def cross_product_flux(g: Grid, q1: np.ndarray, q2: np.ndarray) -> np.ndarray:
+    """CrossProduct(Flux, Flux) = u1 v2 - u2 v1 at the nodes, then coarsified over the
+    overlap regions (src/VectorOperations.cc:465-486)."""
+    f = flux_to_xvel(g, q1) * flux_to_yvel(g, q2)
+    f = f - flux_to_xvel(g, q2) * flux_to_yvel(g, q1)
+    return coarsify(g, f)
+
+
+def adjoint(g: Grid, q: np.ndarray, w: np.ndarray, q0: np.ndarray, w0: np.ndarray) -> np.ndarray:
+    """AdjointIBSolver::N = Laplacian(CrossProduct(q0, q)) - Curl(CrossProduct(q, omega0))
+    (src/IBSolver.cc:218-222)."""
+    return laplacian(g, cross_product_flux(g, q0, q)) - nonlinear(g, q, w0)
+
+
 def linearized(g: Grid, q: np.ndarray, w: np.ndarray, q0: np.ndarray, w0: np.ndarray) -> np.ndarray:
     """LinearizedIBSolver::N = Curl(q0 x omega + q x omega0) (src/IBSolver.cc:211-216); the periodic
     form uses the base state of phase timestep % period (src/IBSolver.cc:224-232)."""
@@ -909,9 +923,10 @@ class IBSolver:
     (src/IBSolver.cc:238-283; omega_hat is the filtered vorticity it starts from)."""
 
     def __init__(self, model: Model, dt: float, scheme: str = "rk3", tol: float = 1e-7, max_iter: int = 3000,
-                 base=None, sfd=None):
+                 base=None, sfd=None, adjoint=False):
         self.model, self.dt, self.coef = model, dt, SCHEMES[scheme]
         self.base = base
+        self.adjoint = adjoint
         self.sfd = None
         if sfd is not None:
             chi, Delta, what = sfd
@@ -932,7 +947,7 @@ class IBSolver:
         for k, (an, bn, cn) in enumerate(self.coef):
             if self.base is not None:
                 w0, q0 = self.base[x.timestep % len(self.base)]
-                n = linearized(g, x.q, x.omega, q0, w0)
+                n = (adjoint if self.adjoint else linearized)(g, x.q, x.omega, q0, w0)
             else:
                 n = nonlinear(g, x.q, x.omega)
             if self.sfd is not None:

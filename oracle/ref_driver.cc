@@ -13,7 +13,7 @@
 //                   -geom FILE -Re R -dt DT -scheme rk3|euler|ab2|rk3b
 //                   -nsteps K [-tol T] [-alpha DEG] [-ic restart.bin]
 //                   [-out PREFIX] [-dump_every K] [-warmup W] [-cholesky_cache BASENAME]
-//                   [-model nonlinear|linear|linearperiodic|sfd] [-baseflow FILE]
+//                   [-model nonlinear|linear|adjoint|linearperiodic|sfd] [-baseflow FILE]
 //                   [-pbase PREFIX -period P] [-chi X -Delta X]
 // -model selects the solver class as the CLI does (src/ibpm.cc:184-229): the
 // linear models get a NavierStokesModel without base flow and the base state(s)
@@ -81,7 +81,7 @@ int main(int argc, char* argv[]) {
     double pi = 4. * atan(1.);
     double alpha = alphaDeg * pi / 180.;
     BaseFlow q_potential(grid, 1.0, alpha);
-    const bool linear = modelName == "linear" || modelName == "linearperiodic";
+    const bool linear = modelName == "linear" || modelName == "linearperiodic" || modelName == "adjoint";
     NavierStokesModel* mp = linear ? new NavierStokesModel(grid, geom, Re) : new NavierStokesModel(grid, geom, Re, q_potential);
     NavierStokesModel& model = *mp;
     IBSolver* sp = NULL;
@@ -92,6 +92,10 @@ int main(int argc, char* argv[]) {
         State x00(grid, geom.getNumPoints());
         if (!x00.load(baseFile)) { std::cerr << "baseflow load failed\n"; return 5; }
         sp = new LinearizedIBSolver(grid, model, dt, st, tol, x00);
+    } else if (modelName == "adjoint") {
+        State x00(grid, geom.getNumPoints());
+        if (!x00.load(baseFile)) { std::cerr << "baseflow load failed\n"; return 5; }
+        sp = new AdjointIBSolver(grid, model, dt, st, tol, x00);
     } else if (modelName == "linearperiodic") {
         std::vector<State> x0;
         for (int k = 0; k < period; ++k) {

@@ -84,6 +84,7 @@ VARIANTS = [
     # name, model, Re, dt, nsteps, scheme, extra
     ("var_linear_l2_rk3", "linear", 150.0, 0.02, 6, "rk3", {}),
     ("var_linearperiodic_l2_rk3", "linearperiodic", 150.0, 0.02, 6, "rk3", {"period": 2}),
+    ("var_adjoint_l2_rk3", "adjoint", 150.0, 0.02, 6, "rk3", {}),
     ("var_sfd_l2_rk3", "sfd", 150.0, 0.02, 6, "rk3", {"chi": 0.5, "Delta": 2.0}),
     ("var_sfd_l2_ab2", "sfd", 150.0, 0.02, 6, "ab2", {"chi": 0.5, "Delta": 2.0}),
 ]
@@ -114,13 +115,13 @@ def run_variant(case):
         bases = [O.load_restart(os.path.join(td, "base_%05d.bin" % k)) for k in (3, 4)]
         args = common + ["-nsteps", str(nsteps), "-model", model, "-out", os.path.join(td, "run")]
         rec = {"model": model}
-        if model in ("linear", "linearperiodic"):
+        if model in ("linear", "linearperiodic", "adjoint"):
             # the perturbation starts as the noise alone (no base flow in a linear model)
             period = extra.get("period", 1)
             for k in range(period):
                 O.save_restart(os.path.join(td, "pb_%d.bin" % k),
                                O.State(g, npts, omega=bases[k]["omega"], q=bases[k]["q"]), g)
-            if model == "linear":
+            if model in ("linear", "adjoint"):
                 args += ["-baseflow", os.path.join(td, "pb_0.bin")]
             else:
                 args += ["-pbase", os.path.join(td, "pb"), "-period", str(period)]

@@ -64,7 +64,7 @@ def oracle_from_variant(d):
     geo = geometry.parse(str(d["geom"]))
     bodies = [O.Body(np.array(b.points, dtype=float)) for b in geo.bodies]
     model_name = str(d["model"])
-    linear = model_name in ("linear", "linearperiodic")
+    linear = model_name in ("linear", "linearperiodic", "adjoint")
     # the linear models run without the uniform base flow, as the reference CLI builds them
     model = O.Model(g, bodies, float(d["Re"]), u_mag=0.0 if linear else 1.0)
     base = sfd = None
@@ -72,6 +72,7 @@ def oracle_from_variant(d):
         base = [(np.array(d["base_omega"][k]), np.array(d["base_q"][k])) for k in range(int(d["period"]))]
     else:
         sfd = (float(d["chi"]), float(d["Delta"]), g.scalar())
-    solver = O.IBSolver(model, float(d["dt"]), str(d["scheme"]), float(d["tol"]), base=base, sfd=sfd)
+    adj = model_name == "adjoint"
+    solver = O.IBSolver(model, float(d["dt"]), str(d["scheme"]), float(d["tol"]), base=base, sfd=sfd, adjoint=adj)
     x = O.State(g, model.npts, omega=np.array(d["omega0"], dtype=float))
     return g, model, solver, x

@@ -1,5 +1,5 @@
 """The other N(x) forms of the reference on the GPU (src/IBSolver.cc:211-283):
-LinearizedIBSolver, LinearizedPeriodicIBSolver and SFDSolver, against fixtures
+LinearizedIBSolver, LinearizedPeriodicIBSolver, AdjointIBSolver and SFDSolver, against fixtures
 the reference itself produced (tests/golden/var_*.npz, made by
 tests/golden/make_golden.py), to the FP64 parity bar."""
 import numpy as np
@@ -14,11 +14,13 @@ def _solver(d):
                    float(d["yoffset"]))
     geo = ib.geometry.parse(str(d["geom"]))
     model_name = str(d["model"])
-    linear = model_name in ("linear", "linearperiodic")
+    linear = model_name in ("linear", "linearperiodic", "adjoint")
     # the linear models run without the uniform base flow, as the reference CLI builds them
     model = ib.NavierStokesModel(grid, geo, float(d["Re"]), u_mag=0.0 if linear else 1.0)
     s = ib.NonlinearIBSolver(grid, model, float(d["dt"]), str(d["scheme"]), float(d["tol"]))
-    if linear:
+    if model_name == "adjoint":
+        s.set_adjoint(d["base_omega"][0], d["base_q"][0])
+    elif linear:
         P = int(d["period"])
         s.set_linearized([d["base_omega"][k] for k in range(P)], [d["base_q"][k] for k in range(P)])
     else:
