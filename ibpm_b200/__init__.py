@@ -186,6 +186,22 @@ class NonlinearIBSolver:
         check(lib().ibg_get_state(self._h, _ptr(om), _ptr(q), _ptr(f), ctypes.byref(ts), ctypes.byref(t)), self._h)
         x.omega, x.q, x.f, x.timestep, x.time = om, q, f, ts.value, t.value
 
+    # -- inner products and energy (src/VectorOperations.cc:222-412) ---------
+    def inner_product(self, a, b, fine_only: bool = False) -> float:
+        """InnerProduct (or FineGridInnerProduct) of two Scalars or two Fluxes."""
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        kind = (2 if a.shape == self.grid.flux().shape else 0) + (1 if fine_only else 0)
+        out = ctypes.c_double()
+        check(lib().ibg_inner_product(self._h, kind, _ptr(a), _ptr(b), ctypes.byref(out)), self._h)
+        return out.value
+
+    def energy(self) -> float:
+        """0.5 InnerProduct(q, q) of the device state (OutputEnergy, src/OutputEnergy.cc:29-33)."""
+        out = ctypes.c_double()
+        check(lib().ibg_energy(self._h, ctypes.byref(out)), self._h)
+        return out.value
+
     # -- the other N(x) forms (src/IBSolver.cc:211-283) ----------------------
     def set_linearized(self, omega0, q0=None):
         """LinearizedIBSolver (one base state) or LinearizedPeriodicIBSolver (a list of

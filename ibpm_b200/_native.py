@@ -67,6 +67,8 @@ SIGNATURES = {
     "ibg_set_linearized": (_I, [_VP, _I, _VP, _VP]),
     "ibg_set_sfd": (_I, [_VP, _D, _D, _VP]),
     "ibg_set_adjoint": (_I, [_VP, _VP, _VP]),
+    "ibg_inner_product": (_I, [_VP, _I, _VP, _VP, _VP]),
+    "ibg_energy": (_I, [_VP, _VP]),
     "ibg_get_sfd_state": (_I, [_VP, _VP]),
     "ibg_ensemble_set_shapes": (_I, [_VP, _I, _I, _I]),
     "ibg_save_restart": (_I, [_VP, ctypes.c_char_p]),

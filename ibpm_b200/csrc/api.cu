@@ -183,6 +183,19 @@ struct ibg_context {
     double* d_rprev = nullptr;   // SFD previous filter right-hand side
     double sfd_chi = 0.0, sfd_Delta = 1.0;
     bool sfd_rhs_saved = false;
+    // inner-product weights (src/VectorOperations.cc:222-412): [0] Scalar, [1] fine Scalar,
+    // [2] Flux, [3] fine Flux; built on first use
+    double* d_ipw[4] = {nullptr, nullptr, nullptr, nullptr};
+    double* d_ip_tmp = nullptr;  // two operands (F each) and the partial sums
+    int build_ip_weights();
+    void release_ip() {
+        for (double*& p : d_ipw) {
+            if (p) cudaFree(p);
+            p = nullptr;
+        }
+        if (d_ip_tmp) cudaFree(d_ip_tmp);
+        d_ip_tmp = nullptr;
+    }
     void release_variant() {
         double* p[] = {d_base_w, d_base_q, d_what, d_rprev};
         for (double* x : p)
@@ -301,6 +314,7 @@ struct ibg_context {
     }
     void release() {
         release_snapshot();
+        release_ip();
         release_variant();
         if (d_ts0) cudaFree(d_ts0);
         d_ts0 = nullptr;
@@ -1200,6 +1214,130 @@ int ibg_snapshot_save(ibg_context* c, const char* filename) {
 // ---------------------------------------------------------------------------
 // the other N(x) forms
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// inner products and energy (src/VectorOperations.cc:222-412, src/OutputEnergy.cc:29-33)
+// ---------------------------------------------------------------------------
+namespace ibg {
+constexpr int kIpBlocks = 256;
+// partial[b] = sum over this block's grid-stride share of w a b (fixed order)
+__global__ void k_wdot_partial(size_t n, const double* __restrict__ w, const double* __restrict__ a,
+                               const double* __restrict__ b, double* __restrict__ partial) {
+    __shared__ double red[32];
+    double s = 0.0;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
+        s += w[t] * a[t] * b[t];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += red[k];
+        partial[blockIdx.x] = t;
+    }
+}
+__global__ void k_sum_partials(int n, const double* __restrict__ partial, double scale, double* __restrict__ out) {
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int k = 0; k < n; ++k) t += partial[k];
+        *out = t * scale;
+    }
+}
+}  // namespace ibg
+
+int ibg_context::build_ip_weights() {
+    if (d_ipw[0]) return IBG_OK;
+    const int nx = g.nx, ny = g.ny, nx2 = g.nxe, ny2 = g.nye, L = g.L;
+    const int NI = g.NI, NJ = g.NJ, nXf = g.nXf;
+    std::vector<double> ws(S, 0.0), wsf(S, 0.0), wf(F, 0.0), wff(F, 0.0);
+    auto sw = [&](std::vector<double>& w, int lev, int i, int j, double v) {
+        w[(size_t)lev * g.N1 + (size_t)(i - 1) * NJ + (j - 1)] += v;
+    };
+    for (int i = 1; i <= NI; ++i)
+        for (int j = 1; j <= NJ; ++j) {
+            sw(ws, 0, i, j, 1.0);
+            sw(wsf, 0, i, j, 1.0);
+        }
+    for (int lev = 1; lev < L; ++lev) {
+        const int il = nx2, ir = nx / 2 + nx2, jb = ny2, jt = ny / 2 + ny2;
+        sw(ws, lev, il, jb, 15. / 16); sw(ws, lev, ir, jb, 15. / 16); sw(ws, lev, il, jt, 15. / 16); sw(ws, lev, ir, jt, 15. / 16);
+        for (int j = jb + 1; j < jt; ++j) { sw(ws, lev, il, j, 0.75); sw(ws, lev, ir, j, 0.75); }
+        for (int i = il + 1; i < ir; ++i) { sw(ws, lev, i, jb, 0.75); sw(ws, lev, i, jt, 0.75); }
+        for (int i = 1; i < il; ++i) for (int j = 1; j < ny; ++j) sw(ws, lev, i, j, 1.0);
+        for (int i = ir + 1; i < nx; ++i) for (int j = 1; j < ny; ++j) sw(ws, lev, i, j, 1.0);
+        for (int i = il; i <= ir; ++i) {
+            for (int j = 1; j < jb; ++j) sw(ws, lev, i, j, 1.0);
+            for (int j = jt + 1; j < ny; ++j) sw(ws, lev, i, j, 1.0);
+        }
+    }
+    for (int lev = 0; lev < L; ++lev) {
+        const double d = lev_dx(g, lev), d2 = d * d;
+        for (size_t k = 0; k < (size_t)g.N1; ++k) {
+            ws[(size_t)lev * g.N1 + k] *= d2;
+            wsf[(size_t)lev * g.N1 + k] *= d2;
+        }
+    }
+    auto xw = [&](std::vector<double>& w, int lev, int i, int j, double v) { w[(size_t)lev * g.F1 + (size_t)i * ny + j] += v; };
+    auto yw = [&](std::vector<double>& w, int lev, int i, int j, double v) {
+        w[(size_t)lev * g.F1 + nXf + (size_t)i * (ny + 1) + j] += v;
+    };
+    for (int j = 0; j < ny; ++j) for (int i = 1; i < nx; ++i) { xw(wf, 0, i, j, 1.0); xw(wff, 0, i, j, 1.0); }
+    for (int i = 0; i < nx; ++i) for (int j = 1; j < ny; ++j) { yw(wf, 0, i, j, 1.0); yw(wff, 0, i, j, 1.0); }
+    for (int lev = 1; lev < L; ++lev) {
+        const int il = nx2, ir = nx / 2 + nx2, jb = ny2, jt = ny / 2 + ny2;
+        for (int j = jb; j < jt; ++j) { xw(wf, lev, il, j, 0.75); xw(wf, lev, ir, j, 0.75); }
+        for (int j = 0; j < ny; ++j) {
+            for (int i = 1; i < il; ++i) xw(wf, lev, i, j, 1.0);
+            for (int i = ir + 1; i < nx; ++i) xw(wf, lev, i, j, 1.0);
+        }
+        for (int i = il; i <= ir; ++i) {
+            for (int j = 0; j < jb; ++j) xw(wf, lev, i, j, 1.0);
+            for (int j = jt; j < ny; ++j) xw(wf, lev, i, j, 1.0);
+        }
+        for (int i = il; i < ir; ++i) { yw(wf, lev, i, jb, 0.75); yw(wf, lev, i, jt, 0.75); }
+        for (int i = 0; i < nx; ++i) {
+            for (int j = 1; j < jb; ++j) yw(wf, lev, i, j, 1.0);
+            for (int j = jt + 1; j < ny; ++j) yw(wf, lev, i, j, 1.0);
+        }
+        for (int j = jb; j <= jt; ++j) {
+            for (int i = 0; i < il; ++i) yw(wf, lev, i, j, 1.0);
+            for (int i = ir; i < nx; ++i) yw(wf, lev, i, j, 1.0);
+        }
+    }
+    const std::vector<double>* src[4] = {&ws, &wsf, &wf, &wff};
+    for (int k = 0; k < 4; ++k) {
+        if (alloc(&d_ipw[k], src[k]->size(), false)) return IBG_ERR_CUDA;
+        cudaMemcpy(d_ipw[k], src[k]->data(), sizeof(double) * src[k]->size(), cudaMemcpyHostToDevice);
+    }
+    if (alloc(&d_ip_tmp, 2 * (size_t)F + kIpBlocks + 1, false)) return IBG_ERR_CUDA;
+    return cuda_check("inner-product weights");
+}
+
+static int device_ip(ibg_context* c, int kind, const double* da, const double* db, double scale, double* out) {
+    const size_t n = kind < 2 ? c->S : c->F;
+    double* partial = c->d_ip_tmp + 2 * (size_t)c->F;
+    ibg::k_wdot_partial<<<ibg::kIpBlocks, 256, 0, c->st>>>(n, c->d_ipw[kind], da, db, partial);
+    ibg::k_sum_partials<<<1, 32, 0, c->st>>>(ibg::kIpBlocks, partial, scale, partial + ibg::kIpBlocks);
+    cudaMemcpyAsync(out, partial + ibg::kIpBlocks, sizeof(double), cudaMemcpyDeviceToHost, c->st);
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->cuda_check("inner product");
+    return c->cuda_check("inner product");
+}
+
+int ibg_inner_product(ibg_context* c, int kind, const double* a, const double* b, double* ip) {
+    if (!c || kind < 0 || kind > 3 || !a || !b || !ip) return IBG_ERR_ARG;
+    if (c->build_ip_weights()) return IBG_ERR_CUDA;
+    const size_t n = kind < 2 ? c->S : c->F;
+    cudaMemcpyAsync(c->d_ip_tmp, a, sizeof(double) * n, cudaMemcpyHostToDevice, c->st);
+    cudaMemcpyAsync(c->d_ip_tmp + c->F, b, sizeof(double) * n, cudaMemcpyHostToDevice, c->st);
+    return device_ip(c, kind, c->d_ip_tmp, c->d_ip_tmp + c->F, 1.0, ip);
+}
+
+int ibg_energy(ibg_context* c, double* energy) {
+    if (!c || !energy) return IBG_ERR_ARG;
+    if (c->build_ip_weights()) return IBG_ERR_CUDA;
+    c->to64();
+    return device_ip(c, 2, c->b64.q, c->b64.q, 0.5, energy);
+}
+
 int ibg_set_linearized(ibg_context* c, int period, const double* omega0, const double* q0) {
     if (!c || period < 0 || (period > 0 && (!omega0 || !q0))) return IBG_ERR_ARG;
     if (c->fp32) return c->fail(IBG_ERR_UNSUPPORTED, "ibg_set_linearized: the linearized forms run in FP64 only");

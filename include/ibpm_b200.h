@@ -133,6 +133,16 @@ IBG_API int ibg_load_restart(ibg_context* ctx, const char* filename);
 IBG_API int ibg_snapshot(ibg_context* ctx);
 IBG_API int ibg_snapshot_save(ibg_context* ctx, const char* filename);
 
+/* --- inner products and energy ---------------------------------------------------
+ * ibg_inner_product: kind 0 InnerProduct(Scalar, Scalar), 1 FineGridInnerProduct
+ * (Scalar), 2 InnerProduct(Flux, Flux), 3 FineGridInnerProduct(Flux)
+ * (src/VectorOperations.cc:222-412), with the reference's multi-domain weights, of
+ * two host arrays in the Scalar or Flux layout, computed on the device.
+ * ibg_energy: 0.5 InnerProduct(q, q) of the current state, what OutputEnergy
+ * writes (src/OutputEnergy.cc:29-33), without moving q to the host. */
+IBG_API int ibg_inner_product(ibg_context* ctx, int kind, const double* a, const double* b, double* ip);
+IBG_API int ibg_energy(ibg_context* ctx, double* energy);
+
 /* --- the other N(x) forms (src/IBSolver.cc:211-283), FP64 ------------------------
  * ibg_set_linearized: LinearizedIBSolver (period 1) or LinearizedPeriodicIBSolver
  * (period P): N(x) = Curl(q0 x omega + q x omega0) with the base state of phase

@@ -980,6 +980,72 @@ class IBSolver:
 
 
 # ----------------------------------------------------------------------------
+# Inner products with multi-domain weights (src/VectorOperations.cc:222-412)
+# ----------------------------------------------------------------------------
+
+
+def scalar_ip_weights(g: Grid, fine_only: bool = False) -> np.ndarray:
+    """Weight of every Scalar node in InnerProduct(Scalar, Scalar): dx^2 of its level,
+    times 15/16 at the corners and 3/4 on the edges of the finer domain's footprint,
+    0 inside it (src/VectorOperations.cc:222-310); FineGridInnerProduct keeps level 0."""
+    nx, ny, nx2, ny2 = g.nx, g.ny, g.nxext, g.nyext
+    w = np.zeros((g.ngrid, nx + 1, ny + 1))
+    w[0, 1:nx, 1:ny] = 1.0
+    if not fine_only:
+        for lev in range(1, g.ngrid):
+            W = w[lev]
+            for (i, j) in ((nx2, ny2), (nx // 2 + nx2, ny2), (nx2, ny // 2 + ny2), (nx // 2 + nx2, ny // 2 + ny2)):
+                W[i, j] += 15.0 / 16
+            for j in range(ny2 + 1, ny // 2 + ny2):
+                W[nx2, j] += 0.75
+                W[nx // 2 + nx2, j] += 0.75
+            for i in range(nx2 + 1, nx // 2 + nx2):
+                W[i, ny2] += 0.75
+                W[i, ny // 2 + ny2] += 0.75
+            W[1:nx2, 1:ny] += 1.0
+            W[nx // 2 + nx2 + 1:nx, 1:ny] += 1.0
+            W[nx2:nx // 2 + nx2 + 1, 1:ny2] += 1.0
+            W[nx2:nx // 2 + nx2 + 1, ny // 2 + ny2 + 1:ny] += 1.0
+    for lev in range(g.ngrid):
+        w[lev] *= (g.dx * 2 ** lev) ** 2
+    return w[:, 1:nx, 1:ny]
+
+
+def flux_ip_weights(g: Grid, fine_only: bool = False) -> np.ndarray:
+    """Weight of every flux in InnerProduct(Flux, Flux) (src/VectorOperations.cc:312-412)."""
+    nx, ny, nx2, ny2 = g.nx, g.ny, g.nxext, g.nyext
+    nXf = (nx + 1) * ny
+    w = np.zeros((g.ngrid, nXf + nx * (ny + 1)))
+    X = lambda lev: w[lev, :nXf].reshape(nx + 1, ny)
+    Y = lambda lev: w[lev, nXf:].reshape(nx, ny + 1)
+    X(0)[1:nx, :] = 1.0
+    Y(0)[:, 1:ny] = 1.0
+    if not fine_only:
+        for lev in range(1, g.ngrid):
+            x, y = X(lev), Y(lev)
+            x[nx2, ny2:ny // 2 + ny2] += 0.75
+            x[nx // 2 + nx2, ny2:ny // 2 + ny2] += 0.75
+            x[1:nx2, :] += 1.0
+            x[nx // 2 + nx2 + 1:nx, :] += 1.0
+            x[nx2:nx // 2 + nx2 + 1, 0:ny2] += 1.0
+            x[nx2:nx // 2 + nx2 + 1, ny // 2 + ny2:ny] += 1.0
+            y[nx2:nx // 2 + nx2, ny2] += 0.75
+            y[nx2:nx // 2 + nx2, ny // 2 + ny2] += 0.75
+            y[:, 1:ny2] += 1.0
+            y[:, ny // 2 + ny2 + 1:ny] += 1.0
+            y[0:nx2, ny2:ny // 2 + ny2 + 1] += 1.0
+            y[nx // 2 + nx2:nx, ny2:ny // 2 + ny2 + 1] += 1.0
+    return w
+
+
+def inner_product(g: Grid, kind: int, a: np.ndarray, b: np.ndarray) -> float:
+    """kind 0 InnerProduct(Scalar), 1 FineGridInnerProduct(Scalar), 2 InnerProduct(Flux),
+    3 FineGridInnerProduct(Flux) (src/VectorOperations.cc:222-412)."""
+    w = scalar_ip_weights(g, kind == 1) if kind < 2 else flux_ip_weights(g, kind == 3)
+    return float(np.sum(w * np.asarray(a) * np.asarray(b)))
+
+
+# ----------------------------------------------------------------------------
 # Restart file (src/State.cc:65-223)
 # ----------------------------------------------------------------------------
 

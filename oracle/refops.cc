@@ -234,4 +234,17 @@ void refops_apply_m(const int* gi, const double* gd, int npts, const double* xy,
     fromBV(yy, y);
 }
 
+// kind 0 InnerProduct(Scalar, Scalar), 1 FineGridInnerProduct(Scalar, Scalar),
+// 2 InnerProduct(Flux, Flux), 3 FineGridInnerProduct(Flux, Flux) (src/VectorOperations.cc:222-412)
+void refops_inner_product(const int* gi, const double* gd, int kind, const double* a, const double* b, double* out) {
+    Grid g = mkgrid(gi, gd);
+    if (kind < 2) {
+        Scalar x(g), y(g); toScalar(a, x); toScalar(b, y);
+        *out = kind == 0 ? InnerProduct(x, y) : FineGridInnerProduct(x, y);
+    } else {
+        Flux x(g), y(g); toFlux(a, x); toFlux(b, y);
+        *out = kind == 2 ? InnerProduct(x, y) : FineGridInnerProduct(x, y);
+    }
+}
+
 }  // extern "C"

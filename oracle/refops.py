@@ -159,3 +159,11 @@ def apply_m(g, xy, Re, beta, f):
     lib().refops_apply_m(gi, gd, ctypes.c_int(xy.shape[0]), xy.ctypes.data_as(_P), ctypes.c_double(Re),
                          ctypes.c_double(beta), fa.ctypes.data_as(_P), out.ctypes.data_as(_P))
     return out
+
+
+def inner_product(g, kind, a, b):
+    """kind 0 InnerProduct(Scalar), 1 FineGridInnerProduct(Scalar), 2 InnerProduct(Flux), 3 FineGrid(Flux)."""
+    gi, gd = _gi(g)
+    out = np.zeros(1)
+    lib().refops_inner_product(gi, gd, ctypes.c_int(kind), _d(a), _d(b), out.ctypes.data_as(_P))
+    return float(out[0])
