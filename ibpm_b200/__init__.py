@@ -129,8 +129,13 @@ class NonlinearIBSolver:
             bodies[k].xy = xy.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
             bodies[k].xcenter, bodies[k].ycenter = b.center
             bodies[k].motion = b.motion
-            for j in range(6):
+            for j in range(12):
                 bodies[k].params[j] = b.params[j] if j < len(b.params) else 0.0
+            if b.table is not None and len(b.table):
+                tab = np.ascontiguousarray(np.asarray(b.table, dtype=np.float64).reshape(-1, 7))
+                self._keep.append(tab)
+                bodies[k].table_rows = tab.shape[0]
+                bodies[k].table = tab.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
         p = ibg_params(model.Re, dt, SCHEMES[scheme], tol, cg_max_iter, model.u_mag, model.alpha,
                        PRECISIONS[precision], device, PRECONDS[precond], pc_refresh, int(cg_graph),
                        pc_fallback_iter)
@@ -249,6 +254,15 @@ class NonlinearIBSolver:
 
     def update_operators(self, time: float):
         check(lib().ibg_update_operators(self._h, float(time)), self._h)
+
+    def boundary(self):
+        """Geometry::getPoints / getVelocities at the last time the bodies were
+        moved, as (npoints, 2) arrays of positions and velocities."""
+        n = self.model.geom.num_points
+        pts = np.empty(2 * n)
+        vel = np.empty(2 * n)
+        check(lib().ibg_get_boundary(self._h, _ptr(pts), _ptr(vel)), self._h)
+        return pts.reshape(2, n).T.copy(), vel.reshape(2, n).T.copy()
 
     def refresh_state(self, x: State):
         """model->refreshState(x): q from omega on the device."""

@@ -21,7 +21,8 @@ class ibg_grid(ctypes.Structure):
 
 class ibg_body(ctypes.Structure):
     _fields_ = [("npoints", ctypes.c_int), ("xy", c_double_p), ("xcenter", ctypes.c_double),
-                ("ycenter", ctypes.c_double), ("motion", ctypes.c_int), ("params", ctypes.c_double * 6)]
+                ("ycenter", ctypes.c_double), ("motion", ctypes.c_int), ("params", ctypes.c_double * 12),
+                ("table_rows", ctypes.c_int), ("table", c_double_p)]
 
 
 class ibg_params(ctypes.Structure):
@@ -52,6 +53,7 @@ SIGNATURES = {
     "ibg_get_state": (_I, [_VP, _VP, _VP, _VP, ctypes.POINTER(_I), ctypes.POINTER(_D)]),
     "ibg_get_boundary_force": (_I, [_VP, _VP, ctypes.POINTER(_I), ctypes.POINTER(_D)]),
     "ibg_update_operators": (_I, [_VP, _D]),
+    "ibg_get_boundary": (_I, [_VP, _VP, _VP]),
     "ibg_refresh_state": (_I, [_VP]),
     "ibg_advance": (_I, [_VP, _I]),
     "ibg_get_net_force": (_I, [_VP, ctypes.POINTER(_D), ctypes.POINTER(_D)]),

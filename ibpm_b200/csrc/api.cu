@@ -137,6 +137,13 @@ struct ibg_context {
     double *d_ref = nullptr, *d_pts = nullptr, *d_vel = nullptr;
     int* d_body_of = nullptr;
     BodyDev* d_bodies = nullptr;
+    // motion history (stateful motions) and the bodies' motion tables
+    std::vector<double> h_mtab;
+    MotionState* d_mstate = nullptr;
+    MotionState* d_mstate_keep = nullptr;
+    double* d_mtab = nullptr;
+    int nbodies = 0;
+    bool stateful = false;
     RegSlots slots;
     double* d_b = nullptr;
     double* d_time = nullptr;
@@ -328,7 +335,7 @@ struct ibg_context {
         if (lb.len) cudaFree(lb.len);
         if (lb.closed) cudaFree(lb.closed);
         lb = LpcBodies{};
-        void* ptrs[] = {d_ref, d_pts, d_vel, d_body_of, d_bodies, slots.idx, slots.w, slots.n, d_b, d_time, f,
+        void* ptrs[] = {d_ref, d_pts, d_vel, d_body_of, d_bodies, d_mstate, d_mstate_keep, d_mtab, slots.idx, slots.w, slots.n, d_b, d_time, f,
                         flux0, rhsb, btmp, d_status, cg_r, cg_d, cg_q, cg_scal, cg_flags, d_hist, d_hist_count, cg_z, cg_zold};
         for (void* p : ptrs)
             if (p) cudaFree(p);
@@ -350,6 +357,8 @@ struct ibg_context {
         d_ref = d_pts = d_vel = nullptr;
         d_body_of = nullptr;
         d_bodies = nullptr;
+        d_mstate = d_mstate_keep = nullptr;
+        d_mtab = nullptr;
         slots = RegSlots{};
         d_b = d_time = f = flux0 = rhsb = btmp = nullptr;
         d_status = nullptr;
@@ -556,8 +565,13 @@ struct ibg_context {
         launches += solve_launches() + 1;
     }
 
+    // Geometry::moveBodies(time + toff) and Regularizer::update (src/NavierStokesModel.cc:93-99)
     void move_bodies(double toff) {
-        launch_kinematics(npts, d_ref, d_body_of, d_bodies, d_time, toff, d_pts, d_vel, st);
+        if (stateful) {
+            launch_motion_state(nbodies, d_bodies, d_time, toff, d_mstate, st);
+            launches += 1;
+        }
+        launch_kinematics(npts, d_ref, d_body_of, d_bodies, d_mstate, d_mtab, d_time, toff, d_pts, d_vel, st);
         launch_reg_update(g, npts, d_pts, d_vel, slots, d_b, u0, v0, st);
         launches += 2;
     }
@@ -801,6 +815,71 @@ const char* ibg_last_error(const ibg_context* ctx) {
     return ctx->err.c_str();
 }
 
+// RigidBody's motion (src/RigidBody.cc:349-493) as device parameters: the
+// geometry file's numbers, the PitchPlunge frequencies times 2 pi
+// (src/PitchPlunge.h:38-40), the Eldredge family's normalisers maxG computed
+// as their constructors do, and the rows of a motion file appended to tab.
+// Returns an error message, or nullptr.
+static const char* body_motion(const ibg_body& B, double twopi, BodyDev& d, std::vector<double>& tab) {
+    static const int nparams[] = {0, 3, 6, 3, 3, 4, 4, 6, 12, 6, 6, 0, 1};
+    if (B.motion < IBG_MOTION_NONE || B.motion > IBG_MOTION_FILE_PERIODIC) return "unsupported motion type";
+    const int np = nparams[B.motion];
+    for (int k = 0; k < np; ++k) {
+        if (!std::isfinite(B.params[k])) return "motion parameter is not finite";
+        d.p[k] = B.params[k];
+    }
+    // maxG = G((t2 + t3) / 2) of the ramp (a, t1, t2, t3, t4) (src/EldredgeManeuver.h:42-43);
+    // the pitch ramp of EldredgeCombined2 takes `a` in its t4 factor (src/EldredgeCombined2.h:59)
+    auto maxG = [](double a, double a4, double t1, double t2, double t3, double t4) {
+        const double tt = (t2 + t3) / 2.;
+        return log((cosh(a * (tt - t1)) * cosh(a4 * (tt - t4))) / (cosh(a * (tt - t2)) * cosh(a * (tt - t3))));
+    };
+    switch (B.motion) {
+        case IBG_MOTION_PITCHPLUNGE:
+            d.p[1] *= twopi;
+            d.p[4] *= twopi;
+            break;
+        case IBG_MOTION_SIGMOIDALSTEP:
+            if (d.p[1] == 0) return "sigmoidalstep: DUR must be non-zero";
+            break;
+        case IBG_MOTION_LAGSTEP1:
+        case IBG_MOTION_LAGSTEP2:
+            if (d.p[1] == 0 || d.p[2] == 0) return "lagstep: PW and TAU must be non-zero";
+            break;
+        case IBG_MOTION_ELDREDGE:
+        case IBG_MOTION_ELDREDGE1:
+        case IBG_MOTION_ELDREDGE2:
+            d.p[6] = maxG(d.p[1], d.p[1], d.p[2], d.p[3], d.p[4], d.p[5]);
+            if (!std::isfinite(d.p[6]) || d.p[6] == 0) return "eldredge: the ramp's maximum G is zero or not finite";
+            break;
+        case IBG_MOTION_ELDREDGECOMBINED2:
+            d.p[12] = maxG(d.p[1], d.p[1], d.p[2], d.p[3], d.p[4], d.p[5]);
+            d.p[13] = maxG(d.p[7], d.p[1], d.p[8], d.p[9], d.p[10], d.p[11]);
+            if (!std::isfinite(d.p[12]) || d.p[12] == 0 || !std::isfinite(d.p[13]) || d.p[13] == 0)
+                return "eldredgecombined2: a ramp's maximum G is zero or not finite";
+            break;
+        case IBG_MOTION_FILE_PERIODIC:
+            if (d.p[0] == 0) return "motionfileperiodic: period must be non-zero";
+            /* fall through */
+        case IBG_MOTION_FILE: {
+            if (B.table_rows < 0 || (B.table_rows > 0 && !B.table)) return "motion file: missing table";
+            for (int r = 0; r < B.table_rows; ++r) {
+                for (int k = 0; k < 7; ++k)
+                    if (!std::isfinite(B.table[7 * (size_t)r + k])) return "motion file: value is not finite";
+                if (r > 0 && B.table[7 * (size_t)r] < B.table[7 * (size_t)(r - 1)])
+                    return "motion file: time must increase monotonically";
+            }
+            d.trows = B.table_rows;
+            d.trow0 = (int)(tab.size() / 7);
+            tab.insert(tab.end(), B.table, B.table + 7 * (size_t)B.table_rows);
+            break;
+        }
+        default:
+            break;
+    }
+    return nullptr;
+}
+
 int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const ibg_params* params,
                void* cuda_stream, ibg_context** out) {
     if (!out || !grid || !params || (nbodies > 0 && !bodies) || nbodies < 1) {
@@ -885,16 +964,14 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
         d.xc = B.xcenter;
         d.yc = B.ycenter;
         d.motion = B.motion;
-        for (int k = 0; k < 6; ++k) d.p[k] = B.params[k];
-        if (B.motion == IBG_MOTION_PITCHPLUNGE) {
-            d.p[1] *= twopi;  // PitchPlunge stores 2 pi f (src/PitchPlunge.h:38-40)
-            d.p[4] *= twopi;
-            c->moving = true;
-        } else if (B.motion != IBG_MOTION_NONE && B.motion != IBG_MOTION_FIXED) {
+        const char* merr = body_motion(B, twopi, d, c->h_mtab);
+        if (merr) {
             delete c;
-            g_create_error = "ibg_create: unsupported motion type";
-            return IBG_ERR_UNSUPPORTED;
+            g_create_error = std::string("ibg_create: ") + merr;
+            return B.motion < IBG_MOTION_NONE || B.motion > IBG_MOTION_FILE_PERIODIC ? IBG_ERR_UNSUPPORTED : IBG_ERR_ARG;
         }
+        if (B.motion != IBG_MOTION_NONE && B.motion != IBG_MOTION_FIXED) c->moving = true;
+        if (motion_is_stateful(B.motion)) c->stateful = true;
         c->h_bodies.push_back(d);
         for (int p = 0; p < B.npoints; ++p) {
             c->h_ref.push_back(B.xy[2 * p]);
@@ -976,6 +1053,8 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
         c->alloc(&c->btmp, m) || c->alloc(&c->d_ref, 2 * (size_t)c->npts) ||
         c->alloc(&c->d_pts, 2 * (size_t)c->npts) || c->alloc(&c->d_vel, 2 * (size_t)c->npts) ||
         c->alloc(&c->d_body_of, (size_t)c->npts) || c->alloc(&c->d_bodies, c->h_bodies.size()) ||
+        c->alloc(&c->d_mstate, c->h_bodies.size()) || c->alloc(&c->d_mstate_keep, c->h_bodies.size()) ||
+        c->alloc(&c->d_mtab, std::max<size_t>(c->h_mtab.size(), 7)) ||
         c->alloc(&c->slots.idx, kSlots * m) || c->alloc(&c->slots.w, kSlots * m) || c->alloc(&c->slots.n, m) ||
         c->alloc(&c->d_b, m) || c->alloc(&c->d_time, 1) || c->alloc(&c->d_status, 1) || c->alloc(&c->cg_r, m) ||
         c->alloc(&c->cg_d, m) || c->alloc(&c->cg_q, m) || c->alloc(&c->cg_z, m) || c->alloc(&c->cg_zold, m) || c->alloc(&c->cg_scal, 4) || c->alloc(&c->cg_flags, 10) ||
@@ -999,6 +1078,10 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
     cudaMemcpy(c->lb.closed, bclosed.data(), sizeof(int) * nbodies, cudaMemcpyHostToDevice);
     cudaMemcpy(c->d_body_of, body_of.data(), sizeof(int) * body_of.size(), cudaMemcpyHostToDevice);
     cudaMemcpy(c->d_bodies, c->h_bodies.data(), sizeof(BodyDev) * c->h_bodies.size(), cudaMemcpyHostToDevice);
+    c->nbodies = (int)c->h_bodies.size();
+    cudaMemset(c->d_mstate, 0, sizeof(MotionState) * c->h_bodies.size());  // fresh Motion objects: zero history
+    if (!c->h_mtab.empty())
+        cudaMemcpy(c->d_mtab, c->h_mtab.data(), sizeof(double) * c->h_mtab.size(), cudaMemcpyHostToDevice);
     double sc[4] = {0, 0, c->prm.cg_tol * c->prm.cg_tol, 0};
     cudaMemcpy(c->cg_scal, sc, sizeof(sc), cudaMemcpyHostToDevice);
     int fl[10] = {0, 0, c->prm.cg_max_iter, 0, 0, 0, 0, 0, 0, c->prm.pc_fallback_iter};
@@ -1428,11 +1511,28 @@ int ibg_get_boundary_force(ibg_context* c, double* f, int* timestep, double* tim
 
 int ibg_update_operators(ibg_context* c, double time) {
     if (!c) return IBG_ERR_ARG;
-    c->time = time;
-    cudaMemcpyAsync(c->d_time, &c->time, sizeof(double), cudaMemcpyHostToDevice, c->st);
+    // the state's own time stays as it is
+    const double keep = c->time;
+    cudaMemcpyAsync(c->d_time, &time, sizeof(double), cudaMemcpyHostToDevice, c->st);
     if (c->moving) c->move_bodies(0.0);
+    cudaMemcpyAsync(c->d_time, &keep, sizeof(double), cudaMemcpyHostToDevice, c->st);
     if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->cuda_check("ibg_update_operators");
     return c->cuda_check("ibg_update_operators");
+}
+
+int ibg_get_boundary(ibg_context* c, double* points, double* velocities) {
+    if (!c) return IBG_ERR_ARG;
+    const size_t n = (size_t)c->npts;
+    std::vector<double> h(4 * n);
+    cudaMemcpyAsync(h.data(), c->d_pts, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, c->st);
+    cudaMemcpyAsync(h.data() + 2 * n, c->d_vel, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, c->st);
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->cuda_check("ibg_get_boundary");
+    for (size_t p = 0; p < n; ++p)
+        for (int d = 0; d < 2; ++d) {
+            if (points) points[d * n + p] = h[2 * p + d];
+            if (velocities) velocities[d * n + p] = h[2 * n + 2 * p + d];
+        }
+    return c->cuda_check("ibg_get_boundary");
 }
 
 int ibg_refresh_state(ibg_context* c) {
@@ -1838,6 +1938,8 @@ int ibg_lpc_generate(ibg_context* c, int nconfig, double t0, double t1, float* g
     std::vector<double> Mh((size_t)m * m);
     const double keep_time = c->time;
     int status = IBG_OK;
+    // the sampled configurations are not part of the body's motion history
+    cudaMemcpyAsync(c->d_mstate_keep, c->d_mstate, sizeof(MotionState) * c->nbodies, cudaMemcpyDeviceToDevice, c->st);
     for (int cf = 0; cf < nconfig && !status; ++cf) {
         const double t = nconfig == 1 ? t0 : t0 + (t1 - t0) * cf / (nconfig - 1);
         cudaMemcpyAsync(c->d_time, &t, sizeof(double), cudaMemcpyHostToDevice, c->st);
@@ -1857,6 +1959,7 @@ int ibg_lpc_generate(ibg_context* c, int nconfig, double t0, double t1, float* g
             for (int j = 0; j < m; ++j) out[(size_t)i * m + j] = (float)(Mh[(size_t)j * m + i] / c->beta[k]);
     }
     // back to the current configuration
+    cudaMemcpyAsync(c->d_mstate, c->d_mstate_keep, sizeof(MotionState) * c->nbodies, cudaMemcpyDeviceToDevice, c->st);
     cudaMemcpyAsync(c->d_time, &keep_time, sizeof(double), cudaMemcpyHostToDevice, c->st);
     c->move_bodies(0.0);
     if (cudaStreamSynchronize(c->st) != cudaSuccess && !status) status = c->cuda_check("ibg_lpc_generate");

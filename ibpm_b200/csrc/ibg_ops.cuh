@@ -6,11 +6,24 @@ namespace ibg {
 
 // Rigid-body motion on the device: motion 0 = none, 1 = fixed (x, y, theta),
 // 2 = pitch/plunge with p = (A_theta, 2 pi f_theta, phi_theta, A_y, 2 pi f_y, phi_y).
+// A rigid body's motion on the device: p holds the geometry file's numbers
+// (PITCHPLUNGE frequencies times 2 pi; the Eldredge family's normalisers
+// maxG appended after them), trows / trow0 the rows of its motion table in
+// the context's table (7 doubles a row: t x y theta xdot ydot thetadot).
 struct BodyDev {
     double xc, yc;
     int motion;
-    double p[6];
+    double p[14];
+    int trows, trow0;
 };
+// Running integrals of the motions whose transformation depends on the times
+// they were called at (src/FixedVelocity.h:42-50, src/Eldredge2.h:52-71,
+// src/EldredgeCombined2.h:64-87): position integrals, the integral of G, and
+// the last time.
+struct MotionState {
+    double ix, iy, ith, ig, told;
+};
+bool motion_is_stateful(int motion);
 
 // Regularizer association slots: up to kSlots level-0 fluxes per boundary component.
 constexpr int kSlots = 16;
@@ -34,8 +47,13 @@ void launch_reg_gather(const GridDev& g, int ncomp, const RegSlots& s, const dou
                        cudaStream_t st);
 template <typename T>
 void launch_refresh_flux(const GridDev& g, const T* psi, T* q, double u0, double v0, cudaStream_t st);
+// Geometry::moveBodies at time *time_ptr + toff: advance the history of the
+// stateful motions (one thread per body), then move every point.
+void launch_motion_state(int nbodies, const BodyDev* bodies, const double* time_ptr, double toff, MotionState* ms,
+                         cudaStream_t st);
 void launch_kinematics(int npts, const double* ref_xy, const int* body_of, const BodyDev* bodies,
-                       const double* time_ptr, double toff, double* pts, double* vel, cudaStream_t st);
+                       const MotionState* ms, const double* mtab, const double* time_ptr, double toff, double* pts,
+                       double* vel, cudaStream_t st);
 void launch_reg_update(const GridDev& g, int npts, const double* pts, const double* vel, RegSlots& s, double* bcon,
                        double u0, double v0, cudaStream_t st);
 template <typename T>

@@ -8,12 +8,14 @@
 //   k_rhs          IBSolver::advanceSubstep RHS        src/IBSolver.cc:168-183
 //                  with Laplacian = -Curl(Curl())      src/VectorOperations.cc:63-146
 //   k_refresh_flux computeFlux = Curl(psi) + q0         src/NavierStokesModel.cc:114-125
-//   k_kinematics   RigidBody::moveBody + PitchPlunge   src/RigidBody.cc:586-609, src/PitchPlunge.h:52-58
+//   k_kinematics   RigidBody::moveBody + Motion        src/RigidBody.cc:586-609, src/Motion.h subclasses
+//   k_motion_state the history of FixedVelocity / Eldredge2 / EldredgeCombined2
 //   k_reg_update   Regularizer::update                 src/Regularizer.cc:54-90
 //   k_reg_interp   Regularizer::toBoundary o Curl(psi) src/Regularizer.cc:111-128
 //   k_reg_smear/k_bf  Regularizer::toFlux, Curl, *beta  src/Regularizer.cc:92-109, src/ProjectionSolver.cc:87-90
 #include "ibg_internal.cuh"
 #include "ibg_ops.cuh"
+#include "../../include/ibpm_b200.h"
 
 namespace ibg {
 
@@ -340,14 +342,165 @@ __global__ void k_refresh_flux(GridDev g, const T* __restrict__ psi, T* __restri
 // ---------------------------------------------------------------------------
 // bodies
 // ---------------------------------------------------------------------------
+__host__ __device__ inline bool motion_is_stateful_dev(int motion) {
+    return motion == IBG_MOTION_FIXEDVEL || motion == IBG_MOTION_ELDREDGE2 || motion == IBG_MOTION_ELDREDGECOMBINED2;
+}
+bool motion_is_stateful(int motion) { return motion_is_stateful_dev(motion); }
+
+// G(t) = log(cosh(a(t - t1)) cosh(a(t - t4)) / (cosh(a(t - t2)) cosh(a(t - t3)))) and dG/dt of
+// Eldredge's smoothed ramp (src/EldredgeManeuver.h:56-59), with q = (a, t1, t2, t3, t4)
+__device__ __forceinline__ double eld_G(const double* q, double t) {
+    const double a = q[0];
+    return log((cosh(a * (t - q[1])) * cosh(a * (t - q[4]))) / (cosh(a * (t - q[2])) * cosh(a * (t - q[3]))));
+}
+__device__ __forceinline__ double eld_dG(const double* q, double t) {
+    const double a = q[0];
+    return a * (tanh(a * (t - q[1])) - tanh(a * (t - q[2])) - tanh(a * (t - q[3])) + tanh(a * (t - q[4])));
+}
+
+// The reference's Motion objects that keep a running integral update it on
+// every getTransformation call; a second call at the same time adds nothing.
+__device__ void advance_history(const BodyDev& b, MotionState& s, double t) {
+    if (!motion_is_stateful_dev(b.motion)) return;
+    double dtt = t - s.told;
+    if (b.motion == IBG_MOTION_FIXEDVEL) {  // src/FixedVelocity.h:42-48
+        if (dtt > 1) dtt = 0.;
+        s.ix = s.ix + b.p[0] * dtt;
+        s.iy = s.iy + b.p[1] * dtt;
+        s.ith = s.ith + b.p[2] * dtt;
+    } else {  // src/Eldredge2.h:62-66, src/EldredgeCombined2.h:81-85 (G of the plunge ramp a)
+        s.ig = s.ig + eld_G(b.p + 1, t) * dtt;
+    }
+    s.told = t;
+}
+
+// one thread per body
+__global__ void k_motion_state(int nbodies, const BodyDev* __restrict__ bodies, const double* __restrict__ time_ptr,
+                               double toff, MotionState* __restrict__ ms) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nbodies) return;
+    const BodyDev& b = bodies[k];
+    if (!motion_is_stateful_dev(b.motion)) return;
+    MotionState s = ms[k];
+    advance_history(b, s, *time_ptr + toff);
+    ms[k] = s;
+}
+
+// Motion::getTransformation(t): (x, y, theta, xdot, ydot, thetadot) of the body frame.
+__device__ void body_frame(const BodyDev& b, const MotionState& s, const double* __restrict__ mtab, double t,
+                           double& x, double& y, double& th, double& xd, double& yd, double& thd) {
+    const double pi = 3.141592653589793;  // 4 atan(1), as the reference computes it
+    x = y = th = xd = yd = thd = 0.0;
+    const double* p = b.p;
+    switch (b.motion) {
+        case IBG_MOTION_FIXED:  // src/FixedPosition.h:42-44
+            x = p[0]; y = p[1]; th = p[2];
+            break;
+        case IBG_MOTION_PITCHPLUNGE:  // src/PitchPlunge.h:52-58 (frequencies already times 2 pi)
+            y = p[3] * sin(p[4] * t + p[5]);
+            yd = p[3] * p[4] * cos(p[4] * t + p[5]);
+            th = p[0] * sin(p[1] * t + p[2]);
+            thd = p[0] * p[1] * cos(p[1] * t + p[2]);
+            break;
+        case IBG_MOTION_FIXEDVEL:  // src/FixedVelocity.h:49
+            x = s.ix; y = s.iy; th = s.ith;
+            xd = p[0]; yd = p[1]; thd = p[2];
+            break;
+        case IBG_MOTION_SIGMOIDALSTEP: {  // src/SigmoidalStep.h:41-51: AMP, DUR, t0
+            const double arg = ((12. * (t - p[2]) / p[1]) - 6.);
+            const double coeff = 12. / (p[1] * sqrt(pi));
+            th = (1. / 2) * p[0] * (pi / 180) * (1. + erf(arg));
+            thd = p[0] * (pi / 180) * coeff * exp(-arg * arg);
+            break;
+        }
+        case IBG_MOTION_LAGSTEP1:    // src/LagStep1.h:41-62: AMP, PW, TAU, T0
+        case IBG_MOTION_LAGSTEP2: {  // src/LagStep2.h:41-62
+            const double ampr = p[0] * (pi / 180), PW = p[1], TAU = p[2], td = t - p[3];
+            double a = 0., ad = 0.;
+            if (td > 0 && td <= PW) {
+                if (b.motion == IBG_MOTION_LAGSTEP1) {
+                    a = td + TAU * exp(-td / TAU) - TAU;
+                    ad = 1 - exp(-td / TAU);
+                } else {
+                    a = td + (2 * TAU + td) * exp(-td / TAU) - 2 * TAU;
+                    ad = 1. - (1. + td / TAU) * exp(-td / TAU);
+                }
+            } else if (td > PW) {
+                if (b.motion == IBG_MOTION_LAGSTEP1) {
+                    a = PW + TAU * exp(-td / TAU) - TAU * exp(-(td - PW) / TAU);
+                    ad = -1. * exp(-td / TAU) + exp(-(td - PW) / TAU);
+                } else {
+                    a = PW + (2 * TAU + td) * exp(-td / TAU) + (PW - 2 * TAU) * exp(-(td - PW) / TAU) -
+                        td * exp(-(td - PW) / TAU);
+                    ad = -(1. + td / TAU) * exp(-td / TAU) + (1. + (td - PW) / TAU) * exp(-(td - PW) / TAU);
+                }
+            }
+            th = a * ampr / PW;
+            thd = ad * ampr / PW;
+            break;
+        }
+        case IBG_MOTION_ELDREDGE: {  // src/EldredgeManeuver.h:48-61: pitch; p[6] = maxG
+            const double ampr = p[0] * (pi / 180);
+            th = eld_G(p + 1, t) * ampr / p[6];
+            thd = eld_dG(p + 1, t) * ampr / p[6];
+            break;
+        }
+        case IBG_MOTION_ELDREDGE1:  // src/Eldredge1.h:46-56: plunge
+            y = eld_G(p + 1, t) * p[0] / p[6];
+            yd = eld_dG(p + 1, t) * p[0] / p[6];
+            break;
+        case IBG_MOTION_ELDREDGE2:  // src/Eldredge2.h:52-71: plunge velocity G, position its integral
+            y = s.ig * p[0] / p[6];
+            yd = eld_G(p + 1, t) * p[0] / p[6];
+            break;
+        case IBG_MOTION_ELDREDGECOMBINED2: {  // src/EldredgeCombined2.h:64-87; p[12] = maxGa, p[13] = maxGb
+            const double ampr = p[6] * (pi / 180);
+            y = s.ig * p[0] / p[12];
+            th = eld_G(p + 7, t) * ampr / p[13];
+            yd = eld_G(p + 1, t) * p[0] / p[12];
+            thd = eld_dG(p + 7, t) * ampr / p[13];
+            break;
+        }
+        case IBG_MOTION_FILE:
+        case IBG_MOTION_FILE_PERIODIC: {  // src/MotionFile.h:90-115, src/MotionFilePeriodic.h:91-117
+            const double tt = b.motion == IBG_MOTION_FILE_PERIODIC ? fmod(t, p[0]) : t;
+            const double* r = mtab + 7 * (size_t)b.trow0;
+            const int n = b.trows;
+            // the interval [t_i, t_i+1) holding tt: the last row with t_i <= tt, unless it is the last row
+            // (rows are non-decreasing in t, so that interval is the reference's scan result)
+            if (n < 2 || !(tt >= r[0])) break;
+            int lo = 0, hi = n - 1;  // r[7 lo] <= tt
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) / 2;
+                if (r[7 * mid] <= tt) lo = mid; else hi = mid;
+            }
+            if (r[7 * hi] <= tt) break;  // tt at or past the last row
+            const double* r0 = r + 7 * lo;
+            const double* r1 = r0 + 7;
+            const double al = (tt - r0[0]) / (r1[0] - r0[0]);
+            x = al * r1[1] + (1 - al) * r0[1];
+            y = al * r1[2] + (1 - al) * r0[2];
+            th = al * r1[3] + (1 - al) * r0[3];
+            xd = al * r1[4] + (1 - al) * r0[4];
+            yd = al * r1[5] + (1 - al) * r0[5];
+            thd = al * r1[6] + (1 - al) * r0[6];
+            break;
+        }
+        default:
+            break;
+    }
+}
+
 __global__ void k_kinematics(int npts, const double* __restrict__ ref_xy, const int* __restrict__ body_of,
-                             const BodyDev* __restrict__ bodies, const double* __restrict__ time_ptr, double toff,
+                             const BodyDev* __restrict__ bodies, const MotionState* __restrict__ ms,
+                             const double* __restrict__ mtab, const double* __restrict__ time_ptr, double toff,
                              double* __restrict__ pts, double* __restrict__ vel) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npts) return;
-    const BodyDev b = bodies[body_of[p]];
+    const int k = body_of[p];
+    const BodyDev& b = bodies[k];
     const double rx = ref_xy[2 * p], ry = ref_xy[2 * p + 1];
-    if (b.motion == 0) {
+    if (b.motion == IBG_MOTION_NONE) {
         pts[2 * p] = rx;
         pts[2 * p + 1] = ry;
         vel[2 * p] = 0.0;
@@ -356,17 +509,8 @@ __global__ void k_kinematics(int npts, const double* __restrict__ ref_xy, const 
     }
     const double t = *time_ptr + toff;
     double x, y, th, xd, yd, thd;
-    if (b.motion == 1) {
-        x = b.p[0]; y = b.p[1]; th = b.p[2];
-        xd = yd = thd = 0.0;
-    } else {
-        // PitchPlunge: frequencies already multiplied by 2 pi
-        x = 0.0; xd = 0.0;
-        y = b.p[3] * sin(b.p[4] * t + b.p[5]);
-        yd = b.p[3] * b.p[4] * cos(b.p[4] * t + b.p[5]);
-        th = b.p[0] * sin(b.p[1] * t + b.p[2]);
-        thd = b.p[0] * b.p[1] * cos(b.p[1] * t + b.p[2]);
-    }
+    body_frame(b, ms[k], mtab, t, x, y, th, xd, yd, thd);
+    // TangentSE2::mapPosition / mapVelocity about the centre (src/TangentSE2.h:83-107)
     const double a = rx - b.xc, bb = ry - b.yc;
     const double c = cos(th), s = sin(th);
     pts[2 * p] = (x + a * c - bb * s) + b.xc;
@@ -576,9 +720,15 @@ void launch_refresh_flux(const GridDev& g, const T* psi, T* q, double u0, double
     k_refresh_flux<T><<<nblk(F, 256), 256, 0, st>>>(g, psi, q, u0, v0);
 }
 
+void launch_motion_state(int nbodies, const BodyDev* bodies, const double* time_ptr, double toff, MotionState* ms,
+                         cudaStream_t st) {
+    k_motion_state<<<nblk(nbodies, 32), 32, 0, st>>>(nbodies, bodies, time_ptr, toff, ms);
+}
+
 void launch_kinematics(int npts, const double* ref_xy, const int* body_of, const BodyDev* bodies,
-                       const double* time_ptr, double toff, double* pts, double* vel, cudaStream_t st) {
-    k_kinematics<<<nblk(npts, 128), 128, 0, st>>>(npts, ref_xy, body_of, bodies, time_ptr, toff, pts, vel);
+                       const MotionState* ms, const double* mtab, const double* time_ptr, double toff, double* pts,
+                       double* vel, cudaStream_t st) {
+    k_kinematics<<<nblk(npts, 128), 128, 0, st>>>(npts, ref_xy, body_of, bodies, ms, mtab, time_ptr, toff, pts, vel);
 }
 
 void launch_reg_update(const GridDev& g, int npts, const double* pts, const double* vel, RegSlots& s, double* bcon,

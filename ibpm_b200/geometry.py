@@ -3,22 +3,54 @@ rigid-body motions, expressed as the plain arrays the C-ABI takes.
 
 Follows the reference's parser (src/Geometry.cc:143-205, src/RigidBody.cc:248-529)
 for the commands the time step uses: ``body``/``end``, ``circle``, ``circle_n``,
-``line``, ``line_n``, ``line_aoa``, ``point``, ``raw``, ``center`` and
-``motion fixed | pitchplunge``.  Point generation follows
-src/RigidBody.cc:92-170.  Other motion types are rejected with a clear error.
+``line``, ``line_n``, ``line_aoa``, ``point``, ``raw``, ``center``, ``name`` and
+every ``motion`` type of src/RigidBody.cc:349-493 (fixed, fixedvel,
+pitchplunge, sigmoidalstep, lagstep1, lagstep2, eldredge, eldredgecombined2,
+eldredge1, eldredge2, motionfile, motionfileperiodic).  Point generation
+follows src/RigidBody.cc:92-170; a motion file is read as src/MotionFile.h:47-69
+reads it (a row count, then rows of t x y theta xdot ydot thetadot).  The
+kinematics themselves are evaluated on the device.
 """
 from __future__ import annotations
 
 import math
 import os
 from dataclasses import dataclass, field
-from typing import List, Tuple
+from typing import List, Optional, Tuple
 
 import numpy as np
 
 MOTION_NONE = 0
 MOTION_FIXED = 1
 MOTION_PITCHPLUNGE = 2
+MOTION_FIXEDVEL = 3
+MOTION_SIGMOIDALSTEP = 4
+MOTION_LAGSTEP1 = 5
+MOTION_LAGSTEP2 = 6
+MOTION_ELDREDGE = 7
+MOTION_ELDREDGECOMBINED2 = 8
+MOTION_ELDREDGE1 = 9
+MOTION_ELDREDGE2 = 10
+MOTION_FILE = 11
+MOTION_FILE_PERIODIC = 12
+
+# `motion` keyword -> (code, count of numbers after it) (src/RigidBody.cc:349-493)
+MOTIONS = {
+    "fixed": (MOTION_FIXED, 3),
+    "fixedvel": (MOTION_FIXEDVEL, 3),
+    "pitchplunge": (MOTION_PITCHPLUNGE, 6),
+    "sigmoidalstep": (MOTION_SIGMOIDALSTEP, 3),
+    "lagstep1": (MOTION_LAGSTEP1, 4),
+    "lagstep2": (MOTION_LAGSTEP2, 4),
+    "eldredge": (MOTION_ELDREDGE, 6),
+    "eldredgecombined2": (MOTION_ELDREDGECOMBINED2, 12),
+    "eldredge1": (MOTION_ELDREDGE1, 6),
+    "eldredge2": (MOTION_ELDREDGE2, 6),
+    "motionfile": (MOTION_FILE, 0),
+    "motionfileperiodic": (MOTION_FILE_PERIODIC, 1),
+}
+MOTION_NAMES = {code: name for name, (code, _) in MOTIONS.items()}
+MOTION_NAMES[MOTION_NONE] = "none"
 
 
 @dataclass
@@ -27,11 +59,13 @@ class RigidBody:
     points: List[Tuple[float, float]] = field(default_factory=list)
     center: Tuple[float, float] = (0.0, 0.0)
     motion: int = MOTION_NONE
-    params: Tuple[float, ...] = (0.0,) * 6
+    params: Tuple[float, ...] = ()
+    table: Optional[np.ndarray] = None    # motion file rows (t, x, y, theta, xdot, ydot, thetadot)
 
     @property
     def stationary(self) -> bool:
-        return self.motion != MOTION_PITCHPLUNGE
+        # Motion::isStationary is true only for FixedPosition (src/Motion.h:28, src/FixedPosition.h:39)
+        return self.motion in (MOTION_NONE, MOTION_FIXED)
 
     def add_circle_n(self, xc, yc, r, n):  # src/RigidBody.cc:105-118
         twopi = 8.0 * math.atan(1.0)
@@ -78,35 +112,6 @@ class Geometry:
 
     def ref_points(self) -> np.ndarray:
         return np.array([p for b in self.bodies for p in b.points], dtype=np.float64).reshape(-1, 2)
-
-    def points_velocities(self, t: float):
-        """Geometry::moveBodies + getPoints/getVelocities at time t
-        (src/Geometry.cc:79-121, src/RigidBody.cc:586-609)."""
-        pos, vel = [], []
-        for b in self.bodies:
-            P = np.array(b.points, dtype=np.float64).reshape(-1, 2)
-            if b.motion == MOTION_NONE:
-                pos.append(P)
-                vel.append(np.zeros_like(P))
-                continue
-            if b.motion == MOTION_FIXED:
-                x, y, th = b.params[:3]
-                xd = yd = thd = 0.0
-            else:
-                twopi = 8.0 * math.atan(1.0)
-                ap, fp, php, ay, fy, phy = b.params
-                wp, wy = fp * twopi, fy * twopi
-                x, xd = 0.0, 0.0
-                y = ay * math.sin(wy * t + phy)
-                yd = ay * wy * math.cos(wy * t + phy)
-                th = ap * math.sin(wp * t + php)
-                thd = ap * wp * math.cos(wp * t + php)
-            a = P[:, 0] - b.center[0]
-            bb = P[:, 1] - b.center[1]
-            c, s = math.cos(th), math.sin(th)
-            pos.append(np.stack([x + a * c - bb * s + b.center[0], y + a * s + bb * c + b.center[1]], 1))
-            vel.append(np.stack([-a * s * thd - bb * c * thd + xd, a * c * thd - bb * s * thd + yd], 1))
-        return np.concatenate(pos), np.concatenate(vel)
 
 
 class GeometryError(ValueError):
@@ -161,16 +166,18 @@ def parse(text: str, basedir: str = ".") -> Geometry:
                     body.name = " ".join(a)
                 elif c == "motion":
                     kind = a[0].lower()
-                    if kind == "fixed":
-                        body.motion = MOTION_FIXED
-                        body.params = tuple(float(v) for v in a[1:4]) + (0.0, 0.0, 0.0)
-                    elif kind == "pitchplunge":
-                        body.motion = MOTION_PITCHPLUNGE
-                        body.params = tuple(float(v) for v in a[1:7])
-                        if len(body.params) != 6:
-                            raise GeometryError("pitchplunge takes 6 numbers (src/RigidBody.cc:373-384)")
+                    if kind not in MOTIONS:
+                        raise GeometryError(f"unknown motion type {kind!r}")
+                    code, npar = MOTIONS[kind]
+                    body.motion = code
+                    if code in (MOTION_FILE, MOTION_FILE_PERIODIC):
+                        path = a[1] if os.path.isabs(a[1]) else os.path.join(basedir, a[1])
+                        body.table = read_motion_file(path)
+                        body.params = tuple(float(v) for v in a[2:2 + npar])
                     else:
-                        raise GeometryError(f"motion type {kind!r} is not supported by the GPU time step")
+                        body.params = tuple(float(v) for v in a[1:1 + npar])
+                    if len(body.params) != npar:
+                        raise GeometryError(f"motion {kind} takes {npar} numbers")
                 else:
                     raise GeometryError(f"could not parse line: {braw!r}")
             except (IndexError, ValueError) as e:
@@ -179,6 +186,24 @@ def parse(text: str, basedir: str = ".") -> Geometry:
                 raise GeometryError(f"bad arguments in line: {braw!r}") from e
         geo.bodies.append(body)
     return geo
+
+
+def read_motion_file(path: str) -> np.ndarray:
+    """Rows (t, x, y, theta, xdot, ydot, thetadot) of a motion file: a row
+    count, then that many rows (src/MotionFile.h:47-69); t non-decreasing."""
+    with open(path) as fh:
+        vals = fh.read().split()
+    try:
+        n = int(vals[0])
+        rows = np.array([float(v) for v in vals[1:1 + 7 * n]], dtype=np.float64)
+    except (IndexError, ValueError) as e:
+        raise GeometryError(f"motion file {path} formatted incorrectly") from e
+    if n < 0 or rows.size != 7 * n:
+        raise GeometryError(f"motion file {path} formatted incorrectly")
+    rows = rows.reshape(n, 7)
+    if n > 1 and np.any(np.diff(rows[:, 0]) < 0):
+        raise GeometryError(f"motion file {path}: time must increase monotonically")
+    return rows
 
 
 def load(path: str) -> Geometry:

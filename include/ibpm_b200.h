@@ -36,19 +36,41 @@ typedef struct {
     double length, xoffset, yoffset;
 } ibg_grid;
 
-/* motion kinds of a rigid body (src/Motion.h, src/FixedPosition.h, src/PitchPlunge.h) */
-enum { IBG_MOTION_NONE = 0, IBG_MOTION_FIXED = 1, IBG_MOTION_PITCHPLUNGE = 2 };
+/* motion kinds of a rigid body, one per `motion` keyword of the geometry file
+ * (src/RigidBody.cc:349-493; src/Motion.h and its subclasses) */
+enum {
+    IBG_MOTION_NONE = 0,
+    IBG_MOTION_FIXED = 1,               /* fixed x y theta                    src/FixedPosition.h */
+    IBG_MOTION_PITCHPLUNGE = 2,         /* pitchplunge Ap fp php Ay fy phy    src/PitchPlunge.h */
+    IBG_MOTION_FIXEDVEL = 3,            /* fixedvel xdot ydot thetadot        src/FixedVelocity.h */
+    IBG_MOTION_SIGMOIDALSTEP = 4,       /* sigmoidalstep AMP DUR t0           src/SigmoidalStep.h */
+    IBG_MOTION_LAGSTEP1 = 5,            /* lagstep1 AMP PW TAU T0             src/LagStep1.h */
+    IBG_MOTION_LAGSTEP2 = 6,            /* lagstep2 AMP PW TAU T0             src/LagStep2.h */
+    IBG_MOTION_ELDREDGE = 7,            /* eldredge AMP a t1 t2 t3 t4         src/EldredgeManeuver.h */
+    IBG_MOTION_ELDREDGECOMBINED2 = 8,   /* eldredgecombined2 AMPa a a1..a4 AMPb b b1..b4  src/EldredgeCombined2.h */
+    IBG_MOTION_ELDREDGE1 = 9,           /* eldredge1 AMP a t1 t2 t3 t4        src/Eldredge1.h */
+    IBG_MOTION_ELDREDGE2 = 10,          /* eldredge2 AMP a t1 t2 t3 t4        src/Eldredge2.h */
+    IBG_MOTION_FILE = 11,               /* motionfile FILE                    src/MotionFile.h */
+    IBG_MOTION_FILE_PERIODIC = 12       /* motionfileperiodic FILE period     src/MotionFilePeriodic.h */
+};
 
 /* RigidBody: reference points, centre and motion (src/RigidBody.h:35-190).
- * FIXED: params = (x, y, theta).  PITCHPLUNGE: params = (pitch amplitude,
- * pitch frequency, pitch phase, plunge amplitude, plunge frequency, plunge
- * phase) exactly as the geometry file's `motion pitchplunge` line. */
+ * params holds the numbers of the geometry file's `motion` line in their
+ * order (PITCHPLUNGE frequencies in cycles per time unit, as written there;
+ * FILE_PERIODIC: params[0] = period).  FILE and FILE_PERIODIC take the
+ * file's rows as `table`: table_rows rows of (t, x, y, theta, xdot, ydot,
+ * thetadot), t non-decreasing (src/MotionFile.h:62-87).  FIXEDVEL, ELDREDGE2
+ * and ELDREDGECOMBINED2 integrate over the times at which the bodies are
+ * moved, as the reference's Motion objects do; that history belongs to the
+ * context and starts at time 0 when it is created. */
 typedef struct {
     int npoints;
     const double* xy;       /* npoints interleaved (x, y) reference points */
     double xcenter, ycenter;
     int motion;
-    double params[6];
+    double params[12];
+    int table_rows;
+    const double* table;    /* table_rows x 7, row-major; NULL when table_rows == 0 */
 } ibg_body;
 
 /* time-stepping schemes (src/Scheme.h:13-61) */
@@ -111,8 +133,13 @@ IBG_API int ibg_set_state(ibg_context* ctx, const double* omega, const double* q
 IBG_API int ibg_get_state(ibg_context* ctx, double* omega, double* q, double* f, int* timestep, double* time);
 /* only f, timestep and time (what the reference CLI reads every step) */
 IBG_API int ibg_get_boundary_force(ibg_context* ctx, double* f, int* timestep, double* time);
-/* NavierStokesModel::updateOperators(time) + refreshState(x) (src/NavierStokesModel.cc:93-99, :127-129) */
+/* NavierStokesModel::updateOperators(time) (src/NavierStokesModel.cc:93-99):
+ * moves the bodies to `time`; the state's own time is unchanged. */
 IBG_API int ibg_update_operators(ibg_context* ctx, double time);
+/* Geometry::getPoints / getVelocities (src/Geometry.cc:79-110) at the last
+ * time the bodies were moved: 2 npoints values each in the BoundaryVector
+ * layout (every x, then every y).  Either pointer may be NULL. */
+IBG_API int ibg_get_boundary(ibg_context* ctx, double* points, double* velocities);
 IBG_API int ibg_refresh_state(ibg_context* ctx);
 
 /* --- restart files ------------------------------------------------------------

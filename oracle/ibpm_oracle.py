@@ -682,36 +682,134 @@ def _batched_add(acc, idx, vals):
 
 
 # ----------------------------------------------------------------------------
-# Bodies and kinematics (src/RigidBody.cc:105-131, :586-609; src/PitchPlunge.h:52-58;
-# src/TangentSE2.h:83-107; src/FixedPosition.h)
+# Bodies and kinematics (src/RigidBody.cc:105-131, :586-609; src/TangentSE2.h:83-107;
+# the Motion subclasses named below)
 # ----------------------------------------------------------------------------
+
+MOTION_PARAMS = {"none": 0, "fixed": 3, "pitchplunge": 6, "fixedvel": 3, "sigmoidalstep": 3, "lagstep1": 4,
+                 "lagstep2": 4, "eldredge": 6, "eldredgecombined2": 12, "eldredge1": 6, "eldredge2": 6,
+                 "motionfile": 0, "motionfileperiodic": 1}
+
+
+def _eld_G(a, t1, t2, t3, t4, t):
+    """G(t) of Eldredge's smoothed ramp (src/EldredgeManeuver.h:56-57)."""
+    return math.log((math.cosh(a * (t - t1)) * math.cosh(a * (t - t4))) /
+                    (math.cosh(a * (t - t2)) * math.cosh(a * (t - t3))))
+
+
+def _eld_dG(a, t1, t2, t3, t4, t):
+    return a * (math.tanh(a * (t - t1)) - math.tanh(a * (t - t2)) - math.tanh(a * (t - t3)) + math.tanh(a * (t - t4)))
+
+
+def _eld_max(a, a4, t1, t2, t3, t4):
+    """maxG = G((t2 + t3)/2) (src/EldredgeManeuver.h:42-43); EldredgeCombined2 uses `a` in the t4 factor of its
+    pitch ramp (src/EldredgeCombined2.h:59), hence the separate a4."""
+    tt = (t2 + t3) / 2.0
+    return math.log((math.cosh(a * (tt - t1)) * math.cosh(a4 * (tt - t4))) /
+                    (math.cosh(a * (tt - t2)) * math.cosh(a * (tt - t3))))
 
 
 @dataclass
 class Body:
     ref_xy: np.ndarray                 # (n, 2) reference points
     center: tuple = (0.0, 0.0)
-    motion: str = "none"               # none | fixed | pitchplunge
-    params: tuple = ()                 # fixed: (x, y, theta); pitchplunge: (Ap, fp, php, Ay, fy, phy)
+    motion: str = "none"               # a key of MOTION_PARAMS
+    params: tuple = ()                 # the geometry file's numbers, in order
+    table: np.ndarray = None           # motion file rows (t, x, y, theta, xdot, ydot, thetadot)
+    # running integrals of FixedVelocity / Eldredge2 / EldredgeCombined2 (fresh Motion object)
+    hist: dict = field(default_factory=lambda: {"x": 0.0, "y": 0.0, "th": 0.0, "g": 0.0, "told": 0.0})
 
     @property
     def stationary(self) -> bool:
         return self.motion in ("none", "fixed")
 
     def transformation(self, t: float):
-        """(x, y, theta, xdot, ydot, thetadot) of the body frame at time t."""
-        if self.motion == "pitchplunge":  # src/PitchPlunge.h:30-58
+        """Motion::getTransformation(t): (x, y, theta, xdot, ydot, thetadot) of the body frame.  The
+        stateful motions advance their history, as the reference's mutable members do."""
+        pi = 4.0 * math.atan(1.0)
+        m, p, h = self.motion, self.params, self.hist
+        if m == "pitchplunge":  # src/PitchPlunge.h:30-58
             twopi = 8.0 * math.atan(1.0)
-            ap, fp, php, ay, fy, phy = self.params
+            ap, fp, php, ay, fy, phy = p
             fp, fy = fp * twopi, fy * twopi
             y = ay * math.sin(fy * t + phy)
             ydot = ay * fy * math.cos(fy * t + phy)
             th = ap * math.sin(fp * t + php)
             thdot = ap * fp * math.cos(fp * t + php)
             return (0.0, y, th, 0.0, ydot, thdot)
-        if self.motion == "fixed":
-            x, y, th = self.params
+        if m == "fixed":  # src/FixedPosition.h:42-44
+            x, y, th = p
             return (x, y, th, 0.0, 0.0, 0.0)
+        if m == "fixedvel":  # src/FixedVelocity.h:42-50
+            dtt = t - h["told"]
+            if dtt > 1:
+                dtt = 0.0
+            h["x"] += p[0] * dtt
+            h["y"] += p[1] * dtt
+            h["th"] += p[2] * dtt
+            h["told"] = t
+            return (h["x"], h["y"], h["th"], p[0], p[1], p[2])
+        if m == "sigmoidalstep":  # src/SigmoidalStep.h:41-51
+            amp, dur, t0 = p
+            arg = 12.0 * (t - t0) / dur - 6.0
+            coeff = 12.0 / (dur * math.sqrt(pi))
+            return (0.0, 0.0, 0.5 * amp * (pi / 180) * (1.0 + math.erf(arg)), 0.0, 0.0,
+                    amp * (pi / 180) * coeff * math.exp(-arg * arg))
+        if m in ("lagstep1", "lagstep2"):  # src/LagStep1.h:41-62, src/LagStep2.h:41-62
+            amp, pw, tau, t0 = p
+            td = t - t0
+            ampr = amp * (pi / 180)
+            if td <= 0:
+                a = ad = 0.0
+            elif td <= pw:
+                if m == "lagstep1":
+                    a, ad = td + tau * math.exp(-td / tau) - tau, 1 - math.exp(-td / tau)
+                else:
+                    a = td + (2 * tau + td) * math.exp(-td / tau) - 2 * tau
+                    ad = 1.0 - (1.0 + td / tau) * math.exp(-td / tau)
+            else:
+                e1, e2 = math.exp(-td / tau), math.exp(-(td - pw) / tau)
+                if m == "lagstep1":
+                    a, ad = pw + tau * e1 - tau * e2, -e1 + e2
+                else:
+                    a = pw + (2 * tau + td) * e1 + (pw - 2 * tau) * e2 - td * e2
+                    ad = -(1.0 + td / tau) * e1 + (1.0 + (td - pw) / tau) * e2
+            return (0.0, 0.0, a * ampr / pw, 0.0, 0.0, ad * ampr / pw)
+        if m in ("eldredge", "eldredge1", "eldredge2"):
+            # src/EldredgeManeuver.h:48-61 (pitch), src/Eldredge1.h:46-56 (plunge),
+            # src/Eldredge2.h:52-71 (plunge velocity G, position its running integral)
+            amp, a = p[0], p[1]
+            q = (a,) + tuple(p[2:6])
+            mx = _eld_max(a, a, *p[2:6])
+            G, dG = _eld_G(*q, t), _eld_dG(*q, t)
+            if m == "eldredge":
+                r = amp * (pi / 180)
+                return (0.0, 0.0, G * r / mx, 0.0, 0.0, dG * r / mx)
+            if m == "eldredge1":
+                return (0.0, G * amp / mx, 0.0, 0.0, dG * amp / mx, 0.0)
+            h["g"] += G * (t - h["told"])
+            h["told"] = t
+            return (0.0, h["g"] * amp / mx, 0.0, 0.0, G * amp / mx, 0.0)
+        if m == "eldredgecombined2":  # src/EldredgeCombined2.h:64-87
+            ampa, a, a1, a2, a3, a4, ampb, b, b1, b2, b3, b4 = p
+            mxa, mxb = _eld_max(a, a, a1, a2, a3, a4), _eld_max(b, a, b1, b2, b3, b4)
+            Ga = _eld_G(a, a1, a2, a3, a4, t)
+            h["g"] += Ga * (t - h["told"])
+            h["told"] = t
+            r = ampb * (pi / 180)
+            return (0.0, h["g"] * ampa / mxa, _eld_G(b, b1, b2, b3, b4, t) * r / mxb, 0.0, Ga * ampa / mxa,
+                    _eld_dG(b, b1, b2, b3, b4, t) * r / mxb)
+        if m in ("motionfile", "motionfileperiodic"):  # src/MotionFile.h:90-115, src/MotionFilePeriodic.h:91-117
+            tt = math.fmod(t, p[0]) if m == "motionfileperiodic" else t
+            d = self.table
+            idx = -1
+            for i in range(len(d) - 1):  # the last interval holding tt, as the reference scans
+                if d[i, 0] <= tt < d[i + 1, 0]:
+                    idx = i
+            if idx < 0:
+                return (0.0,) * 6
+            al = (tt - d[idx, 0]) / (d[idx + 1, 0] - d[idx, 0])
+            return tuple(al * d[idx + 1, k] + (1 - al) * d[idx, k] for k in range(1, 7))
         return None
 
     def points_velocities(self, t: float):

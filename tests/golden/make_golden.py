@@ -42,12 +42,18 @@ CASES = [
 ]
 
 
-def run(case):
+def run(case, files=None):
+    """files: {name: text} written beside the geometry file; the driver runs
+    there, so a `motion motionfile NAME` line finds NAME as the reference does."""
     name, nx, ny, ngrid, length, xoff, yoff, geom, Re, dt, nsteps, scheme, tol, noise = case
+    files = files or {}
     with tempfile.TemporaryDirectory() as td:
         gpath = os.path.join(td, "body.geom")
         with open(gpath, "w") as fh:
             fh.write(geom)
+        for fname, text in files.items():
+            with open(os.path.join(td, fname), "w") as fh:
+                fh.write(text)
         args = [DRIVER, "-nx", str(nx), "-ny", str(ny), "-ngrid", str(ngrid), "-length", repr(length),
                 "-xoffset", repr(xoff), "-yoffset", repr(yoff), "-geom", gpath, "-Re", repr(Re),
                 "-dt", repr(dt), "-scheme", scheme, "-nsteps", str(nsteps), "-tol", repr(tol),
@@ -64,16 +70,54 @@ def run(case):
             ic = os.path.join(td, "ic.bin")
             O.save_restart(ic, st, g)
             args += ["-ic", ic]
-        subprocess.run(args, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        subprocess.run(args, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, cwd=td)
         forces = np.loadtxt(os.path.join(td, "run.forces")).reshape(-1, 6)
         fin = O.load_restart(os.path.join(td, "run_final.bin"))
+    extra = {}
+    if files:
+        extra = {"file_names": np.array(list(files.keys())), "file_texts": np.array(list(files.values()))}
     np.savez_compressed(
         os.path.join(HERE, name + ".npz"),
         nx=nx, ny=ny, ngrid=ngrid, length=length, xoffset=xoff, yoffset=yoff, geom=geom, Re=Re, dt=dt,
         nsteps=nsteps, scheme=scheme, tol=tol,
         omega0=(w0 if w0 is not None else np.zeros((ngrid, nx - 1, ny - 1))),
-        forces=forces, omega=fin["omega"], q=fin["q"], f=fin["f"], timestep=fin["timestep"], time=fin["time"])
+        forces=forces, omega=fin["omega"], q=fin["q"], f=fin["f"], timestep=fin["timestep"], time=fin["time"],
+        **extra)
     print(name, "written", forces[-1, 2:4])
+
+
+# Every other `motion` type of the reference's geometry files (src/RigidBody.cc:349-493) on the
+# pitching-plate case above, its parameters chosen so that the 6 steps (t in [0, 0.06]) cross the
+# motions' branches and ramps.
+def _motion_table(t, seed):
+    rng = np.random.default_rng(seed)
+    rows = np.column_stack([t] + [np.cumsum(rng.uniform(-0.02, 0.02, len(t))) for _ in range(3)] +
+                           [rng.uniform(-1.0, 1.0, len(t)) for _ in range(3)])
+    return "%d\n" % len(t) + "".join(" ".join(repr(float(v)) for v in r) + "\n" for r in rows)
+
+
+MOTION_FILE = _motion_table(np.array([0.0, 0.008, 0.02, 0.033, 0.041, 0.05, 0.07]), 1)
+MOTION_FILE_PERIODIC = _motion_table(np.array([0.0, 0.007, 0.015, 0.022, 0.03]), 2)
+MOTION_CASES = [
+    # name, motion line, files
+    ("fixedvel", "fixedvel 0.4 -0.25 0.8", None),
+    ("sigmoidalstep", "sigmoidalstep 15 0.08 0.005", None),
+    ("lagstep1", "lagstep1 5 0.03 0.01 0.005", None),
+    ("lagstep2", "lagstep2 5 0.03 0.008 0.004", None),
+    ("eldredge", "eldredge 10 120 0.005 0.02 0.035 0.05", None),
+    ("eldredge1", "eldredge1 0.05 120 0.005 0.02 0.035 0.05", None),
+    ("eldredge2", "eldredge2 0.5 120 0.005 0.02 0.035 0.05", None),
+    ("eldredgecombined2", "eldredgecombined2 0.5 120 0.005 0.02 0.035 0.05 8 100 0.0 0.015 0.03 0.045", None),
+    ("motionfile", "motionfile plate.motion", {"plate.motion": MOTION_FILE}),
+    ("motionfileperiodic", "motionfileperiodic plate.motion 0.03", {"plate.motion": MOTION_FILE_PERIODIC}),
+]
+
+
+def run_motion(case):
+    kind, line, files = case
+    geom = configs.plate_geom(chord=1.0, npts=17, freq=0.5)
+    geom = "\n".join(("  motion " + line) if ln.strip().startswith("motion") else ln for ln in geom.splitlines()) + "\n"
+    run(("motion_" + kind, 64, 32, 2, 4.0, -2.0, -1.0, geom, 300.0, 0.01, 6, "rk3", 1e-10, None), files)
 
 
 # The other N(x) variants of the reference (src/IBSolver.cc:211-311) on one small two-domain case.
@@ -148,6 +192,9 @@ if __name__ == "__main__":
     for c in CASES:
         if not only or c[0] in only:
             run(c)
+    for c in MOTION_CASES:
+        if not only or "motion_" + c[0] in only:
+            run_motion(c)
     for c in VARIANTS:
         if not only or c[0] in only:
             run_variant(c)

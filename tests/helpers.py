@@ -31,17 +31,30 @@ def load_golden(name):
     return {k: (z[k].item() if z[k].ndim == 0 else z[k]) for k in z.files}
 
 
+def golden_geometry(d):
+    """The fixture's geometry, with the files its `motion` lines name (motion
+    files) written beside it first, as the reference reads them."""
+    import tempfile
+    from ibpm_b200 import geometry
+    if "file_names" not in d:
+        return geometry.parse(str(d["geom"]))
+    with tempfile.TemporaryDirectory() as td:
+        for name, text in zip(np.atleast_1d(d["file_names"]), np.atleast_1d(d["file_texts"])):
+            with open(os.path.join(td, str(name)), "w") as fh:
+                fh.write(str(text))
+        return geometry.parse(str(d["geom"]), td)
+
+
 def oracle_from_golden(d):
     from oracle import ibpm_oracle as O
     from ibpm_b200 import geometry
     g = O.Grid(int(d["nx"]), int(d["ny"]), int(d["ngrid"]), float(d["length"]), float(d["xoffset"]),
                float(d["yoffset"]))
-    geo = geometry.parse(str(d["geom"]))
+    geo = golden_geometry(d)
     bodies = []
     for b in geo.bodies:
-        motion = {0: "none", 1: "fixed", 2: "pitchplunge"}[b.motion]
-        params = b.params[:3] if motion == "fixed" else tuple(b.params)
-        bodies.append(O.Body(np.array(b.points, dtype=float), tuple(b.center), motion, params))
+        motion = geometry.MOTION_NAMES[b.motion]
+        bodies.append(O.Body(np.array(b.points, dtype=float), tuple(b.center), motion, tuple(b.params), b.table))
     model = O.Model(g, bodies, float(d["Re"]))
     solver = O.IBSolver(model, float(d["dt"]), str(d["scheme"]), float(d["tol"]))
     x = O.State(g, model.npts, omega=np.array(d["omega0"], dtype=float))

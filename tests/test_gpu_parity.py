@@ -8,7 +8,7 @@ reference library directly.  FP64 bar: relative L2 <= 1e-10 (operators
 import numpy as np
 import pytest
 
-from helpers import FP64_TOL, golden_names, load_golden, oracle_from_golden, rel_l2
+from helpers import FP64_TOL, golden_geometry, golden_names, load_golden, oracle_from_golden, rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -98,7 +98,7 @@ def test_time_step_matches_reference_golden(name):
     d = load_golden(name)
     grid = ib.Grid(int(d["nx"]), int(d["ny"]), int(d["ngrid"]), float(d["length"]), float(d["xoffset"]),
                    float(d["yoffset"]))
-    geo = ib.geometry.parse(str(d["geom"]))
+    geo = golden_geometry(d)
     model = ib.NavierStokesModel(grid, geo, float(d["Re"]))
     s = ib.NonlinearIBSolver(grid, model, float(d["dt"]), str(d["scheme"]), float(d["tol"]))
     x = ib.State(grid, geo.num_points, omega=np.array(d["omega0"], dtype=float))
