@@ -90,12 +90,15 @@ class State:
 @dataclass
 class NavierStokesModel:
     """NavierStokesModel(grid, geometry, Re, q_potential) (src/NavierStokesModel.h:35-122);
-    the base flow is uniform with magnitude `u_mag` and angle `alpha` (radians)."""
+    the base flow is uniform with magnitude `u_mag` and angle `alpha` (radians).
+    ``ubf=True`` is the CLI's unsteady base flow (src/ibpm.cc:166-178): the
+    single body's motion is carried by the base flow instead."""
     grid: Grid
     geom: _geometry.Geometry
     Re: float
     u_mag: float = 1.0
     alpha: float = 0.0
+    ubf: bool = False
 
     def getAlpha(self) -> float:
         return 1.0 / self.Re
@@ -145,6 +148,8 @@ class NonlinearIBSolver:
         self._h = h
         self.npoints = model.geom.num_points
         self._synced = None
+        if model.ubf:
+            check(L.ibg_set_moving_frame(h), h)
 
     # -- lifetime -----------------------------------------------------------
     def close(self):

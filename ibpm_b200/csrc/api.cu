@@ -144,6 +144,13 @@ struct ibg_context {
     double* d_mtab = nullptr;
     int nbodies = 0;
     bool stateful = false;
+    // moving-frame base flow: the first body's motion carried by the base flow
+    bool ubf = false;
+    BodyDev* d_bf = nullptr;
+    MotionState* d_bf_state = nullptr;
+    double* d_bfv = nullptr;   // (xdot', ydot', thetadot') of the flow
+    double* d_q0 = nullptr;    // the base flow on every level
+    double bf_xc = 0, bf_yc = 0;
     RegSlots slots;
     double* d_b = nullptr;
     double* d_time = nullptr;
@@ -335,7 +342,8 @@ struct ibg_context {
         if (lb.len) cudaFree(lb.len);
         if (lb.closed) cudaFree(lb.closed);
         lb = LpcBodies{};
-        void* ptrs[] = {d_ref, d_pts, d_vel, d_body_of, d_bodies, d_mstate, d_mstate_keep, d_mtab, slots.idx, slots.w, slots.n, d_b, d_time, f,
+        void* ptrs[] = {d_ref, d_pts, d_vel, d_body_of, d_bodies, d_mstate, d_mstate_keep, d_mtab, d_bf, d_bf_state, d_bfv, d_q0,
+                        slots.idx, slots.w, slots.n, d_b, d_time, f,
                         flux0, rhsb, btmp, d_status, cg_r, cg_d, cg_q, cg_scal, cg_flags, d_hist, d_hist_count, cg_z, cg_zold};
         for (void* p : ptrs)
             if (p) cudaFree(p);
@@ -359,6 +367,9 @@ struct ibg_context {
         d_bodies = nullptr;
         d_mstate = d_mstate_keep = nullptr;
         d_mtab = nullptr;
+        d_bf = nullptr;
+        d_bf_state = nullptr;
+        d_bfv = d_q0 = nullptr;
         slots = RegSlots{};
         d_b = d_time = f = flux0 = rhsb = btmp = nullptr;
         d_status = nullptr;
@@ -561,7 +572,7 @@ struct ibg_context {
     template <typename T>
     void refresh(Bulk<T>& B) {
         B.poisson.solve(call<T>(B, B.w, B.psi, (T)-1), st);
-        launch_refresh_flux<T>(g, B.psi, B.q, u0, v0, st);
+        launch_refresh_flux<T>(g, B.psi, B.q, u0, v0, ubf ? d_q0 : nullptr, st);
         launches += solve_launches() + 1;
     }
 
@@ -574,6 +585,14 @@ struct ibg_context {
         launch_kinematics(npts, d_ref, d_body_of, d_bodies, d_mstate, d_mtab, d_time, toff, d_pts, d_vel, st);
         launch_reg_update(g, npts, d_pts, d_vel, slots, d_b, u0, v0, st);
         launches += 2;
+    }
+
+    // BaseFlow::moveFlow(time + toff) (src/NavierStokesModel.cc:94) and the constraints it sets
+    void frame_flow(double toff) {
+        launch_frame_flow(d_bf, d_bf_state, d_mtab, d_time, toff, prm.u_mag, prm.alpha, d_bfv, st);
+        launch_frame_flux(g, d_bfv, bf_xc, bf_yc, d_q0, st);
+        launch_bcon_field(ncomp, slots, d_vel, d_q0, g.dx, d_b, st);
+        launches += 3;
     }
 
     // IBSolver::advanceSubstep (src/IBSolver.cc:162-198)
@@ -614,6 +633,7 @@ struct ibg_context {
             launch_nonlinear<T>(g, B.q, B.w, B.U, B.V, B.C, Nk, 1, S, F, st);
         }
         launches += 2 + g.L;
+        if (ubf) frame_flow(cn * prm.dt);
         if (moving) move_bodies(cn * prm.dt);
         const T* Nprev = nullptr;
         if (bn != 0) Nprev = old_saved ? Np : Nk;
@@ -1484,6 +1504,8 @@ int ibg_set_state(ibg_context* c, const double* omega, const double* q, const do
     if (q) {
         cudaMemcpyAsync(B.q, q, sizeof(double) * c->F, cudaMemcpyHostToDevice, c->st);
     } else {
+        // model->updateOperators(x.time); model->refreshState(x) (src/ibpm.cc:300-305)
+        if (c->ubf) c->frame_flow(0.0);
         if (c->moving) c->move_bodies(0.0);
         c->refresh<double>(B);
     }
@@ -1514,10 +1536,41 @@ int ibg_update_operators(ibg_context* c, double time) {
     // the state's own time stays as it is
     const double keep = c->time;
     cudaMemcpyAsync(c->d_time, &time, sizeof(double), cudaMemcpyHostToDevice, c->st);
+    if (c->ubf) c->frame_flow(0.0);
     if (c->moving) c->move_bodies(0.0);
     cudaMemcpyAsync(c->d_time, &keep, sizeof(double), cudaMemcpyHostToDevice, c->st);
     if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->cuda_check("ibg_update_operators");
     return c->cuda_check("ibg_update_operators");
+}
+
+int ibg_set_moving_frame(ibg_context* c) {
+    if (!c) return IBG_ERR_ARG;
+    if (c->nbodies != 1)
+        return c->fail(IBG_ERR_ARG, "ibg_set_moving_frame: the unsteady base flow needs exactly one body");
+    if (c->ubf) return IBG_OK;
+    BodyDev& b = c->h_bodies[0];
+    if (b.motion == IBG_MOTION_NONE || b.motion == IBG_MOTION_FIXED) return IBG_OK;  // stationary: flag ignored
+    if (c->chol_ready) return c->fail(IBG_ERR_STATE, "ibg_set_moving_frame: call before ibg_init");
+    c->drop_graph();  // a captured step of the moving body no longer applies
+    if (c->alloc(&c->d_bf, 1) || c->alloc(&c->d_bf_state, 1) || c->alloc(&c->d_bfv, 3) || c->alloc(&c->d_q0, c->F))
+        return IBG_ERR_CUDA;
+    // Geometry::transferMotion: the base flow takes a fresh copy of the motion, the body keeps none
+    cudaMemcpyAsync(c->d_bf, &b, sizeof(BodyDev), cudaMemcpyHostToDevice, c->st);
+    c->bf_xc = b.xc;
+    c->bf_yc = b.yc;
+    b.motion = IBG_MOTION_NONE;
+    cudaMemcpyAsync(c->d_bodies, &b, sizeof(BodyDev), cudaMemcpyHostToDevice, c->st);
+    c->moving = false;
+    c->stateful = false;
+    c->ubf = true;
+    // the body at its reference points; BaseFlow's initial field is the uniform flow (src/BaseFlow.cc:65-78)
+    c->move_bodies(0.0);
+    const double uv[3] = {c->u0, c->v0, 0.0};
+    cudaMemcpyAsync(c->d_bfv, uv, sizeof(uv), cudaMemcpyHostToDevice, c->st);
+    launch_frame_flux(c->g, c->d_bfv, c->bf_xc, c->bf_yc, c->d_q0, c->st);
+    launch_bcon_field(c->ncomp, c->slots, c->d_vel, c->d_q0, c->g.dx, c->d_b, c->st);
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->cuda_check("ibg_set_moving_frame");
+    return c->cuda_check("ibg_set_moving_frame");
 }
 
 int ibg_get_boundary(ibg_context* c, double* points, double* velocities) {
@@ -1782,8 +1835,8 @@ int ibg_ensemble_create(int n, ibg_context* const* members, ibg_ensemble** out) 
             g_ens_error = "ibg_ensemble_create: null member";
             return IBG_ERR_ARG;
         }
-        if (c->moving) {
-            g_ens_error = "ibg_ensemble_create: members must have fixed bodies (their step is one graph)";
+        if (c->moving || c->ubf) {
+            g_ens_error = "ibg_ensemble_create: members must have fixed bodies and a steady base flow";
             return IBG_ERR_UNSUPPORTED;
         }
         if (!c->chol_ready) {

@@ -46,7 +46,17 @@ void launch_laplacian(const GridDev& g, const T* w, T* out, cudaStream_t st);
 void launch_reg_gather(const GridDev& g, int ncomp, const RegSlots& s, const double* q0, double* out,
                        cudaStream_t st);
 template <typename T>
-void launch_refresh_flux(const GridDev& g, const T* psi, T* q, double u0, double v0, cudaStream_t st);
+// q = Curl(psi) + q0, q0 the uniform flow (u0, v0) dx_lev, or the field q0f (every level) when given
+void launch_refresh_flux(const GridDev& g, const T* psi, T* q, double u0, double v0, const double* q0f,
+                         cudaStream_t st);
+// Moving-frame base flow at time *time_ptr + toff: the flow's velocities
+// (xdot', ydot', thetadot') into out[3], the flux field q0 (all levels) from
+// them, and the constraints b = body velocity - E(q0).
+void launch_frame_flow(const BodyDev* bf, MotionState* ms, const double* mtab, const double* time_ptr, double toff,
+                       double magBF, double alphaBF, double* out, cudaStream_t st);
+void launch_frame_flux(const GridDev& g, const double* fv, double xc, double yc, double* q0, cudaStream_t st);
+void launch_bcon_field(int ncomp, const RegSlots& s, const double* vel, const double* q0, double h, double* bcon,
+                       cudaStream_t st);
 // Geometry::moveBodies at time *time_ptr + toff: advance the history of the
 // stateful motions (one thread per body), then move every point.
 void launch_motion_state(int nbodies, const BodyDev* bodies, const double* time_ptr, double toff, MotionState* ms,

@@ -10,6 +10,7 @@
 //   k_refresh_flux computeFlux = Curl(psi) + q0         src/NavierStokesModel.cc:114-125
 //   k_kinematics   RigidBody::moveBody + Motion        src/RigidBody.cc:586-609, src/Motion.h subclasses
 //   k_motion_state the history of FixedVelocity / Eldredge2 / EldredgeCombined2
+//   k_frame_flow / k_frame_flux / k_bcon_field  BaseFlow::moveFlow (moving frame), getConstraints
 //   k_reg_update   Regularizer::update                 src/Regularizer.cc:54-90
 //   k_reg_interp   Regularizer::toBoundary o Curl(psi) src/Regularizer.cc:111-128
 //   k_reg_smear/k_bf  Regularizer::toFlux, Curl, *beta  src/Regularizer.cc:92-109, src/ProjectionSolver.cc:87-90
@@ -327,7 +328,8 @@ __device__ __forceinline__ T curl_scalar_at(const GridDev& g, const T* f, const 
 
 // q = Curl(psi) + q0 on every level
 template <typename T>
-__global__ void k_refresh_flux(GridDev g, const T* __restrict__ psi, T* __restrict__ q, double u0, double v0) {
+__global__ void k_refresh_flux(GridDev g, const T* __restrict__ psi, T* __restrict__ q, double u0, double v0,
+                               const double* __restrict__ q0f) {
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= (size_t)g.L * g.F1) return;
     const int lev = (int)(tid / g.F1);
@@ -335,7 +337,7 @@ __global__ void k_refresh_flux(GridDev g, const T* __restrict__ psi, T* __restri
     const T* f = psi + (size_t)lev * g.N1;
     const T* c = (lev < g.L - 1) ? psi + (size_t)(lev + 1) * g.N1 : nullptr;
     const double dxl = lev_dx(g, lev);
-    const T base = (T)((idx < g.nXf ? u0 : v0) * dxl);
+    const T base = q0f ? (T)q0f[tid] : (T)((idx < g.nXf ? u0 : v0) * dxl);
     q[tid] = curl_scalar_at(g, f, c, idx) + base;
 }
 
@@ -517,6 +519,69 @@ __global__ void k_kinematics(int npts, const double* __restrict__ ref_xy, const 
     pts[2 * p + 1] = (y + a * s + bb * c) + b.yc;
     vel[2 * p] = -a * s * thd - bb * c * thd + xd;
     vel[2 * p + 1] = a * c * thd - bb * s * thd + yd;
+}
+
+// ---------------------------------------------------------------------------
+// moving-frame base flow: the body's motion carried by the base flow
+// (src/BaseFlow.cc:114-150 setAlphaMag / moveFlow, src/Flux.cc:101-129 setFlow)
+// ---------------------------------------------------------------------------
+// One thread: out = (xdot', ydot', thetadot') of the flow seen from the body.
+__global__ void k_frame_flow(const BodyDev* __restrict__ bf, MotionState* __restrict__ ms,
+                             const double* __restrict__ mtab, const double* __restrict__ time_ptr, double toff,
+                             double magBF, double alphaBF, double* __restrict__ out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double t = *time_ptr + toff;
+    const BodyDev b = *bf;
+    MotionState s = *ms;
+    advance_history(b, s, t);
+    *ms = s;
+    double x, y, th, xd, yd, thd;
+    body_frame(b, s, mtab, t, x, y, th, xd, yd, thd);
+    // setAlphaMag: the free stream relative to the moving body, in the body's frame
+    const double xdT = xd - magBF * cos(alphaBF);
+    const double ydT = yd - magBF * sin(alphaBF);
+    const double gamma = atan2(ydT, -1. * xdT);
+    const double alpha = -1. * th - gamma;
+    const double mag = sqrt(xdT * xdT + ydT * ydT);
+    out[0] = mag * cos(alpha);
+    out[1] = mag * sin(alpha);
+    out[2] = -1. * thd;
+}
+
+// Flux::setFlow: q0 = ((xdot' - thetadot' (y - yc)) dx, (ydot' + thetadot' (x - xc)) dx) at every flux of
+// every level, at the flux positions of Grid::getXEdge / getXCenter with zero shift (src/Grid.cc:104-139)
+__global__ void k_frame_flux(GridDev g, const double* __restrict__ fv, double xc, double yc, double* __restrict__ q0) {
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (size_t)g.L * g.F1) return;
+    const int lev = (int)(tid / g.F1);
+    const int idx = (int)(tid % g.F1);
+    const double dxl = lev_dx(g, lev);
+    const double offx = g.x0 + 0.5 * (0.0 - 1) * ((1 << lev) - 1) * (g.nx * g.dx);
+    const double offy = g.y0 + 0.5 * (0.0 - 1) * ((1 << lev) - 1) * (g.ny * g.dx);
+    const double xdot = fv[0], ydot = fv[1], thdot = fv[2];
+    if (idx < g.nXf) {
+        const int j = idx % g.ny;
+        const double yd = (offy + (j + 0.5) * dxl) - yc;
+        q0[tid] = (xdot - thdot * yd) * dxl;
+    } else {
+        const int i = (idx - g.nXf) / (g.ny + 1);
+        const double xd = (offx + (i + 0.5) * dxl) - xc;
+        q0[tid] = (ydot + thdot * xd) * dxl;
+    }
+}
+
+// getConstraints with a base-flow field: b_c = body velocity - Regularizer::toBoundary(q0)_c
+// (src/NavierStokesModel.cc:86-91, src/Regularizer.cc:111-128)
+__global__ void k_bcon_field(int ncomp, const int* __restrict__ sidx, const double* __restrict__ sw,
+                             const int* __restrict__ sn, const double* __restrict__ vel, const double* __restrict__ q0,
+                             double h, double* __restrict__ bcon) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncomp) return;
+    const int npts = ncomp / 2, dir = c / npts, p = c % npts;
+    double e = 0.0;
+    const int n = sn[c];
+    for (int k = 0; k < n; ++k) e = e + sw[(size_t)c * kSlots + k] * q0[sidx[(size_t)c * kSlots + k]];
+    bcon[c] = vel[2 * p + dir] - e / h;
 }
 
 __device__ __forceinline__ double delta_fn(double r) {
@@ -715,9 +780,25 @@ void launch_reg_gather(const GridDev& g, int ncomp, const RegSlots& s, const dou
 }
 
 template <typename T>
-void launch_refresh_flux(const GridDev& g, const T* psi, T* q, double u0, double v0, cudaStream_t st) {
+void launch_refresh_flux(const GridDev& g, const T* psi, T* q, double u0, double v0, const double* q0f,
+                         cudaStream_t st) {
     const size_t F = (size_t)g.L * g.F1;
-    k_refresh_flux<T><<<nblk(F, 256), 256, 0, st>>>(g, psi, q, u0, v0);
+    k_refresh_flux<T><<<nblk(F, 256), 256, 0, st>>>(g, psi, q, u0, v0, q0f);
+}
+
+void launch_frame_flow(const BodyDev* bf, MotionState* ms, const double* mtab, const double* time_ptr, double toff,
+                       double magBF, double alphaBF, double* out, cudaStream_t st) {
+    k_frame_flow<<<1, 32, 0, st>>>(bf, ms, mtab, time_ptr, toff, magBF, alphaBF, out);
+}
+
+void launch_frame_flux(const GridDev& g, const double* fv, double xc, double yc, double* q0, cudaStream_t st) {
+    const size_t F = (size_t)g.L * g.F1;
+    k_frame_flux<<<nblk(F, 256), 256, 0, st>>>(g, fv, xc, yc, q0);
+}
+
+void launch_bcon_field(int ncomp, const RegSlots& s, const double* vel, const double* q0, double h, double* bcon,
+                       cudaStream_t st) {
+    k_bcon_field<<<nblk(ncomp, 128), 128, 0, st>>>(ncomp, s.idx, s.w, s.n, vel, q0, h, bcon);
 }
 
 void launch_motion_state(int nbodies, const BodyDev* bodies, const double* time_ptr, double toff, MotionState* ms,
@@ -766,7 +847,7 @@ void launch_smear_bf_unit(const GridDev& g, int ncomp, int col0, int batch, cons
     template void launch_rhs<T>(const GridDev&, const T*, const T*, const T*, T*, double, double, double,      \
                                 double, cudaStream_t);                                                         \
     template void launch_laplacian<T>(const GridDev&, const T*, T*, cudaStream_t);                             \
-    template void launch_refresh_flux<T>(const GridDev&, const T*, T*, double, double, cudaStream_t);          \
+    template void launch_refresh_flux<T>(const GridDev&, const T*, T*, double, double, const double*, cudaStream_t);          \
     template void launch_reg_interp<T>(const GridDev&, int, const RegSlots&, const T*, size_t, int,            \
                                        const double*, double*, size_t, cudaStream_t);                          \
     template void launch_smear_bf<T>(const GridDev&, int, const RegSlots&, const double*, double*, T*, double, \

@@ -134,8 +134,20 @@ IBG_API int ibg_get_state(ibg_context* ctx, double* omega, double* q, double* f,
 /* only f, timestep and time (what the reference CLI reads every step) */
 IBG_API int ibg_get_boundary_force(ibg_context* ctx, double* f, int* timestep, double* time);
 /* NavierStokesModel::updateOperators(time) (src/NavierStokesModel.cc:93-99):
- * moves the bodies to `time`; the state's own time is unchanged. */
+ * moves the base flow (moving frame) and the bodies to `time`; the state's
+ * own time is unchanged. */
 IBG_API int ibg_update_operators(ibg_context* ctx, double time);
+/* The CLI's -ubf option (src/ibpm.cc:166-178): Geometry::transferMotion
+ * (src/Geometry.cc:48-71) and BaseFlow::setMotion/setCenter
+ * (src/BaseFlow.cc:104-112, src/BaseFlow.h:60).  The single body's motion
+ * moves to the base flow, which from then on is the free stream seen from the
+ * moving body plus its rotation about the body's centre (BaseFlow::setAlphaMag
+ * and moveFlow, Flux::setFlow; src/BaseFlow.cc:114-150, src/Flux.cc:101-129),
+ * recomputed at every sub-step; the body stays at its reference points, so
+ * the force solve is the fixed-body Cholesky one.  Call before ibg_init.  A
+ * stationary body leaves everything unchanged (the reference ignores the
+ * flag); more than one body is an error (the reference exits). */
+IBG_API int ibg_set_moving_frame(ibg_context* ctx);
 /* Geometry::getPoints / getVelocities (src/Geometry.cc:79-110) at the last
  * time the bodies were moved: 2 npoints values each in the BoundaryVector
  * layout (every x, then every y).  Either pointer may be NULL. */

@@ -872,11 +872,49 @@ class Model:
             self.q0[lev, g.n_xflux:] = v * dx
         self.npts = sum(b.ref_xy.shape[0] for b in bodies)
         self.time = 0.0
+        self.u_mag, self.alpha_bf = u_mag, alpha
+        self.frame = None      # the motion carried by the base flow (moving frame)
         self.move(0.0)
 
     @property
     def stationary(self) -> bool:
         return all(b.stationary for b in self.bodies)
+
+    @property
+    def time_dependent(self) -> bool:  # isTimeDependent (src/NavierStokesModel.cc:59-63)
+        return not self.stationary or self.frame is not None
+
+    def moving_frame(self) -> None:
+        """The CLI's -ubf (src/ibpm.cc:166-178): Geometry::transferMotion (src/Geometry.cc:48-71) gives a
+        fresh copy of the single moving body's motion to the base flow; the body keeps none."""
+        if len(self.bodies) != 1:
+            raise ValueError("the unsteady base flow needs exactly one body")
+        b = self.bodies[0]
+        if b.stationary:
+            return
+        self.frame = Body(b.ref_xy, b.center, b.motion, b.params, b.table)
+        self.bodies[0] = Body(b.ref_xy, b.center)
+        self.move(0.0)
+
+    def move_flow(self, t: float) -> None:
+        """BaseFlow::setAlphaMag + moveFlow (src/BaseFlow.cc:114-150) and Flux::setFlow (src/Flux.cc:101-129)."""
+        x, y, th, xd, yd, thd = self.frame.transformation(t)
+        xdT = xd - self.u_mag * math.cos(self.alpha_bf)
+        ydT = yd - self.u_mag * math.sin(self.alpha_bf)
+        gamma = math.atan2(ydT, -1.0 * xdT)
+        alpha = -1.0 * th - gamma
+        mag = math.sqrt(xdT * xdT + ydT * ydT)
+        u, v, w = mag * math.cos(alpha), mag * math.sin(alpha), -1.0 * thd
+        g = self.g
+        xc, yc = self.frame.center
+        for lev in range(g.ngrid):
+            dx = g.dx_lev(lev)
+            ycen = g.y_offset(lev) + (np.arange(g.ny) + 0.5) * dx     # x-flux y (getYCenter)
+            xcen = g.x_offset(lev) + (np.arange(g.nx) + 0.5) * dx     # y-flux x (getXCenter)
+            qx = np.broadcast_to((u - w * (ycen - yc)) * dx, (g.nx + 1, g.ny))
+            qy = np.broadcast_to(((v + w * (xcen - xc)) * dx)[:, None], (g.nx, g.ny + 1))
+            self.q0[lev, : g.n_xflux] = qx.reshape(-1)
+            self.q0[lev, g.n_xflux:] = qy.reshape(-1)
 
     def move(self, t: float) -> None:
         pts, vel = [], []
@@ -889,6 +927,8 @@ class Model:
         self.reg.update(self.points)
 
     def update_operators(self, t: float) -> None:  # src/NavierStokesModel.cc:93-99
+        if self.frame is not None:
+            self.move_flow(t)
         if not self.stationary:
             self.move(t)
 
@@ -1058,7 +1098,7 @@ class IBSolver:
                     a_f = a_f + bn * (sf["rhs_prev"] if sf["rhs_prev"] is not None else rhs)
                 sf["what"] = sf["what"] + a_f * self.dt
                 sf["rhs_prev"] = rhs
-            if not m.stationary:
+            if m.time_dependent:
                 m.update_operators(x.time + cn * self.dt)
             a = laplacian(g, x.omega) * (0.5 * m.alpha * (an + bn))
             a = a + an * n

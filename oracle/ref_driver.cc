@@ -14,11 +14,13 @@
 //                   -nsteps K [-tol T] [-alpha DEG] [-ic restart.bin]
 //                   [-out PREFIX] [-dump_every K] [-warmup W] [-cholesky_cache BASENAME]
 //                   [-model nonlinear|linear|adjoint|linearperiodic|sfd] [-baseflow FILE]
-//                   [-pbase PREFIX -period P] [-chi X -Delta X]
+//                   [-pbase PREFIX -period P] [-chi X -Delta X] [-ubf 1]
 // -model selects the solver class as the CLI does (src/ibpm.cc:184-229): the
 // linear models get a NavierStokesModel without base flow and the base state(s)
 // from restart files (FILE, or PREFIX_<k>.bin for k < P); sfd reads its filtered
 // state like the CLI (loadFilteredState of the initial condition's name).
+// -ubf 1 hands the single body's motion to the base flow as the CLI's -ubf
+// does (src/ibpm.cc:166-178, :300-303).
 #include "ibpm.h"
 #include <chrono>
 #include <cstdlib>
@@ -39,7 +41,7 @@ int main(int argc, char* argv[]) {
     int nx = 200, ny = 200, ngrid = 1, nsteps = 10, dumpEvery = 0, warmup = 0;
     double length = 4, xoff = -2, yoff = -2, Re = 100, dt = 0.01, tol = 1e-7, alphaDeg = 0;
     std::string geomFile, scheme = "rk3", ic, out, cache, modelName = "nonlinear", baseFile, pbase;
-    int period = 1;
+    int period = 1, ubf = 0;
     double chi = 0.02, Delta = 15.;
     for (int a = 1; a + 1 < argc; a += 2) {
         std::string k = argv[a];
@@ -68,6 +70,7 @@ int main(int argc, char* argv[]) {
         else if (k == "-period") period = atoi(v);
         else if (k == "-chi") chi = atof(v);
         else if (k == "-Delta") Delta = atof(v);
+        else if (k == "-ubf") ubf = atoi(v);
         else { std::cerr << "unknown flag " << k << std::endl; return 2; }
     }
     Scheme::SchemeType st = Scheme::RK3;
@@ -81,6 +84,14 @@ int main(int argc, char* argv[]) {
     double pi = 4. * atan(1.);
     double alpha = alphaDeg * pi / 180.;
     BaseFlow q_potential(grid, 1.0, alpha);
+    if (ubf && !geom.isStationary() && geom.getNumBodies() == 1) {
+        Motion* m = geom.transferMotion();
+        double xC = 0, yC = 0;
+        geom.transferCenter(xC, yC);
+        q_potential.setMotion(*m);
+        q_potential.setCenter(xC, yC);
+    }
+    if (ubf && geom.getNumBodies() != 1) { std::cerr << "-ubf needs exactly one body\n"; return 2; }
     const bool linear = modelName == "linear" || modelName == "linearperiodic" || modelName == "adjoint";
     NavierStokesModel* mp = linear ? new NavierStokesModel(grid, geom, Re) : new NavierStokesModel(grid, geom, Re, q_potential);
     NavierStokesModel& model = *mp;
@@ -128,6 +139,7 @@ int main(int argc, char* argv[]) {
         if (!cache.empty()) solver.save(cache);
     }
     double tInit = now_s() - t0;
+    if (!q_potential.isStationary()) q_potential.setAlphaMag(x.time);
     model.updateOperators(x.time);
     model.refreshState(x);
 

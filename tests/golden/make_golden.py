@@ -42,9 +42,10 @@ CASES = [
 ]
 
 
-def run(case, files=None):
+def run(case, files=None, ubf=False):
     """files: {name: text} written beside the geometry file; the driver runs
-    there, so a `motion motionfile NAME` line finds NAME as the reference does."""
+    there, so a `motion motionfile NAME` line finds NAME as the reference does.
+    ubf: the body's motion is carried by the base flow (the CLI's -ubf)."""
     name, nx, ny, ngrid, length, xoff, yoff, geom, Re, dt, nsteps, scheme, tol, noise = case
     files = files or {}
     with tempfile.TemporaryDirectory() as td:
@@ -57,7 +58,7 @@ def run(case, files=None):
         args = [DRIVER, "-nx", str(nx), "-ny", str(ny), "-ngrid", str(ngrid), "-length", repr(length),
                 "-xoffset", repr(xoff), "-yoffset", repr(yoff), "-geom", gpath, "-Re", repr(Re),
                 "-dt", repr(dt), "-scheme", scheme, "-nsteps", str(nsteps), "-tol", repr(tol),
-                "-out", os.path.join(td, "run")]
+                "-out", os.path.join(td, "run")] + (["-ubf", "1"] if ubf else [])
         w0 = None
         if noise is not None:
             wl = configs.Workload(name, nx, ny, ngrid, length, xoff, yoff, geom, Re, dt, nsteps,
@@ -73,9 +74,9 @@ def run(case, files=None):
         subprocess.run(args, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, cwd=td)
         forces = np.loadtxt(os.path.join(td, "run.forces")).reshape(-1, 6)
         fin = O.load_restart(os.path.join(td, "run_final.bin"))
-    extra = {}
+    extra = {"ubf": 1} if ubf else {}
     if files:
-        extra = {"file_names": np.array(list(files.keys())), "file_texts": np.array(list(files.values()))}
+        extra.update(file_names=np.array(list(files.keys())), file_texts=np.array(list(files.values())))
     np.savez_compressed(
         os.path.join(HERE, name + ".npz"),
         nx=nx, ny=ny, ngrid=ngrid, length=length, xoffset=xoff, yoffset=yoff, geom=geom, Re=Re, dt=dt,
@@ -113,11 +114,23 @@ MOTION_CASES = [
 ]
 
 
-def run_motion(case):
+def run_motion(case, ubf=False):
     kind, line, files = case
     geom = configs.plate_geom(chord=1.0, npts=17, freq=0.5)
     geom = "\n".join(("  motion " + line) if ln.strip().startswith("motion") else ln for ln in geom.splitlines()) + "\n"
-    run(("motion_" + kind, 64, 32, 2, 4.0, -2.0, -1.0, geom, 300.0, 0.01, 6, "rk3", 1e-10, None), files)
+    name = ("ubf_" if ubf else "motion_") + kind
+    run((name, 64, 32, 2, 4.0, -2.0, -1.0, geom, 300.0, 0.01, 6, "rk3", 1e-10, None), files, ubf)
+
+
+# The unsteady base flow (the CLI's -ubf): the same plate, its motion carried by the base flow, so the
+# force solve is the fixed-body Cholesky one; stateful and rotating motions among them.
+UBF_CASES = [
+    ("pitchplunge", "pitchplunge -0.3 0.5 0 0.25 0.5 0", None),
+    ("fixedvel", "fixedvel 0.4 -0.25 0.8", None),
+    ("eldredge2", "eldredge2 0.5 120 0.005 0.02 0.035 0.05", None),
+    ("eldredgecombined2", "eldredgecombined2 0.5 120 0.005 0.02 0.035 0.05 8 100 0.0 0.015 0.03 0.045", None),
+    ("motionfile", "motionfile plate.motion", {"plate.motion": MOTION_FILE}),
+]
 
 
 # The other N(x) variants of the reference (src/IBSolver.cc:211-311) on one small two-domain case.
@@ -195,6 +208,9 @@ if __name__ == "__main__":
     for c in MOTION_CASES:
         if not only or "motion_" + c[0] in only:
             run_motion(c)
+    for c in UBF_CASES:
+        if not only or "ubf_" + c[0] in only:
+            run_motion(c, ubf=True)
     for c in VARIANTS:
         if not only or c[0] in only:
             run_variant(c)

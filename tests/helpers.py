@@ -56,6 +56,8 @@ def oracle_from_golden(d):
         motion = geometry.MOTION_NAMES[b.motion]
         bodies.append(O.Body(np.array(b.points, dtype=float), tuple(b.center), motion, tuple(b.params), b.table))
     model = O.Model(g, bodies, float(d["Re"]))
+    if int(d.get("ubf", 0)):
+        model.moving_frame()
     solver = O.IBSolver(model, float(d["dt"]), str(d["scheme"]), float(d["tol"]))
     x = O.State(g, model.npts, omega=np.array(d["omega0"], dtype=float))
     return g, model, solver, x

@@ -99,7 +99,7 @@ def test_time_step_matches_reference_golden(name):
     grid = ib.Grid(int(d["nx"]), int(d["ny"]), int(d["ngrid"]), float(d["length"]), float(d["xoffset"]),
                    float(d["yoffset"]))
     geo = golden_geometry(d)
-    model = ib.NavierStokesModel(grid, geo, float(d["Re"]))
+    model = ib.NavierStokesModel(grid, geo, float(d["Re"]), ubf=bool(int(d.get("ubf", 0))))
     s = ib.NonlinearIBSolver(grid, model, float(d["dt"]), str(d["scheme"]), float(d["tol"]))
     x = ib.State(grid, geo.num_points, omega=np.array(d["omega0"], dtype=float))
     s.init()

@@ -9,7 +9,9 @@ motion against fixtures the reference wrote runs with the other golden cases
 GPU: the device kinematics (positions and velocities of every boundary point)
 against the oracle over a sequence of update times, including the history of
 the stateful motions and motion-file ends; the learned preconditioner's
-configuration sampling leaves that history untouched.
+configuration sampling leaves that history untouched; the moving-frame base
+flow (-ubf) refuses more than one body and ignores a fixed one.  Its
+time-step parity runs with the golden cases (tests/golden/ubf_*.npz).
 """
 import math
 
@@ -159,4 +161,46 @@ def test_configuration_sampling_keeps_motion_history(kind):
     assert rel_l2(s.force_history(n), d["forces"][:, 2:4]) < FP64_TOL
     s.get_state(x)
     assert rel_l2(x.omega, d["omega"]) < FP64_TOL
+    s.close()
+
+
+def test_oracle_moving_frame_flow_is_the_relative_free_stream():
+    """-ubf with a translating body: the base flow is the free stream minus the body's velocity, in the
+    body's frame; the body itself stays at its reference points."""
+    g = O.Grid(32, 16, 2, 4.0, -2.0, -1.0)
+    b = O.Body(np.array([[0.0, 0.0], [0.5, 0.0]]), (0.0, 0.0), "fixedvel", (0.4, -0.25, 0.0))
+    m = O.Model(g, [b], 100.0)
+    m.moving_frame()
+    assert m.stationary and m.time_dependent
+    m.update_operators(0.3)
+    for lev in range(g.ngrid):
+        dx = g.dx_lev(lev)
+        assert np.allclose(m.q0[lev, : g.n_xflux], 0.6 * dx, rtol=0, atol=1e-15)
+        assert np.allclose(m.q0[lev, g.n_xflux:], 0.25 * dx, rtol=0, atol=1e-15)
+    assert np.array_equal(m.points, b.ref_xy)
+    with pytest.raises(ValueError):
+        O.Model(g, [b, O.Body(np.array([[1.0, 0.5]]))], 100.0).moving_frame()
+
+
+@pytest.mark.gpu
+def test_moving_frame_needs_one_body_and_ignores_a_fixed_one():
+    """ibg_set_moving_frame refuses two bodies, as the reference CLI exits; a fixed body keeps the
+    steady base flow (the reference ignores the flag) and the run stays the reference's."""
+    import ibpm_b200 as ib
+    d = load_golden("cyl_l1_rk3")
+    grid = ib.Grid(int(d["nx"]), int(d["ny"]), int(d["ngrid"]), float(d["length"]), float(d["xoffset"]),
+                   float(d["yoffset"]))
+    geo = golden_geometry(d)
+    two = G.Geometry(geo.bodies + [G.RigidBody(points=[(1.5, 1.5)], motion=G.MOTION_FIXEDVEL,
+                                               params=(0.1, 0.0, 0.0))])
+    with pytest.raises(ib.IbgError):
+        ib.NonlinearIBSolver(grid, ib.NavierStokesModel(grid, two, float(d["Re"]), ubf=True), float(d["dt"]))
+    s = ib.NonlinearIBSolver(grid, ib.NavierStokesModel(grid, geo, float(d["Re"]), ubf=True), float(d["dt"]),
+                             str(d["scheme"]), float(d["tol"]))
+    x = ib.State(grid, geo.num_points, omega=np.array(d["omega0"], dtype=float))
+    s.init()
+    s.set_state(x, with_q=False)
+    n = int(d["nsteps"])
+    s.advance_resident(n)
+    assert rel_l2(s.force_history(n), d["forces"][:, 2:4]) < FP64_TOL
     s.close()
