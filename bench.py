@@ -22,9 +22,12 @@ Workloads (seeded synthetic inputs; no dataset is involved):
 
 One process per GPU (torchrun for N > 1).  One simulation does not shard
 (its multi-domain solve is global per level and levels are serially
-dependent), so N GPUs run N independent replicas (weak scaling) and `value`
-is the total timesteps/s of the job (member-timesteps/s for c4).  Rank 0
-prints one JSON line.
+dependent), so for c2 and c3 N GPUs run N independent replicas (weak
+scaling) and `value` is the total timesteps/s of the job.  The c4 ensemble
+shards by member (rank r advances members r, r + N, ...; strong scaling,
+no exchange while they run, one all-gather of the force histories at the
+end) and `value` is member-timesteps/s of all 64.  Rank 0 prints one JSON
+line.
 
 * value        K steps with the state resident in HBM, CUDA events around each
                step on the stream it runs on, L2 flushed (256 MB write) between
@@ -333,13 +336,18 @@ class Single:
 class Ens:
     """The 64-member ensemble (c4): one graph (ensemble) or member after member (serial)."""
 
-    def __init__(self, form, stream, device, count=64):
+    def __init__(self, form, stream, device, count=64, world_size=1, rank=0):
         import ibpm_b200 as ib
         from ibpm_b200 import configs
+        from ibpm_b200.replicas import shard
         import torch
         self.members = []
+        self.total = count
+        self.device = torch.device("cuda", device)
         prec = "fp32" if form == "ensemble_fp32" else "fp64"
-        for wl in configs.ensemble_members(count=count):
+        everyone = configs.ensemble_members(count=count)
+        # with several GPUs the members shard over the ranks (no exchange while they run)
+        for wl in [everyone[i] for i in shard(count, world_size, rank)]:
             grid, model, s, x = ib.from_workload(wl, stream=stream.cuda_stream, device=device, precision=prec)
             s.init()
             s.set_state(x, with_q=False)
@@ -351,7 +359,7 @@ class Ens:
         if form.startswith("ensemble"):
             self.ens = ib.Ensemble([m[2] for m in self.members])
             self.stream = torch.cuda.ExternalStream(self.ens.stream(), device=torch.device("cuda", device))
-        self.extra = {"members": len(self.members),
+        self.extra = {"members": count, "members_on_rank0": len(self.members),
                       "grid_points_all_levels": int(sum(w.nx * w.ny * w.ngrid for w, *_ in self.members)),
                       "boundary_points": [int(m[3].f.size // 2) for m in self.members][:8] + ["..."]}
 
@@ -366,8 +374,11 @@ class Ens:
         return n
 
     def forces(self, K):
+        """every member's force history, in member order (one all-gather over the ranks)"""
         import numpy as np
-        return np.concatenate([m[2].force_history(K) for m in self.members])
+        from ibpm_b200.replicas import gather_histories
+        local = np.stack([m[2].force_history(K) for m in self.members])
+        return gather_histories(local, self.total, device=self.device).reshape(-1, 2)
 
     def e2e(self, Ke, sync):
         import torch
@@ -406,6 +417,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4"])
     ap.add_argument("--form", default=None)
+    ap.add_argument("--members", type=int, default=64, help="c4: ensemble members (the workload has 64)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-path comparison run")
     ap.add_argument("--profile", action="store_true",
@@ -438,7 +450,9 @@ def main():
 
     def build(f):
         stream = torch.cuda.Stream(device=dev)
-        return Ens(f, stream, local) if wlname == "c4" else Single(wlname, f, stream, local)
+        if wlname == "c4":
+            return Ens(f, stream, local, count=args.members, world_size=ws, rank=rank)
+        return Single(wlname, f, stream, local)
 
     from ibpm_b200.replicas import job_throughput, max_over_ranks
 
@@ -465,8 +479,10 @@ def main():
         torch.cuda.cudart().cudaProfilerStop()
     clk = clocks.stop()
     ms = maxrank(ms)
-    per_step_units = len(run.members) if wlname == "c4" else 1
-    value = job_throughput(ws, K, per_step_units, ms)
+    # units the whole job advances per step: every ensemble member (sharded over the ranks), or one
+    # replica per rank
+    job_units = run.total if wlname == "c4" else ws
+    value = job_throughput(1, K, job_units, ms)
     forces = run.forces(W + K)
     cg = None
     if it0 is not None:
@@ -485,7 +501,7 @@ def main():
     Ke = min(K, 20 if wlname != "c2" else 50)
     e2e_s, bi, bo = run.e2e(Ke, sync)
     e2e_s = maxrank(e2e_s)
-    e2e = {"value": job_throughput(ws, Ke, per_step_units, 1000.0 * e2e_s), "unit": UNIT, "h2d_bytes_per_step": bi,
+    e2e = {"value": job_throughput(1, Ke, job_units, 1000.0 * e2e_s), "unit": UNIT, "h2d_bytes_per_step": bi,
            "d2h_bytes_per_step": bo}
     roof = kernel_roofline(*run.roof_solver(), dtype="float" if form == "fp32" else "double")
     if wlname == "c2" and form == "fp64":
@@ -508,7 +524,7 @@ def main():
         pms, _ = time_steps(K, p.stream, p.step, flush)
         pms = maxrank(pms)
         pforces = p.forces(W + K)
-        plain = {"form": PLAIN[wlname], "value": job_throughput(ws, K, per_step_units, pms), "ms_per_step": pms / K,
+        plain = {"form": PLAIN[wlname], "value": job_throughput(1, K, job_units, pms), "ms_per_step": pms / K,
                  "force_rel_l2_vs_plain": rel_l2(forces, pforces)}
         if pit0 is not None:
             pit1 = p.iterations()
@@ -520,8 +536,8 @@ def main():
         wl = getattr(run, "wl", None)
         dtype = {"fp32": "f32+f64", "ensemble_fp32": "f32+f64"}.get(form, "f64")
         out = {"metric": METRICS[wlname], "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
-               "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-               "dtype": dtype, "data": "synthetic (seeded initial conditions and generated geometry)",
+               "ms_per_step": ms / K, "higher_is_better": True,
+               "scaling": "strong" if wlname == "c4" else "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded initial conditions and generated geometry)",
                "config": _config(wlname, form, wl, extra), "e2e": e2e, "gpu_launches": int(launches),
                "roofline": roof, "clocks": clk,
                "final_force": [float(forces[-1][0]), float(forces[-1][1])] if len(forces) else None}

@@ -260,6 +260,15 @@ class NonlinearIBSolver:
     def update_operators(self, time: float):
         check(lib().ibg_update_operators(self._h, float(time)), self._h)
 
+    def flux_to_velocity(self):
+        """FluxToVelocity of the device state's flux: node velocities (u, v), each (ngrid, nx-1, ny-1);
+        0 on the coarse interior nodes the reference leaves undefined."""
+        g = self.grid
+        u = np.empty((g.ngrid, g.nx - 1, g.ny - 1))
+        v = np.empty_like(u)
+        check(lib().ibg_flux_to_velocity(self._h, _ptr(u), _ptr(v)), self._h)
+        return u, v
+
     def boundary(self):
         """Geometry::getPoints / getVelocities at the last time the bodies were
         moved, as (npoints, 2) arrays of positions and velocities."""

@@ -54,6 +54,7 @@ SIGNATURES = {
     "ibg_get_boundary_force": (_I, [_VP, _VP, ctypes.POINTER(_I), ctypes.POINTER(_D)]),
     "ibg_update_operators": (_I, [_VP, _D]),
     "ibg_get_boundary": (_I, [_VP, _VP, _VP]),
+    "ibg_flux_to_velocity": (_I, [_VP, _VP, _VP]),
     "ibg_set_moving_frame": (_I, [_VP]),
     "ibg_refresh_state": (_I, [_VP]),
     "ibg_advance": (_I, [_VP, _I]),

@@ -1573,6 +1573,17 @@ int ibg_set_moving_frame(ibg_context* c) {
     return c->cuda_check("ibg_set_moving_frame");
 }
 
+int ibg_flux_to_velocity(ibg_context* c, double* u, double* v) {
+    if (!c || !u || !v) return IBG_ERR_ARG;
+    c->to64();
+    // the FP64 node buffers of the nonlinear term are free between steps
+    launch_flux_to_vel(c->g, c->b64.q, c->b64.U, c->b64.V, c->st);
+    cudaMemcpyAsync(u, c->b64.U, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
+    cudaMemcpyAsync(v, c->b64.V, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->cuda_check("ibg_flux_to_velocity");
+    return c->cuda_check("ibg_flux_to_velocity");
+}
+
 int ibg_get_boundary(ibg_context* c, double* points, double* velocities) {
     if (!c) return IBG_ERR_ARG;
     const size_t n = (size_t)c->npts;

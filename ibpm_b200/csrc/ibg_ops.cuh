@@ -49,6 +49,8 @@ template <typename T>
 // q = Curl(psi) + q0, q0 the uniform flow (u0, v0) dx_lev, or the field q0f (every level) when given
 void launch_refresh_flux(const GridDev& g, const T* psi, T* q, double u0, double v0, const double* q0f,
                          cudaStream_t st);
+// FluxToVelocity: node velocities u, v of every level (0 where undefined)
+void launch_flux_to_vel(const GridDev& g, const double* q, double* u, double* v, cudaStream_t st);
 // Moving-frame base flow at time *time_ptr + toff: the flow's velocities
 // (xdot', ydot', thetadot') into out[3], the flux field q0 (all levels) from
 // them, and the constraints b = body velocity - E(q0).

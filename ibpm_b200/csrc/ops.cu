@@ -117,6 +117,22 @@ __global__ void k_node_vel(GridDev g, const T* __restrict__ q, const T* __restri
     V[sb + tid] = dv ? v * wv : (T)0;
 }
 
+// FluxToVelocity (src/VectorOperations.cc:924-927): u and v at every node of every level, 0 on the
+// coarse interior overlap nodes the reference leaves undefined
+__global__ void k_flux_to_vel(GridDev g, const double* __restrict__ q, double* __restrict__ u,
+                              double* __restrict__ v) {
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (size_t)g.L * g.N1) return;
+    const int lev = (int)(tid / g.N1);
+    const int r = (int)(tid % g.N1);
+    const int i = r / g.NJ + 1, j = r % g.NJ + 1;
+    double uu, vv;
+    bool du, dv;
+    node_uv(g, q + (size_t)lev * g.F1, lev, i, j, uu, vv, du, dv);
+    u[tid] = du ? uu : 0.0;
+    v[tid] = dv ? vv : 0.0;
+}
+
 // LinearizedIBSolver / LinearizedPeriodicIBSolver node products (src/IBSolver.cc:211-216, 224-232):
 // CrossProduct(q0, omega) + CrossProduct(q, omega0) before the flux stencils (which are linear),
 // with the base state of phase (timestep % period); the step counter lives on the device
@@ -784,6 +800,11 @@ void launch_refresh_flux(const GridDev& g, const T* psi, T* q, double u0, double
                          cudaStream_t st) {
     const size_t F = (size_t)g.L * g.F1;
     k_refresh_flux<T><<<nblk(F, 256), 256, 0, st>>>(g, psi, q, u0, v0, q0f);
+}
+
+void launch_flux_to_vel(const GridDev& g, const double* q, double* u, double* v, cudaStream_t st) {
+    const size_t S = (size_t)g.L * g.N1;
+    k_flux_to_vel<<<nblk(S, 256), 256, 0, st>>>(g, q, u, v);
 }
 
 void launch_frame_flow(const BodyDev* bf, MotionState* ms, const double* mtab, const double* time_ptr, double toff,

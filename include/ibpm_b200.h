@@ -152,6 +152,11 @@ IBG_API int ibg_set_moving_frame(ibg_context* ctx);
  * time the bodies were moved: 2 npoints values each in the BoundaryVector
  * layout (every x, then every y).  Either pointer may be NULL. */
 IBG_API int ibg_get_boundary(ibg_context* ctx, double* points, double* velocities);
+/* FluxToVelocity(q, u, v) (src/VectorOperations.cc:924-927) of the device
+ * state's flux: the node velocities OutputTecplot writes
+ * (src/OutputTecplot.cc:41-47), S values each in the Scalar layout.  The
+ * coarse-level interior nodes the reference leaves uninitialised are 0. */
+IBG_API int ibg_flux_to_velocity(ibg_context* ctx, double* u, double* v);
 IBG_API int ibg_refresh_state(ibg_context* ctx);
 
 /* --- restart files ------------------------------------------------------------

@@ -14,13 +14,14 @@
 //                   -nsteps K [-tol T] [-alpha DEG] [-ic restart.bin]
 //                   [-out PREFIX] [-dump_every K] [-warmup W] [-cholesky_cache BASENAME]
 //                   [-model nonlinear|linear|adjoint|linearperiodic|sfd] [-baseflow FILE]
-//                   [-pbase PREFIX -period P] [-chi X -Delta X] [-ubf 1]
+//                   [-pbase PREFIX -period P] [-chi X -Delta X] [-ubf 1] [-tecplot PREFIX]
 // -model selects the solver class as the CLI does (src/ibpm.cc:184-229): the
 // linear models get a NavierStokesModel without base flow and the base state(s)
 // from restart files (FILE, or PREFIX_<k>.bin for k < P); sfd reads its filtered
 // state like the CLI (loadFilteredState of the initial condition's name).
 // -ubf 1 hands the single body's motion to the base flow as the CLI's -ubf
-// does (src/ibpm.cc:166-178, :300-303).
+// does (src/ibpm.cc:166-178, :300-303).  -tecplot PREFIX writes the final
+// state as the CLI's Tecplot output of every level, PREFIX<step>_g<lev>.plt.
 #include "ibpm.h"
 #include <chrono>
 #include <cstdlib>
@@ -40,7 +41,7 @@ static double now_s() {
 int main(int argc, char* argv[]) {
     int nx = 200, ny = 200, ngrid = 1, nsteps = 10, dumpEvery = 0, warmup = 0;
     double length = 4, xoff = -2, yoff = -2, Re = 100, dt = 0.01, tol = 1e-7, alphaDeg = 0;
-    std::string geomFile, scheme = "rk3", ic, out, cache, modelName = "nonlinear", baseFile, pbase;
+    std::string geomFile, scheme = "rk3", ic, out, cache, modelName = "nonlinear", baseFile, pbase, tec;
     int period = 1, ubf = 0;
     double chi = 0.02, Delta = 15.;
     for (int a = 1; a + 1 < argc; a += 2) {
@@ -71,6 +72,7 @@ int main(int argc, char* argv[]) {
         else if (k == "-chi") chi = atof(v);
         else if (k == "-Delta") Delta = atof(v);
         else if (k == "-ubf") ubf = atoi(v);
+        else if (k == "-tecplot") tec = v;
         else { std::cerr << "unknown flag " << k << std::endl; return 2; }
     }
     Scheme::SchemeType st = Scheme::RK3;
@@ -165,6 +167,12 @@ int main(int argc, char* argv[]) {
     }
     if (ff) fclose(ff);
     if (!out.empty()) x.save(out + "_final.bin");
+    if (!tec.empty()) {
+        // the CLI's Tecplot output with -tecplotallgrids (src/ibpm.cc:310-311) of the final state
+        OutputTecplot tecplot(tec + "%05d.plt", "Test run, step%05d", true);
+        tecplot.setFilename(tec + "%05d_g%01d.plt");
+        tecplot.doOutput(x);
+    }
     printf("{\"init_s\": %.6f, \"timed_steps\": %d, \"step_s\": %.6f, \"steps_per_s\": %.6f}\n",
            tInit, timed, tSteps, timed > 0 ? timed / tSteps : 0.0);
     return 0;

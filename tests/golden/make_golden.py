@@ -42,6 +42,10 @@ CASES = [
 ]
 
 
+# cases whose final state the reference also writes as Tecplot files of every level (-tecplot)
+TECPLOT_CASES = {"cyl_l3_noise_rk3"}
+
+
 def run(case, files=None, ubf=False):
     """files: {name: text} written beside the geometry file; the driver runs
     there, so a `motion motionfile NAME` line finds NAME as the reference does.
@@ -59,6 +63,8 @@ def run(case, files=None, ubf=False):
                 "-xoffset", repr(xoff), "-yoffset", repr(yoff), "-geom", gpath, "-Re", repr(Re),
                 "-dt", repr(dt), "-scheme", scheme, "-nsteps", str(nsteps), "-tol", repr(tol),
                 "-out", os.path.join(td, "run")] + (["-ubf", "1"] if ubf else [])
+        if name in TECPLOT_CASES:
+            args += ["-tecplot", os.path.join(td, "tec")]
         w0 = None
         if noise is not None:
             wl = configs.Workload(name, nx, ny, ngrid, length, xoff, yoff, geom, Re, dt, nsteps,
@@ -74,7 +80,14 @@ def run(case, files=None, ubf=False):
         subprocess.run(args, check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, cwd=td)
         forces = np.loadtxt(os.path.join(td, "run.forces")).reshape(-1, 6)
         fin = O.load_restart(os.path.join(td, "run_final.bin"))
+        tecs = []
+        if name in TECPLOT_CASES:
+            for lev in range(ngrid):
+                with open(os.path.join(td, "tec%05d_g%01d.plt" % (nsteps, lev))) as fh:
+                    tecs.append(fh.read())
     extra = {"ubf": 1} if ubf else {}
+    if name in TECPLOT_CASES:
+        extra["tecplot_texts"] = np.array(tecs)
     if files:
         extra.update(file_names=np.array(list(files.keys())), file_texts=np.array(list(files.values())))
     np.savez_compressed(
