@@ -88,6 +88,7 @@ namespace ibg {
 // [4] solves, [5] largest count, [6] solves that hit the cap, [7] loop counter.
 // The loop also stops after cap + 2 passes whatever the solver flags say.
 __global__ void k_cg_loop_cond(cudaGraphConditionalHandle h, int* flags) {
+    pdl_enter();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     const int loops = flags[7] + 1;
     flags[7] = loops;
@@ -102,11 +103,13 @@ __global__ void k_cg_loop_cond(cudaGraphConditionalHandle h, int* flags) {
     cudaGraphSetConditional(h, more ? 1u : 0u);
 }
 __global__ void k_cg_loop_reset(int* flags) {
+    pdl_enter();
     if (threadIdx.x == 0 && blockIdx.x == 0) flags[7] = 0;
 }
 
 template <typename A, typename B>
 __global__ void k_convert(size_t n, const A* __restrict__ in, B* __restrict__ out) {
+    pdl_enter();
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = (B)in[i];
 }
@@ -428,7 +431,7 @@ struct ibg_context {
         } else {
             cg_begin(ncomp, b, cg_q, cg_r, cg_d, cg_scal, cg_flags, st);
         }
-        k_cg_loop_reset<<<1, 1, 0, st>>>(cg_flags);
+        launch_k(k_cg_loop_reset, 1, 1, 0, st, cg_flags);
         launches += pc ? 3 : 2;
         cudaStreamCaptureStatus cs;
         unsigned long long id = 0;
@@ -466,7 +469,7 @@ struct ibg_context {
         } else {
             cg_update(ncomp, x, cg_r, cg_d, cg_q, cg_scal, cg_flags, st);
         }
-        k_cg_loop_cond<<<1, 1, 0, st>>>(h, cg_flags);
+        launch_k(k_cg_loop_cond, 1, 1, 0, st, h, cg_flags);
         st = main;
         cudaGraph_t out = nullptr;
         if (cudaStreamEndCapture(side, &out) != cudaSuccess) return cuda_check("cg graph: body end");
@@ -671,14 +674,14 @@ struct ibg_context {
     // make the FP32 copy current (after the FP64 state was written) or the FP64 copy current
     void to32() {
         if (!fp32) return;
-        k_convert<double, float><<<(unsigned)((S + 255) / 256), 256, 0, st>>>(S, b64.w, b32.w);
-        k_convert<double, float><<<(unsigned)((F + 255) / 256), 256, 0, st>>>(F, b64.q, b32.q);
+        launch_k(k_convert<double, float>, (unsigned)((S + 255) / 256), 256, 0, st, S, b64.w, b32.w);
+        launch_k(k_convert<double, float>, (unsigned)((F + 255) / 256), 256, 0, st, F, b64.q, b32.q);
         state_in_32 = true;
     }
     void to64() {
         if (!fp32 || !state_in_32) return;
-        k_convert<float, double><<<(unsigned)((S + 255) / 256), 256, 0, st>>>(S, b32.w, b64.w);
-        k_convert<float, double><<<(unsigned)((F + 255) / 256), 256, 0, st>>>(F, b32.q, b64.q);
+        launch_k(k_convert<float, double>, (unsigned)((S + 255) / 256), 256, 0, st, S, b32.w, b64.w);
+        launch_k(k_convert<float, double>, (unsigned)((F + 255) / 256), 256, 0, st, F, b32.q, b64.q);
     }
 
     void net_force_record();
@@ -781,6 +784,7 @@ struct ibg_context {
 
 namespace ibg {
 __global__ void k_hist_force(int npts, const double* f, double dx2, double* hist, int* count) {
+    pdl_enter();
     double sx = 0.0, sy = 0.0;
     for (int k = threadIdx.x; k < npts; k += 32) {
         sx += f[k];
@@ -804,6 +808,7 @@ namespace ibg {
 // after a fallback to plain CG (flags[8]), the preconditioner is the identity
 __global__ void k_fallback_identity(int m, const int* __restrict__ flags, const double* __restrict__ r,
                                     double* __restrict__ z) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < m && flags[8]) z[i] = r[i];
 }
@@ -812,7 +817,7 @@ __global__ void k_fallback_identity(int m, const int* __restrict__ flags, const 
 void ibg_context::apply_learned_precond(int k, const double* r, double* z) {
     if (lpc_ready) {
         minv_apply(ncomp, Mi[k], r, z, st);
-        k_fallback_identity<<<(ncomp + 255) / 256, 256, 0, st>>>(ncomp, cg_flags, r, z);
+        launch_k(k_fallback_identity, (ncomp + 255) / 256, 256, 0, st, ncomp, cg_flags, r, z);
         launches += 2;
     } else {
         // no network yet: identity (plain CG directions)
@@ -822,7 +827,7 @@ void ibg_context::apply_learned_precond(int k, const double* r, double* z) {
 }
 
 void ibg_context::net_force_record() {
-    ibg::k_hist_force<<<1, 32, 0, st>>>(npts, f, g.dx * g.dx, d_hist, d_hist_count);
+    launch_k(ibg::k_hist_force, 1, 32, 0, st, npts, f, g.dx * g.dx, d_hist, d_hist_count);
 }
 
 // ===========================================================================
@@ -1325,6 +1330,7 @@ constexpr int kIpBlocks = 256;
 // partial[b] = sum over this block's grid-stride share of w a b (fixed order)
 __global__ void k_wdot_partial(size_t n, const double* __restrict__ w, const double* __restrict__ a,
                                const double* __restrict__ b, double* __restrict__ partial) {
+    pdl_enter();
     __shared__ double red[32];
     double s = 0.0;
     for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
@@ -1339,6 +1345,7 @@ __global__ void k_wdot_partial(size_t n, const double* __restrict__ w, const dou
     }
 }
 __global__ void k_sum_partials(int n, const double* __restrict__ partial, double scale, double* __restrict__ out) {
+    pdl_enter();
     if (threadIdx.x == 0) {
         double t = 0.0;
         for (int k = 0; k < n; ++k) t += partial[k];
@@ -1418,8 +1425,8 @@ int ibg_context::build_ip_weights() {
 static int device_ip(ibg_context* c, int kind, const double* da, const double* db, double scale, double* out) {
     const size_t n = kind < 2 ? c->S : c->F;
     double* partial = c->d_ip_tmp + 2 * (size_t)c->F;
-    ibg::k_wdot_partial<<<ibg::kIpBlocks, 256, 0, c->st>>>(n, c->d_ipw[kind], da, db, partial);
-    ibg::k_sum_partials<<<1, 32, 0, c->st>>>(ibg::kIpBlocks, partial, scale, partial + ibg::kIpBlocks);
+    launch_k(ibg::k_wdot_partial, ibg::kIpBlocks, 256, 0, c->st, n, c->d_ipw[kind], da, db, partial);
+    launch_k(ibg::k_sum_partials, 1, 32, 0, c->st, ibg::kIpBlocks, partial, scale, partial + ibg::kIpBlocks);
     cudaMemcpyAsync(out, partial + ibg::kIpBlocks, sizeof(double), cudaMemcpyDeviceToHost, c->st);
     if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->cuda_check("inner product");
     return c->cuda_check("inner product");
@@ -1977,6 +1984,7 @@ const char* ibg_ensemble_last_error(const ibg_ensemble* e) { return e ? e->err.c
 namespace ibg {
 __global__ void k_gather_rows(int nrows, long width, const int* __restrict__ idx, const float* __restrict__ src,
                               float* __restrict__ dst) {
+    pdl_enter();
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)nrows * width) return;
     const long r = t / width, c = t % width;
@@ -2116,8 +2124,8 @@ int ibg_lpc_train(ibg_context* c, int nconfig, const float* geom, const float* m
         for (int b0 = 0; b0 + batch <= nconfig && !s; b0 += batch) {
             cudaMemcpyAsync(didx, perm.data() + b0, sizeof(int) * batch, cudaMemcpyHostToDevice, c->st);
             const long wg = 4L * P, wm = (long)m * m;
-            k_gather_rows<<<(unsigned)((batch * wg + 255) / 256), 256, 0, c->st>>>(batch, wg, didx, d.g, bg);
-            k_gather_rows<<<(unsigned)((batch * wm + 255) / 256), 256, 0, c->st>>>(batch, wm, didx, d.mb, bm);
+            launch_k(k_gather_rows, (unsigned)((batch * wg + 255) / 256), 256, 0, c->st, batch, wg, didx, d.g, bg);
+            launch_k(k_gather_rows, (unsigned)((batch * wm + 255) / 256), 256, 0, c->st, batch, wm, didx, d.mb, bm);
             float l = 0.f;
             s = c->lpc.loss_grad(batch, bg, bm, &l, grad, c->tws, c->st);
             if (s) break;

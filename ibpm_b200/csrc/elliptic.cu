@@ -33,6 +33,14 @@
 
 namespace ibg {
 
+bool pdl_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("IBG_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 int raise_smem_limit(const void* func, int bytes) {
     static std::mutex mu;
     static std::map<std::pair<int, const void*>, int> set;
@@ -178,6 +186,7 @@ __device__ C* fft_smem(C* s0, C* s1, const C* tw, const FftDesc& d, int P) {
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void k_dst_rows(RowPassArgs<T> a) {
+    pdl_enter();
     using C = typename Cplx<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const FftDesc& d = a.fft;
@@ -280,6 +289,7 @@ __device__ __forceinline__ T lifted_coef(T R, int k, int l, const T* edges, int 
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void k_dst_cols(ColPassArgs<T> a) {
+    pdl_enter();
     using C = typename Cplx<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const FftDesc& d = a.fft;
@@ -370,6 +380,7 @@ __device__ __forceinline__ T rhs_node(const T* f_lev, const T* rc_lev, const Gri
 
 template <typename T>
 __global__ void k_coarsify(GridDev g, int lev, const T* f, T* rc, size_t bstride) {
+    pdl_enter();
     const int ni = g.nx / 2 - 1, nj = g.ny / 2 - 1;  // overlap interior extent
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ni * nj) return;
@@ -424,6 +435,7 @@ __device__ void dst_pair_block(const FftDesc& d, int n, const T* a_in, const T* 
 // W_i0, W_i1); every sum is complete inside one block (fixed order).
 template <typename T>
 __global__ void __launch_bounds__(256) k_sweep_sums(SweepArgs<T> a) {
+    pdl_enter();
     __shared__ T red[8][2 * kSweepCols];
     const GridDev& g = a.g;
     const int NI = g.NI, NJ = g.NJ;
@@ -495,6 +507,7 @@ __global__ void __launch_bounds__(256) k_sweep_sums(SweepArgs<T> a) {
 // with W for the left/right values.  blockIdx.y = batch item.
 template <typename T>
 __global__ void __launch_bounds__(512) k_sweep_lines(SweepArgs<T> a) {
+    pdl_enter();
     using C = typename Cplx<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const GridDev& g = a.g;
@@ -541,6 +554,7 @@ __global__ void __launch_bounds__(512) k_sweep_lines(SweepArgs<T> a) {
 // k_sweep_lines applied to unit vectors; k_sweep_edges applies it with one
 // warp per output row, spread over the whole GPU instead of two blocks.
 __global__ void __launch_bounds__(512) k_edge_map(FftDesc d, int n, int ext, double* __restrict__ A) {
+    pdl_enter();
     using C = typename Cplx<double>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* s0 = reinterpret_cast<C*>(smem_raw);
@@ -577,6 +591,7 @@ __global__ void __launch_bounds__(512) k_edge_map(FftDesc d, int n, int ext, dou
 }
 
 __global__ void k_map_to_f32(long n, const double* __restrict__ a, float* __restrict__ b) {
+    pdl_enter();
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t < n) b[t] = (float)a[t];
 }
@@ -587,6 +602,7 @@ constexpr int kEdgeRows = 8;  // output rows (warps) per block of k_sweep_edges
 // blockIdx.z = batch item
 template <typename T>
 __global__ void __launch_bounds__(32 * kEdgeRows) k_sweep_edges(SweepArgs<T> a) {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* v = reinterpret_cast<T*>(smem_raw);
     const GridDev& g = a.g;
@@ -863,8 +879,7 @@ void EllipticPlan<T>::launch_rows(const GridDev& g, const FftDesc& frow, int nle
     A.pairs_per_block = P;
     A.tw_smem = tws;
     const int npairs = (g.NI + 1) / 2;
-    k_dst_rows<T><<<dim3((unsigned)((npairs + P - 1) / P), (unsigned)(nlev * batch)), nt,
-                    fft_smem_bytes<T>(frow.m, P, tws), st>>>(A);
+    launch_k(k_dst_rows<T>, dim3((unsigned)((npairs + P - 1) / P), (unsigned)(nlev * batch)), nt, fft_smem_bytes<T>(frow.m, P, tws), st, A);
 }
 
 template <typename T>
@@ -902,8 +917,7 @@ void EllipticPlan<T>::launch_cols(const GridDev& g, const FftDesc& fcol, int mod
     B.pairs_per_block = P;
     B.tw_smem = tws;
     const int ncolblk = (g.NJ + 2 * P - 1) / (2 * P);
-    k_dst_cols<T><<<dim3((unsigned)ncolblk, (unsigned)(nlev * batch)), nt, fft_smem_bytes<T>(fcol.m, P, tws),
-                    st>>>(B);
+    launch_k(k_dst_cols<T>, dim3((unsigned)ncolblk, (unsigned)(nlev * batch)), nt, fft_smem_bytes<T>(fcol.m, P, tws), st, B);
 }
 
 template <typename T>
@@ -933,7 +947,7 @@ int EllipticPlan<T>::solve(const SolveCall<T>& c, cudaStream_t st) const {
     // 1. coarsify the right-hand side: overlap interiors of levels 1..L-1 into rc
     const int novl = (g.nx / 2 - 1) * (g.ny / 2 - 1);
     for (int lev = 1; lev < L; ++lev)
-        k_coarsify<T><<<dim3((unsigned)((novl + 255) / 256), (unsigned)batch), 256, 0, st>>>(g, lev, c.f, c.rc,
+        launch_k(k_coarsify<T>, dim3((unsigned)((novl + 255) / 256), (unsigned)batch), 256, 0, st, g, lev, c.f, c.rc,
                                                                                           c.bstride);
     // 2. forward transforms of every level
     const T* in[kMaxLevels];
@@ -976,13 +990,12 @@ int EllipticPlan<T>::solve(const SolveCall<T>& c, cudaStream_t st) const {
         s.ax = gt.ax;
         s.ay = gt.ay;
         const int nrb = (g.NI + kSweepRows - 1) / kSweepRows, ncb = (g.NJ + kSweepCols - 1) / kSweepCols;
-        k_sweep_sums<T><<<dim3((unsigned)(nrb + ncb), (unsigned)batch), 256, 0, st>>>(s);
+        launch_k(k_sweep_sums<T>, dim3((unsigned)(nrb + ncb), (unsigned)batch), 256, 0, st, s);
         if (gt.ax && gt.ay && edge_maps) {
             const int nmax = std::max(g.NI, g.NJ);
-            k_sweep_edges<T><<<dim3((unsigned)((nmax + kEdgeRows - 1) / kEdgeRows), 2, (unsigned)batch),
-                               32 * kEdgeRows, sizeof(T) * 2 * (size_t)nmax, st>>>(s);
+            launch_k(k_sweep_edges<T>, dim3((unsigned)((nmax + kEdgeRows - 1) / kEdgeRows), 2, (unsigned)batch), 32 * kEdgeRows, sizeof(T) * 2 * (size_t)nmax, st, s);
         } else {
-            k_sweep_lines<T><<<dim3(2, (unsigned)batch), 512, ssm, st>>>(s);
+            launch_k(k_sweep_lines<T>, dim3(2, (unsigned)batch), 512, ssm, st, s);
         }
     }
     // 4. inverse transforms of every level (lifting + eigen-inverse applied on load)
@@ -1006,7 +1019,7 @@ int EllipticPlan<T>::solve(const SolveCall<T>& c, cudaStream_t st) const {
 void coarsify_field(const GridDev& g, double* f, cudaStream_t st) {
     const int novl = (g.nx / 2 - 1) * (g.ny / 2 - 1);
     for (int lev = 1; lev < g.L; ++lev)
-        k_coarsify<double><<<dim3((unsigned)((novl + 255) / 256), 1), 256, 0, st>>>(g, lev, f, f, 0);
+        launch_k(k_coarsify<double>, dim3((unsigned)((novl + 255) / 256), 1), 256, 0, st, g, lev, f, f, 0);
 }
 
 template <typename T>

@@ -36,6 +36,7 @@ __device__ double block_sum(double v, double* red) {
 __global__ void __launch_bounds__(1024) k_chol_factor(int m, const double* __restrict__ Mcol, double* __restrict__ Lr,
                                                       double* __restrict__ Lc, double* __restrict__ diag,
                                                       int* __restrict__ status) {
+    pdl_enter();
     extern __shared__ double sh[];
     double* rowc = sh;        // L(c, 0..c-1)
     double* red = sh + m;     // 32 partial sums
@@ -129,6 +130,7 @@ __device__ void chol_subst(int m, const double* __restrict__ Lr, const double* _
 __global__ void __launch_bounds__(1024) k_chol_solve(int m, const double* __restrict__ Lr, const double* __restrict__ Lc,
                                                      const double* __restrict__ diag, const double* __restrict__ b,
                                                      double* __restrict__ x_out) {
+    pdl_enter();
     extern __shared__ double sh[];
     double* x = sh;
     double* red = sh + m;
@@ -143,6 +145,7 @@ __global__ void __launch_bounds__(1024) k_chol_solve(int m, const double* __rest
 __global__ void __launch_bounds__(1024) k_chol_inverse(int m, const double* __restrict__ Lr,
                                                        const double* __restrict__ Lc, const double* __restrict__ diag,
                                                        double* __restrict__ Minv) {
+    pdl_enter();
     extern __shared__ double sh[];
     double* x = sh;
     double* red = sh + m;
@@ -156,6 +159,7 @@ __global__ void __launch_bounds__(1024) k_chol_inverse(int m, const double* __re
 // y = Minv b: one warp per row
 __global__ void k_minv_apply(int m, const double* __restrict__ Minv, const double* __restrict__ b,
                              double* __restrict__ y) {
+    pdl_enter();
     const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (row >= m) return;
@@ -173,6 +177,7 @@ __global__ void k_minv_apply(int m, const double* __restrict__ Minv, const doubl
 __global__ void __launch_bounds__(1024) k_cg_begin(int m, const double* __restrict__ b, const double* __restrict__ Mx,
                                                    double* __restrict__ r, double* __restrict__ d,
                                                    double* __restrict__ scal, int* __restrict__ flags) {
+    pdl_enter();
     __shared__ double red[32];
     double part = 0.0;
     for (int k = threadIdx.x; k < m; k += blockDim.x) {
@@ -192,6 +197,7 @@ __global__ void __launch_bounds__(1024) k_cg_begin(int m, const double* __restri
 __global__ void __launch_bounds__(1024) k_cg_update(int m, double* __restrict__ x, double* __restrict__ r,
                                                     double* __restrict__ d, const double* __restrict__ q,
                                                     double* __restrict__ scal, int* __restrict__ flags) {
+    pdl_enter();
     __shared__ double red[32];
     if (flags[0] == 0) return;
     double part = 0.0;
@@ -227,6 +233,7 @@ __global__ void __launch_bounds__(1024) k_cg_update(int m, double* __restrict__ 
 __global__ void __launch_bounds__(1024) k_pcg_begin(int m, const double* __restrict__ b, const double* __restrict__ Mx,
                                                     double* __restrict__ r, double* __restrict__ scal,
                                                     int* __restrict__ flags) {
+    pdl_enter();
     __shared__ double red[32];
     double part = 0.0;
     for (int k = threadIdx.x; k < m; k += blockDim.x) {
@@ -245,6 +252,7 @@ __global__ void __launch_bounds__(1024) k_pcg_begin(int m, const double* __restr
 __global__ void __launch_bounds__(1024) k_pcg_begin2(int m, const double* __restrict__ r, double* __restrict__ z,
                                                      double* __restrict__ d, double* __restrict__ scal,
                                                      int* __restrict__ flags) {
+    pdl_enter();
     __shared__ double red[32];
     double part = 0.0;
     for (int k = threadIdx.x; k < m; k += blockDim.x) part += r[k] * z[k];
@@ -268,6 +276,7 @@ __global__ void __launch_bounds__(1024) k_pcg_step1(int m, double* __restrict__ 
                                                     const double* __restrict__ d, const double* __restrict__ q,
                                                     const double* __restrict__ z, double* __restrict__ zold,
                                                     double* __restrict__ scal, int* __restrict__ flags) {
+    pdl_enter();
     __shared__ double red[32];
     if (flags[0] == 0) return;
     double part = 0.0;
@@ -289,6 +298,7 @@ __global__ void __launch_bounds__(1024) k_pcg_step1(int m, double* __restrict__ 
 __global__ void __launch_bounds__(1024) k_pcg_step2(int m, const double* __restrict__ r, double* __restrict__ z,
                                                     const double* __restrict__ zold, double* __restrict__ d,
                                                     double* __restrict__ scal, int* __restrict__ flags) {
+    pdl_enter();
     __shared__ double red[32];
     __shared__ int restart;
     if (flags[0] == 0) return;
@@ -334,6 +344,7 @@ __global__ void __launch_bounds__(1024) k_pcg_step2(int m, const double* __restr
 
 // net force sum(f) dx^2 in each direction, appended to a history buffer
 __global__ void k_net_force(int npts, const double* __restrict__ f, double dx2, double* __restrict__ out) {
+    pdl_enter();
     double sx = 0.0, sy = 0.0;
     for (int k = threadIdx.x; k < npts; k += 32) {
         sx += f[k];
@@ -348,6 +359,7 @@ __global__ void k_net_force(int npts, const double* __restrict__ f, double dx2, 
 }
 
 __global__ void k_add_time(double* t, double dt) {
+    pdl_enter();
     if (threadIdx.x == 0 && blockIdx.x == 0) *t = *t + dt;
 }
 
@@ -359,14 +371,14 @@ int chol_factor(int m, const double* Mcol, double* Lr, double* Lc, double* diag,
     cudaMemsetAsync(d_status, 0, sizeof(int), st);
     cudaMemsetAsync(Lr, 0, sizeof(double) * m * m, st);
     cudaMemsetAsync(Lc, 0, sizeof(double) * m * m, st);
-    k_chol_factor<<<1, 1024, sm, st>>>(m, Mcol, Lr, Lc, diag, d_status);
+    launch_k(k_chol_factor, 1, 1024, sm, st, m, Mcol, Lr, Lc, diag, d_status);
     return cudaPeekAtLastError() == cudaSuccess ? IBG_OK : IBG_ERR_CUDA;
 }
 
 void chol_solve(int m, const double* Lr, const double* Lc, const double* diag, const double* b, double* x,
                 cudaStream_t st) {
     const size_t sm = sizeof(double) * (m + 32 * 33);
-    k_chol_solve<<<1, 1024, sm, st>>>(m, Lr, Lc, diag, b, x);
+    launch_k(k_chol_solve, 1, 1024, sm, st, m, Lr, Lc, diag, b, x);
 }
 
 int chol_solve_prepare(int m) {
@@ -379,41 +391,41 @@ int chol_solve_prepare(int m) {
 
 void chol_inverse(int m, const double* Lr, const double* Lc, const double* diag, double* Minv, cudaStream_t st) {
     const size_t sm = sizeof(double) * (m + 32 * 33);
-    k_chol_inverse<<<m, 1024, sm, st>>>(m, Lr, Lc, diag, Minv);
+    launch_k(k_chol_inverse, m, 1024, sm, st, m, Lr, Lc, diag, Minv);
 }
 
 void minv_apply(int m, const double* Minv, const double* b, double* y, cudaStream_t st) {
-    k_minv_apply<<<(m + 7) / 8, 256, 0, st>>>(m, Minv, b, y);
+    launch_k(k_minv_apply, (m + 7) / 8, 256, 0, st, m, Minv, b, y);
 }
 
 void cg_begin(int m, const double* b, const double* Mx, double* r, double* d, double* scal, int* flags,
               cudaStream_t st) {
-    k_cg_begin<<<1, 1024, 0, st>>>(m, b, Mx, r, d, scal, flags);
+    launch_k(k_cg_begin, 1, 1024, 0, st, m, b, Mx, r, d, scal, flags);
 }
 
 void cg_update(int m, double* x, double* r, double* d, const double* q, double* scal, int* flags, cudaStream_t st) {
-    k_cg_update<<<1, 1024, 0, st>>>(m, x, r, d, q, scal, flags);
+    launch_k(k_cg_update, 1, 1024, 0, st, m, x, r, d, q, scal, flags);
 }
 
 void pcg_begin(int m, const double* b, const double* Mx, double* r, double* scal, int* flags, cudaStream_t st) {
-    k_pcg_begin<<<1, 1024, 0, st>>>(m, b, Mx, r, scal, flags);
+    launch_k(k_pcg_begin, 1, 1024, 0, st, m, b, Mx, r, scal, flags);
 }
 void pcg_begin2(int m, const double* r, double* z, double* d, double* scal, int* flags, cudaStream_t st) {
-    k_pcg_begin2<<<1, 1024, 0, st>>>(m, r, z, d, scal, flags);
+    launch_k(k_pcg_begin2, 1, 1024, 0, st, m, r, z, d, scal, flags);
 }
 void pcg_step1(int m, double* x, double* r, const double* d, const double* q, const double* z, double* zold,
                double* scal, int* flags, cudaStream_t st) {
-    k_pcg_step1<<<1, 1024, 0, st>>>(m, x, r, d, q, z, zold, scal, flags);
+    launch_k(k_pcg_step1, 1, 1024, 0, st, m, x, r, d, q, z, zold, scal, flags);
 }
 void pcg_step2(int m, const double* r, double* z, const double* zold, double* d, double* scal, int* flags,
                cudaStream_t st) {
-    k_pcg_step2<<<1, 1024, 0, st>>>(m, r, z, zold, d, scal, flags);
+    launch_k(k_pcg_step2, 1, 1024, 0, st, m, r, z, zold, d, scal, flags);
 }
 
 void net_force(int npts, const double* f, double dx2, double* out, cudaStream_t st) {
-    k_net_force<<<1, 32, 0, st>>>(npts, f, dx2, out);
+    launch_k(k_net_force, 1, 32, 0, st, npts, f, dx2, out);
 }
 
-void add_time(double* t, double dt, cudaStream_t st) { k_add_time<<<1, 32, 0, st>>>(t, dt); }
+void add_time(double* t, double dt, cudaStream_t st) { launch_k(k_add_time, 1, 32, 0, st, t, dt); }
 
 }  // namespace ibg

@@ -12,6 +12,8 @@
 #include <cstdio>
 #include <string>
 #include <vector>
+#include <utility>
+#include <cstdlib>
 
 namespace ibg {
 
@@ -36,6 +38,40 @@ struct GridDev {
 };
 
 __host__ __device__ inline double lev_dx(const GridDev& g, int lev) { return g.dx * (double)(1 << lev); }
+
+// ---------------------------------------------------------------------------
+// Programmatic dependent launch.  Kernels of the time step are launched with
+// launch_k, which lets the next kernel on the stream be scheduled while the
+// one ahead of it is still running; every such kernel starts with
+// pdl_enter(): it waits until the kernels it depends on have finished and
+// their writes are visible (griddepcontrol.wait, before any global memory
+// access), then allows the kernel after it to be scheduled
+// (griddepcontrol.launch_dependents).  For a kernel launched without the
+// attribute both are no-ops.  IBG_PDL=0 in the environment turns the
+// attribute off.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+bool pdl_enabled();
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                            Args&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // value of a Scalar level at node (i, j), 1 <= i <= nx-1, 1 <= j <= ny-1
 template <typename T>

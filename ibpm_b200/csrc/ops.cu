@@ -102,6 +102,7 @@ __device__ __forceinline__ void node_uv(const GridDev& g, const T* ql, int lev, 
 template <typename T>
 __global__ void k_node_vel(GridDev g, const T* __restrict__ q, const T* __restrict__ w, T* __restrict__ U,
                            T* __restrict__ V, size_t sstride, size_t fstride) {
+    pdl_enter();
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const size_t total = (size_t)g.L * g.N1;
     if (tid >= total) return;
@@ -121,6 +122,7 @@ __global__ void k_node_vel(GridDev g, const T* __restrict__ q, const T* __restri
 // coarse interior overlap nodes the reference leaves undefined
 __global__ void k_flux_to_vel(GridDev g, const double* __restrict__ q, double* __restrict__ u,
                               double* __restrict__ v) {
+    pdl_enter();
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= (size_t)g.L * g.N1) return;
     const int lev = (int)(tid / g.N1);
@@ -141,6 +143,7 @@ __global__ void k_node_vel_lin(GridDev g, const double* __restrict__ q, const do
                                const double* __restrict__ qb, const double* __restrict__ wb, int period,
                                const int* __restrict__ ts0, const int* __restrict__ count, double* __restrict__ U,
                                double* __restrict__ V) {
+    pdl_enter();
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const size_t total = (size_t)g.L * g.N1;
     if (tid >= total) return;
@@ -163,6 +166,7 @@ __global__ void k_node_vel_lin(GridDev g, const double* __restrict__ q, const do
 // the coarse overlap interior, undefined here as in the reference, is then filled by coarsify
 __global__ void k_flux_cross(GridDev g, const double* __restrict__ q1, const double* __restrict__ q2,
                              double* __restrict__ out) {
+    pdl_enter();
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= (size_t)g.L * g.N1) return;
     const int lev = (int)(tid / g.N1);
@@ -176,6 +180,7 @@ __global__ void k_flux_cross(GridDev g, const double* __restrict__ q1, const dou
 }
 
 __global__ void k_sub(size_t n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ out) {
+    pdl_enter();
     const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t < n) out[t] = a[t] - b[t];
 }
@@ -186,6 +191,7 @@ __global__ void k_sub(size_t n, const double* __restrict__ a, const double* __re
 __global__ void k_sfd(size_t n, const double* __restrict__ w, double* __restrict__ what, double* __restrict__ rprev,
                       double* __restrict__ N, double chi, double Delta, double an, double bn, double dt,
                       int first) {
+    pdl_enter();
     const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     const double d = w[t] - what[t];
@@ -206,6 +212,7 @@ __global__ void k_sfd(size_t n, const double* __restrict__ w, double* __restrict
 template <typename T>
 __global__ void k_cross_flux(GridDev g, int lev, const T* __restrict__ U, const T* __restrict__ V, T* __restrict__ C,
                              size_t sstride, size_t fstride) {
+    pdl_enter();
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= g.F1) return;
     const size_t sb = (size_t)blockIdx.y * sstride, fb = (size_t)blockIdx.y * fstride;
@@ -288,6 +295,7 @@ __global__ void k_cross_flux(GridDev g, int lev, const T* __restrict__ U, const 
 // Curl of a Flux on every level (no inter-level coupling)
 template <typename T>
 __global__ void k_curl_flux(GridDev g, const T* __restrict__ C, T* __restrict__ N, size_t sstride, size_t fstride) {
+    pdl_enter();
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= (size_t)g.L * g.N1) return;
     const size_t sb = (size_t)blockIdx.y * sstride, fb = (size_t)blockIdx.y * fstride;
@@ -304,6 +312,7 @@ __global__ void k_curl_flux(GridDev g, const T* __restrict__ C, T* __restrict__ 
 template <typename T>
 __global__ void k_rhs(GridDev g, const T* __restrict__ w, const T* __restrict__ N, const T* __restrict__ Nprev,
                       T* __restrict__ a, T c1, T an, T bn, T dt, int lap_only) {
+    pdl_enter();
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= (size_t)g.L * g.N1) return;
     const int lev = (int)(tid / g.N1);
@@ -346,6 +355,7 @@ __device__ __forceinline__ T curl_scalar_at(const GridDev& g, const T* f, const 
 template <typename T>
 __global__ void k_refresh_flux(GridDev g, const T* __restrict__ psi, T* __restrict__ q, double u0, double v0,
                                const double* __restrict__ q0f) {
+    pdl_enter();
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= (size_t)g.L * g.F1) return;
     const int lev = (int)(tid / g.F1);
@@ -395,6 +405,7 @@ __device__ void advance_history(const BodyDev& b, MotionState& s, double t) {
 // one thread per body
 __global__ void k_motion_state(int nbodies, const BodyDev* __restrict__ bodies, const double* __restrict__ time_ptr,
                                double toff, MotionState* __restrict__ ms) {
+    pdl_enter();
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nbodies) return;
     const BodyDev& b = bodies[k];
@@ -513,6 +524,7 @@ __global__ void k_kinematics(int npts, const double* __restrict__ ref_xy, const 
                              const BodyDev* __restrict__ bodies, const MotionState* __restrict__ ms,
                              const double* __restrict__ mtab, const double* __restrict__ time_ptr, double toff,
                              double* __restrict__ pts, double* __restrict__ vel) {
+    pdl_enter();
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= npts) return;
     const int k = body_of[p];
@@ -545,6 +557,7 @@ __global__ void k_kinematics(int npts, const double* __restrict__ ref_xy, const 
 __global__ void k_frame_flow(const BodyDev* __restrict__ bf, MotionState* __restrict__ ms,
                              const double* __restrict__ mtab, const double* __restrict__ time_ptr, double toff,
                              double magBF, double alphaBF, double* __restrict__ out) {
+    pdl_enter();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     const double t = *time_ptr + toff;
     const BodyDev b = *bf;
@@ -567,6 +580,7 @@ __global__ void k_frame_flow(const BodyDev* __restrict__ bf, MotionState* __rest
 // Flux::setFlow: q0 = ((xdot' - thetadot' (y - yc)) dx, (ydot' + thetadot' (x - xc)) dx) at every flux of
 // every level, at the flux positions of Grid::getXEdge / getXCenter with zero shift (src/Grid.cc:104-139)
 __global__ void k_frame_flux(GridDev g, const double* __restrict__ fv, double xc, double yc, double* __restrict__ q0) {
+    pdl_enter();
     const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= (size_t)g.L * g.F1) return;
     const int lev = (int)(tid / g.F1);
@@ -591,6 +605,7 @@ __global__ void k_frame_flux(GridDev g, const double* __restrict__ fv, double xc
 __global__ void k_bcon_field(int ncomp, const int* __restrict__ sidx, const double* __restrict__ sw,
                              const int* __restrict__ sn, const double* __restrict__ vel, const double* __restrict__ q0,
                              double h, double* __restrict__ bcon) {
+    pdl_enter();
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncomp) return;
     const int npts = ncomp / 2, dir = c / npts, p = c % npts;
@@ -614,6 +629,7 @@ __device__ __forceinline__ double delta_fn(double r) {
 __global__ void k_reg_update(GridDev g, int npts, const double* __restrict__ pts, const double* __restrict__ vel,
                              int* __restrict__ sidx, double* __restrict__ sw, int* __restrict__ sn,
                              double* __restrict__ bcon, double u0, double v0) {
+    pdl_enter();
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= 2 * npts) return;
     const int dir = c / npts, p = c % npts;
@@ -661,6 +677,7 @@ template <typename T>
 __global__ void k_reg_interp(GridDev g, int ncomp, const int* __restrict__ sidx, const double* __restrict__ sw,
                              const int* __restrict__ sn, const T* __restrict__ psi, size_t sstride,
                              const double* __restrict__ bcon, double* __restrict__ out, size_t ostride) {
+    pdl_enter();
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncomp) return;
     const T* f = psi + (size_t)blockIdx.y * sstride;
@@ -676,6 +693,7 @@ __global__ void k_reg_interp(GridDev g, int ncomp, const int* __restrict__ sidx,
 // smear: flux0[idx] += w f_c (atomic; flux0 is kept zero between uses)
 __global__ void k_reg_smear(int ncomp, const int* __restrict__ sidx, const double* __restrict__ sw,
                             const int* __restrict__ sn, const double* __restrict__ f, double* __restrict__ flux0) {
+    pdl_enter();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int c = t / kSlots, k = t % kSlots;
     if (c >= ncomp || k >= sn[c]) return;
@@ -685,6 +703,7 @@ __global__ void k_reg_smear(int ncomp, const int* __restrict__ sidx, const doubl
 // batched smear of unit vectors: item b carries e_{col0+b}
 __global__ void k_reg_smear_unit(int ncomp, int col0, const int* __restrict__ sidx, const double* __restrict__ sw,
                                  const int* __restrict__ sn, double* __restrict__ flux0, size_t fstride) {
+    pdl_enter();
     const int b = blockIdx.x;
     const int c = col0 + b;
     const int k = threadIdx.x;
@@ -694,6 +713,7 @@ __global__ void k_reg_smear_unit(int ncomp, int col0, const int* __restrict__ si
 
 __global__ void k_reg_zero(int ncomp, int col0, int unit, const int* __restrict__ sidx, const int* __restrict__ sn,
                            double* __restrict__ flux0, size_t fstride) {
+    pdl_enter();
     if (unit) {
         const int b = blockIdx.x, c = col0 + b, k = threadIdx.x;
         if (c >= ncomp || k >= sn[c]) return;
@@ -710,6 +730,7 @@ __global__ void k_reg_zero(int ncomp, int col0, int unit, const int* __restrict_
 template <typename T>
 __global__ void k_bf(GridDev g, const double* __restrict__ flux0, size_t fstride, T* __restrict__ Bf, size_t sstride,
                      double beta) {
+    pdl_enter();
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= g.N1) return;
     const double* q = flux0 + (size_t)blockIdx.y * fstride;
@@ -730,59 +751,60 @@ template <typename T>
 void launch_nonlinear(const GridDev& g, const T* q, const T* w, T* U, T* V, T* C, T* N, int batch, size_t sstride,
                       size_t fstride, cudaStream_t st) {
     const size_t S = (size_t)g.L * g.N1;
-    k_node_vel<T><<<dim3(nblk(S, 256), batch), 256, 0, st>>>(g, q, w, U, V, sstride, fstride);
+    launch_k(k_node_vel<T>, dim3(nblk(S, 256), batch), 256, 0, st, g, q, w, U, V, sstride, fstride);
     for (int lev = 0; lev < g.L; ++lev)
-        k_cross_flux<T><<<dim3(nblk(g.F1, 256), batch), 256, 0, st>>>(g, lev, U, V, C, sstride, fstride);
-    k_curl_flux<T><<<dim3(nblk(S, 256), batch), 256, 0, st>>>(g, C, N, sstride, fstride);
+        launch_k(k_cross_flux<T>, dim3(nblk(g.F1, 256), batch), 256, 0, st, g, lev, U, V, C, sstride, fstride);
+    launch_k(k_curl_flux<T>, dim3(nblk(S, 256), batch), 256, 0, st, g, C, N, sstride, fstride);
 }
 
 void launch_nonlinear_lin(const GridDev& g, const double* q, const double* w, const double* qb, const double* wb,
                           int period, const int* ts0, const int* count, double* U, double* V, double* C, double* N,
                           cudaStream_t st) {
     const size_t S = (size_t)g.L * g.N1, F = (size_t)g.L * g.F1;
-    k_node_vel_lin<<<nblk(S, 256), 256, 0, st>>>(g, q, w, qb, wb, period, ts0, count, U, V);
+    launch_k(k_node_vel_lin, nblk(S, 256), 256, 0, st, g, q, w, qb, wb, period, ts0, count, U, V);
     for (int lev = 0; lev < g.L; ++lev)
-        k_cross_flux<double><<<dim3(nblk(g.F1, 256), 1), 256, 0, st>>>(g, lev, U, V, C, S, F);
-    k_curl_flux<double><<<dim3(nblk(S, 256), 1), 256, 0, st>>>(g, C, N, S, F);
+        launch_k(k_cross_flux<double>, dim3(nblk(g.F1, 256), 1), 256, 0, st, g, lev, U, V, C, S, F);
+    launch_k(k_curl_flux<double>, dim3(nblk(S, 256), 1), 256, 0, st, g, C, N, S, F);
 }
 
 void launch_flux_cross(const GridDev& g, const double* q1, const double* q2, double* out, cudaStream_t st) {
     const size_t S = (size_t)g.L * g.N1;
-    k_flux_cross<<<nblk(S, 256), 256, 0, st>>>(g, q1, q2, out);
+    launch_k(k_flux_cross, nblk(S, 256), 256, 0, st, g, q1, q2, out);
 }
 
 void launch_sub(size_t n, const double* a, const double* b, double* out, cudaStream_t st) {
-    k_sub<<<nblk(n, 256), 256, 0, st>>>(n, a, b, out);
+    launch_k(k_sub, nblk(n, 256), 256, 0, st, n, a, b, out);
 }
 
 void launch_sfd(size_t n, const double* w, double* what, double* rprev, double* N, double chi, double Delta,
                 double an, double bn, double dt, bool first, cudaStream_t st) {
-    k_sfd<<<nblk(n, 256), 256, 0, st>>>(n, w, what, rprev, N, chi, Delta, an, bn, dt, first ? 1 : 0);
+    launch_k(k_sfd, nblk(n, 256), 256, 0, st, n, w, what, rprev, N, chi, Delta, an, bn, dt, first ? 1 : 0);
 }
 
 template <typename T>
 void launch_curl_flux(const GridDev& g, const T* C, T* N, cudaStream_t st) {
     const size_t S = (size_t)g.L * g.N1;
-    k_curl_flux<T><<<dim3(nblk(S, 256), 1), 256, 0, st>>>(g, C, N, S, (size_t)g.L * g.F1);
+    launch_k(k_curl_flux<T>, dim3(nblk(S, 256), 1), 256, 0, st, g, C, N, S, (size_t)g.L * g.F1);
 }
 
 template <typename T>
 void launch_rhs(const GridDev& g, const T* w, const T* N, const T* Nprev, T* a, double c1, double an, double bn,
                 double dt, cudaStream_t st) {
     const size_t S = (size_t)g.L * g.N1;
-    k_rhs<T><<<nblk(S, 256), 256, 0, st>>>(g, w, N, Nprev, a, (T)c1, (T)an, (T)bn, (T)dt, 0);
+    launch_k(k_rhs<T>, nblk(S, 256), 256, 0, st, g, w, N, Nprev, a, (T)c1, (T)an, (T)bn, (T)dt, 0);
 }
 
 template <typename T>
 void launch_laplacian(const GridDev& g, const T* w, T* out, cudaStream_t st) {
     const size_t S = (size_t)g.L * g.N1;
-    k_rhs<T><<<nblk(S, 256), 256, 0, st>>>(g, w, nullptr, nullptr, out, (T)0, (T)0, (T)0, (T)0, 1);
+    launch_k(k_rhs<T>, nblk(S, 256), 256, 0, st, g, w, nullptr, nullptr, out, (T)0, (T)0, (T)0, (T)0, 1);
 }
 
 // E applied to given level-0 fluxes (Regularizer::toBoundary)
 __global__ void k_reg_gather(int ncomp, const int* __restrict__ sidx, const double* __restrict__ sw,
                              const int* __restrict__ sn, const double* __restrict__ q0, double dx,
                              double* __restrict__ out) {
+    pdl_enter();
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncomp) return;
     double acc = 0.0;
@@ -792,73 +814,73 @@ __global__ void k_reg_gather(int ncomp, const int* __restrict__ sidx, const doub
 
 void launch_reg_gather(const GridDev& g, int ncomp, const RegSlots& s, const double* q0, double* out,
                        cudaStream_t st) {
-    k_reg_gather<<<nblk(ncomp, 128), 128, 0, st>>>(ncomp, s.idx, s.w, s.n, q0, g.dx, out);
+    launch_k(k_reg_gather, nblk(ncomp, 128), 128, 0, st, ncomp, s.idx, s.w, s.n, q0, g.dx, out);
 }
 
 template <typename T>
 void launch_refresh_flux(const GridDev& g, const T* psi, T* q, double u0, double v0, const double* q0f,
                          cudaStream_t st) {
     const size_t F = (size_t)g.L * g.F1;
-    k_refresh_flux<T><<<nblk(F, 256), 256, 0, st>>>(g, psi, q, u0, v0, q0f);
+    launch_k(k_refresh_flux<T>, nblk(F, 256), 256, 0, st, g, psi, q, u0, v0, q0f);
 }
 
 void launch_flux_to_vel(const GridDev& g, const double* q, double* u, double* v, cudaStream_t st) {
     const size_t S = (size_t)g.L * g.N1;
-    k_flux_to_vel<<<nblk(S, 256), 256, 0, st>>>(g, q, u, v);
+    launch_k(k_flux_to_vel, nblk(S, 256), 256, 0, st, g, q, u, v);
 }
 
 void launch_frame_flow(const BodyDev* bf, MotionState* ms, const double* mtab, const double* time_ptr, double toff,
                        double magBF, double alphaBF, double* out, cudaStream_t st) {
-    k_frame_flow<<<1, 32, 0, st>>>(bf, ms, mtab, time_ptr, toff, magBF, alphaBF, out);
+    launch_k(k_frame_flow, 1, 32, 0, st, bf, ms, mtab, time_ptr, toff, magBF, alphaBF, out);
 }
 
 void launch_frame_flux(const GridDev& g, const double* fv, double xc, double yc, double* q0, cudaStream_t st) {
     const size_t F = (size_t)g.L * g.F1;
-    k_frame_flux<<<nblk(F, 256), 256, 0, st>>>(g, fv, xc, yc, q0);
+    launch_k(k_frame_flux, nblk(F, 256), 256, 0, st, g, fv, xc, yc, q0);
 }
 
 void launch_bcon_field(int ncomp, const RegSlots& s, const double* vel, const double* q0, double h, double* bcon,
                        cudaStream_t st) {
-    k_bcon_field<<<nblk(ncomp, 128), 128, 0, st>>>(ncomp, s.idx, s.w, s.n, vel, q0, h, bcon);
+    launch_k(k_bcon_field, nblk(ncomp, 128), 128, 0, st, ncomp, s.idx, s.w, s.n, vel, q0, h, bcon);
 }
 
 void launch_motion_state(int nbodies, const BodyDev* bodies, const double* time_ptr, double toff, MotionState* ms,
                          cudaStream_t st) {
-    k_motion_state<<<nblk(nbodies, 32), 32, 0, st>>>(nbodies, bodies, time_ptr, toff, ms);
+    launch_k(k_motion_state, nblk(nbodies, 32), 32, 0, st, nbodies, bodies, time_ptr, toff, ms);
 }
 
 void launch_kinematics(int npts, const double* ref_xy, const int* body_of, const BodyDev* bodies,
                        const MotionState* ms, const double* mtab, const double* time_ptr, double toff, double* pts,
                        double* vel, cudaStream_t st) {
-    k_kinematics<<<nblk(npts, 128), 128, 0, st>>>(npts, ref_xy, body_of, bodies, ms, mtab, time_ptr, toff, pts, vel);
+    launch_k(k_kinematics, nblk(npts, 128), 128, 0, st, npts, ref_xy, body_of, bodies, ms, mtab, time_ptr, toff, pts, vel);
 }
 
 void launch_reg_update(const GridDev& g, int npts, const double* pts, const double* vel, RegSlots& s, double* bcon,
                        double u0, double v0, cudaStream_t st) {
-    k_reg_update<<<nblk(2 * npts, 128), 128, 0, st>>>(g, npts, pts, vel, s.idx, s.w, s.n, bcon, u0, v0);
+    launch_k(k_reg_update, nblk(2 * npts, 128), 128, 0, st, g, npts, pts, vel, s.idx, s.w, s.n, bcon, u0, v0);
 }
 
 template <typename T>
 void launch_reg_interp(const GridDev& g, int ncomp, const RegSlots& s, const T* psi, size_t sstride, int batch,
                        const double* bcon, double* out, size_t ostride, cudaStream_t st) {
-    k_reg_interp<T><<<dim3(nblk(ncomp, 128), batch), 128, 0, st>>>(g, ncomp, s.idx, s.w, s.n, psi, sstride, bcon, out,
+    launch_k(k_reg_interp<T>, dim3(nblk(ncomp, 128), batch), 128, 0, st, g, ncomp, s.idx, s.w, s.n, psi, sstride, bcon, out,
                                                                     ostride);
 }
 
 template <typename T>
 void launch_smear_bf(const GridDev& g, int ncomp, const RegSlots& s, const double* f, double* flux0, T* Bf,
                      double beta, cudaStream_t st) {
-    k_reg_smear<<<nblk((size_t)ncomp * kSlots, 128), 128, 0, st>>>(ncomp, s.idx, s.w, s.n, f, flux0);
-    k_bf<T><<<dim3(nblk(g.N1, 256), 1), 256, 0, st>>>(g, flux0, 0, Bf, 0, beta);
-    k_reg_zero<<<nblk((size_t)ncomp * kSlots, 128), 128, 0, st>>>(ncomp, 0, 0, s.idx, s.n, flux0, 0);
+    launch_k(k_reg_smear, nblk((size_t)ncomp * kSlots, 128), 128, 0, st, ncomp, s.idx, s.w, s.n, f, flux0);
+    launch_k(k_bf<T>, dim3(nblk(g.N1, 256), 1), 256, 0, st, g, flux0, 0, Bf, 0, beta);
+    launch_k(k_reg_zero, nblk((size_t)ncomp * kSlots, 128), 128, 0, st, ncomp, 0, 0, s.idx, s.n, flux0, 0);
 }
 
 template <typename T>
 void launch_smear_bf_unit(const GridDev& g, int ncomp, int col0, int batch, const RegSlots& s, double* flux0,
                           size_t fstride, T* Bf, size_t sstride, double beta, cudaStream_t st) {
-    k_reg_smear_unit<<<batch, 32, 0, st>>>(ncomp, col0, s.idx, s.w, s.n, flux0, fstride);
-    k_bf<T><<<dim3(nblk(g.N1, 256), batch), 256, 0, st>>>(g, flux0, fstride, Bf, sstride, beta);
-    k_reg_zero<<<batch, 32, 0, st>>>(ncomp, col0, 1, s.idx, s.n, flux0, fstride);
+    launch_k(k_reg_smear_unit, batch, 32, 0, st, ncomp, col0, s.idx, s.w, s.n, flux0, fstride);
+    launch_k(k_bf<T>, dim3(nblk(g.N1, 256), batch), 256, 0, st, g, flux0, fstride, Bf, sstride, beta);
+    launch_k(k_reg_zero, batch, 32, 0, st, ncomp, col0, 1, s.idx, s.n, flux0, fstride);
 }
 
 #define IBG_INST(T)                                                                                            \
