@@ -180,6 +180,113 @@ __device__ C* fft_smem(C* s0, C* s1, const C* tw, const FftDesc& d, int P) {
 }
 
 // ---------------------------------------------------------------------------
+// The same Stockham FFT with the length known at compile time, for the lengths
+// of the benchmark grids: the radices follow factorize()'s order (every 4,
+// then 2, 3, 5, 7, ...), so the butterflies, twiddles and their order are
+// those of fft_smem; only the index arithmetic (divisions by the stride and
+// the butterfly count) becomes constant.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int next_radix(int rem) {
+    return rem % 4 == 0 ? 4 : rem % 2 == 0 ? 2 : rem % 3 == 0 ? 3 : rem % 5 == 0 ? 5 : rem % 7 == 0 ? 7 : rem;
+}
+
+template <typename C, int R, int M, int NS>
+__device__ __forceinline__ void bfly_c(const C* __restrict__ sp, C* __restrict__ dp, const C* __restrict__ tw, int j) {
+    constexpr int MR = M / R;
+    constexpr int TSTEP = M / (NS * R);
+    const int jm = j % NS;
+    C v[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+        C x = sp[j + q * MR];
+        v[q] = q == 0 ? x : cmul(x, tw[jm * q * TSTEP]);
+    }
+    C o[R];
+    if (R == 2) {
+        o[0] = cadd(v[0], v[1]);
+        o[1] = csub(v[0], v[1]);
+    } else if (R == 4) {
+        C t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+        C t2 = cadd(v[1], v[3]), t3 = csub(v[1], v[3]);
+        o[0] = cadd(t0, t2);
+        o[2] = csub(t0, t2);
+        o[1] = cmk<C>(t1.x + t3.y, t1.y - t3.x);
+        o[3] = cmk<C>(t1.x - t3.y, t1.y + t3.x);
+    } else if (R == 3) {
+        using V = decltype(v[0].x);
+        const V c3 = (V)-0.5, s3 = (V)-0.86602540378443864676;
+        const C t = cadd(v[1], v[2]), d = csub(v[1], v[2]);
+        o[0] = cadd(v[0], t);
+        const C m1 = cmk<C>(v[0].x + c3 * t.x, v[0].y + c3 * t.y);
+        o[1] = cmk<C>(m1.x - s3 * d.y, m1.y + s3 * d.x);
+        o[2] = cmk<C>(m1.x + s3 * d.y, m1.y - s3 * d.x);
+    } else if (R == 5) {
+        using V = decltype(v[0].x);
+        const V c1 = (V)0.30901699437494742410, c2 = (V)-0.80901699437494742410;
+        const V s1 = (V)-0.95105651629515357212, s2 = (V)-0.58778525229247312917;
+        const C a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
+        const C a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
+        o[0] = cadd(v[0], cadd(a1, a2));
+        const C m1 = cmk<C>(v[0].x + c1 * a1.x + c2 * a2.x, v[0].y + c1 * a1.y + c2 * a2.y);
+        const C m2 = cmk<C>(v[0].x + c2 * a1.x + c1 * a2.x, v[0].y + c2 * a1.y + c1 * a2.y);
+        const V n1r = -(s1 * b1.y + s2 * b2.y), n1i = s1 * b1.x + s2 * b2.x;
+        const V n2r = -(s2 * b1.y - s1 * b2.y), n2i = s2 * b1.x - s1 * b2.x;
+        o[1] = cmk<C>(m1.x + n1r, m1.y + n1i);
+        o[4] = cmk<C>(m1.x - n1r, m1.y - n1i);
+        o[2] = cmk<C>(m2.x + n2r, m2.y + n2i);
+        o[3] = cmk<C>(m2.x - n2r, m2.y - n2i);
+    } else {
+        constexpr int RSTEP = M / R;
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            C acc = v[0];
+#pragma unroll
+            for (int q = 1; q < R; ++q) acc = cadd(acc, cmul(v[q], tw[((k * q) % R) * RSTEP]));
+            o[k] = acc;
+        }
+    }
+    const int idxd = (j / NS) * NS * R + jm;
+#pragma unroll
+    for (int k = 0; k < R; ++k) dp[idxd + k * NS] = o[k];
+}
+
+template <typename C, int M, int NS>
+__device__ __forceinline__ C* fft_stages_c(C* src, C* dst, const C* tw, int P) {
+    if constexpr (NS >= M) {
+        return src;
+    } else {
+        constexpr int R = next_radix(M / NS);
+        constexpr int MR = M / R;
+        const int total = P * MR;
+        for (int t = threadIdx.x; t < total; t += blockDim.x) {
+            const int p = t / MR;
+            const int j = t - p * MR;
+            bfly_c<C, R, M, NS>(src + p * M, dst + p * M, tw, j);
+        }
+        __syncthreads();
+        return fft_stages_c<C, M, NS * R>(dst, src, tw, P);
+    }
+}
+
+// fft_smem with a compile-time length where one is instantiated
+template <typename C>
+__device__ C* fft_any(C* s0, C* s1, const C* tw, const FftDesc& d, int P) {
+    switch (d.m) {
+        case 256: return fft_stages_c<C, 256, 1>(s0, s1, tw, P);
+        case 384: return fft_stages_c<C, 384, 1>(s0, s1, tw, P);
+        case 400: return fft_stages_c<C, 400, 1>(s0, s1, tw, P);
+        case 500: return fft_stages_c<C, 500, 1>(s0, s1, tw, P);
+        case 512: return fft_stages_c<C, 512, 1>(s0, s1, tw, P);
+        case 768: return fft_stages_c<C, 768, 1>(s0, s1, tw, P);
+        case 800: return fft_stages_c<C, 800, 1>(s0, s1, tw, P);
+        case 1000: return fft_stages_c<C, 1000, 1>(s0, s1, tw, P);
+        case 1024: return fft_stages_c<C, 1024, 1>(s0, s1, tw, P);
+        case 2048: return fft_stages_c<C, 2048, 1>(s0, s1, tw, P);
+        default: return fft_smem<C>(s0, s1, tw, d, P);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // rows: DST-I along j for pairs of rows of every level in the launch
 // (blockIdx.y = batch * nlev + level).  Inside a level's overlap interior
 // the input comes from `alt` (the coarsified right-hand side) when given.
@@ -234,7 +341,7 @@ __global__ void k_dst_rows(RowPassArgs<T> a) {
         }
     }
     __syncthreads();
-    C* res = fft_smem<C>(s0, s1, tw, d, P);
+    C* res = fft_any<C>(s0, s1, tw, d, P);
     T* out = a.out[l] + (size_t)b * a.out_bstride;
     T* out2 = a.out2[l] ? a.out2[l] + (size_t)b * a.out_bstride : nullptr;
     const T* base = a.base[l] ? a.base[l] + (size_t)b * a.out_bstride : nullptr;
@@ -335,7 +442,7 @@ __global__ void k_dst_cols(ColPassArgs<T> a) {
         s0[p * m + n + 1] = cmk<C>((T)0, (T)0);
     }
     __syncthreads();
-    C* res = fft_smem<C>(s0, s1, tw, d, P);
+    C* res = fft_any<C>(s0, s1, tw, d, P);
     if (a.mode == 1) {
         C* other = (res == s0) ? s1 : s0;
         for (int t = threadIdx.x; t < P * n; t += blockDim.x) {
@@ -355,7 +462,7 @@ __global__ void k_dst_cols(ColPassArgs<T> a) {
             }
         }
         __syncthreads();
-        res = fft_smem<C>(other, res, tw, d, P);
+        res = fft_any<C>(other, res, tw, d, P);
     }
     for (int t = threadIdx.x; t < n * w; t += blockDim.x) {
         const int i = t / w;

@@ -54,6 +54,24 @@ def test_elliptic_and_stencils(gp):
     s.close()
 
 
+# grids whose DST lengths 2 nx and 2 ny have compile-time FFT plans (256, 384, 400, 512, 768, 800, 1000,
+# 1024, 2048; the small grids above take the general path)
+COMPILED_FFT_GRIDS = [(128, 192, 2, 4.0, -2.0, -3.0), (256, 200, 3, 4.0, -2.0, -1.5625),
+                      (500, 200, 2, 10.0, -5.0, -2.0), (384, 512, 2, 6.0, -3.0, -4.0), (1024, 128, 2, 8.0, -4.0, -0.5)]
+
+
+@pytest.mark.parametrize("gp", COMPILED_FFT_GRIDS)
+def test_compiled_fft_lengths_match_oracle(gp):
+    from oracle import ibpm_oracle as O
+    g = O.Grid(*gp)
+    grid, model, s = _solver_for(gp, O.circle_points(0.0, 0.0, 0.3, 24))
+    rng = np.random.default_rng(gp[0] + gp[1])
+    f = rng.standard_normal(g.scalar().shape)
+    assert rel_l2(s.poisson(f), O.EllipticSolver(g, "poisson").solve(f)) < OP_TOL
+    assert rel_l2(s.helmholtz(-0.0123, f), O.EllipticSolver(g, "helmholtz", -0.0123).solve(f)) < OP_TOL
+    s.close()
+
+
 def test_multidomain_inverse_property_full_size():
     """L(solve(f)) = coarsify(f) on every level at the 400x200, 5-level size
     (the reference's EllipticSolverTest property, src test/EllipticSolverTest.cc:86-121)."""
