@@ -270,7 +270,7 @@ __device__ __forceinline__ C* fft_stages_c(C* src, C* dst, const C* tw, int P) {
 
 // fft_smem with a compile-time length where one is instantiated
 template <typename C>
-__device__ C* fft_any(C* s0, C* s1, const C* tw, const FftDesc& d, int P) {
+__device__ __forceinline__ C* fft_any(C* s0, C* s1, const C* tw, const FftDesc& d, int P) {
     switch (d.m) {
         case 256: return fft_stages_c<C, 256, 1>(s0, s1, tw, P);
         case 384: return fft_stages_c<C, 384, 1>(s0, s1, tw, P);
@@ -316,9 +316,8 @@ __global__ void k_dst_rows(RowPassArgs<T> a) {
     const int pair0 = blockIdx.x * P;
     const int npairs = (g.NI + 1) / 2;
     const int ilo = g.nxe, ihi = g.nx / 2 + g.nxe, jlo = g.nye, jhi = g.ny / 2 + g.nye;
-    for (int t = threadIdx.x; t < P * n; t += blockDim.x) {
-        const int p = t / n;
-        const int k = t - p * n;
+    for (int p = 0; p < P; ++p)
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
         const int pair = pair0 + p;
         C* z = s0 + p * m;
         T va = (T)0, vb = (T)0;
@@ -345,9 +344,8 @@ __global__ void k_dst_rows(RowPassArgs<T> a) {
     T* out = a.out[l] + (size_t)b * a.out_bstride;
     T* out2 = a.out2[l] ? a.out2[l] + (size_t)b * a.out_bstride : nullptr;
     const T* base = a.base[l] ? a.base[l] + (size_t)b * a.out_bstride : nullptr;
-    for (int t = threadIdx.x; t < P * n; t += blockDim.x) {
-        const int p = t / n;
-        const int k = t - p * n;
+    for (int p = 0; p < P; ++p)
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
         const int pair = pair0 + p;
         if (pair >= npairs) continue;
         const C z = res[p * m + k + 1];
@@ -421,9 +419,10 @@ __global__ void k_dst_cols(ColPassArgs<T> a) {
     const T bydx2 = a.bydx2[lev], bcc = a.bc_coef[lev];
     const int col0 = blockIdx.x * 2 * P;
     const int w = 2 * P;
+    const int lw = P == 1 ? 1 : P == 2 ? 2 : 3;  // log2(w), P in {1, 2, 4}
     for (int t = threadIdx.x; t < n * w; t += blockDim.x) {
-        const int i = t / w;
-        const int c = t - i * w;
+        const int i = t >> lw;
+        const int c = t & (w - 1);
         const int col = col0 + c;
         T v = col < NJ ? buf[(size_t)i * NJ + col] : (T)0;
         if (a.mode == 3 && col < NJ)
@@ -445,9 +444,8 @@ __global__ void k_dst_cols(ColPassArgs<T> a) {
     C* res = fft_any<C>(s0, s1, tw, d, P);
     if (a.mode == 1) {
         C* other = (res == s0) ? s1 : s0;
-        for (int t = threadIdx.x; t < P * n; t += blockDim.x) {
-            const int p = t / n;
-            const int k = t - p * n;
+        for (int p = 0; p < P; ++p)
+        for (int k = threadIdx.x; k < n; k += blockDim.x) {
             const C z = res[p * m + k + 1];
             const int ca = col0 + 2 * p, cb = ca + 1;
             const T ea = eig_inverse(a.cosx, a.cosy, k, ca < NJ ? ca : 0, bydx2, a.helmholtz, a.alpha);
@@ -465,8 +463,8 @@ __global__ void k_dst_cols(ColPassArgs<T> a) {
         res = fft_any<C>(other, res, tw, d, P);
     }
     for (int t = threadIdx.x; t < n * w; t += blockDim.x) {
-        const int i = t / w;
-        const int c = t - i * w;
+        const int i = t >> lw;
+        const int c = t & (w - 1);
         const int col = col0 + c;
         if (col >= NJ) continue;
         const C z = res[(c >> 1) * m + i + 1];
@@ -528,7 +526,7 @@ __device__ void dst_pair_block(const FftDesc& d, int n, const T* a_in, const T* 
         s0[n + 1] = cmk<C>((T)0, (T)0);
     }
     __syncthreads();
-    C* res = fft_smem<C>(s0, s1, reinterpret_cast<const C*>(d.tw), d, 1);
+    C* res = fft_any<C>(s0, s1, reinterpret_cast<const C*>(d.tw), d, 1);
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
         const C z = res[k + 1];
         a_out[k] = -z.y * scale;
