@@ -392,6 +392,8 @@ __device__ __forceinline__ T lifted_coef(T R, int k, int l, const T* edges, int 
 // transform; mode 1: transform, eigen-inverse scaling, transform (one level);
 // mode 3: boundary lifting and eigen-inverse on load, then one transform.
 // ---------------------------------------------------------------------------
+constexpr int kColLoads = 4;  // elements each thread of k_dst_cols loads before storing any
+
 template <typename T>
 __global__ void k_dst_cols(ColPassArgs<T> a) {
     pdl_enter();
@@ -420,20 +422,41 @@ __global__ void k_dst_cols(ColPassArgs<T> a) {
     const int col0 = blockIdx.x * 2 * P;
     const int w = 2 * P;
     const int lw = P == 1 ? 1 : P == 2 ? 2 : 3;  // log2(w), P in {1, 2, 4}
-    for (int t = threadIdx.x; t < n * w; t += blockDim.x) {
-        const int i = t >> lw;
-        const int c = t & (w - 1);
-        const int col = col0 + c;
-        T v = col < NJ ? buf[(size_t)i * NJ + col] : (T)0;
-        if (a.mode == 3 && col < NJ)
-            v = lifted_coef(v, i, col, edges, n, NJ, bcc, a.s, a.cosx, a.cosy, bydx2, a.helmholtz, a.alpha);
-        C* z = s0 + (c >> 1) * m;
-        if (c & 1) {
-            z[i + 1].y = v;
-            z[m - 1 - i].y = -v;
-        } else {
-            z[i + 1].x = v;
-            z[m - 1 - i].x = -v;
+    // kColLoads elements per thread are loaded (and lifted) before any is stored, so their global
+    // loads are in flight together
+    const int nw_ = n * w;
+    for (int t0 = threadIdx.x; t0 < nw_; t0 += kColLoads * blockDim.x) {
+        T vals[kColLoads];
+#pragma unroll
+        for (int u = 0; u < kColLoads; ++u) {
+            const int t = t0 + u * (int)blockDim.x;
+            vals[u] = (T)0;
+            if (t < nw_) {
+                const int i = t >> lw;
+                const int col = col0 + (t & (w - 1));
+                if (col < NJ) {
+                    vals[u] = buf[(size_t)i * NJ + col];
+                    if (a.mode == 3)
+                        vals[u] = lifted_coef(vals[u], i, col, edges, n, NJ, bcc, a.s, a.cosx, a.cosy, bydx2,
+                                              a.helmholtz, a.alpha);
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kColLoads; ++u) {
+            const int t = t0 + u * (int)blockDim.x;
+            if (t >= nw_) break;
+            const int i = t >> lw;
+            const int c = t & (w - 1);
+            const T v = vals[u];
+            C* z = s0 + (c >> 1) * m;
+            if (c & 1) {
+                z[i + 1].y = v;
+                z[m - 1 - i].y = -v;
+            } else {
+                z[i + 1].x = v;
+                z[m - 1 - i].x = -v;
+            }
         }
     }
     for (int p = threadIdx.x; p < P; p += blockDim.x) {
@@ -702,6 +725,7 @@ __global__ void k_map_to_f32(long n, const double* __restrict__ a, float* __rest
 }
 
 constexpr int kEdgeRows = 8;  // output rows (warps) per block of k_sweep_edges
+constexpr int kEdgePre = 16;  // edge-map entries per lane loaded ahead of the sums in k_sweep_edges
 
 // blockIdx.y = 0: bottom/top lines (A_x, V sums), 1: left/right (A_y, W sums);
 // blockIdx.z = batch item
@@ -718,13 +742,30 @@ __global__ void __launch_bounds__(32 * kEdgeRows) k_sweep_edges(SweepArgs<T> a) 
     if ((int)blockIdx.x * kEdgeRows >= n) return;
     const int b = blockIdx.z;
     const T* sums = a.vrow + (size_t)b * a.wstride + (xdir ? 0 : 2 * (size_t)NI);
+    const int lane = threadIdx.x & 31;
+    // the first kEdgePre entries per lane of this warp's edge-map row do not depend on the sums:
+    // their loads are issued before the sums are staged, so the two latencies overlap
+    const bool active = row < n;
+    const T* Ar = (xdir ? a.ax : a.ay) + (size_t)(active ? row : 0) * n;
+    T pre[kEdgePre];
+#pragma unroll
+    for (int q = 0; q < kEdgePre; ++q) {
+        const int k = lane + 32 * q;
+        pre[q] = (active && k < n) ? Ar[k] : (T)0;
+    }
     for (int k = threadIdx.x; k < 2 * n; k += blockDim.x) v[k] = sums[k];
     __syncthreads();
-    if (row >= n) return;
-    const T* Ar = (xdir ? a.ax : a.ay) + (size_t)row * n;
-    const int lane = threadIdx.x & 31;
+    if (!active) return;
     T s0 = (T)0, s1 = (T)0;
-    for (int k = lane; k < n; k += 32) {
+#pragma unroll
+    for (int q = 0; q < kEdgePre; ++q) {
+        const int k = lane + 32 * q;
+        if (k < n) {
+            s0 += pre[q] * v[k];
+            s1 += pre[q] * v[n + k];
+        }
+    }
+    for (int k = lane + 32 * kEdgePre; k < n; k += 32) {
         const T w = Ar[k];
         s0 += w * v[k];
         s1 += w * v[n + k];
