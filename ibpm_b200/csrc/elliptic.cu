@@ -316,27 +316,36 @@ __global__ void k_dst_rows(RowPassArgs<T> a) {
     const int pair0 = blockIdx.x * P;
     const int npairs = (g.NI + 1) / 2;
     const int ilo = g.nxe, ihi = g.nx / 2 + g.nxe, jlo = g.nye, jhi = g.ny / 2 + g.nye;
-    for (int p = 0; p < P; ++p)
+    // every pair's two loads for column k are issued before any is stored (P <= 4)
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        const int pair = pair0 + p;
-        C* z = s0 + p * m;
-        T va = (T)0, vb = (T)0;
-        if (pair < npairs) {
-            const int r0 = 2 * pair, r1 = 2 * pair + 1;
-            const int J = k + 1;
-            const bool jin = alt && J > jlo && J < jhi;
-            const T* s0p = (jin && r0 + 1 > ilo && r0 + 1 < ihi) ? alt : in;
-            va = a.in_scale * s0p[(size_t)r0 * n + k];
-            if (r1 < g.NI) {
-                const T* s1p = (jin && r1 + 1 > ilo && r1 + 1 < ihi) ? alt : in;
-                vb = a.in_scale * s1p[(size_t)r1 * n + k];
+        T va[4], vb[4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            va[p] = (T)0;
+            vb[p] = (T)0;
+            const int pair = pair0 + p;
+            if (p < P && pair < npairs) {
+                const int r0 = 2 * pair, r1 = 2 * pair + 1;
+                const int J = k + 1;
+                const bool jin = alt && J > jlo && J < jhi;
+                const T* s0p = (jin && r0 + 1 > ilo && r0 + 1 < ihi) ? alt : in;
+                va[p] = a.in_scale * s0p[(size_t)r0 * n + k];
+                if (r1 < g.NI) {
+                    const T* s1p = (jin && r1 + 1 > ilo && r1 + 1 < ihi) ? alt : in;
+                    vb[p] = a.in_scale * s1p[(size_t)r1 * n + k];
+                }
             }
         }
-        z[k + 1] = cmk<C>(va, vb);
-        z[m - 1 - k] = cmk<C>(-va, -vb);
-        if (k == 0) {
-            z[0] = cmk<C>((T)0, (T)0);
-            z[n + 1] = cmk<C>((T)0, (T)0);
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            if (p >= P) break;
+            C* z = s0 + p * m;
+            z[k + 1] = cmk<C>(va[p], vb[p]);
+            z[m - 1 - k] = cmk<C>(-va[p], -vb[p]);
+            if (k == 0) {
+                z[0] = cmk<C>((T)0, (T)0);
+                z[n + 1] = cmk<C>((T)0, (T)0);
+            }
         }
     }
     __syncthreads();
