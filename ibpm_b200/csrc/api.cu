@@ -1057,7 +1057,7 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
         c->own_stream = true;
     }
     int s = IBG_OK;
-    const size_t S = c->S, F = c->F, m = c->ncomp;
+    const size_t m = c->ncomp;
     if ((s = c->fft.init(2 * g.ny, 2 * g.nx)) || (s = c->cosT.init(g.nx, g.ny, g.nxe, g.nye)) ||
         (g.L > 1 && (s = c->cosT.build_edge_maps(g.nx, g.ny, g.nxe, g.nye, c->fft)))) {
         g_create_error = "ibg_create: FFT table setup failed";
