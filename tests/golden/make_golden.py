@@ -146,6 +146,36 @@ UBF_CASES = [
 ]
 
 
+# Motions under the other schemes (AB2 keeps the previous sub-step's nonlinear term, Euler has one
+# sub-step), and two bodies with different motions in one geometry (a history-dependent plunge and a
+# fixed cylinder).
+def _plate_with(line):
+    geom = configs.plate_geom(chord=1.0, npts=17, freq=0.5)
+    return "\n".join(("  motion " + line) if ln.strip().startswith("motion") else ln for ln in geom.splitlines()) + "\n"
+
+
+def _two_bodies():
+    plate = _plate_with("eldredge2 0.5 120 0.005 0.02 0.035 0.05")
+    cyl = configs.cylinder_geom(16, r=0.15).replace("0.0 0.0", "1.2 0.3", 1)
+    return plate + cyl
+
+
+MIXED_CASES = [
+    # name, geometry, scheme, ubf
+    ("motion_sigmoidalstep_ab2", _plate_with("sigmoidalstep 15 0.08 0.005"), "ab2", False),
+    ("motion_lagstep2_euler", _plate_with("lagstep2 5 0.03 0.008 0.004"), "euler", False),
+    ("ubf_pitchplunge_rk3b", _plate_with("pitchplunge -0.3 0.5 0 0.25 0.5 0"), "rk3b", True),
+    ("motion_two_bodies_rk3", None, "rk3", False),
+]
+
+
+def run_mixed(case):
+    name, geom, scheme, ubf = case
+    if geom is None:
+        geom = _two_bodies()
+    run((name, 64, 32, 2, 4.0, -2.0, -1.0, geom, 300.0, 0.01, 6, scheme, 1e-10, None), None, ubf)
+
+
 # The other N(x) variants of the reference (src/IBSolver.cc:211-311) on one small two-domain case.
 # The base states of the linear models are states of a short nonlinear run written by the reference.
 VARIANT_GRID = dict(nx=32, ny=32, ngrid=2, length=3.0, xoff=-1.5, yoff=-1.5)
@@ -224,6 +254,9 @@ if __name__ == "__main__":
     for c in UBF_CASES:
         if not only or "ubf_" + c[0] in only:
             run_motion(c, ubf=True)
+    for c in MIXED_CASES:
+        if not only or c[0] in only:
+            run_mixed(c)
     for c in VARIANTS:
         if not only or c[0] in only:
             run_variant(c)
