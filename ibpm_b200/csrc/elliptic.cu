@@ -375,9 +375,12 @@ __global__ void k_dst_rows(RowPassArgs<T> a) {
 // eigenvalue of the inverse operator at 0-based mode (k, l):
 // lambda = 2 (cos(pi (k+1)/nx) + cos(pi (l+1)/ny) - 2) / dx^2 (src/EllipticSolver2d.cc:42-54),
 // 1/lambda (Poisson, :115-122) or 1/(1 + alpha lambda) (Helmholtz, :156-163)
+// The FP64 tables hold the cosines and lambda is formed as the reference forms it; the FP32 tables hold
+// cos - 1 (tabulated in double as -2 sin^2(theta / 2)), because in float cos + cos - 2 cancels for the
+// low modes: at n = 512 the lowest eigenvalue would lose three digits and the forces ~1e-4.
 template <typename T>
 __device__ __forceinline__ T eig_inverse(const T* cx, const T* cy, int k, int l, T bydx2, int helm, T alpha) {
-    const T lam = (T)2 * (cx[k + 1] + cy[l + 1] - (T)2) * bydx2;
+    const T lam = sizeof(T) == 8 ? (T)2 * (cx[k + 1] + cy[l + 1] - (T)2) * bydx2 : (T)2 * (cx[k + 1] + cy[l + 1]) * bydx2;
     return helm ? (T)1 / ((T)1 + alpha * lam) : (T)1 / lam;
 }
 
@@ -911,6 +914,10 @@ int CosTables::init(int nx, int ny, int nxe, int nye) {
     fill_grid_tables(nx, ny, nxe, nye, h);
     std::vector<float> hf(h.size());
     for (size_t k = 0; k < h.size(); ++k) hf[k] = (float)h[k];
+    // FP32 eigenvalue tables: cos(pi i / n) - 1 = -2 sin^2(pi i / (2 n)), without cancellation
+    const double pi = 4. * atan(1.0);
+    for (int i = 0; i < nx; ++i) hf[i] = (float)(-2.0 * sin(pi * i / (2.0 * nx)) * sin(pi * i / (2.0 * nx)));
+    for (int j = 0; j < ny; ++j) hf[nx + j] = (float)(-2.0 * sin(pi * j / (2.0 * ny)) * sin(pi * j / (2.0 * ny)));
     if (cudaMalloc(&d64, sizeof(double) * h.size()) || cudaMalloc(&d32, sizeof(float) * h.size()))
         return IBG_ERR_CUDA;
     cudaMemcpy(d64, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice);

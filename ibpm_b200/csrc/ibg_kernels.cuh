@@ -69,7 +69,7 @@ struct ColPassArgs {
 
 template <typename T>
 struct GridTables {
-    const T* cosx = nullptr;   // cos(pi i / nx), i < nx
+    const T* cosx = nullptr;   // cos(pi i / nx), i < nx (FP32 tables: cos(pi i / nx) - 1)
     const T* cosy = nullptr;
     SineTab<T> s{};
     // edge maps of the coarse-to-fine sweep (row-major NI x NI and NJ x NJ; nullptr: FFT path)
