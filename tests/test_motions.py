@@ -204,3 +204,31 @@ def test_moving_frame_needs_one_body_and_ignores_a_fixed_one():
     s.advance_resident(n)
     assert rel_l2(s.force_history(n), d["forces"][:, 2:4]) < FP64_TOL
     s.close()
+
+
+@pytest.mark.gpu
+def test_create_rejects_degenerate_motions():
+    """ibg_create refuses motions whose reference formulas would divide by zero or that are not
+    well formed (the reference would step on with infinities): a zero sigmoid duration, a zero lag
+    time constant, an Eldredge ramp with no plateau, a motion file running backwards in time."""
+    import ibpm_b200 as ib
+    grid = ib.Grid(32, 32, 1, 4.0, -2.0, -2.0)
+    pts = [(x, 0.0) for x in np.linspace(-0.5, 0.5, 9)]
+    bad = [(G.MOTION_SIGMOIDALSTEP, (15.0, 0.0, 0.0), None),
+           (G.MOTION_LAGSTEP1, (5.0, 0.03, 0.0, 0.0), None),
+           (G.MOTION_ELDREDGE, (10.0, 50.0, 0.1, 0.1, 0.1, 0.1), None),
+           (G.MOTION_FILE, (), np.array([[0.1, 0, 0, 0, 0, 0, 0], [0.0, 0, 0, 0, 0, 0, 0]])),
+           (G.MOTION_PITCHPLUNGE, (float("nan"), 0.5, 0.0, 0.1, 0.5, 0.0), None)]
+    for code, params, table in bad:
+        body = G.RigidBody(points=list(pts), center=(0.0, 0.0), motion=code, params=params, table=table)
+        model = ib.NavierStokesModel(grid, G.Geometry([body]), 100.0)
+        with pytest.raises(ib.IbgError):
+            ib.NonlinearIBSolver(grid, model, 0.01)
+    # an empty motion file is the reference's zero transformation: the body stays where it is
+    body = G.RigidBody(points=list(pts), center=(0.0, 0.0), motion=G.MOTION_FILE, params=(),
+                       table=np.zeros((0, 7)))
+    s = ib.NonlinearIBSolver(grid, ib.NavierStokesModel(grid, G.Geometry([body]), 100.0), 0.01)
+    s.update_operators(0.37)
+    p, v = s.boundary()
+    assert np.array_equal(p, np.array(pts)) and not np.any(v)
+    s.close()
