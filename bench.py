@@ -97,7 +97,9 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.p = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device}.csv")
+        # raw samples beside the run (IBG_CLOCKS_DIR, else the temp directory); the JSON line carries the summary
+        import tempfile
+        self.path = os.path.join(os.environ.get("IBG_CLOCKS_DIR", tempfile.gettempdir()), f"clocks_rank{device}.csv")
 
     def start(self):
         try:
