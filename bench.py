@@ -203,7 +203,8 @@ def run_reference(args):
     cb = cpu_baseline(wlname, steps=steps)
     v = cb["value"]
     out = {"metric": METRICS[wlname], "unit": UNIT, "n_gpus": args.gpus, "steps": steps, "warmup": 1,
-           "value": v, "ms_per_step": 1000.0 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "value": v, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+           "scaling": "strong" if wlname == "c4" else "weak", "vs_baseline": None,
            "dtype": "f64", "data": "synthetic", "config": _config(wlname, "reference FP64 CPU"), "impl": "reference",
            "cpu_baseline": dict(cb, sample=cb["sample"] + f" (requested --steps {args.steps}; capped at {cap} to "
                                                           f"bound CPU time)"),
