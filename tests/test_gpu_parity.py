@@ -233,6 +233,26 @@ def test_fp32_form_within_force_and_vorticity_bars(name):
     s.close()
 
 
+@pytest.mark.parametrize("member", [13, 29])
+def test_fp32_member_forces_within_1e4(member):
+    """An FP32-bulk ensemble member (a 512x512 single-domain and a 128x128 two-domain ellipse) against
+    the same member in FP64: forces within 1e-4 over 12 steps from rest.  In float, the eigenvalues'
+    cos + cos - 2 cancels for the low modes; the FP32 tables hold cos - 1 instead."""
+    import ibpm_b200 as ib
+    from ibpm_b200 import configs
+    wl = configs.ensemble_members(count=64)[member]
+    n = 12
+    F = {}
+    for prec in ("fp64", "fp32"):
+        grid, model, s, x = ib.from_workload(wl, precision=prec)
+        s.init()
+        s.set_state(x, with_q=False)
+        s.advance_resident(n)
+        F[prec] = s.force_history(n)
+        s.close()
+    assert rel_l2(F["fp32"], F["fp64"]) < 1e-4
+
+
 def test_ensemble_matches_members_stepped_alone():
     """Members advanced by one ensemble graph give the same forces and
     vorticity as the same members advanced one by one."""
