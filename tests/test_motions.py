@@ -232,3 +232,23 @@ def test_create_rejects_degenerate_motions():
     p, v = s.boundary()
     assert np.array_equal(p, np.array(pts)) and not np.any(v)
     s.close()
+
+
+def test_oracle_moving_frame_flow_is_divergence_free_rigid_motion():
+    """A rotating frame's base flow is rigid: on every level the discrete divergence of q0 vanishes
+    and its vorticity is the same at every interior node, -2 thetadot (seen from the body, the flow
+    turns the other way)."""
+    g = O.Grid(32, 16, 2, 4.0, -2.0, -1.0)
+    b = O.Body(np.array([[0.0, 0.0], [0.5, 0.0]]), (0.1, -0.05), "fixedvel", (0.3, 0.1, 0.7))
+    m = O.Model(g, [b], 100.0)
+    m.moving_frame()
+    m.update_operators(0.2)
+    for lev in range(g.ngrid):
+        qx = m.q0[lev, : g.n_xflux].reshape(g.nx + 1, g.ny)
+        qy = m.q0[lev, g.n_xflux:].reshape(g.nx, g.ny + 1)
+        div = (qx[1:, :] - qx[:-1, :]) + (qy[:, 1:] - qy[:, :-1])
+        assert np.max(np.abs(div)) < 1e-14
+        # circulation around each interior node's dual cell, per unit area: the same everywhere
+        dx = g.dx_lev(lev)
+        circ = (qy[1:, 1:-1] - qy[:-1, 1:-1]) - (qx[1:-1, 1:] - qx[1:-1, :-1])
+        assert np.ptp(circ) < 1e-13 and abs(circ.mean() / (dx * dx) + 2 * 0.7) < 1e-12
