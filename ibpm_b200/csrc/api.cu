@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "../../include/ibpm_b200.h"
+#include "../../include/ibpm_b200_diag.h"
 #include "ibg_force.cuh"
 #include "ibg_internal.cuh"
 #include "ibg_kernels.cuh"

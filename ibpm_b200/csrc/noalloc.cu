@@ -6,8 +6,9 @@
 // pre-plan every byte of HBM.  For them ibg_poisson_solve_static takes device
 // input and output buffers and keeps its scratch (the coarsified right-hand
 // side and the transform workspace) in the file-scope array below, plus the
-// FFT twiddle and eigenvalue cosine tables in two small file-scope arrays.
-// Every GPU that loads the library holds these arrays until the process exits.
+// FFT twiddle and eigenvalue cosine tables of up to kTableSlots grid shapes in
+// two more file-scope arrays.  Every GPU that loads the library holds these
+// arrays until the process exits.
 #include <cmath>
 #include <mutex>
 #include <string>
@@ -24,26 +25,34 @@ namespace {
 // 4 MiB of scratch: the coarsified right-hand side, the spectral coefficients
 // of every level and the coarse-to-fine sweep workspace must fit in it
 constexpr size_t kStaticScratchDoubles = (size_t)1 << 19;
-// twiddles for FFT lengths up to 2 * 2048 (nx, ny <= 2048) and the grid tables
+// twiddles for FFT lengths up to 2 * 2048 (nx, ny <= 2048) and the grid tables,
+// one block per grid shape for up to kTableSlots shapes
 constexpr int kStaticMaxM = 4096;
 constexpr int kStaticMaxN = 2048;
 constexpr size_t kStaticTableDoubles = 10 * (size_t)kStaticMaxN;
+constexpr int kTableSlots = 4;
 
 static __device__ __align__(256) double g_static_scratch[kStaticScratchDoubles];
-static __device__ __align__(256) double2 g_static_twiddles[2 * kStaticMaxM];  // rows, then columns
-static __device__ __align__(256) double g_static_cos[kStaticTableDoubles];    // cosine and sine tables
+static __device__ __align__(256) double2 g_static_twiddles[kTableSlots * 2 * kStaticMaxM];  // per slot: rows, columns
+static __device__ __align__(256) double g_static_cos[kTableSlots * kStaticTableDoubles];     // per slot: cos and sine tables
 
+struct TableSlot {
+    int nx = -1, ny = -1;        // shape the slot holds (-1: empty)
+    unsigned long long used = 0; // last use, for least-recently-used replacement
+};
 struct DeviceSymbols {
     bool ready = false;
     double* scratch = nullptr;
     double2* twiddles = nullptr;
     double* cosines = nullptr;
-    int tab_nx = -1, tab_ny = -1;  // sizes the tables currently hold
+    TableSlot slot[kTableSlots];
+    unsigned long long clock = 0;
 };
 constexpr int kMaxDevices = 64;
 DeviceSymbols g_dev[kMaxDevices];
 std::mutex g_mutex;
-std::string g_static_error;
+// the last failure of the calling thread
+thread_local std::string g_static_error;
 
 // doubles of scratch one solve needs: rc (L N1) + coefficients (L N1) + sweep
 size_t static_scratch_need(int nx, int ny, int L) {
@@ -54,6 +63,30 @@ size_t static_scratch_need(int nx, int ny, int L) {
 int fail(int code, const std::string& m) {
     g_static_error = m;
     return code;
+}
+
+// writes the twiddles and grid tables of an nx x ny grid into table slot `k`
+int fill_slot(DeviceSymbols& ds, int k, int nx, int ny, int nxe, int nye, cudaStream_t st) {
+    const double pi = 3.14159265358979323846264338327950288;
+    std::vector<double2> tw(2 * (size_t)kStaticMaxM);
+    const int mr = 2 * ny, mc = 2 * nx;
+    for (int j = 0; j < mr; ++j) {
+        const double a = -2.0 * pi * (double)j / (double)mr;
+        tw[j] = make_double2(cos(a), sin(a));
+    }
+    for (int j = 0; j < mc; ++j) {
+        const double a = -2.0 * pi * (double)j / (double)mc;
+        tw[kStaticMaxM + j] = make_double2(cos(a), sin(a));
+    }
+    std::vector<double> cs;
+    fill_grid_tables(nx, ny, nxe, nye, cs);
+    if (cudaMemcpyAsync(ds.twiddles + (size_t)k * 2 * kStaticMaxM, tw.data(), sizeof(double2) * tw.size(),
+                        cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(ds.cosines + (size_t)k * kStaticTableDoubles, cs.data(), sizeof(double) * cs.size(),
+                        cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return fail(IBG_ERR_CUDA, "ibg_poisson_solve_static: table upload failed");
+    return IBG_OK;
 }
 
 }  // namespace
@@ -82,6 +115,7 @@ extern "C" int ibg_poisson_solve_static(const ibg_grid* grid, const double* f, d
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
         return fail(IBG_ERR_CUDA, "ibg_poisson_solve_static: no usable CUDA device");
+    const int nxe = (int)floor(nx / 4 + 0.5), nye = (int)floor(ny / 4 + 0.5);
 
     std::lock_guard<std::mutex> lock(g_mutex);
     DeviceSymbols& ds = g_dev[dev];
@@ -96,37 +130,35 @@ extern "C" int ibg_poisson_solve_static(const ibg_grid* grid, const double* f, d
                                           cudaGetErrorString(e));
         ds.ready = true;
     }
-    if (ds.tab_nx != nx || ds.tab_ny != ny) {
-        // the same host-computed tables as the context path (FftTables / CosTables)
-        const double pi2 = 3.14159265358979323846264338327950288;
-        std::vector<double2> tw(2 * (size_t)kStaticMaxM);
-        const int mr = 2 * ny, mc = 2 * nx;
-        for (int k = 0; k < mr; ++k) {
-            const double a = -2.0 * pi2 * (double)k / (double)mr;
-            tw[k] = make_double2(cos(a), sin(a));
-        }
-        for (int k = 0; k < mc; ++k) {
-            const double a = -2.0 * pi2 * (double)k / (double)mc;
-            tw[kStaticMaxM + k] = make_double2(cos(a), sin(a));
-        }
-        std::vector<double> cs;
-        fill_grid_tables(nx, ny, (int)floor(nx / 4 * (1 - 0.0) + 0.5), (int)floor(ny / 4 * (1 - 0.0) + 0.5), cs);
-        if (cudaMemcpyAsync(ds.twiddles, tw.data(), sizeof(double2) * tw.size(), cudaMemcpyHostToDevice, st) !=
-                cudaSuccess ||
-            cudaMemcpyAsync(ds.cosines, cs.data(), sizeof(double) * cs.size(), cudaMemcpyHostToDevice, st) !=
-                cudaSuccess ||
-            cudaStreamSynchronize(st) != cudaSuccess)
-            return fail(IBG_ERR_CUDA, "ibg_poisson_solve_static: table upload failed");
-        ds.tab_nx = nx;
-        ds.tab_ny = ny;
+    // the table slot of this shape, or the least recently used one refilled
+    int k = -1;
+    for (int s = 0; s < kTableSlots; ++s)
+        if (ds.slot[s].nx == nx && ds.slot[s].ny == ny) k = s;
+    if (k < 0) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+            return fail(IBG_ERR_UNSUPPORTED,
+                        "ibg_poisson_solve_static: a grid shape's first call uploads its tables and cannot run while "
+                        "the stream is being captured; call once with this shape before capturing");
+        k = 0;
+        for (int s = 1; s < kTableSlots; ++s)
+            if (ds.slot[s].used < ds.slot[k].used) k = s;
+        ds.slot[k].nx = -1;
+        const int s = fill_slot(ds, k, nx, ny, nxe, nye, st);
+        if (s != IBG_OK) return s;
+        ds.slot[k].nx = nx;
+        ds.slot[k].ny = ny;
     }
+    ds.slot[k].used = ++ds.clock;
+    double2* twid = ds.twiddles + (size_t)k * 2 * kStaticMaxM;
+    double* cosines = ds.cosines + (size_t)k * kStaticTableDoubles;
 
     GridDev g{};
     g.nx = nx;
     g.ny = ny;
     g.L = L;
-    g.nxe = (int)floor(nx / 4 * (1 - 0.0) + 0.5);
-    g.nye = (int)floor(ny / 4 * (1 - 0.0) + 0.5);
+    g.nxe = nxe;
+    g.nye = nye;
     g.NI = nx - 1;
     g.NJ = ny - 1;
     g.N1 = g.NI * g.NJ;
@@ -139,13 +171,18 @@ extern "C" int ibg_poisson_solve_static(const ibg_grid* grid, const double* f, d
     FftTables tables;  // descriptors only; the twiddles live in g_static_twiddles
     fft_describe(2 * ny, tables.row64);
     fft_describe(2 * nx, tables.col64);
-    tables.row64.tw = ds.twiddles;
-    tables.col64.tw = ds.twiddles + kStaticMaxM;
+    tables.row64.tw = twid;
+    tables.col64.tw = twid + kStaticMaxM;
     CosTables ct;  // views into g_static_cos; owns nothing
-    ct.attach(nx, ny, ds.cosines, nullptr);
+    ct.attach(nx, ny, cosines, nullptr);
     EllipticPlan<double> plan;
-    if (plan.init(&g, &tables, false, 0.0, ct) != IBG_OK)
-        return fail(IBG_ERR_CUDA, "ibg_poisson_solve_static: kernel set-up failed");
+    const int si = plan.init(&g, &tables, false, 0.0, ct);
+    if (si == IBG_ERR_UNSUPPORTED)
+        return fail(IBG_ERR_UNSUPPORTED,
+                    "ibg_poisson_solve_static: the transform kernels' shared memory for this grid exceeds 200 KiB "
+                    "(16*max(2nx,2ny)*2 + 48*max(nx-1,ny-1) bytes); use ibg_poisson_solve");
+    if (si != IBG_OK)
+        return fail(IBG_ERR_CUDA, "ibg_poisson_solve_static: raising the kernels' shared-memory limit failed");
 
     SolveCall<double> c{};
     c.f = f;

@@ -227,12 +227,6 @@ IBG_API void* ibg_stream(const ibg_context* ctx);
 /* number of kernel launches issued by the last ibg_advance call */
 IBG_API long long ibg_last_launch_count(const ibg_context* ctx);
 
-/* diagnostics: launch one kernel of the time step `reps` times on the context's
- * stream (0: DST-I row pass of the finest level, 1: its column pass with the
- * eigenvalue scaling, 2: the nonlinear term) and return the algorithmic bytes
- * one launch moves (each operand read once, each result written once). */
-IBG_API long long ibg_run_kernel(ibg_context* ctx, int which, int reps);
-
 /* --- ensembles ------------------------------------------------------------------
  * No single reference interface: an ensemble of independent simulations, each an
  * ibg_context with fixed bodies and its own grid, Reynolds number, time step and
@@ -325,17 +319,27 @@ IBG_API int ibg_projection_solve(ibg_context* ctx, int substep, const double* a,
  * services that budget every byte of HBM up front).
  * ibg_poisson_solve_static solves L u = f on all levels, like ibg_poisson_solve,
  * but takes DEVICE pointers f and u (reference Scalar layout), needs no context
- * and allocates nothing: its scratch is a file-scope device array of 4 MiB
+ * and allocates nothing.  Its memory is file-scope device arrays, held by every
+ * GPU that loads the library until the process exits: 4 MiB of scratch
  * (524288 doubles; a solve needs 2*ngrid*(nx-1)*(ny-1) + 2*(ngrid+1)*(nx+ny-2)
- * of them) plus ~160 KiB
- * of tables (nx, ny <= 2048), held by every GPU that loads the library until the
- * process exits.  Larger grids are rejected with IBG_ERR_UNSUPPORTED.  The first
- * call on a device resolves the arrays' device addresses (cudaGetSymbolAddress)
- * and fills the tables; make that first call before any stream capture.  All
- * calls share the scratch, which keeps the last call's contents (each call
- * writes every scratch value it reads, so nothing needs clearing); calls that
- * overlap on the GPU race.  Runs on `cuda_stream` (a cudaStream_t, may be NULL).
- * ibg_static_last_error() describes the last failure. */
+ * of them) and about 1.1 MiB of tables, room for the FFT twiddles and
+ * eigenvalue/sine tables of 4 grid shapes (288 KiB each).
+ * Limits: nx, ny <= 2048; the scratch need above <= 524288; the transform
+ * kernels' shared memory 64*max(nx,ny) + 48*max(nx-1,ny-1) bytes <= 200 KiB
+ * (max(nx, ny) <= 1828).  Other grids are rejected with IBG_ERR_UNSUPPORTED and
+ * a message.
+ * The first call on a device resolves the arrays' device addresses
+ * (cudaGetSymbolAddress); the first call with a grid shape not among the last
+ * four used uploads its tables (replacing the least recently used shape's) and
+ * synchronises the stream.  Make both before any stream capture: a call that
+ * would upload tables while its stream is capturing is refused with
+ * IBG_ERR_UNSUPPORTED.  All calls share the scratch, which keeps the last
+ * call's contents (each call writes every scratch value it reads, so nothing
+ * needs clearing): calls that overlap on the GPU race on it.  The tables of a
+ * shape are rewritten when a fifth shape replaces them, so a call (or a graph
+ * captured from one) still in flight with that shape then reads the wrong
+ * tables.  Runs on `cuda_stream` (a cudaStream_t, may be NULL).
+ * ibg_static_last_error() describes the calling thread's last failure. */
 IBG_API int ibg_poisson_solve_static(const ibg_grid* grid, const double* f, double* u, void* cuda_stream);
 IBG_API const char* ibg_static_last_error(void);
 

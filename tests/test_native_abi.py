@@ -1,6 +1,7 @@
-"""The C-ABI library loads and exports every entry point that
-include/ibpm_b200.h declares (no compute calls: this runs without a GPU)."""
+"""The C-ABI library loads and exports every entry point that the headers
+under include/ declare (no compute calls: this runs without a GPU)."""
 import ctypes
+import glob
 import os
 import re
 
@@ -8,8 +9,10 @@ from helpers import ROOT
 
 
 def declared_symbols():
-    text = open(os.path.join(ROOT, "include", "ibpm_b200.h")).read()
-    return sorted(set(re.findall(r"\b(ibg_[a-zA-Z0-9_]+)\s*\(", text)))
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        names |= set(re.findall(r"\b(ibg_[a-zA-Z0-9_]+)\s*\(", open(h).read()))
+    return sorted(names)
 
 
 def test_header_and_binding_agree():
