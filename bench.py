@@ -1,50 +1,56 @@
 """Benchmark of the IBPM time step on B200 (timesteps/s).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c2|c3|c4] [--form ...]
+                    [--workload c2|c3|c4|c5] [--form ...]
 
 Workloads (seeded synthetic inputs; no dataset is involved):
 
-* c2 (default) multi-domain shedding cylinder: 400x200 cells, 5 nested
-  domains, 157-point cylinder, Re 200, dt 0.005, RK3, seeded 1e-3 vorticity
-  noise in the wake; forms fp64 (plain, default) and fp32 (FP32 bulk, FP64
-  force solve).
+* c4 (default) ensemble of 64 independent ellipse runs (n in {128..512}, 1-3
+  domains, seeded b, orientation, Re; dt = 0.5 dx): forms ensemble_fp32 (all
+  members' steps as branches of one CUDA graph, FP32 bulk members with the
+  force solve in FP64; default), ensemble_refined (the same with FP32
+  transforms plus one FP64-residual refinement per solve), ensemble (FP64
+  members) and serial (each member's captured FP64 step launched after the
+  other on one stream: the plain path).
+* c2 multi-domain shedding cylinder: 400x200 cells, 5 nested domains,
+  157-point cylinder, Re 200, dt 0.005, RK3, seeded 1e-3 vorticity noise in
+  the wake; forms fp32_refined (default), fp32 (FP32 bulk) and fp64 (plain).
 * c3 pitching and plunging plate: 500x250 cells, 3 domains, 51 points,
-  Re 300, dt 0.004, CG tolerance 1e-10; forms cg (the reference's plain CG),
-  cholesky (flexible PCG with the exact inverse rebuilt every 10 steps,
-  default) and learned (flexible PCG with the learned preconditioner,
-  trained first; training time reported, not timed).
-* c4 ensemble of 64 independent ellipse runs (n in {128..512}, 1-3 domains,
-  seeded b, orientation, Re; dt = 0.5 dx): forms ensemble_fp32 (all members'
-  steps as branches of one CUDA graph, FP32 bulk members with the force solve
-  in FP64; default), ensemble (the same with FP64 members) and serial (each
-  member's captured FP64 step launched after the other on one stream).
+  Re 300, dt 0.004, CG tolerance 1e-10; forms cholesky (flexible PCG with the
+  exact inverse rebuilt every --pc-refresh steps, default), learned (flexible
+  PCG with the learned preconditioner, trained first; training time
+  reported, not timed) and cg (the reference's plain CG: the plain path).
+* c5 two cylinders plunging in antiphase: 1024x1024 cells, 5 domains, 2 x 201
+  points, Re 500, dt 0.005, CG tolerance 1e-10; forms cholesky (default),
+  learned and cg (plain), as for c3.
 
 One process per GPU (torchrun for N > 1).  One simulation does not shard
 (its multi-domain solve is global per level and levels are serially
-dependent), so for c2 and c3 N GPUs run N independent replicas (weak
+dependent), so for c2, c3 and c5 N GPUs run N independent replicas (weak
 scaling) and `value` is the total timesteps/s of the job.  The c4 ensemble
-shards by member (rank r advances members r, r + N, ...; strong scaling,
-no exchange while they run, one all-gather of the force histories at the
-end) and `value` is member-timesteps/s of all 64.  Rank 0 prints one JSON
-line.
+shards by member (rank r advances members r, r + N, ...; strong scaling, no
+exchange while they run, one all-gather of the force histories at the end)
+and `value` is member-timesteps/s of all 64.  Rank 0 prints one JSON line.
 
 * value        K steps with the state resident in HBM, CUDA events around each
                step on the stream it runs on, L2 flushed (256 MB write) between
                steps outside the timed events; max over ranks.
-* plain        (c2 fp32, c3, c4) the plain FP64 GPU path of the same workload
-               timed the same way, with the relative L2 difference of the
-               forces of the two runs over the same steps.
+* plain        the plain FP64 GPU path of the same workload timed the same way in
+               the same process: its timesteps/s, the speed-up of the chosen
+               form over it, and the relative L2 differences of the forces over
+               the same W + K steps and of the final vorticity.
 * e2e          the same metric through the public API with the state on the
                host, as the reference's IBSolver::advance(State&) contract has
                it: every step uploads omega, q, f from pinned host memory,
                advances one step and reads omega, q, f back.
 * roofline     the DST-I column pass (the dominant kernel) timed alone with
                CUDA events on the solver's stream against the measured HBM
-               copy bandwidth.
+               copy bandwidth; traffic is null (DRAM bytes come from ncu runs,
+               summarised beside the code under profiles/).
 * cpu_baseline the reference's own CPU code (oracle/_ref/ref_driver: the
                reference sources built with -Ofast and the FFTW shim), one core,
-               a bounded sample of steps of the same workload.
+               a bounded sample of steps of the same workload, with the relative
+               L2 difference of its forces from the GPU run's over the same steps.
 """
 from __future__ import annotations
 
@@ -63,9 +69,15 @@ METRICS = {
     "c2": "timesteps/s (400x200 x5-domain shedding cylinder, RK3)",
     "c3": "timesteps/s (500x250 x3-domain pitching/plunging plate, RK3, CG tol 1e-10)",
     "c4": "member-timesteps/s (ensemble of 64 ellipse runs, n 128-512, 1-3 domains, RK3)",
+    "c5": "timesteps/s (1024x1024 x5-domain pair of plunging cylinders, RK3, CG tol 1e-10)",
 }
-FORMS = {"c2": ("fp64", "fp32"), "c3": ("cholesky", "learned", "cg"), "c4": ("ensemble_fp32", "ensemble", "serial")}
-PLAIN = {"c2": "fp64", "c3": "cg", "c4": "serial"}
+FORMS = {"c2": ("fp32_refined", "fp32", "fp64"), "c3": ("cholesky", "learned", "cg"),
+         "c4": ("ensemble_fp32", "ensemble_refined", "ensemble", "serial"), "c5": ("cholesky", "learned", "cg")}
+PLAIN = {"c2": "fp64", "c3": "cg", "c4": "serial", "c5": "cg"}
+STEPS = {"c2": 200, "c3": 50, "c4": 20, "c5": 10}
+WARMUP = {"c2": 10, "c3": 3, "c4": 3, "c5": 3}
+PC_REFRESH = {"c3": 10, "c5": 50}
+L2_NOTE = "flushed between timed steps (256 MB write outside the events)"
 
 
 def _dist():
@@ -75,15 +87,28 @@ def _dist():
     return ws, rank, local
 
 
-def _config(workload, form, wl=None, extra=None):
-    c = {"workload": workload, "form": form, "l2": "flushed between timed steps (256 MB write outside the events)"}
-    if wl is not None:
-        c.update({"name": wl.name, "nx": wl.nx, "ny": wl.ny, "ngrid": wl.ngrid, "length": wl.length, "Re": wl.Re,
-                  "dt": wl.dt, "scheme": wl.scheme, "cg_tol": wl.tol})
-        if wl.noise_amp:
-            c["initial_condition"] = f"seeded N(0, {wl.noise_amp:g}^2) level-0 wake vorticity (seed {wl.noise_seed})"
-    if extra:
-        c.update(extra)
+def _workload(wlname):
+    from ibpm_b200 import configs
+    return {"c2": configs.c2_shedding_cylinder, "c3": configs.c3_pitching_plate,
+            "c5": configs.c5_two_cylinders}[wlname]()
+
+
+def workload_config(wlname, members=64):
+    """What identifies the workload: the same dict for both arms."""
+    from ibpm_b200 import configs
+    c = {"workload": wlname, "l2": L2_NOTE}
+    if wlname == "c4":
+        ms = configs.ensemble_members(count=members)
+        c.update({"name": f"ensemble of {members} ellipse runs", "members": members, "seed": 11,
+                  "n": [w.nx for w in ms], "ngrid": [w.ngrid for w in ms],
+                  "grid_points_all_levels": int(sum(w.nx * w.ny * w.ngrid for w in ms)), "scheme": "rk3",
+                  "dt": "0.5 dx", "Re": "U[50, 300] seeded"})
+        return c
+    wl = _workload(wlname)
+    c.update({"name": wl.name, "nx": wl.nx, "ny": wl.ny, "ngrid": wl.ngrid, "length": wl.length, "Re": wl.Re,
+              "dt": wl.dt, "scheme": wl.scheme, "cg_tol": wl.tol})
+    if wl.noise_amp:
+        c["initial_condition"] = f"seeded N(0, {wl.noise_amp:g}^2) level-0 wake vorticity (seed {wl.noise_seed})"
     return c
 
 
@@ -148,45 +173,56 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def rel_l2(a, b):
+    import numpy as np
+    a, b = np.asarray(a, dtype=float), np.asarray(b, dtype=float)
+    nb = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+
 # ---------------------------------------------------------------------------
 # CPU baseline: the reference's own code on the host cores (bounded samples)
 # ---------------------------------------------------------------------------
 def _c4_sample():
+    """(member index, workload) of the members the CPU samples: the first two with n <= 256
+    (the larger members' CPU Cholesky set-up is minutes long)."""
     from ibpm_b200 import configs
-    small = [w for w in configs.ensemble_members() if w.nx <= 256][:2]
-    return small
+    return [(k, w) for k, w in enumerate(configs.ensemble_members()) if w.nx <= 256][:2]
 
 
-def cpu_baseline(workload, steps=None):
+CPU_STEPS = {"c2": 10, "c3": 2, "c4": 3, "c5": 1}   # timed reference steps per sample (bounded CPU time)
+CPU_WARMUP = {"c2": 3, "c3": 1, "c4": 3, "c5": 0}
+
+
+def cpu_baseline(wlname, steps=None, warmup=None):
+    """The reference on one host core over a bounded sample; returns (baseline dict, forces per
+    sampled run (W + K steps each), in member order for c4)."""
     from oracle import ref_runner
-    from ibpm_b200 import configs
     if not ref_runner.available():
         return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
-                "sample": "unavailable: oracle/_ref/ref_driver not built"}
+                "sample": "unavailable: oracle/_ref/ref_driver not built"}, None
     cpu = ref_runner.host_cpu()
-    if workload == "c2":
-        n = steps or 10
-        r = ref_runner.run(configs.c2_shedding_cylinder(), "c2", steps=n, warmup=1)
-        return {"value": r["steps_per_s"], "unit": UNIT, "cores": 1, "kind": "reference",
-                "sample": f"{r['timed_steps']} RK3 steps of the same workload after 1 warm-up step, Cholesky set-up "
-                          f"(init {r['init_s']:.1f} s) excluded, reference sources -Ofast + project DST-I FFTW "
-                          f"shim, 1 core of {cpu}"}
-    if workload == "c3":
-        n = steps or 2
-        r = ref_runner.run(configs.c3_pitching_plate(), "c3", steps=n, warmup=1)
-        return {"value": r["steps_per_s"], "unit": UNIT, "cores": 1, "kind": "reference",
-                "sample": f"{r['timed_steps']} RK3 steps (plain CG force solve, tol 1e-10) after 1 warm-up step, "
-                          f"reference sources -Ofast + project DST-I FFTW shim, 1 core of {cpu}"}
-    n = steps or 3
-    tot_s, tot_n, names = 0.0, 0, []
-    for k, wl in enumerate(_c4_sample()):
-        r = ref_runner.run(wl, f"c4_{wl.name}", steps=n, warmup=1)
+    n = steps or CPU_STEPS[wlname]
+    w = CPU_WARMUP[wlname] if warmup is None else warmup
+    if wlname != "c4":
+        r = ref_runner.run(_workload(wlname), wlname, steps=n, warmup=w)
+        what = {"c2": "RK3 steps", "c3": "RK3 steps (plain CG force solve, tol 1e-10)",
+                "c5": "RK3 steps (plain CG force solve, tol 1e-10)"}[wlname]
+        return ({"value": r["steps_per_s"], "unit": UNIT, "cores": 1, "kind": "reference",
+                 "sample": f"{r['timed_steps']} {what} of the same workload after {w} warm-up steps, Cholesky "
+                           f"set-up (init {r['init_s']:.1f} s) excluded, reference sources -Ofast + project DST-I "
+                           f"FFTW shim, 1 core of {cpu}"}, [r["forces"]])
+    tot_s, tot_n, names, forces = 0.0, 0, [], []
+    for k, wl in _c4_sample():
+        r = ref_runner.run(wl, f"c4_{wl.name}", steps=n, warmup=w)
         tot_s += r["timed_steps"] / r["steps_per_s"]
         tot_n += r["timed_steps"]
-        names.append(f"{wl.name} ({wl.nx}^2, ngrid {wl.ngrid})")
-    return {"value": tot_n / tot_s, "unit": UNIT, "cores": 1, "kind": "reference",
-            "sample": f"{n} RK3 steps each of members {', '.join(names)} (the first two with n <= 256; larger "
-                      f"members' CPU Cholesky set-up is too long to sample), Cholesky set-up excluded, 1 core of {cpu}"}
+        names.append(f"{k} ({wl.nx}^2, ngrid {wl.ngrid})")
+        forces.append(r["forces"])
+    return ({"value": tot_n / tot_s, "unit": UNIT, "cores": 1, "kind": "reference",
+             "sample": f"{n} RK3 steps after {w} warm-up steps each of members {', '.join(names)} (the first two "
+                       f"with n <= 256; larger members' CPU Cholesky set-up is too long to sample), Cholesky "
+                       f"set-up excluded, 1 core of {cpu}"}, forces)
 
 
 def run_reference(args):
@@ -198,16 +234,19 @@ def run_reference(args):
     if not ref_runner.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_driver is not built on this host"}))
         return 0
-    cap = {"c2": 20, "c3": 3, "c4": 3}[wlname]
+    cap = {"c2": 20, "c3": 3, "c4": 3, "c5": 1}[wlname]
     steps = max(1, min(args.steps, cap))
-    cb = cpu_baseline(wlname, steps=steps)
+    warm = min(args.warmup, {"c2": 10, "c3": 1, "c4": 3, "c5": 0}[wlname])
+    cb, _ = cpu_baseline(wlname, steps=steps, warmup=warm)
     v = cb["value"]
-    out = {"metric": METRICS[wlname], "unit": UNIT, "n_gpus": args.gpus, "steps": steps, "warmup": 1,
+    out = {"metric": METRICS[wlname], "unit": UNIT, "n_gpus": args.gpus, "steps": steps, "warmup": warm,
            "value": v, "ms_per_step": 1000.0 / v, "higher_is_better": True,
            "scaling": "strong" if wlname == "c4" else "weak", "vs_baseline": None,
-           "dtype": "f64", "data": "synthetic", "config": _config(wlname, "reference FP64 CPU"), "impl": "reference",
-           "cpu_baseline": dict(cb, sample=cb["sample"] + f" (requested --steps {args.steps}; capped at {cap} to "
-                                                          f"bound CPU time)"),
+           "dtype": "f64", "data": "synthetic (seeded initial conditions and generated geometry)",
+           "config": workload_config(wlname, args.members), "form": "reference FP64 CPU", "impl": "reference",
+           "cpu_baseline": dict(cb, sample=cb["sample"] + f" (requested --steps {args.steps} --warmup "
+                                                          f"{args.warmup}; capped at {cap} and {warm} to bound CPU "
+                                                          f"time)"),
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
     return 0
@@ -229,13 +268,6 @@ def time_steps(K, stream, step, flush):
             ev[k][1].record(stream)
     torch.cuda.synchronize()
     return sum(a.elapsed_time(b) for a, b in ev), launches
-
-
-def rel_l2(a, b):
-    import numpy as np
-    a, b = np.asarray(a, dtype=float), np.asarray(b, dtype=float)
-    nb = np.linalg.norm(b)
-    return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
 
 
 def _pinned_state(x):
@@ -267,41 +299,37 @@ def _download(s, h):
     h["ts"], h["t"] = ts.value, t.value
 
 
-def _round_trip(s, h, advance):
-    _upload(s, h)
-    advance(1)
-    _download(s, h)
-
-
 class Single:
-    """One simulation (c2, c3) in a given form."""
+    """One simulation (c2, c3, c5) in a given form."""
 
-    def __init__(self, workload, form, stream, device):
+    def __init__(self, wlname, form, stream, device, pc_refresh=10, lpc_train=None):
         import ibpm_b200 as ib
-        from ibpm_b200 import configs
-        self.wl = configs.c2_shedding_cylinder() if workload == "c2" else configs.c3_pitching_plate()
+        self.wl = _workload(wlname)
         kw = {}
-        if workload == "c2":
+        if wlname == "c2":
             kw["precision"] = form
         else:
             kw["precond"] = {"cg": "none", "cholesky": "cholesky", "learned": "learned"}[form]
-            kw["pc_refresh"] = 10
+            kw["pc_refresh"] = pc_refresh
         self.grid, self.model, self.s, self.x = ib.from_workload(self.wl, stream=stream.cuda_stream, device=device,
                                                                  **kw)
-        self.extra = {}
+        self.run = {}
+        if form == "cholesky":
+            self.run["pc_refresh"] = pc_refresh
         if form == "learned":
+            nconf, epochs = lpc_train
             t0 = time.perf_counter()
-            geom, mb = self.s.lpc_generate(64, 0.0, 8.0)
+            geom, mb = self.s.lpc_generate(nconf, 0.0, 8.0)
             t1 = time.perf_counter()
-            hist = self.s.lpc_train(geom, mb, epochs=1500, batch=4, lr=2e-3, seed=1)
+            hist = self.s.lpc_train(geom, mb, epochs=epochs, batch=4, lr=2e-3, seed=1)
             t2 = time.perf_counter()
-            self.extra = {"training": {"configurations": 64, "times": [0.0, 8.0], "epochs": 1500, "batch": 4,
-                                       "lr": 2e-3,
-                                       "generate_s": t1 - t0, "train_s": t2 - t1, "loss_first": float(hist[0]),
-                                       "loss_last": float(hist[-1])}}
+            self.run["training"] = {"configurations": nconf, "times": [0.0, 8.0], "epochs": epochs, "batch": 4,
+                                    "lr": 2e-3, "generate_s": t1 - t0, "train_s": t2 - t1,
+                                    "loss_first": float(hist[0]), "loss_last": float(hist[-1])}
         self.s.init()
         self.s.set_state(self.x, with_q=False)
         self.stream = stream
+        self.total = 1
 
     def step(self):
         self.s.advance_resident(1)
@@ -310,9 +338,12 @@ class Single:
     def forces(self, K):
         return self.s.force_history(K)
 
+    def omega(self):
+        self.s.get_state(self.x)
+        return self.x.omega.copy()
+
     def iterations(self):
-        it, n = self.s.cg_totals()
-        return it, n
+        return self.s.cg_totals()
 
     def e2e(self, Ke, sync):
         """The reference's contract (src/IBSolver.cc:142-149): the State lives on
@@ -324,7 +355,9 @@ class Single:
         sync()
         t0 = time.perf_counter()
         for _ in range(Ke):
-            _round_trip(self.s, host, self.s.advance_resident)
+            _upload(self.s, host)
+            self.s.advance_resident(1)
+            _download(self.s, host)
         torch.cuda.synchronize()
         nb = int(8 * (x.omega.size + x.q.size + x.f.size))
         return time.perf_counter() - t0, nb, nb
@@ -337,7 +370,7 @@ class Single:
 
 
 class Ens:
-    """The 64-member ensemble (c4): one graph (ensemble) or member after member (serial)."""
+    """The 64-member ensemble (c4): one graph (ensemble*) or member after member (serial)."""
 
     def __init__(self, form, stream, device, count=64, world_size=1, rank=0):
         import ibpm_b200 as ib
@@ -347,10 +380,11 @@ class Ens:
         self.members = []
         self.total = count
         self.device = torch.device("cuda", device)
-        prec = "fp32" if form == "ensemble_fp32" else "fp64"
+        prec = {"ensemble_fp32": "fp32", "ensemble_refined": "fp32_refined"}.get(form, "fp64")
         everyone = configs.ensemble_members(count=count)
+        self.mine = shard(count, world_size, rank)
         # with several GPUs the members shard over the ranks (no exchange while they run)
-        for wl in [everyone[i] for i in shard(count, world_size, rank)]:
+        for wl in [everyone[i] for i in self.mine]:
             grid, model, s, x = ib.from_workload(wl, stream=stream.cuda_stream, device=device, precision=prec)
             s.init()
             s.set_state(x, with_q=False)
@@ -362,9 +396,7 @@ class Ens:
         if form.startswith("ensemble"):
             self.ens = ib.Ensemble([m[2] for m in self.members])
             self.stream = torch.cuda.ExternalStream(self.ens.stream(), device=torch.device("cuda", device))
-        self.extra = {"members": count, "members_on_rank0": len(self.members),
-                      "grid_points_all_levels": int(sum(w.nx * w.ny * w.ngrid for w, *_ in self.members)),
-                      "boundary_points": [int(m[3].f.size // 2) for m in self.members][:8] + ["..."]}
+        self.run = {"members_on_rank0": len(self.members), "member_precision": prec}
 
     def step(self):
         if self.ens is not None:
@@ -381,7 +413,15 @@ class Ens:
         import numpy as np
         from ibpm_b200.replicas import gather_histories
         local = np.stack([m[2].force_history(K) for m in self.members])
-        return gather_histories(local, self.total, device=self.device).reshape(-1, 2)
+        return gather_histories(local, self.total, device=self.device)
+
+    def omega(self):
+        import numpy as np
+        out = []
+        for _, _, s, x in self.members:
+            s.get_state(x)
+            out.append(x.omega.ravel().copy())
+        return np.concatenate(out)
 
     def e2e(self, Ke, sync):
         import torch
@@ -418,9 +458,11 @@ def main():
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=None)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4"])
+    ap.add_argument("--workload", default="c4", choices=["c2", "c3", "c4", "c5"])
     ap.add_argument("--form", default=None)
     ap.add_argument("--members", type=int, default=64, help="c4: ensemble members (the workload has 64)")
+    ap.add_argument("--pc-refresh", type=int, default=None, help="c3/c5 cholesky: steps between rebuilds")
+    ap.add_argument("--lpc-train", default=None, help="c3/c5 learned: CONFIGS,EPOCHS of the training run")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-path comparison run")
     ap.add_argument("--profile", action="store_true",
@@ -429,15 +471,18 @@ def main():
     args = ap.parse_args()
     wlname = args.workload
     if args.steps is None:
-        args.steps = {"c2": 200, "c3": 50, "c4": 20}[wlname]
+        args.steps = STEPS[wlname]
     if args.warmup is None:
-        args.warmup = {"c2": 10, "c3": 3, "c4": 3}[wlname]
+        args.warmup = WARMUP[wlname]
     if args.impl == "reference":
         return run_reference(args)
     form = args.form or FORMS[wlname][0]
     if form not in FORMS[wlname]:
         raise SystemExit(f"--form for {wlname} must be one of {FORMS[wlname]}")
+    pc_refresh = args.pc_refresh or PC_REFRESH.get(wlname, 10)
+    lpc_train = tuple(int(v) for v in (args.lpc_train or ("64,1500" if wlname == "c3" else "16,300")).split(","))
 
+    import numpy as np
     import torch
     import torch.distributed as dist
 
@@ -455,7 +500,7 @@ def main():
         stream = torch.cuda.Stream(device=dev)
         if wlname == "c4":
             return Ens(f, stream, local, count=args.members, world_size=ws, rank=rank)
-        return Single(wlname, f, stream, local)
+        return Single(wlname, f, stream, local, pc_refresh=pc_refresh, lpc_train=lpc_train)
 
     from ibpm_b200.replicas import job_throughput, max_over_ranks
 
@@ -487,6 +532,7 @@ def main():
     job_units = run.total if wlname == "c4" else ws
     value = job_throughput(1, K, job_units, ms)
     forces = run.forces(W + K)
+    omega = run.omega()
     cg = None
     if it0 is not None:
         it1 = run.iterations()
@@ -506,15 +552,12 @@ def main():
     e2e_s = maxrank(e2e_s)
     e2e = {"value": job_throughput(1, Ke, job_units, 1000.0 * e2e_s), "unit": UNIT, "h2d_bytes_per_step": bi,
            "d2h_bytes_per_step": bo}
-    roof = kernel_roofline(*run.roof_solver(), dtype="float" if form == "fp32" else "double")
-    if wlname == "c2" and form == "fp64":
-        # dram__bytes_read.sum + dram__bytes_write.sum of one k_dst_cols<double> launch on this workload
-        # (ncu --set full, cold launch; profiles/step_kernels_c2_fp64.md)
-        roof["traffic"] = 3.22e6
-        roof["traffic_note"] = "ncu dram read + write of one cold launch; writes stay in L2"
-    extra = dict(run.extra)
+    roof = kernel_roofline(*run.roof_solver(),
+                           dtype="float" if form in ("fp32", "ensemble_fp32", "fp32_refined", "ensemble_refined")
+                           else "double")
+    info = dict(run.run)
     import ibpm_b200 as ib
-    extra["autotuned_dst_shapes"] = ib.autotune_log()
+    info["autotuned_dst_shapes"] = ib.autotune_log()
     run.close()
 
     plain = None
@@ -527,8 +570,12 @@ def main():
         pms, _ = time_steps(K, p.stream, p.step, flush)
         pms = maxrank(pms)
         pforces = p.forces(W + K)
+        pomega = p.omega()
         plain = {"form": PLAIN[wlname], "value": job_throughput(1, K, job_units, pms), "ms_per_step": pms / K,
-                 "force_rel_l2_vs_plain": rel_l2(forces, pforces)}
+                 "force_rel_l2_vs_plain": rel_l2(forces, pforces),
+                 "force_max_member_rel_l2_vs_plain": (max(rel_l2(a, b) for a, b in zip(forces, pforces))
+                                                      if wlname == "c4" else None),
+                 "omega_rel_l2_vs_plain": rel_l2(omega, pomega) if ws == 1 else None}
         if pit0 is not None:
             pit1 = p.iterations()
             plain["iterations_per_solve"] = (pit1[0] - pit0[0]) / max(1, pit1[1] - pit0[1])
@@ -536,21 +583,34 @@ def main():
         p.close()
 
     if rank == 0:
-        wl = getattr(run, "wl", None)
-        dtype = {"fp32": "f32+f64", "ensemble_fp32": "f32+f64"}.get(form, "f64")
+        dtype = {"fp32": "f32+f64", "ensemble_fp32": "f32+f64", "fp32_refined": "f32+f64 refined",
+                 "ensemble_refined": "f32+f64 refined"}.get(form, "f64")
+        last = forces[-1] if wlname != "c4" else forces[0][-1]
         out = {"metric": METRICS[wlname], "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
                "ms_per_step": ms / K, "higher_is_better": True,
-               "scaling": "strong" if wlname == "c4" else "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded initial conditions and generated geometry)",
-               "config": _config(wlname, form, wl, extra), "e2e": e2e, "gpu_launches": int(launches),
-               "roofline": roof, "clocks": clk,
-               "final_force": [float(forces[-1][0]), float(forces[-1][1])] if len(forces) else None}
+               "scaling": "strong" if wlname == "c4" else "weak", "vs_baseline": None, "dtype": dtype,
+               "data": "synthetic (seeded initial conditions and generated geometry)",
+               "config": workload_config(wlname, args.members), "form": form, "run": info, "e2e": e2e,
+               "gpu_launches": int(launches), "roofline": roof, "clocks": clk,
+               "final_force": [float(last[0]), float(last[1])] if len(forces) else None}
+        if wlname != "c4":
+            out["grid_point_updates_per_s"] = value * run.wl.ngrid * (run.wl.nx - 1) * (run.wl.ny - 1)
         if cg:
             out["cg"] = cg
         if plain:
             out["plain"] = plain
         if ws == 1 and not args.no_cpu_baseline:
             try:
-                out["cpu_baseline"] = cpu_baseline(wlname)
+                cb, ref_forces = cpu_baseline(wlname)
+                if ref_forces is not None:
+                    mine = [forces] if wlname != "c4" else [forces[k] for k, _ in _c4_sample()]
+                    errs = []
+                    for a, b in zip(mine, ref_forces):
+                        n = min(len(a), len(b))
+                        errs.append(rel_l2(a[:n], b[:n]))
+                    cb["force_rel_l2_vs_gpu_run"] = max(errs)
+                    cb["force_steps_compared"] = int(min(len(a) for a in ref_forces))
+                out["cpu_baseline"] = cb
             except Exception as e:  # the baseline is reported, never required
                 out["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
                                        "sample": f"failed: {e}"}

@@ -404,6 +404,10 @@ class NonlinearIBSolver:
     def reg_to_boundary(self, q0):
         return self._op("ibg_reg_to_boundary", q0, out_shape=(2 * self.npoints,))
 
+    def reg_to_flux(self, f):
+        """Regularizer::toFlux: the Flux (every level) of a boundary vector."""
+        return self._op("ibg_reg_to_flux", f, out_shape=self.grid.flux().shape)
+
     def projection_solve(self, k, a, b, f0):
         a = np.ascontiguousarray(a, dtype=np.float64)
         b = np.ascontiguousarray(b, dtype=np.float64)

@@ -94,6 +94,13 @@ SIGNATURES = {
     "ibg_model_B": (_I, [_VP, _VP, _VP]),
     "ibg_model_C": (_I, [_VP, _VP, _VP]),
     "ibg_reg_to_boundary": (_I, [_VP, _VP, _VP]),
+    "ibg_reg_to_flux": (_I, [_VP, _VP, _VP]),
+    "ibg_elliptic_create": (_I, [ctypes.POINTER(ibg_grid), _I, ctypes.c_double, _VP, _VP]),
+    "ibg_elliptic_solve": (_I, [_VP, _VP, _VP]),
+    "ibg_elliptic_destroy": (_I, [_VP]),
+    "ibg_elliptic_last_error": (ctypes.c_char_p, [_VP]),
+    "ibg_set_external_kinematics": (_I, [_VP]),
+    "ibg_set_step_kinematics": (_I, [_VP, _I, _VP, _VP]),
     "ibg_projection_solve": (_I, [_VP, _I, _VP, _VP, _VP, _VP]),
     "ibg_poisson_solve_static": (_I, [ctypes.POINTER(ibg_grid), _VP, _VP, _VP]),
     "ibg_ensemble_create": (_I, [_I, ctypes.POINTER(_VP), ctypes.POINTER(_VP)]),

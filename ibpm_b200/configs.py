@@ -80,7 +80,7 @@ def plate_geom(chord=1.0, npts=51, mean_aoa_deg=20.0, pitch_amp_deg=10.0, freq=0
 
 def two_cylinders_geom(seed=5, n=201, amp=0.2, freq=0.2) -> str:
     rng = np.random.default_rng(seed)
-    e1, e2 = rng.uniform(-0.1, 0.1, size=2)
+    e1, e2 = (float(e) for e in rng.uniform(-0.1, 0.1, size=2))
     out = []
     for (yc, sgn) in ((0.75 + e1, 1.0), (-0.75 + e2, -1.0)):
         out.append(f"body Cylinder\n  circle_n 0 {yc!r} 0.5 {n}\n  center 0 {yc!r}\n"

@@ -62,6 +62,7 @@ Scheme make_scheme(int s) {
 }
 
 constexpr int kHistCap = 1 << 16;
+constexpr int kExtNow = 4;  // external-kinematics slot of "now" (slots 0..3: the sub-steps)
 }  // namespace
 
 // bulk fields and solver plans in one arithmetic type
@@ -108,6 +109,18 @@ __global__ void k_cg_loop_reset(int* flags) {
     if (threadIdx.x == 0 && blockIdx.x == 0) flags[7] = 0;
 }
 
+// one external-kinematics slot ([x.., y..] points then velocities) into the interleaved device layout
+__global__ void k_ext_boundary(int npts, const double* __restrict__ ext, double* __restrict__ pts,
+                               double* __restrict__ vel) {
+    pdl_enter();
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npts) return;
+    pts[2 * p] = ext[p];
+    pts[2 * p + 1] = ext[npts + p];
+    vel[2 * p] = ext[2 * npts + p];
+    vel[2 * p + 1] = ext[3 * npts + p];
+}
+
 template <typename A, typename B>
 __global__ void k_convert(size_t n, const A* __restrict__ in, B* __restrict__ out) {
     pdl_enter();
@@ -125,7 +138,13 @@ struct ibg_context {
     double u0 = 0, v0 = 0;
     int npts = 0, ncomp = 0;
     bool moving = false;
+    // external kinematics: the caller moves the bodies (host Geometry) and hands the device the points
+    // and velocities of each sub-step; d_ext holds kExtNow + 1 slots of [points | velocities] (2 npts
+    // each, BoundaryVector layout)
+    bool ext_kin = false;
+    double* d_ext = nullptr;
     bool fp32 = false;  // bulk fields of the time step in FP32
+    bool refined = false;  // FP64 state, every time-step solve from FP32 transforms + one FP64-residual refinement
     cudaStream_t st = nullptr;
     bool own_stream = false;
     std::string err;
@@ -346,6 +365,8 @@ struct ibg_context {
         if (lb.len) cudaFree(lb.len);
         if (lb.closed) cudaFree(lb.closed);
         lb = LpcBodies{};
+        if (d_ext) cudaFree(d_ext);
+        d_ext = nullptr;
         void* ptrs[] = {d_ref, d_pts, d_vel, d_body_of, d_bodies, d_mstate, d_mstate_keep, d_mtab, d_bf, d_bf_state, d_bfv, d_q0,
                         slots.idx, slots.w, slots.n, d_b, d_time, f,
                         flux0, rhsb, btmp, d_status, cg_r, cg_d, cg_q, cg_scal, cg_flags, d_hist, d_hist_count, cg_z, cg_zold};
@@ -402,14 +423,30 @@ struct ibg_context {
         c.base = base;
         return c;
     }
-    long long solve_launches() const { return b64.poisson.launches(); }
+    long long solve_launches() const {
+        return refined ? refined_solve_launches(g, b32.poisson) : b64.poisson.launches();
+    }
+
+    // one multi-domain solve of the time step: plan `which` (-1 Poisson, k the sub-step's
+    // Helmholtz); FP64 solves of the refined form run as FP32 solves plus one refinement
+    template <typename T>
+    void esolve(Bulk<T>& B, int which, const SolveCall<T>& c) {
+        if constexpr (std::is_same<T, double>::value) {
+            if (refined) {
+                const EllipticPlan<float>& p32 = which < 0 ? b32.poisson : b32.helm[which];
+                refined_solve(g, p32, c, b64.rc, b32.a, b32.ws, b32.cc, b32.tbuf, b32.sweep, st);
+                return;
+            }
+        }
+        (which < 0 ? B.poisson : B.helm[which]).solve(c, st);
+    }
 
     // M d = C A^-1 B d  (src/ProjectionSolver.cc:96-101)
     template <typename T>
     void m_apply(Bulk<T>& B, int k, const double* din, double* dout) {
         launch_smear_bf<T>(g, ncomp, slots, din, flux0, B.Bf, beta[k], st);
-        B.helm[k].solve(call<T>(B, B.Bf, B.cc, (T)1), st);
-        B.poisson.solve(call<T>(B, B.cc, B.psi, (T)-1), st);
+        esolve<T>(B, k, call<T>(B, B.Bf, B.cc, (T)1));
+        esolve<T>(B, -1, call<T>(B, B.cc, B.psi, (T)-1));
         launch_reg_interp<T>(g, ncomp, slots, B.psi, S, 1, nullptr, dout, 0, st);
         launches += 3 + 2 * solve_launches() + 1;
     }
@@ -555,8 +592,8 @@ struct ibg_context {
     // the projection of one sub-step (src/ProjectionSolver.cc:57-79) given a and b
     template <typename T>
     int projection(Bulk<T>& B, int k, const T* a_in, const double* b_in) {
-        B.helm[k].solve(call<T>(B, a_in, B.ws, (T)1), st);                        // omega* = A^-1 a
-        B.poisson.solve(call<T>(B, B.ws, B.psi, (T)-1), st);                      // psi* = L^-1(-omega*)
+        esolve<T>(B, k, call<T>(B, a_in, B.ws, (T)1));                             // omega* = A^-1 a
+        esolve<T>(B, -1, call<T>(B, B.ws, B.psi, (T)-1));                          // psi* = L^-1(-omega*)
         launch_reg_interp<T>(g, ncomp, slots, B.psi, S, 1, b_in, rhsb, 0, st);   // C omega* - b
         launches += 2 * solve_launches() + 1;
         if (!moving) {
@@ -567,7 +604,7 @@ struct ibg_context {
             if (s) return s;
         }
         launch_smear_bf<T>(g, ncomp, slots, f, flux0, B.Bf, beta[k], st);         // B f
-        B.helm[k].solve(call<T>(B, B.Bf, B.cc, (T)1, B.w, B.ws), st);            // omega = omega* - A^-1 B f
+        esolve<T>(B, k, call<T>(B, B.Bf, B.cc, (T)1, B.w, B.ws));                 // omega = omega* - A^-1 B f
         launches += 3 + solve_launches();
         return IBG_OK;
     }
@@ -575,13 +612,21 @@ struct ibg_context {
     // q = Curl(L^-1(-omega)) + q0 (src/NavierStokesModel.cc:121-140)
     template <typename T>
     void refresh(Bulk<T>& B) {
-        B.poisson.solve(call<T>(B, B.w, B.psi, (T)-1), st);
+        esolve<T>(B, -1, call<T>(B, B.w, B.psi, (T)-1));
         launch_refresh_flux<T>(g, B.psi, B.q, u0, v0, ubf ? d_q0 : nullptr, st);
         launches += solve_launches() + 1;
     }
 
     // Geometry::moveBodies(time + toff) and Regularizer::update (src/NavierStokesModel.cc:93-99)
-    void move_bodies(double toff) {
+    void move_bodies(double toff, int slot = -1) {
+        if (ext_kin) {
+            // positions and velocities the caller computed (sub-step `slot` of the next step, or now)
+            launch_k(k_ext_boundary, (unsigned)((npts + 127) / 128), 128, 0, st, npts,
+                     (const double*)(d_ext + (size_t)(slot < 0 ? kExtNow : slot) * 4 * npts), d_pts, d_vel);
+            launch_reg_update(g, npts, d_pts, d_vel, slots, d_b, u0, v0, st);
+            launches += 2;
+            return;
+        }
         if (stateful) {
             launch_motion_state(nbodies, d_bodies, d_time, toff, d_mstate, st);
             launches += 1;
@@ -638,7 +683,7 @@ struct ibg_context {
         }
         launches += 2 + g.L;
         if (ubf) frame_flow(cn * prm.dt);
-        if (moving) move_bodies(cn * prm.dt);
+        if (moving) move_bodies(cn * prm.dt, k);
         const T* Nprev = nullptr;
         if (bn != 0) Nprev = old_saved ? Np : Nk;
         const double c1 = 0.5 * (1.0 / prm.Re) * (an + bn);
@@ -933,9 +978,10 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
         g_create_error = "ibg_create: Re and dt must be positive";
         return IBG_ERR_ARG;
     }
-    if (params->precision != IBG_PRECISION_FP64 && params->precision != IBG_PRECISION_FP32) {
-        g_create_error = "ibg_create: precision must be IBG_PRECISION_FP64 or IBG_PRECISION_FP32";
-        return IBG_ERR_UNSUPPORTED;
+    if (params->precision != IBG_PRECISION_FP64 && params->precision != IBG_PRECISION_FP32 &&
+        params->precision != IBG_PRECISION_FP32_REFINED) {
+        g_create_error = "ibg_create: unknown precision";
+        return IBG_ERR_ARG;
     }
     if (!fft_supported(2 * G.nx) || !fft_supported(2 * G.ny)) {
         g_create_error = "ibg_create: 2*nx and 2*ny must factor into primes <= 13";
@@ -1068,8 +1114,9 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
     for (int k = 0; k < sch.nsub; ++k) c->beta[k] = (sch.an[k] + sch.bn[k]) * c->prm.dt;  // src/IBSolver.cc:110-114
     c->nring = sch.nsub == 1 ? 2 : sch.nsub;
     c->fp32 = (c->prm.precision == IBG_PRECISION_FP32);
+    c->refined = (c->prm.precision == IBG_PRECISION_FP32_REFINED);
     s = c->alloc_bulk(c->b64);
-    if (!s && c->fp32) s = c->alloc_bulk(c->b32);
+    if (!s && (c->fp32 || c->refined)) s = c->alloc_bulk(c->b32);
     if (s) {
         g_create_error = "ibg_create: solver set-up or device allocation failed";
         delete c;
@@ -1592,6 +1639,35 @@ int ibg_flux_to_velocity(ibg_context* c, double* u, double* v) {
     return c->cuda_check("ibg_flux_to_velocity");
 }
 
+int ibg_set_external_kinematics(ibg_context* c) {
+    if (!c) return IBG_ERR_ARG;
+    if (c->ubf) return c->fail(IBG_ERR_STATE, "ibg_set_external_kinematics: the moving frame carries the motion");
+    if (!c->d_ext && c->alloc(&c->d_ext, (size_t)(kExtNow + 1) * 4 * c->npts)) return IBG_ERR_CUDA;
+    // the current configuration becomes every slot until the caller writes them
+    std::vector<double> h(4 * (size_t)c->npts);
+    const int s = ibg_get_boundary(c, h.data(), h.data() + 2 * (size_t)c->npts);
+    if (s) return s;
+    for (int k = 0; k <= kExtNow; ++k)
+        cudaMemcpyAsync(c->d_ext + (size_t)k * 4 * c->npts, h.data(), sizeof(double) * h.size(),
+                        cudaMemcpyHostToDevice, c->st);
+    c->ext_kin = true;
+    c->moving = true;
+    c->stateful = false;
+    c->drop_graph();
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->cuda_check("ibg_set_external_kinematics");
+    return c->cuda_check("ibg_set_external_kinematics");
+}
+int ibg_set_step_kinematics(ibg_context* c, int slot, const double* points, const double* velocities) {
+    if (!c || !points || !velocities) return IBG_ERR_ARG;
+    if (!c->ext_kin) return c->fail(IBG_ERR_STATE, "ibg_set_step_kinematics: call ibg_set_external_kinematics first");
+    if (slot < -1 || slot >= c->sch.nsub) return c->fail(IBG_ERR_ARG, "ibg_set_step_kinematics: slot out of range");
+    const size_t n2 = 2 * (size_t)c->npts;
+    double* dst = c->d_ext + (size_t)(slot < 0 ? kExtNow : slot) * 2 * n2;
+    cudaMemcpyAsync(dst, points, sizeof(double) * n2, cudaMemcpyHostToDevice, c->st);
+    cudaMemcpyAsync(dst + n2, velocities, sizeof(double) * n2, cudaMemcpyHostToDevice, c->st);
+    if (slot < 0) c->move_bodies(0.0, -1);
+    return c->cuda_check("ibg_set_step_kinematics");
+}
 int ibg_get_boundary(ibg_context* c, double* points, double* velocities) {
     if (!c) return IBG_ERR_ARG;
     const size_t n = (size_t)c->npts;
@@ -1790,6 +1866,26 @@ int ibg_model_C(ibg_context* c, const double* omega, double* fb) {
     return finish(c, "ibg_model_C");
 }
 
+namespace ibg {
+__global__ void k_scale(size_t n, const double* __restrict__ in, double s, double* __restrict__ out) {
+    pdl_enter();
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = s * in[i];
+}
+}  // namespace ibg
+int ibg_reg_to_flux(ibg_context* c, const double* fb, double* q) {
+    if (!c || !fb || !q) return IBG_ERR_ARG;
+    const GridDev& g = c->g;
+    cudaMemcpyAsync(c->btmp, fb, sizeof(double) * c->ncomp, cudaMemcpyHostToDevice, c->st);
+    // level 0: sum of weight * f over the associations, times dx; every coarser level is zero
+    launch_reg_smear(c->ncomp, c->slots, c->btmp, c->flux0, c->st);
+    launch_k(k_scale, (unsigned)((g.F1 + 255) / 256), 256, 0, c->st, (size_t)g.F1, (const double*)c->flux0, g.dx,
+             c->b64.qtmp);
+    launch_reg_zero(c->ncomp, c->slots, c->flux0, c->st);
+    if (g.L > 1) cudaMemsetAsync(c->b64.qtmp + g.F1, 0, sizeof(double) * (c->F - g.F1), c->st);
+    cudaMemcpyAsync(q, c->b64.qtmp, sizeof(double) * c->F, cudaMemcpyDeviceToHost, c->st);
+    return finish(c, "ibg_reg_to_flux");
+}
 int ibg_reg_to_boundary(ibg_context* c, const double* qin, double* fb) {
     if (!c || !qin || !fb) return IBG_ERR_ARG;
     cudaMemcpyAsync(c->b64.qtmp, qin, sizeof(double) * c->g.F1, cudaMemcpyHostToDevice, c->st);
@@ -1812,6 +1908,119 @@ int ibg_projection_solve(ibg_context* c, int k, const double* ain, const double*
     cudaMemcpyAsync(fio, c->f, sizeof(double) * c->ncomp, cudaMemcpyDeviceToHost, c->st);
     return finish(c, "ibg_projection_solve");
 }
+
+// ---------------------------------------------------------------------------
+// standalone multi-domain elliptic solvers (PoissonSolver / HelmholtzSolver)
+// ---------------------------------------------------------------------------
+struct ibg_elliptic {
+    GridDev g{};
+    size_t S = 0;
+    FftTables fft;
+    CosTables cosT;
+    EllipticPlan<double> plan;
+    double *f = nullptr, *u = nullptr, *rc = nullptr, *tbuf = nullptr, *sweep = nullptr;
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+    std::string err;
+    ~ibg_elliptic() {
+        double* p[] = {f, u, rc, tbuf, sweep};
+        for (double* x : p)
+            if (x) cudaFree(x);
+        fft.release();
+        cosT.release();
+        if (own_stream && st) cudaStreamDestroy(st);
+    }
+};
+namespace {
+thread_local std::string g_elliptic_error;
+}
+
+int ibg_elliptic_create(const ibg_grid* grid, int helmholtz, double alpha, void* cuda_stream, ibg_elliptic** out) {
+    if (!grid || !out) {
+        g_elliptic_error = "ibg_elliptic_create: null argument";
+        return IBG_ERR_ARG;
+    }
+    *out = nullptr;
+    const ibg_grid& G = *grid;
+    if (G.nx < 4 || G.ny < 4 || G.ngrid < 1 || G.ngrid > 16 || !(G.length > 0) ||
+        (G.ngrid > 1 && (G.nx % 2 || G.ny % 2))) {
+        g_elliptic_error = "ibg_elliptic_create: invalid grid";
+        return IBG_ERR_ARG;
+    }
+    if (!fft_supported(2 * G.nx) || !fft_supported(2 * G.ny)) {
+        g_elliptic_error = "ibg_elliptic_create: 2*nx and 2*ny must factor into primes <= 13";
+        return IBG_ERR_UNSUPPORTED;
+    }
+    auto* e = new ibg_elliptic();
+    GridDev& g = e->g;
+    g.nx = G.nx;
+    g.ny = G.ny;
+    g.L = G.ngrid;
+    g.nxe = (int)floor(G.nx / 4 + 0.5);  // src/Grid.h:60-62 with zero shift
+    g.nye = (int)floor(G.ny / 4 + 0.5);
+    g.NI = G.nx - 1;
+    g.NJ = G.ny - 1;
+    g.N1 = g.NI * g.NJ;
+    g.nXf = (G.nx + 1) * G.ny;
+    g.F1 = 2 * G.nx * G.ny + G.nx + G.ny;
+    g.dx = G.length / G.nx;
+    g.x0 = G.xoffset;
+    g.y0 = G.yoffset;
+    e->S = (size_t)g.L * g.N1;
+    if (cuda_stream) {
+        e->st = (cudaStream_t)cuda_stream;
+    } else if (cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking) != cudaSuccess) {
+        delete e;
+        g_elliptic_error = "ibg_elliptic_create: no CUDA device or stream creation failed";
+        return IBG_ERR_CUDA;
+    } else {
+        e->own_stream = true;
+    }
+    int s = e->fft.init(2 * g.ny, 2 * g.nx);
+    if (!s) s = e->cosT.init(g.nx, g.ny, g.nxe, g.nye);
+    if (!s && g.L > 1) s = e->cosT.build_edge_maps(g.nx, g.ny, g.nxe, g.nye, e->fft);
+    if (!s) s = e->plan.init(&e->g, &e->fft, helmholtz != 0, alpha, e->cosT);
+    const size_t sw = sweep_doubles(g.nx, g.ny, g.L);
+    if (!s && (cudaMalloc(&e->f, sizeof(double) * e->S) || cudaMalloc(&e->u, sizeof(double) * e->S) ||
+               cudaMalloc(&e->rc, sizeof(double) * e->S) || cudaMalloc(&e->tbuf, sizeof(double) * e->S) ||
+               cudaMalloc(&e->sweep, sizeof(double) * sw)))
+        s = IBG_ERR_CUDA;
+    if (s) {
+        g_elliptic_error = "ibg_elliptic_create: set-up or device allocation failed";
+        delete e;
+        return s;
+    }
+    *out = e;
+    return IBG_OK;
+}
+int ibg_elliptic_solve(ibg_elliptic* e, const double* f, double* u) {
+    if (!e || !f || !u) return IBG_ERR_ARG;
+    cudaMemcpyAsync(e->f, f, sizeof(double) * e->S, cudaMemcpyHostToDevice, e->st);
+    SolveCall<double> c{};
+    c.f = e->f;
+    c.u = e->u;
+    c.rc = e->rc;
+    c.tbuf = e->tbuf;
+    c.sweep = e->sweep;
+    c.bstride = e->S;
+    c.batch = 1;
+    c.in_scale = 1.0;
+    int s = e->plan.solve(c, e->st);
+    cudaMemcpyAsync(u, e->u, sizeof(double) * e->S, cudaMemcpyDeviceToHost, e->st);
+    const cudaError_t ce = cudaStreamSynchronize(e->st);
+    if (s || ce != cudaSuccess) {
+        e->err = std::string("ibg_elliptic_solve: ") + cudaGetErrorString(ce != cudaSuccess ? ce : cudaGetLastError());
+        return IBG_ERR_CUDA;
+    }
+    return IBG_OK;
+}
+int ibg_elliptic_destroy(ibg_elliptic* e) {
+    if (!e) return IBG_ERR_ARG;
+    if (e->st) cudaStreamSynchronize(e->st);
+    delete e;
+    return IBG_OK;
+}
+const char* ibg_elliptic_last_error(const ibg_elliptic* e) { return e ? e->err.c_str() : g_elliptic_error.c_str(); }
 
 // ---------------------------------------------------------------------------
 // ensembles: one graph whose independent branches are the members' steps
@@ -2208,18 +2417,25 @@ int ibg_autotune_log(int* out, int max_rows) {
 }
 
 long long ibg_run_kernel(ibg_context* c, int which, int reps) {
-    if (!c || reps < 0) return IBG_ERR_ARG;
+    if (!c || reps < 0 || which < 0 || which > 2) return IBG_ERR_ARG;
     const GridDev& g = c->g;
-    long long bytes = 0;
+    // the transforms in the arithmetic the context's time step uses
+    const bool f32 = c->fp32 || c->refined;
     for (int r = 0; r < reps; ++r) {
-        Bulk<double>& B = c->b64;
-        if (which == 0) B.poisson.run_pass(0, B.w, B.tbuf, c->st);
-        else if (which == 1) B.poisson.run_pass(1, B.tbuf, B.tbuf, c->st);
-        else if (which == 2) launch_nonlinear<double>(g, B.q, B.w, B.U, B.V, B.C, B.Nbuf[0], 1, c->S, c->F, c->st);
-        else return IBG_ERR_ARG;
+        if (which == 2) {
+            Bulk<double>& B = c->b64;
+            launch_nonlinear<double>(g, B.q, B.w, B.U, B.V, B.C, B.Nbuf[0], 1, c->S, c->F, c->st);
+        } else if (f32) {
+            Bulk<float>& B = c->b32;
+            B.poisson.run_pass(which, which == 0 ? B.w : B.tbuf, B.tbuf, c->st);
+        } else {
+            Bulk<double>& B = c->b64;
+            B.poisson.run_pass(which, which == 0 ? B.w : B.tbuf, B.tbuf, c->st);
+        }
     }
-    if (which == 0 || which == 1) bytes = 16LL * (long long)c->S;      // every level read + written once
-    else bytes = 8LL * (long long)(c->F + c->S + 2 * c->S + c->F + c->F + c->S);  // q,w in; U,V; C; N
+    long long bytes;
+    if (which == 0 || which == 1) bytes = (f32 ? 8LL : 16LL) * (long long)c->S;  // every level read + written once
+    else bytes = 8LL * (long long)(c->F + c->S + 2 * c->S + c->F + c->F + c->S);   // q,w in; U,V; C; N
     if (c->cuda_check("ibg_run_kernel")) return IBG_ERR_CUDA;
     return bytes;
 }

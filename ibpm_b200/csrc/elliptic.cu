@@ -1107,17 +1107,19 @@ int EllipticPlan<T>::solve(const SolveCall<T>& c, cudaStream_t st) const {
     }
     const size_t tS = (size_t)L * N1;  // coefficients per batch item
     // 1. coarsify the right-hand side: overlap interiors of levels 1..L-1 into rc
+    //    (rc == nullptr: every level of f is already the right-hand side as it stands)
     const int novl = (g.nx / 2 - 1) * (g.ny / 2 - 1);
-    for (int lev = 1; lev < L; ++lev)
-        launch_k(k_coarsify<T>, dim3((unsigned)((novl + 255) / 256), (unsigned)batch), 256, 0, st, g, lev, c.f, c.rc,
-                                                                                          c.bstride);
+    if (c.rc)
+        for (int lev = 1; lev < L; ++lev)
+            launch_k(k_coarsify<T>, dim3((unsigned)((novl + 255) / 256), (unsigned)batch), 256, 0, st, g, lev, c.f,
+                     c.rc, c.bstride);
     // 2. forward transforms of every level
     const T* in[kMaxLevels];
     const T* alt[kMaxLevels];
     T* tb[kMaxLevels];
     for (int l = 0; l < L; ++l) {
         in[l] = c.f + (size_t)l * N1;
-        alt[l] = (l == 0) ? nullptr : c.rc + (size_t)l * N1;
+        alt[l] = (l == 0 || !c.rc) ? nullptr : c.rc + (size_t)l * N1;
         tb[l] = c.tbuf + (size_t)l * N1;
     }
     launch_rows(g, frow, L, batch, in, alt, c.bstride, tb, tS, nullptr, nullptr, c.in_scale, (T)1, st);
@@ -1184,10 +1186,17 @@ void coarsify_field(const GridDev& g, double* f, cudaStream_t st) {
         launch_k(k_coarsify<double>, dim3((unsigned)((novl + 255) / 256), 1), 256, 0, st, g, lev, f, f, 0);
 }
 
+// the coarsified overlap interiors of levels 1..L-1 of f into rc (f unchanged), as step 1 of a solve
+void coarsify_rhs(const GridDev& g, const double* f, double* rc, cudaStream_t st) {
+    const int novl = (g.nx / 2 - 1) * (g.ny / 2 - 1);
+    for (int lev = 1; lev < g.L; ++lev)
+        launch_k(k_coarsify<double>, dim3((unsigned)((novl + 255) / 256), 1), 256, 0, st, g, lev, f, rc, (size_t)0);
+}
+
 template <typename T>
-int EllipticPlan<T>::launches() const {
+int EllipticPlan<T>::launches(bool coarsify) const {
     const int L = grid->L;
-    return L == 1 ? 3 : (L - 1) + 2 + 2 * (L - 1) + 2;
+    return L == 1 ? 3 : (coarsify ? L - 1 : 0) + 2 + 2 * (L - 1) + 2;
 }
 
 template <typename T>

@@ -142,6 +142,8 @@ struct CosTables {
 bool fft_supported(int m);
 // Scalar::coarsify of a field in place (every level, finest first)
 void coarsify_field(const GridDev& g, double* f, cudaStream_t st);
+// the coarsified overlap interiors of levels 1..L-1 of f into rc (f unchanged)
+void coarsify_rhs(const GridDev& g, const double* f, double* rc, cudaStream_t st);
 // factor m into the radices the shared-memory FFT uses (no device allocation)
 void fft_describe(int m, FftDesc& d);
 
@@ -150,7 +152,8 @@ template <typename T>
 struct SolveCall {
     const T* f;       // right-hand side, all levels
     T* u;             // solution, all levels
-    T* rc;            // scratch: coarsified right-hand side (levels 1..L-1), bstride per item
+    T* rc;            // scratch: coarsified right-hand side (levels 1..L-1), bstride per item;
+                      // nullptr: f is already coarsified (its levels are used as they stand)
     T* tbuf;          // scratch: spectral coefficients of all levels (L * N1 per batch item)
     T* sweep;         // scratch: sweep_doubles(nx, ny, L) per batch item
     size_t bstride;   // batch stride of f, u, rc, out2, base
@@ -173,7 +176,7 @@ struct EllipticPlan {
     bool edge_maps = true;  // the sweep applies the precomputed edge maps (else the per-step line FFTs)
     int init(const GridDev* g, const FftTables* t, bool helm, double a, const CosTables& ct);
     int solve(const SolveCall<T>& c, cudaStream_t st) const;
-    int launches() const;
+    int launches(bool coarsify = true) const;
     // one pass of the forward transform of all levels alone (0: rows, 1: columns), for timing
     void run_pass(int which, const T* in, T* tbuf, cudaStream_t st) const;
     const GridTables<T>& tabs() const;
@@ -193,6 +196,14 @@ struct TuneResult {
     int wbytes, pass, m, nlines, nlev, P, threads, tw_smem;
 };
 std::vector<TuneResult> tune_log();
+
+// One FP64-accurate solve from FP32 transforms (refine.cu): the FP32 solve of the
+// coarsified right-hand side, its FP64 residual on every level, the FP32 solve of
+// the residual, and the FP64 sum.  rc64 (S doubles) and f32, u32, d32 (S floats)
+// are scratch, tbuf32 and sweep32 the FP32 plan's transform scratch; batch 1.
+int refined_solve(const GridDev& g, const EllipticPlan<float>& plan32, const SolveCall<double>& c, double* rc64,
+                  float* f32, float* u32, float* d32, float* tbuf32, float* sweep32, cudaStream_t st);
+int refined_solve_launches(const GridDev& g, const EllipticPlan<float>& plan32);
 
 template <>
 inline const GridTables<double>& EllipticPlan<double>::tabs() const { return cos->t64; }

@@ -71,6 +71,10 @@ void launch_reg_update(const GridDev& g, int npts, const double* pts, const doub
 template <typename T>
 void launch_reg_interp(const GridDev& g, int ncomp, const RegSlots& s, const T* psi, size_t sstride, int batch,
                        const double* bcon, double* out, size_t ostride, cudaStream_t st);
+// Regularizer::toFlux without the dx factor: flux0 (level 0) += sum of weight * f over the
+// associations; launch_reg_zero clears the entries the smear touched
+void launch_reg_smear(int ncomp, const RegSlots& s, const double* f, double* flux0, cudaStream_t st);
+void launch_reg_zero(int ncomp, const RegSlots& s, double* flux0, cudaStream_t st);
 template <typename T>
 void launch_smear_bf(const GridDev& g, int ncomp, const RegSlots& s, const double* f, double* flux0, T* Bf,
                      double beta, cudaStream_t st);

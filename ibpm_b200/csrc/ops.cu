@@ -875,6 +875,13 @@ void launch_smear_bf(const GridDev& g, int ncomp, const RegSlots& s, const doubl
     launch_k(k_reg_zero, nblk((size_t)ncomp * kSlots, 128), 128, 0, st, ncomp, 0, 0, s.idx, s.n, flux0, 0);
 }
 
+void launch_reg_smear(int ncomp, const RegSlots& s, const double* f, double* flux0, cudaStream_t st) {
+    launch_k(k_reg_smear, nblk((size_t)ncomp * kSlots, 128), 128, 0, st, ncomp, s.idx, s.w, s.n, f, flux0);
+}
+void launch_reg_zero(int ncomp, const RegSlots& s, double* flux0, cudaStream_t st) {
+    launch_k(k_reg_zero, nblk((size_t)ncomp * kSlots, 128), 128, 0, st, ncomp, 0, 0, s.idx, s.n, flux0, 0);
+}
+
 template <typename T>
 void launch_smear_bf_unit(const GridDev& g, int ncomp, int col0, int batch, const RegSlots& s, double* flux0,
                           size_t fstride, T* Bf, size_t sstride, double beta, cudaStream_t st) {

@@ -227,6 +227,33 @@ IBG_API void* ibg_stream(const ibg_context* ctx);
 /* number of kernel launches issued by the last ibg_advance call */
 IBG_API long long ibg_last_launch_count(const ibg_context* ctx);
 
+/* --- standalone multi-domain elliptic solvers --------------------------------------
+ * PoissonSolver(grid) and HelmholtzSolver(grid, alpha) (src/EllipticSolver.h:26-76):
+ * EllipticSolver::solve(f, u) (src/EllipticSolver.cc:47-73) with L u = f
+ * (helmholtz 0) or (1 + alpha L) u = f (helmholtz 1) on every level of the
+ * grid, coarsifying f first; with ngrid 1 it is EllipticSolver2d::solve with
+ * zero boundary values (src/EllipticSolver2d.cc:53-85).  f and u are host arrays
+ * in the Scalar layout.  `cuda_stream` as for ibg_create. */
+typedef struct ibg_elliptic ibg_elliptic;
+IBG_API int ibg_elliptic_create(const ibg_grid* grid, int helmholtz, double alpha, void* cuda_stream,
+                                ibg_elliptic** out);
+IBG_API int ibg_elliptic_solve(ibg_elliptic* solver, const double* f, double* u);
+IBG_API int ibg_elliptic_destroy(ibg_elliptic* solver);
+IBG_API const char* ibg_elliptic_last_error(const ibg_elliptic* solver);
+
+/* --- bodies moved by the caller -----------------------------------------------------
+ * Geometry::moveBodies (src/Geometry.cc:79-110) run by the caller: for motions the
+ * device does not model (a caller's own Motion subclass), the caller moves its
+ * bodies on the host and hands the device their points and velocities.
+ * ibg_set_external_kinematics switches a context to that mode (the force solve
+ * becomes CG, as for any moving body, src/IBSolver.cc:122-135); every slot starts
+ * as the current configuration.  ibg_set_step_kinematics sets the points and
+ * velocities (BoundaryVector layout, 2 npts values each) the next ibg_advance
+ * uses at sub-step `slot` (the time t + c_slot dt of src/IBSolver.cc:165-166), or,
+ * with slot -1, moves the bodies there now (NavierStokesModel::updateOperators). */
+IBG_API int ibg_set_external_kinematics(ibg_context* ctx);
+IBG_API int ibg_set_step_kinematics(ibg_context* ctx, int slot, const double* points, const double* velocities);
+
 /* --- ensembles ------------------------------------------------------------------
  * No single reference interface: an ensemble of independent simulations, each an
  * ibg_context with fixed bodies and its own grid, Reynolds number, time step and
@@ -306,6 +333,9 @@ IBG_API int ibg_laplacian(ibg_context* ctx, const double* f, double* out);
 IBG_API int ibg_model_B(ibg_context* ctx, const double* f, double* omega);
 /* NavierStokesModel::C: E(Curl(L^-1(-omega))) (src/NavierStokesModel.cc:107-112) */
 IBG_API int ibg_model_C(ibg_context* ctx, const double* omega, double* f);
+/* Regularizer::toFlux (src/Regularizer.cc:92-109): boundary vector -> Flux of every
+ * level (level 0 holds the smeared values times dx, coarser levels are zero) */
+IBG_API int ibg_reg_to_flux(ibg_context* ctx, const double* f, double* q);
 /* Regularizer::toBoundary (src/Regularizer.cc:111-128): level-0 fluxes -> boundary */
 IBG_API int ibg_reg_to_boundary(ibg_context* ctx, const double* q, double* f);
 /* ProjectionSolver::solve for sub-step k's beta (src/ProjectionSolver.cc:57-79):

@@ -42,12 +42,15 @@ def _write_inputs(wl, tag: str):
 
 
 def run(wl, tag: str, steps: int, warmup: int = 1, timeout: float = 1800.0, cores: int = 1) -> dict:
-    """Run W + K steps of workload `wl`; returns the driver's JSON plus wall time."""
+    """Run W + K steps of workload `wl`; returns the driver's JSON plus wall time
+    and the net force (x, y) after each of the W + K steps ("forces")."""
+    import numpy as np
     gpath, ic = _write_inputs(wl, tag)
+    out_prefix = os.path.join(CACHE, tag + "_run")
     args = [DRIVER, "-nx", str(wl.nx), "-ny", str(wl.ny), "-ngrid", str(wl.ngrid), "-length", repr(wl.length),
             "-xoffset", repr(wl.xoffset), "-yoffset", repr(wl.yoffset), "-geom", gpath, "-Re", repr(wl.Re),
             "-dt", repr(wl.dt), "-scheme", wl.scheme, "-nsteps", str(steps + warmup), "-warmup", str(warmup),
-            "-tol", repr(wl.tol), "-cholesky_cache", os.path.join(CACHE, tag)]
+            "-tol", repr(wl.tol), "-cholesky_cache", os.path.join(CACHE, tag), "-out", out_prefix]
     if ic:
         args += ["-ic", ic]
     if cores == 1:
@@ -58,6 +61,12 @@ def run(wl, tag: str, steps: int, warmup: int = 1, timeout: float = 1800.0, core
     line = [l for l in p.stdout.splitlines() if l.startswith("{")][-1]
     out = json.loads(line)
     out["wall_s"] = wall
+    out["forces"] = np.loadtxt(out_prefix + ".forces").reshape(-1, 6)[:, 2:4]
+    for suffix in (".forces", "_final.bin"):
+        try:
+            os.remove(out_prefix + suffix)
+        except OSError:
+            pass
     return out
 
 

@@ -18,7 +18,7 @@ FP64_TOL = 1e-10
 def golden_names():
     """Fixtures of the nonlinear solver (NonlinearIBSolver)."""
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz"))
-                  if not os.path.basename(p).startswith("var_"))
+                  if not os.path.basename(p).startswith(("var_", "full_")))
 
 
 def variant_names():

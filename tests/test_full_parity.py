@@ -1,0 +1,132 @@
+"""Parity at the workloads' full sizes against the reference's own runs.
+
+The fixtures tests/golden/full_*.npz were written by the reference library
+(oracle/_ref/ref_driver_parity, -O2 without fast-math) through
+tests/golden/make_full.py: per-step forces and the final state after a
+truncated number of steps of each named workload at its full grid size.
+
+Bars (relative L2 against the reference's FP64 run):
+* plain FP64 path: 1e-10 for vorticity, flux, streamfunction and forces
+  (the boundary force vector itself 1e-9);
+* moving bodies: the force solve is CG to the absolute tolerance |r| <= tol;
+  plain CG follows the reference's iteration and is held to 1e-10; the
+  preconditioned forms stop at a different iterate of the same tolerance and
+  are held to 1e-8;
+* reduced precision (FP32 transforms + one FP64-residual refinement per
+  solve): 1e-5 vorticity, 1e-4 forces.
+"""
+import numpy as np
+import pytest
+
+from helpers import FP64_TOL, load_golden, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+W_TOL_REDUCED = 1e-5
+F_TOL_REDUCED = 1e-4
+PCG_TOL = 1e-8
+
+
+def _run(wl, nsteps, keep=False, **kw):
+    import ibpm_b200 as ib
+    grid, model, s, x = ib.from_workload(wl, **kw)
+    s.init()
+    s.set_state(x, with_q=False)
+    s.advance_resident(nsteps)
+    forces = s.force_history(nsteps)
+    s.get_state(x)
+    if not keep:
+        s.close()
+        s = None
+    return forces, x, s
+
+
+def test_c1_all_250_steps_fp64():
+    """200x200 fixed cylinder, Re 100, dt 0.01, RK3, from rest: all 250 steps."""
+    from ibpm_b200 import configs
+    d = load_golden("full_c1")
+    forces, x, s = _run(configs.c1_fixed_cylinder(), 250, keep=True)
+    assert rel_l2(forces, d["forces"][:, 2:4]) < FP64_TOL
+    assert rel_l2(forces[:, 0], d["forces"][:, 2]) < FP64_TOL  # drag alone
+    assert rel_l2(x.omega, d["omega"]) < FP64_TOL
+    assert rel_l2(x.q, d["q"]) < FP64_TOL
+    assert rel_l2(s.poisson(-x.omega), d["psi"]) < FP64_TOL  # streamfunction (vorticityToStreamfunction)
+    assert rel_l2(x.f, d["f"]) < 1e-9
+    assert x.timestep == 250
+    s.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_refined"])
+def test_c2_first_20_steps(precision):
+    """400x200 x5 domains, seeded wake noise, Re 200, dt 0.005: the first 20 steps."""
+    from ibpm_b200 import configs
+    d = load_golden("full_c2")
+    forces, x, _ = _run(configs.c2_shedding_cylinder(), 20, precision=precision)
+    ef = rel_l2(forces, d["forces"][:, 2:4])
+    ew = rel_l2(x.omega, d["omega"])
+    if precision == "fp64":
+        assert ef < FP64_TOL and ew < FP64_TOL, (ef, ew)
+    else:
+        assert ef < F_TOL_REDUCED and ew < W_TOL_REDUCED, (ef, ew)
+    # the force history step by step (lift and drag of every step, not only the run's norm)
+    per_step = np.abs(forces - d["forces"][:, 2:4]).max(axis=1) / np.abs(d["forces"][:, 2:4]).max()
+    assert per_step.max() < (FP64_TOL if precision == "fp64" else F_TOL_REDUCED)
+
+
+@pytest.mark.parametrize("precond", ["none", "cholesky", "learned"])
+def test_c3_first_3_steps(precond):
+    """500x250 x3 domains, pitching and plunging plate, CG at tol 1e-10: plain CG
+    (the reference's method), Cholesky-preconditioned and learned-preconditioned
+    flexible CG converge to the same forces."""
+    import ibpm_b200 as ib
+    from ibpm_b200 import configs
+    d = load_golden("full_c3")
+    wl = configs.c3_pitching_plate()
+    if precond == "learned":
+        grid, model, s, x = ib.from_workload(wl, precond="learned")
+        geom, mb = s.lpc_generate(16, 0.0, 8.0)
+        s.lpc_train(geom, mb, epochs=150, batch=4, lr=2e-3, seed=1)
+        s.init()
+        s.set_state(x, with_q=False)
+        s.advance_resident(3)
+        forces = s.force_history(3)
+        s.get_state(x)
+        s.close()
+    else:
+        forces, x, _ = _run(wl, 3, precond=precond)
+    tol = FP64_TOL if precond == "none" else PCG_TOL
+    assert rel_l2(forces, d["forces"][:, 2:4]) < tol
+    assert rel_l2(x.omega, d["omega"]) < tol
+    assert rel_l2(x.f, d["f"]) < 10 * tol
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "fp32_refined"])
+@pytest.mark.parametrize("member", [0, 1])
+def test_c4_members_10_steps(member, precision):
+    """Two ensemble members (the first two with n <= 256) for 10 steps, FP64, the
+    FP32-bulk form the ensemble benchmark runs, and the refined form."""
+    from ibpm_b200 import configs
+    k, wl = [(k, w) for k, w in enumerate(configs.ensemble_members()) if w.nx <= 256][member]
+    d = load_golden(f"full_c4_{k}")
+    forces, x, _ = _run(wl, 10, precision=precision)
+    ef = rel_l2(forces, d["forces"][:, 2:4])
+    ew = rel_l2(x.omega, d["omega"])
+    if precision == "fp64":
+        assert ef < FP64_TOL and ew < FP64_TOL, (ef, ew)
+    else:
+        assert ef < F_TOL_REDUCED and ew < W_TOL_REDUCED, (ef, ew)
+
+
+def test_c5_first_2_steps_fp64():
+    """1024x1024 x5 domains, two cylinders plunging in antiphase, plain CG at tol
+    1e-10: the first 2 steps.  The fixture holds omega on every 8th node of every
+    level and each level's L2 norm (the whole field is 42 MB)."""
+    from ibpm_b200 import configs
+    d = load_golden("full_c5")
+    forces, x, _ = _run(configs.c5_two_cylinders(), 2)
+    k = int(d["sample"])
+    assert rel_l2(forces, d["forces"][:, 2:4]) < FP64_TOL
+    assert rel_l2(x.omega[:, ::k, ::k], d["omega_sample"]) < FP64_TOL
+    norms = np.linalg.norm(x.omega.reshape(x.omega.shape[0], -1), axis=1)
+    assert rel_l2(norms, d["omega_level_norms"]) < FP64_TOL
+    assert rel_l2(x.f, d["f"]) < 1e-9

@@ -51,6 +51,7 @@ def test_elliptic_and_stencils(gp):
     model_o = O.Model(g, [O.Body(pts)], 100.0)
     assert rel_l2(s.model_C(f), model_o.C(f)) < OP_TOL
     assert rel_l2(s.reg_to_boundary(q[0]), reg.to_boundary(q)) < OP_TOL
+    assert rel_l2(s.reg_to_flux(fb), reg.to_flux(fb)) < OP_TOL
     s.close()
 
 
@@ -207,12 +208,16 @@ def test_c1_size_steps_match_oracle():
     s.close()
 
 
+@pytest.mark.parametrize("precision", ["fp32_refined", "fp32"])
 @pytest.mark.parametrize("name", ["cyl_l3_noise_rk3", "plate_l2_pitchplunge_cg"])
-def test_fp32_form_within_force_and_vorticity_bars(name):
-    """The FP32 bulk form against the reference run: vorticity within 1e-5
-    relative; forces within 3e-4 on these short runs from rest.  (The
-    constraint right-hand side C w* - b is a small difference of O(1) terms,
-    and M^-1 amplifies the FP32 state error.)"""
+def test_reduced_precision_forms_against_reference(name, precision):
+    """The reduced-precision forms against the reference run.  fp32_refined
+    (FP32 transforms with one FP64-residual refinement per solve, FP64 state)
+    is held to the bars of the reduced-precision form: vorticity within 1e-5
+    and forces within 1e-4 relative.  fp32 (the whole bulk in FP32, no
+    refinement) keeps vorticity within 1e-5 but its forces only within 3e-4 on
+    these short runs from rest: the constraint right-hand side C w* - b is a
+    small difference of O(1) terms and M^-1 amplifies the FP32 state error."""
     import ibpm_b200 as ib
     d = load_golden(name)
     grid = ib.Grid(int(d["nx"]), int(d["ny"]), int(d["ngrid"]), float(d["length"]), float(d["xoffset"]),
@@ -220,7 +225,7 @@ def test_fp32_form_within_force_and_vorticity_bars(name):
     geo = ib.geometry.parse(str(d["geom"]))
     model = ib.NavierStokesModel(grid, geo, float(d["Re"]))
     s = ib.NonlinearIBSolver(grid, model, float(d["dt"]), str(d["scheme"]), max(float(d["tol"]), 1e-7),
-                             precision="fp32")
+                             precision=precision)
     x = ib.State(grid, geo.num_points, omega=np.array(d["omega0"], dtype=float))
     s.init()
     s.set_state(x, with_q=False)
@@ -228,7 +233,7 @@ def test_fp32_form_within_force_and_vorticity_bars(name):
     s.advance_resident(n)
     forces = s.force_history(n)
     s.get_state(x)
-    assert rel_l2(forces, d["forces"][:, 2:4]) < 3e-4
+    assert rel_l2(forces, d["forces"][:, 2:4]) < (1e-4 if precision == "fp32_refined" else 3e-4)
     assert rel_l2(x.omega, d["omega"]) < 1e-5
     s.close()
 
