@@ -1139,6 +1139,7 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
         return IBG_ERR_CUDA;
     }
     cudaMemcpy(c->d_ref, c->h_ref.data(), sizeof(double) * c->h_ref.size(), cudaMemcpyHostToDevice);
+    c->slots.pts = c->d_pts;
     c->lb.n = nbodies;
     c->lb.body_of = c->d_body_of;
     if (c->alloc(&c->lb.start, nbodies) || c->alloc(&c->lb.len, nbodies) || c->alloc(&c->lb.closed, nbodies)) {
@@ -1878,7 +1879,7 @@ int ibg_reg_to_flux(ibg_context* c, const double* fb, double* q) {
     const GridDev& g = c->g;
     cudaMemcpyAsync(c->btmp, fb, sizeof(double) * c->ncomp, cudaMemcpyHostToDevice, c->st);
     // level 0: sum of weight * f over the associations, times dx; every coarser level is zero
-    launch_reg_smear(c->ncomp, c->slots, c->btmp, c->flux0, c->st);
+    launch_reg_smear(c->ncomp, c->slots, g.dx, c->btmp, c->flux0, c->st);
     launch_k(k_scale, (unsigned)((g.F1 + 255) / 256), 256, 0, c->st, (size_t)g.F1, (const double*)c->flux0, g.dx,
              c->b64.qtmp);
     launch_reg_zero(c->ncomp, c->slots, c->flux0, c->st);
@@ -2399,6 +2400,21 @@ int ibg_lpc_apply(ibg_context* c, int k, const double* r, double* z, float* geom
     return c->cuda_check("ibg_lpc_apply");
 }
 
+int ibg_lpc_set_tensor_cores(ibg_context* c, int on) {
+    if (!c) return IBG_ERR_ARG;
+    if (lpc_ensure(c)) return IBG_ERR_CUDA;
+    c->lpc.tensor_cores = on != 0;
+    c->drop_graph();
+    return IBG_OK;
+}
+int ibg_lpc_status(ibg_context* c) {
+    if (!c) return IBG_ERR_ARG;
+    if (!c->lpc.err) return 0;
+    int e = 0;
+    cudaMemcpyAsync(&e, c->lpc.err, sizeof(int), cudaMemcpyDeviceToHost, c->st);
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->cuda_check("ibg_lpc_status");
+    return e;
+}
 int ibg_substep_beta(ibg_context* c, int k, double* beta) {
     if (!c || !beta || k < 0 || k >= c->sch.nsub) return IBG_ERR_ARG;
     *beta = c->beta[k];

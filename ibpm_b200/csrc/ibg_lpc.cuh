@@ -34,6 +34,10 @@ struct Lpc {
     float* geom = nullptr;     // current geometry features (P x 4)
     float* gbar = nullptr;     // their neighbour means (P x 4)
     float* kraw = nullptr;     // network output per point pair (P^2 x 4)
+    void* w2op = nullptr;      // W2 in BF16 as the tensor-core kernel's B operand (lpc_tc.cu)
+    int* err = nullptr;        // set by the tensor-core kernel when a bounded wait ran out
+    bool tensor_cores = true;  // inference on tcgen05 (else the CUDA-core kernel)
+    int num_sms = 148;
     int init(int npts, const std::vector<int>& nbr_h, const std::vector<int>& cnt_h);
     void release();
     void refresh_bf16(cudaStream_t st);
@@ -47,6 +51,12 @@ struct Lpc {
     int loss_grad(int B, const float* g, const float* Mb, float* loss, float* grad, TrainScratch& ws,
                   cudaStream_t st) const;
 };
+
+// tensor-core inference (lpc_tc.cu)
+int lpc_infer_tc_setup();
+void lpc_w2_operand(const float* params, void* w2op, cudaStream_t st);
+void lpc_infer_tc(int P, const float* g, const float* gbar, const float* params, const void* w2op, float* kraw,
+                  int* err, int num_sms, cudaStream_t st);
 
 void adam_step(long n, float* p, const float* g, float* m1, float* m2, float lr, int t, cudaStream_t st);
 

@@ -31,6 +31,7 @@ struct RegSlots {
     int* idx = nullptr;     // [2 npts][kSlots] flux index (level 0)
     double* w = nullptr;    // [2 npts][kSlots] weight delta(dx) delta(dy)
     int* n = nullptr;       // [2 npts] number of slots used
+    const double* pts = nullptr;  // [npts][2] the boundary points the slots were built from
 };
 
 template <typename T>
@@ -73,7 +74,7 @@ void launch_reg_interp(const GridDev& g, int ncomp, const RegSlots& s, const T* 
                        const double* bcon, double* out, size_t ostride, cudaStream_t st);
 // Regularizer::toFlux without the dx factor: flux0 (level 0) += sum of weight * f over the
 // associations; launch_reg_zero clears the entries the smear touched
-void launch_reg_smear(int ncomp, const RegSlots& s, const double* f, double* flux0, cudaStream_t st);
+void launch_reg_smear(int ncomp, const RegSlots& s, double h, const double* f, double* flux0, cudaStream_t st);
 void launch_reg_zero(int ncomp, const RegSlots& s, double* flux0, cudaStream_t st);
 template <typename T>
 void launch_smear_bf(const GridDev& g, int ncomp, const RegSlots& s, const double* f, double* flux0, T* Bf,

@@ -402,8 +402,13 @@ int Lpc::init(int npts, const std::vector<int>& nbr_h, const std::vector<int>& c
     if (cudaMalloc(&params, sizeof(float) * kNParams) || cudaMalloc(&nbr, sizeof(int) * 8 * P) ||
         cudaMalloc(&cnt, sizeof(int) * P) || cudaMalloc(&wbf, sizeof(__nv_bfloat16) * w) ||
         cudaMalloc(&geom, sizeof(float) * 4 * P) || cudaMalloc(&gbar, sizeof(float) * 4 * P) ||
-        cudaMalloc(&kraw, sizeof(float) * (size_t)P * P * kO))
+        cudaMalloc(&kraw, sizeof(float) * (size_t)P * P * kO) || cudaMalloc(&w2op, sizeof(__nv_bfloat16) * kH * kH) ||
+        cudaMalloc(&err, sizeof(int)))
         return IBG_ERR_CUDA;
+    cudaMemset(err, 0, sizeof(int));
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (lpc_infer_tc_setup()) return IBG_ERR_CUDA;
     cudaMemcpy(nbr, nbr_h.data(), sizeof(int) * 8 * P, cudaMemcpyHostToDevice);
     cudaMemcpy(cnt, cnt_h.data(), sizeof(int) * P, cudaMemcpyHostToDevice);
     // He initialisation with a fixed seed; the output layer starts small
@@ -423,18 +428,20 @@ int Lpc::init(int npts, const std::vector<int>& nbr_h, const std::vector<int>& c
 }
 
 void Lpc::release() {
-    void* p[] = {params, nbr, cnt, wbf, geom, gbar, kraw};
+    void* p[] = {params, nbr, cnt, wbf, geom, gbar, kraw, w2op, err};
     for (void* x : p)
         if (x) cudaFree(x);
     params = nullptr;
     nbr = cnt = nullptr;
-    wbf = nullptr;
+    wbf = w2op = nullptr;
+    err = nullptr;
     geom = gbar = kraw = nullptr;
 }
 
 void Lpc::refresh_bf16(cudaStream_t st) {
     const long w = (long)kH * kF + (long)kH * kH + (long)kO * kH;
     k_lpc_to_bf16<<<(unsigned)((w + 255) / 256), 256, 0, st>>>(params, (__nv_bfloat16*)wbf);
+    lpc_w2_operand(params, w2op, st);
 }
 
 void Lpc::geometry(const double* pts, const LpcBodies& bodies, cudaStream_t st) const {
@@ -449,8 +456,11 @@ void Lpc::operators(int nsub, const double* beta, double* const* Kout, cudaStrea
     const __nv_bfloat16* W2t = W1 + (size_t)kH * kF;
     const __nv_bfloat16* W3 = W2t + (size_t)kH * kH;
     const long npairs = (long)P * P;
-    k_lpc_pair_infer<<<(unsigned)((npairs + kPairsPerCta - 1) / kPairsPerCta), 256, 0, st>>>(
-        P, geom, gbar, W1, params + oB1, W2t, params + oB2, W3, params + oB3, kraw);
+    if (tensor_cores)
+        lpc_infer_tc(P, geom, gbar, params, w2op, kraw, err, num_sms, st);
+    else
+        k_lpc_pair_infer<<<(unsigned)((npairs + kPairsPerCta - 1) / kPairsPerCta), 256, 0, st>>>(
+            P, geom, gbar, W1, params + oB1, W2t, params + oB2, W3, params + oB3, kraw);
     KOut o{};
     for (int k = 0; k < nsub && k < 4; ++k) {
         o.p[k] = Kout[k];

@@ -691,13 +691,38 @@ __global__ void k_reg_interp(GridDev g, int ncomp, const int* __restrict__ sidx,
 }
 
 // smear: flux0[idx] += w f_c (atomic; flux0 is kept zero between uses)
+// Regularizer::toFlux without the dx factor (src/Regularizer.cc:92-109), in a
+// fixed order: the thread of each (component, slot) looks for the other
+// components of the same direction whose slots hold the same flux (only points
+// within 3.5 cells can share one: each reaches 1.5 cells); the first of them in
+// component order writes the sum over all of them in increasing component
+// order, which is the order of the reference's association list
+// (src/Regularizer.cc:54-90) starting from zero, products rounded before the
+// sum as the reference's host arithmetic does.  No atomics, so the result is
+// the same in every run.
 __global__ void k_reg_smear(int ncomp, const int* __restrict__ sidx, const double* __restrict__ sw,
-                            const int* __restrict__ sn, const double* __restrict__ f, double* __restrict__ flux0) {
+                            const int* __restrict__ sn, const double* __restrict__ pts, double h,
+                            const double* __restrict__ f, double* __restrict__ flux0) {
     pdl_enter();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int c = t / kSlots, k = t % kSlots;
     if (c >= ncomp || k >= sn[c]) return;
-    atomicAdd(&flux0[sidx[c * kSlots + k]], sw[c * kSlots + k] * f[c]);
+    const int npts = ncomp / 2, dir = c / npts, p = c % npts;
+    const int j = sidx[c * kSlots + k];
+    const double px = pts[2 * p], py = pts[2 * p + 1], lim = 3.5 * h;
+    double sum = 0.0;
+    for (int q = 0; q < npts; ++q) {
+        if (fabs(pts[2 * q] - px) > lim || fabs(pts[2 * q + 1] - py) > lim) continue;
+        const int c2 = dir * npts + q;
+        const int n2 = sn[c2];
+        for (int k2 = 0; k2 < n2; ++k2) {
+            if (sidx[c2 * kSlots + k2] != j) continue;
+            if (c2 < c) return;  // an earlier component writes this flux
+            sum = __dadd_rn(sum, __dmul_rn(sw[c2 * kSlots + k2], f[c2]));
+            break;
+        }
+    }
+    flux0[j] = sum;
 }
 
 // batched smear of unit vectors: item b carries e_{col0+b}
@@ -870,13 +895,15 @@ void launch_reg_interp(const GridDev& g, int ncomp, const RegSlots& s, const T* 
 template <typename T>
 void launch_smear_bf(const GridDev& g, int ncomp, const RegSlots& s, const double* f, double* flux0, T* Bf,
                      double beta, cudaStream_t st) {
-    launch_k(k_reg_smear, nblk((size_t)ncomp * kSlots, 128), 128, 0, st, ncomp, s.idx, s.w, s.n, f, flux0);
+    launch_k(k_reg_smear, nblk((size_t)ncomp * kSlots, 128), 128, 0, st, ncomp, (const int*)s.idx,
+             (const double*)s.w, (const int*)s.n, s.pts, g.dx, f, flux0);
     launch_k(k_bf<T>, dim3(nblk(g.N1, 256), 1), 256, 0, st, g, flux0, 0, Bf, 0, beta);
     launch_k(k_reg_zero, nblk((size_t)ncomp * kSlots, 128), 128, 0, st, ncomp, 0, 0, s.idx, s.n, flux0, 0);
 }
 
-void launch_reg_smear(int ncomp, const RegSlots& s, const double* f, double* flux0, cudaStream_t st) {
-    launch_k(k_reg_smear, nblk((size_t)ncomp * kSlots, 128), 128, 0, st, ncomp, s.idx, s.w, s.n, f, flux0);
+void launch_reg_smear(int ncomp, const RegSlots& s, double h, const double* f, double* flux0, cudaStream_t st) {
+    launch_k(k_reg_smear, nblk((size_t)ncomp * kSlots, 128), 128, 0, st, ncomp, (const int*)s.idx,
+             (const double*)s.w, (const int*)s.n, s.pts, h, f, flux0);
 }
 void launch_reg_zero(int ncomp, const RegSlots& s, double* flux0, cudaStream_t st) {
     launch_k(k_reg_zero, nblk((size_t)ncomp * kSlots, 128), 128, 0, st, ncomp, 0, 0, s.idx, s.n, flux0, 0);

@@ -20,6 +20,14 @@ extern "C" {
  * negative status. */
 IBG_API long long ibg_run_kernel(ibg_context* ctx, int which, int reps);
 
+/* The learned preconditioner's network evaluation: on = 1 (the default) runs
+ * its 256 x 256 layer on the tensor cores (tcgen05), on = 0 on the CUDA cores
+ * (the two agree to BF16 rounding); the step graph is recaptured.
+ * ibg_lpc_status returns 1 if a tensor-core evaluation ran out of a bounded
+ * wait (its output is then not valid), 0 otherwise. */
+IBG_API int ibg_lpc_set_tensor_cores(ibg_context* ctx, int on);
+IBG_API int ibg_lpc_status(ibg_context* ctx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -143,3 +143,47 @@ def test_gpu_training_lowers_loss_and_pcg_iterations():
         assert rel_l2(x.omega, d["omega"]) < 1e-9
         s.close()
     assert its["learned"] < its["none"], its
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["plate", "two_cylinders_402"])
+def test_tensor_core_inference_matches_cuda_cores_and_oracle(case):
+    """The network's 256 x 256 layer on tcgen05 (the default) against the same
+    evaluation on the CUDA cores and against the float64 forward: both use BF16
+    weights and activations with FP32 accumulation, so they agree to BF16
+    rounding.  The two-cylinder case has 402 points (161,604 pairs, 1263 tiles of
+    128 pairs over the persistent CTAs)."""
+    import ctypes
+    import ibpm_b200 as ib
+    from ibpm_b200 import _native, configs
+    if case == "plate":
+        ib, d, grid, geo = _plate()
+        s = ib.NonlinearIBSolver(grid, ib.NavierStokesModel(grid, geo, float(d["Re"])), float(d["dt"]), "rk3",
+                                 float(d["tol"]), precond="learned")
+    else:
+        wl = configs.c5_two_cylinders()
+        grid = ib.Grid(128, 128, 1, 4.0, -2.0, -2.0)
+        geo = ib.geometry.parse(wl.geom)
+        s = ib.NonlinearIBSolver(grid, ib.NavierStokesModel(grid, geo, wl.Re), wl.dt, "rk3", 1e-7,
+                                 precond="learned")
+    L = _native.lib()
+    rng = np.random.default_rng(3)
+    p = s.lpc_params()
+    p[:-1] += 0.05 * rng.standard_normal(p.size - 1)  # away from the initialisation, as after training
+    p[LP.O_C0] = 2.5
+    s.lpc_set_params(p)
+    r = rng.standard_normal(2 * geo.num_points)
+    z_tc, gm = s.lpc_apply(0, r)
+    assert L.ibg_lpc_status(s.handle) == 0
+    assert L.ibg_lpc_set_tensor_cores(s.handle, 0) == 0
+    z_cc, _ = s.lpc_apply(0, r)
+    assert L.ibg_lpc_set_tensor_cores(s.handle, 1) == 0
+    nbr, cnt = _nbr_of(geo)
+    zc = LP.operator(s.lpc_params(), gm, nbr, cnt, s.beta(0)) @ r
+    assert rel_l2(z_tc, z_cc) < 1e-2, rel_l2(z_tc, z_cc)
+    assert rel_l2(z_tc, zc) < 3e-2
+    assert rel_l2(z_cc, zc) < 3e-2
+    # twice in a row gives the same result (the persistent CTAs hold no state between calls)
+    z_tc2, _ = s.lpc_apply(0, r)
+    assert np.array_equal(z_tc, z_tc2)
+    s.close()
