@@ -76,7 +76,7 @@ FORMS = {"c2": ("fp32_refined", "fp32", "fp64"), "c3": ("cholesky", "learned", "
 PLAIN = {"c2": "fp64", "c3": "cg", "c4": "serial", "c5": "cg"}
 STEPS = {"c2": 200, "c3": 50, "c4": 20, "c5": 10}
 WARMUP = {"c2": 10, "c3": 3, "c4": 3, "c5": 3}
-PC_REFRESH = {"c3": 10, "c5": 50}
+PC_REFRESH = {"c3": 10, "c5": 12}
 L2_NOTE = "flushed between timed steps (256 MB write outside the events)"
 
 
@@ -302,7 +302,7 @@ def _download(s, h):
 class Single:
     """One simulation (c2, c3, c5) in a given form."""
 
-    def __init__(self, wlname, form, stream, device, pc_refresh=10, lpc_train=None):
+    def __init__(self, wlname, form, stream, device, pc_refresh=10, lpc_train=None, cg_graph=True, precision=None):
         import ibpm_b200 as ib
         self.wl = _workload(wlname)
         kw = {}
@@ -311,6 +311,9 @@ class Single:
         else:
             kw["precond"] = {"cg": "none", "cholesky": "cholesky", "learned": "learned"}[form]
             kw["pc_refresh"] = pc_refresh
+            kw["cg_graph"] = cg_graph
+            if precision:
+                kw["precision"] = precision
         self.grid, self.model, self.s, self.x = ib.from_workload(self.wl, stream=stream.cuda_stream, device=device,
                                                                  **kw)
         self.run = {}
@@ -463,6 +466,11 @@ def main():
     ap.add_argument("--members", type=int, default=64, help="c4: ensemble members (the workload has 64)")
     ap.add_argument("--pc-refresh", type=int, default=None, help="c3/c5 cholesky: steps between rebuilds")
     ap.add_argument("--lpc-train", default=None, help="c3/c5 learned: CONFIGS,EPOCHS of the training run")
+    ap.add_argument("--precision", default=None, choices=["fp64", "fp32_refined", "fp32"],
+                    help="c3/c5: arithmetic of the bulk fields and solves (default fp64)")
+    ap.add_argument("--host-cg", action="store_true",
+                    help="c3/c5: the CG loop driven from the host instead of a device WHILE node in the step "
+                         "graph (profilers cannot see the kernels of a graph with conditional nodes)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-path comparison run")
     ap.add_argument("--profile", action="store_true",
@@ -500,7 +508,10 @@ def main():
         stream = torch.cuda.Stream(device=dev)
         if wlname == "c4":
             return Ens(f, stream, local, count=args.members, world_size=ws, rank=rank)
-        return Single(wlname, f, stream, local, pc_refresh=pc_refresh, lpc_train=lpc_train)
+        # the plain path is always FP64; --precision applies to the chosen form
+        prec = args.precision if f != PLAIN[wlname] else None
+        return Single(wlname, f, stream, local, pc_refresh=pc_refresh, lpc_train=lpc_train,
+                      cg_graph=not args.host_cg, precision=prec)
 
     from ibpm_b200.replicas import job_throughput, max_over_ranks
 
@@ -552,12 +563,13 @@ def main():
     e2e_s = maxrank(e2e_s)
     e2e = {"value": job_throughput(1, Ke, job_units, 1000.0 * e2e_s), "unit": UNIT, "h2d_bytes_per_step": bi,
            "d2h_bytes_per_step": bo}
-    roof = kernel_roofline(*run.roof_solver(), flush,
-                           dtype="float" if form in ("fp32", "ensemble_fp32", "fp32_refined", "ensemble_refined")
-                           else "double")
+    f32 = form in ("fp32", "ensemble_fp32", "fp32_refined", "ensemble_refined") or args.precision in (
+        "fp32", "fp32_refined")
+    roof = kernel_roofline(*run.roof_solver(), flush, dtype="float" if f32 else "double")
     info = dict(run.run)
     import ibpm_b200 as ib
     info["autotuned_dst_shapes"] = ib.autotune_log()
+    info["dst_form"] = ib.dst_form_log()
     run.close()
 
     plain = None
@@ -591,13 +603,15 @@ def main():
 
     if rank == 0:
         dtype = {"fp32": "f32+f64", "ensemble_fp32": "f32+f64", "fp32_refined": "f32+f64 refined",
-                 "ensemble_refined": "f32+f64 refined"}.get(form, "f64")
+                 "ensemble_refined": "f32+f64 refined"}.get(args.precision or form, "f64")
         last = forces[-1] if wlname != "c4" else forces[0][-1]
         out = {"metric": METRICS[wlname], "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
                "ms_per_step": ms / K, "higher_is_better": True,
                "scaling": "strong" if wlname == "c4" else "weak", "vs_baseline": None, "dtype": dtype,
                "data": "synthetic (seeded initial conditions and generated geometry)",
-               "config": workload_config(wlname, args.members), "form": form, "run": info, "e2e": e2e,
+               "config": workload_config(wlname, args.members), "form": form + (
+                   f" ({args.precision})" if args.precision and wlname in ("c3", "c5") else ""),
+               "run": info, "e2e": e2e,
                "gpu_launches": int(launches), "roofline": roof, "clocks": clk,
                "final_force": [float(last[0]), float(last[1])] if len(forces) else None}
         if wlname != "c4":

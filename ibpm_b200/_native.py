@@ -69,6 +69,10 @@ SIGNATURES = {
     "ibg_run_kernel": (ctypes.c_longlong, [_VP, _I, _I]),
     "ibg_lpc_set_tensor_cores": (_I, [_VP, _I]),
     "ibg_lpc_status": (_I, [_VP]),
+    "ibg_set_dst_gemm": (_I, [_VP, _I]),
+    "ibg_dst_form_log": (_I, [_VP, _I]),
+    "ibg_dst_gemm_status": (_I, [_VP]),
+    "ibg_solve_fp32": (_I, [_VP, _I, _VP, _VP]),
     "ibg_autotune_log": (_I, [_VP, _I]),
     "ibg_set_linearized": (_I, [_VP, _I, _VP, _VP]),
     "ibg_set_sfd": (_I, [_VP, _D, _D, _VP]),

@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libibpm_b200.so")
-SOURCES = ["elliptic.cu", "ops.cu", "force.cu", "api.cu", "noalloc.cu", "lpc.cu", "lpc_tc.cu", "refine.cu"]
+SOURCES = ["elliptic.cu", "ops.cu", "force.cu", "api.cu", "noalloc.cu", "lpc.cu", "lpc_tc.cu", "refine.cu", "dst_gemm.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "--expt-relaxed-constexpr"]

@@ -17,6 +17,9 @@
 #include <sstream>
 #include <string>
 #include <vector>
+#include <array>
+#include <map>
+#include <mutex>
 
 #include "../../include/ibpm_b200.h"
 #include "../../include/ibpm_b200_diag.h"
@@ -71,14 +74,15 @@ struct Bulk {
     T *w = nullptr, *q = nullptr, *a = nullptr, *ws = nullptr, *psi = nullptr, *cc = nullptr, *rc = nullptr;
     T *tbuf = nullptr, *sweep = nullptr, *U = nullptr, *V = nullptr, *C = nullptr, *Bf = nullptr, *qtmp = nullptr;
     T* Nbuf[4] = {nullptr, nullptr, nullptr, nullptr};
+    T* tbuf2 = nullptr;  // FP32 plans: the GEMM passes' second coefficient buffer
     EllipticPlan<T> poisson;
     EllipticPlan<T> helm[4];
     bool ready = false;
     void release() {
-        T* ptrs[] = {w, q, a, ws, psi, cc, rc, tbuf, sweep, U, V, C, Bf, qtmp, Nbuf[0], Nbuf[1], Nbuf[2], Nbuf[3]};
+        T* ptrs[] = {w, q, a, ws, psi, cc, rc, tbuf, sweep, U, V, C, Bf, qtmp, Nbuf[0], Nbuf[1], Nbuf[2], Nbuf[3], tbuf2};
         for (T* p : ptrs)
             if (p) cudaFree(p);
-        w = q = a = ws = psi = cc = rc = tbuf = sweep = U = V = C = Bf = qtmp = nullptr;
+        w = q = a = ws = psi = cc = rc = tbuf = sweep = U = V = C = Bf = qtmp = tbuf2 = nullptr;
         for (auto& n : Nbuf) n = nullptr;
         ready = false;
     }
@@ -121,6 +125,12 @@ __global__ void k_ext_boundary(int npts, const double* __restrict__ ext, double*
     vel[2 * p + 1] = ext[3 * npts + p];
 }
 
+__global__ void k_scale(size_t n, const double* __restrict__ in, double s, double* __restrict__ out) {
+    pdl_enter();
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = s * in[i];
+}
+
 template <typename A, typename B>
 __global__ void k_convert(size_t n, const A* __restrict__ in, B* __restrict__ out) {
     pdl_enter();
@@ -128,6 +138,35 @@ __global__ void k_convert(size_t n, const A* __restrict__ in, B* __restrict__ ou
     if (i < n) out[i] = (B)in[i];
 }
 }  // namespace ibg
+
+namespace {
+// The autotuner's choice between the FFT and the sine-matrix GEMM form of the FP32
+// DST passes, once per grid shape in the process: {nx, ny, levels} -> {gemm chosen,
+// FFT us, GEMM us} (median of 5 trials of 8 whole Poisson solves each).
+std::mutex g_form_mu;
+std::map<std::array<int, 3>, std::array<double, 3>> g_form;
+
+double time_solves(const EllipticPlan<float>& p, const SolveCall<float>& c, cudaStream_t st) {
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (int w = 0; w < 3; ++w) p.solve(c, st);
+    std::vector<float> ms;
+    for (int t = 0; t < 5; ++t) {
+        cudaEventRecord(e0, st);
+        for (int r = 0; r < 8; ++r) p.solve(c, st);
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float v = 0.f;
+        cudaEventElapsedTime(&v, e0, e1);
+        ms.push_back(v);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::sort(ms.begin(), ms.end());
+    return 1000.0 * ms[2] / 8.0;
+}
+}  // namespace
 
 struct ibg_context {
     // configuration
@@ -153,6 +192,42 @@ struct ibg_context {
     CosTables cosT;
     Bulk<double> b64;
     Bulk<float> b32;
+    SineMats sines;  // FP32 plans: S_x, S_y split for 3xTF32 (dst_gemm.cu)
+    // every FP32 plan's DST passes as sine-matrix GEMMs on the tensor cores, or as FFTs
+    void set_dst_gemm(bool on) {
+        b32.poisson.gemm = on;
+        for (int k = 0; k < 4; ++k) b32.helm[k].gemm = on;
+        drop_graph();
+    }
+    // time whole FP32 solves with the FFT and the GEMM passes the first time a grid shape is
+    // created in the process; keep the GEMM form if it is at least 3 % faster
+    int choose_dst_form() {
+        const std::array<int, 3> key = {g.nx, g.ny, g.L};
+        {
+            std::lock_guard<std::mutex> lock(g_form_mu);
+            auto it = g_form.find(key);
+            if (it != g_form.end()) {
+                set_dst_gemm(it->second[0] > 0.5);
+                return IBG_OK;
+            }
+        }
+        SolveCall<float> c = call<float>(b32, b32.a, b32.ws, 1.0f);
+        cudaMemsetAsync(b32.a, 0, sizeof(float) * S, st);
+        set_dst_gemm(false);
+        const double t_fft = time_solves(b32.poisson, c, st);
+        set_dst_gemm(true);
+        const double t_gemm = time_solves(b32.poisson, c, st);
+        int e = 0;
+        if (sines.err) {
+            cudaMemcpyAsync(&e, sines.err, sizeof(int), cudaMemcpyDeviceToHost, st);
+            cudaStreamSynchronize(st);
+        }
+        const bool use = e == 0 && t_gemm < 0.97 * t_fft;
+        set_dst_gemm(use);
+        std::lock_guard<std::mutex> lock(g_form_mu);
+        g_form[key] = {use ? 1.0 : 0.0, t_fft, t_gemm};
+        return cuda_check("choose_dst_form");
+    }
     double beta[4] = {0, 0, 0, 0};
     // bodies
     std::vector<BodyDev> h_bodies;
@@ -276,6 +351,10 @@ struct ibg_context {
                 alloc(&B.sweep, sweep_doubles(g.nx, g.ny, g.L)) || alloc(&B.U, S) || alloc(&B.V, S) ||
                 alloc(&B.C, F) || alloc(&B.Bf, S) || alloc(&B.qtmp, F);
         for (int k = 0; k < nring && !s; ++k) s = alloc(&B.Nbuf[k], S);
+        if (!s && std::is_same<T, float>::value) {
+            // the sine-matrix GEMM form of the FP32 DST passes (chosen per grid, see set_dst_gemm)
+            s = alloc(&B.tbuf2, S) || sines.init(g.nx, g.ny) || gemm_pass_setup();
+        }
         if (s) return IBG_ERR_CUDA;
         // time the DST passes' launch shapes for this grid once per process (before the plans read them)
         s = tune_passes<T>(&g, &fft, cosT, call<T>(B, B.a, B.ws, (T)1), st);
@@ -286,6 +365,17 @@ struct ibg_context {
             s = B.helm[k].init(&g, &fft, true, alpha, cosT);
         }
         if (s) return s;
+        if constexpr (std::is_same<T, float>::value) {
+            B.poisson.sines = &sines;
+            for (int k = 0; k < 4; ++k) B.helm[k].sines = &sines;
+            const char* e = std::getenv("IBG_DST_GEMM");
+            if (e && (e[0] == '0' || e[0] == '1')) {
+                set_dst_gemm(e[0] == '1');
+            } else {
+                s = choose_dst_form();
+                if (s) return s;
+            }
+        }
         B.ready = true;
         return IBG_OK;
     }
@@ -358,6 +448,7 @@ struct ibg_context {
         drop_graph();
         b64.release();
         b32.release();
+        sines.release();
         release_build_scratch();
         lpc.release();
         tws.release();
@@ -368,7 +459,7 @@ struct ibg_context {
         if (d_ext) cudaFree(d_ext);
         d_ext = nullptr;
         void* ptrs[] = {d_ref, d_pts, d_vel, d_body_of, d_bodies, d_mstate, d_mstate_keep, d_mtab, d_bf, d_bf_state, d_bfv, d_q0,
-                        slots.idx, slots.w, slots.n, d_b, d_time, f,
+                        slots.idx, slots.w, slots.n, slots.own, slots.contrib, d_b, d_time, f,
                         flux0, rhsb, btmp, d_status, cg_r, cg_d, cg_q, cg_scal, cg_flags, d_hist, d_hist_count, cg_z, cg_zold};
         for (void* p : ptrs)
             if (p) cudaFree(p);
@@ -416,6 +507,7 @@ struct ibg_context {
         c.rc = B.rc;
         c.tbuf = B.tbuf;
         c.sweep = B.sweep;
+        c.tbuf2 = B.tbuf2;
         c.bstride = S;
         c.batch = 1;
         c.in_scale = scale;
@@ -434,7 +526,7 @@ struct ibg_context {
         if constexpr (std::is_same<T, double>::value) {
             if (refined) {
                 const EllipticPlan<float>& p32 = which < 0 ? b32.poisson : b32.helm[which];
-                refined_solve(g, p32, c, b64.rc, b32.a, b32.ws, b32.cc, b32.tbuf, b32.sweep, st);
+                refined_solve(g, p32, c, b64.rc, b32.a, b32.ws, b32.cc, b32.tbuf, b32.tbuf2, b32.sweep, st);
                 return;
             }
         }
@@ -624,7 +716,7 @@ struct ibg_context {
             launch_k(k_ext_boundary, (unsigned)((npts + 127) / 128), 128, 0, st, npts,
                      (const double*)(d_ext + (size_t)(slot < 0 ? kExtNow : slot) * 4 * npts), d_pts, d_vel);
             launch_reg_update(g, npts, d_pts, d_vel, slots, d_b, u0, v0, st);
-            launches += 2;
+            launches += 3;
             return;
         }
         if (stateful) {
@@ -633,7 +725,7 @@ struct ibg_context {
         }
         launch_kinematics(npts, d_ref, d_body_of, d_bodies, d_mstate, d_mtab, d_time, toff, d_pts, d_vel, st);
         launch_reg_update(g, npts, d_pts, d_vel, slots, d_b, u0, v0, st);
-        launches += 2;
+        launches += 3;
     }
 
     // BaseFlow::moveFlow(time + toff) (src/NavierStokesModel.cc:94) and the constraints it sets
@@ -788,7 +880,11 @@ struct ibg_context {
                            alloc(&Ld[k], (size_t)m, false) || alloc(&Mi[k], (size_t)m * m, false)))
                 return fail(IBG_ERR_CUDA, "not enough device memory for the Cholesky factors");
         int s = IBG_OK;
-        for (int k = 0; k < sch.nsub && !s; ++k) {
+        // the moving-body preconditioner: M_k = beta_k C A_k^-1 B differs between sub-steps only
+        // through A_k = 1 - beta_k / (2 Re) L, close to 1 at these Reynolds numbers, so one operator
+        // (sub-step 0) scaled by beta_0 / beta_k serves every sub-step and the rebuild costs a third
+        const bool shared = moving && prm.cg_precond == IBG_PRECOND_CHOLESKY;
+        for (int k = 0; k < (shared ? 1 : sch.nsub) && !s; ++k) {
             s = build_m(k);
             if (s) break;
             s = chol_factor(m, bs_M, Lr[k], Lc[k], Ld[k], d_status, st);
@@ -799,6 +895,10 @@ struct ibg_context {
             if (!s && hs) s = fail(IBG_ERR_NUMERIC, "matrix M is not positive definite");
         }
         if (s) return s;
+        if (shared)
+            for (int k = 1; k < sch.nsub; ++k)
+                launch_k(k_scale, (unsigned)(((size_t)m * m + 255) / 256), 256, 0, st, (size_t)m * m,
+                         (const double*)Mi[0], beta[0] / beta[k], Mi[k]);
         chol_ready = true;
         return cuda_check("force operator build");
     }
@@ -1129,6 +1229,7 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
         c->alloc(&c->d_mstate, c->h_bodies.size()) || c->alloc(&c->d_mstate_keep, c->h_bodies.size()) ||
         c->alloc(&c->d_mtab, std::max<size_t>(c->h_mtab.size(), 7)) ||
         c->alloc(&c->slots.idx, kSlots * m) || c->alloc(&c->slots.w, kSlots * m) || c->alloc(&c->slots.n, m) ||
+        c->alloc(&c->slots.own, kSlots * m) || c->alloc(&c->slots.contrib, kSlots * m * kMaxContrib) ||
         c->alloc(&c->d_b, m) || c->alloc(&c->d_time, 1) || c->alloc(&c->d_status, 1) || c->alloc(&c->cg_r, m) ||
         c->alloc(&c->cg_d, m) || c->alloc(&c->cg_q, m) || c->alloc(&c->cg_z, m) || c->alloc(&c->cg_zold, m) || c->alloc(&c->cg_scal, 4) || c->alloc(&c->cg_flags, 10) ||
         c->alloc(&c->d_hist, 2 * (size_t)kHistCap) || c->alloc(&c->d_hist_count, 1) || c->alloc(&c->d_ts0, 1);
@@ -1867,13 +1968,6 @@ int ibg_model_C(ibg_context* c, const double* omega, double* fb) {
     return finish(c, "ibg_model_C");
 }
 
-namespace ibg {
-__global__ void k_scale(size_t n, const double* __restrict__ in, double s, double* __restrict__ out) {
-    pdl_enter();
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = s * in[i];
-}
-}  // namespace ibg
 int ibg_reg_to_flux(ibg_context* c, const double* fb, double* q) {
     if (!c || !fb || !q) return IBG_ERR_ARG;
     const GridDev& g = c->g;
@@ -2400,6 +2494,33 @@ int ibg_lpc_apply(ibg_context* c, int k, const double* r, double* z, float* geom
     return c->cuda_check("ibg_lpc_apply");
 }
 
+int ibg_set_dst_gemm(ibg_context* c, int on) {
+    if (!c) return IBG_ERR_ARG;
+    if (!c->b32.ready) return c->fail(IBG_ERR_STATE, "ibg_set_dst_gemm: the context has no FP32 plans");
+    c->set_dst_gemm(on != 0);
+    return IBG_OK;
+}
+int ibg_dst_gemm_status(ibg_context* c) {
+    if (!c) return IBG_ERR_ARG;
+    if (!c->sines.err) return 0;
+    int e = 0;
+    cudaMemcpyAsync(&e, c->sines.err, sizeof(int), cudaMemcpyDeviceToHost, c->st);
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return c->cuda_check("ibg_dst_gemm_status");
+    return e;
+}
+int ibg_solve_fp32(ibg_context* c, int substep, const double* f, double* u) {
+    if (!c || !f || !u || substep < -1 || substep >= c->sch.nsub) return IBG_ERR_ARG;
+    if (!c->b32.ready) return c->fail(IBG_ERR_STATE, "ibg_solve_fp32: the context has no FP32 plans");
+    Bulk<float>& B = c->b32;
+    Bulk<double>& D = c->b64;
+    cudaMemcpyAsync(D.a, f, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
+    launch_k(k_convert<double, float>, (unsigned)((c->S + 255) / 256), 256, 0, c->st, c->S, (const double*)D.a, B.a);
+    const EllipticPlan<float>& p = substep < 0 ? B.poisson : B.helm[substep];
+    p.solve(c->call<float>(B, B.a, B.psi, 1.0f), c->st);
+    launch_k(k_convert<float, double>, (unsigned)((c->S + 255) / 256), 256, 0, c->st, c->S, (const float*)B.psi, D.psi);
+    cudaMemcpyAsync(u, D.psi, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
+    return finish(c, "ibg_solve_fp32");
+}
 int ibg_lpc_set_tensor_cores(ibg_context* c, int on) {
     if (!c) return IBG_ERR_ARG;
     if (lpc_ensure(c)) return IBG_ERR_CUDA;
@@ -2421,6 +2542,19 @@ int ibg_substep_beta(ibg_context* c, int k, double* beta) {
     return IBG_OK;
 }
 
+int ibg_dst_form_log(double* out, int max_rows) {
+    std::lock_guard<std::mutex> lock(g_form_mu);
+    int k = 0;
+    for (const auto& kv : g_form) {
+        if (out && k < max_rows) {
+            const double row[6] = {(double)kv.first[0], (double)kv.first[1], (double)kv.first[2], kv.second[0],
+                                   kv.second[1], kv.second[2]};
+            for (int q = 0; q < 6; ++q) out[6 * k + q] = row[q];
+        }
+        ++k;
+    }
+    return k;
+}
 int ibg_autotune_log(int* out, int max_rows) {
     const std::vector<TuneResult> r = tune_log();
     if (out)

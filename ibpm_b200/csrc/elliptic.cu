@@ -372,33 +372,6 @@ __global__ void k_dst_rows(RowPassArgs<T> a) {
     }
 }
 
-// eigenvalue of the inverse operator at 0-based mode (k, l):
-// lambda = 2 (cos(pi (k+1)/nx) + cos(pi (l+1)/ny) - 2) / dx^2 (src/EllipticSolver2d.cc:42-54),
-// 1/lambda (Poisson, :115-122) or 1/(1 + alpha lambda) (Helmholtz, :156-163)
-// The FP64 tables hold the cosines and lambda is formed as the reference forms it; the FP32 tables hold
-// cos - 1 (tabulated in double as -2 sin^2(theta / 2)), because in float cos + cos - 2 cancels for the
-// low modes: at n = 512 the lowest eigenvalue would lose three digits and the forces ~1e-4.
-template <typename T>
-__device__ __forceinline__ T eig_inverse(const T* cx, const T* cy, int k, int l, T bydx2, int helm, T alpha) {
-    const T lam = sizeof(T) == 8 ? (T)2 * (cx[k + 1] + cy[l + 1] - (T)2) * bydx2 : (T)2 * (cx[k + 1] + cy[l + 1]) * bydx2;
-    return helm ? (T)1 / ((T)1 + alpha * lam) : (T)1 / lam;
-}
-
-// Coefficient (k, l) of a level after the boundary lifting and the eigen-inverse:
-// U = E (R - c Slift), Slift = sy1 B(k) + syn T(k) + sx1 L(l) + sxn R(l), where
-// B, T, L, R are the 1-D DSTs of the level's bottom, top, left, right boundary values.
-template <typename T>
-__device__ __forceinline__ T lifted_coef(T R, int k, int l, const T* edges, int NI, int NJ, T c,
-                                         const SineTab<T>& s, const T* cx, const T* cy, T bydx2, int helm,
-                                         T alpha) {
-    if (edges) {
-        const T sl = s.sy1[l] * edges[k] + s.syn[l] * edges[NI + k] + s.sx1[k] * edges[2 * NI + l] +
-                     s.sxn[k] * edges[2 * NI + NJ + l];
-        R = R - c * sl;
-    }
-    return R * eig_inverse(cx, cy, k, l, bydx2, helm, alpha);
-}
-
 // ---------------------------------------------------------------------------
 // columns: DST-I along i for pairs of columns (in place).  mode 0 / 2: one
 // transform; mode 1: transform, eigen-inverse scaling, transform (one level);
@@ -1082,6 +1055,57 @@ void EllipticPlan<T>::launch_cols(const GridDev& g, const FftDesc& fcol, int mod
     launch_k(k_dst_cols<T>, dim3((unsigned)ncolblk, (unsigned)(nlev * batch)), nt, fft_smem_bytes<T>(fcol.m, P, tws), st, B);
 }
 
+// the coarse-to-fine sweep of a solve: the boundary DSTs of levels L-2 .. 0 from the
+// forward coefficients `coef` of every level (batch stride L N1)
+template <typename T>
+void EllipticPlan<T>::run_sweep(const SolveCall<T>& c, const T* coef, cudaStream_t st) const {
+    const GridDev& g = *grid;
+    const int L = g.L;
+    const size_t N1 = g.N1;
+    const int batch = c.batch;
+    const size_t tS = (size_t)L * N1;
+    const FftDesc& frow = sizeof(T) == 8 ? tables->row64 : tables->row32;
+    const FftDesc& fcol = sizeof(T) == 8 ? tables->col64 : tables->col32;
+    const T norm = (T)(1.0 / (double)(2 * g.nx * 2 * g.ny));
+    const size_t es = sweep_doubles(g.nx, g.ny, L);
+    const size_t el = 2 * (size_t)g.NI + 2 * (size_t)g.NJ;
+    const GridTables<T>& gt = tabs();
+    const int M = std::max(frow.m, fcol.m);
+    const size_t ssm = sweep_smem_bytes<T>(g, M);
+    for (int lev = L - 1; lev >= 1; --lev) {
+        const double dxl = lev_dx(g, lev);
+        SweepArgs<T> s{};
+        s.g = g;
+        s.frow = frow;
+        s.fcol = fcol;
+        s.buf = coef + (size_t)lev * N1;
+        s.bstride = tS;
+        s.cosx = gt.cosx;
+        s.cosy = gt.cosy;
+        s.s = gt.s;
+        s.bydx2 = (T)(1.0 / (dxl * dxl));
+        s.helmholtz = helmholtz;
+        s.alpha = (T)alpha;
+        s.bc_coef = helmholtz ? (T)(alpha / (dxl * dxl)) : (T)(1.0 / (dxl * dxl));
+        s.edges_in = (lev < L - 1) ? c.sweep + (size_t)lev * el : nullptr;
+        s.edges_out = c.sweep + (size_t)(lev - 1) * el;
+        s.estride = es;
+        s.vrow = c.sweep + (size_t)L * el;
+        s.wstride = es;
+        s.norm = norm;
+        s.ax = gt.ax;
+        s.ay = gt.ay;
+        const int nrb = (g.NI + kSweepRows - 1) / kSweepRows, ncb = (g.NJ + kSweepCols - 1) / kSweepCols;
+        launch_k(k_sweep_sums<T>, dim3((unsigned)(nrb + ncb), (unsigned)batch), 256, 0, st, s);
+        if (gt.ax && gt.ay && edge_maps) {
+            const int nmax = std::max(g.NI, g.NJ);
+            launch_k(k_sweep_edges<T>, dim3((unsigned)((nmax + kEdgeRows - 1) / kEdgeRows), 2, (unsigned)batch), 32 * kEdgeRows, sizeof(T) * 2 * (size_t)nmax, st, s);
+        } else {
+            launch_k(k_sweep_lines<T>, dim3(2, (unsigned)batch), 512, ssm, st, s);
+        }
+    }
+}
+
 template <typename T>
 int EllipticPlan<T>::solve(const SolveCall<T>& c, cudaStream_t st) const {
     const GridDev& g = *grid;
@@ -1089,6 +1113,7 @@ int EllipticPlan<T>::solve(const SolveCall<T>& c, cudaStream_t st) const {
     const size_t N1 = g.N1;
     const int batch = c.batch;
     if (batch < 1 || batch * L > 65535) return IBG_ERR_ARG;
+    if (gemm && sines && c.tbuf2) return solve_gemm(c, st);
     const FftDesc& frow = sizeof(T) == 8 ? tables->row64 : tables->row32;
     const FftDesc& fcol = sizeof(T) == 8 ? tables->col64 : tables->col32;
     const T norm = (T)(1.0 / (double)(2 * g.nx * 2 * g.ny));  // src/EllipticSolver2d.cc:80
@@ -1125,45 +1150,9 @@ int EllipticPlan<T>::solve(const SolveCall<T>& c, cudaStream_t st) const {
     launch_rows(g, frow, L, batch, in, alt, c.bstride, tb, tS, nullptr, nullptr, c.in_scale, (T)1, st);
     launch_cols(g, fcol, 0, L, batch, c.tbuf, N1, tS, nullptr, 0, st);
     // 3. coarse-to-fine sweep: boundary DSTs of levels L-2 .. 0
-    const size_t es = sweep_doubles(g.nx, g.ny, L);
-    const size_t el = 2 * (size_t)g.NI + 2 * (size_t)g.NJ;
-    const GridTables<T>& gt = tabs();
-    const int M = std::max(frow.m, fcol.m);
-    const size_t ssm = sweep_smem_bytes<T>(g, M);
-    for (int lev = L - 1; lev >= 1; --lev) {
-        const double dxl = lev_dx(g, lev);
-        SweepArgs<T> s{};
-        s.g = g;
-        s.frow = frow;
-        s.fcol = fcol;
-        s.buf = c.tbuf + (size_t)lev * N1;
-        s.bstride = tS;
-        s.cosx = gt.cosx;
-        s.cosy = gt.cosy;
-        s.s = gt.s;
-        s.bydx2 = (T)(1.0 / (dxl * dxl));
-        s.helmholtz = helmholtz;
-        s.alpha = (T)alpha;
-        s.bc_coef = helmholtz ? (T)(alpha / (dxl * dxl)) : (T)(1.0 / (dxl * dxl));
-        s.edges_in = (lev < L - 1) ? c.sweep + (size_t)lev * el : nullptr;
-        s.edges_out = c.sweep + (size_t)(lev - 1) * el;
-        s.estride = es;
-        s.vrow = c.sweep + (size_t)L * el;
-        s.wstride = es;
-        s.norm = norm;
-        s.ax = gt.ax;
-        s.ay = gt.ay;
-        const int nrb = (g.NI + kSweepRows - 1) / kSweepRows, ncb = (g.NJ + kSweepCols - 1) / kSweepCols;
-        launch_k(k_sweep_sums<T>, dim3((unsigned)(nrb + ncb), (unsigned)batch), 256, 0, st, s);
-        if (gt.ax && gt.ay && edge_maps) {
-            const int nmax = std::max(g.NI, g.NJ);
-            launch_k(k_sweep_edges<T>, dim3((unsigned)((nmax + kEdgeRows - 1) / kEdgeRows), 2, (unsigned)batch), 32 * kEdgeRows, sizeof(T) * 2 * (size_t)nmax, st, s);
-        } else {
-            launch_k(k_sweep_lines<T>, dim3(2, (unsigned)batch), 512, ssm, st, s);
-        }
-    }
+    run_sweep(c, c.tbuf, st);
     // 4. inverse transforms of every level (lifting + eigen-inverse applied on load)
-    launch_cols(g, fcol, 3, L, batch, c.tbuf, N1, tS, c.sweep, es, st);
+    launch_cols(g, fcol, 3, L, batch, c.tbuf, N1, tS, c.sweep, sweep_doubles(g.nx, g.ny, L), st);
     T* uo[kMaxLevels];
     T* o2[kMaxLevels];
     const T* bs[kMaxLevels];
@@ -1177,6 +1166,95 @@ int EllipticPlan<T>::solve(const SolveCall<T>& c, cudaStream_t st) const {
     launch_rows(g, frow, L, batch, tin, nullptr, tS, uo, c.bstride, c.out2 ? o2 : nullptr, c.base ? bs : nullptr,
                 (T)1, norm, st);
     return cudaPeekAtLastError() == cudaSuccess ? IBG_OK : IBG_ERR_CUDA;
+}
+
+// The same solve with every DST pass a sine-matrix GEMM on the tensor cores
+// (dst_gemm.cu; FP32 plans).  The column passes cannot work in place (several
+// CTAs read the same coefficients), so the forward column pass writes tbuf2,
+// the sweep reads the coefficients there, and the inverse column pass writes
+// back to tbuf.  One level: rows, columns, columns with the eigen-inverse on
+// load, rows.
+template <>
+int EllipticPlan<float>::solve_gemm(const SolveCall<float>& c, cudaStream_t st) const {
+    const GridDev& g = *grid;
+    const int L = g.L;
+    const size_t N1 = g.N1;
+    const int batch = c.batch;
+    const size_t tS = (size_t)L * N1;
+    const GridTables<float>& gt = tabs();
+    GemmPassArgs a{};
+    a.g = g;
+    a.nlev = L;
+    a.err = sines->err;
+    a.cosx = gt.cosx;
+    a.cosy = gt.cosy;
+    a.s = gt.s;
+    a.helmholtz = helmholtz;
+    a.alpha = (float)alpha;
+    for (int l = 0; l < L; ++l) {
+        const double dxl = lev_dx(g, l);
+        a.bydx2[l] = (float)(1.0 / (dxl * dxl));
+        a.bc_coef[l] = helmholtz ? (float)(alpha / (dxl * dxl)) : (float)(1.0 / (dxl * dxl));
+    }
+    // 1. coarsify the right-hand side (rc == nullptr: already coarsified)
+    const int novl = (g.nx / 2 - 1) * (g.ny / 2 - 1);
+    if (c.rc && L > 1)
+        for (int lev = 1; lev < L; ++lev)
+            launch_k(k_coarsify<float>, dim3((unsigned)((novl + 255) / 256), (unsigned)batch), 256, 0, st, g, lev,
+                     c.f, c.rc, c.bstride);
+    // 2. rows forward: f (alt inside the overlap interiors) -> tbuf
+    a.mode = 0;
+    for (int l = 0; l < L; ++l) {
+        a.in[l] = c.f + (size_t)l * N1;
+        a.alt[l] = (l == 0 || !c.rc) ? nullptr : c.rc + (size_t)l * N1;
+        a.out[l] = c.tbuf + (size_t)l * N1;
+    }
+    a.in_bstride = c.bstride;
+    a.out_bstride = tS;
+    a.in_scale = c.in_scale;
+    a.s_hi = sines->sy_hi;
+    a.s_lo = sines->sy_lo;
+    launch_gemm_pass(a, batch, st);
+    // 3. columns forward: tbuf -> tbuf2
+    a.mode = 2;
+    a.src = c.tbuf;
+    a.dst = c.tbuf2;
+    a.lstride = N1;
+    a.bstride = tS;
+    a.s_hi = sines->sx_hi;
+    a.s_lo = sines->sx_lo;
+    launch_gemm_pass(a, batch, st);
+    // 4. the coarse-to-fine sweep from the coefficients in tbuf2
+    if (L > 1) run_sweep(c, c.tbuf2, st);
+    // 5. columns inverse with the lifting (levels below the coarsest) and the eigen-inverse: tbuf2 -> tbuf
+    a.mode = 3;
+    a.src = c.tbuf2;
+    a.dst = c.tbuf;
+    a.edges = L > 1 ? c.sweep : nullptr;
+    a.estride = sweep_doubles(g.nx, g.ny, L);
+    a.elstride = 2 * (size_t)g.NI + 2 * (size_t)g.NJ;
+    launch_gemm_pass(a, batch, st);
+    // 6. rows inverse: tbuf -> u (x 1/(4 nx ny), out2 = base - u)
+    a.mode = 1;
+    for (int l = 0; l < L; ++l) {
+        a.in[l] = c.tbuf + (size_t)l * N1;
+        a.alt[l] = nullptr;
+        a.out[l] = c.u + (size_t)l * N1;
+        a.out2[l] = c.out2 ? c.out2 + (size_t)l * N1 : nullptr;
+        a.base[l] = c.base ? c.base + (size_t)l * N1 : nullptr;
+    }
+    a.in_bstride = tS;
+    a.out_bstride = c.bstride;
+    a.in_scale = 1.0f;
+    a.norm = (float)(1.0 / (double)(2 * g.nx * 2 * g.ny));  // src/EllipticSolver2d.cc:80
+    a.s_hi = sines->sy_hi;
+    a.s_lo = sines->sy_lo;
+    launch_gemm_pass(a, batch, st);
+    return cudaPeekAtLastError() == cudaSuccess ? IBG_OK : IBG_ERR_CUDA;
+}
+template <>
+int EllipticPlan<double>::solve_gemm(const SolveCall<double>&, cudaStream_t) const {
+    return IBG_ERR_UNSUPPORTED;  // FP64 has no tensor-core kind
 }
 
 // Scalar::coarsify (src/Scalar.cc:46-64) of a field in place, finest level first
@@ -1196,6 +1274,7 @@ void coarsify_rhs(const GridDev& g, const double* f, double* rc, cudaStream_t st
 template <typename T>
 int EllipticPlan<T>::launches(bool coarsify) const {
     const int L = grid->L;
+    if (gemm && sines) return L == 1 ? 4 : (coarsify ? L - 1 : 0) + 2 + 2 * (L - 1) + 2;
     return L == 1 ? 3 : (coarsify ? L - 1 : 0) + 2 + 2 * (L - 1) + 2;
 }
 

@@ -101,6 +101,79 @@ struct SweepArgs {
     const T* ay;
 };
 
+// eigenvalue of the inverse operator at 0-based mode (k, l):
+// lambda = 2 (cos(pi (k+1)/nx) + cos(pi (l+1)/ny) - 2) / dx^2 (src/EllipticSolver2d.cc:42-54),
+// 1/lambda (Poisson, :115-122) or 1/(1 + alpha lambda) (Helmholtz, :156-163)
+// The FP64 tables hold the cosines and lambda is formed as the reference forms it; the FP32 tables hold
+// cos - 1 (tabulated in double as -2 sin^2(theta / 2)), because in float cos + cos - 2 cancels for the
+// low modes: at n = 512 the lowest eigenvalue would lose three digits and the forces ~1e-4.
+template <typename T>
+__device__ __forceinline__ T eig_inverse(const T* cx, const T* cy, int k, int l, T bydx2, int helm, T alpha) {
+    const T lam = sizeof(T) == 8 ? (T)2 * (cx[k + 1] + cy[l + 1] - (T)2) * bydx2 : (T)2 * (cx[k + 1] + cy[l + 1]) * bydx2;
+    return helm ? (T)1 / ((T)1 + alpha * lam) : (T)1 / lam;
+}
+
+// Coefficient (k, l) of a level after the boundary lifting and the eigen-inverse:
+// U = E (R - c Slift), Slift = sy1 B(k) + syn T(k) + sx1 L(l) + sxn R(l), where
+// B, T, L, R are the 1-D DSTs of the level's bottom, top, left, right boundary values.
+template <typename T>
+__device__ __forceinline__ T lifted_coef(T R, int k, int l, const T* edges, int NI, int NJ, T c,
+                                         const SineTab<T>& s, const T* cx, const T* cy, T bydx2, int helm,
+                                         T alpha) {
+    if (edges) {
+        const T sl = s.sy1[l] * edges[k] + s.syn[l] * edges[NI + k] + s.sx1[k] * edges[2 * NI + l] +
+                     s.sxn[k] * edges[2 * NI + NJ + l];
+        R = R - c * sl;
+    }
+    return R * eig_inverse(cx, cy, k, l, bydx2, helm, alpha);
+}
+
+// ---------------------------------------------------------------------------
+// sine-matrix GEMM form of the FP32 DST passes (dst_gemm.cu)
+// ---------------------------------------------------------------------------
+// the sine matrices S_x (NI x NI) and S_y (NJ x NJ), S[a][c] = 2 sin(pi (a+1)(c+1) / (n+1)),
+// split into TF32 hi and lo parts (row-major FP32 arrays)
+struct SineMats {
+    float *sx_hi = nullptr, *sx_lo = nullptr, *sy_hi = nullptr, *sy_lo = nullptr;
+    int* err = nullptr;  // set by a GEMM pass whose bounded wait ran out
+    int init(int nx, int ny);
+    void release();
+};
+
+struct GemmPassArgs {
+    GridDev g;
+    int mode;        // 0 rows forward, 1 rows inverse, 2 columns forward, 3 columns inverse (lifting + eigen-inverse)
+    int nlev;
+    int n_tile, tmem_cols;
+    // rows passes: A = the level's data, B = S_y
+    const float* in[kMaxLevels];
+    const float* alt[kMaxLevels];
+    size_t in_bstride;
+    float* out[kMaxLevels];
+    float* out2[kMaxLevels];
+    const float* base[kMaxLevels];
+    size_t out_bstride;
+    float in_scale, norm;
+    // columns passes: A = S_x, B = the level's coefficients transposed
+    const float* src;
+    float* dst;
+    size_t lstride, bstride;
+    const float* edges;
+    size_t estride, elstride;
+    const float* cosx;
+    const float* cosy;
+    SineTab<float> s;
+    float bydx2[kMaxLevels];
+    float bc_coef[kMaxLevels];
+    int helmholtz;
+    float alpha;
+    const float* s_hi;   // the pass's sine matrix
+    const float* s_lo;
+    int* err;
+};
+int gemm_pass_setup();
+void launch_gemm_pass(GemmPassArgs& a, int batch, cudaStream_t st);
+
 struct FftTables {
     FftDesc row64{}, col64{}, row32{}, col32{};
     void* tw_row64 = nullptr;
@@ -161,6 +234,7 @@ struct SolveCall {
     T in_scale;       // multiplies the right-hand side (+1 or -1)
     T* out2;          // optional: out2 = base - u
     const T* base;
+    T* tbuf2 = nullptr;  // scratch of the GEMM passes (L * N1 per batch item; FP32 plans with gemm)
 };
 
 template <typename T>
@@ -174,6 +248,11 @@ struct EllipticPlan {
     // tuned launch shape of the row and column passes for batch 1 (0: rule-based)
     int rows_P = 0, rows_T = 0, cols_P = 0, cols_T = 0, rows_tws = 0, cols_tws = 0;
     bool edge_maps = true;  // the sweep applies the precomputed edge maps (else the per-step line FFTs)
+    // FP32 plans: the DST passes as sine-matrix GEMMs on the tensor cores (dst_gemm.cu) instead of FFTs
+    bool gemm = false;
+    const SineMats* sines = nullptr;
+    int solve_gemm(const SolveCall<T>& c, cudaStream_t st) const;
+    void run_sweep(const SolveCall<T>& c, const T* coef, cudaStream_t st) const;
     int init(const GridDev* g, const FftTables* t, bool helm, double a, const CosTables& ct);
     int solve(const SolveCall<T>& c, cudaStream_t st) const;
     int launches(bool coarsify = true) const;
@@ -200,9 +279,9 @@ std::vector<TuneResult> tune_log();
 // One FP64-accurate solve from FP32 transforms (refine.cu): the FP32 solve of the
 // coarsified right-hand side, its FP64 residual on every level, the FP32 solve of
 // the residual, and the FP64 sum.  rc64 (S doubles) and f32, u32, d32 (S floats)
-// are scratch, tbuf32 and sweep32 the FP32 plan's transform scratch; batch 1.
+// are scratch, tbuf32, tbuf2_32 and sweep32 the FP32 plan's transform scratch; batch 1.
 int refined_solve(const GridDev& g, const EllipticPlan<float>& plan32, const SolveCall<double>& c, double* rc64,
-                  float* f32, float* u32, float* d32, float* tbuf32, float* sweep32, cudaStream_t st);
+                  float* f32, float* u32, float* d32, float* tbuf32, float* tbuf2_32, float* sweep32, cudaStream_t st);
 int refined_solve_launches(const GridDev& g, const EllipticPlan<float>& plan32);
 
 template <>

@@ -23,6 +23,7 @@ struct TrainScratch {
     int cfgs = 0;
     float *gbar = nullptr, *X = nullptr, *H1 = nullptr, *H2 = nullptr, *KO = nullptr, *K = nullptr, *E = nullptr;
     float *dK = nullptr, *dKO = nullptr, *dH2 = nullptr, *dH1 = nullptr, *lossc = nullptr;
+    float* part = nullptr;  // split-K partial products of the weight gradients
     void release();
 };
 

@@ -32,7 +32,13 @@ struct RegSlots {
     double* w = nullptr;    // [2 npts][kSlots] weight delta(dx) delta(dy)
     int* n = nullptr;       // [2 npts] number of slots used
     const double* pts = nullptr;  // [npts][2] the boundary points the slots were built from
+    // the smear's fixed summation order, rebuilt with the slots: own[e] is the number of entries
+    // (component, slot) holding the flux of entry e when e is the first of them in component order,
+    // 0 otherwise; contrib[e] lists them (entry indices c * kSlots + k, in component order)
+    int* own = nullptr;           // [2 npts][kSlots]
+    int* contrib = nullptr;       // [2 npts][kSlots][kMaxContrib]
 };
+constexpr int kMaxContrib = 16;
 
 template <typename T>
 void launch_nonlinear(const GridDev& g, const T* q, const T* w, T* U, T* V, T* C, T* N, int batch, size_t sstride,

@@ -50,16 +50,22 @@ size_t lpc_num_params() { return kNParams; }
 // generic batched FP32 GEMM: C[z][M x N] = alpha op(A) op(B) + beta C, element
 // (i, k) of op(A) at A[z sA + i as0 + k as1], (k, j) of op(B) at
 // B[z sB + k bs0 + j bs1].  64 x 64 tiles, 256 threads, 4 x 4 outputs per thread.
+// With kchunk > 0, item z covers K indices [z kchunk, min(K, (z + 1) kchunk)) (split-K:
+// sA, sB step over K and C[z] receives the partial product).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_sgemm(int M, int N, int K, float alpha, const float* __restrict__ A,
                                                long as0, long as1, long sA, const float* __restrict__ B, long bs0,
                                                long bs1, long sB, float beta, float* __restrict__ C, long ldc,
-                                               long sC) {
+                                               long sC, long kchunk) {
     __shared__ float As[16][64 + 1];
     __shared__ float Bs[16][64 + 1];
     A += blockIdx.z * sA;
     B += blockIdx.z * sB;
     C += blockIdx.z * sC;
+    if (kchunk > 0) {
+        const long rest = (long)K - (long)blockIdx.z * kchunk;
+        K = (int)(rest < kchunk ? rest : kchunk);
+    }
     const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
     const long i0 = (long)blockIdx.y * 64, j0 = (long)blockIdx.x * 64;
     float acc[4][4] = {};
@@ -111,7 +117,34 @@ static void sgemm(long M, int N, int K, float alpha, const float* A, long as0, l
                   long bs1, float beta, float* C, long ldc, cudaStream_t st, int batch = 1, long sA = 0, long sB = 0,
                   long sC = 0) {
     dim3 grid((N + 63) / 64, (unsigned)((M + 63) / 64), batch);
-    k_sgemm<<<grid, 256, 0, st>>>((int)M, N, K, alpha, A, as0, as1, sA, B, bs0, bs1, sB, beta, C, ldc, sC);
+    k_sgemm<<<grid, 256, 0, st>>>((int)M, N, K, alpha, A, as0, as1, sA, B, bs0, bs1, sB, beta, C, ldc, sC, 0L);
+}
+
+// out[i] = sum over z of part[z][i], z in order
+__global__ void k_sum_partials(int nz, long n, const float* __restrict__ part, float* __restrict__ out) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float v = 0.f;
+    for (int z = 0; z < nz; ++z) v += part[(long)z * n + i];
+    out[i] = v;
+}
+
+// A weight gradient C (M x N, contiguous) = op(A) op(B) over a long K (the point pairs of a batch):
+// split-K over up to kMaxSplit chunks of at least 2048 pairs, so that the few output tiles still
+// spread over the whole GPU; the partial products land in `part`, summed in chunk order.
+constexpr int kMaxSplit = 256;
+static void sgemm_wgrad(int M, int N, long K, const float* A, long as0, long as1, const float* B, long bs0, long bs1,
+                        float* C, float* part, cudaStream_t st) {
+    int nsplit = (int)((K + 2047) / 2048);
+    if (nsplit > kMaxSplit) nsplit = kMaxSplit;
+    if (nsplit < 1) nsplit = 1;
+    const long kchunk = (K + nsplit - 1) / nsplit;
+    nsplit = (int)((K + kchunk - 1) / kchunk);
+    dim3 grid((N + 63) / 64, (unsigned)((M + 63) / 64), nsplit);
+    k_sgemm<<<grid, 256, 0, st>>>(M, N, (int)K, 1.f, A, as0, as1, kchunk * as1, B, bs0, bs1, kchunk * bs0, 0.f, part,
+                                  N, (long)M * N, kchunk);
+    const long n = (long)M * N;
+    k_sum_partials<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(nsplit, n, part, C);
 }
 
 // ---------------------------------------------------------------------------
@@ -482,7 +515,8 @@ int Lpc::loss_grad(int B, const float* g, const float* Mb, float* loss, float* g
             cudaMalloc(&ws.KO, sizeof(float) * rows * kO) || cudaMalloc(&ws.K, sizeof(float) * mm) ||
             cudaMalloc(&ws.E, sizeof(float) * mm) || cudaMalloc(&ws.dK, sizeof(float) * mm) ||
             cudaMalloc(&ws.dKO, sizeof(float) * rows * kO) || cudaMalloc(&ws.dH2, sizeof(float) * rows * kH) ||
-            cudaMalloc(&ws.dH1, sizeof(float) * rows * kH) || cudaMalloc(&ws.lossc, sizeof(float) * B)) {
+            cudaMalloc(&ws.dH1, sizeof(float) * rows * kH) || cudaMalloc(&ws.lossc, sizeof(float) * B) ||
+            cudaMalloc(&ws.part, sizeof(float) * (size_t)kMaxSplit * kH * kH)) {
             ws.release();
             return IBG_ERR_CUDA;
         }
@@ -516,17 +550,17 @@ int Lpc::loss_grad(int B, const float* g, const float* Mb, float* loss, float* g
         sgemm(m, m, m, 1.f / c0, ws.E, m, 1, Mb, 1, m, 0.f, ws.dK, m, st, B, mm, mm, mm);
         k_lpc_dko<<<blocks(rows * kO), 256, 0, st>>>(B, P, ws.dK, ws.dKO);
         // layer 3: dW3 = dKO^T H2, db3, dH2 = dKO W3 (masked)
-        sgemm(kO, kH, (int)rows, 1.f, ws.dKO, 1, kO, ws.H2, kH, 1, 0.f, grad + oW3, kH, st);
+        sgemm_wgrad(kO, kH, rows, ws.dKO, 1, kO, ws.H2, kH, 1, grad + oW3, ws.part, st);
         k_colsum<<<kO, 256, 0, st>>>(rows, kO, ws.dKO, grad + oB3);
         sgemm(rows, kH, kO, 1.f, ws.dKO, kO, 1, W3, kH, 1, 0.f, ws.dH2, kH, st);
         k_relu_mask<<<blocks(rows * kH), 256, 0, st>>>(rows * kH, ws.H2, ws.dH2);
         // layer 2: dW2 = dH2^T H1, db2, dH1 = dH2 W2 (masked)
-        sgemm(kH, kH, (int)rows, 1.f, ws.dH2, 1, kH, ws.H1, kH, 1, 0.f, grad + oW2, kH, st);
+        sgemm_wgrad(kH, kH, rows, ws.dH2, 1, kH, ws.H1, kH, 1, grad + oW2, ws.part, st);
         k_colsum<<<kH, 256, 0, st>>>(rows, kH, ws.dH2, grad + oB2);
         sgemm(rows, kH, kH, 1.f, ws.dH2, kH, 1, W2, kH, 1, 0.f, ws.dH1, kH, st);
         k_relu_mask<<<blocks(rows * kH), 256, 0, st>>>(rows * kH, ws.H1, ws.dH1);
         // layer 1: dW1 = dH1^T X, db1
-        sgemm(kH, kF, (int)rows, 1.f, ws.dH1, 1, kH, ws.X, kF, 1, 0.f, grad + oW1, kF, st);
+        sgemm_wgrad(kH, kF, rows, ws.dH1, 1, kH, ws.X, kF, 1, grad + oW1, ws.part, st);
         k_colsum<<<kH, 256, 0, st>>>(rows, kH, ws.dH1, grad + oB1);
         cudaMemsetAsync(grad + oC0, 0, sizeof(float), st);
     }
@@ -540,10 +574,10 @@ int Lpc::loss_grad(int B, const float* g, const float* Mb, float* loss, float* g
 }
 
 void TrainScratch::release() {
-    float* p[] = {gbar, X, H1, H2, KO, K, E, dK, dKO, dH2, dH1, lossc};
+    float* p[] = {gbar, X, H1, H2, KO, K, E, dK, dKO, dH2, dH1, lossc, part};
     for (float* x : p)
         if (x) cudaFree(x);
-    gbar = X = H1 = H2 = KO = K = E = dK = dKO = dH2 = dH1 = lossc = nullptr;
+    gbar = X = H1 = H2 = KO = K = E = dK = dKO = dH2 = dH1 = lossc = part = nullptr;
     rows = 0;
     cfgs = 0;
 }

@@ -691,38 +691,84 @@ __global__ void k_reg_interp(GridDev g, int ncomp, const int* __restrict__ sidx,
 }
 
 // smear: flux0[idx] += w f_c (atomic; flux0 is kept zero between uses)
-// Regularizer::toFlux without the dx factor (src/Regularizer.cc:92-109), in a
-// fixed order: the thread of each (component, slot) looks for the other
-// components of the same direction whose slots hold the same flux (only points
-// within 3.5 cells can share one: each reaches 1.5 cells); the first of them in
-// component order writes the sum over all of them in increasing component
-// order, which is the order of the reference's association list
-// (src/Regularizer.cc:54-90) starting from zero, products rounded before the
-// sum as the reference's host arithmetic does.  No atomics, so the result is
-// the same in every run.
-__global__ void k_reg_smear(int ncomp, const int* __restrict__ sidx, const double* __restrict__ sw,
-                            const int* __restrict__ sn, const double* __restrict__ pts, double h,
-                            const double* __restrict__ f, double* __restrict__ flux0) {
+// The smear's summation order (Regularizer::toFlux, src/Regularizer.cc:92-109),
+// rebuilt whenever the slots are: the thread of each (component, slot) entry
+// looks for the entries of the other components of the same direction that
+// hold the same flux (only points within 3.5 cells can: each reaches 1.5
+// cells).  The first of them in component order -- the order of the
+// reference's association list (src/Regularizer.cc:54-90) -- records how many
+// there are and which, in that order; the others record 0.
+__global__ void k_reg_owners(int ncomp, const int* __restrict__ sidx, const int* __restrict__ sn,
+                             const double* __restrict__ pts, double h, int* __restrict__ own,
+                             int* __restrict__ contrib) {
     pdl_enter();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int c = t / kSlots, k = t % kSlots;
-    if (c >= ncomp || k >= sn[c]) return;
+    if (c >= ncomp) return;
+    if (k >= sn[c]) {
+        own[t] = 0;
+        return;
+    }
     const int npts = ncomp / 2, dir = c / npts, p = c % npts;
-    const int j = sidx[c * kSlots + k];
+    const int j = sidx[t];
     const double px = pts[2 * p], py = pts[2 * p + 1], lim = 3.5 * h;
-    double sum = 0.0;
+    int cnt = 0;
     for (int q = 0; q < npts; ++q) {
         if (fabs(pts[2 * q] - px) > lim || fabs(pts[2 * q + 1] - py) > lim) continue;
         const int c2 = dir * npts + q;
         const int n2 = sn[c2];
         for (int k2 = 0; k2 < n2; ++k2) {
             if (sidx[c2 * kSlots + k2] != j) continue;
-            if (c2 < c) return;  // an earlier component writes this flux
-            sum = __dadd_rn(sum, __dmul_rn(sw[c2 * kSlots + k2], f[c2]));
+            if (c2 < c) {  // an earlier component writes this flux
+                own[t] = 0;
+                return;
+            }
+            if (cnt < kMaxContrib) contrib[(size_t)t * kMaxContrib + cnt] = c2 * kSlots + k2;
+            ++cnt;
             break;
         }
     }
-    flux0[j] = sum;
+    own[t] = cnt;
+}
+
+// Regularizer::toFlux without the dx factor: the first entry of each flux writes
+// the sum over its entries in the recorded order, starting from zero, products
+// rounded before the sum as the reference's host arithmetic does.  No atomics,
+// so the result is the same in every run.  (A flux reached by more than
+// kMaxContrib entries is summed by scanning the points again, in the same order.)
+__global__ void k_reg_smear(int ncomp, const int* __restrict__ sidx, const double* __restrict__ sw,
+                            const int* __restrict__ sn, const int* __restrict__ own,
+                            const int* __restrict__ contrib, const double* __restrict__ pts, double h,
+                            const double* __restrict__ f, double* __restrict__ flux0) {
+    pdl_enter();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = t / kSlots, k = t % kSlots;
+    if (c >= ncomp || k >= sn[c]) return;
+    const int cnt = own[t];
+    if (cnt == 0) return;
+    double sum = 0.0;
+    if (cnt <= kMaxContrib) {
+        const int* lst = contrib + (size_t)t * kMaxContrib;
+        for (int q = 0; q < cnt; ++q) {
+            const int e = lst[q];
+            sum = __dadd_rn(sum, __dmul_rn(sw[e], f[e / kSlots]));
+        }
+    } else {
+        const int npts = ncomp / 2, dir = c / npts, p = c % npts;
+        const int j = sidx[t];
+        const double px = pts[2 * p], py = pts[2 * p + 1], lim = 3.5 * h;
+        for (int q = 0; q < npts; ++q) {
+            if (fabs(pts[2 * q] - px) > lim || fabs(pts[2 * q + 1] - py) > lim) continue;
+            const int c2 = dir * npts + q;
+            const int n2 = sn[c2];
+            for (int k2 = 0; k2 < n2; ++k2) {
+                if (sidx[c2 * kSlots + k2] != j) continue;
+                sum = __dadd_rn(sum, __dmul_rn(sw[c2 * kSlots + k2], f[c2]));
+                break;
+            }
+        }
+    }
+    flux0[sidx[t]] = sum;
 }
 
 // batched smear of unit vectors: item b carries e_{col0+b}
@@ -883,6 +929,8 @@ void launch_kinematics(int npts, const double* ref_xy, const int* body_of, const
 void launch_reg_update(const GridDev& g, int npts, const double* pts, const double* vel, RegSlots& s, double* bcon,
                        double u0, double v0, cudaStream_t st) {
     launch_k(k_reg_update, nblk(2 * npts, 128), 128, 0, st, g, npts, pts, vel, s.idx, s.w, s.n, bcon, u0, v0);
+    launch_k(k_reg_owners, nblk((size_t)2 * npts * kSlots, 128), 128, 0, st, 2 * npts, (const int*)s.idx,
+             (const int*)s.n, pts, g.dx, s.own, s.contrib);
 }
 
 template <typename T>
@@ -896,14 +944,14 @@ template <typename T>
 void launch_smear_bf(const GridDev& g, int ncomp, const RegSlots& s, const double* f, double* flux0, T* Bf,
                      double beta, cudaStream_t st) {
     launch_k(k_reg_smear, nblk((size_t)ncomp * kSlots, 128), 128, 0, st, ncomp, (const int*)s.idx,
-             (const double*)s.w, (const int*)s.n, s.pts, g.dx, f, flux0);
+             (const double*)s.w, (const int*)s.n, (const int*)s.own, (const int*)s.contrib, s.pts, g.dx, f, flux0);
     launch_k(k_bf<T>, dim3(nblk(g.N1, 256), 1), 256, 0, st, g, flux0, 0, Bf, 0, beta);
     launch_k(k_reg_zero, nblk((size_t)ncomp * kSlots, 128), 128, 0, st, ncomp, 0, 0, s.idx, s.n, flux0, 0);
 }
 
 void launch_reg_smear(int ncomp, const RegSlots& s, double h, const double* f, double* flux0, cudaStream_t st) {
     launch_k(k_reg_smear, nblk((size_t)ncomp * kSlots, 128), 128, 0, st, ncomp, (const int*)s.idx,
-             (const double*)s.w, (const int*)s.n, s.pts, h, f, flux0);
+             (const double*)s.w, (const int*)s.n, (const int*)s.own, (const int*)s.contrib, s.pts, h, f, flux0);
 }
 void launch_reg_zero(int ncomp, const RegSlots& s, double* flux0, cudaStream_t st) {
     launch_k(k_reg_zero, nblk((size_t)ncomp * kSlots, 128), 128, 0, st, ncomp, 0, 0, s.idx, s.n, flux0, 0);

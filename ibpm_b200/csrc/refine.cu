@@ -103,7 +103,7 @@ __global__ void k_refine_finish(size_t n, const float* __restrict__ u1, const fl
 }
 
 int refined_solve(const GridDev& g, const EllipticPlan<float>& plan32, const SolveCall<double>& c, double* rc64,
-                  float* f32, float* u32, float* d32, float* tbuf32, float* sweep32, cudaStream_t st) {
+                  float* f32, float* u32, float* d32, float* tbuf32, float* tbuf2_32, float* sweep32, cudaStream_t st) {
     if (c.batch != 1) return IBG_ERR_ARG;
     const size_t S = (size_t)g.L * g.N1;
     const dim3 grid((unsigned)((g.N1 + 255) / 256), (unsigned)g.L);
@@ -114,6 +114,7 @@ int refined_solve(const GridDev& g, const EllipticPlan<float>& plan32, const Sol
     s.u = u32;
     s.rc = nullptr;  // the right-hand side is coarsified already
     s.tbuf = tbuf32;
+    s.tbuf2 = tbuf2_32;
     s.sweep = sweep32;
     s.bstride = S;
     s.batch = 1;

@@ -285,6 +285,15 @@ IBG_API const char* ibg_ensemble_last_error(const ibg_ensemble* ens);
  * pass (0 rows, 1 columns), FFT length, lines, levels, pairs per CTA, threads,
  * twiddles in shared memory} and returns the number of tuned shapes. */
 IBG_API int ibg_autotune_log(int* out, int max_rows);
+/* The autotuner's choice of form for the FP32 DST passes (the FP32 and FP32-refined
+ * contexts): the first time a grid shape is created in the process, whole FP32
+ * Poisson solves are timed with the shared-memory FFT passes and with the
+ * sine-matrix GEMM passes on the tensor cores (tcgen05 kind::tf32, 3xTF32), and
+ * the GEMM form is kept if it is at least 3 % faster (IBG_DST_GEMM=0 or 1 in the
+ * environment fixes the form instead).  ibg_dst_form_log writes up to max_rows
+ * rows of 6 doubles {nx, ny, levels, GEMM chosen (0/1), FFT solve us, GEMM solve
+ * us} and returns the number of grid shapes timed. */
+IBG_API int ibg_dst_form_log(double* out, int max_rows);
 
 /* --- learned preconditioner (no reference counterpart) -----------------------
  * For moving bodies the reference runs plain CG on M f = r every sub-step

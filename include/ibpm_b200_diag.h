@@ -26,6 +26,17 @@ IBG_API long long ibg_run_kernel(ibg_context* ctx, int which, int reps);
  * ibg_lpc_status returns 1 if a tensor-core evaluation ran out of a bounded
  * wait (its output is then not valid), 0 otherwise. */
 IBG_API int ibg_lpc_set_tensor_cores(ibg_context* ctx, int on);
+
+/* The FP32 plans' DST passes (the FP32 and FP32-refined forms): on = 1 runs
+ * them as sine-matrix GEMMs on the tensor cores (tcgen05 kind::tf32, 3xTF32),
+ * on = 0 as shared-memory FFTs (the default unless IBG_DST_GEMM=1 is set in the
+ * environment when the context is created); the step graph is recaptured.
+ * ibg_dst_gemm_status returns 1 if a GEMM pass ran out of a bounded wait.
+ * ibg_solve_fp32 solves with the FP32 plan (substep -1: Poisson, k: the
+ * Helmholtz problem of sub-step k) between FP64 host arrays. */
+IBG_API int ibg_set_dst_gemm(ibg_context* ctx, int on);
+IBG_API int ibg_dst_gemm_status(ibg_context* ctx);
+IBG_API int ibg_solve_fp32(ibg_context* ctx, int substep, const double* f, double* u);
 IBG_API int ibg_lpc_status(ibg_context* ctx);
 
 #ifdef __cplusplus
