@@ -144,6 +144,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_dst_gemm(GemmPassArgs a) {
     const uint32_t idesc = idesc_tf32(NT);
 
     // stage chunk c into shared-memory stage st
+    // stage chunk c into shared-memory stage st.  Each thread first issues all of its global loads
+    // for the chunk (held in registers), then converts and stores, so the loads are in flight together.
     auto stage_chunk = [&](int c, int st) {
         unsigned char* S0 = smem + (size_t)st * kStage;
         unsigned char* Ahi = S0;
@@ -151,55 +153,89 @@ __global__ void __launch_bounds__(kThreads, 1) k_dst_gemm(GemmPassArgs a) {
         unsigned char* Bhi = S0 + 2 * kAbytes;
         unsigned char* Blo = Bhi + Bbytes;
         const int k0 = c * kKc;
-        // A: 128 rows x 32 K
-        for (int e = tid; e < kM * kKc; e += kThreads) {
+        // A: 128 rows x 32 K, 16 elements per thread
+        constexpr int kAper = kM * kKc / kThreads;
+        float av[kAper], al[kAper];
+#pragma unroll
+        for (int u = 0; u < kAper; ++u) {
+            const int e = tid + u * kThreads;
             const int r = e >> 5, kk = e & 31;
             const int gr = m0 + r, gk = k0 + kk;
-            float v = 0.f;
+            av[u] = 0.f;
+            al[u] = 0.f;
             if (gr < Mdim && gk < Kdim) {
                 if (rows) {
                     const float* src = (Xalt && in_overlap(g, gr + 1, gk + 1)) ? Xalt : X;
-                    v = a.in_scale * src[(size_t)gr * Ndim + gk];
+                    av[u] = src[(size_t)gr * Ndim + gk];
                 } else {
-                    v = a.s_hi[(size_t)gr * Kdim + gk];
+                    av[u] = a.s_hi[(size_t)gr * Kdim + gk];
+                    al[u] = a.s_lo[(size_t)gr * Kdim + gk];
                 }
             }
-            float hi, lo;
+        }
+#pragma unroll
+        for (int u = 0; u < kAper; ++u) {
+            const int e = tid + u * kThreads;
+            float hi = av[u], lo = al[u];
             if (rows) {
+                const float v = a.in_scale * av[u];
                 hi = tf32_rna(v);
                 lo = tf32_rna(v - hi);
-            } else {
-                hi = v;
-                lo = (gr < Mdim && gk < Kdim) ? a.s_lo[(size_t)gr * Kdim + gk] : 0.f;
             }
-            const uint32_t off = core32(r, kk);
+            const uint32_t off = core32(e >> 5, e & 31);
             *(float*)(Ahi + off) = hi;
             *(float*)(Alo + off) = lo;
         }
-        // B: NT rows (output columns n) x 32 K
-        for (int e = tid; e < NT * kKc; e += kThreads) {
+        // B: NT rows (output columns n) x 32 K, up to 32 elements per thread
+        constexpr int kBper = kBbytesMax / 4 / kThreads;
+        const int nB = NT * kKc;
+        float bv[kBper], bl[kBper];
+#pragma unroll
+        for (int u = 0; u < kBper; ++u) {
+            const int e = tid + u * kThreads;
+            bv[u] = 0.f;
+            bl[u] = 0.f;
+            if (e < nB) {
+                int n, kk;
+                if (rows) {
+                    n = e >> 5;
+                    kk = e & 31;
+                } else {
+                    kk = e / NT;  // consecutive threads read consecutive columns of one row of T
+                    n = e - kk * NT;
+                }
+                const int gn = n0 + n, gk = k0 + kk;
+                if (gn < Ndim && gk < Kdim) {
+                    if (rows) {
+                        bv[u] = a.s_hi[(size_t)gn * Kdim + gk];
+                        bl[u] = a.s_lo[(size_t)gn * Kdim + gk];
+                    } else {
+                        bv[u] = T[(size_t)gk * Ndim + gn];
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kBper; ++u) {
+            const int e = tid + u * kThreads;
+            if (e >= nB) break;
             int n, kk;
             if (rows) {
                 n = e >> 5;
                 kk = e & 31;
             } else {
-                kk = e / NT;  // consecutive threads read consecutive columns of one row of T
+                kk = e / NT;
                 n = e - kk * NT;
             }
-            const int gn = n0 + n, gk = k0 + kk;
-            float hi = 0.f, lo = 0.f;
-            if (gn < Ndim && gk < Kdim) {
-                if (rows) {
-                    hi = a.s_hi[(size_t)gn * Kdim + gk];
-                    lo = a.s_lo[(size_t)gn * Kdim + gk];
-                } else {
-                    float v = T[(size_t)gk * Ndim + gn];
-                    if (a.mode == 3)
-                        v = lifted_coef(v, gk, gn, edges, Mdim, Ndim, bcc, a.s, a.cosx, a.cosy, bydx2, a.helmholtz,
-                                        a.alpha);
-                    hi = tf32_rna(v);
-                    lo = tf32_rna(v - hi);
-                }
+            float hi = bv[u], lo = bl[u];
+            if (!rows) {
+                const int gn = n0 + n, gk = k0 + kk;
+                float v = bv[u];
+                if (a.mode == 3 && gn < Ndim && gk < Kdim)
+                    v = lifted_coef(v, gk, gn, edges, Mdim, Ndim, bcc, a.s, a.cosx, a.cosy, bydx2, a.helmholtz,
+                                    a.alpha);
+                hi = tf32_rna(v);
+                lo = tf32_rna(v - hi);
             }
             const uint32_t off = core32(n, kk);
             *(float*)(Bhi + off) = hi;
@@ -377,7 +413,9 @@ int gemm_pass_setup() {
 void launch_gemm_pass(GemmPassArgs& a, int batch, cudaStream_t st) {
     const GridDev& g = a.g;
     const int N = g.NJ;
-    int nt = N <= 256 ? ((N + 15) / 16) * 16 : 256;
+    // at least four column tiles per level, so that small levels still spread over several SMs
+    int nt = (((N + 3) / 4) + 15) / 16 * 16;
+    nt = nt < 32 ? 32 : nt > 256 ? 256 : nt;
     a.n_tile = nt;
     a.tmem_cols = nt <= 32 ? 32 : nt <= 64 ? 64 : nt <= 128 ? 128 : 256;
     const dim3 grid((unsigned)((g.NI + kM - 1) / kM), (unsigned)((N + nt - 1) / nt), (unsigned)(a.nlev * batch));

@@ -272,6 +272,10 @@ __device__ __forceinline__ C* fft_stages_c(C* src, C* dst, const C* tw, int P) {
 template <typename C>
 __device__ __forceinline__ C* fft_any(C* s0, C* s1, const C* tw, const FftDesc& d, int P) {
     switch (d.m) {
+        case 128: return fft_stages_c<C, 128, 1>(s0, s1, tw, P);
+        case 192: return fft_stages_c<C, 192, 1>(s0, s1, tw, P);
+        case 200: return fft_stages_c<C, 200, 1>(s0, s1, tw, P);
+        case 250: return fft_stages_c<C, 250, 1>(s0, s1, tw, P);
         case 256: return fft_stages_c<C, 256, 1>(s0, s1, tw, P);
         case 384: return fft_stages_c<C, 384, 1>(s0, s1, tw, P);
         case 400: return fft_stages_c<C, 400, 1>(s0, s1, tw, P);
@@ -287,6 +291,79 @@ __device__ __forceinline__ C* fft_any(C* s0, C* s1, const C* tw, const FftDesc& 
 }
 
 // ---------------------------------------------------------------------------
+// Two forms of the DST-I of the passes, both with two real lines (a, b) packed
+// into one complex FFT:
+//
+// * odd extension (FP32 plans): the line's odd extension of length 2N,
+//   [0, f_1 .. f_n, 0, -f_n .. -f_1] (N = n + 1), is transformed and the DST is
+//   -Im (line a) and Re (line b) of outputs 1 .. n (the transform of an odd real
+//   sequence is imaginary: G_k = -2i sum_j f_j sin(pi j k / N)).
+// * half length (FP64 plans): with s_j = sin(pi j / N) (f_0 = 0) the sequence
+//   y_j = s_j (f_j + f_{N-j}) + (f_j - f_{N-j}) / 2 has DFT sums
+//   C_k = sum y_j cos(2 pi j k / N) and S_k = sum y_j sin(2 pi j k / N) with
+//     DST_{2m+1} = 2 S_{m+1}                  (the odd 0-based outputs)
+//     DST_{2m}   = C_0 + 2 sum_{q=1..m} C_q   (the even ones, a prefix sum)
+//   (y's symmetric part s_j (f_j + f_{N-j}) gives the cosine sums, its
+//   antisymmetric part the sine sums).  z = y^a + i y^b is transformed once
+//   and the two lines' sums separated from Z_k and Z_{N-k}.  Half the FFT
+//   length, so half the shared memory and one radix stage less; but the prefix
+//   sum adds the FFT's rounding of up to N/2 terms, sqrt(N) times the error of
+//   the odd-extension form.  In FP64 that is ~1e-14 relative; in FP32 it
+//   reached 7.7e-5 on the vorticity of a 10-step 256^2 run against 1.2e-5, so
+//   the FP32 plans keep the odd extension.
+// Both forms return 2 sum_j f_j sin(pi j k / N), FFTW's RODFT00 scaling.
+// ---------------------------------------------------------------------------
+template <typename T>
+__host__ __device__ constexpr bool half_dst() { return sizeof(T) == 8; }
+
+template <typename T>
+__device__ __forceinline__ void dst_pre(T fj, T fNj, T s, T& yj, T& yNj) {
+    const T sum = s * (fj + fNj), dif = (T)0.5 * (fj - fNj);
+    yj = sum + dif;
+    yNj = sum - dif;
+}
+
+// O[p][k] = (DST(a)_k, DST(b)_k), k < N - 1, from the half-length FFTs Z of P line pairs (length N each)
+template <typename C>
+__device__ void dst_post(const C* __restrict__ Z, C* __restrict__ O, int N, int P) {
+    using T = decltype(C::x);
+    const int half = N / 2, kh = (N + 1) / 2;  // odd N needs S_k up to k = (N - 1) / 2
+    for (int t = threadIdx.x; t < P * kh; t += blockDim.x) {
+        const int p = t / kh, k = t - p * kh;
+        const C zk = Z[p * N + k], zn = Z[p * N + (k == 0 ? 0 : N - k)];
+        const T ca = (T)0.5 * (zk.x + zn.x), cb = (T)0.5 * (zk.y + zn.y);
+        C* o = O + p * N;
+        o[2 * k] = k == 0 ? cmk<C>(ca, cb) : cmk<C>((T)2 * ca, (T)2 * cb);  // prefix-sum terms
+        if (k >= 1) o[2 * k - 1] = cmk<C>(zn.y - zk.y, zk.x - zn.x);      // 2 S_k of a and b
+    }
+    __syncthreads();
+    // inclusive prefix sums over the even entries, one warp per line pair, 32 terms at a time
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    for (int p = warp; p < P; p += nwarps) {
+        C* o = O + p * N;
+        T ca = (T)0, cb = (T)0;
+        for (int c0 = 0; c0 < half; c0 += 32) {
+            const int mi = c0 + lane;
+            C v = mi < half ? o[2 * mi] : cmk<C>((T)0, (T)0);
+#pragma unroll
+            for (int dd = 1; dd < 32; dd <<= 1) {
+                const T ua = __shfl_up_sync(0xffffffffu, v.x, dd), ub = __shfl_up_sync(0xffffffffu, v.y, dd);
+                if (lane >= dd) {
+                    v.x += ua;
+                    v.y += ub;
+                }
+            }
+            v.x += ca;
+            v.y += cb;
+            if (mi < half) o[2 * mi] = v;
+            ca = __shfl_sync(0xffffffffu, v.x, 31);
+            cb = __shfl_sync(0xffffffffu, v.y, 31);
+        }
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
 // rows: DST-I along j for pairs of rows of every level in the launch
 // (blockIdx.y = batch * nlev + level).  Inside a level's overlap interior
 // the input comes from `alt` (the coarsified right-hand side) when given.
@@ -295,9 +372,10 @@ template <typename T>
 __global__ void k_dst_rows(RowPassArgs<T> a) {
     pdl_enter();
     using C = typename Cplx<T>::type;
+    constexpr bool H = half_dst<T>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const FftDesc& d = a.fft;
-    const int m = d.m;
+    const int m = d.m;  // N = ny (half length) or 2 ny (odd extension)
     const int P = a.pairs_per_block;
     C* s0 = reinterpret_cast<C*>(smem_raw);
     C* s1 = s0 + P * m;
@@ -316,40 +394,79 @@ __global__ void k_dst_rows(RowPassArgs<T> a) {
     const int pair0 = blockIdx.x * P;
     const int npairs = (g.NI + 1) / 2;
     const int ilo = g.nxe, ihi = g.nx / 2 + g.nxe, jlo = g.nye, jhi = g.ny / 2 + g.nye;
-    // every pair's two loads for column k are issued before any is stored (P <= 4)
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        T va[4], vb[4];
+    const T sc = a.in_scale;
+    // value of row r (0-based) at node J (1-based) of this level, the overlap interior from alt
+    auto val = [&](int r, int J) -> T {
+        const bool in_ovl = alt && J > jlo && J < jhi && r + 1 > ilo && r + 1 < ihi;
+        return sc * (in_ovl ? alt : in)[(size_t)r * n + (J - 1)];
+    };
+    if constexpr (H) {
+        // positions j and N - j of every pair are loaded before any is stored (P <= 4)
+        for (int j = 1 + threadIdx.x; j <= m / 2; j += blockDim.x) {
+            const int Nj = m - j;
+            const T s = a.sinh[j];
+            T fa[4], fna[4], fb[4], fnb[4];
 #pragma unroll
-        for (int p = 0; p < 4; ++p) {
-            va[p] = (T)0;
-            vb[p] = (T)0;
-            const int pair = pair0 + p;
-            if (p < P && pair < npairs) {
-                const int r0 = 2 * pair, r1 = 2 * pair + 1;
-                const int J = k + 1;
-                const bool jin = alt && J > jlo && J < jhi;
-                const T* s0p = (jin && r0 + 1 > ilo && r0 + 1 < ihi) ? alt : in;
-                va[p] = a.in_scale * s0p[(size_t)r0 * n + k];
-                if (r1 < g.NI) {
-                    const T* s1p = (jin && r1 + 1 > ilo && r1 + 1 < ihi) ? alt : in;
-                    vb[p] = a.in_scale * s1p[(size_t)r1 * n + k];
+            for (int p = 0; p < 4; ++p) {
+                fa[p] = fna[p] = fb[p] = fnb[p] = (T)0;
+                const int pair = pair0 + p;
+                if (p < P && pair < npairs) {
+                    const int r0 = 2 * pair, r1 = 2 * pair + 1;
+                    fa[p] = val(r0, j);
+                    fna[p] = val(r0, Nj);
+                    if (r1 < g.NI) {
+                        fb[p] = val(r1, j);
+                        fnb[p] = val(r1, Nj);
+                    }
                 }
             }
-        }
 #pragma unroll
-        for (int p = 0; p < 4; ++p) {
-            if (p >= P) break;
-            C* z = s0 + p * m;
-            z[k + 1] = cmk<C>(va[p], vb[p]);
-            z[m - 1 - k] = cmk<C>(-va[p], -vb[p]);
-            if (k == 0) {
-                z[0] = cmk<C>((T)0, (T)0);
-                z[n + 1] = cmk<C>((T)0, (T)0);
+            for (int p = 0; p < 4; ++p) {
+                if (p >= P) break;
+                T ya, yna, yb, ynb;
+                dst_pre(fa[p], fna[p], s, ya, yna);
+                dst_pre(fb[p], fnb[p], s, yb, ynb);
+                C* z = s0 + p * m;
+                z[j] = cmk<C>(ya, yb);
+                z[Nj] = cmk<C>(yna, ynb);
+            }
+        }
+        for (int p = threadIdx.x; p < P; p += blockDim.x) s0[p * m] = cmk<C>((T)0, (T)0);
+    } else {
+        // every pair's two loads for column k are issued before any is stored (P <= 4)
+        for (int k = threadIdx.x; k < n; k += blockDim.x) {
+            T va[4], vb[4];
+#pragma unroll
+            for (int p = 0; p < 4; ++p) {
+                va[p] = (T)0;
+                vb[p] = (T)0;
+                const int pair = pair0 + p;
+                if (p < P && pair < npairs) {
+                    va[p] = val(2 * pair, k + 1);
+                    if (2 * pair + 1 < g.NI) vb[p] = val(2 * pair + 1, k + 1);
+                }
+            }
+#pragma unroll
+            for (int p = 0; p < 4; ++p) {
+                if (p >= P) break;
+                C* z = s0 + p * m;
+                z[k + 1] = cmk<C>(va[p], vb[p]);
+                z[m - 1 - k] = cmk<C>(-va[p], -vb[p]);
+                if (k == 0) {
+                    z[0] = cmk<C>((T)0, (T)0);
+                    z[n + 1] = cmk<C>((T)0, (T)0);
+                }
             }
         }
     }
     __syncthreads();
     C* res = fft_any<C>(s0, s1, tw, d, P);
+    const C* O = res + 1;  // odd extension: output k at k + 1, the DST in (-Im, Re)
+    if constexpr (H) {
+        C* o = (res == s0) ? s1 : s0;
+        dst_post<C>(res, o, m, P);
+        O = o;  // half length: output k at k, the DST in (Re, Im)
+    }
     T* out = a.out[l] + (size_t)b * a.out_bstride;
     T* out2 = a.out2[l] ? a.out2[l] + (size_t)b * a.out_bstride : nullptr;
     const T* base = a.base[l] ? a.base[l] + (size_t)b * a.out_bstride : nullptr;
@@ -357,10 +474,10 @@ __global__ void k_dst_rows(RowPassArgs<T> a) {
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
         const int pair = pair0 + p;
         if (pair >= npairs) continue;
-        const C z = res[p * m + k + 1];
+        const C z = O[p * m + k];
         const int r0 = 2 * pair, r1 = 2 * pair + 1;
         const size_t i0 = (size_t)r0 * n + k;
-        T va = -z.y, vb = z.x;
+        T va = H ? z.x : -z.y, vb = H ? z.y : z.x;
         if (a.norm != (T)1) { va = va * a.norm; vb = vb * a.norm; }
         out[i0] = va;
         if (out2) out2[i0] = base[i0] - va;
@@ -383,9 +500,10 @@ template <typename T>
 __global__ void k_dst_cols(ColPassArgs<T> a) {
     pdl_enter();
     using C = typename Cplx<T>::type;
+    constexpr bool H = half_dst<T>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const FftDesc& d = a.fft;
-    const int m = d.m;
+    const int m = d.m;  // N = nx (half length) or 2 nx (odd extension)
     const int P = a.pairs_per_block;
     C* s0 = reinterpret_cast<C*>(smem_raw);
     C* s1 = s0 + P * m;
@@ -407,76 +525,149 @@ __global__ void k_dst_cols(ColPassArgs<T> a) {
     const int col0 = blockIdx.x * 2 * P;
     const int w = 2 * P;
     const int lw = P == 1 ? 1 : P == 2 ? 2 : 3;  // log2(w), P in {1, 2, 4}
-    // kColLoads elements per thread are loaded (and lifted) before any is stored, so their global
-    // loads are in flight together
-    const int nw_ = n * w;
-    for (int t0 = threadIdx.x; t0 < nw_; t0 += kColLoads * blockDim.x) {
-        T vals[kColLoads];
+    auto load = [&](int i, int col) -> T {
+        T v = buf[(size_t)i * NJ + col];
+        if (a.mode == 3)
+            v = lifted_coef(v, i, col, edges, n, NJ, bcc, a.s, a.cosx, a.cosy, bydx2, a.helmholtz, a.alpha);
+        return v;
+    };
+    if constexpr (H) {
+        // positions j and N - j of every column; kColLoads of them per thread are loaded (and lifted)
+        // before any is stored, so their global loads are in flight together
+        const int nw_ = (m / 2) * w;
+        for (int t0 = threadIdx.x; t0 < nw_; t0 += kColLoads * blockDim.x) {
+            T vj[kColLoads], vn[kColLoads];
 #pragma unroll
-        for (int u = 0; u < kColLoads; ++u) {
-            const int t = t0 + u * (int)blockDim.x;
-            vals[u] = (T)0;
-            if (t < nw_) {
-                const int i = t >> lw;
-                const int col = col0 + (t & (w - 1));
-                if (col < NJ) {
-                    vals[u] = buf[(size_t)i * NJ + col];
-                    if (a.mode == 3)
-                        vals[u] = lifted_coef(vals[u], i, col, edges, n, NJ, bcc, a.s, a.cosx, a.cosy, bydx2,
-                                              a.helmholtz, a.alpha);
+            for (int u = 0; u < kColLoads; ++u) {
+                const int t = t0 + u * (int)blockDim.x;
+                vj[u] = vn[u] = (T)0;
+                if (t < nw_) {
+                    const int j = (t >> lw) + 1;
+                    const int col = col0 + (t & (w - 1));
+                    if (col < NJ) {
+                        vj[u] = load(j - 1, col);
+                        vn[u] = load(m - j - 1, col);
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kColLoads; ++u) {
+                const int t = t0 + u * (int)blockDim.x;
+                if (t >= nw_) break;
+                const int j = (t >> lw) + 1;
+                const int c = t & (w - 1);
+                T yj, yn;
+                dst_pre(vj[u], vn[u], a.sinh[j], yj, yn);
+                C* z = s0 + (c >> 1) * m;
+                if (c & 1) {
+                    z[j].y = yj;
+                    z[m - j].y = yn;
+                } else {
+                    z[j].x = yj;
+                    z[m - j].x = yn;
                 }
             }
         }
+        for (int p = threadIdx.x; p < P; p += blockDim.x) s0[p * m] = cmk<C>((T)0, (T)0);
+    } else {
+        // kColLoads elements per thread are loaded (and lifted) before any is stored
+        const int nw_ = n * w;
+        for (int t0 = threadIdx.x; t0 < nw_; t0 += kColLoads * blockDim.x) {
+            T vals[kColLoads];
 #pragma unroll
-        for (int u = 0; u < kColLoads; ++u) {
-            const int t = t0 + u * (int)blockDim.x;
-            if (t >= nw_) break;
-            const int i = t >> lw;
-            const int c = t & (w - 1);
-            const T v = vals[u];
-            C* z = s0 + (c >> 1) * m;
-            if (c & 1) {
-                z[i + 1].y = v;
-                z[m - 1 - i].y = -v;
-            } else {
-                z[i + 1].x = v;
-                z[m - 1 - i].x = -v;
+            for (int u = 0; u < kColLoads; ++u) {
+                const int t = t0 + u * (int)blockDim.x;
+                vals[u] = (T)0;
+                if (t < nw_) {
+                    const int col = col0 + (t & (w - 1));
+                    if (col < NJ) vals[u] = load(t >> lw, col);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kColLoads; ++u) {
+                const int t = t0 + u * (int)blockDim.x;
+                if (t >= nw_) break;
+                const int i = t >> lw;
+                const int c = t & (w - 1);
+                const T v = vals[u];
+                C* z = s0 + (c >> 1) * m;
+                if (c & 1) {
+                    z[i + 1].y = v;
+                    z[m - 1 - i].y = -v;
+                } else {
+                    z[i + 1].x = v;
+                    z[m - 1 - i].x = -v;
+                }
             }
         }
-    }
-    for (int p = threadIdx.x; p < P; p += blockDim.x) {
-        s0[p * m] = cmk<C>((T)0, (T)0);
-        s0[p * m + n + 1] = cmk<C>((T)0, (T)0);
+        for (int p = threadIdx.x; p < P; p += blockDim.x) {
+            s0[p * m] = cmk<C>((T)0, (T)0);
+            s0[p * m + n + 1] = cmk<C>((T)0, (T)0);
+        }
     }
     __syncthreads();
     C* res = fft_any<C>(s0, s1, tw, d, P);
+    C* O = res + 1;  // odd extension: output k at k + 1, in (-Im, Re)
+    if constexpr (H) {
+        O = (res == s0) ? s1 : s0;
+        dst_post<C>(res, O, m, P);  // half length: output k at k, in (Re, Im)
+    }
     if (a.mode == 1) {
-        C* other = (res == s0) ? s1 : s0;
-        for (int p = 0; p < P; ++p)
-        for (int k = threadIdx.x; k < n; k += blockDim.x) {
-            const C z = res[p * m + k + 1];
-            const int ca = col0 + 2 * p, cb = ca + 1;
-            const T ea = eig_inverse(a.cosx, a.cosy, k, ca < NJ ? ca : 0, bydx2, a.helmholtz, a.alpha);
-            const T eb = eig_inverse(a.cosx, a.cosy, k, cb < NJ ? cb : 0, bydx2, a.helmholtz, a.alpha);
-            const T va = -z.y * ea, vb = z.x * eb;
-            C* zo = other + p * m;
-            zo[k + 1] = cmk<C>(va, vb);
-            zo[m - 1 - k] = cmk<C>(-va, -vb);
-            if (k == 0) {
-                zo[0] = cmk<C>((T)0, (T)0);
-                zo[n + 1] = cmk<C>((T)0, (T)0);
+        // eigen-inverse scaling, then the second DST of the same columns
+        if constexpr (H) {
+            // O -> res (pre-processed) -> FFT -> O
+            const int half = m / 2;
+            for (int t = threadIdx.x; t < P * half; t += blockDim.x) {
+                const int p = t / half, j = t - p * half + 1;
+                const int ca = col0 + 2 * p, cb = ca + 1;
+                const int ia = j - 1, ib = m - j - 1;
+                const C va = O[p * m + ia], vn = O[p * m + ib];
+                const T ea = eig_inverse(a.cosx, a.cosy, ia, ca < NJ ? ca : 0, bydx2, a.helmholtz, a.alpha);
+                const T eb = eig_inverse(a.cosx, a.cosy, ia, cb < NJ ? cb : 0, bydx2, a.helmholtz, a.alpha);
+                const T fa = eig_inverse(a.cosx, a.cosy, ib, ca < NJ ? ca : 0, bydx2, a.helmholtz, a.alpha);
+                const T fb = eig_inverse(a.cosx, a.cosy, ib, cb < NJ ? cb : 0, bydx2, a.helmholtz, a.alpha);
+                const T s = a.sinh[j];
+                T ya, yna, yb, ynb;
+                dst_pre(va.x * ea, vn.x * fa, s, ya, yna);
+                dst_pre(va.y * eb, vn.y * fb, s, yb, ynb);
+                C* z = res + p * m;
+                z[j] = cmk<C>(ya, yb);
+                z[m - j] = cmk<C>(yna, ynb);
             }
+            for (int p = threadIdx.x; p < P; p += blockDim.x) res[p * m] = cmk<C>((T)0, (T)0);
+            __syncthreads();
+            C* r2 = fft_any<C>(res, O, tw, d, P);
+            O = (r2 == res) ? O : res;
+            dst_post<C>(r2, O, m, P);
+        } else {
+            // res -> other (odd extension of the scaled coefficients) -> FFT
+            C* other = (res == s0) ? s1 : s0;
+            for (int p = 0; p < P; ++p)
+            for (int k = threadIdx.x; k < n; k += blockDim.x) {
+                const C z = res[p * m + k + 1];
+                const int ca = col0 + 2 * p, cb = ca + 1;
+                const T ea = eig_inverse(a.cosx, a.cosy, k, ca < NJ ? ca : 0, bydx2, a.helmholtz, a.alpha);
+                const T eb = eig_inverse(a.cosx, a.cosy, k, cb < NJ ? cb : 0, bydx2, a.helmholtz, a.alpha);
+                const T va = -z.y * ea, vb = z.x * eb;
+                C* zo = other + p * m;
+                zo[k + 1] = cmk<C>(va, vb);
+                zo[m - 1 - k] = cmk<C>(-va, -vb);
+                if (k == 0) {
+                    zo[0] = cmk<C>((T)0, (T)0);
+                    zo[n + 1] = cmk<C>((T)0, (T)0);
+                }
+            }
+            __syncthreads();
+            O = fft_any<C>(other, res, tw, d, P) + 1;
         }
-        __syncthreads();
-        res = fft_any<C>(other, res, tw, d, P);
     }
     for (int t = threadIdx.x; t < n * w; t += blockDim.x) {
         const int i = t >> lw;
         const int c = t & (w - 1);
         const int col = col0 + c;
         if (col >= NJ) continue;
-        const C z = res[(c >> 1) * m + i + 1];
-        buf[(size_t)i * NJ + col] = (c & 1) ? z.x : -z.y;
+        const C z = O[(c >> 1) * m + i];
+        buf[(size_t)i * NJ + col] = H ? ((c & 1) ? z.y : z.x) : ((c & 1) ? z.x : -z.y);
     }
 }
 
@@ -539,6 +730,32 @@ __device__ void dst_pair_block(const FftDesc& d, int n, const T* a_in, const T* 
         const C z = res[k + 1];
         a_out[k] = -z.y * scale;
         b_out[k] = z.x * scale;
+    }
+    __syncthreads();
+}
+
+// the same pair of DSTs by the half-length FFT (d.m = N = n + 1, sines[j] = sin(pi j / N))
+template <typename T>
+__device__ void dst_pair_half(const FftDesc& d, const T* __restrict__ sines, const T* a_in, const T* b_in, T* a_out,
+                              T* b_out, T scale, typename Cplx<T>::type* s0, typename Cplx<T>::type* s1) {
+    using C = typename Cplx<T>::type;
+    const int N = d.m, n = N - 1;
+    for (int j = 1 + threadIdx.x; j <= N / 2; j += blockDim.x) {
+        T ya, yna, yb, ynb;
+        dst_pre(a_in[j - 1], a_in[N - j - 1], sines[j], ya, yna);
+        dst_pre(b_in[j - 1], b_in[N - j - 1], sines[j], yb, ynb);
+        s0[j] = cmk<C>(ya, yb);
+        s0[N - j] = cmk<C>(yna, ynb);
+    }
+    if (threadIdx.x == 0) s0[0] = cmk<C>((T)0, (T)0);
+    __syncthreads();
+    C* res = fft_any<C>(s0, s1, reinterpret_cast<const C*>(d.tw), d, 1);
+    C* O = (res == s0) ? s1 : s0;
+    dst_post<C>(res, O, N, 1);
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const C z = O[k];
+        a_out[k] = z.x * scale;
+        b_out[k] = z.y * scale;
     }
     __syncthreads();
 }
@@ -628,7 +845,9 @@ __global__ void __launch_bounds__(512) k_sweep_lines(SweepArgs<T> a) {
     const int b = blockIdx.y;
     const bool xdir = blockIdx.x == 0;
     const int n = xdir ? NI : NJ;
-    const FftDesc& d = xdir ? a.fcol : a.frow;
+    // the half-length DSTs in FP64, the odd-extension ones in FP32 (as the passes)
+    const FftDesc& d = half_dst<T>() ? (xdir ? a.fcolh : a.frowh) : (xdir ? a.fcol : a.frow);
+    const T* sines = xdir ? a.sinc : a.sinr;
     C* s0 = reinterpret_cast<C*>(smem_raw);
     C* s1 = s0 + d.m;
     T* v0 = reinterpret_cast<T*>(s1 + d.m);
@@ -643,7 +862,10 @@ __global__ void __launch_bounds__(512) k_sweep_lines(SweepArgs<T> a) {
         v1[k] = sums[n + k];
     }
     __syncthreads();
-    dst_pair_block<T>(d, n, v0, v1, u0, u1, a.norm, s0, s1);
+    if constexpr (half_dst<T>())
+        dst_pair_half<T>(d, sines, v0, v1, u0, u1, a.norm, s0, s1);
+    else
+        dst_pair_block<T>(d, n, v0, v1, u0, u1, a.norm, s0, s1);
     const int ext = xdir ? g.nxe : g.nye;
     for (int i = 1 + threadIdx.x; i <= n; i += blockDim.x) {
         const int ii = i / 2 + ext;
@@ -657,7 +879,10 @@ __global__ void __launch_bounds__(512) k_sweep_lines(SweepArgs<T> a) {
     }
     __syncthreads();
     T* Eo = a.edges_out + (size_t)b * a.estride + (xdir ? 0 : 2 * (size_t)NI);
-    dst_pair_block<T>(d, n, e0, e1, Eo, Eo + n, (T)1, s0, s1);
+    if constexpr (half_dst<T>())
+        dst_pair_half<T>(d, sines, e0, e1, Eo, Eo + n, (T)1, s0, s1);
+    else
+        dst_pair_block<T>(d, n, e0, e1, Eo, Eo + n, (T)1, s0, s1);
 }
 
 // The lines step is linear in the sums: E0 = norm A V0, E1 = norm A V1 with
@@ -808,9 +1033,11 @@ int FftTables::init(int m_rows, int m_cols) {
             h32[k] = make_float2((float)h64[k].x, (float)h64[k].y);
         }
         if (cudaMalloc(d64, sizeof(double2) * m) != cudaSuccess) return IBG_ERR_CUDA;
-        if (cudaMalloc(d32, sizeof(float2) * m) != cudaSuccess) return IBG_ERR_CUDA;
         cudaMemcpy(*d64, h64.data(), sizeof(double2) * m, cudaMemcpyHostToDevice);
-        cudaMemcpy(*d32, h32.data(), sizeof(float2) * m, cudaMemcpyHostToDevice);
+        if (d32) {  // (the half-length tables have no FP32 copy)
+            if (cudaMalloc(d32, sizeof(float2) * m) != cudaSuccess) return IBG_ERR_CUDA;
+            cudaMemcpy(*d32, h32.data(), sizeof(float2) * m, cudaMemcpyHostToDevice);
+        }
         return IBG_OK;
     };
     int st = make(m_rows, &tw_row64, &tw_row32);
@@ -821,12 +1048,42 @@ int FftTables::init(int m_rows, int m_cols) {
     col64.tw = tw_col64;
     row32.tw = tw_row32;
     col32.tw = tw_col32;
-    return IBG_OK;
+    // the half-length FFTs of the FP64 passes and their sine tables
+    const int nr = m_rows / 2, nc = m_cols / 2;
+    factorize(nr, rowh64);
+    factorize(nc, colh64);
+    if (!fft_supported(nr) || !fft_supported(nc)) return IBG_ERR_UNSUPPORTED;
+    st = make(nr, &tw_rowh64, nullptr);
+    if (st) return st;
+    st = make(nc, &tw_colh64, nullptr);
+    if (st) return st;
+    rowh64.tw = tw_rowh64;
+    colh64.tw = tw_colh64;
+    auto sines = [&](int N, void** d64) -> int {
+        std::vector<double> h(N / 2 + 1);
+        fill_dst_sines(N, h.data());
+        if (cudaMalloc(d64, sizeof(double) * h.size()) != cudaSuccess) return IBG_ERR_CUDA;
+        cudaMemcpy(*d64, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice);
+        return IBG_OK;
+    };
+    st = sines(nr, &sin_row64);
+    if (st) return st;
+    return sines(nc, &sin_col64);
+}
+
+// sin(pi j / N) for j = 0 .. N / 2 (the half-length DST's pre-processing sines)
+void fill_dst_sines(int N, double* out) {
+    const double pi = 3.14159265358979323846264338327950288;
+    for (int j = 0; j <= N / 2; ++j) out[j] = (2 * j == N) ? 1.0 : sin(pi * (double)j / (double)N);
 }
 
 void FftTables::release() {
-    cudaFree(tw_row64); cudaFree(tw_row32); cudaFree(tw_col64); cudaFree(tw_col32);
+    void* p[] = {tw_row64, tw_row32, tw_col64, tw_col32, tw_rowh64, tw_colh64, sin_row64, sin_col64};
+    for (void* x : p)
+        if (x) cudaFree(x);
     tw_row64 = tw_row32 = tw_col64 = tw_col32 = nullptr;
+    tw_rowh64 = tw_colh64 = nullptr;
+    sin_row64 = sin_col64 = nullptr;
 }
 
 // host values of every table the solves use (shared by the context and the static path)
@@ -1005,6 +1262,7 @@ void EllipticPlan<T>::launch_rows(const GridDev& g, const FftDesc& frow, int nle
     A.out_bstride = out_bs;
     A.in_scale = scale;
     A.norm = norm;
+    A.sinh = pass_sines<T>(*tables, 0);
     int P = pairs_per_block<T>(frow.m, g.NI, nlev, batch), nt = threads, tws = 0;
     if (batch == 1 && rows_P > 0) {
         P = rows_P;
@@ -1042,6 +1300,7 @@ void EllipticPlan<T>::launch_cols(const GridDev& g, const FftDesc& fcol, int mod
     B.alpha = (T)alpha;
     B.edges = edges;
     B.estride = estride;
+    B.sinh = pass_sines<T>(*tables, 1);
     B.elstride = 2 * (size_t)g.NI + 2 * (size_t)g.NJ;
     int P = pairs_per_block<T>(fcol.m, g.NJ, nlev, batch), nt = threads, tws = 0;
     if (batch == 1 && cols_P > 0) {
@@ -1078,6 +1337,10 @@ void EllipticPlan<T>::run_sweep(const SolveCall<T>& c, const T* coef, cudaStream
         s.g = g;
         s.frow = frow;
         s.fcol = fcol;
+        s.frowh = pass_desc<T>(*tables, 0);
+        s.fcolh = pass_desc<T>(*tables, 1);
+        s.sinr = pass_sines<T>(*tables, 0);
+        s.sinc = pass_sines<T>(*tables, 1);
         s.buf = coef + (size_t)lev * N1;
         s.bstride = tS;
         s.cosx = gt.cosx;
@@ -1114,8 +1377,8 @@ int EllipticPlan<T>::solve(const SolveCall<T>& c, cudaStream_t st) const {
     const int batch = c.batch;
     if (batch < 1 || batch * L > 65535) return IBG_ERR_ARG;
     if (gemm && sines && c.tbuf2) return solve_gemm(c, st);
-    const FftDesc& frow = sizeof(T) == 8 ? tables->row64 : tables->row32;
-    const FftDesc& fcol = sizeof(T) == 8 ? tables->col64 : tables->col32;
+    const FftDesc& frow = pass_desc<T>(*tables, 0);
+    const FftDesc& fcol = pass_desc<T>(*tables, 1);
     const T norm = (T)(1.0 / (double)(2 * g.nx * 2 * g.ny));  // src/EllipticSolver2d.cc:80
     if (L == 1) {
         const T* in[1] = {c.f};
@@ -1281,8 +1544,8 @@ int EllipticPlan<T>::launches(bool coarsify) const {
 template <typename T>
 void EllipticPlan<T>::run_pass(int which, const T* in, T* tbuf, cudaStream_t st) const {
     const GridDev& g = *grid;
-    const FftDesc& frow = sizeof(T) == 8 ? tables->row64 : tables->row32;
-    const FftDesc& fcol = sizeof(T) == 8 ? tables->col64 : tables->col32;
+    const FftDesc& frow = pass_desc<T>(*tables, 0);
+    const FftDesc& fcol = pass_desc<T>(*tables, 1);
     const int L = g.L;
     const size_t N1 = g.N1;
     if (which == 0) {
@@ -1336,8 +1599,8 @@ std::vector<TuneResult> tune_log() {
 
 template <typename T>
 int tune_passes(const GridDev* g, const FftTables* t, const CosTables& ct, const SolveCall<T>& call, cudaStream_t st) {
-    const FftDesc& frow = sizeof(T) == 8 ? t->row64 : t->row32;
-    const FftDesc& fcol = sizeof(T) == 8 ? t->col64 : t->col32;
+    const FftDesc& frow = pass_desc<T>(*t, 0);
+    const FftDesc& fcol = pass_desc<T>(*t, 1);
     int have_r, have_c, tmp, tmp2;
     tuned_config(sizeof(T), 0, frow.m, g->NI, g->L, have_r, tmp, tmp2);
     tuned_config(sizeof(T), 1, fcol.m, g->NJ, g->L, have_c, tmp, tmp2);
@@ -1420,9 +1683,9 @@ int EllipticPlan<T>::init(const GridDev* g, const FftTables* t, bool helm, doubl
     cos = &ct;
     threads = 128;
     if (g->L > kMaxLevels) return IBG_ERR_UNSUPPORTED;
-    const FftDesc& frow = sizeof(T) == 8 ? t->row64 : t->row32;
-    const FftDesc& fcol = sizeof(T) == 8 ? t->col64 : t->col32;
-    const int M = std::max(frow.m, fcol.m);
+    const FftDesc& frow = pass_desc<T>(*t, 0);  // the passes' half-length FFTs
+    const FftDesc& fcol = pass_desc<T>(*t, 1);
+    const int M = std::max(t->row64.m, t->col64.m);  // the sweep's odd-extension FFTs (the longest)
     if (fft_smem_bytes<T>(M, 1) > 200 * 1024 || sweep_smem_bytes<T>(*g, M) > 200 * 1024) return IBG_ERR_UNSUPPORTED;
     // dynamic shared memory each kernel may need (static shared memory comes on top)
     tuned_config(sizeof(T), 0, frow.m, g->NI, g->L, rows_P, rows_T, rows_tws);

@@ -29,6 +29,7 @@ struct RowPassArgs {
     const T* base[kMaxLevels];
     T in_scale;                    // multiplies the input (+1 or -1)
     T norm;                        // multiplies the output
+    const T* sinh;                 // sin(pi j / N), the half-length DST's pre-processing
 };
 
 // sine vectors (mode k + 1) of the spectral boundary lifting and the boundary lines
@@ -64,6 +65,7 @@ struct ColPassArgs {
     T alpha;
     const T* edges;                // boundary DSTs of every level (mode 3)
     size_t estride, elstride;      // batch and level strides of edges
+    const T* sinh;                 // sin(pi j / N), the half-length DST's pre-processing
 };
 
 
@@ -82,6 +84,10 @@ struct SweepArgs {
     GridDev g;
     FftDesc frow;                  // length 2 ny
     FftDesc fcol;                  // length 2 nx
+    FftDesc frowh;                 // length ny: the half-length DSTs of k_sweep_lines
+    FftDesc fcolh;                 // length nx
+    const T* sinr;                 // their pre-processing sines
+    const T* sinc;
     const T* buf;                  // this level's forward coefficients (batch item 0)
     size_t bstride;
     const T* cosx;
@@ -175,14 +181,30 @@ int gemm_pass_setup();
 void launch_gemm_pass(GemmPassArgs& a, int batch, cudaStream_t st);
 
 struct FftTables {
+    // length 2 (n + 1): the odd-extension FFTs of the sweep's boundary lines and the edge maps
     FftDesc row64{}, col64{}, row32{}, col32{};
     void* tw_row64 = nullptr;
     void* tw_row32 = nullptr;
     void* tw_col64 = nullptr;
     void* tw_col32 = nullptr;
+    // length n + 1: the half-length DSTs of the FP64 row and column passes, with their
+    // pre-processing sines sin(pi j / (n + 1)), j = 0 .. (n + 1) / 2
+    FftDesc rowh64{}, colh64{};
+    void *tw_rowh64 = nullptr, *tw_colh64 = nullptr;
+    void *sin_row64 = nullptr, *sin_col64 = nullptr;
     int init(int m_rows, int m_cols);
     void release();
 };
+// the pass descriptor and sine table of a precision (rows: pass 0, columns: pass 1): the FP64
+// passes take the half-length DSTs, the FP32 passes the odd-extension ones (elliptic.cu)
+template <typename T>
+inline const FftDesc& pass_desc(const FftTables& t, int pass) {
+    return sizeof(T) == 8 ? (pass == 0 ? t.rowh64 : t.colh64) : (pass == 0 ? t.row32 : t.col32);
+}
+template <typename T>
+inline const T* pass_sines(const FftTables& t, int pass) {
+    return sizeof(T) == 8 ? (const T*)(pass == 0 ? t.sin_row64 : t.sin_col64) : nullptr;
+}
 
 // doubles in one grid's table block: cos x, cos y, 4 x-sine vectors, 4 y-sine vectors
 inline size_t table_doubles(int nx, int ny) { return (size_t)nx + ny + 4 * (size_t)(nx - 1) + 4 * (size_t)(ny - 1); }
@@ -213,6 +235,8 @@ struct CosTables {
 };
 
 bool fft_supported(int m);
+// sin(pi j / N), j = 0 .. N / 2: the half-length DST's pre-processing sines
+void fill_dst_sines(int N, double* out);
 // Scalar::coarsify of a field in place (every level, finest first)
 void coarsify_field(const GridDev& g, double* f, cudaStream_t st);
 // the coarsified overlap interiors of levels 1..L-1 of f into rc (f unchanged)

@@ -29,12 +29,19 @@ constexpr size_t kStaticScratchDoubles = (size_t)1 << 19;
 // one block per grid shape for up to kTableSlots shapes
 constexpr int kStaticMaxM = 4096;
 constexpr int kStaticMaxN = 2048;
-constexpr size_t kStaticTableDoubles = 10 * (size_t)kStaticMaxN;
+// per slot: the row and column twiddles of the sweep's length-2n FFTs, then those
+// of the passes' length-n FFTs
+constexpr size_t kStaticTwiddles = 2 * (size_t)kStaticMaxM + 2 * (size_t)kStaticMaxN;
+// per slot: the grid's cosine and sine tables, then the passes' pre-processing
+// sines of the rows (from kSinRow) and the columns (from kSinCol), n / 2 + 1 each
+constexpr size_t kSinRow = 10 * (size_t)kStaticMaxN;
+constexpr size_t kSinCol = kSinRow + kStaticMaxN / 2 + 8;
+constexpr size_t kStaticTableDoubles = kSinCol + kStaticMaxN / 2 + 8;
 constexpr int kTableSlots = 4;
 
 static __device__ __align__(256) double g_static_scratch[kStaticScratchDoubles];
-static __device__ __align__(256) double2 g_static_twiddles[kTableSlots * 2 * kStaticMaxM];  // per slot: rows, columns
-static __device__ __align__(256) double g_static_cos[kTableSlots * kStaticTableDoubles];     // per slot: cos and sine tables
+static __device__ __align__(256) double2 g_static_twiddles[kTableSlots * kStaticTwiddles];
+static __device__ __align__(256) double g_static_cos[kTableSlots * kStaticTableDoubles];
 
 struct TableSlot {
     int nx = -1, ny = -1;        // shape the slot holds (-1: empty)
@@ -68,19 +75,23 @@ int fail(int code, const std::string& m) {
 // writes the twiddles and grid tables of an nx x ny grid into table slot `k`
 int fill_slot(DeviceSymbols& ds, int k, int nx, int ny, int nxe, int nye, cudaStream_t st) {
     const double pi = 3.14159265358979323846264338327950288;
-    std::vector<double2> tw(2 * (size_t)kStaticMaxM);
-    const int mr = 2 * ny, mc = 2 * nx;
-    for (int j = 0; j < mr; ++j) {
-        const double a = -2.0 * pi * (double)j / (double)mr;
-        tw[j] = make_double2(cos(a), sin(a));
-    }
-    for (int j = 0; j < mc; ++j) {
-        const double a = -2.0 * pi * (double)j / (double)mc;
-        tw[kStaticMaxM + j] = make_double2(cos(a), sin(a));
-    }
+    std::vector<double2> tw(kStaticTwiddles);
+    auto twiddles = [&](int m, size_t at) {
+        for (int j = 0; j < m; ++j) {
+            const double a = -2.0 * pi * (double)j / (double)m;
+            tw[at + j] = make_double2(cos(a), sin(a));
+        }
+    };
+    twiddles(2 * ny, 0);
+    twiddles(2 * nx, kStaticMaxM);
+    twiddles(ny, 2 * (size_t)kStaticMaxM);
+    twiddles(nx, 2 * (size_t)kStaticMaxM + kStaticMaxN);
     std::vector<double> cs;
     fill_grid_tables(nx, ny, nxe, nye, cs);
-    if (cudaMemcpyAsync(ds.twiddles + (size_t)k * 2 * kStaticMaxM, tw.data(), sizeof(double2) * tw.size(),
+    cs.resize(kStaticTableDoubles, 0.0);
+    fill_dst_sines(ny, cs.data() + kSinRow);
+    fill_dst_sines(nx, cs.data() + kSinCol);
+    if (cudaMemcpyAsync(ds.twiddles + (size_t)k * kStaticTwiddles, tw.data(), sizeof(double2) * tw.size(),
                         cudaMemcpyHostToDevice, st) != cudaSuccess ||
         cudaMemcpyAsync(ds.cosines + (size_t)k * kStaticTableDoubles, cs.data(), sizeof(double) * cs.size(),
                         cudaMemcpyHostToDevice, st) != cudaSuccess ||
@@ -109,7 +120,7 @@ extern "C" int ibg_poisson_solve_static(const ibg_grid* grid, const double* f, d
                     "ibg_poisson_solve_static: the grid needs " + std::to_string(need) +
                         " doubles of scratch, more than the 524288-double (4 MiB) static scratch; "
                         "use ibg_poisson_solve");
-    if (!fft_supported(2 * nx) || !fft_supported(2 * ny))
+    if (!fft_supported(2 * nx) || !fft_supported(2 * ny) || !fft_supported(nx) || !fft_supported(ny))
         return fail(IBG_ERR_UNSUPPORTED, "ibg_poisson_solve_static: 2*nx and 2*ny must factor into primes <= 13");
     cudaStream_t st = (cudaStream_t)cuda_stream;
     int dev = 0;
@@ -150,7 +161,7 @@ extern "C" int ibg_poisson_solve_static(const ibg_grid* grid, const double* f, d
         ds.slot[k].ny = ny;
     }
     ds.slot[k].used = ++ds.clock;
-    double2* twid = ds.twiddles + (size_t)k * 2 * kStaticMaxM;
+    double2* twid = ds.twiddles + (size_t)k * kStaticTwiddles;
     double* cosines = ds.cosines + (size_t)k * kStaticTableDoubles;
 
     GridDev g{};
@@ -168,11 +179,17 @@ extern "C" int ibg_poisson_solve_static(const ibg_grid* grid, const double* f, d
     g.x0 = grid->xoffset;
     g.y0 = grid->yoffset;
 
-    FftTables tables;  // descriptors only; the twiddles live in g_static_twiddles
+    FftTables tables;  // descriptors only; twiddles and sines live in the static arrays
     fft_describe(2 * ny, tables.row64);
     fft_describe(2 * nx, tables.col64);
+    fft_describe(ny, tables.rowh64);
+    fft_describe(nx, tables.colh64);
     tables.row64.tw = twid;
     tables.col64.tw = twid + kStaticMaxM;
+    tables.rowh64.tw = twid + 2 * kStaticMaxM;
+    tables.colh64.tw = twid + 2 * kStaticMaxM + kStaticMaxN;
+    tables.sin_row64 = cosines + kSinRow;
+    tables.sin_col64 = cosines + kSinCol;
     CosTables ct;  // views into g_static_cos; owns nothing
     ct.attach(nx, ny, cosines, nullptr);
     EllipticPlan<double> plan;
