@@ -749,6 +749,7 @@ struct ibg_context {
             Nk = B.Nbuf[k];
             Np = B.Nbuf[(k + sch.nsub - 1) % sch.nsub];
         }
+        bool curl_fused = false;  // the curl of the nonlinear term runs inside the right-hand side's launch
         if constexpr (std::is_same<T, double>::value) {
             if (nmode == 1) {
                 launch_nonlinear_lin(g, B.q, B.w, d_base_q, d_base_w, period, d_ts0, d_hist_count, B.U, B.V, B.C,
@@ -762,8 +763,11 @@ struct ibg_context {
                 launch_nonlinear<T>(g, B.q, d_base_w, B.U, B.V, B.C, Nk, 1, S, F, st);
                 launch_sub(S, B.ws, Nk, Nk, st);
                 launches += 3 + g.L;
-            } else {
+            } else if (nmode == 2) {
                 launch_nonlinear<T>(g, B.q, B.w, B.U, B.V, B.C, Nk, 1, S, F, st);
+            } else {
+                launch_nonlinear_flux<T>(g, B.q, B.w, B.U, B.V, B.C, 1, S, F, st);
+                curl_fused = true;
             }
             if (nmode == 2) {
                 launch_sfd(S, B.w, d_what, d_rprev, Nk, sfd_chi, sfd_Delta, an, bn, prm.dt, !sfd_rhs_saved, st);
@@ -771,15 +775,19 @@ struct ibg_context {
                 launches += 1;
             }
         } else {
-            launch_nonlinear<T>(g, B.q, B.w, B.U, B.V, B.C, Nk, 1, S, F, st);
+            launch_nonlinear_flux<T>(g, B.q, B.w, B.U, B.V, B.C, 1, S, F, st);
+            curl_fused = true;
         }
-        launches += 2 + g.L;
+        launches += 1 + g.L + (curl_fused ? 0 : 1);
         if (ubf) frame_flow(cn * prm.dt);
         if (moving) move_bodies(cn * prm.dt, k);
         const T* Nprev = nullptr;
         if (bn != 0) Nprev = old_saved ? Np : Nk;
         const double c1 = 0.5 * (1.0 / prm.Re) * (an + bn);
-        launch_rhs<T>(g, B.w, Nk, Nprev, B.a, c1, an, bn, prm.dt, st);
+        if (curl_fused)
+            launch_curl_rhs<T>(g, B.C, Nk, B.w, Nprev, B.a, c1, an, bn, prm.dt, st);
+        else
+            launch_rhs<T>(g, B.w, Nk, Nprev, B.a, c1, an, bn, prm.dt, st);
         launches += 1;
         int s = projection<T>(B, k, B.a, d_b);
         if (s) return s;

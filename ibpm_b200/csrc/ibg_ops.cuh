@@ -45,6 +45,14 @@ void launch_nonlinear(const GridDev& g, const T* q, const T* w, T* U, T* V, T* C
                       size_t fstride, cudaStream_t st);
 template <typename T>
 void launch_curl_flux(const GridDev& g, const T* C, T* N, cudaStream_t st);
+// the nonlinear term without its curl (node velocities, cross-product fluxes of every level) ...
+template <typename T>
+void launch_nonlinear_flux(const GridDev& g, const T* q, const T* w, T* U, T* V, T* C, int batch, size_t sstride,
+                           size_t fstride, cudaStream_t st);
+// ... and the curl fused with the right-hand side: N = Curl(C), a = launch_rhs's a
+template <typename T>
+void launch_curl_rhs(const GridDev& g, const T* C, T* N, const T* w, const T* Nprev, T* a, double c1, double an,
+                     double bn, double dt, cudaStream_t st);
 template <typename T>
 void launch_rhs(const GridDev& g, const T* w, const T* N, const T* Nprev, T* a, double c1, double an, double bn,
                 double dt, cudaStream_t st);

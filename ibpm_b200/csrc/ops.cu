@@ -338,6 +338,37 @@ __global__ void k_rhs(GridDev g, const T* __restrict__ w, const T* __restrict__ 
     a[tid] = v + p;
 }
 
+// k_curl_flux and k_rhs of one sub-step in one launch: N = Curl(C) is stored (the next sub-step's
+// N_prev) and used at once.  The same operations in the same order as the two kernels, so the same
+// results.  Nprev may be N itself (the first step of a multistep scheme).
+template <typename T>
+__global__ void k_curl_rhs(GridDev g, const T* __restrict__ C, T* N, const T* __restrict__ w, const T* Nprev,
+                           T* __restrict__ a, T c1, T an, T bn, T dt) {
+    pdl_enter();
+    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= (size_t)g.L * g.N1) return;
+    const int lev = (int)(tid / g.N1);
+    const int r = (int)(tid % g.N1);
+    const int i = r / g.NJ + 1, j = r % g.NJ + 1;
+    const double dxl = lev_dx(g, lev);
+    const T bydx2 = (T)(1. / (dxl * dxl));
+    const T* ql = C + (size_t)lev * g.F1;
+    const T nv = (qy_at(ql, g, i, j) - qy_at(ql, g, i - 1, j) + qx_at(ql, g, i, j - 1) - qx_at(ql, g, i, j)) * bydx2;
+    N[tid] = nv;
+    const T* f = w + (size_t)lev * g.N1;
+    const T* c = (lev < g.L - 1) ? w + (size_t)(lev + 1) * g.N1 : nullptr;
+    const T p = node(f, g, i, j);
+    const T pe = node_bc(f, c, g, i + 1, j), pw = node_bc(f, c, g, i - 1, j);
+    const T pn = node_bc(f, c, g, i, j + 1), ps = node_bc(f, c, g, i, j - 1);
+    const T qy_ij = p - pe, qy_im = pw - p, qx_jm = p - ps, qx_ij = pn - p;
+    const T lap = ((qy_ij - qy_im + qx_jm - qx_ij) * bydx2) * (T)-1;
+    T v = lap * c1;
+    v = v + an * nv;
+    if (Nprev) v = v + bn * (Nprev == N ? nv : Nprev[tid]);
+    v = v * dt;
+    a[tid] = v + p;
+}
+
 // Curl of a Scalar (with boundary values from the next coarser level) at a
 // flux index of level lev.
 template <typename T>
@@ -819,13 +850,27 @@ __global__ void k_bf(GridDev g, const double* __restrict__ flux0, size_t fstride
 static inline unsigned nblk(size_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 template <typename T>
-void launch_nonlinear(const GridDev& g, const T* q, const T* w, T* U, T* V, T* C, T* N, int batch, size_t sstride,
-                      size_t fstride, cudaStream_t st) {
+void launch_nonlinear_flux(const GridDev& g, const T* q, const T* w, T* U, T* V, T* C, int batch, size_t sstride,
+                           size_t fstride, cudaStream_t st) {
     const size_t S = (size_t)g.L * g.N1;
     launch_k(k_node_vel<T>, dim3(nblk(S, 256), batch), 256, 0, st, g, q, w, U, V, sstride, fstride);
     for (int lev = 0; lev < g.L; ++lev)
         launch_k(k_cross_flux<T>, dim3(nblk(g.F1, 256), batch), 256, 0, st, g, lev, U, V, C, sstride, fstride);
+}
+
+template <typename T>
+void launch_nonlinear(const GridDev& g, const T* q, const T* w, T* U, T* V, T* C, T* N, int batch, size_t sstride,
+                      size_t fstride, cudaStream_t st) {
+    const size_t S = (size_t)g.L * g.N1;
+    launch_nonlinear_flux<T>(g, q, w, U, V, C, batch, sstride, fstride, st);
     launch_k(k_curl_flux<T>, dim3(nblk(S, 256), batch), 256, 0, st, g, C, N, sstride, fstride);
+}
+
+template <typename T>
+void launch_curl_rhs(const GridDev& g, const T* C, T* N, const T* w, const T* Nprev, T* a, double c1, double an,
+                     double bn, double dt, cudaStream_t st) {
+    const size_t S = (size_t)g.L * g.N1;
+    launch_k(k_curl_rhs<T>, nblk(S, 256), 256, 0, st, g, C, N, w, Nprev, a, (T)c1, (T)an, (T)bn, (T)dt);
 }
 
 void launch_nonlinear_lin(const GridDev& g, const double* q, const double* w, const double* qb, const double* wb,
@@ -969,6 +1014,10 @@ void launch_smear_bf_unit(const GridDev& g, int ncomp, int col0, int batch, cons
     template void launch_nonlinear<T>(const GridDev&, const T*, const T*, T*, T*, T*, T*, int, size_t, size_t, \
                                       cudaStream_t);                                                           \
     template void launch_curl_flux<T>(const GridDev&, const T*, T*, cudaStream_t);                             \
+    template void launch_nonlinear_flux<T>(const GridDev&, const T*, const T*, T*, T*, T*, int, size_t, size_t, \
+                                           cudaStream_t);                                                      \
+    template void launch_curl_rhs<T>(const GridDev&, const T*, T*, const T*, const T*, T*, double, double,     \
+                                     double, double, cudaStream_t);                                            \
     template void launch_rhs<T>(const GridDev&, const T*, const T*, const T*, T*, double, double, double,      \
                                 double, cudaStream_t);                                                         \
     template void launch_laplacian<T>(const GridDev&, const T*, T*, cudaStream_t);                             \
