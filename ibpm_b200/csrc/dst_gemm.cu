@@ -16,11 +16,16 @@
 // dropped A_lo B_lo term is ~2^-22 relative).
 //
 // One CTA computes a 128 x NT tile of one level (NT <= 256 output columns,
-// a multiple of 16), looping over K in chunks of 32 with two shared-memory
-// stages: all 256 threads stage chunk c + 1 (global loads, the mode's
-// transform, the hi/lo split, the no-swizzle K-major core-matrix layout) while
-// the MMAs of chunk c run; one thread issues 12 tcgen05.mma per chunk (4 K-steps
-// of 8, 3 products each) and commits them to the stage's mbarrier.  The
+// a multiple of 32), looping over K in chunks of 32 with two shared-memory
+// stages.  All 256 threads hold the next chunk's operands in registers (its
+// global loads are issued before the current chunk's MMAs), store them as
+// float4s in the no-swizzle K-major core-matrix layout (each warp's stores fill
+// 512 contiguous bytes, so no bank conflicts), and split the data operand into
+// hi and lo in place, one item at a time; one thread issues 12 tcgen05.mma per
+// chunk (4 K-steps of 8, 3 products each) and commits them to the stage's
+// mbarrier.  Each mode is its own instantiation, so a kernel carries only its
+// mode's code (the first version, one kernel for all modes with every staging
+// loop unrolled, spent most of its time waiting for instruction fetches).  The
 // epilogue reads the accumulator (tcgen05.ld), stages it through shared memory
 // and stores it coalesced.  Every mbarrier wait is bounded: a wait that runs out
 // sets *err and the CTA frees its tensor memory and returns.
@@ -96,33 +101,46 @@ __device__ __forceinline__ bool in_overlap(const GridDev& g, int i, int j) {
 }
 }  // namespace
 
+// Operand staging.  A K-major operand tile of R rows x 32 K values is cut into items of 8 rows x 16 K;
+// in an item, lane l takes row 8 rg + (l & 7) and the four K values 16 kh + 4 (l >> 3) .. + 3, so a
+// warp's float4 stores fill four consecutive core matrices (512 contiguous bytes, no bank conflict)
+// and its global reads of a row-major operand cover 8 rows x 64 bytes (or, for the transposed T,
+// 4 rows of T x 32 bytes).
+constexpr int kAItems = (kM / 8) * 2;  // 32 items: 4 per warp
+
+__device__ __forceinline__ void item_pos(int item, int lane, int& r, int& k) {
+    r = 8 * (item >> 1) + (lane & 7);
+    k = 16 * (item & 1) + 4 * (lane >> 3);
+}
+
+template <int MODE>
 __global__ void __launch_bounds__(kThreads, 1) k_dst_gemm(GemmPassArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
     pdl_enter();
+    constexpr bool ROWS = MODE <= 1;
+    constexpr int kBmaxPer = 256 / 32;  // B items per warp at NT = 256
     const GridDev& g = a.g;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int NT = a.n_tile;
-    const bool rows = a.mode <= 1;
-    const int Mdim = g.NI, Ndim = g.NJ, Kdim = rows ? g.NJ : g.NI;
+    const int NT = a.n_tile;  // a multiple of 32
+    const int Mdim = g.NI, Ndim = g.NJ, Kdim = ROWS ? g.NJ : g.NI;
     const int b = blockIdx.z / a.nlev, lev = blockIdx.z % a.nlev;
     const int m0 = blockIdx.x * kM, n0 = blockIdx.y * NT;
     const int nchunks = (Kdim + kKc - 1) / kKc;
     const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem);
     const uint32_t bar0 = sbase + kOffBar, bar1 = bar0 + 8, tslot = sbase + kOffTmem;
     const uint32_t Bbytes = (uint32_t)NT * kKc * 4;
+    const int bper = NT / 32;  // B items per warp
 
-    // operands of this CTA
-    const float* X = nullptr;    // rows passes: the level's data (A)
+    const float* X = nullptr;  // rows passes: the level's data (A)
     const float* Xalt = nullptr;
-    const float* T = nullptr;    // columns passes: the level's coefficients (B = T^T)
+    const float* T = nullptr;  // columns passes: the level's coefficients (B = T^T)
     const float* edges = nullptr;
-    if (rows) {
+    if (ROWS) {
         X = a.in[lev] + (size_t)b * a.in_bstride;
         Xalt = a.alt[lev] ? a.alt[lev] + (size_t)b * a.in_bstride : nullptr;
     } else {
         T = a.src + (size_t)b * a.bstride + (size_t)lev * a.lstride;
-        if (a.mode == 3 && a.edges && lev < a.nlev - 1)
-            edges = a.edges + (size_t)b * a.estride + (size_t)lev * a.elstride;
+        if (MODE == 3 && a.edges && lev < a.nlev - 1) edges = a.edges + (size_t)b * a.estride + (size_t)lev * a.elstride;
     }
     const float bydx2 = a.bydx2[lev], bcc = a.bc_coef[lev];
 
@@ -143,111 +161,138 @@ __global__ void __launch_bounds__(kThreads, 1) k_dst_gemm(GemmPassArgs a) {
     const uint32_t tmem = *(volatile uint32_t*)(smem + kOffTmem);
     const uint32_t idesc = idesc_tf32(NT);
 
-    // stage chunk c into shared-memory stage st
-    // stage chunk c into shared-memory stage st.  Each thread first issues all of its global loads
-    // for the chunk (held in registers), then converts and stores, so the loads are in flight together.
-    auto stage_chunk = [&](int c, int st) {
+    // registers of the next chunk: the data operand (raw) and the sine operand (hi, lo)
+    float dv[kBmaxPer > 4 ? kBmaxPer * 4 : 16];       // rows: A data (4 items); columns: B data (bper items)
+    float sh[kBmaxPer * 4], sl[kBmaxPer * 4];           // rows: B = S_y (bper items); columns: A = S_x (4 items)
+    auto load = [&](int c) {
+        const int k0 = c * kKc;
+        if (ROWS) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                int r, k;
+                item_pos(warp * 4 + q, lane, r, k);
+                const int gr = m0 + r;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int gk = k0 + k + j;
+                    float v = 0.f;
+                    if (gr < Mdim && gk < Kdim) {
+                        const float* src = (Xalt && in_overlap(g, gr + 1, gk + 1)) ? Xalt : X;
+                        v = src[(size_t)gr * Ndim + gk];
+                    }
+                    dv[4 * q + j] = v;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kBmaxPer; ++q) {
+                if (q >= bper) break;
+                int r, k;
+                item_pos(warp * bper + q, lane, r, k);
+                const int gn = n0 + r;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int gk = k0 + k + j;
+                    const bool in = gn < Ndim && gk < Kdim;
+                    sh[4 * q + j] = in ? a.s_hi[(size_t)gn * Kdim + gk] : 0.f;
+                    sl[4 * q + j] = in ? a.s_lo[(size_t)gn * Kdim + gk] : 0.f;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                int r, k;
+                item_pos(warp * 4 + q, lane, r, k);
+                const int gr = m0 + r;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int gk = k0 + k + j;
+                    const bool in = gr < Mdim && gk < Kdim;
+                    sh[4 * q + j] = in ? a.s_hi[(size_t)gr * Kdim + gk] : 0.f;
+                    sl[4 * q + j] = in ? a.s_lo[(size_t)gr * Kdim + gk] : 0.f;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kBmaxPer; ++q) {
+                if (q >= bper) break;
+                int r, k;
+                item_pos(warp * bper + q, lane, r, k);
+                const int gn = n0 + r;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int gk = k0 + k + j;
+                    dv[4 * q + j] = (gn < Ndim && gk < Kdim) ? T[(size_t)gk * Ndim + gn] : 0.f;
+                }
+            }
+        }
+    };
+    // registers -> stage st: the sine operand as loaded, the data operand raw into its hi area, then
+    // (one item at a time, not unrolled) scaled / lifted and split into hi and lo in place
+    auto store = [&](int c, int st) {
         unsigned char* S0 = smem + (size_t)st * kStage;
         unsigned char* Ahi = S0;
         unsigned char* Alo = S0 + kAbytes;
         unsigned char* Bhi = S0 + 2 * kAbytes;
         unsigned char* Blo = Bhi + Bbytes;
+        unsigned char* Dhi = ROWS ? Ahi : Bhi;  // the data operand
+        unsigned char* Dlo = ROWS ? Alo : Blo;
+        unsigned char* Shi = ROWS ? Bhi : Ahi;  // the sine operand
+        unsigned char* Slo = ROWS ? Blo : Alo;
+        const int nd = ROWS ? 4 : bper, ns = ROWS ? bper : 4;
+        const int dbase = ROWS ? warp * 4 : warp * bper, sbase_ = ROWS ? warp * bper : warp * 4;
+#pragma unroll
+        for (int q = 0; q < kBmaxPer; ++q) {
+            if (q >= ns) break;
+            int r, k;
+            item_pos(sbase_ + q, lane, r, k);
+            *(float4*)(Shi + core32(r, k)) = make_float4(sh[4 * q], sh[4 * q + 1], sh[4 * q + 2], sh[4 * q + 3]);
+            *(float4*)(Slo + core32(r, k)) = make_float4(sl[4 * q], sl[4 * q + 1], sl[4 * q + 2], sl[4 * q + 3]);
+        }
+#pragma unroll
+        for (int q = 0; q < kBmaxPer; ++q) {
+            if (q >= nd) break;
+            int r, k;
+            item_pos(dbase + q, lane, r, k);
+            *(float4*)(Dhi + core32(r, k)) = make_float4(dv[4 * q], dv[4 * q + 1], dv[4 * q + 2], dv[4 * q + 3]);
+        }
         const int k0 = c * kKc;
-        // A: 128 rows x 32 K, 16 elements per thread
-        constexpr int kAper = kM * kKc / kThreads;
-        float av[kAper], al[kAper];
+#pragma unroll 1
+        for (int q = 0; q < nd; ++q) {
+            int r, k;
+            item_pos(dbase + q, lane, r, k);
+            float4 v = *(float4*)(Dhi + core32(r, k));
+            float e[4] = {v.x, v.y, v.z, v.w}, hi[4], lo[4];
 #pragma unroll
-        for (int u = 0; u < kAper; ++u) {
-            const int e = tid + u * kThreads;
-            const int r = e >> 5, kk = e & 31;
-            const int gr = m0 + r, gk = k0 + kk;
-            av[u] = 0.f;
-            al[u] = 0.f;
-            if (gr < Mdim && gk < Kdim) {
-                if (rows) {
-                    const float* src = (Xalt && in_overlap(g, gr + 1, gk + 1)) ? Xalt : X;
-                    av[u] = src[(size_t)gr * Ndim + gk];
-                } else {
-                    av[u] = a.s_hi[(size_t)gr * Kdim + gk];
-                    al[u] = a.s_lo[(size_t)gr * Kdim + gk];
+            for (int j = 0; j < 4; ++j) {
+                float x = e[j];
+                if (ROWS) {
+                    x = a.in_scale * x;
+                } else if (MODE == 3) {
+                    const int gn = n0 + r, gk = k0 + k + j;
+                    if (gn < Ndim && gk < Kdim)
+                        x = lifted_coef(x, gk, gn, edges, Mdim, Ndim, bcc, a.s, a.cosx, a.cosy, bydx2, a.helmholtz,
+                                        a.alpha);
                 }
+                hi[j] = tf32_rna(x);
+                lo[j] = tf32_rna(x - hi[j]);
             }
-        }
-#pragma unroll
-        for (int u = 0; u < kAper; ++u) {
-            const int e = tid + u * kThreads;
-            float hi = av[u], lo = al[u];
-            if (rows) {
-                const float v = a.in_scale * av[u];
-                hi = tf32_rna(v);
-                lo = tf32_rna(v - hi);
-            }
-            const uint32_t off = core32(e >> 5, e & 31);
-            *(float*)(Ahi + off) = hi;
-            *(float*)(Alo + off) = lo;
-        }
-        // B: NT rows (output columns n) x 32 K, up to 32 elements per thread
-        constexpr int kBper = kBbytesMax / 4 / kThreads;
-        const int nB = NT * kKc;
-        float bv[kBper], bl[kBper];
-#pragma unroll
-        for (int u = 0; u < kBper; ++u) {
-            const int e = tid + u * kThreads;
-            bv[u] = 0.f;
-            bl[u] = 0.f;
-            if (e < nB) {
-                int n, kk;
-                if (rows) {
-                    n = e >> 5;
-                    kk = e & 31;
-                } else {
-                    kk = e / NT;  // consecutive threads read consecutive columns of one row of T
-                    n = e - kk * NT;
-                }
-                const int gn = n0 + n, gk = k0 + kk;
-                if (gn < Ndim && gk < Kdim) {
-                    if (rows) {
-                        bv[u] = a.s_hi[(size_t)gn * Kdim + gk];
-                        bl[u] = a.s_lo[(size_t)gn * Kdim + gk];
-                    } else {
-                        bv[u] = T[(size_t)gk * Ndim + gn];
-                    }
-                }
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < kBper; ++u) {
-            const int e = tid + u * kThreads;
-            if (e >= nB) break;
-            int n, kk;
-            if (rows) {
-                n = e >> 5;
-                kk = e & 31;
-            } else {
-                kk = e / NT;
-                n = e - kk * NT;
-            }
-            float hi = bv[u], lo = bl[u];
-            if (!rows) {
-                const int gn = n0 + n, gk = k0 + kk;
-                float v = bv[u];
-                if (a.mode == 3 && gn < Ndim && gk < Kdim)
-                    v = lifted_coef(v, gk, gn, edges, Mdim, Ndim, bcc, a.s, a.cosx, a.cosy, bydx2, a.helmholtz,
-                                    a.alpha);
-                hi = tf32_rna(v);
-                lo = tf32_rna(v - hi);
-            }
-            const uint32_t off = core32(n, kk);
-            *(float*)(Bhi + off) = hi;
-            *(float*)(Blo + off) = lo;
+            *(float4*)(Dhi + core32(r, k)) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+            *(float4*)(Dlo + core32(r, k)) = make_float4(lo[0], lo[1], lo[2], lo[3]);
         }
     };
 
     bool ok = true;
     uint32_t ph[2] = {0u, 0u};
-    stage_chunk(0, 0);
+    load(0);
     for (int c = 0; c < nchunks; ++c) {
         const int st = c & 1;
+        if (c >= 2) {
+            // the MMAs of chunk c - 2 read this stage: wait for them before overwriting it
+            ok = wait_bounded(st ? bar1 : bar0, ph[st]);
+            ph[st] ^= 1u;
+            if (__syncthreads_or(!ok)) break;
+        }
+        store(c, st);
+        if (c + 1 < nchunks) load(c + 1);  // in flight while this chunk is issued
         // make this stage's generic-proxy writes visible to the tensor cores, then issue
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -275,19 +320,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_dst_gemm(GemmPassArgs a) {
                              st ? bar1 : bar0)
                          : "memory");
         }
-        if (c + 1 < nchunks) {
-            const int nst = (c + 1) & 1;
-            if (c >= 1) {
-                // the MMAs of chunk c - 1 read stage nst: wait for them before overwriting it
-                ok = wait_bounded(nst ? bar1 : bar0, ph[nst]);
-                ph[nst] ^= 1u;
-            }
-            if (__syncthreads_or(!ok)) break;
-            stage_chunk(c + 1, nst);
-        }
     }
     if (ok) {
-        // the last chunk's MMAs complete the accumulator (and every earlier one, in issue order)
+        // the last chunk's MMAs complete the accumulator (and every earlier one, in issue order);
+        // the other stage's last commit is waited for too, so that no arrival is left pending
         const int lst = (nchunks - 1) & 1;
         ok = wait_bounded(lst ? bar1 : bar0, ph[lst]);
         if (nchunks >= 2) {
@@ -320,8 +356,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_dst_gemm(GemmPassArgs a) {
                 : "memory");
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-            for (int e = 0; e < 32; ++e)
-                if (c0 + e < NT) Dt[row * ld + c0 + e] = __uint_as_float(r[e]);
+            for (int e = 0; e < 32; ++e) Dt[row * ld + c0 + e] = __uint_as_float(r[e]);
         }
         __syncthreads();
         const int ncols = min(NT, Ndim - n0);
@@ -331,9 +366,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_dst_gemm(GemmPassArgs a) {
             if (cc >= ncols) continue;
             const size_t gi = (size_t)(m0 + rr) * Ndim + (n0 + cc);
             const float v = Dt[rr * ld + cc];
-            if (a.mode == 0) {
+            if (MODE == 0) {
                 a.out[lev][(size_t)b * a.out_bstride + gi] = v;
-            } else if (a.mode == 1) {
+            } else if (MODE == 1) {
                 const float u = v * a.norm;
                 a.out[lev][(size_t)b * a.out_bstride + gi] = u;
                 if (a.out2[lev]) a.out2[lev][(size_t)b * a.out_bstride + gi] = a.base[lev][(size_t)b * a.out_bstride + gi] - u;
@@ -404,8 +439,11 @@ void SineMats::release() {
 int gemm_pass_setup() {
     static bool done = false;
     if (done) return IBG_OK;
-    if (cudaFuncSetAttribute(k_dst_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem) != cudaSuccess)
-        return IBG_ERR_CUDA;
+    const void* fns[4] = {(const void*)k_dst_gemm<0>, (const void*)k_dst_gemm<1>, (const void*)k_dst_gemm<2>,
+                          (const void*)k_dst_gemm<3>};
+    for (const void* f : fns)
+        if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem) != cudaSuccess)
+            return IBG_ERR_CUDA;
     done = true;
     return IBG_OK;
 }
@@ -413,13 +451,19 @@ int gemm_pass_setup() {
 void launch_gemm_pass(GemmPassArgs& a, int batch, cudaStream_t st) {
     const GridDev& g = a.g;
     const int N = g.NJ;
-    // at least four column tiles per level, so that small levels still spread over several SMs
-    int nt = (((N + 3) / 4) + 15) / 16 * 16;
+    // at least four column tiles per level, so that small levels still spread over several SMs;
+    // a multiple of 32 (whole staging items per warp), at most 256 (one MMA)
+    int nt = (((N + 3) / 4) + 31) / 32 * 32;
     nt = nt < 32 ? 32 : nt > 256 ? 256 : nt;
     a.n_tile = nt;
     a.tmem_cols = nt <= 32 ? 32 : nt <= 64 ? 64 : nt <= 128 ? 128 : 256;
     const dim3 grid((unsigned)((g.NI + kM - 1) / kM), (unsigned)((N + nt - 1) / nt), (unsigned)(a.nlev * batch));
-    launch_k(k_dst_gemm, grid, kThreads, (size_t)kSmem, st, a);
+    switch (a.mode) {
+        case 0: launch_k(k_dst_gemm<0>, grid, kThreads, (size_t)kSmem, st, a); break;
+        case 1: launch_k(k_dst_gemm<1>, grid, kThreads, (size_t)kSmem, st, a); break;
+        case 2: launch_k(k_dst_gemm<2>, grid, kThreads, (size_t)kSmem, st, a); break;
+        default: launch_k(k_dst_gemm<3>, grid, kThreads, (size_t)kSmem, st, a); break;
+    }
 }
 
 }  // namespace ibg

@@ -323,44 +323,65 @@ __device__ __forceinline__ void dst_pre(T fj, T fNj, T s, T& yj, T& yNj) {
     yNj = sum - dif;
 }
 
-// O[p][k] = (DST(a)_k, DST(b)_k), k < N - 1, from the half-length FFTs Z of P line pairs (length N each)
+// O[p][k] = (DST(a)_k, DST(b)_k), k < N - 1, from the half-length FFTs Z of P line pairs (length N each,
+// P <= 4, N <= 2048).  The prefix sums over the even outputs run on every warp: segments of 32 terms
+// are scanned with shuffles, then each pair's segment totals (at most 32) by one warp, then the
+// offsets are added.
 template <typename C>
 __device__ void dst_post(const C* __restrict__ Z, C* __restrict__ O, int N, int P) {
     using T = decltype(C::x);
+    __shared__ C seg_tot[4 * 32];
     const int half = N / 2, kh = (N + 1) / 2;  // odd N needs S_k up to k = (N - 1) / 2
-    for (int t = threadIdx.x; t < P * kh; t += blockDim.x) {
-        const int p = t / kh, k = t - p * kh;
-        const C zk = Z[p * N + k], zn = Z[p * N + (k == 0 ? 0 : N - k)];
-        const T ca = (T)0.5 * (zk.x + zn.x), cb = (T)0.5 * (zk.y + zn.y);
-        C* o = O + p * N;
-        o[2 * k] = k == 0 ? cmk<C>(ca, cb) : cmk<C>((T)2 * ca, (T)2 * cb);  // prefix-sum terms
-        if (k >= 1) o[2 * k - 1] = cmk<C>(zn.y - zk.y, zk.x - zn.x);      // 2 S_k of a and b
+    const int nseg = (kh + 31) / 32;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    for (int u = warp; u < P * nseg; u += nwarps) {
+        const int p = u / nseg, k = 32 * (u - p * nseg) + lane;
+        C v = cmk<C>((T)0, (T)0);
+        if (k < kh) {
+            const C zk = Z[p * N + k], zn = Z[p * N + (k == 0 ? 0 : N - k)];
+            const T ca = (T)0.5 * (zk.x + zn.x), cb = (T)0.5 * (zk.y + zn.y);
+            if (k >= 1) O[p * N + 2 * k - 1] = cmk<C>(zn.y - zk.y, zk.x - zn.x);  // 2 S_k of a and b
+            if (k < half) v = k == 0 ? cmk<C>(ca, cb) : cmk<C>((T)2 * ca, (T)2 * cb);  // prefix-sum terms
+        }
+#pragma unroll
+        for (int dd = 1; dd < 32; dd <<= 1) {
+            const T ua = __shfl_up_sync(0xffffffffu, v.x, dd), ub = __shfl_up_sync(0xffffffffu, v.y, dd);
+            if (lane >= dd) {
+                v.x += ua;
+                v.y += ub;
+            }
+        }
+        if (k < half) O[p * N + 2 * k] = v;
+        if (lane == 31) seg_tot[p * 32 + (u - p * nseg)] = v;
     }
     __syncthreads();
-    // inclusive prefix sums over the even entries, one warp per line pair, 32 terms at a time
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-    for (int p = warp; p < P; p += nwarps) {
-        C* o = O + p * N;
-        T ca = (T)0, cb = (T)0;
-        for (int c0 = 0; c0 < half; c0 += 32) {
-            const int mi = c0 + lane;
-            C v = mi < half ? o[2 * mi] : cmk<C>((T)0, (T)0);
+    if (nseg > 1) {
+        // exclusive prefix of each pair's segment totals
+        for (int p = warp; p < P; p += nwarps) {
+            C t = lane < nseg ? seg_tot[p * 32 + lane] : cmk<C>((T)0, (T)0);
 #pragma unroll
             for (int dd = 1; dd < 32; dd <<= 1) {
-                const T ua = __shfl_up_sync(0xffffffffu, v.x, dd), ub = __shfl_up_sync(0xffffffffu, v.y, dd);
+                const T ua = __shfl_up_sync(0xffffffffu, t.x, dd), ub = __shfl_up_sync(0xffffffffu, t.y, dd);
                 if (lane >= dd) {
-                    v.x += ua;
-                    v.y += ub;
+                    t.x += ua;
+                    t.y += ub;
                 }
             }
-            v.x += ca;
-            v.y += cb;
-            if (mi < half) o[2 * mi] = v;
-            ca = __shfl_sync(0xffffffffu, v.x, 31);
-            cb = __shfl_sync(0xffffffffu, v.y, 31);
+            // exclusive: the inclusive sum of the lane before
+            const T ex = __shfl_up_sync(0xffffffffu, t.x, 1), ey = __shfl_up_sync(0xffffffffu, t.y, 1);
+            if (lane < nseg) seg_tot[p * 32 + lane] = lane == 0 ? cmk<C>((T)0, (T)0) : cmk<C>(ex, ey);
         }
+        __syncthreads();
+        for (int t = threadIdx.x; t < P * half; t += blockDim.x) {
+            const int p = t / half, k = t - p * half;
+            if (k < 32) continue;
+            const C off = seg_tot[p * 32 + (k >> 5)];
+            C& o = O[p * N + 2 * k];
+            o.x += off.x;
+            o.y += off.y;
+        }
+        __syncthreads();
     }
-    __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
