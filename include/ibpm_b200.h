@@ -361,8 +361,8 @@ IBG_API int ibg_projection_solve(ibg_context* ctx, int substep, const double* a,
  * and allocates nothing.  Its memory is file-scope device arrays, held by every
  * GPU that loads the library until the process exits: 4 MiB of scratch
  * (524288 doubles; a solve needs 2*ngrid*(nx-1)*(ny-1) + 2*(ngrid+1)*(nx+ny-2)
- * of them) and about 1.1 MiB of tables, room for the FFT twiddles and
- * eigenvalue/sine tables of 4 grid shapes (288 KiB each).
+ * of them) and about 1.5 MiB of tables, room for the FFT twiddles and
+ * eigenvalue/sine tables of 4 grid shapes (368 KiB each).
  * Limits: nx, ny <= 2048; the scratch need above <= 524288; the transform
  * kernels' shared memory 64*max(nx,ny) + 48*max(nx-1,ny-1) bytes <= 200 KiB
  * (max(nx, ny) <= 1828).  Other grids are rejected with IBG_ERR_UNSUPPORTED and
