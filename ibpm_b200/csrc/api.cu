@@ -261,6 +261,7 @@ struct ibg_context {
     // work
     int nring = 0;
     double *flux0 = nullptr, *rhsb = nullptr, *btmp = nullptr;
+    int* d_sweep_cnt = nullptr;  // the fused sweep's two counters (EllipticPlan::sweep_counters)
     // Cholesky factors per sub-step
     double* Lr[4] = {nullptr, nullptr, nullptr, nullptr};
     double* Lc[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -351,6 +352,7 @@ struct ibg_context {
                 alloc(&B.sweep, sweep_doubles(g.nx, g.ny, g.L)) || alloc(&B.U, S) || alloc(&B.V, S) ||
                 alloc(&B.C, F) || alloc(&B.Bf, S) || alloc(&B.qtmp, F);
         for (int k = 0; k < nring && !s; ++k) s = alloc(&B.Nbuf[k], S);
+        if (!s && !d_sweep_cnt) s = alloc(&d_sweep_cnt, 2);
         if (!s && std::is_same<T, float>::value) {
             // the sine-matrix GEMM form of the FP32 DST passes (chosen per grid, see set_dst_gemm)
             s = alloc(&B.tbuf2, S) || sines.init(g.nx, g.ny) || gemm_pass_setup();
@@ -365,6 +367,9 @@ struct ibg_context {
             s = B.helm[k].init(&g, &fft, true, alpha, cosT);
         }
         if (s) return s;
+        // every solve of this context runs on its stream, one after another: one pair of counters
+        B.poisson.sweep_counters = d_sweep_cnt;
+        for (int k = 0; k < 4; ++k) B.helm[k].sweep_counters = d_sweep_cnt;
         if constexpr (std::is_same<T, float>::value) {
             B.poisson.sines = &sines;
             for (int k = 0; k < 4; ++k) B.helm[k].sines = &sines;
@@ -464,7 +469,8 @@ struct ibg_context {
         d_ext = nullptr;
         void* ptrs[] = {d_ref, d_pts, d_vel, d_body_of, d_bodies, d_mstate, d_mstate_keep, d_mtab, d_bf, d_bf_state, d_bfv, d_q0,
                         slots.idx, slots.w, slots.n, slots.own, slots.contrib, d_b, d_time, f,
-                        flux0, rhsb, btmp, d_status, cg_r, cg_d, cg_q, cg_scal, cg_flags, d_hist, d_hist_count, cg_z, cg_zold};
+                        flux0, rhsb, btmp, d_status, cg_r, cg_d, cg_q, cg_scal, cg_flags, d_hist, d_hist_count, cg_z, cg_zold,
+                        d_sweep_cnt};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         for (int k = 0; k < 4; ++k) {
@@ -497,6 +503,7 @@ struct ibg_context {
         cg_flags = nullptr;
         d_hist = nullptr;
         d_hist_count = nullptr;
+        d_sweep_cnt = nullptr;
     }
 
     Bulk<double>& bulk(double*) { return b64; }
@@ -544,7 +551,7 @@ struct ibg_context {
         esolve<T>(B, k, call<T>(B, B.Bf, B.cc, (T)1));
         esolve<T>(B, -1, call<T>(B, B.cc, B.psi, (T)-1));
         launch_reg_interp<T>(g, ncomp, slots, B.psi, S, 1, nullptr, dout, 0, st);
-        launches += 3 + 2 * solve_launches() + 1;
+        launches += 2 + 2 * solve_launches() + 1;
     }
 
     // CG with warm start x = f (src/ConjugateGradientSolver.cc:35-65); host reads the
@@ -701,7 +708,7 @@ struct ibg_context {
         }
         launch_smear_bf<T>(g, ncomp, slots, f, flux0, B.Bf, beta[k], st);         // B f
         esolve<T>(B, k, call<T>(B, B.Bf, B.cc, (T)1, B.w, B.ws));                 // omega = omega* - A^-1 B f
-        launches += 3 + solve_launches();
+        launches += 2 + solve_launches();
         return IBG_OK;
     }
 
@@ -719,8 +726,8 @@ struct ibg_context {
             // positions and velocities the caller computed (sub-step `slot` of the next step, or now)
             launch_k(k_ext_boundary, (unsigned)((npts + 127) / 128), 128, 0, st, npts,
                      (const double*)(d_ext + (size_t)(slot < 0 ? kExtNow : slot) * 4 * npts), d_pts, d_vel);
-            launch_reg_update(g, npts, d_pts, d_vel, slots, d_b, u0, v0, st);
-            launches += 3;
+            launch_reg_update(g, npts, d_pts, d_vel, slots, d_b, u0, v0, flux0, st);
+            launches += 4;
             return;
         }
         if (stateful) {
@@ -728,8 +735,8 @@ struct ibg_context {
             launches += 1;
         }
         launch_kinematics(npts, d_ref, d_body_of, d_bodies, d_mstate, d_mtab, d_time, toff, d_pts, d_vel, st);
-        launch_reg_update(g, npts, d_pts, d_vel, slots, d_b, u0, v0, st);
-        launches += 3;
+        launch_reg_update(g, npts, d_pts, d_vel, slots, d_b, u0, v0, flux0, st);
+        launches += 4;
     }
 
     // BaseFlow::moveFlow(time + toff) (src/NavierStokesModel.cc:94) and the constraints it sets
@@ -796,10 +803,7 @@ struct ibg_context {
         int s = projection<T>(B, k, B.a, d_b);
         if (s) return s;
         refresh<T>(B);
-        if (sch.nsub == 1) {
-            cudaMemcpyAsync(Np, Nk, sizeof(T) * S, cudaMemcpyDeviceToDevice, st);
-            launches += 1;
-        }
+        if (sch.nsub == 1) cudaMemcpyAsync(Np, Nk, sizeof(T) * S, cudaMemcpyDeviceToDevice, st);  // (a copy, not a kernel)
         old_saved = true;
         return IBG_OK;
     }
@@ -978,9 +982,8 @@ void ibg_context::apply_learned_precond(int k, const double* r, double* z) {
         launch_k(k_fallback_identity, (ncomp + 255) / 256, 256, 0, st, ncomp, cg_flags, r, z);
         launches += 2;
     } else {
-        // no network yet: identity (plain CG directions)
+        // no network yet: identity (plain CG directions; a copy, not a kernel)
         cudaMemcpyAsync(z, r, sizeof(double) * ncomp, cudaMemcpyDeviceToDevice, st);
-        launches += 1;
     }
 }
 
@@ -1915,6 +1918,42 @@ int ibg_cg_stats(const ibg_context* c, int* last, int* mx, int* capped) {
 void* ibg_stream(const ibg_context* c) { return c ? (void*)c->st : nullptr; }
 long long ibg_last_launch_count(const ibg_context* c) { return c ? c->last_launches : 0; }
 
+namespace {
+// kernel nodes of a graph, child graphs included; -1 if it holds a conditional node (whose body runs a
+// data-dependent number of times)
+long long count_kernel_nodes(cudaGraph_t gr) {
+    size_t n = 0;
+    if (cudaGraphGetNodes(gr, nullptr, &n) != cudaSuccess) return -1;
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (n && cudaGraphGetNodes(gr, nodes.data(), &n) != cudaSuccess) return -1;
+    long long k = 0;
+    for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) != cudaSuccess) return -1;
+        if (t == cudaGraphNodeTypeKernel) {
+            ++k;
+        } else if (t == cudaGraphNodeTypeGraph) {
+            cudaGraph_t child = nullptr;
+            if (cudaGraphChildGraphNodeGetGraph(nd, &child) != cudaSuccess) return -1;
+            const long long c = count_kernel_nodes(child);
+            if (c < 0) return -1;
+            k += c;
+        } else if (t == cudaGraphNodeTypeConditional) {
+            return -1;
+        }
+    }
+    return k;
+}
+}  // namespace
+
+long long ibg_graph_kernel_nodes(ibg_context* c) {
+    if (!c) return IBG_ERR_ARG;
+    if (!c->graph_def) return IBG_ERR_STATE;
+    return count_kernel_nodes(c->graph_def);
+}
+
+long long ibg_graph_launch_claim(const ibg_context* c) { return c ? c->graph_launches : 0; }
+
 // ---------------------------------------------------------------------------
 // operator entry points
 // ---------------------------------------------------------------------------
@@ -2291,6 +2330,11 @@ int ibg_ensemble_destroy(ibg_ensemble* e) {
     return IBG_OK;
 }
 
+long long ibg_ensemble_kernel_nodes(const ibg_ensemble* e) {
+    if (!e) return IBG_ERR_ARG;
+    if (!e->exec) return IBG_ERR_STATE;
+    return count_kernel_nodes(e->graph);
+}
 void* ibg_ensemble_stream(const ibg_ensemble* e) { return e ? (void*)e->st : nullptr; }
 long long ibg_ensemble_launches_per_step(const ibg_ensemble* e) { return e ? e->launches_per_step : 0; }
 const char* ibg_ensemble_last_error(const ibg_ensemble* e) { return e ? e->err.c_str() : g_ens_error.c_str(); }

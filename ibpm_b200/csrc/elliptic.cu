@@ -781,6 +781,55 @@ __device__ void dst_pair_half(const FftDesc& d, const T* __restrict__ sines, con
     __syncthreads();
 }
 
+// the lines step of one direction (xdir: the row sums V -> bottom/top; else the column sums W ->
+// left/right) of batch item b, by the whole block, in `smem` (sweep_smem_bytes)
+template <typename T>
+__device__ __forceinline__ void sweep_lines_dir(const SweepArgs<T>& a, bool xdir, int b, unsigned char* smem) {
+    using C = typename Cplx<T>::type;
+    const GridDev& g = a.g;
+    const int NI = g.NI, NJ = g.NJ;
+    const int n = xdir ? NI : NJ;
+    // the half-length DSTs in FP64, the odd-extension ones in FP32 (as the passes); a copy, so that the
+    // kernel parameters are not addressed through a run-time choice
+    const FftDesc d = half_dst<T>() ? (xdir ? a.fcolh : a.frowh) : (xdir ? a.fcol : a.frow);
+    const T* sines = xdir ? a.sinc : a.sinr;
+    C* s0 = reinterpret_cast<C*>(smem);
+    C* s1 = s0 + d.m;
+    T* v0 = reinterpret_cast<T*>(s1 + d.m);
+    T* v1 = v0 + n;
+    T* u0 = v1 + n;
+    T* u1 = u0 + n;
+    T* e0 = u1 + n;
+    T* e1 = e0 + n;
+    const T* sums = a.vrow + (size_t)b * a.wstride + (xdir ? 0 : 2 * (size_t)NI);
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        v0[k] = __ldcg(sums + k);  // (written by other blocks of the same launch when fused into the sums)
+        v1[k] = __ldcg(sums + n + k);
+    }
+    __syncthreads();
+    if constexpr (half_dst<T>())
+        dst_pair_half<T>(d, sines, v0, v1, u0, u1, a.norm, s0, s1);
+    else
+        dst_pair_block<T>(d, n, v0, v1, u0, u1, a.norm, s0, s1);
+    const int ext = xdir ? g.nxe : g.nye;
+    for (int i = 1 + threadIdx.x; i <= n; i += blockDim.x) {
+        const int ii = i / 2 + ext;
+        if (i & 1) {
+            e0[i - 1] = (T)0.5 * (u0[ii - 1] + u0[ii]);
+            e1[i - 1] = (T)0.5 * (u1[ii - 1] + u1[ii]);
+        } else {
+            e0[i - 1] = u0[ii - 1];
+            e1[i - 1] = u1[ii - 1];
+        }
+    }
+    __syncthreads();
+    T* Eo = a.edges_out + (size_t)b * a.estride + (xdir ? 0 : 2 * (size_t)NI);
+    if constexpr (half_dst<T>())
+        dst_pair_half<T>(d, sines, e0, e1, Eo, Eo + n, (T)1, s0, s1);
+    else
+        dst_pair_block<T>(d, n, e0, e1, Eo, Eo + n, (T)1, s0, s1);
+}
+
 // sums: blocks [0, nrb) each take kSweepRows full rows (row sums V_j0, V_j1),
 // blocks [nrb, nrb + ncb) each take kSweepCols full columns (column sums
 // W_i0, W_i1); every sum is complete inside one block (fixed order).
@@ -851,6 +900,24 @@ __global__ void __launch_bounds__(256) k_sweep_sums(SweepArgs<T> a) {
             if (l < NJ) sums[2 * (size_t)NI + (size_t)(r & 1) * NJ + l] = sum;
         }
     }
+    if (!a.counters) return;
+    // fused lines step (batch 1): the last block to finish its sums of a direction turns that
+    // direction's sums into the finer level's boundary DSTs (the k_sweep_lines work)
+    __shared__ int last;
+    __threadfence();
+    __syncthreads();
+    const bool rowdir = (int)blockIdx.x < nrb;
+    if (threadIdx.x == 0) {
+        int* cnt = a.counters + (rowdir ? 0 : 1);
+        const int total = rowdir ? nrb : (int)gridDim.x - nrb;
+        last = atomicAdd(cnt, 1) == total - 1;
+        if (last) *cnt = 0;  // every other block of this direction has counted: ready for the next launch
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    sweep_lines_dir<T>(a, rowdir, b, smem_raw);
 }
 
 // lines: block 0 turns V into the lines u(., j0), u(., j1), the bottom/top
@@ -859,51 +926,8 @@ __global__ void __launch_bounds__(256) k_sweep_sums(SweepArgs<T> a) {
 template <typename T>
 __global__ void __launch_bounds__(512) k_sweep_lines(SweepArgs<T> a) {
     pdl_enter();
-    using C = typename Cplx<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const GridDev& g = a.g;
-    const int NI = g.NI, NJ = g.NJ;
-    const int b = blockIdx.y;
-    const bool xdir = blockIdx.x == 0;
-    const int n = xdir ? NI : NJ;
-    // the half-length DSTs in FP64, the odd-extension ones in FP32 (as the passes)
-    const FftDesc& d = half_dst<T>() ? (xdir ? a.fcolh : a.frowh) : (xdir ? a.fcol : a.frow);
-    const T* sines = xdir ? a.sinc : a.sinr;
-    C* s0 = reinterpret_cast<C*>(smem_raw);
-    C* s1 = s0 + d.m;
-    T* v0 = reinterpret_cast<T*>(s1 + d.m);
-    T* v1 = v0 + n;
-    T* u0 = v1 + n;
-    T* u1 = u0 + n;
-    T* e0 = u1 + n;
-    T* e1 = e0 + n;
-    const T* sums = a.vrow + (size_t)b * a.wstride + (xdir ? 0 : 2 * (size_t)NI);
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        v0[k] = sums[k];
-        v1[k] = sums[n + k];
-    }
-    __syncthreads();
-    if constexpr (half_dst<T>())
-        dst_pair_half<T>(d, sines, v0, v1, u0, u1, a.norm, s0, s1);
-    else
-        dst_pair_block<T>(d, n, v0, v1, u0, u1, a.norm, s0, s1);
-    const int ext = xdir ? g.nxe : g.nye;
-    for (int i = 1 + threadIdx.x; i <= n; i += blockDim.x) {
-        const int ii = i / 2 + ext;
-        if (i & 1) {
-            e0[i - 1] = (T)0.5 * (u0[ii - 1] + u0[ii]);
-            e1[i - 1] = (T)0.5 * (u1[ii - 1] + u1[ii]);
-        } else {
-            e0[i - 1] = u0[ii - 1];
-            e1[i - 1] = u1[ii - 1];
-        }
-    }
-    __syncthreads();
-    T* Eo = a.edges_out + (size_t)b * a.estride + (xdir ? 0 : 2 * (size_t)NI);
-    if constexpr (half_dst<T>())
-        dst_pair_half<T>(d, sines, e0, e1, Eo, Eo + n, (T)1, s0, s1);
-    else
-        dst_pair_block<T>(d, n, e0, e1, Eo, Eo + n, (T)1, s0, s1);
+    sweep_lines_dir<T>(a, blockIdx.x == 0, blockIdx.y, smem_raw);
 }
 
 // The lines step is linear in the sums: E0 = norm A V0, E1 = norm A V1 with
@@ -1380,8 +1404,14 @@ void EllipticPlan<T>::run_sweep(const SolveCall<T>& c, const T* coef, cudaStream
         s.ax = gt.ax;
         s.ay = gt.ay;
         const int nrb = (g.NI + kSweepRows - 1) / kSweepRows, ncb = (g.NJ + kSweepCols - 1) / kSweepCols;
+        const bool maps = gt.ax && gt.ay && edge_maps;
+        if (!maps && batch == 1 && sweep_counters) {
+            s.counters = sweep_counters;  // the lines step inside the sums launch
+            launch_k(k_sweep_sums<T>, dim3((unsigned)(nrb + ncb), 1u), 256, ssm, st, s);
+            continue;
+        }
         launch_k(k_sweep_sums<T>, dim3((unsigned)(nrb + ncb), (unsigned)batch), 256, 0, st, s);
-        if (gt.ax && gt.ay && edge_maps) {
+        if (maps) {
             const int nmax = std::max(g.NI, g.NJ);
             launch_k(k_sweep_edges<T>, dim3((unsigned)((nmax + kEdgeRows - 1) / kEdgeRows), 2, (unsigned)batch), 32 * kEdgeRows, sizeof(T) * 2 * (size_t)nmax, st, s);
         } else {
@@ -1558,8 +1588,11 @@ void coarsify_rhs(const GridDev& g, const double* f, double* rc, cudaStream_t st
 template <typename T>
 int EllipticPlan<T>::launches(bool coarsify) const {
     const int L = grid->L;
-    if (gemm && sines) return L == 1 ? 4 : (coarsify ? L - 1 : 0) + 2 + 2 * (L - 1) + 2;
-    return L == 1 ? 3 : (coarsify ? L - 1 : 0) + 2 + 2 * (L - 1) + 2;
+    // sweep launches per level transition: sums and lines (or edge maps), or the fused sums + lines
+    const bool fused = sweep_counters && !(edge_maps && cos && tabs().ax && tabs().ay);
+    const int per = fused ? 1 : 2;
+    if (gemm && sines) return L == 1 ? 4 : (coarsify ? L - 1 : 0) + 2 + per * (L - 1) + 2;
+    return L == 1 ? 3 : (coarsify ? L - 1 : 0) + 2 + per * (L - 1) + 2;
 }
 
 template <typename T>
@@ -1716,7 +1749,8 @@ int EllipticPlan<T>::init(const GridDev* g, const FftTables* t, bool helm, doubl
     const int sweep_need = (int)sweep_smem_bytes<T>(*g, M);
     if (raise_smem_limit((const void*)k_dst_rows<T>, rows_need) ||
         raise_smem_limit((const void*)k_dst_cols<T>, cols_need) ||
-        raise_smem_limit((const void*)k_sweep_lines<T>, sweep_need))
+        raise_smem_limit((const void*)k_sweep_lines<T>, sweep_need) ||
+        raise_smem_limit((const void*)k_sweep_sums<T>, sweep_need))
         return IBG_ERR_CUDA;
     return IBG_OK;
 }

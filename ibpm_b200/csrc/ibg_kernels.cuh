@@ -105,6 +105,7 @@ struct SweepArgs {
     T norm;
     const T* ax;                   // edge maps (k_sweep_edges)
     const T* ay;
+    int* counters;                 // 2 counters: the lines step runs inside k_sweep_sums (nullptr: its own launch)
 };
 
 // eigenvalue of the inverse operator at 0-based mode (k, l):
@@ -272,6 +273,9 @@ struct EllipticPlan {
     // tuned launch shape of the row and column passes for batch 1 (0: rule-based)
     int rows_P = 0, rows_T = 0, cols_P = 0, cols_T = 0, rows_tws = 0, cols_tws = 0;
     bool edge_maps = true;  // the sweep applies the precomputed edge maps (else the per-step line FFTs)
+    // two zeroed device counters owned by the caller: with them (and batch 1) the per-step line FFTs
+    // run inside the sums launch, by the last block of each direction; shared by the plans of one stream
+    int* sweep_counters = nullptr;
     // FP32 plans: the DST passes as sine-matrix GEMMs on the tensor cores (dst_gemm.cu) instead of FFTs
     bool gemm = false;
     const SineMats* sines = nullptr;

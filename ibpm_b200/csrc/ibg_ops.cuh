@@ -82,7 +82,7 @@ void launch_kinematics(int npts, const double* ref_xy, const int* body_of, const
                        const MotionState* ms, const double* mtab, const double* time_ptr, double toff, double* pts,
                        double* vel, cudaStream_t st);
 void launch_reg_update(const GridDev& g, int npts, const double* pts, const double* vel, RegSlots& s, double* bcon,
-                       double u0, double v0, cudaStream_t st);
+                       double u0, double v0, double* flux0, cudaStream_t st);
 template <typename T>
 void launch_reg_interp(const GridDev& g, int ncomp, const RegSlots& s, const T* psi, size_t sstride, int batch,
                        const double* bcon, double* out, size_t ostride, cudaStream_t st);

@@ -972,7 +972,11 @@ void launch_kinematics(int npts, const double* ref_xy, const int* body_of, const
 }
 
 void launch_reg_update(const GridDev& g, int npts, const double* pts, const double* vel, RegSlots& s, double* bcon,
-                       double u0, double v0, cudaStream_t st) {
+                       double u0, double v0, double* flux0, cudaStream_t st) {
+    // flux0 is zero outside the current slots' flux indices (launch_smear_bf): clear the old ones first
+    if (flux0)
+        launch_k(k_reg_zero, nblk((size_t)2 * npts * kSlots, 128), 128, 0, st, 2 * npts, 0, 0, (const int*)s.idx,
+                 (const int*)s.n, flux0, (size_t)0);
     launch_k(k_reg_update, nblk(2 * npts, 128), 128, 0, st, g, npts, pts, vel, s.idx, s.w, s.n, bcon, u0, v0);
     launch_k(k_reg_owners, nblk((size_t)2 * npts * kSlots, 128), 128, 0, st, 2 * npts, (const int*)s.idx,
              (const int*)s.n, pts, g.dx, s.own, s.contrib);
@@ -985,13 +989,15 @@ void launch_reg_interp(const GridDev& g, int ncomp, const RegSlots& s, const T* 
                                                                     ostride);
 }
 
+// flux0 is zero outside the current slots' flux indices.  Every such index has one owner, which
+// writes the full sum, so a smear overwrites exactly the indices the previous smear with the same
+// slots wrote and needs no clearing; launch_reg_update clears the old indices before the slots move.
 template <typename T>
 void launch_smear_bf(const GridDev& g, int ncomp, const RegSlots& s, const double* f, double* flux0, T* Bf,
                      double beta, cudaStream_t st) {
     launch_k(k_reg_smear, nblk((size_t)ncomp * kSlots, 128), 128, 0, st, ncomp, (const int*)s.idx,
              (const double*)s.w, (const int*)s.n, (const int*)s.own, (const int*)s.contrib, s.pts, g.dx, f, flux0);
     launch_k(k_bf<T>, dim3(nblk(g.N1, 256), 1), 256, 0, st, g, flux0, 0, Bf, 0, beta);
-    launch_k(k_reg_zero, nblk((size_t)ncomp * kSlots, 128), 128, 0, st, ncomp, 0, 0, s.idx, s.n, flux0, 0);
 }
 
 void launch_reg_smear(int ncomp, const RegSlots& s, double h, const double* f, double* flux0, cudaStream_t st) {

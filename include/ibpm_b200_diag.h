@@ -39,6 +39,17 @@ IBG_API int ibg_dst_gemm_status(ibg_context* ctx);
 IBG_API int ibg_solve_fp32(ibg_context* ctx, int substep, const double* f, double* u);
 IBG_API int ibg_lpc_status(ibg_context* ctx);
 
+/* The kernel nodes of the context's captured step graph (child graphs
+ * included), to check the launch count the library reports for a step
+ * (ibg_graph_launch_claim: the launches counted while the graph was
+ * captured).  -1 when the graph holds a conditional node (the CG loop of
+ * moving bodies, whose body runs a data-dependent number of times);
+ * IBG_ERR_STATE before the first graph-launched step. */
+IBG_API long long ibg_graph_kernel_nodes(ibg_context* ctx);
+IBG_API long long ibg_graph_launch_claim(const ibg_context* ctx);
+/* The same for an ensemble's graph (against ibg_ensemble_launches_per_step). */
+IBG_API long long ibg_ensemble_kernel_nodes(const ibg_ensemble* ens);
+
 #ifdef __cplusplus
 }
 #endif
