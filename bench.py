@@ -74,7 +74,7 @@ METRICS = {
 FORMS = {"c2": ("fp32_refined", "fp32", "fp64"), "c3": ("cholesky", "learned", "cg"),
          "c4": ("ensemble_fp32", "ensemble_refined", "ensemble", "serial"), "c5": ("cholesky", "learned", "cg")}
 PLAIN = {"c2": "fp64", "c3": "cg", "c4": "serial", "c5": "cg"}
-STEPS = {"c2": 200, "c3": 50, "c4": 20, "c5": 10}
+STEPS = {"c2": 200, "c3": 50, "c4": 60, "c5": 10}
 WARMUP = {"c2": 10, "c3": 3, "c4": 3, "c5": 3}
 PC_REFRESH = {"c3": 10, "c5": 12}
 L2_NOTE = "flushed between timed steps (256 MB write outside the events)"
@@ -131,7 +131,7 @@ class ClockSampler:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.fh = open(self.path, "w")
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                       "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh,
                                       stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.p = None
