@@ -570,6 +570,7 @@ def main():
     import ibpm_b200 as ib
     info["autotuned_dst_shapes"] = ib.autotune_log()
     info["dst_form"] = ib.dst_form_log()
+    info["sweep_form"] = ib.sweep_form_log()
     run.close()
 
     plain = None

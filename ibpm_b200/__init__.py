@@ -437,6 +437,16 @@ def dst_form_log():
     return [dict(zip(keys, (float(v) for v in buf[6 * k:6 * k + 6]))) for k in range(n)]
 
 
+def sweep_form_log():
+    """The autotuner's choice between the sweep's edge maps and its per-step line FFTs in this process:
+    one dict per grid shape and precision timed."""
+    n = lib().ibg_sweep_form_log(None, 0)
+    buf = np.zeros(7 * max(n, 1))
+    n = lib().ibg_sweep_form_log(buf.ctypes.data_as(ctypes.c_void_p), n)
+    keys = ("nx", "ny", "levels", "bytes", "edge_maps", "edge_maps_us", "line_ffts_us")
+    return [dict(zip(keys, (float(v) for v in buf[7 * k:7 * k + 7]))) for k in range(n)]
+
+
 def from_workload(wl, precision: str = "fp64", stream=None, device: int = -1, precond: str = "none",
                   pc_refresh: int = 10, cg_graph: bool = True, pc_fallback_iter: int = 0):
     """Grid, model, solver and initial State for an ibpm_b200.configs.Workload."""

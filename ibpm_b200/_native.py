@@ -76,6 +76,8 @@ SIGNATURES = {
     "ibg_graph_kernel_nodes": (ctypes.c_longlong, [_VP]),
     "ibg_graph_launch_claim": (ctypes.c_longlong, [_VP]),
     "ibg_ensemble_kernel_nodes": (ctypes.c_longlong, [_VP]),
+    "ibg_set_sweep_form": (_I, [_VP, _I]),
+    "ibg_sweep_form_log": (_I, [_VP, _I]),
     "ibg_autotune_log": (_I, [_VP, _I]),
     "ibg_set_linearized": (_I, [_VP, _I, _VP, _VP]),
     "ibg_set_sfd": (_I, [_VP, _D, _D, _VP]),

@@ -146,7 +146,14 @@ namespace {
 std::mutex g_form_mu;
 std::map<std::array<int, 3>, std::array<double, 3>> g_form;
 
-double time_solves(const EllipticPlan<float>& p, const SolveCall<float>& c, cudaStream_t st) {
+// The autotuner's choice between the coarse-to-fine sweep's edge maps and its per-step line FFTs (fused
+// into the sums launch), once per grid shape and precision: {nx, ny, levels, bytes per word} ->
+// {edge maps chosen, edge-map us, line-FFT us} per whole Poisson solve.
+std::mutex g_sweep_mu;
+std::map<std::array<int, 4>, std::array<double, 3>> g_sweep;
+
+template <typename T>
+double time_solves(const EllipticPlan<T>& p, const SolveCall<T>& c, cudaStream_t st) {
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -214,9 +221,9 @@ struct ibg_context {
         SolveCall<float> c = call<float>(b32, b32.a, b32.ws, 1.0f);
         cudaMemsetAsync(b32.a, 0, sizeof(float) * S, st);
         set_dst_gemm(false);
-        const double t_fft = time_solves(b32.poisson, c, st);
+        const double t_fft = time_solves<float>(b32.poisson, c, st);
         set_dst_gemm(true);
-        const double t_gemm = time_solves(b32.poisson, c, st);
+        const double t_gemm = time_solves<float>(b32.poisson, c, st);
         int e = 0;
         if (sines.err) {
             cudaMemcpyAsync(&e, sines.err, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -227,6 +234,37 @@ struct ibg_context {
         std::lock_guard<std::mutex> lock(g_form_mu);
         g_form[key] = {use ? 1.0 : 0.0, t_fft, t_gemm};
         return cuda_check("choose_dst_form");
+    }
+    // time whole solves of plans B with the sweep's edge maps and with its fused line FFTs the first time
+    // a grid shape is created in the process (per precision); keep the edge maps unless the line FFTs
+    // are at least 3 % faster
+    template <typename T>
+    int choose_sweep_form(Bulk<T>& B) {
+        if (g.L < 2 || !B.poisson.tabs().ax) return IBG_OK;
+        const std::array<int, 4> key = {g.nx, g.ny, g.L, (int)sizeof(T)};
+        auto set = [&](bool maps) {
+            B.poisson.edge_maps = maps;
+            for (int k = 0; k < 4; ++k) B.helm[k].edge_maps = maps;
+        };
+        {
+            std::lock_guard<std::mutex> lock(g_sweep_mu);
+            auto it = g_sweep.find(key);
+            if (it != g_sweep.end()) {
+                set(it->second[0] > 0.5);
+                return IBG_OK;
+            }
+        }
+        SolveCall<T> c = call<T>(B, B.a, B.ws, (T)1);
+        cudaMemsetAsync(B.a, 0, sizeof(T) * S, st);
+        set(true);
+        const double t_maps = time_solves<T>(B.poisson, c, st);
+        set(false);
+        const double t_lines = time_solves<T>(B.poisson, c, st);
+        const bool maps = !(t_lines < 0.97 * t_maps);
+        set(maps);
+        std::lock_guard<std::mutex> lock(g_sweep_mu);
+        g_sweep[key] = {maps ? 1.0 : 0.0, t_maps, t_lines};
+        return cuda_check("choose_sweep_form");
     }
     double beta[4] = {0, 0, 0, 0};
     // bodies
@@ -381,6 +419,8 @@ struct ibg_context {
                 if (s) return s;
             }
         }
+        s = choose_sweep_form<T>(B);
+        if (s) return s;
         B.ready = true;
         return IBG_OK;
     }
@@ -1953,6 +1993,34 @@ long long ibg_graph_kernel_nodes(ibg_context* c) {
 }
 
 long long ibg_graph_launch_claim(const ibg_context* c) { return c ? c->graph_launches : 0; }
+
+int ibg_sweep_form_log(double* out, int max_rows) {
+    std::lock_guard<std::mutex> lock(g_sweep_mu);
+    int r = 0;
+    for (const auto& kv : g_sweep) {
+        if (out && r < max_rows) {
+            double* o = out + 7 * r;
+            for (int j = 0; j < 4; ++j) o[j] = kv.first[j];
+            for (int j = 0; j < 3; ++j) o[4 + j] = kv.second[j];
+        }
+        ++r;
+    }
+    return r;
+}
+
+int ibg_set_sweep_form(ibg_context* c, int edge_maps) {
+    if (!c) return IBG_ERR_ARG;
+    cudaStreamSynchronize(c->st);
+    auto set = [&](auto& plan) { plan.edge_maps = edge_maps != 0; };
+    set(c->b64.poisson);
+    set(c->b32.poisson);
+    for (int k = 0; k < 4; ++k) {
+        set(c->b64.helm[k]);
+        set(c->b32.helm[k]);
+    }
+    c->drop_graph();
+    return IBG_OK;
+}
 
 // ---------------------------------------------------------------------------
 // operator entry points

@@ -1374,7 +1374,8 @@ void EllipticPlan<T>::run_sweep(const SolveCall<T>& c, const T* coef, cudaStream
     const size_t es = sweep_doubles(g.nx, g.ny, L);
     const size_t el = 2 * (size_t)g.NI + 2 * (size_t)g.NJ;
     const GridTables<T>& gt = tabs();
-    const int M = std::max(frow.m, fcol.m);
+    // the lines step's FFT length: half length in FP64, the odd extension in FP32 (sweep_lines_dir)
+    const int M = half_dst<T>() ? std::max(tables->rowh64.m, tables->colh64.m) : std::max(frow.m, fcol.m);
     const size_t ssm = sweep_smem_bytes<T>(g, M);
     for (int lev = L - 1; lev >= 1; --lev) {
         const double dxl = lev_dx(g, lev);

@@ -47,6 +47,18 @@ IBG_API int ibg_lpc_status(ibg_context* ctx);
  * IBG_ERR_STATE before the first graph-launched step. */
 IBG_API long long ibg_graph_kernel_nodes(ibg_context* ctx);
 IBG_API long long ibg_graph_launch_claim(const ibg_context* ctx);
+/* The coarse-to-fine sweep of every plan of the context: edge_maps = 1 applies
+ * the precomputed edge maps (two launches per level transition, the default
+ * of a single context), 0 the per-step line FFTs (inside the sums launch, the
+ * default of ensemble members); the step graph is recaptured.  Results agree
+ * to rounding. */
+IBG_API int ibg_set_sweep_form(ibg_context* ctx, int edge_maps);
+/* The autotuner's choice of that form per grid shape and precision (timed on
+ * whole Poisson solves the first time a shape is created in the process; the
+ * edge maps are kept unless the line FFTs are at least 3 % faster): up to
+ * max_rows rows of 7 doubles {nx, ny, levels, bytes per word, edge maps chosen,
+ * edge-map us, line-FFT us}; returns the number of shapes timed. */
+IBG_API int ibg_sweep_form_log(double* out, int max_rows);
 /* The same for an ensemble's graph (against ibg_ensemble_launches_per_step). */
 IBG_API long long ibg_ensemble_kernel_nodes(const ibg_ensemble* ens);
 
