@@ -427,14 +427,22 @@ class Ens:
         return np.concatenate(out)
 
     def e2e(self, Ke, sync):
+        """Every step copies every member's State in from pinned host memory and back out: in the
+        ensemble forms through Ensemble.advance_host (the copies inside the ensemble's graph, each
+        member's overlapping the others' steps), member by member otherwise."""
         import torch
+        from types import SimpleNamespace
         hosts = []
         for wl, grid, s, x in self.members:
             s.get_state(x)
             hosts.append((s, _pinned_state(x)))
+        states = [SimpleNamespace(omega=h["omega"], q=h["q"], f=h["f"]) for _, h in hosts]
         sync()
         t0 = time.perf_counter()
         for _ in range(Ke):
+            if self.ens is not None:
+                self.ens.advance_host(states, 1)
+                continue
             for s, h in hosts:
                 _upload(s, h)
             self.step()

@@ -494,6 +494,26 @@ class Ensemble:
     def launches_per_step(self) -> int:
         return int(lib().ibg_ensemble_launches_per_step(self._h))
 
+    def advance_host(self, states, nsteps: int = 1):
+        """IBSolver::advance(State&) for every member: states[i] holds member i's State arrays omega, q, f
+        (C-contiguous float64 in page-locked host memory, e.g. numpy views of pinned torch tensors).
+        Each step copies every State in, advances and copies it back out, in one graph launch, so
+        that one member's copies overlap the other members' steps."""
+        n = len(self.members)
+        if len(states) != n:
+            raise ValueError("advance_host: one State per member")
+        for x in states:
+            for a in (x.omega, x.q, x.f):
+                if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+                    raise ValueError("advance_host: State arrays must be C-contiguous float64")
+        ptrs = [(ctypes.c_void_p * n)(*[getattr(x, k).ctypes.data for x in states]) for k in ("omega", "q", "f")]
+        st = lib().ibg_ensemble_advance_host(self._h, int(nsteps), *ptrs)
+        if st < 0:
+            raise IbgError(f"ibg_ensemble_advance_host: {lib().ibg_ensemble_last_error(self._h).decode()}")
+
+    def host_launches_per_step(self) -> int:
+        return int(lib().ibg_ensemble_host_launches_per_step(self._h))
+
     def close(self):
         if getattr(self, "_h", None):
             lib().ibg_ensemble_destroy(self._h)

@@ -2249,8 +2249,26 @@ struct ibg_ensemble {
     cudaGraphExec_t exec = nullptr;
     cudaStream_t st = nullptr;
     long long launches_per_step = 0;
+    // the host-state step (ibg_ensemble_advance_host): per member, copies in -> step -> copies out,
+    // for the host arrays it was built with
+    cudaGraph_t hgraph = nullptr;
+    cudaGraphExec_t hexec = nullptr;
+    std::vector<const void*> hptrs;
+    std::vector<cudaGraph_t> hparts;  // the members' captured copy-in and copy-out graphs
+    long long hlaunches_per_step = 0;
     std::string err;
+    void drop_host_graph() {
+        if (hexec) cudaGraphExecDestroy(hexec);
+        if (hgraph) cudaGraphDestroy(hgraph);
+        for (cudaGraph_t g : hparts) cudaGraphDestroy(g);
+        hexec = nullptr;
+        hgraph = nullptr;
+        hparts.clear();
+        hptrs.clear();
+        hlaunches_per_step = 0;
+    }
     ~ibg_ensemble() {
+        drop_host_graph();
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         for (cudaEvent_t x : ev) cudaEventDestroy(x);
@@ -2369,6 +2387,113 @@ int ibg_ensemble_advance(ibg_ensemble* e, int nsteps) {
     return IBG_OK;
 }
 
+// the host-state step graph: member i's branch copies omega[i], q[i], f[i] in (and converts them to
+// FP32 for an FP32 member), runs the member's captured step and copies the state back out
+static int ensemble_build_host(ibg_ensemble* e, double* const* omega, double* const* q, double* const* f) {
+    e->drop_host_graph();
+    if (cudaGraphCreate(&e->hgraph, 0) != cudaSuccess) {
+        e->err = "ibg_ensemble_advance_host: graph creation failed";
+        return IBG_ERR_CUDA;
+    }
+    for (size_t i = 0; i < e->members.size(); ++i) {
+        ibg_context* c = e->members[i];
+        cudaGraph_t pre = nullptr, post = nullptr;
+        const long long l0 = c->launches;
+        if (cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return c->cuda_check("capture");
+        cudaMemcpyAsync(c->b64.w, omega[i], sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
+        cudaMemcpyAsync(c->b64.q, q[i], sizeof(double) * c->F, cudaMemcpyHostToDevice, c->st);
+        cudaMemcpyAsync(c->f, f[i], sizeof(double) * c->ncomp, cudaMemcpyHostToDevice, c->st);
+        c->to32();
+        if (cudaStreamEndCapture(c->st, &pre) != cudaSuccess) return c->cuda_check("capture end");
+        e->hparts.push_back(pre);
+        if (cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return c->cuda_check("capture");
+        c->to64();
+        cudaMemcpyAsync(omega[i], c->b64.w, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);
+        cudaMemcpyAsync(q[i], c->b64.q, sizeof(double) * c->F, cudaMemcpyDeviceToHost, c->st);
+        cudaMemcpyAsync(f[i], c->f, sizeof(double) * c->ncomp, cudaMemcpyDeviceToHost, c->st);
+        if (cudaStreamEndCapture(c->st, &post) != cudaSuccess) return c->cuda_check("capture end");
+        e->hparts.push_back(post);
+        const long long conv = c->fp32 ? 4 : 0;  // k_convert in and out, two arrays each
+        c->launches = l0;
+        cudaGraphNode_t n0, n1, n2;
+        if (cudaGraphAddChildGraphNode(&n0, e->hgraph, nullptr, 0, pre) != cudaSuccess ||
+            cudaGraphAddChildGraphNode(&n1, e->hgraph, &n0, 1, c->graph_def) != cudaSuccess ||
+            cudaGraphAddChildGraphNode(&n2, e->hgraph, &n1, 1, post) != cudaSuccess) {
+            e->err = "ibg_ensemble_advance_host: adding a member's nodes failed";
+            return IBG_ERR_CUDA;
+        }
+        e->hlaunches_per_step += c->graph_launches + conv;
+        e->hptrs.push_back(omega[i]);
+        e->hptrs.push_back(q[i]);
+        e->hptrs.push_back(f[i]);
+    }
+    if (cudaGraphInstantiate(&e->hexec, e->hgraph, 0) != cudaSuccess) {
+        e->err = "ibg_ensemble_advance_host: graph instantiation failed";
+        return IBG_ERR_CUDA;
+    }
+    return IBG_OK;
+}
+
+int ibg_ensemble_advance_host(ibg_ensemble* e, int nsteps, double* const* omega, double* const* q,
+                              double* const* f) {
+    if (!e || nsteps < 0 || !omega || !q || !f) return IBG_ERR_ARG;
+    const size_t n = e->members.size();
+    for (size_t i = 0; i < n; ++i) {
+        if (!omega[i] || !q[i] || !f[i]) return IBG_ERR_ARG;
+        // the copies are captured into a graph: the host arrays must be page-locked
+        const void* p3[3] = {omega[i], q[i], f[i]};
+        for (const void* p : p3) {
+            cudaPointerAttributes at{};
+            if (cudaPointerGetAttributes(&at, p) != cudaSuccess || at.type != cudaMemoryTypeHost) {
+                cudaGetLastError();
+                e->err = "ibg_ensemble_advance_host: the State arrays must be page-locked host memory "
+                         "(cudaHostAlloc / cudaHostRegister)";
+                return IBG_ERR_ARG;
+            }
+        }
+    }
+    if (!e->exec) {
+        e->err = "ibg_ensemble_advance_host: advance the ensemble by ibg_ensemble_advance first";
+        return IBG_ERR_STATE;
+    }
+    bool same = e->hexec && e->hptrs.size() == 3 * n;
+    for (size_t i = 0; same && i < n; ++i)
+        same = e->hptrs[3 * i] == omega[i] && e->hptrs[3 * i + 1] == q[i] && e->hptrs[3 * i + 2] == f[i];
+    if (!same) {
+        cudaStreamSynchronize(e->st);
+        for (ibg_context* c : e->members) cudaStreamSynchronize(c->st);
+        int s = ensemble_build_host(e, omega, q, f);
+        if (s) {
+            e->drop_host_graph();
+            return s;
+        }
+    }
+    for (size_t i = 0; i < n; ++i) {
+        cudaEventRecord(e->ev[i], e->members[i]->st);
+        cudaStreamWaitEvent(e->st, e->ev[i], 0);
+    }
+    for (int k = 0; k < nsteps; ++k) {
+        if (cudaGraphLaunch(e->hexec, e->st) != cudaSuccess) {
+            e->err = std::string("ibg_ensemble_advance_host: ") + cudaGetErrorString(cudaGetLastError());
+            return IBG_ERR_CUDA;
+        }
+        for (ibg_context* c : e->members) {
+            c->timestep += 1;
+            c->time += c->prm.dt;
+            c->hist_steps += 1;
+            c->last_launches = c->graph_launches + (c->fp32 ? 4 : 0);
+        }
+    }
+    if (cudaStreamSynchronize(e->st) != cudaSuccess) {
+        e->err = std::string("ibg_ensemble_advance_host: ") + cudaGetErrorString(cudaGetLastError());
+        return IBG_ERR_CUDA;
+    }
+    for (ibg_context* c : e->members) c->state_in_32 = c->fp32;
+    return IBG_OK;
+}
+
+long long ibg_ensemble_host_launches_per_step(const ibg_ensemble* e) { return e ? e->hlaunches_per_step : 0; }
+
 int ibg_ensemble_set_shapes(ibg_ensemble* e, int pairs_per_cta, int threads, int edge_maps) {
     if (!e || pairs_per_cta < 0 || pairs_per_cta > 2 ||
         (pairs_per_cta > 0 && (threads < 32 || threads > 512 || threads % 32)))
@@ -2379,6 +2504,7 @@ int ibg_ensemble_set_shapes(ibg_ensemble* e, int pairs_per_cta, int threads, int
         c->set_shapes(pairs_per_cta, threads, edge_maps != 0);
     }
     // the parent graph is rebuilt from the members' new captures at the next advance
+    e->drop_host_graph();
     if (e->exec) cudaGraphExecDestroy(e->exec);
     e->exec = nullptr;
     if (e->graph) cudaGraphDestroy(e->graph);

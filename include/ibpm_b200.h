@@ -267,6 +267,19 @@ IBG_API int ibg_set_step_kinematics(ibg_context* ctx, int slot, const double* po
 typedef struct ibg_ensemble ibg_ensemble;
 IBG_API int ibg_ensemble_create(int n, ibg_context* const* members, ibg_ensemble** out);
 IBG_API int ibg_ensemble_advance(ibg_ensemble* ens, int nsteps);
+/* The reference's contract for every member at once (IBSolver::advance(State&),
+ * src/IBSolver.cc:142-149: the State lives on the host): each of the nsteps
+ * steps copies member i's omega[i], q[i], f[i] (its State arrays, reference
+ * layouts, FP64) to the device, advances it and copies them back, all in one
+ * graph launch per step, so that one member's copies overlap the other
+ * members' steps.  The host arrays must be page-locked (cudaHostAlloc or
+ * cudaHostRegister; IBG_ERR_ARG otherwise).  Call ibg_ensemble_advance at least once first; the step
+ * counters and times stay the members' own (ibg_get_state).  The graph is
+ * rebuilt when the host pointers change. */
+IBG_API int ibg_ensemble_advance_host(ibg_ensemble* ens, int nsteps, double* const* omega, double* const* q,
+                                      double* const* f);
+/* kernels launched per ibg_ensemble_advance_host step (the members' steps plus their precision conversions) */
+IBG_API long long ibg_ensemble_host_launches_per_step(const ibg_ensemble* ens);
 IBG_API int ibg_ensemble_destroy(ibg_ensemble* ens);
 /* one launch shape for every member's DST passes: pairs_per_cta 0 (the rule-based default), 1 or 2
  * line pairs per CTA with `threads` threads; edge_maps 1 applies the precomputed sweep edge maps,
