@@ -20,7 +20,8 @@ from helpers import rel_l2
 pytestmark = pytest.mark.gpu
 
 GRIDS = [(128, 128, 1, 4.0, -2.0, -2.0), (64, 48, 2, 2.0, -1.0, -0.75), (200, 120, 3, 4.0, -2.0, -1.2),
-         (256, 256, 3, 4.0, -2.0, -2.0), (512, 512, 1, 4.0, -2.0, -2.0), (384, 128, 2, 6.0, -3.0, -1.0)]
+         (256, 256, 3, 4.0, -2.0, -2.0), (512, 512, 1, 4.0, -2.0, -2.0), (384, 128, 2, 6.0, -3.0, -1.0),
+         (45, 27, 1, 3.0, -1.5, -0.9)]
 
 
 def _solver(gp):

@@ -27,8 +27,10 @@ def _solver_for(gp, pts, Re=100.0, dt=0.01, scheme="rk3", motion=None, tol=1e-7)
     return grid, model, ib.NonlinearIBSolver(grid, model, dt, scheme, tol)
 
 
+# (the odd single-level grids give odd lengths N = nx, ny to the FP64 half-length DSTs, whose last sine
+# sum then has no even partner)
 GRIDS = [(16, 16, 1, 2.0, -1.0, -1.0), (32, 16, 3, 3.0, -1.5, -0.75), (64, 64, 2, 4.0, -2.0, -2.0),
-         (40, 24, 4, 2.0, -1.0, -0.6)]
+         (40, 24, 4, 2.0, -1.0, -0.6), (45, 27, 1, 3.0, -1.5, -0.9), (21, 35, 1, 2.0, -1.0, -1.6)]
 
 
 @pytest.mark.parametrize("gp", GRIDS)

@@ -115,8 +115,8 @@ def test_gpu_loss_and_gradient_match_oracle():
 @pytest.mark.gpu
 def test_gpu_training_lowers_loss_and_pcg_iterations():
     """Train on the plate's own force operators, then advance: the forces match
-    the reference at the same absolute CG tolerance, with fewer iterations than
-    plain CG; the BF16 inference agrees with the float64 forward."""
+    the reference at the same absolute CG tolerance, with at most 0.8 times the
+    iterations of plain CG; the BF16 inference agrees with the float64 forward."""
     ib, d, grid, geo = _plate()
     model = ib.NavierStokesModel(grid, geo, float(d["Re"]))
     n = int(d["nsteps"])
@@ -142,7 +142,8 @@ def test_gpu_training_lowers_loss_and_pcg_iterations():
         assert rel_l2(forces, d["forces"][:, 2:4]) < 1e-8
         assert rel_l2(x.omega, d["omega"]) < 1e-9
         s.close()
-    assert its["learned"] < its["none"], its
+    # measured on the B200: 791 against 1246 iterations over the run (0.63)
+    assert its["learned"] < 0.8 * its["none"], its
 
 
 @pytest.mark.gpu
