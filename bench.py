@@ -375,7 +375,7 @@ class Single:
 class Ens:
     """The 64-member ensemble (c4): one graph (ensemble*) or member after member (serial)."""
 
-    def __init__(self, form, stream, device, count=64, world_size=1, rank=0):
+    def __init__(self, form, stream, device, count=64, world_size=1, rank=0, autotune=False):
         import ibpm_b200 as ib
         from ibpm_b200 import configs
         from ibpm_b200.replicas import shard
@@ -396,10 +396,18 @@ class Ens:
         self.ens = None
         self.stream = stream
         self.member_stream = stream
+        self.run = {"members_on_rank0": len(self.members), "member_precision": prec}
+        self.pre_steps = 0  # steps every member took before the warm-up (the launch-shape trials)
         if form.startswith("ensemble"):
             self.ens = ib.Ensemble([m[2] for m in self.members])
             self.stream = torch.cuda.ExternalStream(self.ens.stream(), device=torch.device("cuda", device))
-        self.run = {"members_on_rank0": len(self.members), "member_precision": prec}
+            if world_size == 1 and autotune:
+                # the members' DST launch shapes per grid class, chosen by timing ensemble steps
+                self.ens.advance(1)
+                self.run["ensemble_shapes"] = self.ens.autotune(2)
+                s0, x0 = self.members[0][2], self.members[0][3]
+                s0.get_state(x0)
+                self.pre_steps = int(x0.timestep)
 
     def step(self):
         if self.ens is not None:
@@ -481,6 +489,9 @@ def main():
                          "graph (profilers cannot see the kernels of a graph with conditional nodes)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-path comparison run")
+    ap.add_argument("--ens-autotune", action="store_true",
+                    help="c4: choose the members' launch shapes per grid class by timing ensemble steps first "
+                         "(the trials advance the members; the plain run takes the same steps)")
     ap.add_argument("--profile", action="store_true",
                     help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off) "
                          "and skip the e2e, roofline, plain and CPU legs")
@@ -515,7 +526,7 @@ def main():
     def build(f):
         stream = torch.cuda.Stream(device=dev)
         if wlname == "c4":
-            return Ens(f, stream, local, count=args.members, world_size=ws, rank=rank)
+            return Ens(f, stream, local, count=args.members, world_size=ws, rank=rank, autotune=args.ens_autotune)
         # the plain path is always FP64; --precision applies to the chosen form
         prec = args.precision if f != PLAIN[wlname] else None
         return Single(wlname, f, stream, local, pc_refresh=pc_refresh, lpc_train=lpc_train,
@@ -550,7 +561,8 @@ def main():
     # replica per rank
     job_units = run.total if wlname == "c4" else ws
     value = job_throughput(1, K, job_units, ms)
-    forces = run.forces(W + K)
+    pre = getattr(run, "pre_steps", 0)
+    forces = run.forces(pre + W + K)
     omega = run.omega()
     cg = None
     if it0 is not None:
@@ -584,13 +596,13 @@ def main():
     plain = None
     if form != PLAIN[wlname] and not args.no_plain:
         p = build(PLAIN[wlname])
-        for _ in range(W):
+        for _ in range(pre + W):  # the same steps as the chosen form's run (its shape trials included)
             p.step()
         pit0 = p.iterations() if hasattr(p, "iterations") else None
         sync()
         pms, _ = time_steps(K, p.stream, p.step, flush)
         pms = maxrank(pms)
-        pforces = p.forces(W + K)
+        pforces = p.forces(pre + W + K)
         pomega = p.omega()
         plain = {"form": PLAIN[wlname], "value": job_throughput(1, K, job_units, pms), "ms_per_step": pms / K,
                  "force_rel_l2_vs_plain": rel_l2(forces, pforces),

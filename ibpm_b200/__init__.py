@@ -511,6 +511,17 @@ class Ensemble:
         if st < 0:
             raise IbgError(f"ibg_ensemble_advance_host: {lib().ibg_ensemble_last_error(self._h).decode()}")
 
+    def autotune(self, steps_per_trial: int = 3):
+        """Choose each grid class's DST launch shape by timing ensemble steps (the trials advance every
+        member); returns one dict per class."""
+        rows = np.zeros(5 * max(1, len(self.members)), dtype=np.int32)
+        n = lib().ibg_ensemble_autotune(self._h, int(steps_per_trial), rows.ctypes.data_as(ctypes.c_void_p),
+                                        len(self.members))
+        if n < 0:
+            raise IbgError(f"ibg_ensemble_autotune: {lib().ibg_ensemble_last_error(self._h).decode()}")
+        keys = ("nx", "ny", "us_per_step", "pairs_per_cta", "threads")
+        return [dict(zip(keys, (int(v) for v in rows[5 * k:5 * k + 5]))) for k in range(n)]
+
     def host_launches_per_step(self) -> int:
         return int(lib().ibg_ensemble_host_launches_per_step(self._h))
 

@@ -120,6 +120,7 @@ SIGNATURES = {
     "ibg_ensemble_stream": (_VP, [_VP]),
     "ibg_ensemble_launches_per_step": (ctypes.c_longlong, [_VP]),
     "ibg_ensemble_advance_host": (_I, [_VP, _I, _VP, _VP, _VP]),
+    "ibg_ensemble_autotune": (_I, [_VP, _I, _VP, _I]),
     "ibg_ensemble_host_launches_per_step": (ctypes.c_longlong, [_VP]),
     "ibg_ensemble_last_error": (ctypes.c_char_p, [_VP]),
     "ibg_static_last_error": (ctypes.c_char_p, []),

@@ -2452,9 +2452,14 @@ int ibg_ensemble_advance_host(ibg_ensemble* e, int nsteps, double* const* omega,
             }
         }
     }
+    for (ibg_context* c : e->members)
+        if (!c->old_saved) {
+            e->err = "ibg_ensemble_advance_host: advance the ensemble by ibg_ensemble_advance first";
+            return IBG_ERR_STATE;
+        }
     if (!e->exec) {
-        e->err = "ibg_ensemble_advance_host: advance the ensemble by ibg_ensemble_advance first";
-        return IBG_ERR_STATE;
+        int s = ensemble_build(e);
+        if (s) return s;
     }
     bool same = e->hexec && e->hptrs.size() == 3 * n;
     for (size_t i = 0; same && i < n; ++i)
@@ -2493,6 +2498,107 @@ int ibg_ensemble_advance_host(ibg_ensemble* e, int nsteps, double* const* omega,
 }
 
 long long ibg_ensemble_host_launches_per_step(const ibg_ensemble* e) { return e ? e->hlaunches_per_step : 0; }
+
+// drop the parent graph (rebuilt from the members' captures at the next advance)
+static int ensemble_reset(ibg_ensemble* e) {
+    e->drop_host_graph();
+    if (e->exec) cudaGraphExecDestroy(e->exec);
+    e->exec = nullptr;
+    if (e->graph) cudaGraphDestroy(e->graph);
+    e->graph = nullptr;
+    e->launches_per_step = 0;
+    if (cudaGraphCreate(&e->graph, 0) != cudaSuccess) {
+        e->err = "ibg_ensemble: graph creation failed";
+        return IBG_ERR_CUDA;
+    }
+    return IBG_OK;
+}
+
+namespace {
+struct EnsTune {
+    int nx, ny, levels, pairs, threads;
+    double ms;  // ensemble step time with this class's chosen shape
+};
+}  // namespace
+
+int ibg_ensemble_autotune(ibg_ensemble* e, int steps_per_trial, int* out, int max_rows) {
+    if (!e || steps_per_trial < 1) return IBG_ERR_ARG;
+    for (ibg_context* c : e->members)
+        if (!c->old_saved) {
+            e->err = "ibg_ensemble_autotune: advance the ensemble by ibg_ensemble_advance first";
+            return IBG_ERR_STATE;
+        }
+    // size classes (grid shape), largest first; every member starts from two pairs and 128 threads
+    std::map<std::pair<int, int>, std::vector<ibg_context*>> cls;
+    for (ibg_context* c : e->members) cls[{c->g.nx, c->g.ny}].push_back(c);
+    std::vector<std::pair<int, int>> order;
+    for (auto& kv : cls) order.push_back(kv.first);
+    std::sort(order.begin(), order.end(), [](auto a, auto b) { return a.first * a.second > b.first * b.second; });
+    const int cand[][2] = {{2, 128}, {1, 128}, {2, 256}, {1, 256}, {2, 96}};
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto trial = [&](double& ms) -> int {
+        int s = ensemble_reset(e);
+        if (s) return s;
+        s = ibg_ensemble_advance(e, 1);  // captures and instantiates; not timed
+        if (s) return s;
+        cudaEventRecord(e0, e->st);
+        s = ibg_ensemble_advance(e, steps_per_trial);
+        if (s) return s;
+        cudaEventRecord(e1, e->st);
+        if (cudaEventSynchronize(e1) != cudaSuccess) return IBG_ERR_CUDA;
+        float v = 0.f;
+        cudaEventElapsedTime(&v, e0, e1);
+        ms = v / steps_per_trial;
+        return IBG_OK;
+    };
+    auto set_class = [&](const std::vector<ibg_context*>& ms, int P, int T) {
+        cudaStreamSynchronize(e->st);
+        for (ibg_context* c : ms) {
+            cudaStreamSynchronize(c->st);
+            c->set_shapes(P, T, false);
+        }
+    };
+    std::vector<EnsTune> log;
+    double best_all = 0.0;
+    int s = trial(best_all);
+    for (size_t ci = 0; ci < order.size() && !s; ++ci) {
+        const auto& ms = cls[order[ci]];
+        int bp = 2, bt = 128;
+        double best = best_all;
+        for (const auto& cd : cand) {
+            if (cd[0] == 2 && cd[1] == 128) continue;
+            set_class(ms, cd[0], cd[1]);
+            double t = 0.0;
+            s = trial(t);
+            if (s) break;
+            if (t < 0.99 * best) {
+                best = t;
+                bp = cd[0];
+                bt = cd[1];
+            }
+        }
+        if (s) break;
+        set_class(ms, bp, bt);
+        best_all = best;
+        log.push_back({order[ci].first, order[ci].second, ms[0]->g.L, bp, bt, best});
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (!s) s = ensemble_reset(e);
+    if (s) return s;
+    if (out)
+        for (size_t r = 0; r < log.size() && (int)r < max_rows; ++r) {
+            int* o = out + 5 * r;
+            o[0] = log[r].nx;
+            o[1] = log[r].ny;
+            o[2] = (int)std::lround(1000.0 * log[r].ms);  // us per ensemble step after this class
+            o[3] = log[r].pairs;
+            o[4] = log[r].threads;
+        }
+    return (int)log.size();
+}
 
 int ibg_ensemble_set_shapes(ibg_ensemble* e, int pairs_per_cta, int threads, int edge_maps) {
     if (!e || pairs_per_cta < 0 || pairs_per_cta > 2 ||

@@ -286,6 +286,15 @@ IBG_API int ibg_ensemble_destroy(ibg_ensemble* ens);
  * 0 the per-step line FFTs (the default for members).  The members' steps are recaptured at the next
  * ibg_ensemble_advance; results do not depend on the shape. */
 IBG_API int ibg_ensemble_set_shapes(ibg_ensemble* ens, int pairs_per_cta, int threads, int edge_maps);
+/* Choose the members' DST launch shapes by timing the ensemble itself: for each class of members with
+ * the same grid (largest first) every candidate shape (line pairs per CTA, threads: 2/128, 1/128,
+ * 2/256, 1/256, 2/96) runs 1 + steps_per_trial ensemble steps, and a class keeps the candidate whose
+ * timed steps are at least 1 % faster than the best so far (else two pairs and 128 threads).  The
+ * trials are real steps: every member advances by (1 + steps_per_trial) per trial, 1 + 4 x classes
+ * trials in all.  Writes up to max_rows rows of 5 ints {nx, ny, us per ensemble step with that
+ * class's choice, pairs per CTA, threads} and returns the number of classes (< 0 on error).  Call
+ * ibg_ensemble_advance at least once first. */
+IBG_API int ibg_ensemble_autotune(ibg_ensemble* ens, int steps_per_trial, int* out, int max_rows);
 IBG_API void* ibg_ensemble_stream(const ibg_ensemble* ens);
 IBG_API long long ibg_ensemble_launches_per_step(const ibg_ensemble* ens);
 IBG_API const char* ibg_ensemble_last_error(const ibg_ensemble* ens);

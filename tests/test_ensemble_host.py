@@ -78,3 +78,37 @@ def test_advance_host_refuses_pageable_arrays():
     ens.close()
     for s, _ in members:
         s.close()
+
+
+def test_autotune_picks_a_shape_per_grid_class_and_keeps_results():
+    """ibg_ensemble_autotune times real ensemble steps per grid class; the shapes it tries compute the
+    same butterflies in the same order, so the members' states match an ensemble advanced by as many
+    plain steps, bit for bit."""
+    import ibpm_b200 as ib
+    a, b = _members(), _members()
+    ens_a = ib.Ensemble([s for s, _ in a])
+    ens_b = ib.Ensemble([s for s, _ in b])
+    ens_a.advance(1)
+    ens_b.advance(1)
+    rows = ens_a.autotune(1)
+    assert len(rows) == len({gp[:2] for gp, _ in MEMBERS})
+    for r in rows:
+        assert (r["pairs_per_cta"], r["threads"]) in {(2, 128), (1, 128), (2, 256), (1, 256), (2, 96)}
+        assert r["us_per_step"] > 0
+    sa, xa = a[0]
+    sa.get_state(xa)
+    steps = int(xa.timestep) - 1
+    assert steps == (1 + 4 * len(rows)) * 2
+    ens_b.advance(steps)
+    ens_a.advance(2)
+    ens_b.advance(2)
+    for (s1, x1), (s2, x2) in zip(a, b):
+        s1.get_state(x1)
+        s2.get_state(x2)
+        assert x1.timestep == x2.timestep
+        assert np.array_equal(x1.omega, x2.omega)
+        assert np.array_equal(x1.f, x2.f)
+    ens_a.close()
+    ens_b.close()
+    for s, _ in a + b:
+        s.close()
