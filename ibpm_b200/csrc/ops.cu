@@ -103,12 +103,12 @@ template <typename T>
 __global__ void k_node_vel(GridDev g, const T* __restrict__ q, const T* __restrict__ w, T* __restrict__ U,
                            T* __restrict__ V, size_t sstride, size_t fstride) {
     pdl_enter();
-    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const size_t total = (size_t)g.L * g.N1;
-    if (tid >= total) return;
-    const size_t sb = (size_t)blockIdx.y * sstride, fb = (size_t)blockIdx.y * fstride;
-    const int lev = (int)(tid / g.N1);
-    const int r = (int)(tid % g.N1);
+    // blockIdx.y: level, blockIdx.z: batch item (32-bit index arithmetic within a level)
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= g.N1) return;
+    const int lev = blockIdx.y;
+    const size_t tid = (size_t)lev * g.N1 + r;
+    const size_t sb = (size_t)blockIdx.z * sstride, fb = (size_t)blockIdx.z * fstride;
     const int i = r / g.NJ + 1, j = r % g.NJ + 1;
     T u, v;
     bool du, dv;
@@ -296,11 +296,11 @@ __global__ void k_cross_flux(GridDev g, int lev, const T* __restrict__ U, const 
 template <typename T>
 __global__ void k_curl_flux(GridDev g, const T* __restrict__ C, T* __restrict__ N, size_t sstride, size_t fstride) {
     pdl_enter();
-    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= (size_t)g.L * g.N1) return;
-    const size_t sb = (size_t)blockIdx.y * sstride, fb = (size_t)blockIdx.y * fstride;
-    const int lev = (int)(tid / g.N1);
-    const int r = (int)(tid % g.N1);
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;  // blockIdx.y: level, blockIdx.z: batch item
+    if (r >= g.N1) return;
+    const int lev = blockIdx.y;
+    const size_t tid = (size_t)lev * g.N1 + r;
+    const size_t sb = (size_t)blockIdx.z * sstride, fb = (size_t)blockIdx.z * fstride;
     const int i = r / g.NJ + 1, j = r % g.NJ + 1;
     const T* ql = C + fb + (size_t)lev * g.F1;
     const double dxl = lev_dx(g, lev);
@@ -313,10 +313,10 @@ template <typename T>
 __global__ void k_rhs(GridDev g, const T* __restrict__ w, const T* __restrict__ N, const T* __restrict__ Nprev,
                       T* __restrict__ a, T c1, T an, T bn, T dt, int lap_only) {
     pdl_enter();
-    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= (size_t)g.L * g.N1) return;
-    const int lev = (int)(tid / g.N1);
-    const int r = (int)(tid % g.N1);
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;  // blockIdx.y: level
+    if (r >= g.N1) return;
+    const int lev = blockIdx.y;
+    const size_t tid = (size_t)lev * g.N1 + r;
     const int i = r / g.NJ + 1, j = r % g.NJ + 1;
     const T* f = w + (size_t)lev * g.N1;
     const T* c = (lev < g.L - 1) ? w + (size_t)(lev + 1) * g.N1 : nullptr;
@@ -345,10 +345,10 @@ template <typename T>
 __global__ void k_curl_rhs(GridDev g, const T* __restrict__ C, T* N, const T* __restrict__ w, const T* Nprev,
                            T* __restrict__ a, T c1, T an, T bn, T dt) {
     pdl_enter();
-    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= (size_t)g.L * g.N1) return;
-    const int lev = (int)(tid / g.N1);
-    const int r = (int)(tid % g.N1);
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;  // blockIdx.y: level
+    if (r >= g.N1) return;
+    const int lev = blockIdx.y;
+    const size_t tid = (size_t)lev * g.N1 + r;
     const int i = r / g.NJ + 1, j = r % g.NJ + 1;
     const double dxl = lev_dx(g, lev);
     const T bydx2 = (T)(1. / (dxl * dxl));
@@ -387,10 +387,10 @@ template <typename T>
 __global__ void k_refresh_flux(GridDev g, const T* __restrict__ psi, T* __restrict__ q, double u0, double v0,
                                const double* __restrict__ q0f) {
     pdl_enter();
-    const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= (size_t)g.L * g.F1) return;
-    const int lev = (int)(tid / g.F1);
-    const int idx = (int)(tid % g.F1);
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;  // blockIdx.y: level
+    if (idx >= g.F1) return;
+    const int lev = blockIdx.y;
+    const size_t tid = (size_t)lev * g.F1 + idx;
     const T* f = psi + (size_t)lev * g.N1;
     const T* c = (lev < g.L - 1) ? psi + (size_t)(lev + 1) * g.N1 : nullptr;
     const double dxl = lev_dx(g, lev);
@@ -852,8 +852,7 @@ static inline unsigned nblk(size_t n, int t) { return (unsigned)((n + t - 1) / t
 template <typename T>
 void launch_nonlinear_flux(const GridDev& g, const T* q, const T* w, T* U, T* V, T* C, int batch, size_t sstride,
                            size_t fstride, cudaStream_t st) {
-    const size_t S = (size_t)g.L * g.N1;
-    launch_k(k_node_vel<T>, dim3(nblk(S, 256), batch), 256, 0, st, g, q, w, U, V, sstride, fstride);
+    launch_k(k_node_vel<T>, dim3(nblk(g.N1, 256), (unsigned)g.L, batch), 256, 0, st, g, q, w, U, V, sstride, fstride);
     for (int lev = 0; lev < g.L; ++lev)
         launch_k(k_cross_flux<T>, dim3(nblk(g.F1, 256), batch), 256, 0, st, g, lev, U, V, C, sstride, fstride);
 }
@@ -861,16 +860,15 @@ void launch_nonlinear_flux(const GridDev& g, const T* q, const T* w, T* U, T* V,
 template <typename T>
 void launch_nonlinear(const GridDev& g, const T* q, const T* w, T* U, T* V, T* C, T* N, int batch, size_t sstride,
                       size_t fstride, cudaStream_t st) {
-    const size_t S = (size_t)g.L * g.N1;
     launch_nonlinear_flux<T>(g, q, w, U, V, C, batch, sstride, fstride, st);
-    launch_k(k_curl_flux<T>, dim3(nblk(S, 256), batch), 256, 0, st, g, C, N, sstride, fstride);
+    launch_k(k_curl_flux<T>, dim3(nblk(g.N1, 256), (unsigned)g.L, batch), 256, 0, st, g, C, N, sstride, fstride);
 }
 
 template <typename T>
 void launch_curl_rhs(const GridDev& g, const T* C, T* N, const T* w, const T* Nprev, T* a, double c1, double an,
                      double bn, double dt, cudaStream_t st) {
-    const size_t S = (size_t)g.L * g.N1;
-    launch_k(k_curl_rhs<T>, nblk(S, 256), 256, 0, st, g, C, N, w, Nprev, a, (T)c1, (T)an, (T)bn, (T)dt);
+    launch_k(k_curl_rhs<T>, dim3(nblk(g.N1, 256), (unsigned)g.L), 256, 0, st, g, C, N, w, Nprev, a, (T)c1, (T)an, (T)bn,
+             (T)dt);
 }
 
 void launch_nonlinear_lin(const GridDev& g, const double* q, const double* w, const double* qb, const double* wb,
@@ -880,7 +878,7 @@ void launch_nonlinear_lin(const GridDev& g, const double* q, const double* w, co
     launch_k(k_node_vel_lin, nblk(S, 256), 256, 0, st, g, q, w, qb, wb, period, ts0, count, U, V);
     for (int lev = 0; lev < g.L; ++lev)
         launch_k(k_cross_flux<double>, dim3(nblk(g.F1, 256), 1), 256, 0, st, g, lev, U, V, C, S, F);
-    launch_k(k_curl_flux<double>, dim3(nblk(S, 256), 1), 256, 0, st, g, C, N, S, F);
+    launch_k(k_curl_flux<double>, dim3(nblk(g.N1, 256), (unsigned)g.L, 1), 256, 0, st, g, C, N, S, F);
 }
 
 void launch_flux_cross(const GridDev& g, const double* q1, const double* q2, double* out, cudaStream_t st) {
@@ -900,20 +898,19 @@ void launch_sfd(size_t n, const double* w, double* what, double* rprev, double* 
 template <typename T>
 void launch_curl_flux(const GridDev& g, const T* C, T* N, cudaStream_t st) {
     const size_t S = (size_t)g.L * g.N1;
-    launch_k(k_curl_flux<T>, dim3(nblk(S, 256), 1), 256, 0, st, g, C, N, S, (size_t)g.L * g.F1);
+    launch_k(k_curl_flux<T>, dim3(nblk(g.N1, 256), (unsigned)g.L, 1), 256, 0, st, g, C, N, S, (size_t)g.L * g.F1);
 }
 
 template <typename T>
 void launch_rhs(const GridDev& g, const T* w, const T* N, const T* Nprev, T* a, double c1, double an, double bn,
                 double dt, cudaStream_t st) {
-    const size_t S = (size_t)g.L * g.N1;
-    launch_k(k_rhs<T>, nblk(S, 256), 256, 0, st, g, w, N, Nprev, a, (T)c1, (T)an, (T)bn, (T)dt, 0);
+    launch_k(k_rhs<T>, dim3(nblk(g.N1, 256), (unsigned)g.L), 256, 0, st, g, w, N, Nprev, a, (T)c1, (T)an, (T)bn, (T)dt, 0);
 }
 
 template <typename T>
 void launch_laplacian(const GridDev& g, const T* w, T* out, cudaStream_t st) {
-    const size_t S = (size_t)g.L * g.N1;
-    launch_k(k_rhs<T>, nblk(S, 256), 256, 0, st, g, w, nullptr, nullptr, out, (T)0, (T)0, (T)0, (T)0, 1);
+    launch_k(k_rhs<T>, dim3(nblk(g.N1, 256), (unsigned)g.L), 256, 0, st, g, w, nullptr, nullptr, out, (T)0, (T)0, (T)0,
+             (T)0, 1);
 }
 
 // E applied to given level-0 fluxes (Regularizer::toBoundary)
@@ -936,8 +933,7 @@ void launch_reg_gather(const GridDev& g, int ncomp, const RegSlots& s, const dou
 template <typename T>
 void launch_refresh_flux(const GridDev& g, const T* psi, T* q, double u0, double v0, const double* q0f,
                          cudaStream_t st) {
-    const size_t F = (size_t)g.L * g.F1;
-    launch_k(k_refresh_flux<T>, nblk(F, 256), 256, 0, st, g, psi, q, u0, v0, q0f);
+    launch_k(k_refresh_flux<T>, dim3(nblk(g.F1, 256), (unsigned)g.L), 256, 0, st, g, psi, q, u0, v0, q0f);
 }
 
 void launch_flux_to_vel(const GridDev& g, const double* q, double* u, double* v, cudaStream_t st) {
