@@ -569,6 +569,9 @@ def main():
         it1 = run.iterations()
         solves = it1[1] - it0[1]
         cg = {"iterations_per_solve": (it1[0] - it0[0]) / max(1, solves), "solves": solves}
+        if hasattr(run, "s"):
+            _, mx, capped = run.s.cg_stats()
+            cg["max_iterations"], cg["solves_at_the_cap"] = mx, capped  # capped solves did not converge
 
     if args.profile:
         run.close()

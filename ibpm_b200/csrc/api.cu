@@ -1150,7 +1150,9 @@ int ibg_create(const ibg_grid* grid, int nbodies, const ibg_body* bodies, const 
     c->prm = *params;
     if (c->prm.cg_max_iter <= 0) c->prm.cg_max_iter = 3000;
     if (c->prm.pc_refresh <= 0) c->prm.pc_refresh = 10;
-    if (c->prm.pc_fallback_iter <= 0) c->prm.pc_fallback_iter = c->prm.cg_max_iter;
+    // a preconditioner that has not converged within a quarter of the iteration cap hands the solve to
+    // plain CG, which keeps the other three quarters (at the cap itself no iterations would be left)
+    if (c->prm.pc_fallback_iter <= 0) c->prm.pc_fallback_iter = std::max(1, c->prm.cg_max_iter / 4);
     if (c->prm.cg_precond == IBG_PRECOND_LEARNED && c->prm.pc_refresh <= 0) c->prm.pc_refresh = 10;
     if (c->prm.cg_precond < IBG_PRECOND_NONE || c->prm.cg_precond > IBG_PRECOND_LEARNED) {
         delete c;

@@ -96,7 +96,7 @@ typedef struct {
     int cg_graph;           /* moving bodies: 1 = the whole step, CG loop included, is one CUDA graph
                                (the loop is a device-side WHILE node), 0 = host-driven CG loop */
     int pc_fallback_iter;   /* LEARNED: iterations after which the solve restarts as plain CG
-                               (also when r.z <= 0); <= 0 means cg_max_iter */
+                               (also when r.z <= 0); <= 0 means cg_max_iter / 4 */
 } ibg_params;
 
 /* preconditioners of the moving-body force solve (all keep the reference's

@@ -188,3 +188,30 @@ def test_tensor_core_inference_matches_cuda_cores_and_oracle(case):
     z_tc2, _ = s.lpc_apply(0, r)
     assert np.array_equal(z_tc, z_tc2)
     s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fallback_iter", [0, 20])
+def test_a_useless_network_still_gives_the_references_forces(fallback_iter):
+    """A network with random weights: the flexible PCG falls back to plain CG (when r.z <= 0, or after
+    pc_fallback_iter iterations; 0 = a quarter of the iteration cap) and the solve still converges to
+    the reference's tolerance, no solve stopping at the cap."""
+    ib, d, grid, geo = _plate()
+    model = ib.NavierStokesModel(grid, geo, float(d["Re"]))
+    n = int(d["nsteps"])
+    s = ib.NonlinearIBSolver(grid, model, float(d["dt"]), "rk3", float(d["tol"]), precond="learned",
+                             pc_fallback_iter=fallback_iter)
+    p = s.lpc_params()
+    rng = np.random.default_rng(7)
+    p[:-1] = rng.standard_normal(len(p) - 1).astype(p.dtype) * 0.5
+    p[-1] = 1.0  # the operator scale c0
+    s.lpc_set_params(p)
+    x = ib.State(grid, geo.num_points, omega=np.array(d["omega0"], dtype=float))
+    s.init()
+    s.set_state(x, with_q=False)
+    s.advance_resident(n)
+    forces = s.force_history(n)
+    _, _, capped = s.cg_stats()
+    assert capped == 0
+    assert rel_l2(forces, d["forces"][:, 2:4]) < 1e-8
+    s.close()
