@@ -74,9 +74,9 @@ METRICS = {
 FORMS = {"c2": ("fp32_refined", "fp32", "fp64"), "c3": ("cholesky", "learned", "cg"),
          "c4": ("ensemble_fp32", "ensemble_refined", "ensemble", "serial"), "c5": ("cholesky", "learned", "cg")}
 PLAIN = {"c2": "fp64", "c3": "cg", "c4": "serial", "c5": "cg"}
-STEPS = {"c2": 200, "c3": 50, "c4": 60, "c5": 10}
+STEPS = {"c2": 200, "c3": 50, "c4": 60, "c5": 24}
 WARMUP = {"c2": 10, "c3": 3, "c4": 3, "c5": 3}
-PC_REFRESH = {"c3": 10, "c5": 12}
+PC_REFRESH = {"c3": 10, "c5": 24}  # one rebuild per timed window
 L2_NOTE = "flushed between timed steps (256 MB write outside the events)"
 
 
