@@ -495,7 +495,13 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off) "
                          "and skip the e2e, roofline, plain and CPU legs")
+    ap.add_argument("--kernel-probe", default=None, choices=["roofline", "gemm"],
+                    help="for ncu --profile-from-start off: run only the c4 roofline kernel (the largest member's "
+                         "FP32 column pass, members' launch shape) or four FP32 Poisson solves of a 256x256 grid "
+                         "with the sine-matrix GEMM passes, bracketed by cudaProfilerStart/Stop")
     args = ap.parse_args()
+    if args.kernel_probe:
+        return kernel_probe(args.kernel_probe)
     wlname = args.workload
     if args.steps is None:
         args.steps = STEPS[wlname]
@@ -662,6 +668,52 @@ def main():
         print(json.dumps(out))
     if ws > 1:
         dist.destroy_process_group()
+    return 0
+
+
+def kernel_probe(which):
+    """Launch one kernel family alone between cudaProfilerStart/Stop (for an ncu capture of just it)."""
+    import ctypes
+    import numpy as np
+    import torch
+    import ibpm_b200 as ib
+    from ibpm_b200 import configs, geometry
+    L = ib._native.lib()
+    if which == "roofline":
+        # the largest c4 member as a one-member ensemble (which applies the members' launch shape)
+        wl = max(configs.ensemble_members(count=64), key=lambda w: w.nx * w.ny * w.ngrid)
+        grid, model, s, x = ib.from_workload(wl, precision="fp32")
+        s.init()
+        s.set_state(x, with_q=False)
+        ens = ib.Ensemble([s])
+        ens.advance(2)
+        L.ibg_run_kernel(s.handle, 1, 1)
+        torch.cuda.synchronize()
+        torch.cuda.cudart().cudaProfilerStart()
+        nb = L.ibg_run_kernel(s.handle, 1, 3)
+        torch.cuda.synchronize()
+        torch.cuda.cudart().cudaProfilerStop()
+        print(json.dumps({"kernel_probe": which, "member": [wl.nx, wl.ny, wl.ngrid], "algorithmic_bytes": nb}))
+        ens.close()
+        s.close()
+        return 0
+    # four FP32 Poisson solves of a 256 x 256 single-level grid with the GEMM form of the DST passes
+    grid = ib.Grid(256, 256, 1, 4.0, -2.0, -2.0)
+    geo = geometry.parse(configs.cylinder_geom(24, r=0.3))
+    s = ib.NonlinearIBSolver(grid, ib.NavierStokesModel(grid, geo, 100.0), 0.01, "rk3", precision="fp32")
+    ib._native.check(L.ibg_set_dst_gemm(s.handle, 1), s.handle)
+    f = np.random.default_rng(0).standard_normal(grid.scalar().shape)
+    u = np.zeros_like(f)
+    fp, up = f.ctypes.data_as(ctypes.c_void_p), u.ctypes.data_as(ctypes.c_void_p)
+    ib._native.check(L.ibg_solve_fp32(s.handle, -1, fp, up), s.handle)
+    torch.cuda.synchronize()
+    torch.cuda.cudart().cudaProfilerStart()
+    for _ in range(4):
+        ib._native.check(L.ibg_solve_fp32(s.handle, -1, fp, up), s.handle)
+    torch.cuda.synchronize()
+    torch.cuda.cudart().cudaProfilerStop()
+    print(json.dumps({"kernel_probe": which, "grid": [256, 256, 1], "gemm_status": L.ibg_dst_gemm_status(s.handle)}))
+    s.close()
     return 0
 
 
