@@ -600,6 +600,7 @@ def main():
     info["autotuned_dst_shapes"] = ib.autotune_log()
     info["dst_form"] = ib.dst_form_log()
     info["sweep_form"] = ib.sweep_form_log()
+    info["fp64_pass_form"] = ib.pass_form_log()
     run.close()
 
     plain = None

@@ -447,6 +447,16 @@ def sweep_form_log():
     return [dict(zip(keys, (float(v) for v in buf[7 * k:7 * k + 7]))) for k in range(n)]
 
 
+def pass_form_log():
+    """The autotuner's choice of the FP64 DST passes' form (half length or odd extension) in this
+    process: one dict per grid shape timed."""
+    n = lib().ibg_pass_form_log(None, 0)
+    buf = np.zeros(6 * max(n, 1))
+    n = lib().ibg_pass_form_log(buf.ctypes.data_as(ctypes.c_void_p), n)
+    keys = ("nx", "ny", "levels", "half_length", "half_length_us", "odd_extension_us")
+    return [dict(zip(keys, (float(v) for v in buf[6 * k:6 * k + 6]))) for k in range(n)]
+
+
 def from_workload(wl, precision: str = "fp64", stream=None, device: int = -1, precond: str = "none",
                   pc_refresh: int = 10, cg_graph: bool = True, pc_fallback_iter: int = 0):
     """Grid, model, solver and initial State for an ibpm_b200.configs.Workload."""

@@ -146,6 +146,11 @@ namespace {
 std::mutex g_form_mu;
 std::map<std::array<int, 3>, std::array<double, 3>> g_form;
 
+// The autotuner's choice of the FP64 DST passes' form, once per grid shape: {nx, ny, levels} ->
+// {half length chosen, half-length us, odd-extension us} per whole Poisson solve.
+std::mutex g_pform_mu;
+std::map<std::array<int, 3>, std::array<double, 3>> g_pform;
+
 // The autotuner's choice between the coarse-to-fine sweep's edge maps and its per-step line FFTs (fused
 // into the sums launch), once per grid shape and precision: {nx, ny, levels, bytes per word} ->
 // {edge maps chosen, edge-map us, line-FFT us} per whole Poisson solve.
@@ -234,6 +239,36 @@ struct ibg_context {
         std::lock_guard<std::mutex> lock(g_form_mu);
         g_form[key] = {use ? 1.0 : 0.0, t_fft, t_gemm};
         return cuda_check("choose_dst_form");
+    }
+    // time whole FP64 solves with the half-length and with the odd-extension DST passes the first time a
+    // grid shape is created in the process; keep the half length unless the odd extension is at least 3 %
+    // faster (the half length saves an FFT stage and half the shared memory; its pre- and
+    // post-processing, a prefix scan among them, cost more than that saves on short lines)
+    int choose_pass_form(Bulk<double>& B) {
+        const std::array<int, 3> key = {g.nx, g.ny, g.L};
+        auto set = [&](bool h) -> int {
+            int e = B.poisson.set_half(h);
+            for (int k = 0; k < 4 && !e; ++k)
+                if (B.helm[k].grid) e = B.helm[k].set_half(h);
+            return e ? fail(IBG_ERR_CUDA, "DST pass form: shared-memory limit") : IBG_OK;
+        };
+        {
+            std::lock_guard<std::mutex> lock(g_pform_mu);
+            auto it = g_pform.find(key);
+            if (it != g_pform.end()) return set(it->second[0] > 0.5);
+        }
+        SolveCall<double> c = call<double>(B, B.a, B.ws, 1.0);
+        cudaMemsetAsync(B.a, 0, sizeof(double) * S, st);
+        int e = set(true);
+        if (e) return e;
+        const double t_half = time_solves<double>(B.poisson, c, st);
+        if ((e = set(false))) return e;
+        const double t_odd = time_solves<double>(B.poisson, c, st);
+        const bool half = !(t_odd < 0.97 * t_half);
+        if ((e = set(half))) return e;
+        std::lock_guard<std::mutex> lock(g_pform_mu);
+        g_pform[key] = {half ? 1.0 : 0.0, t_half, t_odd};
+        return cuda_check("choose_pass_form");
     }
     // time whole solves of plans B with the sweep's edge maps and with its fused line FFTs the first time
     // a grid shape is created in the process (per precision); keep the edge maps unless the line FFTs
@@ -397,7 +432,9 @@ struct ibg_context {
         }
         if (s) return IBG_ERR_CUDA;
         // time the DST passes' launch shapes for this grid once per process (before the plans read them)
-        s = tune_passes<T>(&g, &fft, cosT, call<T>(B, B.a, B.ws, (T)1), st);
+        s = tune_passes<T>(&g, &fft, cosT, call<T>(B, B.a, B.ws, (T)1), st, true);
+        if (!s && std::is_same<T, double>::value)  // FP64 passes have the odd-extension form too
+            s = tune_passes<T>(&g, &fft, cosT, call<T>(B, B.a, B.ws, (T)1), st, false);
         if (s) return s;
         s = B.poisson.init(&g, &fft, false, 0.0, cosT);
         for (int k = 0; k < sch.nsub && !s; ++k) {
@@ -418,6 +455,10 @@ struct ibg_context {
                 s = choose_dst_form();
                 if (s) return s;
             }
+        }
+        if constexpr (std::is_same<T, double>::value) {
+            s = choose_pass_form(B);
+            if (s) return s;
         }
         s = choose_sweep_form<T>(B);
         if (s) return s;
@@ -1995,6 +2036,20 @@ long long ibg_graph_kernel_nodes(ibg_context* c) {
 }
 
 long long ibg_graph_launch_claim(const ibg_context* c) { return c ? c->graph_launches : 0; }
+
+int ibg_pass_form_log(double* out, int max_rows) {
+    std::lock_guard<std::mutex> lock(g_pform_mu);
+    int r = 0;
+    for (const auto& kv : g_pform) {
+        if (out && r < max_rows) {
+            double* o = out + 6 * r;
+            for (int j = 0; j < 3; ++j) o[j] = kv.first[j];
+            for (int j = 0; j < 3; ++j) o[3 + j] = kv.second[j];
+        }
+        ++r;
+    }
+    return r;
+}
 
 int ibg_sweep_form_log(double* out, int max_rows) {
     std::lock_guard<std::mutex> lock(g_sweep_mu);

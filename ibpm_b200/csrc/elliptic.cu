@@ -389,11 +389,10 @@ __device__ void dst_post(const C* __restrict__ Z, C* __restrict__ O, int N, int 
 // (blockIdx.y = batch * nlev + level).  Inside a level's overlap interior
 // the input comes from `alt` (the coarsified right-hand side) when given.
 // ---------------------------------------------------------------------------
-template <typename T>
+template <typename T, bool H>
 __global__ void k_dst_rows(RowPassArgs<T> a) {
     pdl_enter();
     using C = typename Cplx<T>::type;
-    constexpr bool H = half_dst<T>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const FftDesc& d = a.fft;
     const int m = d.m;  // N = ny (half length) or 2 ny (odd extension)
@@ -517,11 +516,10 @@ __global__ void k_dst_rows(RowPassArgs<T> a) {
 // ---------------------------------------------------------------------------
 constexpr int kColLoads = 4;  // elements each thread of k_dst_cols loads before storing any
 
-template <typename T>
+template <typename T, bool H>
 __global__ void k_dst_cols(ColPassArgs<T> a) {
     pdl_enter();
     using C = typename Cplx<T>::type;
-    constexpr bool H = half_dst<T>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const FftDesc& d = a.fft;
     const int m = d.m;  // N = nx (half length) or 2 nx (odd extension)
@@ -690,6 +688,20 @@ __global__ void k_dst_cols(ColPassArgs<T> a) {
         const C z = O[(c >> 1) * m + i];
         buf[(size_t)i * NJ + col] = H ? ((c & 1) ? z.y : z.x) : ((c & 1) ? z.x : -z.y);
     }
+}
+
+// the pass kernels of a precision and DST form (the half-length form exists for FP64 only)
+template <typename T>
+const void* rows_kernel(bool half) {
+    if constexpr (half_dst<T>())
+        if (half) return (const void*)k_dst_rows<T, true>;
+    return (const void*)k_dst_rows<T, false>;
+}
+template <typename T>
+const void* cols_kernel(bool half) {
+    if constexpr (half_dst<T>())
+        if (half) return (const void*)k_dst_cols<T, true>;
+    return (const void*)k_dst_cols<T, false>;
 }
 
 // ---------------------------------------------------------------------------
@@ -1307,7 +1319,7 @@ void EllipticPlan<T>::launch_rows(const GridDev& g, const FftDesc& frow, int nle
     A.out_bstride = out_bs;
     A.in_scale = scale;
     A.norm = norm;
-    A.sinh = pass_sines<T>(*tables, 0);
+    A.sinh = psines(0);
     int P = pairs_per_block<T>(frow.m, g.NI, nlev, batch), nt = threads, tws = 0;
     if (batch == 1 && rows_P > 0) {
         P = rows_P;
@@ -1317,7 +1329,14 @@ void EllipticPlan<T>::launch_rows(const GridDev& g, const FftDesc& frow, int nle
     A.pairs_per_block = P;
     A.tw_smem = tws;
     const int npairs = (g.NI + 1) / 2;
-    launch_k(k_dst_rows<T>, dim3((unsigned)((npairs + P - 1) / P), (unsigned)(nlev * batch)), nt, fft_smem_bytes<T>(frow.m, P, tws), st, A);
+    const dim3 grid_((unsigned)((npairs + P - 1) / P), (unsigned)(nlev * batch));
+    const size_t smem = fft_smem_bytes<T>(frow.m, P, tws);
+    if constexpr (half_dst<T>())
+        if (half) {
+            launch_k(k_dst_rows<T, true>, grid_, nt, smem, st, A);
+            return;
+        }
+    launch_k(k_dst_rows<T, false>, grid_, nt, smem, st, A);
 }
 
 template <typename T>
@@ -1345,7 +1364,7 @@ void EllipticPlan<T>::launch_cols(const GridDev& g, const FftDesc& fcol, int mod
     B.alpha = (T)alpha;
     B.edges = edges;
     B.estride = estride;
-    B.sinh = pass_sines<T>(*tables, 1);
+    B.sinh = psines(1);
     B.elstride = 2 * (size_t)g.NI + 2 * (size_t)g.NJ;
     int P = pairs_per_block<T>(fcol.m, g.NJ, nlev, batch), nt = threads, tws = 0;
     if (batch == 1 && cols_P > 0) {
@@ -1356,7 +1375,14 @@ void EllipticPlan<T>::launch_cols(const GridDev& g, const FftDesc& fcol, int mod
     B.pairs_per_block = P;
     B.tw_smem = tws;
     const int ncolblk = (g.NJ + 2 * P - 1) / (2 * P);
-    launch_k(k_dst_cols<T>, dim3((unsigned)ncolblk, (unsigned)(nlev * batch)), nt, fft_smem_bytes<T>(fcol.m, P, tws), st, B);
+    const dim3 grid_((unsigned)ncolblk, (unsigned)(nlev * batch));
+    const size_t smem = fft_smem_bytes<T>(fcol.m, P, tws);
+    if constexpr (half_dst<T>())
+        if (half) {
+            launch_k(k_dst_cols<T, true>, grid_, nt, smem, st, B);
+            return;
+        }
+    launch_k(k_dst_cols<T, false>, grid_, nt, smem, st, B);
 }
 
 // the coarse-to-fine sweep of a solve: the boundary DSTs of levels L-2 .. 0 from the
@@ -1383,8 +1409,8 @@ void EllipticPlan<T>::run_sweep(const SolveCall<T>& c, const T* coef, cudaStream
         s.g = g;
         s.frow = frow;
         s.fcol = fcol;
-        s.frowh = pass_desc<T>(*tables, 0);
-        s.fcolh = pass_desc<T>(*tables, 1);
+        s.frowh = tables->rowh64;  // the sweep's line DSTs: half length in FP64 whatever the passes' form
+        s.fcolh = tables->colh64;
         s.sinr = pass_sines<T>(*tables, 0);
         s.sinc = pass_sines<T>(*tables, 1);
         s.buf = coef + (size_t)lev * N1;
@@ -1429,8 +1455,8 @@ int EllipticPlan<T>::solve(const SolveCall<T>& c, cudaStream_t st) const {
     const int batch = c.batch;
     if (batch < 1 || batch * L > 65535) return IBG_ERR_ARG;
     if (gemm && sines && c.tbuf2) return solve_gemm(c, st);
-    const FftDesc& frow = pass_desc<T>(*tables, 0);
-    const FftDesc& fcol = pass_desc<T>(*tables, 1);
+    const FftDesc& frow = pdesc(0);
+    const FftDesc& fcol = pdesc(1);
     const T norm = (T)(1.0 / (double)(2 * g.nx * 2 * g.ny));  // src/EllipticSolver2d.cc:80
     if (L == 1) {
         const T* in[1] = {c.f};
@@ -1599,8 +1625,8 @@ int EllipticPlan<T>::launches(bool coarsify) const {
 template <typename T>
 void EllipticPlan<T>::run_pass(int which, const T* in, T* tbuf, cudaStream_t st) const {
     const GridDev& g = *grid;
-    const FftDesc& frow = pass_desc<T>(*tables, 0);
-    const FftDesc& fcol = pass_desc<T>(*tables, 1);
+    const FftDesc& frow = pdesc(0);
+    const FftDesc& fcol = pdesc(1);
     const int L = g.L;
     const size_t N1 = g.N1;
     if (which == 0) {
@@ -1653,14 +1679,17 @@ std::vector<TuneResult> tune_log() {
 }
 
 template <typename T>
-int tune_passes(const GridDev* g, const FftTables* t, const CosTables& ct, const SolveCall<T>& call, cudaStream_t st) {
-    const FftDesc& frow = pass_desc<T>(*t, 0);
-    const FftDesc& fcol = pass_desc<T>(*t, 1);
+int tune_passes(const GridDev* g, const FftTables* t, const CosTables& ct, const SolveCall<T>& call, cudaStream_t st,
+                bool half) {
+    EllipticPlan<T> p;
+    p.half = half_dst<T>() && half;
+    p.tables = t;
+    const FftDesc& frow = p.pdesc(0);
+    const FftDesc& fcol = p.pdesc(1);
     int have_r, have_c, tmp, tmp2;
     tuned_config(sizeof(T), 0, frow.m, g->NI, g->L, have_r, tmp, tmp2);
     tuned_config(sizeof(T), 1, fcol.m, g->NJ, g->L, have_c, tmp, tmp2);
     if (have_r > 0 && have_c > 0) return IBG_OK;
-    EllipticPlan<T> p;
     int s = p.init(g, t, false, 0.0, ct);
     if (s) return s;
     cudaEvent_t e0, e1;
@@ -1702,7 +1731,7 @@ int tune_passes(const GridDev* g, const FftTables* t, const CosTables& ct, const
                     if (P == ruleP && nt == p.threads && tws == 0) continue;
                     const size_t smem = fft_smem_bytes<T>(m, P, tws);
                     if (smem > 200 * 1024) continue;
-                    const void* fn = pass == 0 ? (const void*)k_dst_rows<T> : (const void*)k_dst_cols<T>;
+                    const void* fn = pass == 0 ? rows_kernel<T>(p.half) : cols_kernel<T>(p.half);
                     if (raise_smem_limit(fn, (int)smem)) continue;
                     set(P, nt, tws);
                     float ms = 0.f;
@@ -1725,9 +1754,9 @@ int tune_passes(const GridDev* g, const FftTables* t, const CosTables& ct, const
 }
 
 template int tune_passes<double>(const GridDev*, const FftTables*, const CosTables&, const SolveCall<double>&,
-                                 cudaStream_t);
+                                 cudaStream_t, bool);
 template int tune_passes<float>(const GridDev*, const FftTables*, const CosTables&, const SolveCall<float>&,
-                                cudaStream_t);
+                                cudaStream_t, bool);
 
 template <typename T>
 int EllipticPlan<T>::init(const GridDev* g, const FftTables* t, bool helm, double a, const CosTables& ct) {
@@ -1738,20 +1767,30 @@ int EllipticPlan<T>::init(const GridDev* g, const FftTables* t, bool helm, doubl
     cos = &ct;
     threads = 128;
     if (g->L > kMaxLevels) return IBG_ERR_UNSUPPORTED;
-    const FftDesc& frow = pass_desc<T>(*t, 0);  // the passes' half-length FFTs
-    const FftDesc& fcol = pass_desc<T>(*t, 1);
     const int M = std::max(t->row64.m, t->col64.m);  // the sweep's odd-extension FFTs (the longest)
     if (fft_smem_bytes<T>(M, 1) > 200 * 1024 || sweep_smem_bytes<T>(*g, M) > 200 * 1024) return IBG_ERR_UNSUPPORTED;
-    // dynamic shared memory each kernel may need (static shared memory comes on top)
+    if (set_half(half)) return IBG_ERR_CUDA;
+    const int sweep_need = (int)sweep_smem_bytes<T>(*g, M);
+    if (raise_smem_limit((const void*)k_sweep_lines<T>, sweep_need) ||
+        raise_smem_limit((const void*)k_sweep_sums<T>, sweep_need))
+        return IBG_ERR_CUDA;
+    return IBG_OK;
+}
+
+// the form of the DST passes (half length or odd extension; FP64 only has both): the tuned launch
+// shapes of that form's FFT lengths and the kernels' shared-memory limits
+template <typename T>
+int EllipticPlan<T>::set_half(bool h) {
+    half = half_dst<T>() && h;
+    const GridDev* g = grid;
+    const FftDesc& frow = pdesc(0);
+    const FftDesc& fcol = pdesc(1);
     tuned_config(sizeof(T), 0, frow.m, g->NI, g->L, rows_P, rows_T, rows_tws);
     tuned_config(sizeof(T), 1, fcol.m, g->NJ, g->L, cols_P, cols_T, cols_tws);
+    // dynamic shared memory each kernel may need (static shared memory comes on top)
     const int rows_need = (int)std::min<size_t>(fft_smem_bytes<T>(frow.m, std::max(2, rows_P), 1), 200 * 1024);
     const int cols_need = (int)std::min<size_t>(fft_smem_bytes<T>(fcol.m, std::max(2, cols_P), 1), 200 * 1024);
-    const int sweep_need = (int)sweep_smem_bytes<T>(*g, M);
-    if (raise_smem_limit((const void*)k_dst_rows<T>, rows_need) ||
-        raise_smem_limit((const void*)k_dst_cols<T>, cols_need) ||
-        raise_smem_limit((const void*)k_sweep_lines<T>, sweep_need) ||
-        raise_smem_limit((const void*)k_sweep_sums<T>, sweep_need))
+    if (raise_smem_limit(rows_kernel<T>(half), rows_need) || raise_smem_limit(cols_kernel<T>(half), cols_need))
         return IBG_ERR_CUDA;
     return IBG_OK;
 }

@@ -276,6 +276,14 @@ struct EllipticPlan {
     // two zeroed device counters owned by the caller: with them (and batch 1) the per-step line FFTs
     // run inside the sums launch, by the last block of each direction; shared by the plans of one stream
     int* sweep_counters = nullptr;
+    // the passes' DST form: half-length FFTs (FP64 only) or the odd extension
+    bool half = sizeof(T) == 8;
+    int set_half(bool h);
+    const FftDesc& pdesc(int pass) const {
+        if (half) return pass == 0 ? tables->rowh64 : tables->colh64;
+        return sizeof(T) == 8 ? (pass == 0 ? tables->row64 : tables->col64) : (pass == 0 ? tables->row32 : tables->col32);
+    }
+    const T* psines(int pass) const { return half ? pass_sines<T>(*tables, pass) : nullptr; }
     // FP32 plans: the DST passes as sine-matrix GEMMs on the tensor cores (dst_gemm.cu) instead of FFTs
     bool gemm = false;
     const SineMats* sines = nullptr;
@@ -297,7 +305,8 @@ struct EllipticPlan {
 // autotuner of the row/column passes (elliptic.cu): time the launch shapes once per
 // (precision, pass, FFT length, line count, level count) in the process
 template <typename T>
-int tune_passes(const GridDev* g, const FftTables* t, const CosTables& ct, const SolveCall<T>& call, cudaStream_t st);
+int tune_passes(const GridDev* g, const FftTables* t, const CosTables& ct, const SolveCall<T>& call, cudaStream_t st,
+                bool half);
 void tuned_config(int wbytes, int pass, int m, int nlines, int nlev, int& P, int& nt, int& tws);
 struct TuneResult {
     int wbytes, pass, m, nlines, nlev, P, threads, tw_smem;

@@ -59,6 +59,11 @@ IBG_API int ibg_set_sweep_form(ibg_context* ctx, int edge_maps);
  * max_rows rows of 7 doubles {nx, ny, levels, bytes per word, edge maps chosen,
  * edge-map us, line-FFT us}; returns the number of shapes timed. */
 IBG_API int ibg_sweep_form_log(double* out, int max_rows);
+/* The autotuner's choice of the FP64 DST passes' form per grid shape (half-length FFTs or the odd
+ * extension, timed on whole Poisson solves when a shape is first created; the half length is kept
+ * unless the odd extension is at least 3 % faster): up to max_rows rows of 6 doubles {nx, ny, levels,
+ * half length chosen, half-length us, odd-extension us}; returns the number of shapes timed. */
+IBG_API int ibg_pass_form_log(double* out, int max_rows);
 /* The same for an ensemble's graph (against ibg_ensemble_launches_per_step). */
 IBG_API long long ibg_ensemble_kernel_nodes(const ibg_ensemble* ens);
 
