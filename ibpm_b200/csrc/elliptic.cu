@@ -801,9 +801,10 @@ __device__ __forceinline__ void sweep_lines_dir(const SweepArgs<T>& a, bool xdir
     const GridDev& g = a.g;
     const int NI = g.NI, NJ = g.NJ;
     const int n = xdir ? NI : NJ;
-    // the half-length DSTs in FP64, the odd-extension ones in FP32 (as the passes); a copy, so that the
-    // kernel parameters are not addressed through a run-time choice
-    const FftDesc d = half_dst<T>() ? (xdir ? a.fcolh : a.frowh) : (xdir ? a.fcol : a.frow);
+    // the passes' DST form (the half length exists in FP64 only); a copy, so that the kernel parameters
+    // are not addressed through a run-time choice
+    const bool H = half_dst<T>() && a.half;
+    const FftDesc d = H ? (xdir ? a.fcolh : a.frowh) : (xdir ? a.fcol : a.frow);
     const T* sines = xdir ? a.sinc : a.sinr;
     C* s0 = reinterpret_cast<C*>(smem);
     C* s1 = s0 + d.m;
@@ -819,7 +820,7 @@ __device__ __forceinline__ void sweep_lines_dir(const SweepArgs<T>& a, bool xdir
         v1[k] = __ldcg(sums + n + k);
     }
     __syncthreads();
-    if constexpr (half_dst<T>())
+    if (H)
         dst_pair_half<T>(d, sines, v0, v1, u0, u1, a.norm, s0, s1);
     else
         dst_pair_block<T>(d, n, v0, v1, u0, u1, a.norm, s0, s1);
@@ -836,7 +837,7 @@ __device__ __forceinline__ void sweep_lines_dir(const SweepArgs<T>& a, bool xdir
     }
     __syncthreads();
     T* Eo = a.edges_out + (size_t)b * a.estride + (xdir ? 0 : 2 * (size_t)NI);
-    if constexpr (half_dst<T>())
+    if (H)
         dst_pair_half<T>(d, sines, e0, e1, Eo, Eo + n, (T)1, s0, s1);
     else
         dst_pair_block<T>(d, n, e0, e1, Eo, Eo + n, (T)1, s0, s1);
@@ -1400,8 +1401,8 @@ void EllipticPlan<T>::run_sweep(const SolveCall<T>& c, const T* coef, cudaStream
     const size_t es = sweep_doubles(g.nx, g.ny, L);
     const size_t el = 2 * (size_t)g.NI + 2 * (size_t)g.NJ;
     const GridTables<T>& gt = tabs();
-    // the lines step's FFT length: half length in FP64, the odd extension in FP32 (sweep_lines_dir)
-    const int M = half_dst<T>() ? std::max(tables->rowh64.m, tables->colh64.m) : std::max(frow.m, fcol.m);
+    // the lines step's FFT length: the passes' form (sweep_lines_dir)
+    const int M = half ? std::max(tables->rowh64.m, tables->colh64.m) : std::max(frow.m, fcol.m);
     const size_t ssm = sweep_smem_bytes<T>(g, M);
     for (int lev = L - 1; lev >= 1; --lev) {
         const double dxl = lev_dx(g, lev);
@@ -1409,8 +1410,9 @@ void EllipticPlan<T>::run_sweep(const SolveCall<T>& c, const T* coef, cudaStream
         s.g = g;
         s.frow = frow;
         s.fcol = fcol;
-        s.frowh = tables->rowh64;  // the sweep's line DSTs: half length in FP64 whatever the passes' form
+        s.frowh = tables->rowh64;  // the sweep's line DSTs take the passes' form
         s.fcolh = tables->colh64;
+        s.half = half ? 1 : 0;
         s.sinr = pass_sines<T>(*tables, 0);
         s.sinc = pass_sines<T>(*tables, 1);
         s.buf = coef + (size_t)lev * N1;

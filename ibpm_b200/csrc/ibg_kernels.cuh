@@ -84,8 +84,9 @@ struct SweepArgs {
     GridDev g;
     FftDesc frow;                  // length 2 ny
     FftDesc fcol;                  // length 2 nx
-    FftDesc frowh;                 // length ny: the half-length DSTs of k_sweep_lines
+    FftDesc frowh;                 // length ny: the half-length DSTs of k_sweep_lines (FP64, half = 1)
     FftDesc fcolh;                 // length nx
+    int half;                      // the lines' DSTs by the half-length FFTs (else the odd extension)
     const T* sinr;                 // their pre-processing sines
     const T* sinc;
     const T* buf;                  // this level's forward coefficients (batch item 0)
