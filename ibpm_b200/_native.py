@@ -79,6 +79,7 @@ SIGNATURES = {
     "ibg_set_sweep_form": (_I, [_VP, _I]),
     "ibg_sweep_form_log": (_I, [_VP, _I]),
     "ibg_pass_form_log": (_I, [_VP, _I]),
+    "ibg_set_pass_form": (_I, [_VP, _I]),
     "ibg_autotune_log": (_I, [_VP, _I]),
     "ibg_set_linearized": (_I, [_VP, _I, _VP, _VP]),
     "ibg_set_sfd": (_I, [_VP, _D, _D, _VP]),

@@ -2065,6 +2065,16 @@ int ibg_sweep_form_log(double* out, int max_rows) {
     return r;
 }
 
+int ibg_set_pass_form(ibg_context* c, int half_length) {
+    if (!c) return IBG_ERR_ARG;
+    cudaStreamSynchronize(c->st);
+    int e = c->b64.poisson.grid ? c->b64.poisson.set_half(half_length != 0) : 0;
+    for (int k = 0; k < 4 && !e; ++k)
+        if (c->b64.helm[k].grid) e = c->b64.helm[k].set_half(half_length != 0);
+    c->drop_graph();
+    return e ? IBG_ERR_CUDA : IBG_OK;
+}
+
 int ibg_set_sweep_form(ibg_context* c, int edge_maps) {
     if (!c) return IBG_ERR_ARG;
     cudaStreamSynchronize(c->st);
@@ -2101,6 +2111,9 @@ int ibg_helmholtz_solve(ibg_context* c, double alpha, const double* f, double* u
     EllipticPlan<double> h;
     if (h.init(&c->g, &c->fft, true, alpha, c->cosT)) return c->fail(IBG_ERR_CUDA, "helmholtz plan");
     Bulk<double>& B = c->b64;
+    // the context's choices of the DST form and the sweep
+    if (h.set_half(B.poisson.half)) return c->fail(IBG_ERR_CUDA, "helmholtz plan");
+    h.edge_maps = B.poisson.edge_maps;
     cudaMemcpyAsync(B.a, f, sizeof(double) * c->S, cudaMemcpyHostToDevice, c->st);
     h.solve(c->call<double>(B, B.a, B.psi, 1.0), c->st);
     cudaMemcpyAsync(u, B.psi, sizeof(double) * c->S, cudaMemcpyDeviceToHost, c->st);

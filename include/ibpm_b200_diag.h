@@ -64,6 +64,9 @@ IBG_API int ibg_sweep_form_log(double* out, int max_rows);
  * unless the odd extension is at least 3 % faster): up to max_rows rows of 6 doubles {nx, ny, levels,
  * half length chosen, half-length us, odd-extension us}; returns the number of shapes timed. */
 IBG_API int ibg_pass_form_log(double* out, int max_rows);
+/* The form of every FP64 plan's DST passes and sweep lines: half_length = 1 the half-length FFTs, 0
+ * the odd extension; the step graph is recaptured.  Results agree to rounding. */
+IBG_API int ibg_set_pass_form(ibg_context* ctx, int half_length);
 /* The same for an ensemble's graph (against ibg_ensemble_launches_per_step). */
 IBG_API long long ibg_ensemble_kernel_nodes(const ibg_ensemble* ens);
 

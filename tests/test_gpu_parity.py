@@ -63,6 +63,23 @@ COMPILED_FFT_GRIDS = [(128, 192, 2, 4.0, -2.0, -3.0), (256, 200, 3, 4.0, -2.0, -
                       (500, 200, 2, 10.0, -5.0, -2.0), (384, 512, 2, 6.0, -3.0, -4.0), (1024, 128, 2, 8.0, -4.0, -0.5)]
 
 
+@pytest.mark.parametrize("gp", GRIDS + COMPILED_FFT_GRIDS[:2])
+@pytest.mark.parametrize("half", [0, 1])
+def test_both_fp64_dst_forms_match_oracle(gp, half):
+    """The FP64 passes and sweep lines in either DST form (half-length FFTs or the odd extension; a
+    context picks one per grid by timing) against the oracle's multi-domain solves."""
+    from oracle import ibpm_oracle as O
+    from ibpm_b200 import _native
+    g = O.Grid(*gp)
+    grid, model, s = _solver_for(gp, O.circle_points(0.0, 0.0, 0.2 * gp[3] / 2, 12))
+    assert _native.lib().ibg_set_pass_form(s.handle, half) == 0
+    rng = np.random.default_rng(gp[0] + 3 * gp[1] + half)
+    f = rng.standard_normal(g.scalar().shape)
+    assert rel_l2(s.poisson(f), O.EllipticSolver(g, "poisson").solve(f)) < OP_TOL
+    assert rel_l2(s.helmholtz(-0.0123, f), O.EllipticSolver(g, "helmholtz", -0.0123).solve(f)) < OP_TOL
+    s.close()
+
+
 @pytest.mark.parametrize("gp", COMPILED_FFT_GRIDS)
 def test_compiled_fft_lengths_match_oracle(gp):
     from oracle import ibpm_oracle as O
