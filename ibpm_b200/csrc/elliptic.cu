@@ -294,11 +294,11 @@ __device__ __forceinline__ C* fft_any(C* s0, C* s1, const C* tw, const FftDesc& 
 // Two forms of the DST-I of the passes, both with two real lines (a, b) packed
 // into one complex FFT:
 //
-// * odd extension (FP32 plans): the line's odd extension of length 2N,
+// * odd extension (FP32 plans, and FP64 plans where it is faster): the line's odd extension of length 2N,
 //   [0, f_1 .. f_n, 0, -f_n .. -f_1] (N = n + 1), is transformed and the DST is
 //   -Im (line a) and Re (line b) of outputs 1 .. n (the transform of an odd real
 //   sequence is imaginary: G_k = -2i sum_j f_j sin(pi j k / N)).
-// * half length (FP64 plans): with s_j = sin(pi j / N) (f_0 = 0) the sequence
+// * half length (FP64 plans where it is faster): with s_j = sin(pi j / N) (f_0 = 0) the sequence
 //   y_j = s_j (f_j + f_{N-j}) + (f_j - f_{N-j}) / 2 has DFT sums
 //   C_k = sum y_j cos(2 pi j k / N) and S_k = sum y_j sin(2 pi j k / N) with
 //     DST_{2m+1} = 2 S_{m+1}                  (the odd 0-based outputs)
@@ -310,9 +310,13 @@ __device__ __forceinline__ C* fft_any(C* s0, C* s1, const C* tw, const FftDesc& 
 //   sum adds the FFT's rounding of up to N/2 terms, sqrt(N) times the error of
 //   the odd-extension form.  In FP64 that is ~1e-14 relative; in FP32 it
 //   reached 7.7e-5 on the vorticity of a 10-step 256^2 run against 1.2e-5, so
-//   the FP32 plans keep the odd extension.
+//   the FP32 plans keep the odd extension.  An FP64 plan times both forms on whole
+//   solves when its context is created (EllipticPlan::set_half): the half length
+//   wins on long lines, the odd extension on short ones, where the half length's
+//   pre- and post-processing cost more than its saved radix stage.
 // Both forms return 2 sum_j f_j sin(pi j k / N), FFTW's RODFT00 scaling.
 // ---------------------------------------------------------------------------
+// whether a precision has the half-length form at all
 template <typename T>
 __host__ __device__ constexpr bool half_dst() { return sizeof(T) == 8; }
 

@@ -197,12 +197,7 @@ struct FftTables {
     int init(int m_rows, int m_cols);
     void release();
 };
-// the pass descriptor and sine table of a precision (rows: pass 0, columns: pass 1): the FP64
-// passes take the half-length DSTs, the FP32 passes the odd-extension ones (elliptic.cu)
-template <typename T>
-inline const FftDesc& pass_desc(const FftTables& t, int pass) {
-    return sizeof(T) == 8 ? (pass == 0 ? t.rowh64 : t.colh64) : (pass == 0 ? t.row32 : t.col32);
-}
+// the half-length DSTs' pre-processing sines of a precision (rows: pass 0, columns: pass 1; FP64 only)
 template <typename T>
 inline const T* pass_sines(const FftTables& t, int pass) {
     return sizeof(T) == 8 ? (const T*)(pass == 0 ? t.sin_row64 : t.sin_col64) : nullptr;
