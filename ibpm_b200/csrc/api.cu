@@ -507,12 +507,24 @@ struct ibg_context {
     }
 
     // one launch shape for every DST pass of every plan (pairs 0: the rule); the next step recaptures
-    void set_shapes(int pairs, int threads, bool edge_maps) {
+    // one launch shape for every plan's DST passes; fails (shape unchanged where refused) when a
+    // plan's passes would need more shared memory than a CTA may take
+    int set_shapes(int pairs, int threads, bool edge_maps) {
+        int st = IBG_OK;
         auto set = [&](auto& plan) {
+            const int P0 = plan.rows_P, T0 = plan.rows_T, C0 = plan.cols_P, U0 = plan.cols_T;
+            const int rt = plan.rows_tws, ct = plan.cols_tws;
             plan.rows_P = plan.cols_P = pairs;
             plan.rows_T = plan.cols_T = pairs > 0 ? threads : 0;
             plan.rows_tws = plan.cols_tws = 0;
             plan.edge_maps = edge_maps;
+            if (!plan.grid) return;
+            const int e = plan.raise_pass_limits();
+            if (e) {
+                plan.rows_P = P0, plan.rows_T = T0, plan.cols_P = C0, plan.cols_T = U0;
+                plan.rows_tws = rt, plan.cols_tws = ct;
+                if (!st) st = e;
+            }
         };
         set(b64.poisson);
         set(b32.poisson);
@@ -521,6 +533,7 @@ struct ibg_context {
             set(b32.helm[k]);
         }
         drop_graph();
+        return st;
     }
 
     void drop_graph() {
@@ -2604,6 +2617,7 @@ int ibg_ensemble_autotune(ibg_ensemble* e, int steps_per_trial, int* out, int ma
     std::vector<std::pair<int, int>> order;
     for (auto& kv : cls) order.push_back(kv.first);
     std::sort(order.begin(), order.end(), [](auto a, auto b) { return a.first * a.second > b.first * b.second; });
+    // (four pairs per CTA, 4/128 and 4/256, lost to 2/128 on the whole 64-member set: not tried here)
     const int cand[][2] = {{2, 128}, {1, 128}, {2, 256}, {1, 256}, {2, 96}};
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -2623,12 +2637,15 @@ int ibg_ensemble_autotune(ibg_ensemble* e, int steps_per_trial, int* out, int ma
         ms = v / steps_per_trial;
         return IBG_OK;
     };
-    auto set_class = [&](const std::vector<ibg_context*>& ms, int P, int T) {
+    auto set_class = [&](const std::vector<ibg_context*>& ms, int P, int T) -> int {
         cudaStreamSynchronize(e->st);
+        int r = IBG_OK;
         for (ibg_context* c : ms) {
             cudaStreamSynchronize(c->st);
-            c->set_shapes(P, T, false);
+            const int q = c->set_shapes(P, T, false);
+            if (q && !r) r = q;
         }
+        return r;
     };
     std::vector<EnsTune> log;
     double best_all = 0.0;
@@ -2639,7 +2656,7 @@ int ibg_ensemble_autotune(ibg_ensemble* e, int steps_per_trial, int* out, int ma
         double best = best_all;
         for (const auto& cd : cand) {
             if (cd[0] == 2 && cd[1] == 128) continue;
-            set_class(ms, cd[0], cd[1]);
+            if (set_class(ms, cd[0], cd[1])) continue;  // a shape too large for this grid class
             double t = 0.0;
             s = trial(t);
             if (s) break;
@@ -2650,7 +2667,8 @@ int ibg_ensemble_autotune(ibg_ensemble* e, int steps_per_trial, int* out, int ma
             }
         }
         if (s) break;
-        set_class(ms, bp, bt);
+        s = set_class(ms, bp, bt);
+        if (s) break;
         best_all = best;
         log.push_back({order[ci].first, order[ci].second, ms[0]->g.L, bp, bt, best});
     }
@@ -2671,13 +2689,15 @@ int ibg_ensemble_autotune(ibg_ensemble* e, int steps_per_trial, int* out, int ma
 }
 
 int ibg_ensemble_set_shapes(ibg_ensemble* e, int pairs_per_cta, int threads, int edge_maps) {
-    if (!e || pairs_per_cta < 0 || pairs_per_cta > 2 ||
+    if (!e || pairs_per_cta < 0 || pairs_per_cta > 4 || pairs_per_cta == 3 ||
         (pairs_per_cta > 0 && (threads < 32 || threads > 512 || threads % 32)))
         return IBG_ERR_ARG;
     cudaStreamSynchronize(e->st);
+    int st = IBG_OK;
     for (ibg_context* c : e->members) {
         cudaStreamSynchronize(c->st);
-        c->set_shapes(pairs_per_cta, threads, edge_maps != 0);
+        const int q = c->set_shapes(pairs_per_cta, threads, edge_maps != 0);
+        if (q && !st) st = q;
     }
     // the parent graph is rebuilt from the members' new captures at the next advance
     e->drop_host_graph();
@@ -2690,7 +2710,9 @@ int ibg_ensemble_set_shapes(ibg_ensemble* e, int pairs_per_cta, int threads, int
         e->err = "ibg_ensemble_set_shapes: graph creation failed";
         return IBG_ERR_CUDA;
     }
-    return IBG_OK;
+    if (st) e->err = "ibg_ensemble_set_shapes: the shape needs more shared memory than a CTA may take for some "
+                     "member; those members keep their previous shape";
+    return st;
 }
 
 int ibg_ensemble_destroy(ibg_ensemble* e) {

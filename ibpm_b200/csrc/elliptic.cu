@@ -1793,10 +1793,19 @@ int EllipticPlan<T>::set_half(bool h) {
     const FftDesc& fcol = pdesc(1);
     tuned_config(sizeof(T), 0, frow.m, g->NI, g->L, rows_P, rows_T, rows_tws);
     tuned_config(sizeof(T), 1, fcol.m, g->NJ, g->L, cols_P, cols_T, cols_tws);
-    // dynamic shared memory each kernel may need (static shared memory comes on top)
-    const int rows_need = (int)std::min<size_t>(fft_smem_bytes<T>(frow.m, std::max(2, rows_P), 1), 200 * 1024);
-    const int cols_need = (int)std::min<size_t>(fft_smem_bytes<T>(fcol.m, std::max(2, cols_P), 1), 200 * 1024);
-    if (raise_smem_limit(rows_kernel<T>(half), rows_need) || raise_smem_limit(cols_kernel<T>(half), cols_need))
+    return raise_pass_limits();
+}
+
+template <typename T>
+int EllipticPlan<T>::raise_pass_limits() const {
+    // dynamic shared memory each kernel may need (static shared memory comes on top): the shape's
+    // line pairs (the rule's two at least), with a twiddle copy where the tuned shape keeps one
+    const size_t rows_need = fft_smem_bytes<T>(pdesc(0).m, std::max(2, rows_P), rows_P > 2 ? rows_tws : 1);
+    const size_t cols_need = fft_smem_bytes<T>(pdesc(1).m, std::max(2, cols_P), cols_P > 2 ? cols_tws : 1);
+    const size_t cap = 200 * 1024;
+    if ((rows_P > 2 && rows_need > cap) || (cols_P > 2 && cols_need > cap)) return IBG_ERR_UNSUPPORTED;
+    if (raise_smem_limit(rows_kernel<T>(half), (int)std::min(rows_need, cap)) ||
+        raise_smem_limit(cols_kernel<T>(half), (int)std::min(cols_need, cap)))
         return IBG_ERR_CUDA;
     return IBG_OK;
 }

@@ -275,6 +275,9 @@ struct EllipticPlan {
     // the passes' DST form: half-length FFTs (FP64 only) or the odd extension
     bool half = sizeof(T) == 8;
     int set_half(bool h);
+    // raises the passes' dynamic shared-memory limits to what rows_P / cols_P line pairs need
+    // (at least two pairs); IBG_ERR_UNSUPPORTED when that is above 200 KiB
+    int raise_pass_limits() const;
     const FftDesc& pdesc(int pass) const {
         if (half) return pass == 0 ? tables->rowh64 : tables->colh64;
         return sizeof(T) == 8 ? (pass == 0 ? tables->row64 : tables->col64) : (pass == 0 ? tables->row32 : tables->col32);

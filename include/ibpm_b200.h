@@ -281,10 +281,12 @@ IBG_API int ibg_ensemble_advance_host(ibg_ensemble* ens, int nsteps, double* con
 /* kernels launched per ibg_ensemble_advance_host step (the members' steps plus their precision conversions) */
 IBG_API long long ibg_ensemble_host_launches_per_step(const ibg_ensemble* ens);
 IBG_API int ibg_ensemble_destroy(ibg_ensemble* ens);
-/* one launch shape for every member's DST passes: pairs_per_cta 0 (the rule-based default), 1 or 2
+/* one launch shape for every member's DST passes: pairs_per_cta 0 (the rule-based default), 1, 2 or 4
  * line pairs per CTA with `threads` threads; edge_maps 1 applies the precomputed sweep edge maps,
  * 0 the per-step line FFTs (the default for members).  The members' steps are recaptured at the next
- * ibg_ensemble_advance; results do not depend on the shape. */
+ * ibg_ensemble_advance; results do not depend on the shape.  IBG_ERR_UNSUPPORTED when a member's
+ * passes would need more than 200 KiB of shared memory with that shape (that member keeps its
+ * previous shape; the others take the new one). */
 IBG_API int ibg_ensemble_set_shapes(ibg_ensemble* ens, int pairs_per_cta, int threads, int edge_maps);
 /* Choose the members' DST launch shapes by timing the ensemble itself: for each class of members with
  * the same grid (largest first) every candidate shape (line pairs per CTA, threads: 2/128, 1/128,

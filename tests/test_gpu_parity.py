@@ -419,17 +419,19 @@ def test_ensemble_shapes_do_not_change_results():
         return s
 
     alone = make()
-    alone.advance_resident(6)
-    fa = alone.force_history(6)
+    alone.advance_resident(8)
+    fa = alone.force_history(8)
     a, b = make(), make()
     ens = ib.Ensemble([a, b])
     ens.advance(2)
     ens.set_shapes(2, 64, edge_maps=True)
     ens.advance(2)
+    ens.set_shapes(4, 256)
+    ens.advance(2)
     ens.set_shapes(0)
     ens.advance(2)
     for s in (a, b):
-        assert rel_l2(s.force_history(6), fa) < 1e-12
+        assert rel_l2(s.force_history(8), fa) < 1e-12
     with pytest.raises(ib.IbgError):
         ens.set_shapes(3, 128)
     ens.close()
