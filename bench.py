@@ -647,6 +647,13 @@ def main():
                "final_force": [float(last[0]), float(last[1])] if len(forces) else None}
         if wlname != "c4":
             out["grid_point_updates_per_s"] = value * run.wl.ngrid * (run.wl.nx - 1) * (run.wl.ny - 1)
+        else:
+            # every member advances once per ensemble step: (member-steps/s / members) x the nodes of
+            # all members' levels
+            from ibpm_b200 import configs
+            ms = configs.ensemble_members(count=args.members)
+            nodes = sum(w.ngrid * (w.nx - 1) * (w.ny - 1) for w in ms)
+            out["grid_point_updates_per_s"] = value / len(ms) * nodes
         if cg:
             out["cg"] = cg
         if plain:
