@@ -183,11 +183,11 @@ def rel_l2(a, b):
 # ---------------------------------------------------------------------------
 # CPU baseline: the reference's own code on the host cores (bounded samples)
 # ---------------------------------------------------------------------------
-def _c4_sample():
-    """(member index, workload) of the members the CPU samples: the first two with n <= 256
+def _c4_sample(count):
+    """(member index, workload) of the members the CPU samples: the first `count` with n <= 256
     (the larger members' CPU Cholesky set-up is minutes long)."""
     from ibpm_b200 import configs
-    return [(k, w) for k, w in enumerate(configs.ensemble_members()) if w.nx <= 256][:2]
+    return [(k, w) for k, w in enumerate(configs.ensemble_members()) if w.nx <= 256][:count]
 
 
 CPU_STEPS = {"c2": 10, "c3": 2, "c4": 3, "c5": 1}   # timed reference steps per sample (bounded CPU time)
@@ -195,12 +195,13 @@ CPU_WARMUP = {"c2": 3, "c3": 1, "c4": 3, "c5": 0}
 
 
 def cpu_baseline(wlname, steps=None, warmup=None):
-    """The reference on one host core over a bounded sample; returns (baseline dict, forces per
-    sampled run (W + K steps each), in member order for c4)."""
+    """The reference over a bounded sample: one simulation on one host core (the reference is
+    single-threaded), or for the c4 ensemble one member per usable core, side by side.  Returns
+    (baseline dict, forces per sampled run (W + K steps each), member indices of the c4 sample)."""
     from oracle import ref_runner
     if not ref_runner.available():
         return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
-                "sample": "unavailable: oracle/_ref/ref_driver not built"}, None
+                "sample": "unavailable: oracle/_ref/ref_driver not built"}, None, None
     cpu = ref_runner.host_cpu()
     n = steps or CPU_STEPS[wlname]
     w = CPU_WARMUP[wlname] if warmup is None else warmup
@@ -211,18 +212,18 @@ def cpu_baseline(wlname, steps=None, warmup=None):
         return ({"value": r["steps_per_s"], "unit": UNIT, "cores": 1, "kind": "reference",
                  "sample": f"{r['timed_steps']} {what} of the same workload after {w} warm-up steps, Cholesky "
                            f"set-up (init {r['init_s']:.1f} s) excluded, reference sources -Ofast + project DST-I "
-                           f"FFTW shim, 1 core of {cpu}"}, [r["forces"]])
-    tot_s, tot_n, names, forces = 0.0, 0, [], []
-    for k, wl in _c4_sample():
-        r = ref_runner.run(wl, f"c4_{wl.name}", steps=n, warmup=w)
-        tot_s += r["timed_steps"] / r["steps_per_s"]
-        tot_n += r["timed_steps"]
-        names.append(f"{k} ({wl.nx}^2, ngrid {wl.ngrid})")
-        forces.append(r["forces"])
-    return ({"value": tot_n / tot_s, "unit": UNIT, "cores": 1, "kind": "reference",
-             "sample": f"{n} RK3 steps after {w} warm-up steps each of members {', '.join(names)} (the first two "
-                       f"with n <= 256; larger members' CPU Cholesky set-up is too long to sample), Cholesky "
-                       f"set-up excluded, 1 core of {cpu}"}, forces)
+                           f"FFTW shim, 1 core of {cpu} (the reference is single-threaded)"}, [r["forces"]], None)
+    # the ensemble's members are independent simulations: one per usable core, side by side
+    sample = _c4_sample(len(ref_runner.usable_cpus()))
+    res = ref_runner.run_parallel([(wl, f"c4_{wl.name}") for _, wl in sample], steps=n, warmup=w)
+    value = sum(r["steps_per_s"] for r in res)
+    sizes = sorted({(wl.nx, wl.ngrid) for _, wl in sample})
+    return ({"value": value, "unit": UNIT, "cores": len(sample), "kind": "reference",
+             "sample": f"{n} RK3 steps after {w} warm-up steps each of members {[k for k, _ in sample]} (the first "
+                       f"{len(sample)} with n <= 256, grids (n, ngrid) {sizes}; larger members' CPU Cholesky set-up "
+                       f"is too long to sample), one member per core side by side, the value the sum of their "
+                       f"step rates; Cholesky set-up excluded, {len(sample)} cores of {cpu}"},
+            [r["forces"] for r in res], [k for k, _ in sample])
 
 
 def run_reference(args):
@@ -237,7 +238,7 @@ def run_reference(args):
     cap = {"c2": 20, "c3": 3, "c4": 3, "c5": 1}[wlname]
     steps = max(1, min(args.steps, cap))
     warm = min(args.warmup, {"c2": 10, "c3": 1, "c4": 3, "c5": 0}[wlname])
-    cb, _ = cpu_baseline(wlname, steps=steps, warmup=warm)
+    cb, _, _ = cpu_baseline(wlname, steps=steps, warmup=warm)
     v = cb["value"]
     out = {"metric": METRICS[wlname], "unit": UNIT, "n_gpus": args.gpus, "steps": steps, "warmup": warm,
            "value": v, "ms_per_step": 1000.0 / v, "higher_is_better": True,
@@ -660,9 +661,9 @@ def main():
             out["plain"] = plain
         if ws == 1 and not args.no_cpu_baseline:
             try:
-                cb, ref_forces = cpu_baseline(wlname)
+                cb, ref_forces, sample_idx = cpu_baseline(wlname)
                 if ref_forces is not None:
-                    mine = [forces] if wlname != "c4" else [forces[k] for k, _ in _c4_sample()]
+                    mine = [forces] if wlname != "c4" else [forces[k] for k in sample_idx]
                     errs = []
                     for a, b in zip(mine, ref_forces):
                         n = min(len(a), len(b))

@@ -3,9 +3,11 @@ with -Ofast and the FFTW shim) on a named workload and report steps/s.
 
 TEST AND BASELINE INFRASTRUCTURE ONLY: used by bench.py's CPU-baseline leg and
 its `--impl reference` arm, never by the product path.  The reference is
-single-threaded; one run uses one host core.  The Cholesky factors are cached
-with the reference's own save/load (src/IBSolver.cc:77-108) under
-oracle/_ref/cache/, so repeated samples time the steps, not the set-up.
+single-threaded; one run uses one host core (pinned with taskset to a core this
+process may use), and independent runs can go side by side on several cores
+(`run_parallel`).  The Cholesky factors are cached with the reference's own
+save/load (src/IBSolver.cc:77-108) under oracle/_ref/cache/, so repeated samples
+time the steps, not the set-up; runs with keep_cache=False remove their files.
 """
 from __future__ import annotations
 
@@ -41,9 +43,18 @@ def _write_inputs(wl, tag: str):
     return gpath, ic
 
 
-def run(wl, tag: str, steps: int, warmup: int = 1, timeout: float = 1800.0, cores: int = 1) -> dict:
-    """Run W + K steps of workload `wl`; returns the driver's JSON plus wall time
-    and the net force (x, y) after each of the W + K steps ("forces")."""
+def usable_cpus() -> list:
+    """The host cores this process may run on."""
+    try:
+        return sorted(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return list(range(os.cpu_count() or 1))
+
+
+def run(wl, tag: str, steps: int, warmup: int = 1, timeout: float = 1800.0, cpu=None,
+        keep_cache: bool = True) -> dict:
+    """Run W + K steps of workload `wl` on one core (`cpu`, default the first usable one); returns the
+    driver's JSON plus wall time and the net force (x, y) after each of the W + K steps ("forces")."""
     import numpy as np
     gpath, ic = _write_inputs(wl, tag)
     out_prefix = os.path.join(CACHE, tag + "_run")
@@ -53,21 +64,50 @@ def run(wl, tag: str, steps: int, warmup: int = 1, timeout: float = 1800.0, core
             "-tol", repr(wl.tol), "-cholesky_cache", os.path.join(CACHE, tag), "-out", out_prefix]
     if ic:
         args += ["-ic", ic]
-    if cores == 1:
-        args = ["taskset", "-c", "0"] + args if _has_taskset() else args
+    if _has_taskset():
+        args = ["taskset", "-c", str(usable_cpus()[0] if cpu is None else cpu)] + args
     t0 = time.time()
-    p = subprocess.run(args, capture_output=True, text=True, timeout=timeout, check=True)
-    wall = time.time() - t0
-    line = [l for l in p.stdout.splitlines() if l.startswith("{")][-1]
-    out = json.loads(line)
-    out["wall_s"] = wall
-    out["forces"] = np.loadtxt(out_prefix + ".forces").reshape(-1, 6)[:, 2:4]
-    for suffix in (".forces", "_final.bin"):
-        try:
-            os.remove(out_prefix + suffix)
-        except OSError:
-            pass
+    try:
+        p = subprocess.run(args, capture_output=True, text=True, timeout=timeout, check=True)
+        wall = time.time() - t0
+        line = [l for l in p.stdout.splitlines() if l.startswith("{")][-1]
+        out = json.loads(line)
+        out["wall_s"] = wall
+        out["forces"] = np.loadtxt(out_prefix + ".forces").reshape(-1, 6)[:, 2:4]
+    finally:
+        junk = [out_prefix + ".forces", out_prefix + "_final.bin"]
+        if not keep_cache:
+            junk += [gpath] + ([ic] if ic else [])
+            junk += [os.path.join(CACHE, f) for f in os.listdir(CACHE)
+                     if f.startswith(tag + "_") and f.endswith(".cholesky")]
+        for f in junk:
+            try:
+                os.remove(f)
+            except OSError:
+                pass
     return out
+
+
+def run_parallel(jobs, steps: int, warmup: int, timeout: float = 1800.0, keep_cache: bool = False) -> list:
+    """Independent runs side by side, one per usable core (at most as many at once as there are cores):
+    jobs = [(workload, tag), ...]; returns run()'s results in job order."""
+    import queue
+    from concurrent.futures import ThreadPoolExecutor
+    cpus = usable_cpus()[:max(1, len(jobs))]
+    free = queue.Queue()
+    for c in cpus:
+        free.put(c)
+
+    def one(wl, tag):
+        c = free.get()  # a core no other run holds
+        try:
+            return run(wl, tag, steps, warmup, timeout, c, keep_cache)
+        finally:
+            free.put(c)
+
+    with ThreadPoolExecutor(max_workers=len(cpus)) as ex:
+        futs = [ex.submit(one, wl, tag) for wl, tag in jobs]
+        return [f.result() for f in futs]
 
 
 def _has_taskset() -> bool:
